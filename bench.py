@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Benchmark of the GPU GRMHD block update (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--grid 128|64] [--impl ours|reference]
+
+Workload: the uniform magnetised box -- rho = 1, p = 0.1 (1 + 0.01 N(0,1)),
+v = 0, B = (0.5, 0.3, 0) + curl of a random vector potential (|k| <= 4,
+RMS 1e-2), flat tree metric (M = a = Q = 0), Gamma = 4/3, periodic,
+PLM-minmod + HLLD + constrained transport, RK2 at CFL 0.4, all FP64 in the
+reference-faithful form -- on a 128^3 grid of 8^3 patches of 16^3 cells
+(``--grid 64``: the 64^3 box of 4^3 patches).  Synthetic seeded data.
+
+A step is one full rk2integrator::step (dtcomp, two RK stages with ghost
+fill, con2prim, fluxes, CT and update, floors) over the whole grid,
+restarted every step from the seeded initial state (a device-to-device
+copy inside the timed region), so every step does the same work.
+
+value : zone-updates/s, inputs resident in HBM, device-timed with CUDA
+        events, max over ranks.  N > 1 runs one independent box per GPU
+        (weak scaling, no data-path collective).
+e2e   : same metric through the public API with host buffers: per step the
+        H2D copy of the state (U, W, Bf) from pinned memory, the step, and
+        the D2H copy of the new state.
+roofline : the flux kernel (k_flux, the largest share of the step),
+        algorithmic bytes per launch / its CUDA-event duration inside the
+        timed region, against the measured HBM copy bandwidth.
+cpu_baseline : the reference solver's own rk2integrator::step compiled from
+        its sources (oracle/_ref), on all host cores, on a 64^3 sample.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "black-hole-simulator_b200"))
+sys.path.insert(0, REPO)
+
+METRIC = "zone-updates/s"
+GAMMA = 4.0 / 3.0
+CFL = 0.4
+LO, HI = 10.0, 12.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--grid", type=int, default=128, choices=[64, 128])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    return ap.parse_args()
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clock sampling during the timed region
+class Clocks:
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if bus_id:
+            cmd += ["-i", bus_id]
+        try:
+            self.p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0])); mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def make_tree(nq, seed):
+    import bhgpu
+    from bhgpu import configs
+    from bhgpu.mesh import Quilt
+    q = Quilt([LO] * 3, [HI] * 3, nq, periodic=True)
+    tree = bhgpu.AmrTree(q.dom_l, q.dom_h, nq, M=0.0, a=0.0, Q=0.0, gm=GAMMA, periodic=True,
+                         limiter="minmod", quilt=q, init_floor=False)
+    W, Bf = configs.magnetised_box(q, seed=seed, gamma=GAMMA)
+    tree.load(W=W, Bf=Bf)
+    tree.prim_to_cons()
+    return tree
+
+
+# algorithmic bytes of one k_flux launch over the whole pool: for each of
+# the 3 directions and each patch, the primitives (8 doubles) of the
+# 20x16x16 cells the 4-point stencil touches, their (r, theta), the normal
+# face B of the 17x16x16 flux faces, and the 8 flux components written.
+def flux_alg_bytes(npatch):
+    per_dir = (20 * 16 * 16) * (8 + 2) * 8 + (17 * 16 * 16) * 8 + (17 * 16 * 16) * 8 * 8
+    return 3 * per_dir * npatch
+
+
+STEP_BYTES = 296   # algorithmic HBM bytes per zone-update of a whole RK2 step
+
+
+def cpu_reference_sample(threads):
+    """The reference's own rk2integrator::step on a 64^3 box (4^3 patches),
+    all host threads; returns (zone-updates/s, kind, sample)."""
+    import numpy as np
+    import oracle
+    from bhgpu import configs
+    from bhgpu.mesh import Quilt
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    q = Quilt([LO] * 3, [HI] * 3, 4, periodic=False)
+    W, Bf = configs.magnetised_box(q, seed=1, gamma=GAMMA)
+    orc = oracle.Oracle(0.0, 0.0, 0.0, GAMMA, limiter=1)
+    hp = oracle.HostPool(q.tables())
+    orc.geometry(hp)
+    hp.W[:] = W; hp.Bf[:] = Bf
+    for p in range(hp.npatch):
+        hp.U[p] = orc.ptoc(W[p], hp.rth[p, 0], hp.rth[p, 1])[0]
+    zones = 64 ** 3
+    if oracle.ref_available():
+        ref = oracle.RefSolver([LO] * 3, [HI] * 3, 4, 0.0, 0.0, 0.0, GAMMA)
+        times = []
+        for _ in range(3):
+            ref.put(hp)
+            t0 = time.perf_counter()
+            ref.step_native(CFL)
+            times.append(time.perf_counter() - t0)
+        t = statistics.median(times)
+        return zones / t, "reference", ("reference rk2integrator::step (its own OpenMP loops, outflow ghosts, "
+                                        f"van Leer) on the 64^3 box, median of 3 steps from the initial state, "
+                                        f"{t:.2f} s/step")
+    times = []
+    for _ in range(3):
+        h = hp.copy()
+        t0 = time.perf_counter()
+        orc.step(h, CFL)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    return zones / t, "port", f"C restatement step on the 64^3 box, median of 3 steps, {t:.2f} s/step"
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return 0
+    import numpy as np
+    import oracle
+    from bhgpu import configs
+    from bhgpu.mesh import Quilt
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    nq = 4
+    q = Quilt([LO] * 3, [HI] * 3, nq, periodic=False)
+    W, Bf = configs.magnetised_box(q, seed=1, gamma=GAMMA)
+    orc = oracle.Oracle(0.0, 0.0, 0.0, GAMMA, limiter=1)
+    hp = oracle.HostPool(q.tables())
+    orc.geometry(hp)
+    hp.W[:] = W; hp.Bf[:] = Bf
+    for p in range(hp.npatch):
+        hp.U[p] = orc.ptoc(W[p], hp.rth[p, 0], hp.rth[p, 1])[0]
+    zones = (nq * 16) ** 3
+    if oracle.ref_available():
+        ref = oracle.RefSolver([LO] * 3, [HI] * 3, nq, 0.0, 0.0, 0.0, GAMMA)
+        kind = "reference"
+
+        def one():
+            ref.put(hp)
+            ref.step_native(CFL)
+    else:
+        kind = "port"
+
+        def one():
+            orc.step(hp.copy(), CFL)
+    for _ in range(args.warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    t = time.perf_counter() - t0
+    value = zones * args.steps / t
+    sample = (f"each step: the {'reference rk2integrator::step' if kind == 'reference' else 'C restatement step'} "
+              f"on a 64^3 sample of the box (4^3 patches of 16^3, outflow ghosts, van Leer: the reference's "
+              f"own loop), restarted from the initial state")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": "magnetised box, reference CPU sample",
+                                                      "grid": "64^3", "patches": nq ** 3},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    rank, local_rank, world = env_rank()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+    import bhgpu
+    from bhgpu.solver import _p, _stream
+
+    nq = args.grid // 16
+    tree = make_tree(nq, seed=1)
+    zones = (nq * 16) ** 3
+    U0, W0, B0 = tree.U.clone(), tree.W.clone(), tree.Bf.clone()
+    L = bhgpu.lib
+    P = tree.params()
+    pool = C.byref(tree.pool)
+    dtp = _p(tree.dt)
+    ev_pairs = []
+    KL_PER_STEP = 15   # dt_init, dtcomp, 2 x (ghost_fill, prims, flux, emf, bfupdate, update), floors
+
+    def step(record=False):
+        s = _stream()
+        tree.U.copy_(U0); tree.W.copy_(W0); tree.Bf.copy_(B0)
+        L.bh_dtcomp(P, pool, CFL, dtp, s)
+        for stage in (0, 1):
+            L.bh_ghosts_prims(P, pool, s)
+            if record:
+                a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+                a.record(); L.bh_fluxcomp(P, pool, s); b.record()
+                ev_pairs.append((a, b))
+            else:
+                L.bh_fluxcomp(P, pool, s)
+            L.bh_emfcomp(pool, s)
+            L.bh_bfupdate(pool, dtp, s)
+            L.bh_update(P, pool, dtp, stage, s)
+        L.bh_floors(P, pool, s)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    tree.clear_error()
+    bus = None
+    try:
+        u = str(torch.cuda.get_device_properties(local_rank).uuid)
+        bus = u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        pass
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(bus)
+    t_start = torch.cuda.Event(enable_timing=True); t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record()
+    for _ in range(args.steps):
+        step(record=True)
+    t_end.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ck = clocks.stop()
+    ms = t_start.elapsed_time(t_end)
+    flux_ms = [a.elapsed_time(b) for a, b in ev_pairs]
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    err = tree.read_error()
+
+    # ---- end to end through the public API with host buffers --------------
+    pin = lambda x: x.cpu().pin_memory()
+    hU, hW, hB = pin(U0), pin(W0), pin(B0)
+    oU, oW, oB = torch.empty_like(hU).pin_memory(), torch.empty_like(hW).pin_memory(), torch.empty_like(hB).pin_memory()
+    rk = bhgpu.RK2Integrator(CFL)
+
+    def e2e_step():
+        tree.U.copy_(hU, non_blocking=True); tree.W.copy_(hW, non_blocking=True); tree.Bf.copy_(hB, non_blocking=True)
+        rk.step(tree, sync=False, check_domain=False)
+        oU.copy_(tree.U, non_blocking=True); oW.copy_(tree.W, non_blocking=True); oB.copy_(tree.Bf, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    b.record()
+    torch.cuda.synchronize()
+    te = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = float(te.item()) / args.e2e_steps
+    h2d = (hU.numel() + hW.numel() + hB.numel()) * 8
+    d2h = h2d
+
+    if rank == 0:
+        value = world * zones * args.steps / (ms_max / 1e3)
+        peak, peak_kind = measured_peaks()
+        flux_avg = statistics.mean(flux_ms) / 1e3
+        achieved = flux_alg_bytes(tree.npatch) / flux_avg / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"magnetised box {args.grid}^3: flat metric, periodic, PLM-minmod + HLLD + CT, "
+                                   f"RK2 CFL 0.4, reference-faithful FP64", "grid": f"{args.grid}^3",
+                       "patches": tree.npatch, "patch": "16^3 + 2 ghosts", "parallelism": f"replicas x{world}",
+                       "l2": "working set > L2 (inputs and outputs larger than 126 MB)",
+                       "restart": "each step restarts from the seeded state (D2D copy inside the timed region)"},
+            "e2e": {"value": world * zones / (e2e_ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": KL_PER_STEP * args.steps,
+            "roofline": {"bound": "hbm", "kernel": "k_flux", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "flux_ms_per_launch": flux_avg * 1e3,
+                         "step_frac": value / world * STEP_BYTES / (peak * 1e9)},
+            "clocks": ck,
+            "device_error_word": err,
+        }
+        if world == 1:
+            threads = os.cpu_count() or 1
+            v, kind, sample = cpu_reference_sample(threads)
+            line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,12 @@
+"""bhgpu -- B200 (sm_100a) GRMHD block update for black-hole-simulator.
+
+Hand-written CUDA kernels (libbhgpu.so, C ABI in include/bhgpu.h) behind a
+Python API named after the reference solver's C++ entry points.
+"""
+from ._lib import lib, LIB_PATH, BhError  # noqa: F401  (raises if the CUDA library is missing)
+from .mesh import Quilt, BLOCK, GHOST, CPN, NC, NF, NE  # noqa: F401
+from .solver import (Metric, State, Conserved, hlld, AmrTree, RK2Integrator, DomainError,  # noqa: F401
+                     BH_MINMOD, BH_VANLEER, BH_MC)
+from . import configs  # noqa: F401
+
+__version__ = "0.1.0"

@@ -1,0 +1,608 @@
+// bh_items.cuh -- the per-item work of every kernel (one cell, face, edge
+// or ghost cell), written once as __host__ __device__ functions.
+//
+// The __global__ kernels in bh_kernels.cu map their thread index to an
+// item and call these; the CPU check of the kernel logic
+// (tests/hostcheck) compiles the same functions for the host and runs
+// them in loops.  Items of one launch never depend on each other.
+#pragma once
+#include "bh_phys.cuh"
+
+namespace bh {
+
+struct KP {                 // kernel-side copy of bh_params
+    MP tree, cell;
+    double gamma, tol;
+    int limiter, maxiter;
+};
+inline KP kp_of(const bh_params* P) {
+    KP k;
+    k.tree = MP{P->M, P->a, P->Q};
+    k.cell = MP{P->cM, P->ca, P->cQ};
+    k.gamma = P->gamma; k.tol = P->tol; k.limiter = P->limiter; k.maxiter = P->maxiter;
+    return k;
+}
+
+struct Pool {               // kernel-side view of bh_pool
+    double *U, *W, *dU, *F, *Bf, *EMF, *rth;
+    const double* pgeo;
+    const int32_t* nbr;
+    int32_t* err;
+};
+inline Pool pool_of(const bh_pool* p) {
+    return Pool{p->U, p->W, p->dU, p->F, p->Bf, p->EMF, p->rth, p->pgeo, p->nbr, p->err};
+}
+
+BH_HD inline double* Uv(const Pool& P, int p, int v) { return P.U + ((size_t)p * 8 + v) * NC; }
+BH_HD inline double* Wv(const Pool& P, int p, int v) { return P.W + ((size_t)p * 8 + v) * NC; }
+BH_HD inline double* dUv(const Pool& P, int p, int v) { return P.dU + ((size_t)p * 8 + v) * NC; }
+BH_HD inline double* Fv(const Pool& P, int p, int d, int v) { return P.F + (((size_t)p * 3 + d) * 8 + v) * NF; }
+BH_HD inline double* Bfv(const Pool& P, int p, int d) { return P.Bf + ((size_t)p * 3 + d) * NF; }
+BH_HD inline double* Ev(const Pool& P, int p, int d) { return P.EMF + ((size_t)p * 3 + d) * NE; }
+BH_HD inline double rr(const Pool& P, int p, int l) { return P.rth[(size_t)p * 2 * NC + l]; }
+BH_HD inline double tt(const Pool& P, int p, int l) { return P.rth[((size_t)p * 2 + 1) * NC + l]; }
+
+BH_HD inline void load_prim(const Pool& P, int p, int l, Prim& w) {
+    w.rho = Wv(P, p, 0)[l]; w.eps = Wv(P, p, 1)[l];
+    for (int d = 0; d < 3; d++) { w.v[d] = Wv(P, p, 2 + d)[l]; w.B[d] = Wv(P, p, 5 + d)[l]; }
+}
+BH_HD inline void store_prim(const Pool& P, int p, int l, const Prim& w) {
+    Wv(P, p, 0)[l] = w.rho; Wv(P, p, 1)[l] = w.eps;
+    for (int d = 0; d < 3; d++) { Wv(P, p, 2 + d)[l] = w.v[d]; Wv(P, p, 5 + d)[l] = w.B[d]; }
+}
+BH_HD inline void load_cons(const Pool& P, int p, int l, Cons& c) {
+    c.D = Uv(P, p, 0)[l]; c.tau = Uv(P, p, 4)[l];
+    for (int d = 0; d < 3; d++) { c.S[d] = Uv(P, p, 1 + d)[l]; c.B[d] = Uv(P, p, 5 + d)[l]; }
+}
+BH_HD inline void store_cons(const Pool& P, int p, int l, const Cons& c) {
+    Uv(P, p, 0)[l] = c.D; Uv(P, p, 4)[l] = c.tau;
+    for (int d = 0; d < 3; d++) { Uv(P, p, 1 + d)[l] = c.S[d]; Uv(P, p, 5 + d)[l] = c.B[d]; }
+}
+BH_HD inline void lin_ijk(int l, int& i, int& j, int& k) {
+    i = l / (CPN * CPN) - GH; j = (l / CPN) % CPN - GH; k = l % CPN - GH;
+}
+BH_HD inline bool is_ghost(int i, int j, int k) {
+    return i < 0 || i >= BLK || j < 0 || j >= BLK || k < 0 || k >= BLK;
+}
+
+// item counts per patch
+constexpr int N_INT = BLK * BLK * BLK;   // interior cells
+constexpr int N_EDGE = 19 * 19 * 19;     // emfcomp, i,j,k in [-2,17)
+constexpr int N_BUP = 18 * 18 * 18;      // Bfupdate / maxdivB, i,j,k in [-1,17)
+constexpr int N_F2C = 19 * 19 * 19;      // f2cB, i,j,k in [-1,18)
+constexpr int N_STRIP = 6 * 2 * BLK * BLK;  // ghost strip cells
+
+// W = pvfs(r) with the cell's B kept; U = ptoc(W) (integrator.cpp:211-218,
+// grid.cpp:484-487, grid.cpp:349-353)
+BH_HD inline void floor_reset(const KP& k, const Pool& P, int p, int l, Prim& w, Cons& u) {
+    double r = rr(P, p, l), th = tt(P, p, l);
+    pvfs(r, w.rho, w.eps);
+    w.v[0] = w.v[1] = w.v[2] = 0.0;
+    Met mc;
+    met_comp(k.tree, r, th, mc);
+    if (!ptoc(k.gamma, mc, w, u)) flag(P.err, BH_ERR_DOMAIN);
+}
+
+// ctop of one cell with the tree metric, rkstg's fallback on failure
+BH_HD inline void recover_cell(const KP& k, const Pool& P, int p, int l, Prim& w, Cons& u, bool& dirty) {
+    Met mc;
+    met_comp(k.tree, rr(P, p, l), tt(P, p, l), mc);
+    Prim pv;
+    bool dom = false;
+    int ok = ctop(k.gamma, k.maxiter, k.tol, mc, u, pv, dom);
+    if (dom) flag(P.err, BH_ERR_DOMAIN);
+    if (ok) w = pv;
+    else { floor_reset(k, P, p, l, w, u); dirty = true; }
+}
+
+// ctop of one ghost cell as amrtree::ghosts does it (grid.cpp:538-570): on
+// failure only rho and eps take the floor values, v and B stay, U = ptoc(W)
+BH_HD inline void ghost_recover(const KP& kp, const Pool& P, int p, int l, Prim& w, Cons& u, bool& dirty) {
+    double r = rr(P, p, l), th = tt(P, p, l);
+    Met mc;
+    met_comp(kp.tree, r, th, mc);
+    Prim pv;
+    bool dom = false;
+    int ok = ctop(kp.gamma, kp.maxiter, kp.tol, mc, u, pv, dom);
+    if (dom) flag(P.err, BH_ERR_DOMAIN);
+    if (ok) { w = pv; return; }
+    pvfs(r, w.rho, w.eps);
+    if (!ptoc(kp.gamma, mc, w, u)) flag(P.err, BH_ERR_DOMAIN);
+    dirty = true;
+}
+
+// ---- geometry: patch::cell_init (grid.cpp:149-175) ---------------------
+BH_HD inline void geometry_item(const Pool& P, int p, int l) {
+    int i, j, k;
+    lin_ijk(l, i, j, k);
+    const double* g = P.pgeo + 6 * p;
+    double xc = g[0] + (i + 0.5) * g[3];
+    double yc = g[1] + (j + 0.5) * g[4];
+    double zc = g[2] + (k + 0.5) * g[5];
+    double r = sqrt(xc * xc + yc * yc + zc * zc);
+    if (r < 1e-10) r = 1e-10;
+    double th = acos(smax(-1.0, smin(1.0, zc / r)));
+    P.rth[(size_t)p * 2 * NC + l] = r;
+    P.rth[((size_t)p * 2 + 1) * NC + l] = th;
+}
+
+// ---- face index of patch::fluxcomp's loops (grid.cpp:258-328) ------------
+BH_HD inline void face_ijk(int dim, int f, int& i, int& j, int& k) {
+    if (dim == 0) { i = f / 256 - 1; j = (f / 16) % 16; k = f % 16; }
+    else if (dim == 1) { i = f / (17 * 16); j = (f / 16) % 17 - 1; k = f % 16; }
+    else { i = f / (16 * 17); j = (f / 17) % 16; k = f % 17 - 1; }
+}
+
+// reconfp (reconstruction.cpp:40-97) for the face between cells (i,j,k)
+// and (i,j,k)+e_dim of patch p
+BH_HD inline void reconfp(const KP& kp, const Pool& P, int p, int i, int j, int k, int dim, int lim, Prim& L,
+                          Prim& R) {
+    int di = dim == 0, dj = dim == 1, dk = dim == 2;
+    int lm = lindx(i - di, j - dj, k - dk), lc = lindx(i, j, k);
+    int lp = lindx(i + di, j + dj, k + dk), lpp = lindx(i + 2 * di, j + 2 * dj, k + 2 * dk);
+    const double* Wr = Wv(P, p, 0);
+    recon_scal(log(Wr[lm]), log(Wr[lc]), log(Wr[lp]), log(Wr[lpp]), lim, L.rho, R.rho);
+    L.rho = exp(L.rho); R.rho = exp(R.rho);
+    const double* We = Wv(P, p, 1);
+    recon_scal(log(We[lm]), log(We[lc]), log(We[lp]), log(We[lpp]), lim, L.eps, R.eps);
+    L.eps = exp(L.eps); R.eps = exp(R.eps);
+    for (int d = 0; d < 3; d++) {
+        const double* x = Wv(P, p, 2 + d);
+        recon_scal(x[lm], x[lc], x[lp], x[lpp], lim, L.v[d], R.v[d]);
+    }
+    Met mL, mR;
+    met_comp(kp.cell, rr(P, p, lc), tt(P, p, lc), mL);
+    met_comp(kp.cell, rr(P, p, lp), tt(P, p, lp), mR);
+    causalv(L.v, mL);
+    causalv(R.v, mR);
+    for (int d = 0; d < 3; d++) {
+        const double* x = Wv(P, p, 5 + d);
+        if (d == dim) { L.B[d] = x[lc]; R.B[d] = x[lp]; }
+        else recon_scal(x[lm], x[lc], x[lp], x[lpp], lim, L.B[d], R.B[d]);
+    }
+}
+
+BH_HD inline void reconfp_item(const KP& kp, const Pool& P, int p, int dim, int f, int lim, int64_t n, double* Lo,
+                               double* Ro) {
+    int i, j, k;
+    face_ijk(dim, f, i, j, k);
+    Prim L, R;
+    reconfp(kp, P, p, i, j, k, dim, lim, L, R);
+    int64_t q = (int64_t)p * NFACE + f;
+    Lo[q] = L.rho; Lo[n + q] = L.eps; Ro[q] = R.rho; Ro[n + q] = R.eps;
+    for (int d = 0; d < 3; d++) {
+        Lo[(2 + d) * n + q] = L.v[d]; Lo[(5 + d) * n + q] = L.B[d];
+        Ro[(2 + d) * n + q] = R.v[d]; Ro[(5 + d) * n + q] = R.B[d];
+    }
+}
+
+// one face of patch::fluxcomp (grid.cpp:255-329)
+BH_HD inline void flux_item(const KP& kp, const Pool& P, int p, int dim, int f) {
+    int i, j, k;
+    face_ijk(dim, f, i, j, k);
+    Prim L, R;
+    reconfp(kp, P, p, i, j, k, dim, kp.limiter, L, R);
+    double bn;
+    int fi;
+    if (dim == 0) { bn = Bfv(P, p, 0)[xfc(i + 1, j, k)]; fi = xfc(i, j, k); }
+    else if (dim == 1) { bn = Bfv(P, p, 1)[yfc(i, j + 1, k)]; fi = yfc(i, j, k); }
+    else { bn = Bfv(P, p, 2)[zfc(i, j, k + 1)]; fi = zfc(i, j, k); }
+    L.B[dim] = bn; R.B[dim] = bn;
+    int lL = lindx(i, j, k), lR = lindx(i + (dim == 0), j + (dim == 1), k + (dim == 2));
+    double rf = (rr(P, p, lL) + rr(P, p, lR)) / 2;
+    double thf = (tt(P, p, lL) + tt(P, p, lR)) / 2;
+    Met mc;
+    met_comp(kp.tree, rf, thf, mc);
+    Cons UL, UR;
+    bool ok = ptoc(kp.gamma, mc, L, UL);
+    ok &= ptoc(kp.gamma, mc, R, UR);
+    double F[8], cts;
+    ok &= hlld(kp.gamma, mc, L, R, UL, UR, 0 /* every call site passes dim 0 */, F, cts);
+    if (!ok) flag(P.err, BH_ERR_DOMAIN);
+    for (int v = 0; v < 8; v++) Fv(P, p, dim, v)[fi] = F[v];
+}
+
+// ---- constrained transport (transport.cpp) ----------------------------
+BH_HD inline void emf_item(const Pool& P, int p, int e) {                // emfcomp :11-36
+    int i = e / 361 - 2, j = (e / 19) % 19 - 2, k = e % 19 - 2;
+    const double *FxB1 = Fv(P, p, 0, 6), *FxB2 = Fv(P, p, 0, 7);
+    const double *FyB0 = Fv(P, p, 1, 5), *FyB2 = Fv(P, p, 1, 7);
+    const double *FzB0 = Fv(P, p, 2, 5), *FzB1 = Fv(P, p, 2, 6);
+    Ev(P, p, 0)[exi(i, j, k)] = (FyB2[yfc(i, j, k)] + FyB2[yfc(i, j, k + 1)] - FzB1[zfc(i, j, k)] - FzB1[zfc(i, j + 1, k)]) / 4;
+    Ev(P, p, 1)[eyi(i, j, k)] = (FzB0[zfc(i, j, k)] + FzB0[zfc(i + 1, j, k)] - FxB2[xfc(i, j, k)] - FxB2[xfc(i, j, k + 1)]) / 4;
+    Ev(P, p, 2)[ezi(i, j, k)] = (FxB1[xfc(i, j, k)] + FxB1[xfc(i, j + 1, k)] - FyB0[yfc(i, j, k)] - FyB0[yfc(i + 1, j, k)]) / 4;
+}
+
+BH_HD inline void bfupdate_item(const Pool& P, int p, int e, double dt) {  // Bfupdate :38-58
+    int i = e / 324 - 1, j = (e / 18) % 18 - 1, k = e % 18 - 1;
+    const double* g = P.pgeo + 6 * p;
+    double dx = g[3], dy = g[4], dz = g[5];
+    const double *Ex = Ev(P, p, 0), *Ey = Ev(P, p, 1), *Ez = Ev(P, p, 2);
+    double dEz_dy = (Ez[ezi(i, j, k)] - Ez[ezi(i, j - 1, k)]) / dy;
+    double dEy_dz = (Ey[eyi(i, j, k)] - Ey[eyi(i, j, k - 1)]) / dz;
+    Bfv(P, p, 0)[xfc(i, j, k)] += dt * (dEz_dy - dEy_dz);
+    double dEz_dx = (Ez[ezi(i, j, k)] - Ez[ezi(i - 1, j, k)]) / dx;
+    double dEx_dz = (Ex[exi(i, j, k)] - Ex[exi(i, j, k - 1)]) / dz;
+    Bfv(P, p, 1)[yfc(i, j, k)] += dt * (dEx_dz - dEz_dx);
+    double dEy_dx = (Ey[eyi(i, j, k)] - Ey[eyi(i - 1, j, k)]) / dx;
+    double dEx_dy = (Ex[exi(i, j, k)] - Ex[exi(i, j - 1, k)]) / dy;
+    Bfv(P, p, 2)[zfc(i, j, k)] += dt * (dEy_dx - dEx_dy);
+}
+
+BH_HD inline double maxdivb_item(const Pool& P, int p, int e) {        // maxdivB :77-89
+    int i = e / 324 - 1, j = (e / 18) % 18 - 1, k = e % 18 - 1;
+    const double* g = P.pgeo + 6 * p;
+    double dx = g[3], dy = g[4], dz = g[5];
+    const double *Bx = Bfv(P, p, 0), *By = Bfv(P, p, 1), *Bz = Bfv(P, p, 2);
+    double divB = (Bx[xfc(i, j, k)] - Bx[xfc(i - 1, j, k)]) / dx + (By[yfc(i, j, k)] - By[yfc(i, j - 1, k)]) / dy +
+                  (Bz[zfc(i, j, k)] - Bz[zfc(i, j, k - 1)]) / dz;
+    return fabs(divB);
+}
+
+// f2cB (:60-75) for one cell: the face-averaged B and the cell's sqrt(-g)
+BH_HD inline void f2cb_cell(const KP& kp, const Pool& P, int p, int i, int j, int k, double B[3], double& sg) {
+    const double *Bx = Bfv(P, p, 0), *By = Bfv(P, p, 1), *Bz = Bfv(P, p, 2);
+    B[0] = (Bx[xfc(i, j, k)] + Bx[xfc(i - 1, j, k)]) / 2;
+    B[1] = (By[yfc(i, j, k)] + By[yfc(i, j - 1, k)]) / 2;
+    B[2] = (Bz[zfc(i, j, k)] + Bz[zfc(i, j, k - 1)]) / 2;
+    int l = lindx(i, j, k);
+    Met mc;
+    met_comp(kp.cell, rr(P, p, l), tt(P, p, l), mc);
+    sg = mc.sqrtdetg;
+}
+
+BH_HD inline void f2cb_item(const KP& kp, const Pool& P, int p, int e) {
+    int i = e / 361 - 1, j = (e / 19) % 19 - 1, k = e % 19 - 1;
+    double B[3], sg;
+    f2cb_cell(kp, P, p, i, j, k, B, sg);
+    int l = lindx(i, j, k);
+    for (int d = 0; d < 3; d++) { Wv(P, p, 5 + d)[l] = B[d]; Uv(P, p, 5 + d)[l] = sg * B[d]; }
+}
+
+// ---- div_flux + source (integrator.cpp:18-153) -------------------------
+BH_HD inline void div_flux(const Pool& P, int p, int i, int j, int k, double sg, double out[8]) {
+    const double* g = P.pgeo + 6 * p;
+    double dx = g[3], dy = g[4], dz = g[5];
+    int xr = xfc(i, j, k), xl = xfc(i - 1, j, k);
+    int yr = yfc(i, j, k), yl = yfc(i, j - 1, k);
+    int zr = zfc(i, j, k), zl = zfc(i, j, k - 1);
+    for (int v = 0; v < 5; v++) {
+        const double *Fx = Fv(P, p, 0, v), *Fy = Fv(P, p, 1, v), *Fz = Fv(P, p, 2, v);
+        out[v] = -((Fx[xr] - Fx[xl]) / dx + (Fy[yr] - Fy[yl]) / dy + (Fz[zr] - Fz[zl]) / dz) / sg;
+    }
+    out[5] = out[6] = out[7] = 0.0;
+}
+
+// geometric source (:41-153) with the full cell metric; false where the EOS throws
+BH_HD inline bool source(const KP& kp, const MetFull& mc, const Prim& W, double out[8]) {
+    double gam[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) gam[i][j] = mc.g[i + 1][j + 1];
+    double v2 = 0.0, vlow[3] = {0, 0, 0}, Blow[3] = {0, 0, 0};
+    for (int m = 0; m < 3; m++) {
+        for (int n = 0; n < 3; n++) {
+            vlow[m] += gam[m][n] * W.v[n];
+            Blow[m] += gam[m][n] * W.B[n];
+        }
+        v2 += vlow[m] * W.v[m];
+    }
+    v2 = smin(v2, 1 - 1e-10);
+    double ltz2 = 1.0 / (1.0 - v2);
+    double ltz = sqrt(ltz2);
+    double Bv = 0.0, Bsq = 0.0;
+    for (int m = 0; m < 3; m++) { Bv += Blow[m] * W.v[m]; Bsq += Blow[m] * W.B[m]; }
+    double b2 = Bv * Bv + Bsq / ltz2;
+    bool ok = eos_ok(W.rho);
+    double px = press(kp.gamma, W.rho, W.eps);
+    double h = enth(kp.gamma, W.eps);
+    double u4[4], b4[4];
+    u4[0] = ltz / mc.alpha;
+    for (int m = 0; m < 3; m++) u4[m + 1] = ltz * (W.v[m] - mc.beta[m] / mc.alpha);
+    b4[0] = ltz * Bv / mc.alpha;
+    for (int m = 0; m < 3; m++) b4[m + 1] = (W.B[m] + mc.alpha * b4[0] * u4[m + 1]) / ltz;
+    double T44[4][4];
+    double rhohb2 = W.rho * h + b2;
+    for (int m = 0; m < 4; m++)
+        for (int n = 0; n < 4; n++) T44[m][n] = rhohb2 * u4[m] * u4[n] + px * mc.gi[m][n] - b4[m] * b4[n];
+    double src[4];
+    for (int m = 0; m < 4; m++) {
+        double acc = 0.0;
+        for (int n = 0; n < 4; n++)
+            for (int q = 0; q < 4; q++) {
+                double G_ = 0.0;   // lowered Christoffel g[m][s] Gamma[s][n][q], summed over s
+                for (int s = 0; s < 4; s++) G_ += mc.g[m][s] * mc.G[s][n][q];
+                acc += T44[n][q] * G_;
+            }
+        src[m] = acc * mc.sqrtdetg;
+    }
+    out[0] = 0.0;
+    out[4] = src[0];
+    out[1] = src[1]; out[2] = src[2]; out[3] = src[3];
+    out[5] = out[6] = out[7] = 0.0;
+    return ok;
+}
+
+BH_HD inline void div_source_item(const KP& kp, const Pool& P, int p, int c, double* dv, double* sv) {
+    int i = c / 256, j = (c / 16) % 16, k = c % 16;
+    int l = lindx(i, j, k);
+    MetFull mf;
+    met_full(kp.cell, rr(P, p, l), tt(P, p, l), mf);
+    double d8[8], s8[8];
+    div_flux(P, p, i, j, k, mf.sqrtdetg, d8);
+    Prim w;
+    load_prim(P, p, l, w);
+    if (!source(kp, mf, w, s8)) flag(P.err, BH_ERR_DOMAIN);
+    for (int v = 0; v < 8; v++) {
+        dv[((size_t)p * 8 + v) * NC + l] = d8[v];
+        sv[((size_t)p * 8 + v) * NC + l] = s8[v];
+    }
+}
+
+// f2cB + the conserved update of rkstg (integrator.cpp:325-347), fused:
+// cells in [-1,18)^3 take the face-averaged B; interior cells then add
+// dt * (div_flux + source) and refresh U.B = sqrt(-g) W.B
+BH_HD inline void update_item(const KP& kp, const Pool& P, int p, int e, double dt, int stage) {
+    int i = e / 361 - 1, j = (e / 19) % 19 - 1, k = e % 19 - 1;
+    double B[3], sg;
+    f2cb_cell(kp, P, p, i, j, k, B, sg);
+    int l = lindx(i, j, k);
+    for (int d = 0; d < 3; d++) Wv(P, p, 5 + d)[l] = B[d];
+    if (is_ghost(i, j, k)) {
+        for (int d = 0; d < 3; d++) Uv(P, p, 5 + d)[l] = sg * B[d];
+        return;
+    }
+    MetFull mf;
+    met_full(kp.cell, rr(P, p, l), tt(P, p, l), mf);
+    double d8[8], s8[8];
+    div_flux(P, p, i, j, k, mf.sqrtdetg, d8);
+    Prim w;
+    load_prim(P, p, l, w);
+    if (!source(kp, mf, w, s8)) flag(P.err, BH_ERR_DOMAIN);
+    for (int v = 0; v < 5; v++) {
+        double dU = d8[v] + s8[v];
+        double u = Uv(P, p, v)[l];
+        if (stage == 0) {
+            dUv(P, p, v)[l] = u;
+            Uv(P, p, v)[l] = u + dU * dt;
+        } else {
+            Uv(P, p, v)[l] = (dUv(P, p, v)[l] + u + dU * dt) * 0.5;
+        }
+    }
+    if (stage == 0)   // c.dU = c.U after f2cB has set U.B = sqrt(-g) W.B
+        for (int d = 0; d < 3; d++) dUv(P, p, 5 + d)[l] = sg * B[d];
+    for (int d = 0; d < 3; d++) Uv(P, p, 5 + d)[l] = mf.sqrtdetg * B[d];
+}
+
+// ---- ghost fill: amrtree::ghosts (grid.cpp:390-571) ---------------------
+// strip cell e of patch p: face slot s = dim*2 + (side>0), layer gg,
+// transverse t1, t2 in [0,16) (edges and corners are never filled, :418)
+BH_HD inline void strip_ijk(int dim, int pos, int t1, int t2, int& i, int& j, int& k) {
+    if (dim == 0) { i = pos; j = t1; k = t2; }
+    else if (dim == 1) { i = t1; j = pos; k = t2; }
+    else { i = t1; j = t2; k = pos; }
+}
+
+BH_HD inline void ghost_fill_item(const KP& kp, const Pool& P, int p, int e) {
+    int s = e / 512, rem = e % 512;
+    int gg = rem / 256, t1 = (rem / 16) % 16, t2 = rem % 16;
+    int dim = s / 2, side = (s & 1) ? 1 : -1;
+    int nb = P.nbr[(p * 6 + s) * 2], kind = P.nbr[(p * 6 + s) * 2 + 1];
+    int pstart = side == 1 ? BLK : -GH;
+    int gi, gj, gk;
+    strip_ijk(dim, pstart + gg, t1, t2, gi, gj, gk);
+    int lg = lindx(gi, gj, gk);
+    if (kind == BH_NB_COPY || kind == BH_NB_BNDY) {
+        int src_p, ai, aj, ak;
+        if (kind == BH_NB_COPY) {                   // gh_copy :390-425
+            src_p = nb;
+            strip_ijk(dim, (side == 1 ? 0 : BLK - GH) + gg, t1, t2, ai, aj, ak);
+        } else {                                    // gh_bndy :494-522
+            src_p = p;
+            strip_ijk(dim, side == 1 ? BLK - 1 - gg : gg, t1, t2, ai, aj, ak);
+        }
+        int la = lindx(ai, aj, ak);
+        for (int v = 0; v < 8; v++) {
+            Uv(P, p, v)[lg] = Uv(P, src_p, v)[la];
+            Wv(P, p, v)[lg] = Wv(P, src_p, v)[la];
+        }
+        return;
+    }
+    // gh_prolong (:427-492): minmod-limited interpolation from the coarse patch
+    int ci = (dim == 0) ? gg / 2 : t1 / 2;
+    int cj = (dim == 1) ? gg / 2 : (dim == 0 ? t1 / 2 : t2 / 2);
+    int ck = (dim == 2) ? gg / 2 : t2 / 2;
+    double offg = (gg % 2 == 0) ? -0.25 : 0.25;
+    double offt1 = (t1 % 2 == 0) ? -0.25 : 0.25;
+    double offt2 = (t2 % 2 == 0) ? -0.25 : 0.25;
+    double on, ot1, ot2;
+    if (dim == 0) { on = offg; ot1 = offt1; ot2 = offt2; }
+    else if (dim == 1) { on = offt1; ot1 = offg; ot2 = offt2; }
+    else { on = offt1; ot1 = offt2; ot2 = offg; }
+    int lc = lindx(ci, cj, ck);
+    int lxm = lindx(ci - 1, cj, ck), lxp = lindx(ci + 1, cj, ck);
+    int lym = lindx(ci, cj - 1, ck), lyp = lindx(ci, cj + 1, ck);
+    int lzm = lindx(ci, cj, ck - 1), lzp = lindx(ci, cj, ck + 1);
+    double u8[8];
+    for (int v = 0; v < 8; v++) {
+        const double* c = Uv(P, nb, v);
+        double vc = c[lc];
+        double sn = minmod(vc - c[lxm], c[lxp] - vc);
+        double st1 = minmod(vc - c[lym], c[lyp] - vc);
+        double st2 = minmod(vc - c[lzm], c[lzp] - vc);
+        u8[v] = vc + sn * on + st1 * ot1 + st2 * ot2;
+    }
+    Cons u;
+    u.D = u8[0]; u.tau = u8[4];
+    for (int d = 0; d < 3; d++) { u.S[d] = u8[1 + d]; u.B[d] = u8[5 + d]; }
+    Prim w;
+    load_prim(P, p, lg, w);
+    bool dirty = false;
+    recover_cell(kp, P, p, lg, w, u, dirty);
+    store_cons(P, p, lg, u);
+    store_prim(P, p, lg, w);
+}
+
+// ghost ctop of amrtree::ghosts for one cell of a patch of one wave
+BH_HD inline void ghost_ctop_item(const KP& kp, const Pool& P, int p, int l) {
+    int i, j, k;
+    lin_ijk(l, i, j, k);
+    if (!is_ghost(i, j, k)) return;
+    Prim w; Cons u;
+    load_prim(P, p, l, w);
+    load_cons(P, p, l, u);
+    bool dirty = false;
+    ghost_recover(kp, P, p, l, w, u, dirty);
+    store_prim(P, p, l, w);
+    if (dirty) store_cons(P, p, l, u);
+}
+
+// reconstruction loop of rkstg (integrator.cpp:288-310) for one cell of a
+// leaf patch.  With ghost_first, ghost cells first take amrtree::ghosts'
+// ctop; a second ctop on an unchanged U reproduces the first, so it only
+// runs after a fallback changed U.
+BH_HD inline void prims_item(const KP& kp, const Pool& P, int p, int l, int ghost_first) {
+    int i, j, k;
+    lin_ijk(l, i, j, k);
+    Prim w; Cons u;
+    load_cons(P, p, l, u);
+    bool dirty = false, need = true;
+    if (ghost_first && is_ghost(i, j, k)) {
+        load_prim(P, p, l, w);
+        ghost_recover(kp, P, p, l, w, u, dirty);
+        need = dirty;
+    } else {
+        w.rho = w.eps = 0.0;
+        w.v[0] = w.v[1] = w.v[2] = 0.0;
+        for (int d = 0; d < 3; d++) w.B[d] = Wv(P, p, 5 + d)[l];
+    }
+    if (need) recover_cell(kp, P, p, l, w, u, dirty);
+    store_prim(P, p, l, w);
+    if (dirty) store_cons(P, p, l, u);
+}
+
+// ---- floors: patch::floors (grid.cpp:331-358) ---------------------------
+BH_HD inline void floors_item(const KP& kp, const Pool& P, int p, int c) {
+    int l = lindx(c / 256, (c / 16) % 16, c % 16);
+    Cons u;
+    load_cons(P, p, l, u);
+    double r = rr(P, p, l), th = tt(P, p, l);
+    bool bhl = !isfinite(u.D) || !isfinite(u.tau) || u.D <= 0.0 || u.tau <= 0.0;
+    Prim w;
+    load_prim(P, p, l, w);
+    bool wrote = false;
+    if (!bhl) {
+        Met mc;
+        met_comp(kp.tree, r, th, mc);
+        Prim pv;
+        bool dom = false;
+        int ok = ctop(kp.gamma, kp.maxiter, kp.tol, mc, u, pv, dom);
+        if (dom) flag(P.err, BH_ERR_DOMAIN);
+        bhl = !ok;
+        if (!bhl && !(pv.rho <= 0.0 || pv.eps <= 0.0)) { w = pv; wrote = true; }
+    }
+    double frho, feps;
+    pvfs(r, frho, feps);
+    if (bhl || w.rho <= frho) {
+        floor_reset(kp, P, p, l, w, u);
+        store_cons(P, p, l, u);
+        wrote = true;
+    }
+    if (wrote) store_prim(P, p, l, w);
+}
+
+// ---- dtcomp (integrator.cpp:156-189): one cell's CFL candidate -----------
+constexpr double DBL_BIG = 1.7976931348623157e308;   // std::numeric_limits<double>::max()
+BH_HD inline double dt_item(const KP& kp, const Pool& P, int p, int c, double cfl) {
+    double best = DBL_BIG;
+    int l = lindx(c / 256, (c / 16) % 16, c % 16);
+    double rho = Wv(P, p, 0)[l], eps = Wv(P, p, 1)[l];
+    if (!eos_ok(rho)) flag(P.err, BH_ERR_DOMAIN);
+    double cs = sqrt(cs2f(kp.gamma, rho, eps));
+    Met mc;
+    met_comp(kp.cell, rr(P, p, l), tt(P, p, l), mc);
+    const double* g = P.pgeo + 6 * p;
+    for (int d = 0; d < 3; d++) {
+        double v = Wv(P, p, 2 + d)[l];
+        double ld_p = fabs(mc.alpha * (v + cs) - mc.beta[d]);
+        double ld_m = fabs(mc.alpha * (v - cs) - mc.beta[d]);
+        double vmax = smax(ld_p, ld_m);
+        if (vmax > 1e-14) best = smin(best, cfl * g[3 + d] / vmax);
+    }
+    return best;
+}
+
+// ---- batched physics items ----------------------------------------------
+BH_HD inline void metric_item(const KP& k, const double* r, const double* th, int64_t q, double* out) {
+    MetFull f;
+    met_full(k.tree, r[q], th[q], f);
+    Met m;
+    met_comp(k.tree, r[q], th[q], m);
+    double* o = out + q * 120;
+    // struct metriccomp member order (metric.hpp:11-21)
+    for (int i = 0; i < 16; i++) o[i] = f.g[i / 4][i % 4];
+    for (int i = 0; i < 16; i++) o[16 + i] = f.gi[i / 4][i % 4];
+    for (int i = 0; i < 64; i++) o[32 + i] = f.G[i / 16][(i / 4) % 4][i % 4];
+    o[96] = m.sqrtdetg;
+    for (int i = 0; i < 9; i++) o[97 + i] = m.gam[i / 3][i % 3];
+    for (int i = 0; i < 9; i++) o[106 + i] = m.gam_inv[i / 3][i % 3];
+    o[115] = m.sqrtdetgam;
+    o[116] = m.alpha;
+    for (int i = 0; i < 3; i++) o[117 + i] = m.beta[i];
+}
+
+BH_HD inline void ptoc_item(const KP& k, const double* W, const double* r, const double* th, int64_t n, int64_t q,
+                            double* U, double* Wd, int32_t* err) {
+    Prim w;
+    w.rho = W[q]; w.eps = W[n + q];
+    for (int d = 0; d < 3; d++) { w.v[d] = W[(2 + d) * n + q]; w.B[d] = W[(5 + d) * n + q]; }
+    Met mc;
+    met_comp(k.tree, r[q], th[q], mc);
+    Cons c;
+    PtocOut po;
+    if (!ptoc(k.gamma, mc, w, c, &po)) flag(err, BH_ERR_DOMAIN);
+    U[q] = c.D; U[4 * n + q] = c.tau;
+    for (int d = 0; d < 3; d++) { U[(1 + d) * n + q] = c.S[d]; U[(5 + d) * n + q] = c.B[d]; }
+    if (Wd) { Wd[q] = po.lor; Wd[n + q] = po.p; Wd[2 * n + q] = po.h; Wd[3 * n + q] = po.b2; }
+}
+
+BH_HD inline void ctop_item(const KP& k, const double* U, const double* r, const double* th, int64_t n, int64_t q,
+                            double* W, double* Wd, int32_t* status, int32_t* iters, int32_t* path) {
+    Cons c;
+    c.D = U[q]; c.tau = U[4 * n + q];
+    for (int d = 0; d < 3; d++) { c.S[d] = U[(1 + d) * n + q]; c.B[d] = U[(5 + d) * n + q]; }
+    Met mc;
+    met_comp(k.tree, r[q], th[q], mc);
+    Prim w = {0, 0, {0, 0, 0}, {0, 0, 0}};
+    CtopOut co = {0, 0, 0, 0, 0, 0, 0};
+    bool dom = false;
+    int ok = ctop(k.gamma, k.maxiter, k.tol, mc, c, w, dom, &co);
+    W[q] = w.rho; W[n + q] = w.eps;
+    for (int d = 0; d < 3; d++) { W[(2 + d) * n + q] = w.v[d]; W[(5 + d) * n + q] = w.B[d]; }
+    if (Wd) { Wd[q] = co.p; Wd[n + q] = co.T; Wd[2 * n + q] = co.h; Wd[3 * n + q] = co.lor; Wd[4 * n + q] = co.b2; }
+    status[q] = dom ? -1 : ok;
+    if (iters) iters[q] = co.iters;
+    if (path) path[q] = co.path;
+}
+
+BH_HD inline void hlld_item(const KP& k, const double* WL, const double* WR, const double* UL, const double* UR,
+                            const double* r, const double* th, int dim, int64_t n, int64_t q, double* F,
+                            double* cts) {
+    Prim l, rw;
+    Cons ul, ur;
+    l.rho = WL[q]; l.eps = WL[n + q]; rw.rho = WR[q]; rw.eps = WR[n + q];
+    ul.D = UL[q]; ul.tau = UL[4 * n + q]; ur.D = UR[q]; ur.tau = UR[4 * n + q];
+    for (int d = 0; d < 3; d++) {
+        l.v[d] = WL[(2 + d) * n + q]; l.B[d] = WL[(5 + d) * n + q];
+        rw.v[d] = WR[(2 + d) * n + q]; rw.B[d] = WR[(5 + d) * n + q];
+        ul.S[d] = UL[(1 + d) * n + q]; ul.B[d] = UL[(5 + d) * n + q];
+        ur.S[d] = UR[(1 + d) * n + q]; ur.B[d] = UR[(5 + d) * n + q];
+    }
+    Met mc;
+    met_comp(k.tree, r[q], th[q], mc);
+    double f[8], c = 0;
+    hlld(k.gamma, mc, l, rw, ul, ur, dim, f, c);
+    for (int v = 0; v < 8; v++) F[v * n + q] = f[v];
+    cts[q] = c;
+}
+
+}  // namespace bh

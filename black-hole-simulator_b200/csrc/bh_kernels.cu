@@ -1,0 +1,267 @@
+// bh_kernels.cu -- sm_100a kernels and the C ABI of the GRMHD block update.
+//
+// One thread per cell / face / edge; patches are the unit of parallel work
+// (blockIdx.y walks a patch list, blockIdx.x the items of one patch), so a
+// CTA never straddles two patches and all per-patch arrays are read with
+// unit stride along the reference's fastest index k.  Everything is FP64
+// and compiled with --fmad=false: this is the reference-faithful form.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+#include "bhgpu.h"
+#include "bh_items.cuh"
+
+using namespace bh;
+
+namespace {
+
+constexpr int TPB = 128;
+
+// ---- thin kernels: thread index -> item --------------------------------
+#define ITEM(n) int e = blockIdx.x * blockDim.x + threadIdx.x; if (e >= (n)) return
+#define BATCH int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; if (q >= n) return
+
+__global__ void k_geometry(Pool P, const int32_t* list) { ITEM(NC); geometry_item(P, list[blockIdx.y], e); }
+
+__global__ void k_metric(KP k, const double* r, const double* th, int64_t n, double* out) { BATCH; metric_item(k, r, th, q, out); }
+__global__ void k_ptoc(KP k, const double* W, const double* r, const double* th, int64_t n, double* U, double* Wd) {
+    BATCH; ptoc_item(k, W, r, th, n, q, U, Wd, nullptr);
+}
+__global__ void k_ctop(KP k, const double* U, const double* r, const double* th, int64_t n, double* W, double* Wd,
+                       int32_t* st, int32_t* it, int32_t* pa) {
+    BATCH; ctop_item(k, U, r, th, n, q, W, Wd, st, it, pa);
+}
+__global__ void k_hlld(KP k, const double* WL, const double* WR, const double* UL, const double* UR, const double* r,
+                       const double* th, int dim, int64_t n, double* F, double* cts) {
+    BATCH; hlld_item(k, WL, WR, UL, UR, r, th, dim, n, q, F, cts);
+}
+__global__ void k_reconfp(KP kp, Pool P, int dim, int lim, int64_t n, double* Lo, double* Ro) {
+    ITEM(NFACE); reconfp_item(kp, P, blockIdx.y, dim, e, lim, n, Lo, Ro);
+}
+// patch::fluxcomp: one face per thread, direction blockIdx.z
+__global__ void __launch_bounds__(TPB) k_flux(KP kp, Pool P, const int32_t* list) {
+    ITEM(NFACE); flux_item(kp, P, list[blockIdx.y], blockIdx.z, e);
+}
+__global__ void k_emf(Pool P, const int32_t* list) { ITEM(N_EDGE); emf_item(P, list[blockIdx.y], e); }
+__global__ void k_bfupdate(Pool P, const int32_t* list, const double* dtp) {
+    ITEM(N_BUP); bfupdate_item(P, list[blockIdx.y], e, *dtp);
+}
+__global__ void k_f2cb(KP kp, Pool P, const int32_t* list) { ITEM(N_F2C); f2cb_item(kp, P, list[blockIdx.y], e); }
+__global__ void k_div_source(KP kp, Pool P, const int32_t* list, double* dv, double* sv) {
+    ITEM(N_INT); div_source_item(kp, P, list[blockIdx.y], e, dv, sv);
+}
+__global__ void __launch_bounds__(TPB) k_update(KP kp, Pool P, const int32_t* list, const double* dtp, int stage) {
+    ITEM(N_F2C); update_item(kp, P, list[blockIdx.y], e, *dtp, stage);
+}
+__global__ void k_ghost_fill(KP kp, Pool P, const int32_t* list) { ITEM(N_STRIP); ghost_fill_item(kp, P, list[blockIdx.y], e); }
+__global__ void k_ghost_ctop(KP kp, Pool P, const int32_t* list) { ITEM(NC); ghost_ctop_item(kp, P, list[blockIdx.y], e); }
+__global__ void __launch_bounds__(TPB) k_prims(KP kp, Pool P, const int32_t* list, int ghost_first) {
+    ITEM(NC); prims_item(kp, P, list[blockIdx.y], e, ghost_first);
+}
+__global__ void __launch_bounds__(TPB) k_floors(KP kp, Pool P, const int32_t* list) {
+    ITEM(N_INT); floors_item(kp, P, list[blockIdx.y], e);
+}
+
+// constrans::maxdivB: one CTA per patch, max-reduction in shared memory
+__global__ void k_maxdivb(Pool P, double* out) {
+    int p = blockIdx.x;
+    double m = 0.0;
+    for (int e = threadIdx.x; e < N_BUP; e += blockDim.x) m = smax(m, maxdivb_item(P, p, e));
+    __shared__ double red[256];
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] = smax(red[threadIdx.x], red[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[p] = red[0];
+}
+
+// rk2integrator::dtcomp: per-cell candidates, warp and block minimum, then
+// one atomicMin per block on the 64-bit pattern (positive doubles order
+// like their bit patterns, and min is exact, so the result is deterministic)
+__global__ void k_dt_init(double* dt) { *dt = DBL_BIG; }
+__global__ void k_dtcomp(KP kp, Pool P, const int32_t* list, double cfl, double* dt) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double best = c < N_INT ? dt_item(kp, P, list[blockIdx.y], c, cfl) : DBL_BIG;
+    unsigned long long b = __double_as_longlong(best);
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+        b = x < b ? x : b;
+    }
+    __shared__ unsigned long long red[TPB / 32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) b = red[w] < b ? red[w] : b;
+        b = red[0] < b ? red[0] : b;
+        atomicMin((unsigned long long*)dt, b);
+    }
+}
+
+// ==========================================================================
+// host helpers
+// ==========================================================================
+inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+inline int launched() { return cudaGetLastError() == cudaSuccess ? BH_OK : BH_ECUDA; }
+inline bool bad_pool(const bh_pool* p) { return !p || p->npatch <= 0 || !p->all; }
+inline dim3 grid2(int items, int npatch, int z = 1) { return dim3((items + TPB - 1) / TPB, npatch, z); }
+
+}  // namespace
+
+// ==========================================================================
+// C ABI
+// ==========================================================================
+extern "C" {
+
+int bh_abi_version(void) { return BHGPU_ABI_VERSION; }
+
+int bh_read_error(const bh_pool* pool, int32_t* out, void* stream) {
+    if (!pool || !pool->err || !out) return BH_EINVAL;
+    if (cudaMemcpyAsync(out, pool->err, sizeof(int32_t), cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess) return BH_ECUDA;
+    return cudaStreamSynchronize(S(stream)) == cudaSuccess ? BH_OK : BH_ECUDA;
+}
+int bh_clear_error(const bh_pool* pool, void* stream) {
+    if (!pool || !pool->err) return BH_EINVAL;
+    return cudaMemsetAsync(pool->err, 0, sizeof(int32_t), S(stream)) == cudaSuccess ? BH_OK : BH_ECUDA;
+}
+
+int bh_metric_comp(const bh_params* P, const double* r, const double* th, int64_t n, double* out, void* stream) {
+    if (!P || n < 0) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    k_metric<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), r, th, n, out);
+    return launched();
+}
+int bh_ptoc(const bh_params* P, const double* W, const double* r, const double* th, int64_t n, double* U, double* Wd,
+            void* stream) {
+    if (!P || n < 0) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    k_ptoc<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), W, r, th, n, U, Wd);
+    return launched();
+}
+int bh_ctop(const bh_params* P, const double* U, const double* r, const double* th, int64_t n, double* W, double* Wd,
+            int32_t* status, int32_t* iters, int32_t* path, void* stream) {
+    if (!P || n < 0 || (n > 0 && !status)) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    k_ctop<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), U, r, th, n, W, Wd, status, iters, path);
+    return launched();
+}
+int bh_hlld(const bh_params* P, const double* WL, const double* WR, const double* UL, const double* UR,
+            const double* r, const double* th, int32_t dim, int64_t n, double* F, double* ctspeed, void* stream) {
+    if (!P || n < 0 || dim < 0 || dim > 2) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    k_hlld<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), WL, WR, UL, UR, r, th, dim, n, F,
+                                                                    ctspeed);
+    return launched();
+}
+
+int bh_geometry(const bh_pool* pool, void* stream) {
+    if (bad_pool(pool)) return BH_EINVAL;
+    k_geometry<<<grid2(NC, pool->npatch), TPB, 0, S(stream)>>>(pool_of(pool), pool->all);
+    return launched();
+}
+int bh_reconfp(const bh_params* P, const bh_pool* pool, int32_t dim, int32_t limiter, double* L, double* R,
+               void* stream) {
+    if (!P || bad_pool(pool) || dim < 0 || dim > 2) return BH_EINVAL;
+    int64_t n = (int64_t)pool->npatch * NFACE;
+    k_reconfp<<<grid2(NFACE, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), dim, limiter, n, L, R);
+    return launched();
+}
+int bh_fluxcomp(const bh_params* P, const bh_pool* pool, void* stream) {
+    if (!P || bad_pool(pool)) return BH_EINVAL;
+    k_flux<<<grid2(NFACE, pool->npatch, 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    return launched();
+}
+int bh_emfcomp(const bh_pool* pool, void* stream) {
+    if (bad_pool(pool)) return BH_EINVAL;
+    k_emf<<<grid2(N_EDGE, pool->npatch), TPB, 0, S(stream)>>>(pool_of(pool), pool->all);
+    return launched();
+}
+int bh_bfupdate(const bh_pool* pool, const double* dt_dev, void* stream) {
+    if (bad_pool(pool) || !dt_dev) return BH_EINVAL;
+    k_bfupdate<<<grid2(N_BUP, pool->npatch), TPB, 0, S(stream)>>>(pool_of(pool), pool->all, dt_dev);
+    return launched();
+}
+int bh_f2cb(const bh_params* P, const bh_pool* pool, void* stream) {
+    if (!P || bad_pool(pool)) return BH_EINVAL;
+    k_f2cb<<<grid2(N_F2C, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    return launched();
+}
+int bh_maxdivb(const bh_pool* pool, double* out, void* stream) {
+    if (bad_pool(pool) || !out) return BH_EINVAL;
+    k_maxdivb<<<pool->npatch, 256, 0, S(stream)>>>(pool_of(pool), out);
+    return launched();
+}
+int bh_div_source(const bh_params* P, const bh_pool* pool, double* div, double* src, void* stream) {
+    if (!P || bad_pool(pool) || !div || !src) return BH_EINVAL;
+    k_div_source<<<grid2(N_INT, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, div,
+                                                                               src);
+    return launched();
+}
+int bh_ghosts(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
+    if (!P || bad_pool(pool) || n < 0 || (n > 0 && !patches)) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    k_ghost_fill<<<grid2(N_STRIP, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
+    k_ghost_ctop<<<grid2(NC, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
+    return launched();
+}
+int bh_prims(const bh_params* P, const bh_pool* pool, void* stream) {
+    if (!P || bad_pool(pool)) return BH_EINVAL;
+    if (pool->nleaf == 0) return BH_OK;
+    k_prims<<<grid2(NC, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves, 0);
+    return launched();
+}
+int bh_ghosts_prims(const bh_params* P, const bh_pool* pool, void* stream) {
+    if (!P || bad_pool(pool)) return BH_EINVAL;
+    if (pool->nleaf == 0) return BH_OK;
+    k_ghost_fill<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves);
+    k_prims<<<grid2(NC, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves, 1);
+    return launched();
+}
+int bh_update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, void* stream) {
+    if (!P || bad_pool(pool) || !dt_dev || (stage != 0 && stage != 1)) return BH_EINVAL;
+    k_update<<<grid2(N_F2C, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, dt_dev, stage);
+    return launched();
+}
+int bh_floors(const bh_params* P, const bh_pool* pool, void* stream) {
+    if (!P || bad_pool(pool)) return BH_EINVAL;
+    k_floors<<<grid2(N_INT, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    return launched();
+}
+int bh_dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
+    if (!P || bad_pool(pool) || !dt_dev) return BH_EINVAL;
+    k_dt_init<<<1, 1, 0, S(stream)>>>(dt_dev);
+    if (pool->nleaf > 0)
+        k_dtcomp<<<grid2(N_INT, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves,
+                                                                             cfl, dt_dev);
+    return launched();
+}
+int bh_rkstg(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, const int32_t* waves,
+             const int32_t* wave_off, int32_t nwave, void* stream) {
+    if (!P || bad_pool(pool) || !dt_dev || nwave < 0 || (nwave > 1 && (!waves || !wave_off))) return BH_EINVAL;
+    int rc;
+    if (nwave <= 1) {
+        rc = bh_ghosts_prims(P, pool, stream);
+    } else {
+        for (int w = 0; w < nwave; w++) {
+            rc = bh_ghosts(P, pool, waves + wave_off[w], wave_off[w + 1] - wave_off[w], stream);
+            if (rc) return rc;
+        }
+        rc = bh_prims(P, pool, stream);
+    }
+    if (rc) return rc;
+    if ((rc = bh_fluxcomp(P, pool, stream))) return rc;
+    if ((rc = bh_emfcomp(pool, stream))) return rc;
+    if ((rc = bh_bfupdate(pool, dt_dev, stream))) return rc;
+    return bh_update(P, pool, dt_dev, stage, stream);
+}
+int bh_step(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, const int32_t* waves,
+            const int32_t* wave_off, int32_t nwave, void* stream) {
+    int rc;
+    if ((rc = bh_dtcomp(P, pool, cfl, dt_dev, stream))) return rc;
+    if ((rc = bh_rkstg(P, pool, dt_dev, 0, waves, wave_off, nwave, stream))) return rc;
+    if ((rc = bh_rkstg(P, pool, dt_dev, 1, waves, wave_off, nwave, stream))) return rc;
+    return bh_floors(P, pool, stream);
+}
+
+}  // extern "C"

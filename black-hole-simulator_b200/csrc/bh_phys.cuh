@@ -1,0 +1,664 @@
+// bh_phys.cuh -- device physics of the GRMHD block update (FP64).
+//
+// Each function restates one function of the reference fluid solver
+// (Fjoerde/black-hole-simulator, src/fluid; paths below are relative to
+// it).  Floating-point expressions keep the reference's left-to-right
+// evaluation and its explicit zero metric entries, so that with
+// --fmad=false results differ from the reference only through the last
+// bits of sin/cos/acos/log/exp/pow.  Conditions where the reference throws
+// std::domain_error (thermo.cpp:11-31) set BH_ERR_DOMAIN in *err and the
+// computation continues.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "bhgpu.h"
+
+#ifndef BH_HD
+#define BH_HD __host__ __device__
+#endif
+
+namespace bh {
+
+// ---- powers the reference takes from libm pow() ------------------------
+// On the GPU they are plain multiplies/divides; a host build of this header
+// (the bit-exact CPU check of the kernel logic) calls pow() like the
+// reference does.
+#ifdef __CUDA_ARCH__
+BH_HD inline double pow_m1(double x) { return 1.0 / x; }
+BH_HD inline double pow_m2(double x) { return 1.0 / (x * x); }
+BH_HD inline double pow_mhalf(double x) { return 1.0 / sqrt(x); }
+BH_HD inline double pow_3(double x) { return x * x * x; }
+BH_HD inline double pow_4(double x) { return x * x * x * x; }
+#else
+BH_HD inline double pow_m1(double x) { return pow(x, -1); }
+BH_HD inline double pow_m2(double x) { return pow(x, -2); }
+BH_HD inline double pow_mhalf(double x) { return pow(x, -1.0 / 2.0); }
+BH_HD inline double pow_3(double x) { return pow(x, 3.0); }
+BH_HD inline double pow_4(double x) { return pow(x, 4); }
+#endif
+
+constexpr int BLK = 16, GH = 2, CPN = 20;
+constexpr int NC = CPN * CPN * CPN;                 // 8000 cells / patch
+constexpr int NF = (CPN + 1) * CPN * CPN;           // 8400 faces / direction
+constexpr int NE = CPN * (CPN + 1) * (CPN + 1);     // 8820 edges / direction
+constexpr int NFACE = (BLK + 1) * BLK * BLK;        // 4352 flux faces / direction
+
+// ---- std::min / std::max semantics (NaN included) ----------------------
+BH_HD inline double smin(double a, double b) { return (b < a) ? b : a; }
+BH_HD inline double smax(double a, double b) { return (a < b) ? b : a; }
+
+BH_HD inline void flag(int32_t* err, int bit) {
+#ifdef __CUDA_ARCH__
+    if (err) atomicOr(err, bit);
+#else
+    if (err) __atomic_fetch_or(err, bit, __ATOMIC_RELAXED);
+#endif
+}
+
+// ---- indices (grid.cpp:51-89) -------------------------------------------
+BH_HD inline int lindx(int i, int j, int k) { return (i + GH) * CPN * CPN + (j + GH) * CPN + (k + GH); }
+BH_HD inline int xfc(int i, int j, int k) { return (i + GH) * CPN * CPN + (j + GH) * CPN + (k + GH); }
+BH_HD inline int yfc(int i, int j, int k) { return (i + GH) * (CPN + 1) * CPN + (j + GH) * CPN + (k + GH); }
+BH_HD inline int zfc(int i, int j, int k) { return (i + GH) * CPN * (CPN + 1) + (j + GH) * (CPN + 1) + (k + GH); }
+BH_HD inline int exi(int i, int j, int k) { return (i + GH) * (CPN + 1) * (CPN + 1) + (j + GH) * (CPN + 1) + (k + GH); }
+BH_HD inline int eyi(int i, int j, int k) { return (i + GH) * CPN * (CPN + 1) + (j + GH) * (CPN + 1) + (k + GH); }
+BH_HD inline int ezi(int i, int j, int k) { return (i + GH) * (CPN + 1) * CPN + (j + GH) * CPN + (k + GH); }
+
+// ======================================================================
+// metric (physics/spacetime.cpp)
+// ======================================================================
+struct MP { double M, a, Q; };
+
+// Spatial 3+1 part of metric::comp: gam = g[i+1][j+1], gam_inv =
+// g_inv[i+1][j+1] (dense, with the reference's structural zeros), lapse,
+// shift, sqrt(-g), sqrt(gamma).
+struct Met {
+    double gam[3][3], gam_inv[3][3];
+    double alpha, beta[3], sqrtdetg, sqrtdetgam;
+};
+
+struct Trig { double c, s; };
+BH_HD inline Trig trig(double th) {
+    Trig t;
+#ifdef __CUDA_ARCH__
+    sincos(th, &t.s, &t.c);
+#else
+    t.s = sin(th); t.c = cos(th);
+#endif
+    return t;
+}
+
+BH_HD inline double Sigma_(const MP& m, double r, const Trig& t) {   // :12-14
+    return r * r + m.a * m.a * (t.c * t.c);
+}
+BH_HD inline double H_(const MP& m, double r, double Sig) {           // :15-17
+    return (2 * m.M * r - m.Q * m.Q) * pow_m1(Sig);
+}
+
+BH_HD inline void met_comp(const MP& m, double r, double th, Met& o) {
+    Trig t = trig(th);
+    const double a = m.a;
+    double Sig = Sigma_(m, r, t);
+    double H = H_(m, r, Sig);
+    double s2 = t.s * t.s;
+    // gcova (:20-34), spatial block
+    double g11 = 1 + H, g13 = -H * a * s2, g22 = Sig;
+    double g33 = (r * r + a * a + H * a * a * s2) * s2;
+    // gcntr (:35-49)
+    double gi00 = -1 - H, gi01 = H, gi11 = 1 - H, gi22 = pow_m1(Sig), gi13 = a * pow_m1(Sig);
+    double gi33 = pow_m1(Sig * t.s * t.s);
+    o.gam[0][0] = g11; o.gam[0][1] = 0.0; o.gam[0][2] = g13;
+    o.gam[1][0] = 0.0; o.gam[1][1] = g22; o.gam[1][2] = 0.0;
+    o.gam[2][0] = g13; o.gam[2][1] = 0.0; o.gam[2][2] = g33;
+    o.gam_inv[0][0] = gi11; o.gam_inv[0][1] = 0.0; o.gam_inv[0][2] = gi13;
+    o.gam_inv[1][0] = 0.0;  o.gam_inv[1][1] = gi22; o.gam_inv[1][2] = 0.0;
+    o.gam_inv[2][0] = gi13; o.gam_inv[2][1] = 0.0; o.gam_inv[2][2] = gi33;
+    o.sqrtdetg = (r * r + a * a * s2) * t.s;                // gdet :52-54
+    o.alpha = pow_mhalf(1 + H);                             // lapse :93-95
+    o.beta[0] = -gi01 / gi00;                               // shift :96-100
+    o.beta[1] = -0.0 / gi00;
+    o.beta[2] = -0.0 / gi00;
+    o.sqrtdetgam = o.alpha * o.sqrtdetg;                    // :117-119
+}
+
+// Full metric for the geometric source: g, g_inv and the Christoffel
+// symbols (christ, :57-90) built from the eight distinct derivatives.
+struct MetFull {
+    double g[4][4], gi[4][4], G[4][4][4];
+    double alpha, beta[3], sqrtdetg;
+};
+BH_HD inline void met_full(const MP& m, double r, double th, MetFull& o) {
+    Trig t = trig(th);
+    const double M = m.M, a = m.a, Q = m.Q;
+    double Sig = Sigma_(m, r, t);
+    double H = H_(m, r, Sig);
+    double s2 = t.s * t.s, c2 = t.c * t.c;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) { o.g[i][j] = 0.0; o.gi[i][j] = 0.0; }
+    o.g[0][0] = -1 + H;
+    o.g[0][1] = o.g[1][0] = H;
+    o.g[1][1] = 1 + H;
+    o.g[2][2] = Sig;
+    o.g[0][3] = o.g[1][3] = o.g[3][0] = o.g[3][1] = -H * a * s2;
+    o.g[3][3] = (r * r + a * a + H * a * a * s2) * s2;
+    o.gi[0][0] = -1 - H;
+    o.gi[0][1] = o.gi[1][0] = H;
+    o.gi[1][1] = 1 - H;
+    o.gi[2][2] = pow_m1(Sig);
+    o.gi[1][3] = o.gi[3][1] = a * pow_m1(Sig);
+    o.gi[3][3] = pow_m1(Sig * t.s * t.s);
+    o.sqrtdetg = (r * r + a * a * s2) * t.s;
+    o.alpha = pow_mhalf(1 + H);
+    for (int i = 0; i < 3; i++) o.beta[i] = -o.gi[0][i + 1] / o.gi[0][0];
+    // metric derivatives d[l][m][n] = d_l g_mn (:72-80)
+    double sig = r * r + a * a * c2;
+    double isig = pow_m1(sig), isig2 = pow_m2(sig);
+    double d[4][4][4];
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+            for (int k = 0; k < 4; k++) d[i][j][k] = 0;
+    double A1 = -2 * (M * r * r - Q * Q * r - M * a * a * c2) * isig2;
+    double A2 = 2 * a * a * (2 * M * r - Q * Q) * t.c * t.s * isig;
+    double A3 = 2 * a * a * s2 * (M * r * r - Q * Q * r - M * a * a * c2) * isig2;
+    double A4 = 2 * a * t.c * t.s * (2 * M * r - Q * Q) * (r * r + a * a) * isig2;
+    double A5 = s2 * (((2 * M * a * a * s2) * isig) + ((2 * r * a * a * s2 * (2 * M * r - Q * Q)) * isig2) + 2 * r);
+    double A6 = s2 * (((2 * pow_4(a) * (2 * M * r - Q * Q) * t.c * pow_3(t.s)) * isig2) +
+                      ((2 * a * a * (2 * M * r - Q * Q) * t.c * t.s) * isig)) +
+                t.c * t.s * (((a * a * s2 * (2 * M * r - Q * Q)) * isig) + r * r + a * a);
+    d[1][0][0] = d[1][0][1] = d[1][1][0] = d[1][1][1] = A1;
+    d[2][0][0] = d[2][0][1] = d[2][1][0] = d[2][1][1] = A2;
+    d[1][2][2] = 2 * r;
+    d[2][2][2] = -a * a * t.c * t.s;
+    d[1][0][3] = d[1][3][0] = d[1][1][3] = d[1][3][1] = A3;
+    d[2][0][3] = d[2][3][0] = d[2][1][3] = d[2][3][1] = A4;
+    d[1][3][3] = A5;
+    d[2][3][3] = A6;
+#pragma unroll
+    for (int l = 0; l < 4; l++)
+#pragma unroll
+        for (int mm = 0; mm < 4; mm++)
+#pragma unroll
+            for (int n = 0; n < 4; n++)
+                o.G[l][mm][n] = 0.5 * (o.gi[l][0] * (d[mm][0][n] + d[n][0][mm] - d[0][mm][n]) +
+                                       o.gi[l][1] * (d[mm][1][n] + d[n][1][mm] - d[1][mm][n]) +
+                                       o.gi[l][2] * (d[mm][2][n] + d[n][2][mm] - d[2][mm][n]) +
+                                       o.gi[l][3] * (d[mm][3][n] + d[n][3][mm] - d[3][mm][n]));
+}
+
+// ======================================================================
+// EOS (physics/thermo.cpp:10-35)
+// ======================================================================
+BH_HD inline bool eos_ok(double rho) { return !(rho <= 0.0); }
+BH_HD inline double press(double g, double rho, double eps) { return (g - 1.0) * rho * eps; }
+BH_HD inline double enth(double g, double eps) { return 1.0 + g * eps; }
+BH_HD inline double cs2f(double g, double rho, double eps) {
+    double p = press(g, rho, eps), h = enth(g, eps);
+    return (g * p) / (rho * h);
+}
+
+// primitive / conserved vectors in the reference member order
+struct Prim { double rho, eps, v[3], B[3]; };
+struct Cons { double D, S[3], tau, B[3]; };
+
+// ======================================================================
+// prim -> cons, conserved::ptoc (physics/conserved.cpp:17-73)
+// returns false where the reference throws (rho <= 0)
+// ======================================================================
+struct PtocOut { double lor, p, h, b2; };
+BH_HD inline bool ptoc(double gamma, const Met& mc, const Prim& pv, Cons& CV, PtocOut* po = nullptr) {
+    double sg = mc.sqrtdetgam;
+    double v2 = 0.0, vlow[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) vlow[i] += mc.gam[i][j] * pv.v[j];
+        v2 += vlow[i] * pv.v[i];
+    }
+    v2 = smin(v2, 1.0 - 1e-10);
+    double lor = 1.0 / sqrt(1.0 - v2);
+    bool ok = eos_ok(pv.rho);
+    double p = press(gamma, pv.rho, pv.eps);
+    double h = enth(gamma, pv.eps);
+    double Blow[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) Blow[i] += mc.gam[i][j] * pv.B[j];
+    double Bv = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) Bv += Blow[i] * pv.v[i];
+    double Bsq = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) Bsq += Blow[i] * mc.gam[i][j] * pv.B[j];
+    double b2 = (Bv * Bv + Bsq) / (lor);
+    double bt = lor * Bv / mc.alpha;
+    double pstar = p + b2 / 2;
+    double w = pv.rho * h + b2;
+    CV.D = sg * pv.rho * lor;
+    CV.tau = sg * (w * lor * lor - pstar - bt * bt) - CV.D;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        double bi = (Blow[i] + mc.alpha * bt * lor * vlow[i]) / lor;
+        CV.S[i] = sg * (w * lor * lor * vlow[i] - mc.alpha * bt * bi);
+        CV.B[i] = sg * pv.B[i];
+    }
+    if (po) { po->lor = lor; po->p = p; po->h = h; po->b2 = b2; }
+    return ok;
+}
+
+// ======================================================================
+// cons -> prim, conserved::ctop + f_df + cp_bd (physics/conserved.cpp:80-285)
+// ======================================================================
+BH_HD inline double f_df(double gamma, double xi, double Ssq, double Bsq, double SB,
+                                       double Dn, double taun, double& df) {
+    double Yi = SB * SB;
+    double K = Bsq;
+    double X = xi * xi;
+    double xipK = xi + K;
+    double vsq = (Ssq * X + Yi * (2.0 * xi + K)) / (X + xipK * xipK);
+    if (vsq >= 1.0) { df = 0.0; return 1e30; }
+    double ltz2 = 1.0 / (1.0 - vsq);
+    double ltz = sqrt(ltz2);
+    double rho = Dn / ltz;
+    double G = gamma - 1.0;
+    double p = (G / gamma) * (xi / ltz2 - Dn / ltz);
+    double pstar = p + K / (2 * ltz2) + Yi / (2 * X);
+    if (p < 0.0 || rho < 0.0) { df = 0.0; return 1e32; }
+    double f = xi - taun - Dn - pstar;
+    double N = Ssq * X + Yi * (2.0 * xi + K);
+    double Mq = X * xipK * xipK;
+    double dN = 2.0 * Ssq * xi + 2.0 * Yi;
+    double dM = 2.0 * xi * xipK * xipK + 2.0 * X * X;
+    double dvv = (dN * Mq - dM * N) / (Mq * Mq);
+    double dltz2 = ltz2 * ltz2 * dvv;
+    double dltz = dltz2 / (2.0 * ltz);
+    double dp = (G / gamma) * ((1.0 / ltz2) - (xi * dltz2) / (ltz2 * ltz2) + Dn * dltz / ltz2);
+    double dpstar = dp - (K * dltz2) / (2.0 * ltz2 * ltz2) - Yi / (xi * X);
+    df = 1 - dpstar;
+    return f;
+}
+BH_HD inline double fres(double gamma, double xi, double Ssq, double Bsq, double SB, double Dn,
+                                       double taun) {
+    double d;
+    return f_df(gamma, xi, Ssq, Bsq, SB, Dn, taun, d);
+}
+BH_HD inline bool cp_bd(double gamma, double xa, double xb, double Ssq, double Bsq, double SB, double D,
+                             double tau, double& root, double tol) {
+    double fa = fres(gamma, xa, Ssq, Bsq, SB, D, tau);
+    double fb = fres(gamma, xb, Ssq, Bsq, SB, D, tau);
+    if (fa * fb > 0.0) return false;
+    if (fabs(fa) < fabs(fb)) { double t = xa; xa = xb; xb = t; t = fa; fa = fb; fb = t; }
+    double xc = xa, fc = fa;
+    bool mflag = true;
+    double s = 0.0, d = 0.0;
+    for (int i = 0; i < 100; i++) {
+        if (fabs(xb - xa) < tol) { root = xb; return true; }
+        if (fa != fc && fb != fc)
+            s = (xa * fb * fc) / ((fa - fb) - (fa - fc)) + (xb * fa * fc) / ((fb - fa) - (fb - fc)) +
+                (xc * fa * fb) / ((fc - fa) - (fc - fb));
+        else
+            s = xb - fb * (xb - xa) / (fb - fa);
+        bool c1 = !((3 * xa + 4) / 4 < s && s < xb);
+        bool c2 = mflag && fabs(s - xb) >= fabs(xb - xc) / 2;
+        bool c3 = !mflag && fabs(s - xb) >= fabs(xc - d) / 2;
+        if (c1 || c2 || c3) { s = (xa + xb) / 2; mflag = true; }
+        else mflag = false;
+        double fs = fres(gamma, s, Ssq, Bsq, SB, D, tau);
+        d = xc; xc = xb; fc = fb;
+        if (fa * fs < 0.0) xb = s;
+        else xa = s;
+        if (fabs(fa) < fabs(fb)) { double t = xa; xa = xb; xb = t; t = fa; fa = fb; fb = t; }
+    }
+    return false;
+}
+
+struct CtopOut { double p, T, h, lor, b2; int iters, path; };
+// returns 1 ok / 0 failed; *domain set where the reference throws
+BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, const Cons& cv, Prim& pv,
+                           bool& domain, CtopOut* co = nullptr) {
+    double sg = mc.sqrtdetgam;
+    double D = cv.D / sg;
+    double tau = cv.tau / sg;
+    // conserved.cpp:144-150 reads B[j], S[j] for j > i before they are
+    // assigned; those reads are zero here (the reference's value on a clean stack)
+    double B[3] = {0.0, 0.0, 0.0}, S[3] = {0.0, 0.0, 0.0};
+    double Bu[3], Su[3];
+    double Bsq = 0.0, Ssq = 0.0, SB = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        B[i] = cv.B[i] / sg;
+        S[i] = cv.S[i] / sg;
+        Bu[i] = mc.gam_inv[i][2] * B[2];     // the inner j-loop assigns; j = 2 survives
+        Su[i] = mc.gam_inv[i][2] * S[2];
+        Ssq += S[i] * Su[i];
+        Bsq += B[i] * Bu[i];
+        SB += S[i] * Bu[i];
+    }
+    double xi_l = D;
+    double xi_h = tau + D + Bsq / 2.0 + 1e3;
+    double fl = fres(gamma, xi_l, Ssq, Bsq, SB, D, tau);
+    double fh = fres(gamma, xi_h, Ssq, Bsq, SB, D, tau);
+    while (fl * fh > 0.0 && xi_h < 1e8 * D) {
+        xi_h *= 2.0;
+        fl = fres(gamma, xi_h, Ssq, Bsq, SB, D, tau);
+    }
+    double xi = (xi_l + xi_h) / 2.0;
+    bool nr_ok = true, conv = false;
+    int it = 0;
+    for (int i = 0; i < maxiter; i++) {
+        double dF;
+        double F = f_df(gamma, xi, Ssq, Bsq, SB, D, tau, dF);
+        it = i + 1;
+        if (fabs(F) < tol) { conv = true; break; }
+        if (fabs(dF) < 1e-30) { nr_ok = false; break; }
+        double xin = xi - F / dF;
+        if (xin < xi_l || xin > xi_h) { nr_ok = false; break; }
+        xi = xin;
+    }
+    int path = conv ? 0 : 1;
+    if (!nr_ok) {
+        double xib;
+        if (!cp_bd(gamma, xi_l, xi_h, Ssq, Bsq, SB, D, tau, xib, tol)) {
+            if (co) { co->iters = it; co->path = 3; }
+            return 0;
+        }
+        path = 2;
+        xi = xib;
+    }
+    double xpQ = xi + Bsq;
+    double sdb2 = SB * SB;
+    double vsq = (Ssq * xpQ * xpQ + sdb2 * (2.0 * xi + Bsq)) / (xpQ * xpQ * xi * xi);
+    vsq = smin(vsq, 1.0 - 1e-10);
+    double ltz2 = 1.0 / (1.0 - vsq);
+    double ltz = sqrt(ltz2);
+    pv.rho = D / ltz;
+    double h = xi / (pv.rho * ltz2);
+    pv.eps = (h - 1.0) / (gamma);
+    if (!eos_ok(pv.rho)) domain = true;
+    double p = press(gamma, pv.rho, pv.eps);
+    double hh = enth(gamma, pv.eps);
+    double T = p / pv.rho;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        pv.v[i] = (Su[i] + (SB / xi) * Bu[i]) / xpQ;
+        pv.B[i] = B[i];
+    }
+    if (co) {
+        double Blow[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) Blow[i] += mc.gam[i][j] * B[j];
+        double Bv = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) Bv += Blow[i] * mc.gam[i][j] * pv.v[j];
+        co->b2 = (Bv * Bv + Bsq) / ltz2;
+        co->p = p; co->h = hh; co->T = T; co->lor = ltz; co->iters = it; co->path = path;
+    }
+    if (pv.rho <= 0.0 || pv.eps <= 0.0 || p <= 0.0) return 0;
+    return 1;
+}
+
+// floor state amrtree::pvfs (grid.cpp:133-146; constants grid.hpp:140-143)
+BH_HD inline void pvfs(double r, double& rho, double& eps) {
+    double rfscal = 1.0 / pow(sqrt(smax(r, 1e-10) / 1.0), 3.0);   // libm pow on both sides
+    rho = 1e-7 * rfscal;
+    eps = 1e-5 * rfscal;
+}
+
+// ======================================================================
+// HLLD (solver/hlld.cpp)
+// ======================================================================
+struct Side {
+    double rho, eps, p, h, vn, vt1, vt2, Bn, Bt1, Bt2, ltz2, b2, pt, cf, D, tau, Sn, St1, St2, Bc, E;
+};
+struct Cst { double D, Sn, St1, St2, tau, Bn, Bt1, Bt2; };
+
+BH_HD inline double fastspeed(double rho, double h, double b2, double cs2) {  // :34-39
+    double va2 = b2 / (rho * h + b2);
+    double cf2 = cs2 + va2 * (1 - cs2);
+    cf2 = smin(cf2, 1 - 1e-10);
+    return sqrt(cf2);
+}
+BH_HD inline bool side_(double gamma, const Prim& W, const Cons& U, const Met& mc, double sqrtg, int dim,
+                             Side& s) {                                         // :41-94
+    int t1 = (dim + 1) % 3, t2 = (dim + 2) % 3;
+    s.rho = W.rho; s.eps = W.eps;
+    bool ok = eos_ok(W.rho);
+    s.p = press(gamma, W.rho, W.eps);
+    s.h = enth(gamma, W.eps);
+    double v2 = 0.0, vlow[3] = {0, 0, 0}, Blow[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            vlow[i] += mc.gam[i][j] * W.v[j];
+            Blow[i] += mc.gam[i][j] * W.B[j];
+        }
+        v2 += vlow[i] * W.v[i];
+    }
+    v2 = smin(v2, 1 - 1e-10);
+    s.ltz2 = 1.0 / (1.0 - v2);
+    double Bv = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) Bv += Blow[i] * W.v[i];
+    double Bsq = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) Bsq += Blow[i] * W.B[i];
+    s.b2 = Bv * Bv + Bsq / s.ltz2;
+    s.vn = W.v[dim]; s.vt1 = W.v[t1]; s.vt2 = W.v[t2];
+    s.Bn = W.B[dim]; s.Bt1 = W.B[t1]; s.Bt2 = W.B[t2];
+    s.pt = s.p + s.b2 / 2;
+    double cs2 = cs2f(gamma, W.rho, W.eps);
+    s.cf = fastspeed(s.rho, s.h, s.b2, cs2);
+    s.D = U.D / sqrtg; s.tau = U.tau / sqrtg;
+    s.Sn = U.S[dim] / sqrtg; s.St1 = U.S[t1] / sqrtg; s.St2 = U.S[t2] / sqrtg;
+    s.Bc = U.B[dim] / sqrtg;
+    s.E = s.tau + s.D;
+    return ok;
+}
+BH_HD inline Cst physflux(const Side& s, double a, double btn) {     // :97-122
+    Cst F;
+    double vn = s.vn;
+    F.D = s.D * vn;
+    F.tau = (s.E + s.pt) * vn - s.Bn * (s.Bn * vn + s.Bt1 * s.vt1 + s.Bt2 * s.vt2) / s.ltz2;
+    F.Sn = s.Sn * vn - s.Bn * s.Bn / s.ltz2 + s.pt;
+    F.St1 = s.St1 * vn - s.Bt1 * s.Bn / s.ltz2;
+    F.St2 = s.St2 * vn - s.Bt2 * s.Bn / s.ltz2;
+    F.Bn = 0.0;
+    F.Bt1 = s.Bt1 * vn - s.Bn * s.vt1;
+    F.Bt2 = s.Bt2 * vn - s.Bn * s.vt2;
+    F.D = a * F.D - btn * s.D;
+    F.tau = a * F.tau - btn * s.tau;
+    F.Sn = a * F.Sn - btn * s.Sn;
+    F.St1 = a * F.St1 - btn * s.St1;
+    F.St2 = a * F.St2 - btn * s.St2;
+    F.Bn = a * F.Bn - btn * s.Bn;
+    F.Bt1 = a * F.Bt1 - btn * s.Bt1;
+    F.Bt2 = a * F.Bt2 - btn * s.Bt2;
+    return F;
+}
+BH_HD inline Cst hll_flux(const Side& L, const Side& R, const Cst& FL, const Cst& FR, double SL,
+                                        double SR) {                            // :124-137
+    double dS = SR - SL;
+    Cst F;
+    F.D = (SR * FL.D - SL * FR.D + SL * SR * (R.D - L.D)) / dS;
+    F.tau = (SR * FL.tau - SL * FR.tau + SL * SR * (R.tau - L.tau)) / dS;
+    F.Sn = (SR * FL.Sn - SL * FR.Sn + SL * SR * (R.Sn - L.Sn)) / dS;
+    F.St1 = (SR * FL.St1 - SL * FR.St1 + SL * SR * (R.St1 - L.St1)) / dS;
+    F.St2 = (SR * FL.St2 - SL * FR.St2 + SL * SR * (R.St2 - L.St2)) / dS;
+    F.Bn = (SR * FL.Bn - SL * FR.Bn + SL * SR * (R.Bn - L.Bn)) / dS;
+    F.Bt1 = (SR * FL.Bt1 - SL * FR.Bt1 + SL * SR * (R.Bt1 - L.Bt1)) / dS;
+    F.Bt2 = (SR * FL.Bt2 - SL * FR.Bt2 + SL * SR * (R.Bt2 - L.Bt2)) / dS;
+    return F;
+}
+BH_HD inline Cst star_stt(const Side& s, double SK, double SM, double pt_x) {  // :140-159
+    Cst Ux;
+    Ux.D = s.D * (SK - s.vn) / (SK - SM);
+    Ux.tau = (s.E * (SK - s.vn) - s.pt * s.vn + pt_x * SM) / (SK - SM) - Ux.D;
+    Ux.Sn = (s.Sn * (SK - s.vn) - s.pt + pt_x) / (SK - SM);
+    Ux.St1 = s.St1 * (SK - s.vn) / (SK - SM);
+    Ux.St2 = s.St2 * (SK - s.vn) / (SK - SM);
+    Ux.Bn = s.Bc;
+    double den = s.D * (SK - s.vn) * (SK - SM) - s.Bn * s.Bn;
+    if (fabs(den) > 1e-14) {
+        double k = s.Bn * (SM - s.vn) / den;
+        Ux.Bt1 = s.Bt1 - s.Bn * (s.vt1 * (SK - s.vn) + s.Bn * s.Bt1 / s.D) * k;
+        Ux.Bt2 = s.Bt2 - s.Bn * (s.vt2 * (SK - s.vn) + s.Bn * s.Bt2 / s.D) * k;
+    } else {
+        Ux.Bt1 = s.Bt1; Ux.Bt2 = s.Bt2;
+    }
+    return Ux;
+}
+// alfstar_stt (:161-201); its degenerate branch (:171-173) is overwritten
+// by the assignments after it and has no effect
+BH_HD inline void alfstar_stt(const Cst& UxL, const Cst& UxR, double Bn, double SM, Cst& UxxL,
+                                            Cst& UxxR) {
+    UxxL.D = UxL.D; UxxL.tau = UxL.tau;
+    UxxR.D = UxR.D; UxxR.tau = UxR.tau;
+    UxxL.Bn = UxL.Bn; UxxR.Bn = UxR.Bn;
+    double sq_DL = sqrt(fabs(UxL.D));
+    double sq_DR = sqrt(fabs(UxR.D));
+    double den = sq_DL + sq_DR;
+    double sgnBn = (Bn >= 0.0) ? 1.0 : -1.0;
+    double vt1xx = (sq_DL * UxL.St1 / UxL.D + sq_DR * UxR.St1 / UxR.D + sgnBn * (UxR.Bt1 - UxL.Bt1)) / den;
+    double vt2xx = (sq_DL * UxL.St2 / UxL.D + sq_DR * UxR.St2 / UxR.D + sgnBn * (UxR.Bt2 - UxL.Bt2)) / den;
+    double Bt1xx = (sq_DL * UxL.Bt1 / UxL.D + sq_DR * UxR.Bt1 / UxR.D +
+                    sgnBn * sq_DL * sq_DR * (UxR.St1 / UxR.D - UxL.St1 / UxL.D)) / den;
+    double Bt2xx = (sq_DL * UxL.Bt2 / UxL.D + sq_DR * UxR.Bt2 / UxR.D +
+                    sgnBn * sq_DL * sq_DR * (UxR.St2 / UxR.D - UxL.St2 / UxL.D)) / den;
+    UxxL.St1 = UxL.D * vt1xx; UxxR.St1 = UxR.D * vt1xx;
+    UxxL.St2 = UxL.D * vt2xx; UxxR.St2 = UxR.D * vt2xx;
+    UxxL.Bt1 = Bt1xx; UxxR.Bt1 = Bt1xx;
+    UxxL.Bt2 = Bt2xx; UxxR.Bt2 = Bt2xx;
+    UxxL.Sn = UxL.D * SM; UxxR.Sn = UxR.D * SM;
+    const double vt1xL = UxL.St1 / UxL.D, vt2xL = UxL.St2 / UxL.D;
+    const double vt1xR = UxR.St1 / UxR.D, vt2xR = UxR.St2 / UxR.D;
+    double dE_L = sq_DL * sgnBn * (vt1xx * Bt1xx + vt2xx * Bt2xx - vt1xL * UxL.Bt1 - vt2xL * UxL.Bt2);
+    double dE_R = sq_DR * sgnBn * (vt1xx * Bt1xx + vt2xx * Bt2xx - vt1xR * UxR.Bt1 - vt2xR * UxR.Bt2);
+    UxxL.tau = UxL.tau - dE_L;
+    UxxR.tau = UxR.tau + dE_R;
+}
+BH_HD inline Cst interflux(const Cst& FK, double SK, const Cst& Ux, const Side& s) {  // :203-216
+    Cst F;
+    F.D = FK.D + SK * (Ux.D - s.D);
+    F.tau = FK.tau + SK * (Ux.tau - (s.E - s.D));
+    F.Sn = FK.Sn + SK * (Ux.Sn - s.Sn);
+    F.St1 = FK.St1 + SK * (Ux.St1 - s.St1);
+    F.St2 = FK.St2 + SK * (Ux.St2 - s.St2);
+    F.Bn = FK.Bn + SK * (Ux.Bn - s.Bc);
+    F.Bt1 = FK.Bt1 + SK * (Ux.Bt1 - s.Bt1);
+    F.Bt2 = FK.Bt2 + SK * (Ux.Bt2 - s.Bt2);
+    return F;
+}
+// flux (:218-227): out in cons order D,S0,S1,S2,tau,B0,B1,B2, times sqrt(-g)
+BH_HD inline void flux_out(const Cst& F, double sg, int dim, double o[8]) {
+    int t1 = (dim + 1) % 3, t2 = (dim + 2) % 3;
+    o[0] = sg * F.D; o[4] = sg * F.tau;
+    o[5 + dim] = sg * F.Bn; o[5 + t1] = sg * F.Bt1; o[5 + t2] = sg * F.Bt2;
+    o[1 + dim] = sg * F.Sn; o[1 + t1] = sg * F.St1; o[1 + t2] = sg * F.St2;
+}
+// hlld (:230-312); returns false where the reference throws
+BH_HD inline bool hlld(double gamma, const Met& mc, const Prim& WL, const Prim& WR, const Cons& UL,
+                            const Cons& UR, int dim, double Fo[8], double& ctspeed) {
+    double sg = mc.sqrtdetg;
+    Side L, R;
+    bool ok = side_(gamma, WL, UL, mc, sg, dim, L);
+    ok &= side_(gamma, WR, UR, mc, sg, dim, R);
+    double a = mc.alpha, bd = mc.beta[dim];
+    double SL = smin(a * (L.vn - L.cf) - bd, a * (R.vn - R.cf) - bd);
+    double SR = smax(a * (L.vn + L.cf) - bd, a * (R.vn + R.cf) - bd);
+    Cst FL = physflux(L, a, bd), FR = physflux(R, a, bd);
+    double cts = smax(fabs(SL), fabs(SR));
+    ctspeed = cts;
+    // :244-246 computes an HLL flux that every later path overwrites
+    if (SL >= 0.0) { flux_out(FL, sg, dim, Fo); return ok; }
+    if (SR <= 0.0) { flux_out(FR, sg, dim, Fo); return ok; }
+    double pt_x = (SR * L.pt - SL * R.pt + SL * SR * (R.Sn - L.Sn)) / (SR - SL);
+    double SM_u = SR * L.E - SL * R.E - FR.tau - FR.D + FL.tau + FL.D;
+    double SM_d = SR * L.D - SL * R.D - FR.D + FL.D;
+    if (fabs(SM_d) < 1e-12) { flux_out(hll_flux(L, R, FL, FR, SL, SR), sg, dim, Fo); return ok; }
+    double SM = SM_u / SM_d;
+    Cst UxL = star_stt(L, SL, SM, pt_x);
+    Cst UxR = star_stt(R, SR, SM, pt_x);
+    double SLx = SM - fabs(L.Bn) / sqrt(fabs(UxL.D));
+    double SRx = SM + fabs(R.Bn) / sqrt(fabs(UxR.D));
+    if (UxL.D <= 0.0 || UxR.D <= 0.0) { flux_out(hll_flux(L, R, FL, FR, SL, SR), sg, dim, Fo); return ok; }
+    Cst Fs;
+    if (SM >= 0.0) {
+        if (SLx >= 0.0) {
+            Fs = interflux(FL, SL, UxL, L);
+        } else {
+            Cst UxxL, UxxR;
+            alfstar_stt(UxL, UxR, L.Bn, SM, UxxL, UxxR);
+            Cst FLx = interflux(FL, SL, UxL, L);
+            Fs = interflux(FLx, SLx, UxxL, L);
+        }
+    } else {
+        if (SRx >= 0.0) {
+            Fs = interflux(FR, SR, UxR, R);
+        } else {
+            Cst UxxL, UxxR;
+            alfstar_stt(UxL, UxR, L.Bn, SM, UxxL, UxxR);
+            Cst FRx = interflux(FR, SR, UxR, R);
+            Fs = interflux(FRx, SRx, UxxR, R);
+        }
+    }
+    double F[8];
+    flux_out(Fs, sg, dim, F);
+    bool fin = true;
+#pragma unroll
+    for (int q = 0; q < 8; q++) fin &= isfinite(F[q]);
+    if (!fin || cts > 1.0) {
+        flux_out(hll_flux(L, R, FL, FR, SL, SR), sg, dim, F);
+        if (cts > 1.0) ctspeed = smin(cts, 1.0);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) Fo[q] = F[q];
+    return ok;
+}
+
+// ======================================================================
+// PLM reconstruction (recon.hpp:16-41, grid/reconstruction.cpp:28-97)
+// ======================================================================
+BH_HD inline double minmod(double a, double b) {
+    if (a * b <= 0.0) return 0.0;
+    return (fabs(a) < fabs(b)) ? a : b;
+}
+BH_HD inline double vanleer(double a, double b) {
+    if (a * b <= 0.0) return 0.0;
+    return 2.0 * a * b / (a + b);
+}
+BH_HD inline double mclim(double a, double b) {
+    if (a * b <= 0.0) return 0.0;
+    double c = (a + b) / 2;
+    double s = (a > 0.0) ? 1.0 : -1.0;
+    return s * minmod(fabs(2 * a), minmod(fabs(2 * b), fabs(c)));
+}
+BH_HD inline double limit(double dl, double dr, int lim) {
+    return lim == BH_VANLEER ? vanleer(dl, dr) : lim == BH_MC ? mclim(dl, dr) : minmod(dl, dr);
+}
+BH_HD inline void recon_scal(double Wm, double Wc, double Wp, double Wpp, int lim, double& fL,
+                                           double& fR) {
+    fL = Wc + limit(Wc - Wm, Wp - Wc, lim) / 2.0;
+    fR = Wp - limit(Wp - Wc, Wpp - Wp, lim) / 2.0;
+}
+// causality rescale of reconfp (:69-83) with the cell's metric
+BH_HD inline void causalv(double v[3], const Met& mc) {
+    double v2 = 0.0;
+#pragma unroll
+    for (int m = 0; m < 3; m++)
+#pragma unroll
+        for (int n = 0; n < 3; n++) v2 += mc.gam[m][n] * v[m] * v[n];
+    if (v2 >= 1.0) {
+        double s = (1 - 1e-10) / sqrt(v2);
+#pragma unroll
+        for (int a = 0; a < 3; a++) v[a] *= s;
+    }
+}
+
+}  // namespace bh

@@ -1,0 +1,159 @@
+/*
+ * bhgpu.h -- C ABI of the B200 (sm_100a) GRMHD block update.
+ *
+ * A drop-in for the fluid hot path of Fjoerde/black-hole-simulator
+ * (src/fluid): the reference's C++ entry points (file:line below, paths
+ * relative to src/fluid) map one to one onto these functions.  Every
+ * function takes plain device pointers and sizes, launches on the caller's
+ * CUDA stream (`stream`, a cudaStream_t passed as void*, NULL = legacy
+ * default stream) and returns without synchronising.
+ *
+ * Ownership: the caller allocates every device buffer (the reference's
+ * patch members, grid.hpp:27-105) and describes them in a bh_pool; the
+ * library allocates nothing unless a function says so.
+ *
+ * Errors: nothing throws.  Functions return BH_OK or a negative BH_E*
+ * code for bad arguments or a CUDA launch error.  Conditions the reference
+ * reports by throwing std::domain_error from its EOS (thermo.cpp:11-31)
+ * are detected on the device and recorded in *pool->err (bit BH_ERR_DOMAIN);
+ * the caller reads that word (bh_read_error) once the stream has drained.
+ *
+ * Layout (reference per-patch linear indices, grid.cpp:51-89): a pool
+ * holds npatch patches of 16^3 interior cells + 2 ghost layers (20^3
+ * cells), structure of arrays per patch:
+ *   U, W, dU  [npatch][8][8000]    conserved D,S0,S1,S2,tau,B0,B1,B2 /
+ *                                  primitive rho,eps,v0,v1,v2,B0,B1,B2
+ *   F         [npatch][3][8][8400] face fluxes Fx, Fy, Fz (cons order)
+ *   Bf        [npatch][3][8400]    face B: Bfx, Bfy, Bfz
+ *   EMF       [npatch][3][8820]    edge EMFs: EMFx, EMFy, EMFz
+ *   rth       [npatch][2][8000]    cell-centre r, theta
+ */
+#ifndef BHGPU_H
+#define BHGPU_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BHGPU_ABI_VERSION 1
+
+enum {
+    BH_OK = 0,
+    BH_EINVAL = -1,   /* bad argument                          */
+    BH_ECUDA = -2,    /* a CUDA call or kernel launch failed   */
+    BH_ERANGE = -3    /* size above a documented maximum       */
+};
+/* bits of the device error word */
+enum {
+    BH_ERR_DOMAIN = 1   /* density <= 0 reached the EOS (reference throws) */
+};
+
+/* reconstruction limiter (recon.hpp:36) */
+enum { BH_MINMOD = 0, BH_VANLEER = 1, BH_MC = 2 };
+/* neighbour kinds of the ghost fill (grid.cpp:528-534) */
+enum { BH_NB_BNDY = 0, BH_NB_COPY = 1, BH_NB_PROLONG = 2 };
+
+typedef struct bh_params {
+    double M, a, Q;      /* tree metric, metric(M,a,Q)          metric.hpp:31       */
+    double gamma;        /* adiabatic index, state(gm)          state.hpp:11        */
+    int32_t limiter;     /* BH_MINMOD / BH_VANLEER / BH_MC      recon.hpp:41        */
+    int32_t maxiter;     /* con2prim Newton cap (500)           cons.hpp:75         */
+    double tol;          /* con2prim tolerance (1e-10)          cons.hpp:75         */
+    double cM, ca, cQ;   /* metric carried by every cell: the default metric()
+                            = (1, 0, 0) in the reference       cell.hpp:25, metric.hpp:30 */
+} bh_params;
+
+typedef struct bh_pool {
+    int32_t npatch;
+    double *U, *W, *dU;  /* [np][8][8000]                                        */
+    double *F;           /* [np][3][8][8400]                                     */
+    double *Bf;          /* [np][3][8400]                                        */
+    double *EMF;         /* [np][3][8820]                                        */
+    double *rth;         /* [np][2][8000]   written by bh_geometry               */
+    const double *pgeo;  /* [np][6]  xedge[0], yedge[0], zedge[0], dx, dy, dz    */
+    const int32_t *nbr;  /* [np][6][2] (neighbour, kind), slot dim*2 + (side>0)  */
+    const int32_t *all;  /* [npatch] patch indices 0..np-1 (flux/CT/update/floors) */
+    const int32_t *leaves; int32_t nleaf;  /* leaf patch indices (ghosts, prims, dt) */
+    int32_t *err;        /* device error word (BH_ERR_* bits)                    */
+} bh_pool;
+
+/* ---- library --------------------------------------------------------------- */
+int bh_abi_version(void);
+/* copy the device error word to *out (synchronises the stream) */
+int bh_read_error(const bh_pool *pool, int32_t *out, void *stream);
+int bh_clear_error(const bh_pool *pool, void *stream);
+
+/* ---- L0/L1 physics, batched over n independent items (SoA [k][n]) ---------- */
+/* metric::comp (physics/spacetime.cpp:122-134): out [n][120] in the member
+ * order of struct metriccomp (metric.hpp:11-21) */
+int bh_metric_comp(const bh_params *P, const double *r, const double *th, int64_t n,
+                   double *out, void *stream);
+/* conserved::ptoc (physics/conserved.cpp:17-73): W [8][n] -> U [8][n];
+ * Wd [4][n] (may be NULL) receives lor, p, h, b2 -- the fields ptoc mutates */
+int bh_ptoc(const bh_params *P, const double *W, const double *r, const double *th, int64_t n,
+            double *U, double *Wd, void *stream);
+/* conserved::ctop (physics/conserved.cpp:135-285): U [8][n] -> W [8][n];
+ * Wd [5][n] = p, T, h, lor, b2 (may be NULL); status[n] = 1 ok, 0 failed,
+ * -1 domain error; iters/path (may be NULL) = Newton iterations and the
+ * route taken (0 Newton, 1 Newton cap, 2 Brent root, 3 Brent failed) */
+int bh_ctop(const bh_params *P, const double *U, const double *r, const double *th, int64_t n,
+            double *W, double *Wd, int32_t *status, int32_t *iters, int32_t *path, void *stream);
+/* hlld (solver/hlld.cpp:230-312): per item L/R primitive and conserved
+ * states at face coordinates (r, th); F [8][n], ctspeed [n] */
+int bh_hlld(const bh_params *P, const double *WL, const double *WR, const double *UL,
+            const double *UR, const double *r, const double *th, int32_t dim, int64_t n,
+            double *F, double *ctspeed, void *stream);
+
+/* ---- L1/L2 over a patch pool -------------------------------------------- */
+/* patch::cell_init geometry (grid/grid.cpp:149-175): fills pool->rth */
+int bh_geometry(const bh_pool *pool, void *stream);
+/* reconfp (grid/reconstruction.cpp:40-97) at every flux face of direction
+ * dim of every patch, in the loop order of patch::fluxcomp; L, R [8][np*4352] */
+int bh_reconfp(const bh_params *P, const bh_pool *pool, int32_t dim, int32_t limiter,
+               double *L, double *R, void *stream);
+/* patch::fluxcomp (grid/grid.cpp:255-329) on every patch */
+int bh_fluxcomp(const bh_params *P, const bh_pool *pool, void *stream);
+/* constrans::emfcomp / Bfupdate / f2cB (grid/transport.cpp:11-75), every patch;
+ * dt is read from device memory */
+int bh_emfcomp(const bh_pool *pool, void *stream);
+int bh_bfupdate(const bh_pool *pool, const double *dt_dev, void *stream);
+int bh_f2cb(const bh_params *P, const bh_pool *pool, void *stream);
+/* constrans::maxdivB (grid/transport.cpp:77-89): out [npatch] */
+int bh_maxdivb(const bh_pool *pool, double *out, void *stream);
+/* rk2integrator::div_flux and ::source (solver/integrator.cpp:18-153) at
+ * every interior cell: div, src [np][8][8000] (ghost entries untouched) */
+int bh_div_source(const bh_params *P, const bh_pool *pool, double *div, double *src, void *stream);
+/* amrtree::ghosts (grid/grid.cpp:524-571) for the leaf patches listed in
+ * `patches` (one ghost-fill wave; waves must run in order) */
+int bh_ghosts(const bh_params *P, const bh_pool *pool, const int32_t *patches, int32_t n,
+              void *stream);
+/* reconstruction loop of rk2integrator::rkstg (solver/integrator.cpp:288-310) */
+int bh_prims(const bh_params *P, const bh_pool *pool, void *stream);
+/* ghosts + reconstruction loop fused, valid when every leaf patch is in a
+ * single ghost-fill wave (no prolongation dependencies) */
+int bh_ghosts_prims(const bh_params *P, const bh_pool *pool, void *stream);
+/* conserved update loop of rkstg (solver/integrator.cpp:325-347) */
+int bh_update(const bh_params *P, const bh_pool *pool, const double *dt_dev, int32_t stage,
+              void *stream);
+/* patch::floors (grid/grid.cpp:331-358) on every patch */
+int bh_floors(const bh_params *P, const bh_pool *pool, void *stream);
+
+/* ---- L3 integrator ------------------------------------------------------ */
+/* rk2integrator::dtcomp (solver/integrator.cpp:156-189): *dt_dev = CFL step */
+int bh_dtcomp(const bh_params *P, const bh_pool *pool, double cfl, double *dt_dev, void *stream);
+/* rk2integrator::rkstg (solver/integrator.cpp:191-260): one RK2 stage.
+ * waves/nwave: ghost-fill waves (concatenated patch lists, wave_off[nwave+1]);
+ * nwave == 1 uses the fused ghost+reconstruction kernel */
+int bh_rkstg(const bh_params *P, const bh_pool *pool, const double *dt_dev, int32_t stage,
+             const int32_t *waves, const int32_t *wave_off_host, int32_t nwave, void *stream);
+/* rk2integrator::step (solver/integrator.cpp:262-275): dtcomp, two stages,
+ * floors; dt stays on the device in *dt_dev */
+int bh_step(const bh_params *P, const bh_pool *pool, double cfl, double *dt_dev,
+            const int32_t *waves, const int32_t *wave_off_host, int32_t nwave, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

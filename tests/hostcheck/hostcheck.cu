@@ -1,0 +1,135 @@
+// hostcheck.cu -- runs the kernels' per-item functions (csrc/bh_items.cuh)
+// on the CPU, launch by launch in the order the C ABI issues them, on host
+// copies of the pool.  Built with nvcc as host code, the math functions
+// are the host libm's, so a bit-exact match with the oracle shows the
+// kernel logic is the reference's; GPU-vs-oracle tests then only see the
+// last-bit differences of the device math library.  Test code only.
+#include <stdint.h>
+#include "bhgpu.h"
+#include "bh_items.cuh"
+
+using namespace bh;
+
+extern "C" {
+
+void hc_metric(const bh_params* P, const double* r, const double* th, int64_t n, double* out) {
+    KP k = kp_of(P);
+    for (int64_t q = 0; q < n; q++) metric_item(k, r, th, q, out);
+}
+void hc_ptoc(const bh_params* P, const double* W, const double* r, const double* th, int64_t n, double* U, double* Wd) {
+    KP k = kp_of(P);
+    for (int64_t q = 0; q < n; q++) ptoc_item(k, W, r, th, n, q, U, Wd, nullptr);
+}
+void hc_ctop(const bh_params* P, const double* U, const double* r, const double* th, int64_t n, double* W, double* Wd,
+             int32_t* st, int32_t* it, int32_t* pa) {
+    KP k = kp_of(P);
+    for (int64_t q = 0; q < n; q++) ctop_item(k, U, r, th, n, q, W, Wd, st, it, pa);
+}
+void hc_hlld(const bh_params* P, const double* WL, const double* WR, const double* UL, const double* UR, const double* r,
+             const double* th, int dim, int64_t n, double* F, double* cts) {
+    KP k = kp_of(P);
+    for (int64_t q = 0; q < n; q++) hlld_item(k, WL, WR, UL, UR, r, th, dim, n, q, F, cts);
+}
+void hc_geometry(const bh_pool* pool) {
+    Pool P = pool_of(pool);
+    for (int i = 0; i < pool->npatch; i++)
+        for (int l = 0; l < NC; l++) geometry_item(P, pool->all[i], l);
+}
+void hc_reconfp(const bh_params* Pp, const bh_pool* pool, int dim, int lim, double* L, double* R) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    int64_t n = (int64_t)pool->npatch * NFACE;
+    for (int p = 0; p < pool->npatch; p++)
+        for (int f = 0; f < NFACE; f++) reconfp_item(k, P, p, dim, f, lim, n, L, R);
+}
+void hc_fluxcomp(const bh_params* Pp, const bh_pool* pool) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int i = 0; i < pool->npatch; i++)
+        for (int dim = 0; dim < 3; dim++)
+            for (int f = 0; f < NFACE; f++) flux_item(k, P, pool->all[i], dim, f);
+}
+void hc_emfcomp(const bh_pool* pool) {
+    Pool P = pool_of(pool);
+    for (int i = 0; i < pool->npatch; i++)
+        for (int e = 0; e < N_EDGE; e++) emf_item(P, pool->all[i], e);
+}
+void hc_bfupdate(const bh_pool* pool, double dt) {
+    Pool P = pool_of(pool);
+    for (int i = 0; i < pool->npatch; i++)
+        for (int e = 0; e < N_BUP; e++) bfupdate_item(P, pool->all[i], e, dt);
+}
+void hc_f2cb(const bh_params* Pp, const bh_pool* pool) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int i = 0; i < pool->npatch; i++)
+        for (int e = 0; e < N_F2C; e++) f2cb_item(k, P, pool->all[i], e);
+}
+void hc_maxdivb(const bh_pool* pool, double* out) {
+    Pool P = pool_of(pool);
+    for (int p = 0; p < pool->npatch; p++) {
+        double m = 0.0;
+        for (int e = 0; e < N_BUP; e++) m = smax(m, maxdivb_item(P, p, e));
+        out[p] = m;
+    }
+}
+void hc_div_source(const bh_params* Pp, const bh_pool* pool, double* dv, double* sv) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int i = 0; i < pool->npatch; i++)
+        for (int c = 0; c < N_INT; c++) div_source_item(k, P, pool->all[i], c, dv, sv);
+}
+void hc_ghosts(const bh_params* Pp, const bh_pool* pool, const int32_t* list, int n) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int i = 0; i < n; i++)
+        for (int e = 0; e < N_STRIP; e++) ghost_fill_item(k, P, list[i], e);
+    for (int i = 0; i < n; i++)
+        for (int l = 0; l < NC; l++) ghost_ctop_item(k, P, list[i], l);
+}
+void hc_prims(const bh_params* Pp, const bh_pool* pool, int ghost_first) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int i = 0; i < pool->nleaf; i++)
+        for (int l = 0; l < NC; l++) prims_item(k, P, pool->leaves[i], l, ghost_first);
+}
+void hc_ghosts_prims(const bh_params* Pp, const bh_pool* pool) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int i = 0; i < pool->nleaf; i++)
+        for (int e = 0; e < N_STRIP; e++) ghost_fill_item(k, P, pool->leaves[i], e);
+    hc_prims(Pp, pool, 1);
+}
+void hc_update(const bh_params* Pp, const bh_pool* pool, double dt, int stage) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int i = 0; i < pool->npatch; i++)
+        for (int e = 0; e < N_F2C; e++) update_item(k, P, pool->all[i], e, dt, stage);
+}
+void hc_floors(const bh_params* Pp, const bh_pool* pool) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int i = 0; i < pool->npatch; i++)
+        for (int c = 0; c < N_INT; c++) floors_item(k, P, pool->all[i], c);
+}
+double hc_dtcomp(const bh_params* Pp, const bh_pool* pool, double cfl) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    double best = DBL_BIG;
+    for (int i = 0; i < pool->nleaf; i++)
+        for (int c = 0; c < N_INT; c++) best = smin(best, dt_item(k, P, pool->leaves[i], c, cfl));
+    return best;
+}
+// bh_rkstg / bh_step in the order the ABI launches them
+void hc_rkstg(const bh_params* Pp, const bh_pool* pool, double dt, int stage, const int32_t* waves,
+              const int32_t* off, int nwave) {
+    if (nwave <= 1) hc_ghosts_prims(Pp, pool);
+    else {
+        for (int w = 0; w < nwave; w++) hc_ghosts(Pp, pool, waves + off[w], off[w + 1] - off[w]);
+        hc_prims(Pp, pool, 0);
+    }
+    hc_fluxcomp(Pp, pool);
+    hc_emfcomp(pool);
+    hc_bfupdate(pool, dt);
+    hc_update(Pp, pool, dt, stage);
+}
+double hc_step(const bh_params* Pp, const bh_pool* pool, double cfl, const int32_t* waves, const int32_t* off,
+               int nwave) {
+    double dt = hc_dtcomp(Pp, pool, cfl);
+    hc_rkstg(Pp, pool, dt, 0, waves, off, nwave);
+    hc_rkstg(Pp, pool, dt, 1, waves, off, nwave);
+    hc_floors(Pp, pool);
+    return dt;
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+"""The kernels' per-item functions (csrc/bh_items.cuh), compiled for the
+host and run in the order the C ABI launches them, equal the oracle bit for
+bit.  This pins the kernel logic on a CPU-only host; the GPU tests then
+only see the last-bit differences of the device math library."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from helpers import box_case, random_prims, GAMMA
+from hostcheck import HostKernels, _d
+
+import oracle
+from bhgpu.mesh import Quilt
+
+
+def eq(a, b):
+    return np.array_equal(a, b, equal_nan=True)
+
+
+@pytest.mark.parametrize("M,a,Q", [(0.0, 0.0, 0.0), (1.0, 0.9375, 0.0), (1.0, 0.9, 0.1)])
+def test_physics_items_bitwise(M, a, Q):
+    rng = np.random.default_rng(2)
+    W, r, th = random_prims(5000, rng)
+    orc = oracle.Oracle(M, a, Q, GAMMA)
+    hk = HostKernels(M, a, Q, GAMMA, 1)
+    n = W.shape[1]
+    out = np.zeros((n, 120))
+    hk.call("hc_metric", _d(r), _d(th), C.c_int64(n), _d(out))
+    assert eq(out, orc.metric(r, th))
+    U = np.zeros((8, n)); Wd = np.zeros((4, n))
+    hk.call("hc_ptoc", _d(W), _d(r), _d(th), C.c_int64(n), _d(U), _d(Wd))
+    Uc, Wdc = orc.ptoc(W, r, th)
+    assert eq(U, Uc) and eq(Wd, Wdc)
+    Wo = np.zeros((8, n)); Wdo = np.zeros((5, n))
+    st = np.zeros(n, np.int32); it = np.zeros(n, np.int32); pa = np.zeros(n, np.int32)
+    hk.call("hc_ctop", _d(Uc), _d(r), _d(th), C.c_int64(n), _d(Wo), _d(Wdo), _d(st), _d(it), _d(pa))
+    Wc, Wdc5, stc, itc, pac = orc.ctop(Uc, r, th)
+    assert eq(st, stc) and eq(it, itc) and eq(pa, pac)
+    ok = stc == 1
+    assert eq(Wo[:, ok], Wc[:, ok]) and eq(Wdo[:, ok], Wdc5[:, ok])
+    WR = W.copy(); WR[0] *= 1.07; WR[2:5] += 0.01
+    UR, _ = orc.ptoc(WR, r, th)
+    for dim in range(3):
+        F = np.zeros((8, n)); cts = np.zeros(n)
+        hk.call("hc_hlld", _d(W), _d(WR), _d(Uc), _d(UR), _d(r), _d(th), C.c_int(dim), C.c_int64(n), _d(F), _d(cts))
+        Fc, cc, _ = orc.hlld(W, WR, Uc, UR, r, th, dim)
+        assert eq(F, Fc) and eq(cts, cc)
+
+
+CASES = [dict(periodic=True, lim=0, M=0.0, a=0.0, lo=10.0, hi=12.0),
+         dict(periodic=False, lim=1, M=0.0, a=0.0, lo=10.0, hi=12.0),
+         dict(periodic=True, lim=2, M=1.0, a=0.9375, lo=-6.0, hi=6.0)]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_kernel_items_bitwise(case):
+    q, orc, hp = box_case(2, seed=3, **case)
+    hk = HostKernels(case["M"], case["a"], 0.0, GAMMA, case["lim"])
+    hh = hp.copy()
+    hh.rth[:] = 0
+    pool = hk.pool(hh)
+    hk.L.hc_geometry(C.byref(pool))
+    assert eq(hh.rth, hp.rth)
+    lst = np.arange(hp.npatch, dtype=np.int32)
+    hk.call("hc_ghosts", C.byref(pool), _d(lst), C.c_int(hp.npatch)); orc.ghosts(hp)
+    assert eq(hh.U, hp.U) and eq(hh.W, hp.W)
+    hk.call("hc_prims", C.byref(pool), C.c_int(0)); orc.prims(hp)
+    assert eq(hh.U, hp.U) and eq(hh.W, hp.W)
+    n = hp.npatch * 4352
+    for dim in range(3):
+        L = np.zeros((8, n)); R = np.zeros((8, n))
+        hk.call("hc_reconfp", C.byref(pool), C.c_int(dim), C.c_int(case["lim"]), _d(L), _d(R))
+        Lc, Rc = orc.reconfp_all(hp, dim, case["lim"])
+        assert eq(L, Lc) and eq(R, Rc)
+    hk.call("hc_fluxcomp", C.byref(pool)); orc.fluxcomp(hp)
+    assert eq(hh.F, hp.F)
+    dt = hk.L.hc_dtcomp(C.byref(hk.P), C.byref(pool), 0.4)
+    assert dt == orc.dtcomp(hp, 0.4)
+    hk.L.hc_emfcomp(C.byref(pool)); orc.emfcomp(hp)
+    hk.L.hc_bfupdate(C.byref(pool), dt); orc.bfupdate(hp, dt)
+    assert eq(hh.EMF, hp.EMF) and eq(hh.Bf, hp.Bf)
+    dv = np.zeros_like(hh.U); sv = np.zeros_like(hh.U)
+    hk.call("hc_div_source", C.byref(pool), _d(dv), _d(sv))
+    dc, sc = orc.div_source(hp)
+    from bhgpu.mesh import interior_mask
+    m = interior_mask()
+    assert eq(dv[:, :, m], dc[:, :, m]) and eq(sv[:, :, m], sc[:, :, m])
+    hk.L.hc_update(C.byref(hk.P), C.byref(pool), dt, 0); orc.f2cb(hp); orc.update(hp, dt, 0)
+    assert eq(hh.U, hp.U) and eq(hh.W, hp.W) and eq(hh.dU, hp.dU)
+    hk.call("hc_floors", C.byref(pool)); orc.floors(hp)
+    assert eq(hh.U, hp.U) and eq(hh.W, hp.W)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_steps_bitwise(case):
+    q, orc, hp = box_case(2, seed=4, **case)
+    hk = HostKernels(case["M"], case["a"], 0.0, GAMMA, case["lim"])
+    hh = hp.copy()
+    pool = hk.pool(hh)
+    off = np.array([0, hp.npatch], np.int32)
+    waves = np.arange(hp.npatch, dtype=np.int32)
+    for _ in range(3):
+        dt = hk.L.hc_step(C.byref(hk.P), C.byref(pool), 0.4, _d(waves), _d(off), 1)
+        assert dt == orc.step(hp, 0.4)
+        assert eq(hh.U, hp.U) and eq(hh.W, hp.W) and eq(hh.Bf, hp.Bf) and eq(hh.dU, hp.dU)
+
+
+def test_refined_quilt_ghost_waves_bitwise():
+    """Two refinement levels: the wave-ordered ghost fill with coarse->fine
+    prolongation equals the serial quilt-order fill."""
+    lo, hi = [10.0] * 3, [12.0] * 3
+    q = Quilt(lo, hi, 2)
+    q.refine(0); q.refine(9)
+    T = q.tables()
+    waves = q.ghost_waves(T["nbr"], T["leaf"])
+    assert len(waves) >= 2
+    orc = oracle.Oracle(0, 0, 0, GAMMA, limiter=0)
+    hp = oracle.HostPool(T)
+    orc.geometry(hp)
+    rng = np.random.default_rng(5)
+    hp.W[:, 0] = 1.0 + 0.1 * rng.random(hp.W[:, 0].shape)
+    hp.W[:, 1] = 0.3 + 0.05 * rng.random(hp.W[:, 1].shape)
+    hp.W[:, 5] = 0.5
+    for p in range(hp.npatch):
+        hp.U[p] = orc.ptoc(hp.W[p], hp.rth[p, 0], hp.rth[p, 1])[0]
+    hk = HostKernels(0, 0, 0, GAMMA, 0)
+    hh = hp.copy()
+    pool = hk.pool(hh)
+    flat = np.concatenate(waves).astype(np.int32)
+    off = np.zeros(len(waves) + 1, np.int32)
+    off[1:] = np.cumsum([len(w) for w in waves])
+    for w in range(len(waves)):
+        hk.call("hc_ghosts", C.byref(pool), _d(flat[off[w]:].copy()), C.c_int(int(off[w + 1] - off[w])))
+    orc.ghosts(hp)
+    assert eq(hh.U, hp.U) and eq(hh.W, hp.W)
+    dt = hk.L.hc_step(C.byref(hk.P), C.byref(pool), 0.4, _d(flat), _d(off), len(waves))
+    assert dt == orc.step(hp, 0.4)
+    assert eq(hh.U, hp.U) and eq(hh.W, hp.W)
