@@ -127,16 +127,32 @@ def make_tree(nq, seed):
     return tree
 
 
-# algorithmic bytes of one k_flux launch over the whole pool: for each of
-# the 3 directions and each patch, the primitives (8 doubles) of the
-# 20x16x16 cells the 4-point stencil touches, their (r, theta), the normal
-# face B of the 17x16x16 flux faces, and the 8 flux components written.
-def flux_alg_bytes(npatch):
-    per_dir = (20 * 16 * 16) * (8 + 2) * 8 + (17 * 16 * 16) * 8 + (17 * 16 * 16) * 8 * 8
-    return 3 * per_dir * npatch
+# Algorithmic HBM bytes of one launch of each stage call over the whole pool
+# (the data the computation must read and write once, nothing re-read):
+#   ghosts_prims: per leaf patch, the ghost-strip copy (3072 cells x U and W,
+#       read and written) and con2prim of all 20^3 cells (U and r, theta in,
+#       W out)
+#   fluxcomp: per direction, the primitives and (r, theta) of the 20x16x16
+#       stencil cells, the normal face B and the 8 flux components of the
+#       17x16x16 faces
+#   update: per interior cell, 3 faces x 8 flux components, W, U and dU read,
+#       U and dU written, 3 face B, (r, theta); per shell cell W.B and U.B
+#   floors: per interior cell U, W, (r, theta) read, W written
+def alg_bytes(call, npatch):
+    per = {
+        "ghosts_prims": 3072 * 16 * 8 * 2 + 8000 * (8 + 2 + 8) * 8,
+        "fluxcomp": 3 * ((20 * 16 * 16) * (8 + 2) * 8 + (17 * 16 * 16) * 8 + (17 * 16 * 16) * 8 * 8),
+        "update": 4096 * (24 + 8 + 8 + 8 + 8 + 8 + 3 + 2) * 8 + (6859 - 4096) * (3 + 6) * 8,
+        "floors": 4096 * (8 + 8 + 2 + 8) * 8,
+    }
+    return per[call] * npatch
 
 
 STEP_BYTES = 296   # algorithmic HBM bytes per zone-update of a whole RK2 step
+
+# DRAM bytes (read + write) per launch from ncu captures of this workload,
+# keyed by (call, grid); see profiles/ for the captures they come from
+TRAFFIC = {}
 
 
 def cpu_reference_sample(threads):
@@ -253,25 +269,30 @@ def run_ours(args):
     P = tree.params()
     pool = C.byref(tree.pool)
     dtp = _p(tree.dt)
-    ev_pairs = []
-    KL_PER_STEP = 15   # dt_init, dtcomp, 2 x (ghost_fill, prims, flux, emf, bfupdate, update), floors
+    ev = {k: [] for k in ("ghosts_prims", "fluxcomp", "update", "floors")}
+    # my kernels per step: dt_init, dtcomp, 2 x (ghost_fill, prims_interior,
+    # prims_ghost, flux, emf, bfupdate, update), floors
+    KL_PER_STEP = 17
+
+    def timed(name, record, fn):
+        if record:
+            a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+            a.record(); fn(); b.record()
+            ev[name].append((a, b))
+        else:
+            fn()
 
     def step(record=False):
         s = _stream()
         tree.U.copy_(U0); tree.W.copy_(W0); tree.Bf.copy_(B0)
         L.bh_dtcomp(P, pool, CFL, dtp, s)
         for stage in (0, 1):
-            L.bh_ghosts_prims(P, pool, s)
-            if record:
-                a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
-                a.record(); L.bh_fluxcomp(P, pool, s); b.record()
-                ev_pairs.append((a, b))
-            else:
-                L.bh_fluxcomp(P, pool, s)
+            timed("ghosts_prims", record, lambda: L.bh_ghosts_prims(P, pool, s))
+            timed("fluxcomp", record, lambda: L.bh_fluxcomp(P, pool, s))
             L.bh_emfcomp(pool, s)
             L.bh_bfupdate(pool, dtp, s)
-            L.bh_update(P, pool, dtp, stage, s)
-        L.bh_floors(P, pool, s)
+            timed("update", record, lambda: L.bh_update(P, pool, dtp, stage, s))
+        timed("floors", record, lambda: L.bh_floors(P, pool, s))
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -297,7 +318,7 @@ def run_ours(args):
         dist.barrier()
     ck = clocks.stop()
     ms = t_start.elapsed_time(t_end)
-    flux_ms = [a.elapsed_time(b) for a, b in ev_pairs]
+    call_ms = {k: [a.elapsed_time(b) for a, b in v] for k, v in ev.items()}
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -335,8 +356,10 @@ def run_ours(args):
     if rank == 0:
         value = world * zones * args.steps / (ms_max / 1e3)
         peak, peak_kind = measured_peaks()
-        flux_avg = statistics.mean(flux_ms) / 1e3
-        achieved = flux_alg_bytes(tree.npatch) / flux_avg / 1e9
+        share = {k: sum(v) / ms for k, v in call_ms.items()}
+        top = max(share, key=share.get)
+        top_avg = statistics.mean(call_ms[top]) / 1e3
+        achieved = alg_bytes(top, tree.npatch) / top_avg / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -349,9 +372,10 @@ def run_ours(args):
             "e2e": {"value": world * zones / (e2e_ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": KL_PER_STEP * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "k_flux", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                         "flux_ms_per_launch": flux_avg * 1e3,
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": TRAFFIC.get((top, args.grid)), "peak_source": peak_kind,
+                         "ms_per_launch": top_avg * 1e3,
+                         "step_share": {k: round(v, 4) for k, v in share.items()},
                          "step_frac": value / world * STEP_BYTES / (peak * 1e9)},
             "clocks": ck,
             "device_error_word": err,

@@ -186,6 +186,9 @@ class AmrTree:
         leaves = np.nonzero(T["leaf"])[0].astype(np.int32)
         self.leaves = torch.as_tensor(leaves, device=d)
         self.err = torch.zeros(1, dtype=torch.int32, device=d)
+        self.leafmask = torch.as_tensor(np.ascontiguousarray(T["leaf"], np.uint8), device=d)
+        # scratch: con2prim outcome of every interior cell in the current stage
+        self.status = torch.zeros((n, NC), dtype=torch.uint8, device=d)
         waves = self.quilt.ghost_waves(T["nbr"], T["leaf"])
         self.nwave = len(waves)
         off = np.zeros(self.nwave + 1, np.int32)
@@ -196,7 +199,7 @@ class AmrTree:
         self.dt = torch.zeros(1, dtype=f64, device=d)
         self.pool = BhPool(n, _p(self.U), _p(self.W), _p(self.dU), _p(self.F), _p(self.Bf), _p(self.EMF),
                            _p(self.rth), _p(self.pgeo), _p(self.nbr), _p(self.all), _p(self.leaves),
-                           len(leaves), _p(self.err))
+                           len(leaves), _p(self.err), _p(self.leafmask), _p(self.status))
         check(lib.bh_geometry(C.byref(self.pool), _stream()), "patch::cell_init")
 
     def params(self, maxiter=500, tol=1e-10) -> BhParams:

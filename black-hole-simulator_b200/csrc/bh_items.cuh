@@ -28,9 +28,11 @@ struct Pool {               // kernel-side view of bh_pool
     const double* pgeo;
     const int32_t* nbr;
     int32_t* err;
+    const uint8_t* leafmask;
+    uint8_t* status;
 };
 inline Pool pool_of(const bh_pool* p) {
-    return Pool{p->U, p->W, p->dU, p->F, p->Bf, p->EMF, p->rth, p->pgeo, p->nbr, p->err};
+    return Pool{p->U, p->W, p->dU, p->F, p->Bf, p->EMF, p->rth, p->pgeo, p->nbr, p->err, p->leafmask, p->status};
 }
 
 BH_HD inline double* Uv(const Pool& P, int p, int v) { return P.U + ((size_t)p * 8 + v) * NC; }
@@ -71,6 +73,30 @@ constexpr int N_EDGE = 19 * 19 * 19;     // emfcomp, i,j,k in [-2,17)
 constexpr int N_BUP = 18 * 18 * 18;      // Bfupdate / maxdivB, i,j,k in [-1,17)
 constexpr int N_F2C = 19 * 19 * 19;      // f2cB, i,j,k in [-1,18)
 constexpr int N_STRIP = 6 * 2 * BLK * BLK;  // ghost strip cells
+constexpr int N_GHOST = NC - N_INT;         // all ghost cells
+constexpr int N_EDGEC = N_GHOST - N_STRIP;  // edge and corner ghost cells (832)
+
+// linear indices of the edge and corner ghost cells (two or three of
+// i, j, k outside [0,16)), in lindx order
+struct EdgeCells {
+    short l[N_EDGEC];
+    constexpr EdgeCells() : l() {
+        int n = 0;
+        for (int i = -GH; i < BLK + GH; i++)
+            for (int j = -GH; j < BLK + GH; j++)
+                for (int k = -GH; k < BLK + GH; k++) {
+                    int out = (i < 0 || i >= BLK) + (j < 0 || j >= BLK) + (k < 0 || k >= BLK);
+                    if (out >= 2) l[n++] = (short)((i + GH) * CPN * CPN + (j + GH) * CPN + (k + GH));
+                }
+    }
+};
+__constant__ EdgeCells kEdgeCells = EdgeCells();          // device copy
+static constexpr EdgeCells hEdgeCells = EdgeCells();      // host copy
+#ifdef __CUDA_ARCH__
+#define BH_EDGE_CELLS kEdgeCells
+#else
+#define BH_EDGE_CELLS hEdgeCells
+#endif
 
 // W = pvfs(r) with the cell's B kept; U = ptoc(W) (integrator.cpp:211-218,
 // grid.cpp:484-487, grid.cpp:349-353)
@@ -458,26 +484,119 @@ BH_HD inline void ghost_ctop_item(const KP& kp, const Pool& P, int p, int l) {
 
 // reconstruction loop of rkstg (integrator.cpp:288-310) for one cell of a
 // leaf patch.  With ghost_first, ghost cells first take amrtree::ghosts'
-// ctop; a second ctop on an unchanged U reproduces the first, so it only
-// runs after a fallback changed U.
+// ctop (grid.cpp:538-570); a second ctop on an unchanged U reproduces the
+// first, so it only runs after a fallback changed U.  One ctop call site
+// serves both passes, so ghost and interior cells of a warp do not diverge.
 BH_HD inline void prims_item(const KP& kp, const Pool& P, int p, int l, int ghost_first) {
     int i, j, k;
     lin_ijk(l, i, j, k);
-    Prim w; Cons u;
+    Cons u;
     load_cons(P, p, l, u);
-    bool dirty = false, need = true;
-    if (ghost_first && is_ghost(i, j, k)) {
+    bool g = ghost_first && is_ghost(i, j, k);
+    Prim w;
+    if (g) {
         load_prim(P, p, l, w);
-        ghost_recover(kp, P, p, l, w, u, dirty);
-        need = dirty;
     } else {
         w.rho = w.eps = 0.0;
         w.v[0] = w.v[1] = w.v[2] = 0.0;
         for (int d = 0; d < 3; d++) w.B[d] = Wv(P, p, 5 + d)[l];
     }
-    if (need) recover_cell(kp, P, p, l, w, u, dirty);
+    double r = rr(P, p, l), th = tt(P, p, l);
+    Met mc;
+    met_comp(kp.tree, r, th, mc);
+    bool dirty = false;
+    for (int pass = g ? 0 : 1; pass < 2; pass++) {
+        Prim pv;
+        bool dom = false;
+        int ok = ctop(kp.gamma, kp.maxiter, kp.tol, mc, u, pv, dom);
+        if (dom) flag(P.err, BH_ERR_DOMAIN);
+        if (ok) { w = pv; break; }
+        // pass 0 (ghosts): floor rho, eps, keep v and B; pass 1 (rkstg):
+        // floor state with the cell's B; then U = ptoc(W) either way
+        pvfs(r, w.rho, w.eps);
+        if (pass == 1) w.v[0] = w.v[1] = w.v[2] = 0.0;
+        if (!ptoc(kp.gamma, mc, w, u)) flag(P.err, BH_ERR_DOMAIN);
+        dirty = true;
+    }
     store_prim(P, p, l, w);
     if (dirty) store_cons(P, p, l, u);
+}
+
+// ---- reconstruction with reuse of interior outcomes ----------------------
+// interior cell c of a leaf patch: rkstg's ctop and fallback; records the
+// outcome (1 recovered, 0 floored) in the status scratch
+BH_HD inline void prims_interior_item(const KP& kp, const Pool& P, int p, int c) {
+    int l = lindx(c / 256, (c / 16) % 16, c % 16);
+    Cons u;
+    load_cons(P, p, l, u);
+    Prim w;
+    w.rho = w.eps = 0.0;
+    w.v[0] = w.v[1] = w.v[2] = 0.0;
+    for (int d = 0; d < 3; d++) w.B[d] = Wv(P, p, 5 + d)[l];
+    bool dirty = false;
+    recover_cell(kp, P, p, l, w, u, dirty);
+    store_prim(P, p, l, w);
+    if (dirty) store_cons(P, p, l, u);
+    P.status[(size_t)p * NC + l] = dirty ? 0 : 1;
+}
+
+// the two con2prim passes of a ghost cell: amrtree::ghosts' ctop with its
+// fallback, then (only if that changed U) rkstg's ctop with its fallback
+BH_HD inline void ghost_two_pass(const KP& kp, const Pool& P, int p, int l) {
+    Cons u;
+    load_cons(P, p, l, u);
+    Prim w;
+    load_prim(P, p, l, w);
+    double r = rr(P, p, l), th = tt(P, p, l);
+    Met mc;
+    met_comp(kp.tree, r, th, mc);
+    bool dirty = false;
+    for (int pass = 0; pass < 2; pass++) {
+        Prim pv;
+        bool dom = false;
+        int ok = ctop(kp.gamma, kp.maxiter, kp.tol, mc, u, pv, dom);
+        if (dom) flag(P.err, BH_ERR_DOMAIN);
+        if (ok) { w = pv; break; }
+        pvfs(r, w.rho, w.eps);
+        if (pass == 1) w.v[0] = w.v[1] = w.v[2] = 0.0;
+        if (!ptoc(kp.gamma, mc, w, u)) flag(P.err, BH_ERR_DOMAIN);
+        dirty = true;
+    }
+    store_prim(P, p, l, w);
+    if (dirty) store_cons(P, p, l, u);
+}
+
+// ghost cell e of a leaf patch after the interior pass: items [0, 3072)
+// are the face strips in the order of ghost_fill_item, items [3072, 3904)
+// the edge and corner cells
+BH_HD inline void prims_ghost_item(const KP& kp, const Pool& P, int p, int e) {
+    if (e >= N_STRIP) {
+        ghost_two_pass(kp, P, p, BH_EDGE_CELLS.l[e - N_STRIP]);
+        return;
+    }
+    int s = e / 512, rem = e % 512;
+    int gg = rem / 256, t1 = (rem / 16) % 16, t2 = rem % 16;
+    int dim = s / 2, side = (s & 1) ? 1 : -1;
+    int nb = P.nbr[(p * 6 + s) * 2], kind = P.nbr[(p * 6 + s) * 2 + 1];
+    int gi, gj, gk;
+    strip_ijk(dim, (side == 1 ? BLK : -GH) + gg, t1, t2, gi, gj, gk);
+    int lg = lindx(gi, gj, gk);
+    if (kind == BH_NB_COPY || kind == BH_NB_BNDY) {
+        int src_p = kind == BH_NB_COPY ? nb : p;
+        int ai, aj, ak;
+        if (kind == BH_NB_COPY) strip_ijk(dim, (side == 1 ? 0 : BLK - GH) + gg, t1, t2, ai, aj, ak);
+        else strip_ijk(dim, side == 1 ? BLK - 1 - gg : gg, t1, t2, ai, aj, ak);
+        int la = lindx(ai, aj, ak);
+        // same U and the same (r, theta) bit for bit as the source, whose
+        // ctop succeeded: the same primitives (not so across a periodic
+        // wrap or an outflow copy, where the ghost sits elsewhere)
+        if (P.leafmask[src_p] && P.status[(size_t)src_p * NC + la] == 1 && rr(P, p, lg) == rr(P, src_p, la) &&
+            tt(P, p, lg) == tt(P, src_p, la)) {
+            for (int v = 0; v < 8; v++) Wv(P, p, v)[lg] = Wv(P, src_p, v)[la];
+            return;
+        }
+    }
+    ghost_two_pass(kp, P, p, lg);
 }
 
 // ---- floors: patch::floors (grid.cpp:331-358) ---------------------------

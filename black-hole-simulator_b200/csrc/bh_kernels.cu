@@ -16,6 +16,20 @@ using namespace bh;
 namespace {
 
 constexpr int TPB = 128;
+// minimum resident CTAs per SM requested from ptxas for the heavy kernels
+// (caps their registers per thread); tuned on B200
+#ifndef BH_MINB_PRIMS
+#define BH_MINB_PRIMS 1
+#endif
+#ifndef BH_MINB_FLUX
+#define BH_MINB_FLUX 1
+#endif
+#ifndef BH_MINB_FLOORS
+#define BH_MINB_FLOORS 1
+#endif
+#ifndef BH_MINB_UPDATE
+#define BH_MINB_UPDATE 1
+#endif
 
 // ---- thin kernels: thread index -> item --------------------------------
 #define ITEM(n) int e = blockIdx.x * blockDim.x + threadIdx.x; if (e >= (n)) return
@@ -39,7 +53,7 @@ __global__ void k_reconfp(KP kp, Pool P, int dim, int lim, int64_t n, double* Lo
     ITEM(NFACE); reconfp_item(kp, P, blockIdx.y, dim, e, lim, n, Lo, Ro);
 }
 // patch::fluxcomp: one face per thread, direction blockIdx.z
-__global__ void __launch_bounds__(TPB) k_flux(KP kp, Pool P, const int32_t* list) {
+__global__ void __launch_bounds__(TPB, BH_MINB_FLUX) k_flux(KP kp, Pool P, const int32_t* list) {
     ITEM(NFACE); flux_item(kp, P, list[blockIdx.y], blockIdx.z, e);
 }
 __global__ void k_emf(Pool P, const int32_t* list) { ITEM(N_EDGE); emf_item(P, list[blockIdx.y], e); }
@@ -50,15 +64,21 @@ __global__ void k_f2cb(KP kp, Pool P, const int32_t* list) { ITEM(N_F2C); f2cb_i
 __global__ void k_div_source(KP kp, Pool P, const int32_t* list, double* dv, double* sv) {
     ITEM(N_INT); div_source_item(kp, P, list[blockIdx.y], e, dv, sv);
 }
-__global__ void __launch_bounds__(TPB) k_update(KP kp, Pool P, const int32_t* list, const double* dtp, int stage) {
+__global__ void __launch_bounds__(TPB, BH_MINB_UPDATE) k_update(KP kp, Pool P, const int32_t* list, const double* dtp, int stage) {
     ITEM(N_F2C); update_item(kp, P, list[blockIdx.y], e, *dtp, stage);
 }
 __global__ void k_ghost_fill(KP kp, Pool P, const int32_t* list) { ITEM(N_STRIP); ghost_fill_item(kp, P, list[blockIdx.y], e); }
 __global__ void k_ghost_ctop(KP kp, Pool P, const int32_t* list) { ITEM(NC); ghost_ctop_item(kp, P, list[blockIdx.y], e); }
-__global__ void __launch_bounds__(TPB) k_prims(KP kp, Pool P, const int32_t* list, int ghost_first) {
+__global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_prims(KP kp, Pool P, const int32_t* list, int ghost_first) {
     ITEM(NC); prims_item(kp, P, list[blockIdx.y], e, ghost_first);
 }
-__global__ void __launch_bounds__(TPB) k_floors(KP kp, Pool P, const int32_t* list) {
+__global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_prims_interior(KP kp, Pool P, const int32_t* list) {
+    ITEM(N_INT); prims_interior_item(kp, P, list[blockIdx.y], e);
+}
+__global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_prims_ghost(KP kp, Pool P, const int32_t* list) {
+    ITEM(N_GHOST); prims_ghost_item(kp, P, list[blockIdx.y], e);
+}
+__global__ void __launch_bounds__(TPB, BH_MINB_FLOORS) k_floors(KP kp, Pool P, const int32_t* list) {
     ITEM(N_INT); floors_item(kp, P, list[blockIdx.y], e);
 }
 
@@ -215,7 +235,12 @@ int bh_ghosts_prims(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     if (pool->nleaf == 0) return BH_OK;
     k_ghost_fill<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves);
-    k_prims<<<grid2(NC, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves, 1);
+    if (pool->status && pool->leafmask) {
+        k_prims_interior<<<grid2(N_INT, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves);
+        k_prims_ghost<<<grid2(N_GHOST, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves);
+    } else {
+        k_prims<<<grid2(NC, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves, 1);
+    }
     return launched();
 }
 int bh_update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, void* stream) {

@@ -77,6 +77,10 @@ typedef struct bh_pool {
     const int32_t *all;  /* [npatch] patch indices 0..np-1 (flux/CT/update/floors) */
     const int32_t *leaves; int32_t nleaf;  /* leaf patch indices (ghosts, prims, dt) */
     int32_t *err;        /* device error word (BH_ERR_* bits)                    */
+    const uint8_t *leafmask; /* [npatch] 1 for leaf patches                       */
+    uint8_t *status;     /* [np][8000] scratch: con2prim outcome of the interior
+                            cells in the current stage; NULL disables the reuse
+                            of those outcomes by the ghost cells copied from them */
 } bh_pool;
 
 /* ---- library --------------------------------------------------------------- */
@@ -132,7 +136,12 @@ int bh_ghosts(const bh_params *P, const bh_pool *pool, const int32_t *patches, i
 /* reconstruction loop of rk2integrator::rkstg (solver/integrator.cpp:288-310) */
 int bh_prims(const bh_params *P, const bh_pool *pool, void *stream);
 /* ghosts + reconstruction loop fused, valid when every leaf patch is in a
- * single ghost-fill wave (no prolongation dependencies) */
+ * single ghost-fill wave (no prolongation dependencies).  With
+ * pool->status set, interior cells are recovered first and a ghost cell
+ * copied from a leaf cell at the same (r, theta) whose con2prim succeeded
+ * takes that cell's primitives: the reference's two con2prim calls on the
+ * identical U and position return exactly them (grid.cpp:538-570,
+ * integrator.cpp:288-310). */
 int bh_ghosts_prims(const bh_params *P, const bh_pool *pool, void *stream);
 /* conserved update loop of rkstg (solver/integrator.cpp:325-347) */
 int bh_update(const bh_params *P, const bh_pool *pool, const double *dt_dev, int32_t stage,

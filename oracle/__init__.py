@@ -100,8 +100,10 @@ def _params(M, a, Q, gamma, limiter=1, maxiter=500, tol=1e-10):
 class Oracle:
     """ctypes front end of liboracle.so (the C restatement)."""
 
-    def __init__(self, M=0.0, a=0.0, Q=0.0, gamma=4.0 / 3.0, limiter=1, maxiter=500, tol=1e-10):
-        path = os.path.join(HERE, "liboracle.so")
+    def __init__(self, M=0.0, a=0.0, Q=0.0, gamma=4.0 / 3.0, limiter=1, maxiter=500, tol=1e-10, fma=False):
+        """fma=True loads the build with fused multiply-add contraction: the
+        same algorithm with different last-bit rounding everywhere."""
+        path = os.path.join(HERE, "liboracle_fma.so" if fma else "liboracle.so")
         if not os.path.exists(path):
             build(ref=False)
         self.lib = C.CDLL(path)

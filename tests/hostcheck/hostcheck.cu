@@ -91,7 +91,14 @@ void hc_ghosts_prims(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < pool->nleaf; i++)
         for (int e = 0; e < N_STRIP; e++) ghost_fill_item(k, P, pool->leaves[i], e);
-    hc_prims(Pp, pool, 1);
+    if (pool->status && pool->leafmask) {
+        for (int i = 0; i < pool->nleaf; i++)
+            for (int c = 0; c < N_INT; c++) prims_interior_item(k, P, pool->leaves[i], c);
+        for (int i = 0; i < pool->nleaf; i++)
+            for (int e = 0; e < N_GHOST; e++) prims_ghost_item(k, P, pool->leaves[i], e);
+    } else {
+        hc_prims(Pp, pool, 1);
+    }
 }
 void hc_update(const bh_params* Pp, const bh_pool* pool, double dt, int stage) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);

@@ -92,12 +92,13 @@ def test_kernel_items_bitwise(case):
     assert eq(hh.U, hp.U) and eq(hh.W, hp.W)
 
 
+@pytest.mark.parametrize("reuse", [True, False])
 @pytest.mark.parametrize("case", CASES)
-def test_steps_bitwise(case):
+def test_steps_bitwise(case, reuse):
     q, orc, hp = box_case(2, seed=4, **case)
     hk = HostKernels(case["M"], case["a"], 0.0, GAMMA, case["lim"])
     hh = hp.copy()
-    pool = hk.pool(hh)
+    pool = hk.pool(hh, reuse=reuse)
     off = np.array([0, hp.npatch], np.int32)
     waves = np.arange(hp.npatch, dtype=np.int32)
     for _ in range(3):
