@@ -1,6 +1,8 @@
 """Compile libbhgpu.so in-tree for sm_100a.
 
-    python -m bhgpu.build      (from black-hole-simulator_b200/)
+    python black-hole-simulator_b200/bhgpu/build.py
+
+(run as a script: importing the package loads the library it builds)
 """
 from __future__ import annotations
 

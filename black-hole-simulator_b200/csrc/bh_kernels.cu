@@ -18,17 +18,19 @@ namespace {
 constexpr int TPB = 128;
 // minimum resident CTAs per SM requested from ptxas for the heavy kernels
 // (caps their registers per thread); tuned on B200
+// (a sweep of 1..6 on the 128^3 box: con2prim and floors run fastest at 6
+// CTAs of 128 threads per SM, the flux kernel at 5, the update at 3)
 #ifndef BH_MINB_PRIMS
-#define BH_MINB_PRIMS 1
+#define BH_MINB_PRIMS 6
 #endif
 #ifndef BH_MINB_FLUX
-#define BH_MINB_FLUX 1
+#define BH_MINB_FLUX 5
 #endif
 #ifndef BH_MINB_FLOORS
-#define BH_MINB_FLOORS 1
+#define BH_MINB_FLOORS 6
 #endif
 #ifndef BH_MINB_UPDATE
-#define BH_MINB_UPDATE 1
+#define BH_MINB_UPDATE 3
 #endif
 
 // ---- thin kernels: thread index -> item --------------------------------

@@ -100,15 +100,29 @@ def _params(M, a, Q, gamma, limiter=1, maxiter=500, tol=1e-10):
 class Oracle:
     """ctypes front end of liboracle.so (the C restatement)."""
 
-    def __init__(self, M=0.0, a=0.0, Q=0.0, gamma=4.0 / 3.0, limiter=1, maxiter=500, tol=1e-10, fma=False):
-        """fma=True loads the build with fused multiply-add contraction: the
-        same algorithm with different last-bit rounding everywhere."""
-        path = os.path.join(HERE, "liboracle_fma.so" if fma else "liboracle.so")
+    def __init__(self, M=0.0, a=0.0, Q=0.0, gamma=4.0 / 3.0, limiter=1, maxiter=500, tol=1e-10, fma=False,
+                 noise=False, seed=0):
+        """fma=True loads the build with fused multiply-add contraction, and
+        noise=True the build whose libm results carry one-ulp noise (pattern
+        chosen by seed): the same algorithm with different last-bit rounding
+        (see bh_oracle.c).  The noise seed is process-wide; it is set again
+        before every call of this object."""
+        name = "liboracle_fma.so" if fma else "liboracle_noise.so" if noise else "liboracle.so"
+        path = os.path.join(HERE, name)
         if not os.path.exists(path):
             build(ref=False)
         self.lib = C.CDLL(path)
         self.P = _params(M, a, Q, gamma, limiter, maxiter, tol)
+        self.noise_seed = seed if noise else None
         L = self.lib
+        if noise:
+            L.orc_set_noise_seed.argtypes = [C.c_uint64]
+            _orig = {}
+            for fname in ("orc_metric_batch", "orc_ptoc_batch", "orc_ctop_batch", "orc_hlld_batch", "orc_geometry",
+                          "orc_fluxcomp_all", "orc_ghosts_all", "orc_prims", "orc_update", "orc_rkstg",
+                          "orc_floors_all", "orc_dtcomp", "orc_step", "orc_ct_all", "orc_div_source_all"):
+                _orig[fname] = getattr(L, fname)
+            self._noise_fns = _orig
         PP, PO = C.POINTER(OrcParams), C.POINTER(OrcPool)
         L.orc_metric_batch.argtypes = [PP, _dp, _dp, C.c_int64, _dp]
         L.orc_ptoc_batch.argtypes = [PP, _dp, _dp, _dp, C.c_int64, _dp, _dp]
@@ -137,6 +151,14 @@ class Oracle:
     def _chk(self, rc):
         if rc < 0:
             raise DomainError("density is not positive (reference thermo.cpp:11)")
+
+    def __getattribute__(self, name):
+        seed = object.__getattribute__(self, "__dict__").get("noise_seed")
+        if seed is not None and name in ("metric", "ptoc", "ctop", "hlld", "geometry", "reconfp_all", "fluxcomp",
+                                         "emfcomp", "bfupdate", "f2cb", "ct", "div_source", "ghosts", "prims",
+                                         "update", "rkstg", "floors", "dtcomp", "step", "maxdivb"):
+            object.__getattribute__(self, "lib").orc_set_noise_seed(seed)
+        return object.__getattribute__(self, name)
 
     # ---- stateless physics (SoA [8][n]) -------------------------------
     def metric(self, r, th):

@@ -11,6 +11,34 @@
 #include <math.h>
 #include <string.h>
 
+#ifdef ORC_NOISE
+/* Built with -DORC_NOISE (liboracle_noise.so): every libm result on the
+ * path (sin, cos, acos, log, exp, pow) is moved by at most one ulp, as a
+ * deterministic function of its bits -- the same algorithm on a different
+ * but equally accurate math library.  Its divergence from the plain build
+ * measures how far the reference's own result is defined. */
+static uint64_t orc_noise_seed = 0;
+void orc_set_noise_seed(uint64_t s) { orc_noise_seed = s; }
+static inline double orc_noise(double y) {
+    if (!isfinite(y) || y == 0.0) return y;
+    uint64_t b;
+    memcpy(&b, &y, sizeof b);
+    uint64_t h = (b ^ (orc_noise_seed * 0xD6E8FEB86659FD93ull)) * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29; h *= 0xBF58476D1CE4E5B9ull; h ^= h >> 32;
+    switch (h % 3) {
+    case 0: return nextafter(y, -INFINITY);
+    case 1: return y;
+    default: return nextafter(y, INFINITY);
+    }
+}
+#define sin(x) orc_noise(sin(x))
+#define cos(x) orc_noise(cos(x))
+#define acos(x) orc_noise(acos(x))
+#define log(x) orc_noise(log(x))
+#define exp(x) orc_noise(exp(x))
+#define pow(x, y) orc_noise(pow(x, y))
+#endif
+
 #define BLK ORC_BLOCK
 #define GH ORC_GHOST
 #define CPN ORC_CPN

@@ -54,6 +54,22 @@ def ulp_sensitivity(orc, hp, steps=1, seed=0):
     return [rel_linf(pert.U[:, v], base.U[:, v]) for v in range(8)]
 
 
+def rel_l1(a, b):
+    """Per-variable relative L1 error over the entries finite in both."""
+    out = []
+    for v in range(a.shape[1]):
+        x = np.asarray(a)[:, v]; y = np.asarray(b)[:, v]
+        m = np.isfinite(x) & np.isfinite(y)
+        den = np.abs(y[m]).mean() if m.any() else 0.0
+        num = np.abs(x[m] - y[m]).mean() if m.any() else 0.0
+        out.append(float(num / den) if den > 0 else float(num))
+    return out
+
+
+def mask_disagreement(a, b):
+    return float(np.mean(np.isfinite(a) != np.isfinite(b)))
+
+
 def same_nan(a, b):
     return np.array_equal(np.isfinite(a), np.isfinite(b))
 

@@ -14,9 +14,15 @@ Tolerances written here:
   one-ulp change of its input (measured on the oracle itself), so Brent
   cells may differ at most at the oracle's own one-ulp flip rate; with
   exactly representable metric inputs Brent results are identical;
-* whole steps: relative L-infinity <= 1e-12 per conserved field (D, the
-  vector S, tau, the vector B), identical NaN masks, and per component
-  within 8x the oracle's own response to a one-ulp input perturbation."""
+* the first step from a seeded state: relative L-infinity <= 1e-12 per
+  conserved field (D, the vector S, tau, the vector B), identical NaN
+  masks, and per component within 8x the oracle's own response to a
+  one-ulp input perturbation;
+* later steps: the reference's own result is only defined up to its
+  response to last-bit rounding (its Brent fallback and the blow-up of the
+  magnetised box amplify one ulp to O(1) within two steps), measured by
+  the oracle built with one-ulp noise on every libm result; the GPU's NaN
+  mask and per-variable L1 error stay within 2x / 8x of that envelope."""
 import math
 
 import numpy as np
@@ -24,8 +30,8 @@ import pytest
 import torch
 
 import oracle
-from helpers import (GAMMA, box_case, field_linf, gpu_tree, rel_linf, random_prims, same_nan,
-                     ulp_sensitivity)
+from helpers import (GAMMA, box_case, field_linf, gpu_tree, mask_disagreement, rel_l1, rel_linf, random_prims,
+                     same_nan, ulp_sensitivity)
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
@@ -203,40 +209,88 @@ def _step_gate(tree, hp, sens, label):
     assert rel_linf(_np(tree.Bf), hp.Bf) <= TOL, label
 
 
-def _divergence(a, b):
-    """(NaN-mask disagreement fraction, per-component relative Linf on the
-    entries finite in both) between two [np][8][n] states."""
-    fa, fb = np.isfinite(a), np.isfinite(b)
-    return float(np.mean(fa != fb)), [rel_linf(a[:, v], b[:, v]) for v in range(a.shape[1])]
+NOISE_SEEDS = range(6)
+
+
+def _envelope(noisy_states, ref_U):
+    """Largest NaN-mask disagreement and per-variable relative L1 error of
+    the noisy-oracle realisations against the plain oracle."""
+    mask = max(mask_disagreement(h.U, ref_U) for h in noisy_states)
+    l1 = np.max([rel_l1(h.U, ref_U) for h in noisy_states], axis=0)
+    return mask, l1
+
+
+def _envelope_gate(gpu_U, ref_U, noisy_states, label):
+    """After the first step the reference's result is defined only up to its
+    own sensitivity to last-bit rounding: the same algorithm with one-ulp
+    noise on every libm result (the noisy oracle, several noise patterns)
+    moves it by this much.  The GPU, whose math library differs from the
+    host's in the last bit, must stay within a small multiple of it."""
+    own_mask, own_l1 = _envelope(noisy_states, ref_U)
+    gpu_mask = mask_disagreement(gpu_U, ref_U)
+    assert gpu_mask <= 2 * own_mask + 1e-3, (label, gpu_mask, own_mask)
+    gpu = rel_l1(gpu_U, ref_U)
+    for v in range(8):
+        assert gpu[v] <= 8 * own_l1[v] + 1e-13, (label, v, gpu[v], own_l1[v])
+
+
+def _noisy(case):
+    return [oracle.Oracle(case["M"], case["a"], 0.0, GAMMA, limiter=case["lim"], noise=True, seed=k)
+            for k in NOISE_SEEDS]
 
 
 @pytest.mark.parametrize("case", CASES)
-def test_two_steps(case):
-    """Step 1 meets the strict gate.  From step 2 on the flat-metric box is
-    chaotic in the reference itself: the same algorithm compiled with fused
-    multiply-add (last-bit rounding changed everywhere, as on the GPU)
-    moves D by tens of per cent and changes the NaN mask.  The GPU must
-    stay within a small multiple of that self-divergence."""
+def test_free_running_steps(case):
+    """Three free-running steps: step 1 meets the strict gate; steps 2-3
+    (where the flat-metric box is chaotic in the reference itself) stay
+    within the envelope of the noisy oracle, each realisation with its own
+    cell geometry as the GPU has its own."""
     import bhgpu
     q, orc, hp = box_case(2, seed=4, **case)
-    pert = hp.copy()
-    orc_fma = oracle.Oracle(case["M"], case["a"], 0.0, GAMMA, limiter=case["lim"], fma=True)
+    noisy = _noisy(case)
+    hns = [hp.copy() for _ in noisy]
+    for o, h in zip(noisy, hns):
+        o.geometry(h)
     sens1 = ulp_sensitivity(orc, hp, steps=1)
     tree = gpu_tree(q, hp, case["M"], case["a"], case["lim"])
     rk = bhgpu.RK2Integrator(0.4)
-    for s in range(2):
-        dtg = rk.step(tree)
+    for s in range(3):
+        dtg = rk.step(tree, check_domain=False)
         dtc = orc.step(hp, 0.4)
-        orc_fma.step(pert, 0.4)
+        for o, h in zip(noisy, hns):
+            o.step(h, 0.4)
         if s == 0:
             assert abs(dtg - dtc) <= TOL * dtc
             _step_gate(tree, hp, sens1, "step 1")
         else:
-            own_mask, own_err = _divergence(pert.U, hp.U)
-            gpu_mask, gpu_err = _divergence(_np(tree.U), hp.U)
-            assert gpu_mask <= 4 * own_mask + 1e-4, (gpu_mask, own_mask)
-            for v in range(8):
-                assert gpu_err[v] <= max(TOL, 8 * own_err[v]), (v, gpu_err[v], own_err[v])
+            _envelope_gate(_np(tree.U), hp.U, hns, f"step {s + 1}")
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_stepwise_from_identical_state(case):
+    """Three consecutive steps, each started from the oracle's state (cell
+    geometry included): each GPU step stays within the envelope of the
+    noisy oracle started from the same state, and the first meets the
+    strict gate."""
+    import bhgpu
+    q, orc, hp = box_case(2, seed=4, **case)
+    noisy = _noisy(case)
+    tree = gpu_tree(q, hp, case["M"], case["a"], case["lim"])
+    tree.rth.copy_(torch.as_tensor(hp.rth))
+    rk = bhgpu.RK2Integrator(0.4)
+    for k in range(3):
+        tree.load(U=hp.U, W=hp.W, Bf=hp.Bf, dU=hp.dU)
+        hns = [hp.copy() for _ in noisy]
+        sens = ulp_sensitivity(orc, hp, steps=1) if k == 0 else None
+        dtg = rk.step(tree, check_domain=False)
+        dtc = orc.step(hp, 0.4)
+        for o, h in zip(noisy, hns):
+            o.step(h, 0.4)
+        if k == 0:
+            assert abs(dtg - dtc) <= TOL * dtc
+            _step_gate(tree, hp, sens, "step 1")
+        else:
+            _envelope_gate(_np(tree.U), hp.U, hns, f"step {k + 1} from the oracle's state")
 
 
 def test_magnetised_box_64cubed_one_step():
