@@ -60,6 +60,7 @@ def _load():
         "bh_ghosts": ([P, PP, _vp, i32, _vp], C.c_int),
         "bh_prims": ([P, PP, _vp], C.c_int),
         "bh_ghosts_prims": ([P, PP, _vp], C.c_int),
+        "bh_ghosts_prims_static": ([P, PP, _vp], C.c_int),
         "bh_update": ([P, PP, _vp, i32, _vp], C.c_int),
         "bh_floors": ([P, PP, _vp], C.c_int),
         "bh_dtcomp": ([P, PP, dbl, _vp, _vp], C.c_int),

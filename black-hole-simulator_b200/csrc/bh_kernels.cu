@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
+#include <mutex>
 #include "bhgpu.h"
 #include "bh_items.cuh"
 
@@ -129,6 +130,30 @@ inline int launched() { return cudaGetLastError() == cudaSuccess ? BH_OK : BH_EC
 inline bool bad_pool(const bh_pool* p) { return !p || p->npatch <= 0 || !p->all; }
 inline dim3 grid2(int items, int npatch, int z = 1) { return dim3((items + TPB - 1) / TPB, npatch, z); }
 
+// ---- library-owned scratch for bh_ghosts_prims_static ---------------------
+// The con2prim outcome of every interior cell, BH_STATIC_MAX_PATCHES x 8000
+// bytes, held by every GPU that loads the library until the process exits.
+// Host code cannot use the array's name as a device address: each device's
+// address is looked up once (cudaGetSymbolAddress, on the first call made
+// with that device current) and handed to the kernels.
+__device__ __align__(256) uint8_t g_static_status[(size_t)BH_STATIC_MAX_PATCHES * NC];
+constexpr int kMaxDevices = 64;
+void* g_static_status_ptr[kMaxDevices] = {nullptr};
+std::mutex g_static_status_mu;
+
+int static_status_ptr(uint8_t** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BH_ECUDA;
+    std::lock_guard<std::mutex> lock(g_static_status_mu);
+    if (!g_static_status_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_static_status) != cudaSuccess || !p) return BH_ECUDA;
+        g_static_status_ptr[dev] = p;
+    }
+    *out = (uint8_t*)g_static_status_ptr[dev];
+    return BH_OK;
+}
+
 }  // namespace
 
 // ==========================================================================
@@ -243,6 +268,20 @@ int bh_ghosts_prims(const bh_params* P, const bh_pool* pool, void* stream) {
     } else {
         k_prims<<<grid2(NC, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves, 1);
     }
+    return launched();
+}
+int bh_ghosts_prims_static(const bh_params* P, const bh_pool* pool, void* stream) {
+    if (!P || bad_pool(pool) || !pool->leafmask) return BH_EINVAL;
+    if (pool->npatch > BH_STATIC_MAX_PATCHES) return BH_ERANGE;
+    if (pool->nleaf == 0) return BH_OK;
+    uint8_t* status = nullptr;
+    int rc = static_status_ptr(&status);
+    if (rc) return rc;
+    Pool pv = pool_of(pool);
+    pv.status = status;   // every entry read below is written by k_prims_interior first
+    k_ghost_fill<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
+    k_prims_interior<<<grid2(N_INT, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
+    k_prims_ghost<<<grid2(N_GHOST, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
     return launched();
 }
 int bh_update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, void* stream) {

@@ -143,6 +143,25 @@ int bh_prims(const bh_params *P, const bh_pool *pool, void *stream);
  * identical U and position return exactly them (grid.cpp:538-570,
  * integrator.cpp:288-310). */
 int bh_ghosts_prims(const bh_params *P, const bh_pool *pool, void *stream);
+/* No counterpart in the reference (it allocates nothing on a GPU): the
+ * ghost fill and reconstruction of bh_ghosts_prims for callers that cannot
+ * allocate device memory -- a host that records the time step into a CUDA
+ * graph (cudaMalloc is not allowed while a stream is being captured) or
+ * one whose memory arena owns every device byte and lends libraries none.
+ * The per-cell con2prim outcome that bh_ghosts_prims keeps in the caller's
+ * pool->status is kept instead in a scratch array inside this library,
+ * BH_STATIC_MAX_PATCHES x 8000 bytes (8 MB), which every GPU that loads
+ * the library holds until the process exits; pool->status is ignored.
+ * Nothing is allocated or freed; pools of more than BH_STATIC_MAX_PATCHES
+ * patches are rejected with BH_ERANGE before anything is launched.
+ * The first call on each device, with that device current, looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Every call uses the same array and leaves its
+ * contents behind; each call writes every entry it later reads, so nothing
+ * needs clearing, but calls that overlap on the GPU (concurrent streams)
+ * race on the array.  Results equal bh_ghosts_prims bit for bit. */
+#define BH_STATIC_MAX_PATCHES 1024
+int bh_ghosts_prims_static(const bh_params *P, const bh_pool *pool, void *stream);
 /* conserved update loop of rkstg (solver/integrator.cpp:325-347) */
 int bh_update(const bh_params *P, const bh_pool *pool, const double *dt_dev, int32_t stage,
               void *stream);
