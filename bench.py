@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--grid", type=int, default=128, choices=[64, 128])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--con2prim-batch", type=int, default=1, help="also measure the 2^24-cell con2prim batch")
+    ap.add_argument("--precision", default="fp64-fma", choices=["fp64", "fp64-fma"],
+                    help="arithmetic variant of the headline value; the other FP64 form is timed beside it")
     return ap.parse_args()
 
 
@@ -114,13 +117,13 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-def make_tree(nq, seed):
+def make_tree(nq, seed, precision="fp64"):
     import bhgpu
     from bhgpu import configs
     from bhgpu.mesh import Quilt
     q = Quilt([LO] * 3, [HI] * 3, nq, periodic=True)
     tree = bhgpu.AmrTree(q.dom_l, q.dom_h, nq, M=0.0, a=0.0, Q=0.0, gm=GAMMA, periodic=True,
-                         limiter="minmod", quilt=q, init_floor=False)
+                         limiter="minmod", quilt=q, init_floor=False, precision=precision)
     W, Bf = configs.magnetised_box(q, seed=seed, gamma=GAMMA)
     tree.load(W=W, Bf=Bf)
     tree.prim_to_cons()
@@ -195,6 +198,57 @@ def cpu_reference_sample(threads):
 
 
 # ---------------------------------------------------------------------------
+# con2prim stress batch: 2^24 independent Kerr cells (a = 0.9375)
+C2P_ALG_BYTES = 8 * 8 + 2 * 8 + 5 * 8 + 4   # U + (r, theta) in; rho, eps, v out; iterations
+
+
+def con2prim_batch(n_cells=1 << 24, reps=3):
+    import numpy as np
+    import torch
+    import bhgpu
+    from bhgpu import configs
+    W, r, th = configs.con2prim_batch(n_cells, seed=4, gamma=GAMMA, a=0.9375)
+    mtr, stt = bhgpu.Metric(1.0, 0.9375, 0.0), bhgpu.State(GAMMA)
+    cn = bhgpu.Conserved(mtr, stt)
+    U, _ = cn.ptoc(W, r, th, check_domain=False)
+    rd, thd = torch.as_tensor(r, device="cuda"), torch.as_tensor(th, device="cuda")
+    cn.ctop(U, rd, thd, check_domain=False)      # warm-up
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        Wg, _, st, it, pa = cn.ctop(U, rd, thd, check_domain=False)
+    b.record(); torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    st, it, pa = st.cpu().numpy(), it.cpu().numpy(), pa.cpu().numpy()
+    out = {"workload": f"configs[3]: {n_cells} independent Kerr-Schild cells (a=0.9375, Gamma=4/3), "
+                       "log-uniform rho, W in [1,20], log-uniform sigma, isotropic v and B, r in [1.5,50]",
+           "cells": n_cells, "ms": ms, "cells_per_s": n_cells / (ms / 1e3),
+           "recovered_frac": float(np.mean(st == 1)), "failed_frac": float(np.mean(st == 0)),
+           "domain_error_frac": float(np.mean(st < 0)),
+           "routes": {"newton": float(np.mean(pa == 0)), "newton_cap": float(np.mean(pa == 1)),
+                      "brent": float(np.mean(pa == 2)), "brent_failed": float(np.mean(pa == 3))},
+           "mean_newton_iters": float(it.mean()),
+           "alg_bytes_per_cell": C2P_ALG_BYTES,
+           "achieved_GBs": n_cells * C2P_ALG_BYTES / (ms / 1e3) / 1e9}
+    # the reference's own conserved::ctop on a sample, all host threads
+    try:
+        import oracle
+        if oracle.ref_available():
+            ns = 1 << 16
+            ref = oracle.RefSolver([LO] * 3, [HI] * 3, 1, 1.0, 0.9375, 0.0, GAMMA)
+            Us = U[:, :ns].cpu().numpy()
+            t0 = time.perf_counter()
+            ref.ctop(Us, r[:ns], th[:ns])
+            t = time.perf_counter() - t0
+            out["cpu_reference"] = {"cells_per_s": ns / t, "cores": os.cpu_count() or 1,
+                                    "sample": f"reference conserved::ctop on the first {ns} cells"}
+    except Exception as e:      # the CPU figure is informational
+        out["cpu_reference"] = {"error": str(e)}
+    return out
+
+
+# ---------------------------------------------------------------------------
 def run_reference(args):
     rank, _, world = env_rank()
     if rank != 0:
@@ -262,7 +316,7 @@ def run_ours(args):
     from bhgpu.solver import _p, _stream
 
     nq = args.grid // 16
-    tree = make_tree(nq, seed=1)
+    tree = make_tree(nq, seed=1, precision=args.precision)
     zones = (nq * 16) ** 3
     U0, W0, B0 = tree.U.clone(), tree.W.clone(), tree.Bf.clone()
     L = bhgpu.lib
@@ -325,6 +379,23 @@ def run_ours(args):
     ms_max = float(t.item())
     err = tree.read_error()
 
+    # ---- the other FP64 form, same workload, for comparison --------------------
+    other = "fp64" if args.precision == "fp64-fma" else "fp64-fma"
+    tree.precision = other
+    P = tree.params()
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    a0 = torch.cuda.Event(enable_timing=True); b0 = torch.cuda.Event(enable_timing=True)
+    k_other = max(10, args.steps // 4)
+    a0.record()
+    for _ in range(k_other):
+        step()
+    b0.record(); torch.cuda.synchronize()
+    other_ms = a0.elapsed_time(b0) / k_other
+    tree.precision = args.precision
+    P = tree.params()
+
     # ---- end to end through the public API with host buffers --------------
     pin = lambda x: x.cpu().pin_memory()
     hU, hW, hB = pin(U0), pin(W0), pin(B0)
@@ -364,6 +435,9 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "precision": args.precision,
+            "other_precision": {"precision": other, "ms_per_step": other_ms,
+                                "value": world * zones / (other_ms / 1e3)},
             "config": {"workload": f"magnetised box {args.grid}^3: flat metric, periodic, PLM-minmod + HLLD + CT, "
                                    f"RK2 CFL 0.4, reference-faithful FP64", "grid": f"{args.grid}^3",
                        "patches": tree.npatch, "patch": "16^3 + 2 ghosts", "parallelism": f"replicas x{world}",
@@ -384,6 +458,8 @@ def run_ours(args):
             threads = os.cpu_count() or 1
             v, kind, sample = cpu_reference_sample(threads)
             line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample}
+            if args.con2prim_batch:
+                line["con2prim_batch"] = con2prim_batch()
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

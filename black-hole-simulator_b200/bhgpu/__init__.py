@@ -5,7 +5,7 @@ Python API named after the reference solver's C++ entry points.
 """
 from ._lib import lib, LIB_PATH, BhError  # noqa: F401  (raises if the CUDA library is missing)
 from .mesh import Quilt, BLOCK, GHOST, CPN, NC, NF, NE  # noqa: F401
-from .solver import (Metric, State, Conserved, hlld, AmrTree, RK2Integrator, DomainError,  # noqa: F401
+from .solver import (Metric, State, Conserved, hlld, AmrTree, RK2Integrator, StepGraph, DomainError,  # noqa: F401
                      BH_MINMOD, BH_VANLEER, BH_MC)
 from . import configs  # noqa: F401
 

@@ -14,13 +14,15 @@ LIB_PATH = os.path.join(HERE, "libbhgpu.so")
 BH_OK, BH_EINVAL, BH_ECUDA, BH_ERANGE = 0, -1, -2, -3
 BH_ERR_DOMAIN = 1
 BH_MINMOD, BH_VANLEER, BH_MC = 0, 1, 2
+BH_FP64, BH_FP64_FMA = 0, 1
 _vp = C.c_void_p
 
 
 class BhParams(C.Structure):
     _fields_ = [("M", C.c_double), ("a", C.c_double), ("Q", C.c_double), ("gamma", C.c_double),
                 ("limiter", C.c_int32), ("maxiter", C.c_int32), ("tol", C.c_double),
-                ("cM", C.c_double), ("ca", C.c_double), ("cQ", C.c_double)]
+                ("cM", C.c_double), ("ca", C.c_double), ("cQ", C.c_double),
+                ("precision", C.c_int32), ("reserved", C.c_int32)]
 
 
 class BhPool(C.Structure):

@@ -17,9 +17,11 @@ CSRC = os.path.join(PKG, "csrc")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# --fmad=false keeps the reference's separate multiply/add roundings
-COMMON = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
           "-I" + os.path.join(REPO, "include"), "-I" + CSRC]
+# --fmad=false keeps the reference's separate multiply/add roundings; only the
+# FMA variant contracts
+FMAD = {"bh_fp64fma.cu": "--fmad=true"}
 
 
 def sources():
@@ -33,12 +35,24 @@ def build(verbose: bool = False) -> str:
     deps.append(os.path.join(REPO, "include", "bhgpu.h"))
     if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
         return out
-    cmd = [NVCC] + ARCH + COMMON + ["-shared", "-o", out] + srcs
+    objs = []
+    bdir = os.path.join(PKG, "_build")
+    os.makedirs(bdir, exist_ok=True)
+    for src in srcs:
+        obj = os.path.join(bdir, os.path.basename(src).replace(".cu", ".o"))
+        cmd = [NVCC] + ARCH + COMMON + [FMAD.get(os.path.basename(src), "--fmad=false"), "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        objs.append(obj)
+    cmd = [NVCC] + ARCH + ["-shared", "-o", out] + objs
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     return out
 
 

@@ -18,13 +18,16 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import BH_ERR_DOMAIN, BH_MC, BH_MINMOD, BH_VANLEER, BhParams, BhPool, check, lib
+from ._lib import BH_ERR_DOMAIN, BH_FP64, BH_FP64_FMA, BH_MC, BH_MINMOD, BH_VANLEER, BhParams, BhPool, check, lib
 from .mesh import NC, NE, NF, Quilt
 
-__all__ = ["Metric", "State", "Conserved", "hlld", "AmrTree", "RK2Integrator", "DomainError",
+__all__ = ["Metric", "State", "Conserved", "hlld", "AmrTree", "RK2Integrator", "StepGraph", "DomainError",
            "BH_MINMOD", "BH_VANLEER", "BH_MC"]
 
 _LIMITERS = {"minmod": BH_MINMOD, "vanleer": BH_VANLEER, "mc": BH_MC, "mclim": BH_MC}
+# arithmetic variants: "fp64" keeps the reference's separate roundings (the
+# parity form); "fp64-fma" contracts multiply-add pairs
+PRECISIONS = {"fp64": BH_FP64, "fp64-fma": BH_FP64_FMA}
 
 
 class DomainError(ValueError):
@@ -73,11 +76,12 @@ class State:
         self.gamma = float(gm)
 
 
-def _params(mtr: Metric, stt: State, limiter=BH_VANLEER, maxiter=500, tol=1e-10) -> BhParams:
+def _params(mtr: Metric, stt: State, limiter=BH_VANLEER, maxiter=500, tol=1e-10, precision="fp64") -> BhParams:
     # every cell carries a default-constructed metric() = (M=1, a=0, Q=0)
     # (cell.hpp:25, metric.hpp:30); the kernels use it where the reference
     # evaluates c.mtr
-    return BhParams(mtr.M, mtr.a, mtr.Q, stt.gamma, int(limiter), int(maxiter), float(tol), 1.0, 0.0, 0.0)
+    prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    return BhParams(mtr.M, mtr.a, mtr.Q, stt.gamma, int(limiter), int(maxiter), float(tol), 1.0, 0.0, 0.0, prec, 0)
 
 
 class Conserved:
@@ -151,14 +155,17 @@ class AmrTree:
 
     ``periodic`` wraps the level-0 neighbour search; ``limiter`` selects the
     slope limiter of the flux reconstruction (the reference's fluxcomp
-    always uses van Leer, recon.hpp:41).
+    always uses van Leer, recon.hpp:41); ``precision`` selects the
+    arithmetic variant ("fp64" reproduces the reference's roundings,
+    "fp64-fma" contracts multiply-add pairs).
     """
 
     def __init__(self, dom_l, dom_h, nqlt: int, M: float = 1.0, a: float = 0.0, Q: float = 0.0,
                  gm: float = 5.0 / 3.0, periodic: bool = False, limiter="vanleer", quilt: Quilt | None = None,
-                 device="cuda", init_floor: bool = True):
+                 device="cuda", init_floor: bool = True, precision: str = "fp64"):
         self.mtr = Metric(M, a, Q)
         self.stt = State(gm)
+        self.precision = precision
         self.limiter = _LIMITERS[limiter] if isinstance(limiter, str) else int(limiter)
         self.quilt = quilt if quilt is not None else Quilt(dom_l, dom_h, nqlt, periodic)
         self.device = torch.device(device)
@@ -203,7 +210,7 @@ class AmrTree:
         check(lib.bh_geometry(C.byref(self.pool), _stream()), "patch::cell_init")
 
     def params(self, maxiter=500, tol=1e-10) -> BhParams:
-        return _params(self.mtr, self.stt, self.limiter, maxiter, tol)
+        return _params(self.mtr, self.stt, self.limiter, maxiter, tol, self.precision)
 
     def _init_floor(self):
         """Every cell starts at amrtree::pvfs and its ptoc (grid.cpp:193-205)."""
@@ -375,3 +382,36 @@ class RK2Integrator:
         if check_domain:
             tree.check()
         return float(tree.dt.item()) if sync else tree.dt
+
+
+class StepGraph:
+    """rk2integrator::step recorded once into a CUDA graph and replayed.
+
+    The step's 17 launches (dtcomp, two stages, floors) read dt from device
+    memory and never synchronise with the host, so the whole step is one
+    graph; ``before`` (optional) is recorded in front of it, e.g. a copy
+    that resets the state.  Replays run on the current stream.  The domain
+    error word is left to the caller (``tree.check()``).
+    """
+
+    def __init__(self, tree: AmrTree, integrator: RK2Integrator, before=None, warmup: int = 1):
+        self.tree, self.integrator, self.before = tree, integrator, before
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                self._body()
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._body()
+
+    def _body(self):
+        if self.before is not None:
+            self.before()
+        self.integrator.step(self.tree, sync=False, check_domain=False)
+
+    def replay(self):
+        self.graph.replay()
+        return self.tree.dt

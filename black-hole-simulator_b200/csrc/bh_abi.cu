@@ -1,0 +1,121 @@
+// bh_abi.cu -- the C ABI (include/bhgpu.h): argument checks and dispatch
+// to the arithmetic variant bh_params.precision selects.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <mutex>
+#include "bhgpu.h"
+#include "bh_api.h"
+#include "bh_phys.cuh"
+
+namespace {
+inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
+inline bool bad_pool(const bh_pool* p) { return !p || p->npatch <= 0 || !p->all; }
+constexpr int NC_ = bh::NC;
+// ---- library-owned scratch for bh_ghosts_prims_static ---------------------
+// The con2prim outcome of every interior cell, BH_STATIC_MAX_PATCHES x 8000
+// bytes, held by every GPU that loads the library until the process exits.
+// Host code cannot use the array's name as a device address: each device's
+// address is looked up once (cudaGetSymbolAddress, on the first call made
+// with that device current) and handed to the kernels.
+__device__ __align__(256) uint8_t g_static_status[(size_t)BH_STATIC_MAX_PATCHES * NC_];
+constexpr int kMaxDevices = 64;
+void* g_static_status_ptr[kMaxDevices] = {nullptr};
+std::mutex g_static_status_mu;
+
+int static_status_ptr(uint8_t** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BH_ECUDA;
+    std::lock_guard<std::mutex> lock(g_static_status_mu);
+    if (!g_static_status_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_static_status) != cudaSuccess || !p) return BH_ECUDA;
+        g_static_status_ptr[dev] = p;
+    }
+    *out = (uint8_t*)g_static_status_ptr[dev];
+    return BH_OK;
+}
+
+}  // namespace
+
+#define BH_DISPATCH(P, call)                                 \
+    switch ((P) ? (P)->precision : -1) {                     \
+    case BH_FP64: return vfp64::call;                        \
+    case BH_FP64_FMA: return vfma::call;                     \
+    default: return BH_EINVAL;                               \
+    }
+
+extern "C" {
+
+int bh_abi_version(void) { return BHGPU_ABI_VERSION; }
+
+int bh_read_error(const bh_pool* pool, int32_t* out, void* stream) {
+    if (!pool || !pool->err || !out) return BH_EINVAL;
+    if (cudaMemcpyAsync(out, pool->err, sizeof(int32_t), cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess) return BH_ECUDA;
+    return cudaStreamSynchronize(S(stream)) == cudaSuccess ? BH_OK : BH_ECUDA;
+}
+int bh_clear_error(const bh_pool* pool, void* stream) {
+    if (!pool || !pool->err) return BH_EINVAL;
+    return cudaMemsetAsync(pool->err, 0, sizeof(int32_t), S(stream)) == cudaSuccess ? BH_OK : BH_ECUDA;
+}
+int bh_metric_comp(const bh_params* P, const double* r, const double* th, int64_t n, double* out, void* stream) {
+    BH_DISPATCH(P, metric_comp(P, r, th, n, out, stream));
+}
+int bh_ptoc(const bh_params* P, const double* W, const double* r, const double* th, int64_t n, double* U, double* Wd,
+            void* stream) {
+    BH_DISPATCH(P, ptoc(P, W, r, th, n, U, Wd, stream));
+}
+int bh_ctop(const bh_params* P, const double* U, const double* r, const double* th, int64_t n, double* W, double* Wd,
+            int32_t* status, int32_t* iters, int32_t* path, void* stream) {
+    BH_DISPATCH(P, ctop(P, U, r, th, n, W, Wd, status, iters, path, stream));
+}
+int bh_hlld(const bh_params* P, const double* WL, const double* WR, const double* UL, const double* UR,
+            const double* r, const double* th, int32_t dim, int64_t n, double* F, double* ctspeed, void* stream) {
+    BH_DISPATCH(P, hlld(P, WL, WR, UL, UR, r, th, dim, n, F, ctspeed, stream));
+}
+int bh_geometry(const bh_pool* pool, void* stream) { return vfp64::geometry(pool, stream); }
+int bh_reconfp(const bh_params* P, const bh_pool* pool, int32_t dim, int32_t limiter, double* L, double* R,
+               void* stream) {
+    BH_DISPATCH(P, reconfp(P, pool, dim, limiter, L, R, stream));
+}
+int bh_fluxcomp(const bh_params* P, const bh_pool* pool, void* stream) { BH_DISPATCH(P, fluxcomp(P, pool, stream)); }
+int bh_emfcomp(const bh_pool* pool, void* stream) { return vfp64::emfcomp(pool, stream); }
+int bh_bfupdate(const bh_pool* pool, const double* dt_dev, void* stream) { return vfp64::bfupdate(pool, dt_dev, stream); }
+int bh_f2cb(const bh_params* P, const bh_pool* pool, void* stream) { BH_DISPATCH(P, f2cb(P, pool, stream)); }
+int bh_maxdivb(const bh_pool* pool, double* out, void* stream) { return vfp64::maxdivb(pool, out, stream); }
+int bh_div_source(const bh_params* P, const bh_pool* pool, double* div, double* src, void* stream) {
+    BH_DISPATCH(P, div_source(P, pool, div, src, stream));
+}
+int bh_ghosts(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
+    BH_DISPATCH(P, ghosts(P, pool, patches, n, stream));
+}
+int bh_prims(const bh_params* P, const bh_pool* pool, void* stream) { BH_DISPATCH(P, prims(P, pool, stream)); }
+int bh_ghosts_prims(const bh_params* P, const bh_pool* pool, void* stream) {
+    BH_DISPATCH(P, ghosts_prims(P, pool, stream));
+}
+int bh_ghosts_prims_static(const bh_params* P, const bh_pool* pool, void* stream) {
+    if (!P || bad_pool(pool) || !pool->leafmask) return BH_EINVAL;
+    if (pool->npatch > BH_STATIC_MAX_PATCHES) return BH_ERANGE;
+    if (pool->nleaf == 0) return BH_OK;
+    uint8_t* status = nullptr;
+    int rc = static_status_ptr(&status);
+    if (rc) return rc;
+    // every entry read is written by the interior pass of the same call first
+    BH_DISPATCH(P, ghosts_prims_status(P, pool, status, stream));
+}
+int bh_update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, void* stream) {
+    BH_DISPATCH(P, update(P, pool, dt_dev, stage, stream));
+}
+int bh_floors(const bh_params* P, const bh_pool* pool, void* stream) { BH_DISPATCH(P, floors(P, pool, stream)); }
+int bh_dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
+    BH_DISPATCH(P, dtcomp(P, pool, cfl, dt_dev, stream));
+}
+int bh_rkstg(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, const int32_t* waves,
+             const int32_t* wave_off, int32_t nwave, void* stream) {
+    BH_DISPATCH(P, rkstg(P, pool, dt_dev, stage, waves, wave_off, nwave, stream));
+}
+int bh_step(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, const int32_t* waves,
+            const int32_t* wave_off, int32_t nwave, void* stream) {
+    BH_DISPATCH(P, step(P, pool, cfl, dt_dev, waves, wave_off, nwave, stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,36 @@
+// bh_api.h -- the launch sequences each arithmetic variant provides
+// (defined in bh_variant.cuh, instantiated by bh_fp64.cu and bh_fp64fma.cu)
+#pragma once
+#include <stdint.h>
+#include "bhgpu.h"
+
+#define BH_VARIANT_API(NS)                                                                                       \
+    namespace NS {                                                                                              \
+    int metric_comp(const bh_params*, const double*, const double*, int64_t, double*, void*);                  \
+    int ptoc(const bh_params*, const double*, const double*, const double*, int64_t, double*, double*, void*);  \
+    int ctop(const bh_params*, const double*, const double*, const double*, int64_t, double*, double*, int32_t*, \
+             int32_t*, int32_t*, void*);                                                                        \
+    int hlld(const bh_params*, const double*, const double*, const double*, const double*, const double*,      \
+             const double*, int32_t, int64_t, double*, double*, void*);                                         \
+    int geometry(const bh_pool*, void*);                                                                        \
+    int reconfp(const bh_params*, const bh_pool*, int32_t, int32_t, double*, double*, void*);                  \
+    int fluxcomp(const bh_params*, const bh_pool*, void*);                                                     \
+    int emfcomp(const bh_pool*, void*);                                                                         \
+    int bfupdate(const bh_pool*, const double*, void*);                                                        \
+    int f2cb(const bh_params*, const bh_pool*, void*);                                                         \
+    int maxdivb(const bh_pool*, double*, void*);                                                                \
+    int div_source(const bh_params*, const bh_pool*, double*, double*, void*);                                 \
+    int ghosts(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
+    int prims(const bh_params*, const bh_pool*, void*);                                                        \
+    int ghosts_prims_status(const bh_params*, const bh_pool*, uint8_t*, void*);                                \
+    int ghosts_prims(const bh_params*, const bh_pool*, void*);                                                 \
+    int update(const bh_params*, const bh_pool*, const double*, int32_t, void*);                               \
+    int floors(const bh_params*, const bh_pool*, void*);                                                       \
+    int dtcomp(const bh_params*, const bh_pool*, double, double*, void*);                                      \
+    int rkstg(const bh_params*, const bh_pool*, const double*, int32_t, const int32_t*, const int32_t*, int32_t, \
+              void*);                                                                                           \
+    int step(const bh_params*, const bh_pool*, double, double*, const int32_t*, const int32_t*, int32_t, void*); \
+    }
+
+BH_VARIANT_API(vfp64)
+BH_VARIANT_API(vfma)

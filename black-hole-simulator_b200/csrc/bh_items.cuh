@@ -90,7 +90,7 @@ struct EdgeCells {
                 }
     }
 };
-__constant__ EdgeCells kEdgeCells = EdgeCells();          // device copy
+static __constant__ EdgeCells kEdgeCells = EdgeCells();   // device copy (one per translation unit)
 static constexpr EdgeCells hEdgeCells = EdgeCells();      // host copy
 #ifdef __CUDA_ARCH__
 #define BH_EDGE_CELLS kEdgeCells

@@ -405,7 +405,7 @@ BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, cons
 
 // floor state amrtree::pvfs (grid.cpp:133-146; constants grid.hpp:140-143)
 BH_HD inline void pvfs(double r, double& rho, double& eps) {
-    double rfscal = 1.0 / pow(sqrt(smax(r, 1e-10) / 1.0), 3.0);   // libm pow on both sides
+    double rfscal = 1.0 / pow_3(sqrt(smax(r, 1e-10) / 1.0));
     rho = 1e-7 * rfscal;
     eps = 1e-5 * rfscal;
 }

@@ -1,17 +1,24 @@
-// bh_kernels.cu -- sm_100a kernels and the C ABI of the GRMHD block update.
+// bh_variant.cuh -- the kernels and their launch sequences, compiled once
+// per arithmetic variant: the including file defines BH_VARIANT (the
+// namespace) and is compiled with the variant's flags (bh_fp64.cu with
+// --fmad=false, the reference's separate roundings; bh_fp64fma.cu with
+// FMA contraction).  bh_abi.cu dispatches the C ABI to one of them.
 //
 // One thread per cell / face / edge; patches are the unit of parallel work
 // (blockIdx.y walks a patch list, blockIdx.x the items of one patch), so a
 // CTA never straddles two patches and all per-patch arrays are read with
-// unit stride along the reference's fastest index k.  Everything is FP64
-// and compiled with --fmad=false: this is the reference-faithful form.
+// unit stride along the reference's fastest index k.
+#pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
-#include <string.h>
-#include <mutex>
 #include "bhgpu.h"
 #include "bh_items.cuh"
 
+#ifndef BH_VARIANT
+#error "define BH_VARIANT before including bh_variant.cuh"
+#endif
+
+namespace BH_VARIANT {
 using namespace bh;
 
 namespace {
@@ -130,70 +137,29 @@ inline int launched() { return cudaGetLastError() == cudaSuccess ? BH_OK : BH_EC
 inline bool bad_pool(const bh_pool* p) { return !p || p->npatch <= 0 || !p->all; }
 inline dim3 grid2(int items, int npatch, int z = 1) { return dim3((items + TPB - 1) / TPB, npatch, z); }
 
-// ---- library-owned scratch for bh_ghosts_prims_static ---------------------
-// The con2prim outcome of every interior cell, BH_STATIC_MAX_PATCHES x 8000
-// bytes, held by every GPU that loads the library until the process exits.
-// Host code cannot use the array's name as a device address: each device's
-// address is looked up once (cudaGetSymbolAddress, on the first call made
-// with that device current) and handed to the kernels.
-__device__ __align__(256) uint8_t g_static_status[(size_t)BH_STATIC_MAX_PATCHES * NC];
-constexpr int kMaxDevices = 64;
-void* g_static_status_ptr[kMaxDevices] = {nullptr};
-std::mutex g_static_status_mu;
-
-int static_status_ptr(uint8_t** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BH_ECUDA;
-    std::lock_guard<std::mutex> lock(g_static_status_mu);
-    if (!g_static_status_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_static_status) != cudaSuccess || !p) return BH_ECUDA;
-        g_static_status_ptr[dev] = p;
-    }
-    *out = (uint8_t*)g_static_status_ptr[dev];
-    return BH_OK;
-}
-
 }  // namespace
 
-// ==========================================================================
-// C ABI
-// ==========================================================================
-extern "C" {
-
-int bh_abi_version(void) { return BHGPU_ABI_VERSION; }
-
-int bh_read_error(const bh_pool* pool, int32_t* out, void* stream) {
-    if (!pool || !pool->err || !out) return BH_EINVAL;
-    if (cudaMemcpyAsync(out, pool->err, sizeof(int32_t), cudaMemcpyDeviceToHost, S(stream)) != cudaSuccess) return BH_ECUDA;
-    return cudaStreamSynchronize(S(stream)) == cudaSuccess ? BH_OK : BH_ECUDA;
-}
-int bh_clear_error(const bh_pool* pool, void* stream) {
-    if (!pool || !pool->err) return BH_EINVAL;
-    return cudaMemsetAsync(pool->err, 0, sizeof(int32_t), S(stream)) == cudaSuccess ? BH_OK : BH_ECUDA;
-}
-
-int bh_metric_comp(const bh_params* P, const double* r, const double* th, int64_t n, double* out, void* stream) {
+int metric_comp(const bh_params* P, const double* r, const double* th, int64_t n, double* out, void* stream) {
     if (!P || n < 0) return BH_EINVAL;
     if (n == 0) return BH_OK;
     k_metric<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), r, th, n, out);
     return launched();
 }
-int bh_ptoc(const bh_params* P, const double* W, const double* r, const double* th, int64_t n, double* U, double* Wd,
+int ptoc(const bh_params* P, const double* W, const double* r, const double* th, int64_t n, double* U, double* Wd,
             void* stream) {
     if (!P || n < 0) return BH_EINVAL;
     if (n == 0) return BH_OK;
     k_ptoc<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), W, r, th, n, U, Wd);
     return launched();
 }
-int bh_ctop(const bh_params* P, const double* U, const double* r, const double* th, int64_t n, double* W, double* Wd,
+int ctop(const bh_params* P, const double* U, const double* r, const double* th, int64_t n, double* W, double* Wd,
             int32_t* status, int32_t* iters, int32_t* path, void* stream) {
     if (!P || n < 0 || (n > 0 && !status)) return BH_EINVAL;
     if (n == 0) return BH_OK;
     k_ctop<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), U, r, th, n, W, Wd, status, iters, path);
     return launched();
 }
-int bh_hlld(const bh_params* P, const double* WL, const double* WR, const double* UL, const double* UR,
+int hlld(const bh_params* P, const double* WL, const double* WR, const double* UL, const double* UR,
             const double* r, const double* th, int32_t dim, int64_t n, double* F, double* ctspeed, void* stream) {
     if (!P || n < 0 || dim < 0 || dim > 2) return BH_EINVAL;
     if (n == 0) return BH_OK;
@@ -202,99 +168,92 @@ int bh_hlld(const bh_params* P, const double* WL, const double* WR, const double
     return launched();
 }
 
-int bh_geometry(const bh_pool* pool, void* stream) {
+int geometry(const bh_pool* pool, void* stream) {
     if (bad_pool(pool)) return BH_EINVAL;
     k_geometry<<<grid2(NC, pool->npatch), TPB, 0, S(stream)>>>(pool_of(pool), pool->all);
     return launched();
 }
-int bh_reconfp(const bh_params* P, const bh_pool* pool, int32_t dim, int32_t limiter, double* L, double* R,
+int reconfp(const bh_params* P, const bh_pool* pool, int32_t dim, int32_t limiter, double* L, double* R,
                void* stream) {
     if (!P || bad_pool(pool) || dim < 0 || dim > 2) return BH_EINVAL;
     int64_t n = (int64_t)pool->npatch * NFACE;
     k_reconfp<<<grid2(NFACE, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), dim, limiter, n, L, R);
     return launched();
 }
-int bh_fluxcomp(const bh_params* P, const bh_pool* pool, void* stream) {
+int fluxcomp(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     k_flux<<<grid2(NFACE, pool->npatch, 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
     return launched();
 }
-int bh_emfcomp(const bh_pool* pool, void* stream) {
+int emfcomp(const bh_pool* pool, void* stream) {
     if (bad_pool(pool)) return BH_EINVAL;
     k_emf<<<grid2(N_EDGE, pool->npatch), TPB, 0, S(stream)>>>(pool_of(pool), pool->all);
     return launched();
 }
-int bh_bfupdate(const bh_pool* pool, const double* dt_dev, void* stream) {
+int bfupdate(const bh_pool* pool, const double* dt_dev, void* stream) {
     if (bad_pool(pool) || !dt_dev) return BH_EINVAL;
     k_bfupdate<<<grid2(N_BUP, pool->npatch), TPB, 0, S(stream)>>>(pool_of(pool), pool->all, dt_dev);
     return launched();
 }
-int bh_f2cb(const bh_params* P, const bh_pool* pool, void* stream) {
+int f2cb(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     k_f2cb<<<grid2(N_F2C, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
     return launched();
 }
-int bh_maxdivb(const bh_pool* pool, double* out, void* stream) {
+int maxdivb(const bh_pool* pool, double* out, void* stream) {
     if (bad_pool(pool) || !out) return BH_EINVAL;
     k_maxdivb<<<pool->npatch, 256, 0, S(stream)>>>(pool_of(pool), out);
     return launched();
 }
-int bh_div_source(const bh_params* P, const bh_pool* pool, double* div, double* src, void* stream) {
+int div_source(const bh_params* P, const bh_pool* pool, double* div, double* src, void* stream) {
     if (!P || bad_pool(pool) || !div || !src) return BH_EINVAL;
     k_div_source<<<grid2(N_INT, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, div,
                                                                                src);
     return launched();
 }
-int bh_ghosts(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
+int ghosts(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
     if (!P || bad_pool(pool) || n < 0 || (n > 0 && !patches)) return BH_EINVAL;
     if (n == 0) return BH_OK;
     k_ghost_fill<<<grid2(N_STRIP, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
     k_ghost_ctop<<<grid2(NC, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
     return launched();
 }
-int bh_prims(const bh_params* P, const bh_pool* pool, void* stream) {
+int prims(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     if (pool->nleaf == 0) return BH_OK;
     k_prims<<<grid2(NC, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves, 0);
     return launched();
 }
-int bh_ghosts_prims(const bh_params* P, const bh_pool* pool, void* stream) {
+// the fused ghost fill + reconstruction; status (may be null) is the
+// per-cell scratch of the interior-first variant
+int ghosts_prims_status(const bh_params* P, const bh_pool* pool, uint8_t* status, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     if (pool->nleaf == 0) return BH_OK;
-    k_ghost_fill<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves);
-    if (pool->status && pool->leafmask) {
-        k_prims_interior<<<grid2(N_INT, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves);
-        k_prims_ghost<<<grid2(N_GHOST, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves);
+    Pool pv = pool_of(pool);
+    pv.status = status;
+    k_ghost_fill<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
+    if (status && pool->leafmask) {
+        k_prims_interior<<<grid2(N_INT, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
+        k_prims_ghost<<<grid2(N_GHOST, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
     } else {
-        k_prims<<<grid2(NC, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves, 1);
+        k_prims<<<grid2(NC, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves, 1);
     }
     return launched();
 }
-int bh_ghosts_prims_static(const bh_params* P, const bh_pool* pool, void* stream) {
-    if (!P || bad_pool(pool) || !pool->leafmask) return BH_EINVAL;
-    if (pool->npatch > BH_STATIC_MAX_PATCHES) return BH_ERANGE;
-    if (pool->nleaf == 0) return BH_OK;
-    uint8_t* status = nullptr;
-    int rc = static_status_ptr(&status);
-    if (rc) return rc;
-    Pool pv = pool_of(pool);
-    pv.status = status;   // every entry read below is written by k_prims_interior first
-    k_ghost_fill<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
-    k_prims_interior<<<grid2(N_INT, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
-    k_prims_ghost<<<grid2(N_GHOST, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
-    return launched();
+int ghosts_prims(const bh_params* P, const bh_pool* pool, void* stream) {
+    return ghosts_prims_status(P, pool, pool ? pool->status : nullptr, stream);
 }
-int bh_update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, void* stream) {
+int update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, void* stream) {
     if (!P || bad_pool(pool) || !dt_dev || (stage != 0 && stage != 1)) return BH_EINVAL;
     k_update<<<grid2(N_F2C, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, dt_dev, stage);
     return launched();
 }
-int bh_floors(const bh_params* P, const bh_pool* pool, void* stream) {
+int floors(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     k_floors<<<grid2(N_INT, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
     return launched();
 }
-int bh_dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
+int dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
     if (!P || bad_pool(pool) || !dt_dev) return BH_EINVAL;
     k_dt_init<<<1, 1, 0, S(stream)>>>(dt_dev);
     if (pool->nleaf > 0)
@@ -302,32 +261,32 @@ int bh_dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_de
                                                                              cfl, dt_dev);
     return launched();
 }
-int bh_rkstg(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, const int32_t* waves,
+int rkstg(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, const int32_t* waves,
              const int32_t* wave_off, int32_t nwave, void* stream) {
     if (!P || bad_pool(pool) || !dt_dev || nwave < 0 || (nwave > 1 && (!waves || !wave_off))) return BH_EINVAL;
     int rc;
     if (nwave <= 1) {
-        rc = bh_ghosts_prims(P, pool, stream);
+        rc = ghosts_prims(P, pool, stream);
     } else {
         for (int w = 0; w < nwave; w++) {
-            rc = bh_ghosts(P, pool, waves + wave_off[w], wave_off[w + 1] - wave_off[w], stream);
+            rc = ghosts(P, pool, waves + wave_off[w], wave_off[w + 1] - wave_off[w], stream);
             if (rc) return rc;
         }
-        rc = bh_prims(P, pool, stream);
+        rc = prims(P, pool, stream);
     }
     if (rc) return rc;
-    if ((rc = bh_fluxcomp(P, pool, stream))) return rc;
-    if ((rc = bh_emfcomp(pool, stream))) return rc;
-    if ((rc = bh_bfupdate(pool, dt_dev, stream))) return rc;
-    return bh_update(P, pool, dt_dev, stage, stream);
+    if ((rc = fluxcomp(P, pool, stream))) return rc;
+    if ((rc = emfcomp(pool, stream))) return rc;
+    if ((rc = bfupdate(pool, dt_dev, stream))) return rc;
+    return update(P, pool, dt_dev, stage, stream);
 }
-int bh_step(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, const int32_t* waves,
+int step(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, const int32_t* waves,
             const int32_t* wave_off, int32_t nwave, void* stream) {
     int rc;
-    if ((rc = bh_dtcomp(P, pool, cfl, dt_dev, stream))) return rc;
-    if ((rc = bh_rkstg(P, pool, dt_dev, 0, waves, wave_off, nwave, stream))) return rc;
-    if ((rc = bh_rkstg(P, pool, dt_dev, 1, waves, wave_off, nwave, stream))) return rc;
-    return bh_floors(P, pool, stream);
+    if ((rc = dtcomp(P, pool, cfl, dt_dev, stream))) return rc;
+    if ((rc = rkstg(P, pool, dt_dev, 0, waves, wave_off, nwave, stream))) return rc;
+    if ((rc = rkstg(P, pool, dt_dev, 1, waves, wave_off, nwave, stream))) return rc;
+    return floors(P, pool, stream);
 }
 
-}  // extern "C"
+}  // namespace BH_VARIANT

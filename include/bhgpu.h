@@ -50,6 +50,11 @@ enum {
     BH_ERR_DOMAIN = 1   /* density <= 0 reached the EOS (reference throws) */
 };
 
+/* arithmetic variant (bh_params.precision) */
+enum {
+    BH_FP64 = 0,      /* FP64 with the reference's separate multiply/add roundings */
+    BH_FP64_FMA = 1   /* FP64 with fused multiply-add contraction                  */
+};
 /* reconstruction limiter (recon.hpp:36) */
 enum { BH_MINMOD = 0, BH_VANLEER = 1, BH_MC = 2 };
 /* neighbour kinds of the ghost fill (grid.cpp:528-534) */
@@ -63,6 +68,8 @@ typedef struct bh_params {
     double tol;          /* con2prim tolerance (1e-10)          cons.hpp:75         */
     double cM, ca, cQ;   /* metric carried by every cell: the default metric()
                             = (1, 0, 0) in the reference       cell.hpp:25, metric.hpp:30 */
+    int32_t precision;   /* BH_FP64 (reference-faithful) or BH_FP64_FMA              */
+    int32_t reserved;
 } bh_params;
 
 typedef struct bh_pool {

@@ -380,6 +380,7 @@ int ref_ptoc_batch(double M, double a, double Q, double gm, const double* W, con
 void ref_ctop_batch(double M, double a, double Q, double gm, const double* U, const double* r,
                     const double* th, int64_t n, double* W, double* Wd, int32_t* status) {
     metric m(M, a, Q); state s(gm); conserved cn(m, s);
+#pragma omp parallel for schedule(dynamic, 256)
     for (int64_t q = 0; q < n; q++) {
         cons c; cons_in(U, n, q, c);
         prim pv{};

@@ -1,0 +1,64 @@
+"""The step recorded into a CUDA graph and replayed equals the eagerly
+launched step bit for bit; the FMA-contracted FP64 variant meets the same
+first-step gate against the oracle as the reference-faithful one."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import GAMMA, box_case, field_linf, gpu_tree, rel_linf, same_nan, ulp_sensitivity
+
+pytestmark = pytest.mark.gpu
+
+
+def test_graph_replay_equals_eager():
+    import bhgpu
+    q, orc, hp = box_case(2, seed=6, periodic=True, lim=0)
+    eager = gpu_tree(q, hp, 0.0, 0.0, 0)
+    graphed = gpu_tree(q, hp, 0.0, 0.0, 0)
+    rk = bhgpu.RK2Integrator(0.4)
+    U0 = graphed.U.clone(); W0 = graphed.W.clone(); B0 = graphed.Bf.clone()
+
+    def reset():
+        graphed.U.copy_(U0); graphed.W.copy_(W0); graphed.Bf.copy_(B0)
+
+    g = bhgpu.StepGraph(graphed, rk, before=reset)
+    for _ in range(2):                      # replaying restarts from the same state
+        g.replay()
+    torch.cuda.synchronize()
+    rk.step(eager)
+    for name in ("U", "W", "Bf", "dU"):
+        assert torch.equal(getattr(eager, name).nan_to_num(7.0), getattr(graphed, name).nan_to_num(7.0)), name
+    assert float(graphed.dt.item()) == float(eager.dt.item())
+    # two steps through a graph without the reset
+    g2 = bhgpu.StepGraph(graphed, rk, warmup=0)
+    reset()
+    e2 = gpu_tree(q, hp, 0.0, 0.0, 0)
+    for _ in range(2):
+        g2.replay()
+        rk.step(e2, check_domain=False)
+    torch.cuda.synchronize()
+    assert torch.equal(e2.U.nan_to_num(7.0), graphed.U.nan_to_num(7.0))
+
+
+@pytest.mark.parametrize("case", [dict(periodic=True, lim=0, M=0.0, a=0.0, lo=10.0, hi=12.0),
+                                  dict(periodic=True, lim=2, M=1.0, a=0.9375, lo=-6.0, hi=6.0)])
+def test_fma_variant_first_step(case):
+    import bhgpu
+    import oracle
+    q, orc, hp = box_case(2, seed=4, **case)
+    sens = ulp_sensitivity(orc, hp, steps=1)
+    fma = oracle.Oracle(case["M"], case["a"], 0.0, GAMMA, limiter=case["lim"], fma=True)
+    hf = hp.copy()
+    fma.step(hf, 0.4)
+    tree = bhgpu.AmrTree(q.dom_l, q.dom_h, q.nqlt, M=case["M"], a=case["a"], Q=0.0, gm=GAMMA,
+                         periodic=q.periodic, limiter=case["lim"], quilt=q, init_floor=False, precision="fp64-fma")
+    tree.load(U=hp.U, W=hp.W, Bf=hp.Bf, dU=hp.dU)
+    dtg = bhgpu.RK2Integrator(0.4).step(tree)
+    dtc = orc.step(hp, 0.4)
+    assert abs(dtg - dtc) <= 1e-12 * dtc
+    U = tree.U.cpu().numpy()
+    assert same_nan(U, hp.U)
+    assert max(field_linf(U, hp.U).values()) <= 1e-12
+    for v in range(8):
+        own = max(sens[v], rel_linf(hf.U[:, v], hp.U[:, v]))
+        assert rel_linf(U[:, v], hp.U[:, v]) <= max(1e-12, 8 * own), v
