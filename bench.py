@@ -6,9 +6,15 @@
 Workload: the uniform magnetised box -- rho = 1, p = 0.1 (1 + 0.01 N(0,1)),
 v = 0, B = (0.5, 0.3, 0) + curl of a random vector potential (|k| <= 4,
 RMS 1e-2), flat tree metric (M = a = Q = 0), Gamma = 4/3, periodic,
-PLM-minmod + HLLD + constrained transport, RK2 at CFL 0.4, all FP64 in the
-reference-faithful form -- on a 128^3 grid of 8^3 patches of 16^3 cells
-(``--grid 64``: the 64^3 box of 4^3 patches).  Synthetic seeded data.
+PLM-minmod + HLLD + constrained transport, RK2 at CFL 0.4 -- on a 128^3
+grid of 8^3 patches of 16^3 cells (``--grid 64``: the 64^3 box of 4^3
+patches).  Synthetic seeded data.
+
+Arithmetic: the headline runs the FP64 kernels with fused multiply-add
+(``--precision``, default fp64-fma); the reference-faithful FP64 form and
+the mixed FP32/FP64 variant are timed beside it on the same workload, with
+the mixed variant's accuracy against FP64 (the magnetised box after one
+step, the unmagnetised box after five).
 
 A step is one full rk2integrator::step (dtcomp, two RK stages with ghost
 fill, con2prim, fluxes, CT and update, floors) over the whole grid,
@@ -57,8 +63,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--con2prim-batch", type=int, default=1, help="also measure the 2^24-cell con2prim batch")
-    ap.add_argument("--precision", default="fp64-fma", choices=["fp64", "fp64-fma"],
-                    help="arithmetic variant of the headline value; the other FP64 form is timed beside it")
+    ap.add_argument("--precision", default="fp64-fma", choices=["fp64", "fp64-fma", "mixed"],
+                    help="arithmetic variant of the headline value; the other variants are timed beside it")
     return ap.parse_args()
 
 
@@ -117,14 +123,14 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-def make_tree(nq, seed, precision="fp64"):
+def make_tree(nq, seed, precision="fp64", **box):
     import bhgpu
     from bhgpu import configs
     from bhgpu.mesh import Quilt
     q = Quilt([LO] * 3, [HI] * 3, nq, periodic=True)
     tree = bhgpu.AmrTree(q.dom_l, q.dom_h, nq, M=0.0, a=0.0, Q=0.0, gm=GAMMA, periodic=True,
                          limiter="minmod", quilt=q, init_floor=False, precision=precision)
-    W, Bf = configs.magnetised_box(q, seed=seed, gamma=GAMMA)
+    W, Bf = configs.magnetised_box(q, seed=seed, gamma=GAMMA, **box)
     tree.load(W=W, Bf=Bf)
     tree.prim_to_cons()
     return tree
@@ -198,7 +204,7 @@ def cpu_reference_sample(threads):
 
 
 # ---------------------------------------------------------------------------
-# con2prim stress batch (configs[3]): 2^24 independent Kerr cells (a = 0.9375)
+# con2prim stress batch: 2^24 independent Kerr cells (a = 0.9375)
 C2P_ALG_BYTES = 8 * 8 + 2 * 8 + 5 * 8 + 4   # U + (r, theta) in; rho, eps, v out; iterations
 
 
@@ -221,7 +227,7 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
     b.record(); torch.cuda.synchronize()
     ms = a.elapsed_time(b) / reps
     st, it, pa = st.cpu().numpy(), it.cpu().numpy(), pa.cpu().numpy()
-    out = {"workload": f"configs[3]: {n_cells} independent Kerr-Schild cells (a=0.9375, Gamma=4/3), "
+    out = {"workload": f"con2prim stress batch: {n_cells} independent Kerr-Schild cells (a=0.9375, Gamma=4/3), "
                        "log-uniform rho, W in [1,20], log-uniform sigma, isotropic v and B, r in [1.5,50]",
            "cells": n_cells, "ms": ms, "cells_per_s": n_cells / (ms / 1e3),
            "recovered_frac": float(np.mean(st == 1)), "failed_frac": float(np.mean(st == 0)),
@@ -246,6 +252,44 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
     except Exception as e:      # the CPU figure is informational
         out["cpu_reference"] = {"error": str(e)}
     return out
+
+
+# ---------------------------------------------------------------------------
+FIELDS = {"D": [0], "S": [1, 2, 3], "tau": [4], "B": [5, 6, 7]}
+
+
+def field_l1(a, b):
+    """Relative L1 difference per conserved field of two [np][8][NC] states
+    (entries finite in both) and the fraction of entries whose NaN masks
+    disagree."""
+    import torch
+    out = {}
+    for name, comps in FIELDS.items():
+        x, y = a[:, comps], b[:, comps]
+        m = torch.isfinite(x) & torch.isfinite(y)
+        den = y[m].abs().mean().item() if m.any() else 0.0
+        num = (x[m] - y[m]).abs().mean().item() if m.any() else 0.0
+        out[name] = num / den if den > 0 else num
+    out["nan_mask"] = (torch.isfinite(a) != torch.isfinite(b)).double().mean().item()
+    return out
+
+
+def variant_accuracy(tree, prec, steps, U0, W0, B0):
+    """``prec`` against the reference-faithful FP64 variant after ``steps``
+    steps from the same state of ``tree``."""
+    import bhgpu
+    rk = bhgpu.RK2Integrator(CFL)
+    res = {}
+    keep = tree.precision
+    for p in ("fp64", prec):
+        tree.precision = p
+        tree.U.copy_(U0); tree.W.copy_(W0); tree.Bf.copy_(B0)
+        for _ in range(steps):
+            rk.step(tree, check_domain=False)
+        res[p] = tree.U.clone()
+    tree.precision = keep
+    tree.clear_error()
+    return field_l1(res[prec], res["fp64"])
 
 
 # ---------------------------------------------------------------------------
@@ -379,22 +423,40 @@ def run_ours(args):
     ms_max = float(t.item())
     err = tree.read_error()
 
-    # ---- the other FP64 form, same workload, for comparison --------------------
-    other = "fp64" if args.precision == "fp64-fma" else "fp64-fma"
-    tree.precision = other
-    P = tree.params()
-    for _ in range(2):
-        step()
-    torch.cuda.synchronize()
-    a0 = torch.cuda.Event(enable_timing=True); b0 = torch.cuda.Event(enable_timing=True)
-    k_other = max(10, args.steps // 4)
-    a0.record()
-    for _ in range(k_other):
-        step()
-    b0.record(); torch.cuda.synchronize()
-    other_ms = a0.elapsed_time(b0) / k_other
+    # ---- the other arithmetic variants, same workload, for comparison --------
+    variants = {}
+    for prec in [p for p in ("fp64", "fp64-fma", "mixed") if p != args.precision]:
+        tree.precision = prec
+        P = tree.params()
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True); b0 = torch.cuda.Event(enable_timing=True)
+        k_other = max(10, args.steps // 4)
+        a0.record()
+        for _ in range(k_other):
+            step()
+        b0.record(); torch.cuda.synchronize()
+        vms = a0.elapsed_time(b0) / k_other
+        variants[prec] = {"ms_per_step": vms, "value": world * zones / (vms / 1e3),
+                          "dtype": "f32+f64" if prec == "mixed" else "f64"}
     tree.precision = args.precision
     P = tree.params()
+    fp64_ms = variants["fp64"]["ms_per_step"] if "fp64" in variants else ms_max / args.steps
+    for prec, v in variants.items():
+        v["speedup_vs_plain_fp64"] = fp64_ms / v["ms_per_step"]
+    # accuracy of the non-faithful variants against the faithful FP64 one
+    accuracy = {}
+    for prec in ("fp64-fma", "mixed"):
+        acc = {"magnetised_box_1_step": variant_accuracy(tree, prec, 1, U0, W0, B0)}
+        if prec == "mixed":
+            hyd = make_tree(4, seed=1, precision="fp64", B0=(0.0, 0.0, 0.0), amp=0.0)
+            acc["unmagnetised_box_64cube_5_steps"] = variant_accuracy(
+                hyd, prec, 5, hyd.U.clone(), hyd.W.clone(), hyd.Bf.clone())
+            del hyd
+        accuracy[prec] = acc
+        if prec in variants:
+            variants[prec]["accuracy_vs_fp64"] = acc
 
     # ---- end to end through the public API with host buffers --------------
     pin = lambda x: x.cpu().pin_memory()
@@ -434,12 +496,14 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded)",
             "precision": args.precision,
-            "other_precision": {"precision": other, "ms_per_step": other_ms,
-                                "value": world * zones / (other_ms / 1e3)},
+            "speedup_vs_plain_fp64": fp64_ms / (ms_max / args.steps),
+            "accuracy_vs_fp64": accuracy.get(args.precision, "identical roundings (the reference-faithful form)"),
+            "variants": variants,
             "config": {"workload": f"magnetised box {args.grid}^3: flat metric, periodic, PLM-minmod + HLLD + CT, "
-                                   f"RK2 CFL 0.4, reference-faithful FP64", "grid": f"{args.grid}^3",
+                                   f"RK2 CFL 0.4, {args.precision} arithmetic", "grid": f"{args.grid}^3",
                        "patches": tree.npatch, "patch": "16^3 + 2 ghosts", "parallelism": f"replicas x{world}",
                        "l2": "working set > L2 (inputs and outputs larger than 126 MB)",
                        "restart": "each step restarts from the seeded state (D2D copy inside the timed region)"},

@@ -19,9 +19,11 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
           "-I" + os.path.join(REPO, "include"), "-I" + CSRC]
-# --fmad=false keeps the reference's separate multiply/add roundings; only the
-# FMA variant contracts
-FMAD = {"bh_fp64fma.cu": "--fmad=true"}
+# --fmad=false keeps the reference's separate multiply/add roundings; the FMA
+# and mixed variants contract, and the mixed variant's FP32 arithmetic uses
+# flush-to-zero and the fast division/square root
+FMAD = {"bh_fp64fma.cu": ["--fmad=true"],
+        "bh_mixed.cu": ["--fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]}
 
 
 def sources():
@@ -40,7 +42,7 @@ def build(verbose: bool = False) -> str:
     os.makedirs(bdir, exist_ok=True)
     for src in srcs:
         obj = os.path.join(bdir, os.path.basename(src).replace(".cu", ".o"))
-        cmd = [NVCC] + ARCH + COMMON + [FMAD.get(os.path.basename(src), "--fmad=false"), "-c", src, "-o", obj]
+        cmd = [NVCC] + ARCH + COMMON + FMAD.get(os.path.basename(src), ["--fmad=false"]) + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         r = subprocess.run(cmd, capture_output=True, text=True)

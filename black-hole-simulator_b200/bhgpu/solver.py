@@ -18,7 +18,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import BH_ERR_DOMAIN, BH_FP64, BH_FP64_FMA, BH_MC, BH_MINMOD, BH_VANLEER, BhParams, BhPool, check, lib
+from ._lib import BH_ERR_DOMAIN, BH_FP64, BH_FP64_FMA, BH_MC, BH_MIXED, BH_MINMOD, BH_VANLEER, BhParams, BhPool, check, lib
 from .mesh import NC, NE, NF, Quilt
 
 __all__ = ["Metric", "State", "Conserved", "hlld", "AmrTree", "RK2Integrator", "StepGraph", "DomainError",
@@ -27,7 +27,7 @@ __all__ = ["Metric", "State", "Conserved", "hlld", "AmrTree", "RK2Integrator", "
 _LIMITERS = {"minmod": BH_MINMOD, "vanleer": BH_VANLEER, "mc": BH_MC, "mclim": BH_MC}
 # arithmetic variants: "fp64" keeps the reference's separate roundings (the
 # parity form); "fp64-fma" contracts multiply-add pairs
-PRECISIONS = {"fp64": BH_FP64, "fp64-fma": BH_FP64_FMA}
+PRECISIONS = {"fp64": BH_FP64, "fp64-fma": BH_FP64_FMA, "mixed": BH_MIXED}
 
 
 class DomainError(ValueError):
@@ -157,7 +157,8 @@ class AmrTree:
     slope limiter of the flux reconstruction (the reference's fluxcomp
     always uses van Leer, recon.hpp:41); ``precision`` selects the
     arithmetic variant ("fp64" reproduces the reference's roundings,
-    "fp64-fma" contracts multiply-add pairs).
+    "fp64-fma" contracts multiply-add pairs, "mixed" computes the face
+    fluxes and the geometric source in FP32 and everything else in FP64).
     """
 
     def __init__(self, dom_l, dom_h, nqlt: int, M: float = 1.0, a: float = 0.0, Q: float = 0.0,

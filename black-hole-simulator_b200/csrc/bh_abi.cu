@@ -41,6 +41,7 @@ int static_status_ptr(uint8_t** out) {
     switch ((P) ? (P)->precision : -1) {                     \
     case BH_FP64: return vfp64::call;                        \
     case BH_FP64_FMA: return vfma::call;                     \
+    case BH_MIXED: return vmixed::call;                      \
     default: return BH_EINVAL;                               \
     }
 

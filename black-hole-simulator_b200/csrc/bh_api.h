@@ -1,5 +1,6 @@
 // bh_api.h -- the launch sequences each arithmetic variant provides
-// (defined in bh_variant.cuh, instantiated by bh_fp64.cu and bh_fp64fma.cu)
+// (defined in bh_variant.cuh, instantiated by bh_fp64.cu, bh_fp64fma.cu and
+// bh_mixed.cu)
 #pragma once
 #include <stdint.h>
 #include "bhgpu.h"
@@ -34,3 +35,4 @@
 
 BH_VARIANT_API(vfp64)
 BH_VARIANT_API(vfma)
+BH_VARIANT_API(vmixed)

@@ -1,7 +1,7 @@
 // bh_items.cuh -- the per-item work of every kernel (one cell, face, edge
 // or ghost cell), written once as __host__ __device__ functions.
 //
-// The __global__ kernels in bh_kernels.cu map their thread index to an
+// The __global__ kernels in bh_variant.cuh map their thread index to an
 // item and call these; the CPU check of the kernel logic
 // (tests/hostcheck) compiles the same functions for the host and runs
 // them in loops.  Items of one launch never depend on each other.
@@ -160,40 +160,43 @@ BH_HD inline void face_ijk(int dim, int f, int& i, int& j, int& k) {
 }
 
 // reconfp (reconstruction.cpp:40-97) for the face between cells (i,j,k)
-// and (i,j,k)+e_dim of patch p
-BH_HD inline void reconfp(const KP& kp, const Pool& P, int p, int i, int j, int k, int dim, int lim, Prim& L,
-                          Prim& R) {
+// and (i,j,k)+e_dim of patch p, computed in RT (the stored primitives and
+// the cell metric are FP64 and rounded to RT)
+template <typename RT>
+BH_HD inline void reconfp(const KP& kp, const Pool& P, int p, int i, int j, int k, int dim, int lim, PrimT<RT>& L,
+                          PrimT<RT>& R) {
     int di = dim == 0, dj = dim == 1, dk = dim == 2;
     int lm = lindx(i - di, j - dj, k - dk), lc = lindx(i, j, k);
     int lp = lindx(i + di, j + dj, k + dk), lpp = lindx(i + 2 * di, j + 2 * dj, k + 2 * dk);
     const double* Wr = Wv(P, p, 0);
-    recon_scal(log(Wr[lm]), log(Wr[lc]), log(Wr[lp]), log(Wr[lpp]), lim, L.rho, R.rho);
+    recon_scal(log(RT(Wr[lm])), log(RT(Wr[lc])), log(RT(Wr[lp])), log(RT(Wr[lpp])), lim, L.rho, R.rho);
     L.rho = exp(L.rho); R.rho = exp(R.rho);
     const double* We = Wv(P, p, 1);
-    recon_scal(log(We[lm]), log(We[lc]), log(We[lp]), log(We[lpp]), lim, L.eps, R.eps);
+    recon_scal(log(RT(We[lm])), log(RT(We[lc])), log(RT(We[lp])), log(RT(We[lpp])), lim, L.eps, R.eps);
     L.eps = exp(L.eps); R.eps = exp(R.eps);
     for (int d = 0; d < 3; d++) {
         const double* x = Wv(P, p, 2 + d);
-        recon_scal(x[lm], x[lc], x[lp], x[lpp], lim, L.v[d], R.v[d]);
+        recon_scal(RT(x[lm]), RT(x[lc]), RT(x[lp]), RT(x[lpp]), lim, L.v[d], R.v[d]);
     }
     Met mL, mR;
     met_comp(kp.cell, rr(P, p, lc), tt(P, p, lc), mL);
     met_comp(kp.cell, rr(P, p, lp), tt(P, p, lp), mR);
-    causalv(L.v, mL);
-    causalv(R.v, mR);
+    causalv(L.v, met_cast<RT>(mL));
+    causalv(R.v, met_cast<RT>(mR));
     for (int d = 0; d < 3; d++) {
         const double* x = Wv(P, p, 5 + d);
-        if (d == dim) { L.B[d] = x[lc]; R.B[d] = x[lp]; }
-        else recon_scal(x[lm], x[lc], x[lp], x[lpp], lim, L.B[d], R.B[d]);
+        if (d == dim) { L.B[d] = RT(x[lc]); R.B[d] = RT(x[lp]); }
+        else recon_scal(RT(x[lm]), RT(x[lc]), RT(x[lp]), RT(x[lpp]), lim, L.B[d], R.B[d]);
     }
 }
 
+template <typename RT>
 BH_HD inline void reconfp_item(const KP& kp, const Pool& P, int p, int dim, int f, int lim, int64_t n, double* Lo,
                                double* Ro) {
     int i, j, k;
     face_ijk(dim, f, i, j, k);
-    Prim L, R;
-    reconfp(kp, P, p, i, j, k, dim, lim, L, R);
+    PrimT<RT> L, R;
+    reconfp<RT>(kp, P, p, i, j, k, dim, lim, L, R);
     int64_t q = (int64_t)p * NFACE + f;
     Lo[q] = L.rho; Lo[n + q] = L.eps; Ro[q] = R.rho; Ro[n + q] = R.eps;
     for (int d = 0; d < 3; d++) {
@@ -202,28 +205,32 @@ BH_HD inline void reconfp_item(const KP& kp, const Pool& P, int p, int dim, int 
     }
 }
 
-// one face of patch::fluxcomp (grid.cpp:255-329)
+// one face of patch::fluxcomp (grid.cpp:255-329): reconstruction, face
+// ptoc and HLLD in RT; face metric evaluated in FP64; flux stored in FP64
+template <typename RT>
 BH_HD inline void flux_item(const KP& kp, const Pool& P, int p, int dim, int f) {
     int i, j, k;
     face_ijk(dim, f, i, j, k);
-    Prim L, R;
-    reconfp(kp, P, p, i, j, k, dim, kp.limiter, L, R);
+    PrimT<RT> L, R;
+    reconfp<RT>(kp, P, p, i, j, k, dim, kp.limiter, L, R);
     double bn;
     int fi;
     if (dim == 0) { bn = Bfv(P, p, 0)[xfc(i + 1, j, k)]; fi = xfc(i, j, k); }
     else if (dim == 1) { bn = Bfv(P, p, 1)[yfc(i, j + 1, k)]; fi = yfc(i, j, k); }
     else { bn = Bfv(P, p, 2)[zfc(i, j, k + 1)]; fi = zfc(i, j, k); }
-    L.B[dim] = bn; R.B[dim] = bn;
+    L.B[dim] = RT(bn); R.B[dim] = RT(bn);
     int lL = lindx(i, j, k), lR = lindx(i + (dim == 0), j + (dim == 1), k + (dim == 2));
     double rf = (rr(P, p, lL) + rr(P, p, lR)) / 2;
     double thf = (tt(P, p, lL) + tt(P, p, lR)) / 2;
-    Met mc;
-    met_comp(kp.tree, rf, thf, mc);
-    Cons UL, UR;
-    bool ok = ptoc(kp.gamma, mc, L, UL);
-    ok &= ptoc(kp.gamma, mc, R, UR);
-    double F[8], cts;
-    ok &= hlld(kp.gamma, mc, L, R, UL, UR, 0 /* every call site passes dim 0 */, F, cts);
+    Met md;
+    met_comp(kp.tree, rf, thf, md);
+    MetT<RT> mc = met_cast<RT>(md);
+    ConsT<RT> UL, UR;
+    RT g = RT(kp.gamma);
+    bool ok = ptoc(g, mc, L, UL);
+    ok &= ptoc(g, mc, R, UR);
+    RT F[8], cts;
+    ok &= hlld(g, mc, L, R, UL, UR, 0 /* every call site passes dim 0 */, F, cts);
     if (!ok) flag(P.err, BH_ERR_DOMAIN);
     for (int v = 0; v < 8; v++) Fv(P, p, dim, v)[fi] = F[v];
 }
@@ -299,12 +306,17 @@ BH_HD inline void div_flux(const Pool& P, int p, int i, int j, int k, double sg,
     out[5] = out[6] = out[7] = 0.0;
 }
 
-// geometric source (:41-153) with the full cell metric; false where the EOS throws
-BH_HD inline bool source(const KP& kp, const MetFull& mc, const Prim& W, double out[8]) {
-    double gam[3][3];
+// geometric source (:41-153) with the full cell metric (evaluated in FP64)
+// and arithmetic in RT; false where the EOS throws
+template <typename RT>
+BH_HD inline bool source(const KP& kp, const MetFull& mc, const Prim& Wd, RT out[8]) {
+    PrimT<RT> W;
+    W.rho = RT(Wd.rho); W.eps = RT(Wd.eps);
+    for (int d = 0; d < 3; d++) { W.v[d] = RT(Wd.v[d]); W.B[d] = RT(Wd.B[d]); }
+    RT gam[3][3];
     for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) gam[i][j] = mc.g[i + 1][j + 1];
-    double v2 = 0.0, vlow[3] = {0, 0, 0}, Blow[3] = {0, 0, 0};
+        for (int j = 0; j < 3; j++) gam[i][j] = RT(mc.g[i + 1][j + 1]);
+    RT v2 = RT(0.0), vlow[3] = {RT(0), RT(0), RT(0)}, Blow[3] = {RT(0), RT(0), RT(0)};
     for (int m = 0; m < 3; m++) {
         for (int n = 0; n < 3; n++) {
             vlow[m] += gam[m][n] * W.v[n];
@@ -312,48 +324,52 @@ BH_HD inline bool source(const KP& kp, const MetFull& mc, const Prim& W, double 
         }
         v2 += vlow[m] * W.v[m];
     }
-    v2 = smin(v2, 1 - 1e-10);
-    double ltz2 = 1.0 / (1.0 - v2);
-    double ltz = sqrt(ltz2);
-    double Bv = 0.0, Bsq = 0.0;
+    v2 = smin(v2, RT(1) - RT(1e-10));
+    RT ltz2 = RT(1.0) / (RT(1.0) - v2);
+    RT ltz = sqrt(ltz2);
+    RT Bv = RT(0.0), Bsq = RT(0.0);
     for (int m = 0; m < 3; m++) { Bv += Blow[m] * W.v[m]; Bsq += Blow[m] * W.B[m]; }
-    double b2 = Bv * Bv + Bsq / ltz2;
+    RT b2 = Bv * Bv + Bsq / ltz2;
     bool ok = eos_ok(W.rho);
-    double px = press(kp.gamma, W.rho, W.eps);
-    double h = enth(kp.gamma, W.eps);
-    double u4[4], b4[4];
-    u4[0] = ltz / mc.alpha;
-    for (int m = 0; m < 3; m++) u4[m + 1] = ltz * (W.v[m] - mc.beta[m] / mc.alpha);
-    b4[0] = ltz * Bv / mc.alpha;
-    for (int m = 0; m < 3; m++) b4[m + 1] = (W.B[m] + mc.alpha * b4[0] * u4[m + 1]) / ltz;
-    double T44[4][4];
-    double rhohb2 = W.rho * h + b2;
+    RT g = RT(kp.gamma);
+    RT px = press(g, W.rho, W.eps);
+    RT h = enth(g, W.eps);
+    RT alpha = RT(mc.alpha);
+    RT u4[4], b4[4];
+    u4[0] = ltz / alpha;
+    for (int m = 0; m < 3; m++) u4[m + 1] = ltz * (W.v[m] - RT(mc.beta[m]) / alpha);
+    b4[0] = ltz * Bv / alpha;
+    for (int m = 0; m < 3; m++) b4[m + 1] = (W.B[m] + alpha * b4[0] * u4[m + 1]) / ltz;
+    RT T44[4][4];
+    RT rhohb2 = W.rho * h + b2;
     for (int m = 0; m < 4; m++)
-        for (int n = 0; n < 4; n++) T44[m][n] = rhohb2 * u4[m] * u4[n] + px * mc.gi[m][n] - b4[m] * b4[n];
-    double src[4];
+        for (int n = 0; n < 4; n++) T44[m][n] = rhohb2 * u4[m] * u4[n] + px * RT(mc.gi[m][n]) - b4[m] * b4[n];
+    RT src[4];
     for (int m = 0; m < 4; m++) {
-        double acc = 0.0;
+        RT acc = RT(0.0);
         for (int n = 0; n < 4; n++)
             for (int q = 0; q < 4; q++) {
-                double G_ = 0.0;   // lowered Christoffel g[m][s] Gamma[s][n][q], summed over s
-                for (int s = 0; s < 4; s++) G_ += mc.g[m][s] * mc.G[s][n][q];
+                RT G_ = RT(0.0);   // lowered Christoffel g[m][s] Gamma[s][n][q], summed over s
+                for (int s = 0; s < 4; s++) G_ += RT(mc.g[m][s]) * RT(mc.G[s][n][q]);
                 acc += T44[n][q] * G_;
             }
-        src[m] = acc * mc.sqrtdetg;
+        src[m] = acc * RT(mc.sqrtdetg);
     }
-    out[0] = 0.0;
+    out[0] = RT(0.0);
     out[4] = src[0];
     out[1] = src[1]; out[2] = src[2]; out[3] = src[3];
-    out[5] = out[6] = out[7] = 0.0;
+    out[5] = out[6] = out[7] = RT(0.0);
     return ok;
 }
 
+template <typename RT>
 BH_HD inline void div_source_item(const KP& kp, const Pool& P, int p, int c, double* dv, double* sv) {
     int i = c / 256, j = (c / 16) % 16, k = c % 16;
     int l = lindx(i, j, k);
     MetFull mf;
     met_full(kp.cell, rr(P, p, l), tt(P, p, l), mf);
-    double d8[8], s8[8];
+    double d8[8];
+    RT s8[8];
     div_flux(P, p, i, j, k, mf.sqrtdetg, d8);
     Prim w;
     load_prim(P, p, l, w);
@@ -367,6 +383,7 @@ BH_HD inline void div_source_item(const KP& kp, const Pool& P, int p, int c, dou
 // f2cB + the conserved update of rkstg (integrator.cpp:325-347), fused:
 // cells in [-1,18)^3 take the face-averaged B; interior cells then add
 // dt * (div_flux + source) and refresh U.B = sqrt(-g) W.B
+template <typename RT>
 BH_HD inline void update_item(const KP& kp, const Pool& P, int p, int e, double dt, int stage) {
     int i = e / 361 - 1, j = (e / 19) % 19 - 1, k = e % 19 - 1;
     double B[3], sg;
@@ -379,13 +396,14 @@ BH_HD inline void update_item(const KP& kp, const Pool& P, int p, int e, double 
     }
     MetFull mf;
     met_full(kp.cell, rr(P, p, l), tt(P, p, l), mf);
-    double d8[8], s8[8];
+    double d8[8];
+    RT s8[8];
     div_flux(P, p, i, j, k, mf.sqrtdetg, d8);
     Prim w;
     load_prim(P, p, l, w);
     if (!source(kp, mf, w, s8)) flag(P.err, BH_ERR_DOMAIN);
     for (int v = 0; v < 5; v++) {
-        double dU = d8[v] + s8[v];
+        double dU = d8[v] + double(s8[v]);
         double u = Uv(P, p, v)[l];
         if (stage == 0) {
             dUv(P, p, v)[l] = u;

@@ -44,8 +44,10 @@ constexpr int NE = CPN * (CPN + 1) * (CPN + 1);     // 8820 edges / direction
 constexpr int NFACE = (BLK + 1) * BLK * BLK;        // 4352 flux faces / direction
 
 // ---- std::min / std::max semantics (NaN included) ----------------------
-BH_HD inline double smin(double a, double b) { return (b < a) ? b : a; }
-BH_HD inline double smax(double a, double b) { return (a < b) ? b : a; }
+template <typename T>
+BH_HD inline T smin(T a, T b) { return (b < a) ? b : a; }
+template <typename T>
+BH_HD inline T smax(T a, T b) { return (a < b) ? b : a; }
 
 BH_HD inline void flag(int32_t* err, int bit) {
 #ifdef __CUDA_ARCH__
@@ -72,10 +74,22 @@ struct MP { double M, a, Q; };
 // Spatial 3+1 part of metric::comp: gam = g[i+1][j+1], gam_inv =
 // g_inv[i+1][j+1] (dense, with the reference's structural zeros), lapse,
 // shift, sqrt(-g), sqrt(gamma).
-struct Met {
-    double gam[3][3], gam_inv[3][3];
-    double alpha, beta[3], sqrtdetg, sqrtdetgam;
+template <typename RT>
+struct MetT {
+    RT gam[3][3], gam_inv[3][3];
+    RT alpha, beta[3], sqrtdetg, sqrtdetgam;
 };
+using Met = MetT<double>;
+// the spatial metric at reduced precision (values computed in FP64)
+template <typename RT>
+BH_HD inline MetT<RT> met_cast(const Met& m) {
+    MetT<RT> o;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) { o.gam[i][j] = RT(m.gam[i][j]); o.gam_inv[i][j] = RT(m.gam_inv[i][j]); }
+    o.alpha = RT(m.alpha); o.sqrtdetg = RT(m.sqrtdetg); o.sqrtdetgam = RT(m.sqrtdetgam);
+    for (int i = 0; i < 3; i++) o.beta[i] = RT(m.beta[i]);
+    return o;
+}
 
 struct Trig { double c, s; };
 BH_HD inline Trig trig(double th) {
@@ -188,65 +202,74 @@ BH_HD inline void met_full(const MP& m, double r, double th, MetFull& o) {
 // ======================================================================
 // EOS (physics/thermo.cpp:10-35)
 // ======================================================================
-BH_HD inline bool eos_ok(double rho) { return !(rho <= 0.0); }
-BH_HD inline double press(double g, double rho, double eps) { return (g - 1.0) * rho * eps; }
-BH_HD inline double enth(double g, double eps) { return 1.0 + g * eps; }
-BH_HD inline double cs2f(double g, double rho, double eps) {
-    double p = press(g, rho, eps), h = enth(g, eps);
+template <typename RT>
+BH_HD inline bool eos_ok(RT rho) { return !(rho <= RT(0.0)); }
+template <typename RT>
+BH_HD inline RT press(RT g, RT rho, RT eps) { return (g - RT(1.0)) * rho * eps; }
+template <typename RT>
+BH_HD inline RT enth(RT g, RT eps) { return RT(1.0) + g * eps; }
+template <typename RT>
+BH_HD inline RT cs2f(RT g, RT rho, RT eps) {
+    RT p = press(g, rho, eps), h = enth(g, eps);
     return (g * p) / (rho * h);
 }
 
 // primitive / conserved vectors in the reference member order
-struct Prim { double rho, eps, v[3], B[3]; };
-struct Cons { double D, S[3], tau, B[3]; };
+template <typename RT> struct PrimT { RT rho, eps, v[3], B[3]; };
+template <typename RT> struct ConsT { RT D, S[3], tau, B[3]; };
 
 // ======================================================================
 // prim -> cons, conserved::ptoc (physics/conserved.cpp:17-73)
 // returns false where the reference throws (rho <= 0)
 // ======================================================================
-struct PtocOut { double lor, p, h, b2; };
-BH_HD inline bool ptoc(double gamma, const Met& mc, const Prim& pv, Cons& CV, PtocOut* po = nullptr) {
-    double sg = mc.sqrtdetgam;
-    double v2 = 0.0, vlow[3] = {0.0, 0.0, 0.0};
+template <typename RT> struct PtocOutT { RT lor, p, h, b2; };
+template <typename RT>
+BH_HD inline bool ptoc(RT gamma, const MetT<RT>& mc, const PrimT<RT>& pv, ConsT<RT>& CV, PtocOutT<RT>* po = nullptr) {
+    RT sg = mc.sqrtdetgam;
+    RT v2 = RT(0.0), vlow[3] = {RT(0.0), RT(0.0), RT(0.0)};
 #pragma unroll
     for (int i = 0; i < 3; i++) {
 #pragma unroll
         for (int j = 0; j < 3; j++) vlow[i] += mc.gam[i][j] * pv.v[j];
         v2 += vlow[i] * pv.v[i];
     }
-    v2 = smin(v2, 1.0 - 1e-10);
-    double lor = 1.0 / sqrt(1.0 - v2);
+    v2 = smin(v2, RT(1.0) - RT(1e-10));
+    RT lor = RT(1.0) / sqrt(RT(1.0) - v2);
     bool ok = eos_ok(pv.rho);
-    double p = press(gamma, pv.rho, pv.eps);
-    double h = enth(gamma, pv.eps);
-    double Blow[3] = {0.0, 0.0, 0.0};
+    RT p = press(gamma, pv.rho, pv.eps);
+    RT h = enth(gamma, pv.eps);
+    RT Blow[3] = {RT(0.0), RT(0.0), RT(0.0)};
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) Blow[i] += mc.gam[i][j] * pv.B[j];
-    double Bv = 0.0;
+    RT Bv = RT(0.0);
 #pragma unroll
     for (int i = 0; i < 3; i++) Bv += Blow[i] * pv.v[i];
-    double Bsq = 0.0;
+    RT Bsq = RT(0.0);
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) Bsq += Blow[i] * mc.gam[i][j] * pv.B[j];
-    double b2 = (Bv * Bv + Bsq) / (lor);
-    double bt = lor * Bv / mc.alpha;
-    double pstar = p + b2 / 2;
-    double w = pv.rho * h + b2;
+    RT b2 = (Bv * Bv + Bsq) / (lor);
+    RT bt = lor * Bv / mc.alpha;
+    RT pstar = p + b2 / 2;
+    RT w = pv.rho * h + b2;
     CV.D = sg * pv.rho * lor;
     CV.tau = sg * (w * lor * lor - pstar - bt * bt) - CV.D;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        double bi = (Blow[i] + mc.alpha * bt * lor * vlow[i]) / lor;
+        RT bi = (Blow[i] + mc.alpha * bt * lor * vlow[i]) / lor;
         CV.S[i] = sg * (w * lor * lor * vlow[i] - mc.alpha * bt * bi);
         CV.B[i] = sg * pv.B[i];
     }
     if (po) { po->lor = lor; po->p = p; po->h = h; po->b2 = b2; }
     return ok;
 }
+
+using Prim = PrimT<double>;
+using Cons = ConsT<double>;
+using PtocOut = PtocOutT<double>;
 
 // ======================================================================
 // cons -> prim, conserved::ctop + f_df + cp_bd (physics/conserved.cpp:80-285)
@@ -413,25 +436,27 @@ BH_HD inline void pvfs(double r, double& rho, double& eps) {
 // ======================================================================
 // HLLD (solver/hlld.cpp)
 // ======================================================================
-struct Side {
-    double rho, eps, p, h, vn, vt1, vt2, Bn, Bt1, Bt2, ltz2, b2, pt, cf, D, tau, Sn, St1, St2, Bc, E;
+template <typename RT> struct SideT {
+    RT rho, eps, p, h, vn, vt1, vt2, Bn, Bt1, Bt2, ltz2, b2, pt, cf, D, tau, Sn, St1, St2, Bc, E;
 };
-struct Cst { double D, Sn, St1, St2, tau, Bn, Bt1, Bt2; };
+template <typename RT> struct CstT { RT D, Sn, St1, St2, tau, Bn, Bt1, Bt2; };
 
-BH_HD inline double fastspeed(double rho, double h, double b2, double cs2) {  // :34-39
-    double va2 = b2 / (rho * h + b2);
-    double cf2 = cs2 + va2 * (1 - cs2);
-    cf2 = smin(cf2, 1 - 1e-10);
+template <typename RT>
+BH_HD inline RT fastspeed(RT rho, RT h, RT b2, RT cs2) {  // :34-39
+    RT va2 = b2 / (rho * h + b2);
+    RT cf2 = cs2 + va2 * (1 - cs2);
+    cf2 = smin(cf2, 1 - RT(1e-10));
     return sqrt(cf2);
 }
-BH_HD inline bool side_(double gamma, const Prim& W, const Cons& U, const Met& mc, double sqrtg, int dim,
-                             Side& s) {                                         // :41-94
+template <typename RT>
+BH_HD inline bool side_(RT gamma, const PrimT<RT>& W, const ConsT<RT>& U, const MetT<RT>& mc, RT sqrtg, int dim,
+                             SideT<RT>& s) {                                         // :41-94
     int t1 = (dim + 1) % 3, t2 = (dim + 2) % 3;
     s.rho = W.rho; s.eps = W.eps;
     bool ok = eos_ok(W.rho);
     s.p = press(gamma, W.rho, W.eps);
     s.h = enth(gamma, W.eps);
-    double v2 = 0.0, vlow[3] = {0, 0, 0}, Blow[3] = {0, 0, 0};
+    RT v2 = RT(0.0), vlow[3] = {0, 0, 0}, Blow[3] = {0, 0, 0};
 #pragma unroll
     for (int i = 0; i < 3; i++) {
 #pragma unroll
@@ -441,19 +466,19 @@ BH_HD inline bool side_(double gamma, const Prim& W, const Cons& U, const Met& m
         }
         v2 += vlow[i] * W.v[i];
     }
-    v2 = smin(v2, 1 - 1e-10);
-    s.ltz2 = 1.0 / (1.0 - v2);
-    double Bv = 0.0;
+    v2 = smin(v2, 1 - RT(1e-10));
+    s.ltz2 = RT(1.0) / (RT(1.0) - v2);
+    RT Bv = RT(0.0);
 #pragma unroll
     for (int i = 0; i < 3; i++) Bv += Blow[i] * W.v[i];
-    double Bsq = 0.0;
+    RT Bsq = RT(0.0);
 #pragma unroll
     for (int i = 0; i < 3; i++) Bsq += Blow[i] * W.B[i];
     s.b2 = Bv * Bv + Bsq / s.ltz2;
     s.vn = W.v[dim]; s.vt1 = W.v[t1]; s.vt2 = W.v[t2];
     s.Bn = W.B[dim]; s.Bt1 = W.B[t1]; s.Bt2 = W.B[t2];
     s.pt = s.p + s.b2 / 2;
-    double cs2 = cs2f(gamma, W.rho, W.eps);
+    RT cs2 = cs2f(gamma, W.rho, W.eps);
     s.cf = fastspeed(s.rho, s.h, s.b2, cs2);
     s.D = U.D / sqrtg; s.tau = U.tau / sqrtg;
     s.Sn = U.S[dim] / sqrtg; s.St1 = U.S[t1] / sqrtg; s.St2 = U.S[t2] / sqrtg;
@@ -461,15 +486,16 @@ BH_HD inline bool side_(double gamma, const Prim& W, const Cons& U, const Met& m
     s.E = s.tau + s.D;
     return ok;
 }
-BH_HD inline Cst physflux(const Side& s, double a, double btn) {     // :97-122
-    Cst F;
-    double vn = s.vn;
+template <typename RT>
+BH_HD inline CstT<RT> physflux(const SideT<RT>& s, RT a, RT btn) {     // :97-122
+    CstT<RT> F;
+    RT vn = s.vn;
     F.D = s.D * vn;
     F.tau = (s.E + s.pt) * vn - s.Bn * (s.Bn * vn + s.Bt1 * s.vt1 + s.Bt2 * s.vt2) / s.ltz2;
     F.Sn = s.Sn * vn - s.Bn * s.Bn / s.ltz2 + s.pt;
     F.St1 = s.St1 * vn - s.Bt1 * s.Bn / s.ltz2;
     F.St2 = s.St2 * vn - s.Bt2 * s.Bn / s.ltz2;
-    F.Bn = 0.0;
+    F.Bn = RT(0.0);
     F.Bt1 = s.Bt1 * vn - s.Bn * s.vt1;
     F.Bt2 = s.Bt2 * vn - s.Bn * s.vt2;
     F.D = a * F.D - btn * s.D;
@@ -482,10 +508,11 @@ BH_HD inline Cst physflux(const Side& s, double a, double btn) {     // :97-122
     F.Bt2 = a * F.Bt2 - btn * s.Bt2;
     return F;
 }
-BH_HD inline Cst hll_flux(const Side& L, const Side& R, const Cst& FL, const Cst& FR, double SL,
-                                        double SR) {                            // :124-137
-    double dS = SR - SL;
-    Cst F;
+template <typename RT>
+BH_HD inline CstT<RT> hll_flux(const SideT<RT>& L, const SideT<RT>& R, const CstT<RT>& FL, const CstT<RT>& FR, RT SL,
+                                        RT SR) {                            // :124-137
+    RT dS = SR - SL;
+    CstT<RT> F;
     F.D = (SR * FL.D - SL * FR.D + SL * SR * (R.D - L.D)) / dS;
     F.tau = (SR * FL.tau - SL * FR.tau + SL * SR * (R.tau - L.tau)) / dS;
     F.Sn = (SR * FL.Sn - SL * FR.Sn + SL * SR * (R.Sn - L.Sn)) / dS;
@@ -496,17 +523,18 @@ BH_HD inline Cst hll_flux(const Side& L, const Side& R, const Cst& FL, const Cst
     F.Bt2 = (SR * FL.Bt2 - SL * FR.Bt2 + SL * SR * (R.Bt2 - L.Bt2)) / dS;
     return F;
 }
-BH_HD inline Cst star_stt(const Side& s, double SK, double SM, double pt_x) {  // :140-159
-    Cst Ux;
+template <typename RT>
+BH_HD inline CstT<RT> star_stt(const SideT<RT>& s, RT SK, RT SM, RT pt_x) {  // :140-159
+    CstT<RT> Ux;
     Ux.D = s.D * (SK - s.vn) / (SK - SM);
     Ux.tau = (s.E * (SK - s.vn) - s.pt * s.vn + pt_x * SM) / (SK - SM) - Ux.D;
     Ux.Sn = (s.Sn * (SK - s.vn) - s.pt + pt_x) / (SK - SM);
     Ux.St1 = s.St1 * (SK - s.vn) / (SK - SM);
     Ux.St2 = s.St2 * (SK - s.vn) / (SK - SM);
     Ux.Bn = s.Bc;
-    double den = s.D * (SK - s.vn) * (SK - SM) - s.Bn * s.Bn;
-    if (fabs(den) > 1e-14) {
-        double k = s.Bn * (SM - s.vn) / den;
+    RT den = s.D * (SK - s.vn) * (SK - SM) - s.Bn * s.Bn;
+    if (fabs(den) > RT(1e-14)) {
+        RT k = s.Bn * (SM - s.vn) / den;
         Ux.Bt1 = s.Bt1 - s.Bn * (s.vt1 * (SK - s.vn) + s.Bn * s.Bt1 / s.D) * k;
         Ux.Bt2 = s.Bt2 - s.Bn * (s.vt2 * (SK - s.vn) + s.Bn * s.Bt2 / s.D) * k;
     } else {
@@ -516,35 +544,37 @@ BH_HD inline Cst star_stt(const Side& s, double SK, double SM, double pt_x) {  /
 }
 // alfstar_stt (:161-201); its degenerate branch (:171-173) is overwritten
 // by the assignments after it and has no effect
-BH_HD inline void alfstar_stt(const Cst& UxL, const Cst& UxR, double Bn, double SM, Cst& UxxL,
-                                            Cst& UxxR) {
+template <typename RT>
+BH_HD inline void alfstar_stt(const CstT<RT>& UxL, const CstT<RT>& UxR, RT Bn, RT SM, CstT<RT>& UxxL,
+                                            CstT<RT>& UxxR) {
     UxxL.D = UxL.D; UxxL.tau = UxL.tau;
     UxxR.D = UxR.D; UxxR.tau = UxR.tau;
     UxxL.Bn = UxL.Bn; UxxR.Bn = UxR.Bn;
-    double sq_DL = sqrt(fabs(UxL.D));
-    double sq_DR = sqrt(fabs(UxR.D));
-    double den = sq_DL + sq_DR;
-    double sgnBn = (Bn >= 0.0) ? 1.0 : -1.0;
-    double vt1xx = (sq_DL * UxL.St1 / UxL.D + sq_DR * UxR.St1 / UxR.D + sgnBn * (UxR.Bt1 - UxL.Bt1)) / den;
-    double vt2xx = (sq_DL * UxL.St2 / UxL.D + sq_DR * UxR.St2 / UxR.D + sgnBn * (UxR.Bt2 - UxL.Bt2)) / den;
-    double Bt1xx = (sq_DL * UxL.Bt1 / UxL.D + sq_DR * UxR.Bt1 / UxR.D +
+    RT sq_DL = sqrt(fabs(UxL.D));
+    RT sq_DR = sqrt(fabs(UxR.D));
+    RT den = sq_DL + sq_DR;
+    RT sgnBn = (Bn >= RT(0.0)) ? RT(1.0) : -RT(1.0);
+    RT vt1xx = (sq_DL * UxL.St1 / UxL.D + sq_DR * UxR.St1 / UxR.D + sgnBn * (UxR.Bt1 - UxL.Bt1)) / den;
+    RT vt2xx = (sq_DL * UxL.St2 / UxL.D + sq_DR * UxR.St2 / UxR.D + sgnBn * (UxR.Bt2 - UxL.Bt2)) / den;
+    RT Bt1xx = (sq_DL * UxL.Bt1 / UxL.D + sq_DR * UxR.Bt1 / UxR.D +
                     sgnBn * sq_DL * sq_DR * (UxR.St1 / UxR.D - UxL.St1 / UxL.D)) / den;
-    double Bt2xx = (sq_DL * UxL.Bt2 / UxL.D + sq_DR * UxR.Bt2 / UxR.D +
+    RT Bt2xx = (sq_DL * UxL.Bt2 / UxL.D + sq_DR * UxR.Bt2 / UxR.D +
                     sgnBn * sq_DL * sq_DR * (UxR.St2 / UxR.D - UxL.St2 / UxL.D)) / den;
     UxxL.St1 = UxL.D * vt1xx; UxxR.St1 = UxR.D * vt1xx;
     UxxL.St2 = UxL.D * vt2xx; UxxR.St2 = UxR.D * vt2xx;
     UxxL.Bt1 = Bt1xx; UxxR.Bt1 = Bt1xx;
     UxxL.Bt2 = Bt2xx; UxxR.Bt2 = Bt2xx;
     UxxL.Sn = UxL.D * SM; UxxR.Sn = UxR.D * SM;
-    const double vt1xL = UxL.St1 / UxL.D, vt2xL = UxL.St2 / UxL.D;
-    const double vt1xR = UxR.St1 / UxR.D, vt2xR = UxR.St2 / UxR.D;
-    double dE_L = sq_DL * sgnBn * (vt1xx * Bt1xx + vt2xx * Bt2xx - vt1xL * UxL.Bt1 - vt2xL * UxL.Bt2);
-    double dE_R = sq_DR * sgnBn * (vt1xx * Bt1xx + vt2xx * Bt2xx - vt1xR * UxR.Bt1 - vt2xR * UxR.Bt2);
+    const RT vt1xL = UxL.St1 / UxL.D, vt2xL = UxL.St2 / UxL.D;
+    const RT vt1xR = UxR.St1 / UxR.D, vt2xR = UxR.St2 / UxR.D;
+    RT dE_L = sq_DL * sgnBn * (vt1xx * Bt1xx + vt2xx * Bt2xx - vt1xL * UxL.Bt1 - vt2xL * UxL.Bt2);
+    RT dE_R = sq_DR * sgnBn * (vt1xx * Bt1xx + vt2xx * Bt2xx - vt1xR * UxR.Bt1 - vt2xR * UxR.Bt2);
     UxxL.tau = UxL.tau - dE_L;
     UxxR.tau = UxR.tau + dE_R;
 }
-BH_HD inline Cst interflux(const Cst& FK, double SK, const Cst& Ux, const Side& s) {  // :203-216
-    Cst F;
+template <typename RT>
+BH_HD inline CstT<RT> interflux(const CstT<RT>& FK, RT SK, const CstT<RT>& Ux, const SideT<RT>& s) {  // :203-216
+    CstT<RT> F;
     F.D = FK.D + SK * (Ux.D - s.D);
     F.tau = FK.tau + SK * (Ux.tau - (s.E - s.D));
     F.Sn = FK.Sn + SK * (Ux.Sn - s.Sn);
@@ -556,66 +586,68 @@ BH_HD inline Cst interflux(const Cst& FK, double SK, const Cst& Ux, const Side& 
     return F;
 }
 // flux (:218-227): out in cons order D,S0,S1,S2,tau,B0,B1,B2, times sqrt(-g)
-BH_HD inline void flux_out(const Cst& F, double sg, int dim, double o[8]) {
+template <typename RT>
+BH_HD inline void flux_out(const CstT<RT>& F, RT sg, int dim, RT o[8]) {
     int t1 = (dim + 1) % 3, t2 = (dim + 2) % 3;
     o[0] = sg * F.D; o[4] = sg * F.tau;
     o[5 + dim] = sg * F.Bn; o[5 + t1] = sg * F.Bt1; o[5 + t2] = sg * F.Bt2;
     o[1 + dim] = sg * F.Sn; o[1 + t1] = sg * F.St1; o[1 + t2] = sg * F.St2;
 }
 // hlld (:230-312); returns false where the reference throws
-BH_HD inline bool hlld(double gamma, const Met& mc, const Prim& WL, const Prim& WR, const Cons& UL,
-                            const Cons& UR, int dim, double Fo[8], double& ctspeed) {
-    double sg = mc.sqrtdetg;
-    Side L, R;
+template <typename RT>
+BH_HD inline bool hlld(RT gamma, const MetT<RT>& mc, const PrimT<RT>& WL, const PrimT<RT>& WR, const ConsT<RT>& UL,
+                            const ConsT<RT>& UR, int dim, RT Fo[8], RT& ctspeed) {
+    RT sg = mc.sqrtdetg;
+    SideT<RT> L, R;
     bool ok = side_(gamma, WL, UL, mc, sg, dim, L);
     ok &= side_(gamma, WR, UR, mc, sg, dim, R);
-    double a = mc.alpha, bd = mc.beta[dim];
-    double SL = smin(a * (L.vn - L.cf) - bd, a * (R.vn - R.cf) - bd);
-    double SR = smax(a * (L.vn + L.cf) - bd, a * (R.vn + R.cf) - bd);
-    Cst FL = physflux(L, a, bd), FR = physflux(R, a, bd);
-    double cts = smax(fabs(SL), fabs(SR));
+    RT a = mc.alpha, bd = mc.beta[dim];
+    RT SL = smin(a * (L.vn - L.cf) - bd, a * (R.vn - R.cf) - bd);
+    RT SR = smax(a * (L.vn + L.cf) - bd, a * (R.vn + R.cf) - bd);
+    CstT<RT> FL = physflux(L, a, bd), FR = physflux(R, a, bd);
+    RT cts = smax(fabs(SL), fabs(SR));
     ctspeed = cts;
     // :244-246 computes an HLL flux that every later path overwrites
-    if (SL >= 0.0) { flux_out(FL, sg, dim, Fo); return ok; }
-    if (SR <= 0.0) { flux_out(FR, sg, dim, Fo); return ok; }
-    double pt_x = (SR * L.pt - SL * R.pt + SL * SR * (R.Sn - L.Sn)) / (SR - SL);
-    double SM_u = SR * L.E - SL * R.E - FR.tau - FR.D + FL.tau + FL.D;
-    double SM_d = SR * L.D - SL * R.D - FR.D + FL.D;
-    if (fabs(SM_d) < 1e-12) { flux_out(hll_flux(L, R, FL, FR, SL, SR), sg, dim, Fo); return ok; }
-    double SM = SM_u / SM_d;
-    Cst UxL = star_stt(L, SL, SM, pt_x);
-    Cst UxR = star_stt(R, SR, SM, pt_x);
-    double SLx = SM - fabs(L.Bn) / sqrt(fabs(UxL.D));
-    double SRx = SM + fabs(R.Bn) / sqrt(fabs(UxR.D));
-    if (UxL.D <= 0.0 || UxR.D <= 0.0) { flux_out(hll_flux(L, R, FL, FR, SL, SR), sg, dim, Fo); return ok; }
-    Cst Fs;
-    if (SM >= 0.0) {
-        if (SLx >= 0.0) {
+    if (SL >= RT(0.0)) { flux_out(FL, sg, dim, Fo); return ok; }
+    if (SR <= RT(0.0)) { flux_out(FR, sg, dim, Fo); return ok; }
+    RT pt_x = (SR * L.pt - SL * R.pt + SL * SR * (R.Sn - L.Sn)) / (SR - SL);
+    RT SM_u = SR * L.E - SL * R.E - FR.tau - FR.D + FL.tau + FL.D;
+    RT SM_d = SR * L.D - SL * R.D - FR.D + FL.D;
+    if (fabs(SM_d) < RT(1e-12)) { flux_out(hll_flux(L, R, FL, FR, SL, SR), sg, dim, Fo); return ok; }
+    RT SM = SM_u / SM_d;
+    CstT<RT> UxL = star_stt(L, SL, SM, pt_x);
+    CstT<RT> UxR = star_stt(R, SR, SM, pt_x);
+    RT SLx = SM - fabs(L.Bn) / sqrt(fabs(UxL.D));
+    RT SRx = SM + fabs(R.Bn) / sqrt(fabs(UxR.D));
+    if (UxL.D <= RT(0.0) || UxR.D <= RT(0.0)) { flux_out(hll_flux(L, R, FL, FR, SL, SR), sg, dim, Fo); return ok; }
+    CstT<RT> Fs;
+    if (SM >= RT(0.0)) {
+        if (SLx >= RT(0.0)) {
             Fs = interflux(FL, SL, UxL, L);
         } else {
-            Cst UxxL, UxxR;
+            CstT<RT> UxxL, UxxR;
             alfstar_stt(UxL, UxR, L.Bn, SM, UxxL, UxxR);
-            Cst FLx = interflux(FL, SL, UxL, L);
+            CstT<RT> FLx = interflux(FL, SL, UxL, L);
             Fs = interflux(FLx, SLx, UxxL, L);
         }
     } else {
-        if (SRx >= 0.0) {
+        if (SRx >= RT(0.0)) {
             Fs = interflux(FR, SR, UxR, R);
         } else {
-            Cst UxxL, UxxR;
+            CstT<RT> UxxL, UxxR;
             alfstar_stt(UxL, UxR, L.Bn, SM, UxxL, UxxR);
-            Cst FRx = interflux(FR, SR, UxR, R);
+            CstT<RT> FRx = interflux(FR, SR, UxR, R);
             Fs = interflux(FRx, SRx, UxxR, R);
         }
     }
-    double F[8];
+    RT F[8];
     flux_out(Fs, sg, dim, F);
     bool fin = true;
 #pragma unroll
     for (int q = 0; q < 8; q++) fin &= isfinite(F[q]);
-    if (!fin || cts > 1.0) {
+    if (!fin || cts > RT(1.0)) {
         flux_out(hll_flux(L, R, FL, FR, SL, SR), sg, dim, F);
-        if (cts > 1.0) ctspeed = smin(cts, 1.0);
+        if (cts > RT(1.0)) ctspeed = smin(cts, RT(1.0));
     }
 #pragma unroll
     for (int q = 0; q < 8; q++) Fo[q] = F[q];
@@ -625,37 +657,43 @@ BH_HD inline bool hlld(double gamma, const Met& mc, const Prim& WL, const Prim& 
 // ======================================================================
 // PLM reconstruction (recon.hpp:16-41, grid/reconstruction.cpp:28-97)
 // ======================================================================
-BH_HD inline double minmod(double a, double b) {
-    if (a * b <= 0.0) return 0.0;
+template <typename RT>
+BH_HD inline RT minmod(RT a, RT b) {
+    if (a * b <= RT(0.0)) return RT(0.0);
     return (fabs(a) < fabs(b)) ? a : b;
 }
-BH_HD inline double vanleer(double a, double b) {
-    if (a * b <= 0.0) return 0.0;
-    return 2.0 * a * b / (a + b);
+template <typename RT>
+BH_HD inline RT vanleer(RT a, RT b) {
+    if (a * b <= RT(0.0)) return RT(0.0);
+    return RT(2.0) * a * b / (a + b);
 }
-BH_HD inline double mclim(double a, double b) {
-    if (a * b <= 0.0) return 0.0;
-    double c = (a + b) / 2;
-    double s = (a > 0.0) ? 1.0 : -1.0;
+template <typename RT>
+BH_HD inline RT mclim(RT a, RT b) {
+    if (a * b <= RT(0.0)) return RT(0.0);
+    RT c = (a + b) / 2;
+    RT s = (a > RT(0.0)) ? RT(1.0) : -RT(1.0);
     return s * minmod(fabs(2 * a), minmod(fabs(2 * b), fabs(c)));
 }
-BH_HD inline double limit(double dl, double dr, int lim) {
+template <typename RT>
+BH_HD inline RT limit(RT dl, RT dr, int lim) {
     return lim == BH_VANLEER ? vanleer(dl, dr) : lim == BH_MC ? mclim(dl, dr) : minmod(dl, dr);
 }
-BH_HD inline void recon_scal(double Wm, double Wc, double Wp, double Wpp, int lim, double& fL,
-                                           double& fR) {
-    fL = Wc + limit(Wc - Wm, Wp - Wc, lim) / 2.0;
-    fR = Wp - limit(Wp - Wc, Wpp - Wp, lim) / 2.0;
+template <typename RT>
+BH_HD inline void recon_scal(RT Wm, RT Wc, RT Wp, RT Wpp, int lim, RT& fL,
+                                           RT& fR) {
+    fL = Wc + limit(Wc - Wm, Wp - Wc, lim) / RT(2.0);
+    fR = Wp - limit(Wp - Wc, Wpp - Wp, lim) / RT(2.0);
 }
 // causality rescale of reconfp (:69-83) with the cell's metric
-BH_HD inline void causalv(double v[3], const Met& mc) {
-    double v2 = 0.0;
+template <typename RT>
+BH_HD inline void causalv(RT v[3], const MetT<RT>& mc) {
+    RT v2 = RT(0.0);
 #pragma unroll
     for (int m = 0; m < 3; m++)
 #pragma unroll
         for (int n = 0; n < 3; n++) v2 += mc.gam[m][n] * v[m] * v[n];
-    if (v2 >= 1.0) {
-        double s = (1 - 1e-10) / sqrt(v2);
+    if (v2 >= RT(1.0)) {
+        RT s = (1 - RT(1e-10)) / sqrt(v2);
 #pragma unroll
         for (int a = 0; a < 3; a++) v[a] *= s;
     }

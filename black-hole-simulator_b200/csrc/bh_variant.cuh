@@ -17,6 +17,11 @@
 #ifndef BH_VARIANT
 #error "define BH_VARIANT before including bh_variant.cuh"
 #endif
+// arithmetic type of reconstruction, face fluxes and sources (FP64 unless
+// the including file asks for the mixed variant)
+#ifndef BH_REAL
+#define BH_REAL double
+#endif
 
 namespace BH_VARIANT {
 using namespace bh;
@@ -60,11 +65,11 @@ __global__ void k_hlld(KP k, const double* WL, const double* WR, const double* U
     BATCH; hlld_item(k, WL, WR, UL, UR, r, th, dim, n, q, F, cts);
 }
 __global__ void k_reconfp(KP kp, Pool P, int dim, int lim, int64_t n, double* Lo, double* Ro) {
-    ITEM(NFACE); reconfp_item(kp, P, blockIdx.y, dim, e, lim, n, Lo, Ro);
+    ITEM(NFACE); reconfp_item<BH_REAL>(kp, P, blockIdx.y, dim, e, lim, n, Lo, Ro);
 }
 // patch::fluxcomp: one face per thread, direction blockIdx.z
 __global__ void __launch_bounds__(TPB, BH_MINB_FLUX) k_flux(KP kp, Pool P, const int32_t* list) {
-    ITEM(NFACE); flux_item(kp, P, list[blockIdx.y], blockIdx.z, e);
+    ITEM(NFACE); flux_item<BH_REAL>(kp, P, list[blockIdx.y], blockIdx.z, e);
 }
 __global__ void k_emf(Pool P, const int32_t* list) { ITEM(N_EDGE); emf_item(P, list[blockIdx.y], e); }
 __global__ void k_bfupdate(Pool P, const int32_t* list, const double* dtp) {
@@ -72,10 +77,10 @@ __global__ void k_bfupdate(Pool P, const int32_t* list, const double* dtp) {
 }
 __global__ void k_f2cb(KP kp, Pool P, const int32_t* list) { ITEM(N_F2C); f2cb_item(kp, P, list[blockIdx.y], e); }
 __global__ void k_div_source(KP kp, Pool P, const int32_t* list, double* dv, double* sv) {
-    ITEM(N_INT); div_source_item(kp, P, list[blockIdx.y], e, dv, sv);
+    ITEM(N_INT); div_source_item<BH_REAL>(kp, P, list[blockIdx.y], e, dv, sv);
 }
 __global__ void __launch_bounds__(TPB, BH_MINB_UPDATE) k_update(KP kp, Pool P, const int32_t* list, const double* dtp, int stage) {
-    ITEM(N_F2C); update_item(kp, P, list[blockIdx.y], e, *dtp, stage);
+    ITEM(N_F2C); update_item<BH_REAL>(kp, P, list[blockIdx.y], e, *dtp, stage);
 }
 __global__ void k_ghost_fill(KP kp, Pool P, const int32_t* list) { ITEM(N_STRIP); ghost_fill_item(kp, P, list[blockIdx.y], e); }
 __global__ void k_ghost_ctop(KP kp, Pool P, const int32_t* list) { ITEM(NC); ghost_ctop_item(kp, P, list[blockIdx.y], e); }

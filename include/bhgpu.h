@@ -53,7 +53,10 @@ enum {
 /* arithmetic variant (bh_params.precision) */
 enum {
     BH_FP64 = 0,      /* FP64 with the reference's separate multiply/add roundings */
-    BH_FP64_FMA = 1   /* FP64 with fused multiply-add contraction                  */
+    BH_FP64_FMA = 1,  /* FP64 with fused multiply-add contraction                  */
+    BH_MIXED = 2      /* reconstruction, face fluxes (ptoc + HLLD) and the geometric
+                         source in FP32; metric, constrained transport, flux
+                         divergence, RK combine, con2prim, floors and dt in FP64  */
 };
 /* reconstruction limiter (recon.hpp:36) */
 enum { BH_MINMOD = 0, BH_VANLEER = 1, BH_MC = 2 };
@@ -68,7 +71,7 @@ typedef struct bh_params {
     double tol;          /* con2prim tolerance (1e-10)          cons.hpp:75         */
     double cM, ca, cQ;   /* metric carried by every cell: the default metric()
                             = (1, 0, 0) in the reference       cell.hpp:25, metric.hpp:30 */
-    int32_t precision;   /* BH_FP64 (reference-faithful) or BH_FP64_FMA              */
+    int32_t precision;   /* BH_FP64 (reference-faithful), BH_FP64_FMA or BH_MIXED    */
     int32_t reserved;
 } bh_params;
 

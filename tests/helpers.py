@@ -54,6 +54,20 @@ def ulp_sensitivity(orc, hp, steps=1, seed=0):
     return [rel_linf(pert.U[:, v], base.U[:, v]) for v in range(8)]
 
 
+def perturbed_response(orc, hp, steps, rel=1e-7, seed=0):
+    """The reference's own response to a relative input perturbation: the
+    oracle run from U and from U (1 + rel N(0,1)) for ``steps`` steps;
+    returns (per-variable relative L1 difference, NaN-mask disagreement)."""
+    rng = np.random.default_rng(seed)
+    base = hp.copy()
+    pert = hp.copy()
+    pert.U[:] = pert.U * (1.0 + rel * rng.standard_normal(pert.U.shape))
+    for _ in range(steps):
+        orc.step(base, 0.4)
+        orc.step(pert, 0.4)
+    return rel_l1(pert.U, base.U), mask_disagreement(pert.U, base.U), base
+
+
 def rel_l1(a, b):
     """Per-variable relative L1 error over the entries finite in both."""
     out = []
@@ -74,13 +88,15 @@ def same_nan(a, b):
     return np.array_equal(np.isfinite(a), np.isfinite(b))
 
 
-def box_case(nq=2, seed=3, periodic=True, lim=0, M=0.0, a=0.0, lo=10.0, hi=12.0):
-    """Magnetised-box state on an nq^3 quilt: (quilt, oracle, host pool)."""
+def box_case(nq=2, seed=3, periodic=True, lim=0, M=0.0, a=0.0, lo=10.0, hi=12.0, **box):
+    """Magnetised-box state on an nq^3 quilt: (quilt, oracle, host pool);
+    ``box`` goes to configs.magnetised_box (B0=(0, 0, 0), amp=0 gives the
+    unmagnetised box)."""
     q = Quilt([lo] * 3, [hi] * 3, nq, periodic=periodic)
     orc = oracle.Oracle(M, a, 0.0, GAMMA, limiter=lim)
     hp = oracle.HostPool(q.tables())
     orc.geometry(hp)
-    W, Bf = configs.magnetised_box(q, seed=seed, gamma=GAMMA)
+    W, Bf = configs.magnetised_box(q, seed=seed, gamma=GAMMA, **box)
     hp.W[:] = W
     hp.Bf[:] = Bf
     for p in range(hp.npatch):
@@ -88,10 +104,10 @@ def box_case(nq=2, seed=3, periodic=True, lim=0, M=0.0, a=0.0, lo=10.0, hi=12.0)
     return q, orc, hp
 
 
-def gpu_tree(q, hp, M=0.0, a=0.0, lim=0):
+def gpu_tree(q, hp, M=0.0, a=0.0, lim=0, precision="fp64"):
     import bhgpu
     tree = bhgpu.AmrTree(q.dom_l, q.dom_h, q.nqlt, M=M, a=a, Q=0.0, gm=GAMMA, periodic=q.periodic,
-                         limiter=lim, quilt=q, init_floor=False)
+                         limiter=lim, quilt=q, init_floor=False, precision=precision)
     tree.load(U=hp.U, W=hp.W, Bf=hp.Bf, dU=hp.dU)
     return tree
 

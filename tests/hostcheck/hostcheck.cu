@@ -39,13 +39,13 @@ void hc_reconfp(const bh_params* Pp, const bh_pool* pool, int dim, int lim, doub
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     int64_t n = (int64_t)pool->npatch * NFACE;
     for (int p = 0; p < pool->npatch; p++)
-        for (int f = 0; f < NFACE; f++) reconfp_item(k, P, p, dim, f, lim, n, L, R);
+        for (int f = 0; f < NFACE; f++) reconfp_item<double>(k, P, p, dim, f, lim, n, L, R);
 }
 void hc_fluxcomp(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < pool->npatch; i++)
         for (int dim = 0; dim < 3; dim++)
-            for (int f = 0; f < NFACE; f++) flux_item(k, P, pool->all[i], dim, f);
+            for (int f = 0; f < NFACE; f++) flux_item<double>(k, P, pool->all[i], dim, f);
 }
 void hc_emfcomp(const bh_pool* pool) {
     Pool P = pool_of(pool);
@@ -73,7 +73,7 @@ void hc_maxdivb(const bh_pool* pool, double* out) {
 void hc_div_source(const bh_params* Pp, const bh_pool* pool, double* dv, double* sv) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < pool->npatch; i++)
-        for (int c = 0; c < N_INT; c++) div_source_item(k, P, pool->all[i], c, dv, sv);
+        for (int c = 0; c < N_INT; c++) div_source_item<double>(k, P, pool->all[i], c, dv, sv);
 }
 void hc_ghosts(const bh_params* Pp, const bh_pool* pool, const int32_t* list, int n) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
@@ -103,7 +103,7 @@ void hc_ghosts_prims(const bh_params* Pp, const bh_pool* pool) {
 void hc_update(const bh_params* Pp, const bh_pool* pool, double dt, int stage) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < pool->npatch; i++)
-        for (int e = 0; e < N_F2C; e++) update_item(k, P, pool->all[i], e, dt, stage);
+        for (int e = 0; e < N_F2C; e++) update_item<double>(k, P, pool->all[i], e, dt, stage);
 }
 void hc_floors(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
