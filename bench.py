@@ -368,9 +368,9 @@ def run_ours(args):
     pool = C.byref(tree.pool)
     dtp = _p(tree.dt)
     ev = {k: [] for k in ("ghosts_prims", "fluxcomp", "update", "floors")}
-    # my kernels per step: dt_init, dtcomp, 2 x (ghost_fill, prims_interior,
-    # prims_ghost, flux, emf, bfupdate, update), floors
-    KL_PER_STEP = 17
+    # my kernels per step: dt_init, dtcomp, 2 x (ghost_copy, ghost_prolong,
+    # prims_interior, prims_ghost, flux, emf, bfupdate, update), floors
+    KL_PER_STEP = 19
 
     def timed(name, record, fn):
         if record:

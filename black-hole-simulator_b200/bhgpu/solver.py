@@ -388,7 +388,7 @@ class RK2Integrator:
 class StepGraph:
     """rk2integrator::step recorded once into a CUDA graph and replayed.
 
-    The step's 17 launches (dtcomp, two stages, floors) read dt from device
+    The step's 19 launches (dtcomp, two stages, floors) read dt from device
     memory and never synchronise with the host, so the whole step is one
     graph; ``before`` (optional) is recorded in front of it, e.g. a copy
     that resets the state.  Replays run on the current stream.  The domain

@@ -273,11 +273,9 @@ BH_HD inline double maxdivb_item(const Pool& P, int p, int e) {        // maxdiv
 }
 
 // f2cB (:60-75) for one cell: the face-averaged B and the cell's sqrt(-g)
+BH_HD inline void face_avg_B(const Pool& P, int p, int i, int j, int k, double B[3]);
 BH_HD inline void f2cb_cell(const KP& kp, const Pool& P, int p, int i, int j, int k, double B[3], double& sg) {
-    const double *Bx = Bfv(P, p, 0), *By = Bfv(P, p, 1), *Bz = Bfv(P, p, 2);
-    B[0] = (Bx[xfc(i, j, k)] + Bx[xfc(i - 1, j, k)]) / 2;
-    B[1] = (By[yfc(i, j, k)] + By[yfc(i, j - 1, k)]) / 2;
-    B[2] = (Bz[zfc(i, j, k)] + Bz[zfc(i, j, k - 1)]) / 2;
+    face_avg_B(P, p, i, j, k, B);
     int l = lindx(i, j, k);
     Met mc;
     met_comp(kp.cell, rr(P, p, l), tt(P, p, l), mc);
@@ -306,10 +304,14 @@ BH_HD inline void div_flux(const Pool& P, int p, int i, int j, int k, double sg,
     out[5] = out[6] = out[7] = 0.0;
 }
 
-// geometric source (:41-153) with the full cell metric (evaluated in FP64)
-// and arithmetic in RT; false where the EOS throws
+// geometric source (:41-153) with the cell metric (evaluated in FP64) and
+// arithmetic in RT; false where the EOS throws.  The contraction
+// src[m] = sum_n sum_q T[n][q] (sum_s g[m][s] Gamma[s][n][q]) runs with
+// (n, q) outermost so that each Christoffel symbol is formed once and used
+// for all four m; every accumulator still adds its terms in the order
+// (n, q) of the reference, so the roundings are the reference's.
 template <typename RT>
-BH_HD inline bool source(const KP& kp, const MetFull& mc, const Prim& Wd, RT out[8]) {
+BH_HD inline bool source(const KP& kp, const MetSrc& mc, const Prim& Wd, RT out[8]) {
     PrimT<RT> W;
     W.rho = RT(Wd.rho); W.eps = RT(Wd.eps);
     for (int d = 0; d < 3; d++) { W.v[d] = RT(Wd.v[d]); W.B[d] = RT(Wd.B[d]); }
@@ -344,17 +346,24 @@ BH_HD inline bool source(const KP& kp, const MetFull& mc, const Prim& Wd, RT out
     RT rhohb2 = W.rho * h + b2;
     for (int m = 0; m < 4; m++)
         for (int n = 0; n < 4; n++) T44[m][n] = rhohb2 * u4[m] * u4[n] + px * RT(mc.gi[m][n]) - b4[m] * b4[n];
-    RT src[4];
-    for (int m = 0; m < 4; m++) {
-        RT acc = RT(0.0);
-        for (int n = 0; n < 4; n++)
-            for (int q = 0; q < 4; q++) {
+    RT acc[4] = {RT(0.0), RT(0.0), RT(0.0), RT(0.0)};
+#pragma unroll
+    for (int n = 0; n < 4; n++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            RT Gs[4];
+#pragma unroll
+            for (int s = 0; s < 4; s++) Gs[s] = RT(christoffel(mc, s, n, q));
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
                 RT G_ = RT(0.0);   // lowered Christoffel g[m][s] Gamma[s][n][q], summed over s
-                for (int s = 0; s < 4; s++) G_ += RT(mc.g[m][s]) * RT(mc.G[s][n][q]);
-                acc += T44[n][q] * G_;
+#pragma unroll
+                for (int s = 0; s < 4; s++) G_ += RT(mc.g[m][s]) * Gs[s];
+                acc[m] += T44[n][q] * G_;
             }
-        src[m] = acc * RT(mc.sqrtdetg);
-    }
+        }
+    RT src[4];
+    for (int m = 0; m < 4; m++) src[m] = acc[m] * RT(mc.sqrtdetg);
     out[0] = RT(0.0);
     out[4] = src[0];
     out[1] = src[1]; out[2] = src[2]; out[3] = src[3];
@@ -366,8 +375,8 @@ template <typename RT>
 BH_HD inline void div_source_item(const KP& kp, const Pool& P, int p, int c, double* dv, double* sv) {
     int i = c / 256, j = (c / 16) % 16, k = c % 16;
     int l = lindx(i, j, k);
-    MetFull mf;
-    met_full(kp.cell, rr(P, p, l), tt(P, p, l), mf);
+    MetSrc mf;
+    met_src(kp.cell, rr(P, p, l), tt(P, p, l), mf);
     double d8[8];
     RT s8[8];
     div_flux(P, p, i, j, k, mf.sqrtdetg, d8);
@@ -380,27 +389,36 @@ BH_HD inline void div_source_item(const KP& kp, const Pool& P, int p, int c, dou
     }
 }
 
-// f2cB + the conserved update of rkstg (integrator.cpp:325-347), fused:
-// cells in [-1,18)^3 take the face-averaged B; interior cells then add
-// dt * (div_flux + source) and refresh U.B = sqrt(-g) W.B
+// f2cB + the conserved update of rkstg (integrator.cpp:325-347), fused.
+// Cells in [-1,18)^3 take the face-averaged B; interior cells then add
+// dt * (div_flux + source) and refresh U.B = sqrt(-g) W.B.  The two kinds
+// of cells are separate items so that a warp holds one kind only:
+// update_interior_item for the 16^3 interior cells, update_shell_item for
+// the 2763 cells of [-1,18)^3 outside it (f2cB alone).
+BH_HD inline void face_avg_B(const Pool& P, int p, int i, int j, int k, double B[3]) {
+    const double *Bx = Bfv(P, p, 0), *By = Bfv(P, p, 1), *Bz = Bfv(P, p, 2);
+    B[0] = (Bx[xfc(i, j, k)] + Bx[xfc(i - 1, j, k)]) / 2;
+    B[1] = (By[yfc(i, j, k)] + By[yfc(i, j - 1, k)]) / 2;
+    B[2] = (Bz[zfc(i, j, k)] + Bz[zfc(i, j, k - 1)]) / 2;
+}
+
 template <typename RT>
-BH_HD inline void update_item(const KP& kp, const Pool& P, int p, int e, double dt, int stage) {
-    int i = e / 361 - 1, j = (e / 19) % 19 - 1, k = e % 19 - 1;
-    double B[3], sg;
-    f2cb_cell(kp, P, p, i, j, k, B, sg);
+BH_HD inline void update_interior_item(const KP& kp, const Pool& P, int p, int c, double dt, int stage) {
+    int i = c / 256, j = (c / 16) % 16, k = c % 16;
     int l = lindx(i, j, k);
+    double B[3];
+    face_avg_B(P, p, i, j, k, B);
     for (int d = 0; d < 3; d++) Wv(P, p, 5 + d)[l] = B[d];
-    if (is_ghost(i, j, k)) {
-        for (int d = 0; d < 3; d++) Uv(P, p, 5 + d)[l] = sg * B[d];
-        return;
-    }
-    MetFull mf;
-    met_full(kp.cell, rr(P, p, l), tt(P, p, l), mf);
+    // the cell metric's sqrt(-g): f2cB's metric::comp and the source's
+    // metric share the expression, hence the value
+    MetSrc mf;
+    met_src(kp.cell, rr(P, p, l), tt(P, p, l), mf);
     double d8[8];
     RT s8[8];
     div_flux(P, p, i, j, k, mf.sqrtdetg, d8);
     Prim w;
-    load_prim(P, p, l, w);
+    w.rho = Wv(P, p, 0)[l]; w.eps = Wv(P, p, 1)[l];
+    for (int d = 0; d < 3; d++) { w.v[d] = Wv(P, p, 2 + d)[l]; w.B[d] = B[d]; }
     if (!source(kp, mf, w, s8)) flag(P.err, BH_ERR_DOMAIN);
     for (int v = 0; v < 5; v++) {
         double dU = d8[v] + double(s8[v]);
@@ -413,8 +431,35 @@ BH_HD inline void update_item(const KP& kp, const Pool& P, int p, int e, double 
         }
     }
     if (stage == 0)   // c.dU = c.U after f2cB has set U.B = sqrt(-g) W.B
-        for (int d = 0; d < 3; d++) dUv(P, p, 5 + d)[l] = sg * B[d];
+        for (int d = 0; d < 3; d++) dUv(P, p, 5 + d)[l] = mf.sqrtdetg * B[d];
     for (int d = 0; d < 3; d++) Uv(P, p, 5 + d)[l] = mf.sqrtdetg * B[d];
+}
+
+constexpr int N_SHELL = N_F2C - N_INT;   // 2763
+// shell cell e in [0, N_SHELL): the planes i = -1, 16, 17 (19 x 19 each),
+// then j = -1, 16, 17 for i in [0,16) (19 each), then k = -1, 16, 17
+BH_HD inline void shell_ijk(int e, int& i, int& j, int& k) {
+    if (e < 1083) {
+        int ii = e / 361;
+        i = ii == 0 ? -1 : 15 + ii; j = (e / 19) % 19 - 1; k = e % 19 - 1;
+    } else if (e < 1995) {
+        e -= 1083;
+        int jj = (e / 19) % 3;
+        i = e / 57; j = jj == 0 ? -1 : 15 + jj; k = e % 19 - 1;
+    } else {
+        e -= 1995;
+        int kk = e % 3;
+        i = e / 48; j = (e / 3) % 16; k = kk == 0 ? -1 : 15 + kk;
+    }
+}
+
+BH_HD inline void update_shell_item(const KP& kp, const Pool& P, int p, int e) {
+    int i, j, k;
+    shell_ijk(e, i, j, k);
+    double B[3], sg;
+    f2cb_cell(kp, P, p, i, j, k, B, sg);
+    int l = lindx(i, j, k);
+    for (int d = 0; d < 3; d++) { Wv(P, p, 5 + d)[l] = B[d]; Uv(P, p, 5 + d)[l] = sg * B[d]; }
 }
 
 // ---- ghost fill: amrtree::ghosts (grid.cpp:390-571) ---------------------
@@ -426,31 +471,46 @@ BH_HD inline void strip_ijk(int dim, int pos, int t1, int t2, int& i, int& j, in
     else { i = t1; j = t2; k = pos; }
 }
 
-BH_HD inline void ghost_fill_item(const KP& kp, const Pool& P, int p, int e) {
-    int s = e / 512, rem = e % 512;
-    int gg = rem / 256, t1 = (rem / 16) % 16, t2 = rem % 16;
+// ghost-strip copy (gh_copy :390-425, gh_bndy :494-522), one double per
+// item: item e of patch p is array a = e / N_STRIP (U components 0-7, W
+// components 8-15) of strip cell e % N_STRIP.  The cells of a slot are
+// ordered so that neighbouring items are neighbours in memory (k fastest;
+// for the k-strips of dim 2 the two layers gg first).  The 128 items of a
+// CTA share one array and one slot, so the neighbour kind is uniform.
+BH_HD inline void ghost_copy_item(const Pool& P, int p, int e) {
+    int a = e / N_STRIP, c = e % N_STRIP;
+    int s = c / 512, rem = c % 512;
     int dim = s / 2, side = (s & 1) ? 1 : -1;
     int nb = P.nbr[(p * 6 + s) * 2], kind = P.nbr[(p * 6 + s) * 2 + 1];
-    int pstart = side == 1 ? BLK : -GH;
-    int gi, gj, gk;
-    strip_ijk(dim, pstart + gg, t1, t2, gi, gj, gk);
-    int lg = lindx(gi, gj, gk);
-    if (kind == BH_NB_COPY || kind == BH_NB_BNDY) {
-        int src_p, ai, aj, ak;
-        if (kind == BH_NB_COPY) {                   // gh_copy :390-425
-            src_p = nb;
-            strip_ijk(dim, (side == 1 ? 0 : BLK - GH) + gg, t1, t2, ai, aj, ak);
-        } else {                                    // gh_bndy :494-522
-            src_p = p;
-            strip_ijk(dim, side == 1 ? BLK - 1 - gg : gg, t1, t2, ai, aj, ak);
-        }
-        int la = lindx(ai, aj, ak);
-        for (int v = 0; v < 8; v++) {
-            Uv(P, p, v)[lg] = Uv(P, src_p, v)[la];
-            Wv(P, p, v)[lg] = Wv(P, src_p, v)[la];
-        }
-        return;
+    if (kind != BH_NB_COPY && kind != BH_NB_BNDY) return;
+    int gg, t1, t2;
+    if (dim == 2) { gg = rem & 1; t2 = (rem >> 1) & 15; t1 = rem >> 5; }
+    else { gg = rem >> 8; t1 = (rem >> 4) & 15; t2 = rem & 15; }
+    int gi, gj, gk, ai, aj, ak, src_p;
+    strip_ijk(dim, (side == 1 ? BLK : -GH) + gg, t1, t2, gi, gj, gk);
+    if (kind == BH_NB_COPY) {
+        src_p = nb;
+        strip_ijk(dim, (side == 1 ? 0 : BLK - GH) + gg, t1, t2, ai, aj, ak);
+    } else {
+        src_p = p;
+        strip_ijk(dim, side == 1 ? BLK - 1 - gg : gg, t1, t2, ai, aj, ak);
     }
+    double* dst = a < 8 ? Uv(P, p, a) : Wv(P, p, a - 8);
+    const double* src = a < 8 ? Uv(P, src_p, a) : Wv(P, src_p, a - 8);
+    dst[lindx(gi, gj, gk)] = src[lindx(ai, aj, ak)];
+}
+
+// ghost-strip prolongation from a coarser neighbour, strip cell e of patch p
+// in [0, N_STRIP) (cells of other neighbour kinds are left to ghost_copy_item)
+BH_HD inline void ghost_prolong_item(const KP& kp, const Pool& P, int p, int e) {
+    int s = e / 512, rem = e % 512;
+    int nb = P.nbr[(p * 6 + s) * 2], kind = P.nbr[(p * 6 + s) * 2 + 1];
+    if (kind != BH_NB_PROLONG) return;
+    int gg = rem / 256, t1 = (rem / 16) % 16, t2 = rem % 16;
+    int dim = s / 2, side = (s & 1) ? 1 : -1;
+    int gi, gj, gk;
+    strip_ijk(dim, (side == 1 ? BLK : -GH) + gg, t1, t2, gi, gj, gk);
+    int lg = lindx(gi, gj, gk);
     // gh_prolong (:427-492): minmod-limited interpolation from the coarse patch
     int ci = (dim == 0) ? gg / 2 : t1 / 2;
     int cj = (dim == 1) ? gg / 2 : (dim == 0 ? t1 / 2 : t2 / 2);

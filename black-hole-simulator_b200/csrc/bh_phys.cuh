@@ -135,13 +135,15 @@ BH_HD inline void met_comp(const MP& m, double r, double th, Met& o) {
     o.sqrtdetgam = o.alpha * o.sqrtdetg;                    // :117-119
 }
 
-// Full metric for the geometric source: g, g_inv and the Christoffel
-// symbols (christ, :57-90) built from the eight distinct derivatives.
-struct MetFull {
-    double g[4][4], gi[4][4], G[4][4][4];
+// Metric for the geometric source: g, g_inv, lapse, shift, sqrt(-g) and the
+// metric derivatives d[l][m][n] = d_l g_mn (christ, :57-90) from which
+// each Christoffel symbol is formed on demand (christoffel below), so that
+// a caller never holds all 64 of them at once.
+struct MetSrc {
+    double g[4][4], gi[4][4], d[4][4][4];
     double alpha, beta[3], sqrtdetg;
 };
-BH_HD inline void met_full(const MP& m, double r, double th, MetFull& o) {
+BH_HD inline void met_src(const MP& m, double r, double th, MetSrc& o) {
     Trig t = trig(th);
     const double M = m.M, a = m.a, Q = m.Q;
     double Sig = Sigma_(m, r, t);
@@ -164,13 +166,12 @@ BH_HD inline void met_full(const MP& m, double r, double th, MetFull& o) {
     o.sqrtdetg = (r * r + a * a * s2) * t.s;
     o.alpha = pow_mhalf(1 + H);
     for (int i = 0; i < 3; i++) o.beta[i] = -o.gi[0][i + 1] / o.gi[0][0];
-    // metric derivatives d[l][m][n] = d_l g_mn (:72-80)
+    // metric derivatives (:72-80)
     double sig = r * r + a * a * c2;
     double isig = pow_m1(sig), isig2 = pow_m2(sig);
-    double d[4][4][4];
     for (int i = 0; i < 4; i++)
         for (int j = 0; j < 4; j++)
-            for (int k = 0; k < 4; k++) d[i][j][k] = 0;
+            for (int k = 0; k < 4; k++) o.d[i][j][k] = 0;
     double A1 = -2 * (M * r * r - Q * Q * r - M * a * a * c2) * isig2;
     double A2 = 2 * a * a * (2 * M * r - Q * Q) * t.c * t.s * isig;
     double A3 = 2 * a * a * s2 * (M * r * r - Q * Q * r - M * a * a * c2) * isig2;
@@ -179,24 +180,41 @@ BH_HD inline void met_full(const MP& m, double r, double th, MetFull& o) {
     double A6 = s2 * (((2 * pow_4(a) * (2 * M * r - Q * Q) * t.c * pow_3(t.s)) * isig2) +
                       ((2 * a * a * (2 * M * r - Q * Q) * t.c * t.s) * isig)) +
                 t.c * t.s * (((a * a * s2 * (2 * M * r - Q * Q)) * isig) + r * r + a * a);
-    d[1][0][0] = d[1][0][1] = d[1][1][0] = d[1][1][1] = A1;
-    d[2][0][0] = d[2][0][1] = d[2][1][0] = d[2][1][1] = A2;
-    d[1][2][2] = 2 * r;
-    d[2][2][2] = -a * a * t.c * t.s;
-    d[1][0][3] = d[1][3][0] = d[1][1][3] = d[1][3][1] = A3;
-    d[2][0][3] = d[2][3][0] = d[2][1][3] = d[2][3][1] = A4;
-    d[1][3][3] = A5;
-    d[2][3][3] = A6;
+    o.d[1][0][0] = o.d[1][0][1] = o.d[1][1][0] = o.d[1][1][1] = A1;
+    o.d[2][0][0] = o.d[2][0][1] = o.d[2][1][0] = o.d[2][1][1] = A2;
+    o.d[1][2][2] = 2 * r;
+    o.d[2][2][2] = -a * a * t.c * t.s;
+    o.d[1][0][3] = o.d[1][3][0] = o.d[1][1][3] = o.d[1][3][1] = A3;
+    o.d[2][0][3] = o.d[2][3][0] = o.d[2][1][3] = o.d[2][3][1] = A4;
+    o.d[1][3][3] = A5;
+    o.d[2][3][3] = A6;
+}
+// Christoffel symbol Gamma^l_{mm n} (christ, :81-90)
+BH_HD inline double christoffel(const MetSrc& o, int l, int mm, int n) {
+    return 0.5 * (o.gi[l][0] * (o.d[mm][0][n] + o.d[n][0][mm] - o.d[0][mm][n]) +
+                  o.gi[l][1] * (o.d[mm][1][n] + o.d[n][1][mm] - o.d[1][mm][n]) +
+                  o.gi[l][2] * (o.d[mm][2][n] + o.d[n][2][mm] - o.d[2][mm][n]) +
+                  o.gi[l][3] * (o.d[mm][3][n] + o.d[n][3][mm] - o.d[3][mm][n]));
+}
+
+// Full metric with every Christoffel symbol (the batched metric::comp)
+struct MetFull {
+    double g[4][4], gi[4][4], G[4][4][4];
+    double alpha, beta[3], sqrtdetg;
+};
+BH_HD inline void met_full(const MP& m, double r, double th, MetFull& o) {
+    MetSrc s;
+    met_src(m, r, th, s);
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) { o.g[i][j] = s.g[i][j]; o.gi[i][j] = s.gi[i][j]; }
+    o.alpha = s.alpha; o.sqrtdetg = s.sqrtdetg;
+    for (int i = 0; i < 3; i++) o.beta[i] = s.beta[i];
 #pragma unroll
     for (int l = 0; l < 4; l++)
 #pragma unroll
         for (int mm = 0; mm < 4; mm++)
 #pragma unroll
-            for (int n = 0; n < 4; n++)
-                o.G[l][mm][n] = 0.5 * (o.gi[l][0] * (d[mm][0][n] + d[n][0][mm] - d[0][mm][n]) +
-                                       o.gi[l][1] * (d[mm][1][n] + d[n][1][mm] - d[1][mm][n]) +
-                                       o.gi[l][2] * (d[mm][2][n] + d[n][2][mm] - d[2][mm][n]) +
-                                       o.gi[l][3] * (d[mm][3][n] + d[n][3][mm] - d[3][mm][n]));
+            for (int n = 0; n < 4; n++) o.G[l][mm][n] = christoffel(s, l, mm, n);
 }
 
 // ======================================================================

@@ -2,7 +2,7 @@
 // per arithmetic variant: the including file defines BH_VARIANT (the
 // namespace) and is compiled with the variant's flags (bh_fp64.cu with
 // --fmad=false, the reference's separate roundings; bh_fp64fma.cu with
-// FMA contraction).  bh_abi.cu dispatches the C ABI to one of them.
+// FMA contraction; bh_mixed.cu with BH_REAL = float).  bh_abi.cu dispatches the C ABI to one of them.
 //
 // One thread per cell / face / edge; patches are the unit of parallel work
 // (blockIdx.y walks a patch list, blockIdx.x the items of one patch), so a
@@ -31,8 +31,8 @@ namespace {
 constexpr int TPB = 128;
 // minimum resident CTAs per SM requested from ptxas for the heavy kernels
 // (caps their registers per thread); tuned on B200
-// (a sweep of 1..6 on the 128^3 box: con2prim and floors run fastest at 6
-// CTAs of 128 threads per SM, the flux kernel at 5, the update at 3)
+// (sweeps on the 128^3 box: con2prim and floors run fastest at 6 CTAs of
+// 128 threads per SM, the flux kernel at 5, the update at 4)
 #ifndef BH_MINB_PRIMS
 #define BH_MINB_PRIMS 6
 #endif
@@ -43,7 +43,7 @@ constexpr int TPB = 128;
 #define BH_MINB_FLOORS 6
 #endif
 #ifndef BH_MINB_UPDATE
-#define BH_MINB_UPDATE 3
+#define BH_MINB_UPDATE 4
 #endif
 
 // ---- thin kernels: thread index -> item --------------------------------
@@ -79,10 +79,25 @@ __global__ void k_f2cb(KP kp, Pool P, const int32_t* list) { ITEM(N_F2C); f2cb_i
 __global__ void k_div_source(KP kp, Pool P, const int32_t* list, double* dv, double* sv) {
     ITEM(N_INT); div_source_item<BH_REAL>(kp, P, list[blockIdx.y], e, dv, sv);
 }
+// f2cB + RK update: CTAs [0, UPD_INT) take the interior cells, the others
+// the shell cells, so no warp mixes the two
+constexpr int UPD_INT = N_INT / TPB;
+constexpr int UPD_BLOCKS = UPD_INT + (N_SHELL + TPB - 1) / TPB;
 __global__ void __launch_bounds__(TPB, BH_MINB_UPDATE) k_update(KP kp, Pool P, const int32_t* list, const double* dtp, int stage) {
-    ITEM(N_F2C); update_item<BH_REAL>(kp, P, list[blockIdx.y], e, *dtp, stage);
+    int p = list[blockIdx.y];
+    if ((int)blockIdx.x < UPD_INT) {
+        update_interior_item<BH_REAL>(kp, P, p, blockIdx.x * TPB + threadIdx.x, *dtp, stage);
+    } else {
+        int e = (blockIdx.x - UPD_INT) * TPB + threadIdx.x;
+        if (e < N_SHELL) update_shell_item(kp, P, p, e);
+    }
 }
-__global__ void k_ghost_fill(KP kp, Pool P, const int32_t* list) { ITEM(N_STRIP); ghost_fill_item(kp, P, list[blockIdx.y], e); }
+// amrtree::ghosts strip fill: one copied double per thread, then the
+// prolonged cells (CTAs whose slot has another neighbour kind exit at once)
+__global__ void k_ghost_copy(Pool P, const int32_t* list) { ITEM(16 * N_STRIP); ghost_copy_item(P, list[blockIdx.y], e); }
+__global__ void k_ghost_prolong(KP kp, Pool P, const int32_t* list) {
+    ITEM(N_STRIP); ghost_prolong_item(kp, P, list[blockIdx.y], e);
+}
 __global__ void k_ghost_ctop(KP kp, Pool P, const int32_t* list) { ITEM(NC); ghost_ctop_item(kp, P, list[blockIdx.y], e); }
 __global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_prims(KP kp, Pool P, const int32_t* list, int ghost_first) {
     ITEM(NC); prims_item(kp, P, list[blockIdx.y], e, ghost_first);
@@ -219,7 +234,8 @@ int div_source(const bh_params* P, const bh_pool* pool, double* div, double* src
 int ghosts(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
     if (!P || bad_pool(pool) || n < 0 || (n > 0 && !patches)) return BH_EINVAL;
     if (n == 0) return BH_OK;
-    k_ghost_fill<<<grid2(N_STRIP, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
+    k_ghost_copy<<<grid2(16 * N_STRIP, n), TPB, 0, S(stream)>>>(pool_of(pool), patches);
+    k_ghost_prolong<<<grid2(N_STRIP, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
     k_ghost_ctop<<<grid2(NC, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
     return launched();
 }
@@ -236,7 +252,8 @@ int ghosts_prims_status(const bh_params* P, const bh_pool* pool, uint8_t* status
     if (pool->nleaf == 0) return BH_OK;
     Pool pv = pool_of(pool);
     pv.status = status;
-    k_ghost_fill<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
+    k_ghost_copy<<<grid2(16 * N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(pv, pool->leaves);
+    k_ghost_prolong<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
     if (status && pool->leafmask) {
         k_prims_interior<<<grid2(N_INT, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
         k_prims_ghost<<<grid2(N_GHOST, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
@@ -250,7 +267,8 @@ int ghosts_prims(const bh_params* P, const bh_pool* pool, void* stream) {
 }
 int update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, void* stream) {
     if (!P || bad_pool(pool) || !dt_dev || (stage != 0 && stage != 1)) return BH_EINVAL;
-    k_update<<<grid2(N_F2C, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, dt_dev, stage);
+    k_update<<<dim3(UPD_BLOCKS, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, dt_dev,
+                                                                    stage);
     return launched();
 }
 int floors(const bh_params* P, const bh_pool* pool, void* stream) {

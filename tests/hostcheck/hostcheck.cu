@@ -78,7 +78,9 @@ void hc_div_source(const bh_params* Pp, const bh_pool* pool, double* dv, double*
 void hc_ghosts(const bh_params* Pp, const bh_pool* pool, const int32_t* list, int n) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < n; i++)
-        for (int e = 0; e < N_STRIP; e++) ghost_fill_item(k, P, list[i], e);
+        for (int e = 0; e < 16 * N_STRIP; e++) ghost_copy_item(P, list[i], e);
+    for (int i = 0; i < n; i++)
+        for (int e = 0; e < N_STRIP; e++) ghost_prolong_item(k, P, list[i], e);
     for (int i = 0; i < n; i++)
         for (int l = 0; l < NC; l++) ghost_ctop_item(k, P, list[i], l);
 }
@@ -90,7 +92,9 @@ void hc_prims(const bh_params* Pp, const bh_pool* pool, int ghost_first) {
 void hc_ghosts_prims(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < pool->nleaf; i++)
-        for (int e = 0; e < N_STRIP; e++) ghost_fill_item(k, P, pool->leaves[i], e);
+        for (int e = 0; e < 16 * N_STRIP; e++) ghost_copy_item(P, pool->leaves[i], e);
+    for (int i = 0; i < pool->nleaf; i++)
+        for (int e = 0; e < N_STRIP; e++) ghost_prolong_item(k, P, pool->leaves[i], e);
     if (pool->status && pool->leafmask) {
         for (int i = 0; i < pool->nleaf; i++)
             for (int c = 0; c < N_INT; c++) prims_interior_item(k, P, pool->leaves[i], c);
@@ -103,7 +107,9 @@ void hc_ghosts_prims(const bh_params* Pp, const bh_pool* pool) {
 void hc_update(const bh_params* Pp, const bh_pool* pool, double dt, int stage) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < pool->npatch; i++)
-        for (int e = 0; e < N_F2C; e++) update_item<double>(k, P, pool->all[i], e, dt, stage);
+        for (int c = 0; c < N_INT; c++) update_interior_item<double>(k, P, pool->all[i], c, dt, stage);
+    for (int i = 0; i < pool->npatch; i++)
+        for (int e = 0; e < N_SHELL; e++) update_shell_item(k, P, pool->all[i], e);
 }
 void hc_floors(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
