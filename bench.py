@@ -24,9 +24,12 @@ copy inside the timed region), so every step does the same work.
 value : zone-updates/s, inputs resident in HBM, device-timed with CUDA
         events, max over ranks.  N > 1 runs one independent box per GPU
         (weak scaling, no data-path collective).
-e2e   : same metric through the public API with host buffers: per step the
-        H2D copy of the state (U, W, Bf) from pinned memory, the step, and
-        the D2H copy of the new state.
+e2e   : same metric through the public API with host buffers
+        (bhgpu.HostPipeline): per step the H2D copy of the state (U, W, Bf)
+        from pinned memory, the step, and the D2H copy of the new state,
+        with consecutive steps on three device trees so that the copies of
+        neighbouring steps overlap the step; the one-tree (serial) figure
+        is reported beside it.
 roofline : the flux kernel (k_flux, the largest share of the step),
         algorithmic bytes per launch / its CUDA-event duration inside the
         timed region, against the measured HBM copy bandwidth.
@@ -61,7 +64,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--grid", type=int, default=128, choices=[64, 128])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--con2prim-batch", type=int, default=1, help="also measure the 2^24-cell con2prim batch")
     ap.add_argument("--precision", default="fp64-fma", choices=["fp64", "fp64-fma", "mixed"],
                     help="arithmetic variant of the headline value; the other variants are timed beside it")
@@ -157,6 +160,7 @@ def alg_bytes(call, npatch):
     return per[call] * npatch
 
 
+E2E_DEPTH = 3      # device trees of the end-to-end pipeline
 STEP_BYTES = 296   # algorithmic HBM bytes per zone-update of a whole RK2 step
 
 # DRAM bytes (read + write) per launch from ncu captures of this workload,
@@ -459,30 +463,40 @@ def run_ours(args):
             variants[prec]["accuracy_vs_fp64"] = acc
 
     # ---- end to end through the public API with host buffers --------------
+    # bhgpu.HostPipeline over E2E_DEPTH device trees: every step uploads the
+    # state from pinned host memory, steps it and downloads the result; the
+    # upload of step n+1 and the download of step n-1 overlap the step n.
+    # The same API with one tree (each upload waits for the previous
+    # download) is timed beside it as the serial figure.
     pin = lambda x: x.cpu().pin_memory()
     hU, hW, hB = pin(U0), pin(W0), pin(B0)
-    oU, oW, oB = torch.empty_like(hU).pin_memory(), torch.empty_like(hW).pin_memory(), torch.empty_like(hB).pin_memory()
     rk = bhgpu.RK2Integrator(CFL)
+    trees = [tree] + [make_tree(nq, seed=1, precision=args.precision) for _ in range(E2E_DEPTH - 1)]
+    outs = [tuple(torch.empty_like(x).pin_memory() for x in (hU, hW, hB)) for _ in range(E2E_DEPTH)]
 
-    def e2e_step():
-        tree.U.copy_(hU, non_blocking=True); tree.W.copy_(hW, non_blocking=True); tree.Bf.copy_(hB, non_blocking=True)
-        rk.step(tree, sync=False, check_domain=False)
-        oU.copy_(tree.U, non_blocking=True); oW.copy_(tree.W, non_blocking=True); oB.copy_(tree.Bf, non_blocking=True)
+    def e2e_run(pipe, nstep):
+        for i in range(len(pipe.trees)):          # warm-up: every tree once
+            pipe.submit(hU, hW, hB, *outs[i])
+        pipe.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+        a.record(pipe.s_in)
+        for i in range(nstep):
+            pipe.submit(hU, hW, hB, *outs[i % len(pipe.trees)])
+        b.record(pipe.s_out)
+        torch.cuda.synchronize()
+        te = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        return float(te.item()) / nstep
 
-    e2e_step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(args.e2e_steps):
-        e2e_step()
-    b.record()
-    torch.cuda.synchronize()
-    te = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_ms = float(te.item()) / args.e2e_steps
+    e2e_ms = e2e_run(bhgpu.HostPipeline(trees, rk), args.e2e_steps)
+    e2e_serial_ms = e2e_run(bhgpu.HostPipeline(trees[:1], rk), max(3, args.e2e_steps // 3))
+    for t_ in trees:
+        t_.clear_error()
+    del trees
     h2d = (hU.numel() + hW.numel() + hB.numel()) * 8
     d2h = h2d
 
@@ -508,7 +522,9 @@ def run_ours(args):
                        "l2": "working set > L2 (inputs and outputs larger than 126 MB)",
                        "restart": "each step restarts from the seeded state (D2D copy inside the timed region)"},
             "e2e": {"value": world * zones / (e2e_ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                    "api": f"bhgpu.HostPipeline, {E2E_DEPTH} device trees, pinned host U/W/Bf in and out every step",
+                    "serial_value": world * zones / (e2e_serial_ms / 1e3), "serial_ms_per_step": e2e_serial_ms},
             "gpu_launches": KL_PER_STEP * args.steps,
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": TRAFFIC.get((top, args.grid)), "peak_source": peak_kind,
