@@ -373,8 +373,8 @@ def run_ours(args):
     dtp = _p(tree.dt)
     ev = {k: [] for k in ("ghosts_prims", "fluxcomp", "update", "floors")}
     # my kernels per step: dt_init, dtcomp, 2 x (ghost_copy, ghost_prolong,
-    # prims_interior, prims_ghost, flux, emf, bfupdate, update), floors
-    KL_PER_STEP = 19
+    # prims_interior, prims_ghost, aux, flux, emf, bfupdate, update), floors
+    KL_PER_STEP = 21
 
     def timed(name, record, fn):
         if record:

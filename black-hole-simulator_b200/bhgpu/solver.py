@@ -197,6 +197,8 @@ class AmrTree:
         self.leafmask = torch.as_tensor(np.ascontiguousarray(T["leaf"], np.uint8), device=d)
         # scratch: con2prim outcome of every interior cell in the current stage
         self.status = torch.zeros((n, NC), dtype=torch.uint8, device=d)
+        # scratch of the flux computation: per-cell logarithms and metric
+        self.aux = torch.zeros((n, 6, NC), dtype=f64, device=d)
         waves = self.quilt.ghost_waves(T["nbr"], T["leaf"])
         self.nwave = len(waves)
         off = np.zeros(self.nwave + 1, np.int32)
@@ -207,7 +209,7 @@ class AmrTree:
         self.dt = torch.zeros(1, dtype=f64, device=d)
         self.pool = BhPool(n, _p(self.U), _p(self.W), _p(self.dU), _p(self.F), _p(self.Bf), _p(self.EMF),
                            _p(self.rth), _p(self.pgeo), _p(self.nbr), _p(self.all), _p(self.leaves),
-                           len(leaves), _p(self.err), _p(self.leafmask), _p(self.status))
+                           len(leaves), _p(self.err), _p(self.leafmask), _p(self.status), _p(self.aux))
         check(lib.bh_geometry(C.byref(self.pool), _stream()), "patch::cell_init")
 
     def params(self, maxiter=500, tol=1e-10) -> BhParams:
@@ -388,7 +390,7 @@ class RK2Integrator:
 class StepGraph:
     """rk2integrator::step recorded once into a CUDA graph and replayed.
 
-    The step's 19 launches (dtcomp, two stages, floors) read dt from device
+    The step's 21 launches (dtcomp, two stages, floors) read dt from device
     memory and never synchronise with the host, so the whole step is one
     graph; ``before`` (optional) is recorded in front of it, e.g. a copy
     that resets the state.  Replays run on the current stream.  The domain

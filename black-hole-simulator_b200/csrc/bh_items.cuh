@@ -30,9 +30,10 @@ struct Pool {               // kernel-side view of bh_pool
     int32_t* err;
     const uint8_t* leafmask;
     uint8_t* status;
+    double* aux;
 };
 inline Pool pool_of(const bh_pool* p) {
-    return Pool{p->U, p->W, p->dU, p->F, p->Bf, p->EMF, p->rth, p->pgeo, p->nbr, p->err, p->leafmask, p->status};
+    return Pool{p->U, p->W, p->dU, p->F, p->Bf, p->EMF, p->rth, p->pgeo, p->nbr, p->err, p->leafmask, p->status, p->aux};
 }
 
 BH_HD inline double* Uv(const Pool& P, int p, int v) { return P.U + ((size_t)p * 8 + v) * NC; }
@@ -159,30 +160,75 @@ BH_HD inline void face_ijk(int dim, int f, int& i, int& j, int& k) {
     else { i = f / (16 * 17); j = (f / 17) % 16; k = f % 17 - 1; }
 }
 
+// per-cell inputs of reconfp, computed once per cell ahead of the face loop
+// (each cell is read by up to 12 faces): log rho and log eps, in RT and
+// stored widened to FP64, and the entries of the cell's spatial metric that
+// causalv reads -- gam00, gam02 (= gam20), gam11, gam22; the other entries
+// are metric::comp's structural zeros
+constexpr int NAUX = 6;
+template <typename RT>
+BH_HD inline void aux_item(const KP& kp, const Pool& P, int p, int l) {
+    double* a = P.aux + (size_t)p * NAUX * NC;
+    a[l] = double(log(RT(Wv(P, p, 0)[l])));
+    a[NC + l] = double(log(RT(Wv(P, p, 1)[l])));
+    Met m;
+    met_comp(kp.cell, rr(P, p, l), tt(P, p, l), m);
+    a[2 * NC + l] = m.gam[0][0];
+    a[3 * NC + l] = m.gam[0][2];
+    a[4 * NC + l] = m.gam[1][1];
+    a[5 * NC + l] = m.gam[2][2];
+}
+template <typename RT>
+BH_HD inline void aux_gam(const Pool& P, int p, int l, RT g[3][3]) {
+    const double* a = P.aux + (size_t)p * NAUX * NC + 2 * NC;
+    g[0][0] = RT(a[l]);          g[0][1] = RT(0.0);           g[0][2] = RT(a[NC + l]);
+    g[1][0] = RT(0.0);           g[1][1] = RT(a[2 * NC + l]); g[1][2] = RT(0.0);
+    g[2][0] = RT(a[NC + l]);     g[2][1] = RT(0.0);           g[2][2] = RT(a[3 * NC + l]);
+}
+
 // reconfp (reconstruction.cpp:40-97) for the face between cells (i,j,k)
 // and (i,j,k)+e_dim of patch p, computed in RT (the stored primitives and
-// the cell metric are FP64 and rounded to RT)
-template <typename RT>
+// the cell metric are FP64 and rounded to RT).  AUX reads the logarithms and
+// the cell metric from the per-cell scratch (aux_item) instead of computing
+// them here; the values are the same.
+template <typename RT, bool AUX = false>
 BH_HD inline void reconfp(const KP& kp, const Pool& P, int p, int i, int j, int k, int dim, int lim, PrimT<RT>& L,
                           PrimT<RT>& R) {
     int di = dim == 0, dj = dim == 1, dk = dim == 2;
     int lm = lindx(i - di, j - dj, k - dk), lc = lindx(i, j, k);
     int lp = lindx(i + di, j + dj, k + dk), lpp = lindx(i + 2 * di, j + 2 * dj, k + 2 * dk);
-    const double* Wr = Wv(P, p, 0);
-    recon_scal(log(RT(Wr[lm])), log(RT(Wr[lc])), log(RT(Wr[lp])), log(RT(Wr[lpp])), lim, L.rho, R.rho);
-    L.rho = exp(L.rho); R.rho = exp(R.rho);
-    const double* We = Wv(P, p, 1);
-    recon_scal(log(RT(We[lm])), log(RT(We[lc])), log(RT(We[lp])), log(RT(We[lpp])), lim, L.eps, R.eps);
-    L.eps = exp(L.eps); R.eps = exp(R.eps);
+    if (AUX) {
+        const double* lr = P.aux + (size_t)p * NAUX * NC;
+        const double* le = lr + NC;
+        recon_scal(RT(lr[lm]), RT(lr[lc]), RT(lr[lp]), RT(lr[lpp]), lim, L.rho, R.rho);
+        L.rho = exp(L.rho); R.rho = exp(R.rho);
+        recon_scal(RT(le[lm]), RT(le[lc]), RT(le[lp]), RT(le[lpp]), lim, L.eps, R.eps);
+        L.eps = exp(L.eps); R.eps = exp(R.eps);
+    } else {
+        const double* Wr = Wv(P, p, 0);
+        recon_scal(log(RT(Wr[lm])), log(RT(Wr[lc])), log(RT(Wr[lp])), log(RT(Wr[lpp])), lim, L.rho, R.rho);
+        L.rho = exp(L.rho); R.rho = exp(R.rho);
+        const double* We = Wv(P, p, 1);
+        recon_scal(log(RT(We[lm])), log(RT(We[lc])), log(RT(We[lp])), log(RT(We[lpp])), lim, L.eps, R.eps);
+        L.eps = exp(L.eps); R.eps = exp(R.eps);
+    }
     for (int d = 0; d < 3; d++) {
         const double* x = Wv(P, p, 2 + d);
         recon_scal(RT(x[lm]), RT(x[lc]), RT(x[lp]), RT(x[lpp]), lim, L.v[d], R.v[d]);
     }
-    Met mL, mR;
-    met_comp(kp.cell, rr(P, p, lc), tt(P, p, lc), mL);
-    met_comp(kp.cell, rr(P, p, lp), tt(P, p, lp), mR);
-    causalv(L.v, met_cast<RT>(mL));
-    causalv(R.v, met_cast<RT>(mR));
+    if (AUX) {
+        RT gL[3][3], gR[3][3];
+        aux_gam(P, p, lc, gL);
+        aux_gam(P, p, lp, gR);
+        causalv_gam(L.v, gL);
+        causalv_gam(R.v, gR);
+    } else {
+        Met mL, mR;
+        met_comp(kp.cell, rr(P, p, lc), tt(P, p, lc), mL);
+        met_comp(kp.cell, rr(P, p, lp), tt(P, p, lp), mR);
+        causalv(L.v, met_cast<RT>(mL));
+        causalv(R.v, met_cast<RT>(mR));
+    }
     for (int d = 0; d < 3; d++) {
         const double* x = Wv(P, p, 5 + d);
         if (d == dim) { L.B[d] = RT(x[lc]); R.B[d] = RT(x[lp]); }
@@ -207,12 +253,12 @@ BH_HD inline void reconfp_item(const KP& kp, const Pool& P, int p, int dim, int 
 
 // one face of patch::fluxcomp (grid.cpp:255-329): reconstruction, face
 // ptoc and HLLD in RT; face metric evaluated in FP64; flux stored in FP64
-template <typename RT>
+template <typename RT, bool AUX = false>
 BH_HD inline void flux_item(const KP& kp, const Pool& P, int p, int dim, int f) {
     int i, j, k;
     face_ijk(dim, f, i, j, k);
     PrimT<RT> L, R;
-    reconfp<RT>(kp, P, p, i, j, k, dim, kp.limiter, L, R);
+    reconfp<RT, AUX>(kp, P, p, i, j, k, dim, kp.limiter, L, R);
     double bn;
     int fi;
     if (dim == 0) { bn = Bfv(P, p, 0)[xfc(i + 1, j, k)]; fi = xfc(i, j, k); }
@@ -471,12 +517,13 @@ BH_HD inline void strip_ijk(int dim, int pos, int t1, int t2, int& i, int& j, in
     else { i = t1; j = t2; k = pos; }
 }
 
-// ghost-strip copy (gh_copy :390-425, gh_bndy :494-522), one double per
-// item: item e of patch p is array a = e / N_STRIP (U components 0-7, W
-// components 8-15) of strip cell e % N_STRIP.  The cells of a slot are
-// ordered so that neighbouring items are neighbours in memory (k fastest;
-// for the k-strips of dim 2 the two layers gg first).  The 128 items of a
-// CTA share one array and one slot, so the neighbour kind is uniform.
+// ghost-strip copy (gh_copy :390-425, gh_bndy :494-522) of one state
+// vector: item e of patch p copies U (a = 0) or W (a = 1), a = e / N_STRIP,
+// of strip cell e % N_STRIP -- eight independent loads, then eight stores.
+// The cells of a slot are ordered so that neighbouring items are neighbours
+// in memory (k fastest; for the k-strips of dim 2 the two layers gg first).
+// The 128 items of a CTA share one array and one slot, so the neighbour
+// kind is uniform.
 BH_HD inline void ghost_copy_item(const Pool& P, int p, int e) {
     int a = e / N_STRIP, c = e % N_STRIP;
     int s = c / 512, rem = c % 512;
@@ -495,9 +542,14 @@ BH_HD inline void ghost_copy_item(const Pool& P, int p, int e) {
         src_p = p;
         strip_ijk(dim, side == 1 ? BLK - 1 - gg : gg, t1, t2, ai, aj, ak);
     }
-    double* dst = a < 8 ? Uv(P, p, a) : Wv(P, p, a - 8);
-    const double* src = a < 8 ? Uv(P, src_p, a) : Wv(P, src_p, a - 8);
-    dst[lindx(gi, gj, gk)] = src[lindx(ai, aj, ak)];
+    double* dst = a == 0 ? Uv(P, p, 0) : Wv(P, p, 0);
+    const double* src = a == 0 ? Uv(P, src_p, 0) : Wv(P, src_p, 0);
+    int lg = lindx(gi, gj, gk), la = lindx(ai, aj, ak);
+    double x[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) x[v] = src[(size_t)v * NC + la];
+#pragma unroll
+    for (int v = 0; v < 8; v++) dst[(size_t)v * NC + lg] = x[v];
 }
 
 // ghost-strip prolongation from a coarser neighbour, strip cell e of patch p
@@ -619,8 +671,10 @@ BH_HD inline void prims_interior_item(const KP& kp, const Pool& P, int p, int c)
 }
 
 // the two con2prim passes of a ghost cell: amrtree::ghosts' ctop with its
-// fallback, then (only if that changed U) rkstg's ctop with its fallback
-BH_HD inline void ghost_two_pass(const KP& kp, const Pool& P, int p, int l) {
+// fallback, then (only if that changed U) rkstg's ctop with its fallback.
+// first_fails: the first ctop is known to fail (it already failed on the
+// same U at the same position), so the cell starts at its fallback.
+BH_HD inline void ghost_two_pass(const KP& kp, const Pool& P, int p, int l, bool first_fails = false) {
     Cons u;
     load_cons(P, p, l, u);
     Prim w;
@@ -632,7 +686,7 @@ BH_HD inline void ghost_two_pass(const KP& kp, const Pool& P, int p, int l) {
     for (int pass = 0; pass < 2; pass++) {
         Prim pv;
         bool dom = false;
-        int ok = ctop(kp.gamma, kp.maxiter, kp.tol, mc, u, pv, dom);
+        int ok = (pass == 0 && first_fails) ? 0 : ctop(kp.gamma, kp.maxiter, kp.tol, mc, u, pv, dom);
         if (dom) flag(P.err, BH_ERR_DOMAIN);
         if (ok) { w = pv; break; }
         pvfs(r, w.rho, w.eps);
@@ -665,13 +719,21 @@ BH_HD inline void prims_ghost_item(const KP& kp, const Pool& P, int p, int e) {
         if (kind == BH_NB_COPY) strip_ijk(dim, (side == 1 ? 0 : BLK - GH) + gg, t1, t2, ai, aj, ak);
         else strip_ijk(dim, side == 1 ? BLK - 1 - gg : gg, t1, t2, ai, aj, ak);
         int la = lindx(ai, aj, ak);
-        // same U and the same (r, theta) bit for bit as the source, whose
-        // ctop succeeded: the same primitives (not so across a periodic
-        // wrap or an outflow copy, where the ghost sits elsewhere)
-        if (P.leafmask[src_p] && P.status[(size_t)src_p * NC + la] == 1 && rr(P, p, lg) == rr(P, src_p, la) &&
-            tt(P, p, lg) == tt(P, src_p, la)) {
-            for (int v = 0; v < 8; v++) Wv(P, p, v)[lg] = Wv(P, src_p, v)[la];
-            return;
+        // same U and the same (r, theta) bit for bit as the source (not so
+        // across a periodic wrap or an outflow copy, where the ghost sits
+        // elsewhere): ctop is a function of U and the position, so the
+        // ghost's first ctop has the source's outcome.  Success: the same
+        // primitives.  Failure: the ghost goes straight to its fallback.
+        if (P.leafmask[src_p] && rr(P, p, lg) == rr(P, src_p, la) && tt(P, p, lg) == tt(P, src_p, la)) {
+            uint8_t st = P.status[(size_t)src_p * NC + la];
+            if (st == 1) {
+                for (int v = 0; v < 8; v++) Wv(P, p, v)[lg] = Wv(P, src_p, v)[la];
+                return;
+            }
+            if (st == 0) {
+                ghost_two_pass(kp, P, p, lg, true);
+                return;
+            }
         }
     }
     ghost_two_pass(kp, P, p, lg);

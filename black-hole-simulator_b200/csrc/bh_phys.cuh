@@ -704,17 +704,19 @@ BH_HD inline void recon_scal(RT Wm, RT Wc, RT Wp, RT Wpp, int lim, RT& fL,
 }
 // causality rescale of reconfp (:69-83) with the cell's metric
 template <typename RT>
-BH_HD inline void causalv(RT v[3], const MetT<RT>& mc) {
+BH_HD inline void causalv_gam(RT v[3], const RT gam[3][3]) {
     RT v2 = RT(0.0);
 #pragma unroll
     for (int m = 0; m < 3; m++)
 #pragma unroll
-        for (int n = 0; n < 3; n++) v2 += mc.gam[m][n] * v[m] * v[n];
+        for (int n = 0; n < 3; n++) v2 += gam[m][n] * v[m] * v[n];
     if (v2 >= RT(1.0)) {
         RT s = (1 - RT(1e-10)) / sqrt(v2);
 #pragma unroll
         for (int a = 0; a < 3; a++) v[a] *= s;
     }
 }
+template <typename RT>
+BH_HD inline void causalv(RT v[3], const MetT<RT>& mc) { causalv_gam(v, mc.gam); }
 
 }  // namespace bh

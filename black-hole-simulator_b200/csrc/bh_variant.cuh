@@ -67,9 +67,14 @@ __global__ void k_hlld(KP k, const double* WL, const double* WR, const double* U
 __global__ void k_reconfp(KP kp, Pool P, int dim, int lim, int64_t n, double* Lo, double* Ro) {
     ITEM(NFACE); reconfp_item<BH_REAL>(kp, P, blockIdx.y, dim, e, lim, n, Lo, Ro);
 }
-// patch::fluxcomp: one face per thread, direction blockIdx.z
+// patch::fluxcomp: one face per thread, direction blockIdx.z; with the
+// per-cell scratch, k_aux first fills it for every cell of every patch
 __global__ void __launch_bounds__(TPB, BH_MINB_FLUX) k_flux(KP kp, Pool P, const int32_t* list) {
     ITEM(NFACE); flux_item<BH_REAL>(kp, P, list[blockIdx.y], blockIdx.z, e);
+}
+__global__ void k_aux(KP kp, Pool P, const int32_t* list) { ITEM(NC); aux_item<BH_REAL>(kp, P, list[blockIdx.y], e); }
+__global__ void __launch_bounds__(TPB, BH_MINB_FLUX) k_flux_aux(KP kp, Pool P, const int32_t* list) {
+    ITEM(NFACE); flux_item<BH_REAL, true>(kp, P, list[blockIdx.y], blockIdx.z, e);
 }
 __global__ void k_emf(Pool P, const int32_t* list) { ITEM(N_EDGE); emf_item(P, list[blockIdx.y], e); }
 __global__ void k_bfupdate(Pool P, const int32_t* list, const double* dtp) {
@@ -94,7 +99,7 @@ __global__ void __launch_bounds__(TPB, BH_MINB_UPDATE) k_update(KP kp, Pool P, c
 }
 // amrtree::ghosts strip fill: one copied double per thread, then the
 // prolonged cells (CTAs whose slot has another neighbour kind exit at once)
-__global__ void k_ghost_copy(Pool P, const int32_t* list) { ITEM(16 * N_STRIP); ghost_copy_item(P, list[blockIdx.y], e); }
+__global__ void k_ghost_copy(Pool P, const int32_t* list) { ITEM(2 * N_STRIP); ghost_copy_item(P, list[blockIdx.y], e); }
 __global__ void k_ghost_prolong(KP kp, Pool P, const int32_t* list) {
     ITEM(N_STRIP); ghost_prolong_item(kp, P, list[blockIdx.y], e);
 }
@@ -202,7 +207,12 @@ int reconfp(const bh_params* P, const bh_pool* pool, int32_t dim, int32_t limite
 }
 int fluxcomp(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
-    k_flux<<<grid2(NFACE, pool->npatch, 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    if (pool->aux) {
+        k_aux<<<grid2(NC, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+        k_flux_aux<<<grid2(NFACE, pool->npatch, 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    } else {
+        k_flux<<<grid2(NFACE, pool->npatch, 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    }
     return launched();
 }
 int emfcomp(const bh_pool* pool, void* stream) {
@@ -234,7 +244,7 @@ int div_source(const bh_params* P, const bh_pool* pool, double* div, double* src
 int ghosts(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
     if (!P || bad_pool(pool) || n < 0 || (n > 0 && !patches)) return BH_EINVAL;
     if (n == 0) return BH_OK;
-    k_ghost_copy<<<grid2(16 * N_STRIP, n), TPB, 0, S(stream)>>>(pool_of(pool), patches);
+    k_ghost_copy<<<grid2(2 * N_STRIP, n), TPB, 0, S(stream)>>>(pool_of(pool), patches);
     k_ghost_prolong<<<grid2(N_STRIP, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
     k_ghost_ctop<<<grid2(NC, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
     return launched();
@@ -252,7 +262,7 @@ int ghosts_prims_status(const bh_params* P, const bh_pool* pool, uint8_t* status
     if (pool->nleaf == 0) return BH_OK;
     Pool pv = pool_of(pool);
     pv.status = status;
-    k_ghost_copy<<<grid2(16 * N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(pv, pool->leaves);
+    k_ghost_copy<<<grid2(2 * N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(pv, pool->leaves);
     k_ghost_prolong<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
     if (status && pool->leafmask) {
         k_prims_interior<<<grid2(N_INT, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);

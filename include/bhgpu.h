@@ -91,6 +91,11 @@ typedef struct bh_pool {
     uint8_t *status;     /* [np][8000] scratch: con2prim outcome of the interior
                             cells in the current stage; NULL disables the reuse
                             of those outcomes by the ghost cells copied from them */
+    double *aux;         /* [np][6][8000] scratch of bh_fluxcomp: log rho, log eps
+                            and the cell-metric entries of the causality check,
+                            computed once per cell instead of once per face that
+                            reads the cell; NULL computes them per face.  Either
+                            way the fluxes are the same bit for bit. */
 } bh_pool;
 
 /* ---- library --------------------------------------------------------------- */
@@ -147,11 +152,12 @@ int bh_ghosts(const bh_params *P, const bh_pool *pool, const int32_t *patches, i
 int bh_prims(const bh_params *P, const bh_pool *pool, void *stream);
 /* ghosts + reconstruction loop fused, valid when every leaf patch is in a
  * single ghost-fill wave (no prolongation dependencies).  With
- * pool->status set, interior cells are recovered first and a ghost cell
- * copied from a leaf cell at the same (r, theta) whose con2prim succeeded
- * takes that cell's primitives: the reference's two con2prim calls on the
- * identical U and position return exactly them (grid.cpp:538-570,
- * integrator.cpp:288-310). */
+ * pool->status set, interior cells are recovered first, and a ghost cell
+ * copied from a leaf cell at the same (r, theta) takes that cell's con2prim
+ * outcome: its primitives where con2prim succeeded (the reference's two
+ * con2prim calls on the identical U and position return exactly them), the
+ * failure where it failed, so that the ghost cell starts at its fallback
+ * (grid.cpp:538-570, integrator.cpp:288-310). */
 int bh_ghosts_prims(const bh_params *P, const bh_pool *pool, void *stream);
 /* No counterpart in the reference (it allocates nothing on a GPU): the
  * ghost fill and reconstruction of bh_ghosts_prims for callers that cannot

@@ -50,18 +50,21 @@ class HostKernels:
         self.L.hc_update.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_int]
         self.L.hc_rkstg.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
 
-    def pool(self, hp, reuse=True):
+    def pool(self, hp, reuse=True, aux=True):
         """bh_pool over the numpy arrays of an oracle.HostPool; reuse=False
-        leaves the status scratch unset (ghost cells recompute con2prim)."""
+        leaves the status scratch unset (ghost cells recompute con2prim),
+        aux=False the per-cell flux scratch (faces compute its values)."""
         self._all = np.arange(hp.npatch, dtype=np.int32)
         self._leaves = np.nonzero(hp.leaf)[0].astype(np.int32)
         self._leafmask = np.ascontiguousarray(hp.leaf, np.uint8)
         self._status = np.full((hp.npatch, 8000), 7, np.uint8)
+        self._aux = np.full((hp.npatch, 6, 8000), np.nan)
         err = np.zeros(1, np.int32)
         self._err = err
         return self.BhPool(hp.npatch, _d(hp.U), _d(hp.W), _d(hp.dU), _d(hp.F), _d(hp.Bf), _d(hp.EMF), _d(hp.rth),
                            _d(hp.pgeo), _d(hp.nbr), _d(self._all), _d(self._leaves), len(self._leaves), _d(err),
-                           _d(self._leafmask), _d(self._status) if reuse else None)
+                           _d(self._leafmask), _d(self._status) if reuse else None,
+                           _d(self._aux) if aux else None)
 
     def call(self, name, *args):
         return getattr(self.L, name)(C.byref(self.P), *args)

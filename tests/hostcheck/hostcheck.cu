@@ -43,6 +43,14 @@ void hc_reconfp(const bh_params* Pp, const bh_pool* pool, int dim, int lim, doub
 }
 void hc_fluxcomp(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
+    if (pool->aux) {
+        for (int i = 0; i < pool->npatch; i++)
+            for (int l = 0; l < NC; l++) aux_item<double>(k, P, pool->all[i], l);
+        for (int i = 0; i < pool->npatch; i++)
+            for (int dim = 0; dim < 3; dim++)
+                for (int f = 0; f < NFACE; f++) flux_item<double, true>(k, P, pool->all[i], dim, f);
+        return;
+    }
     for (int i = 0; i < pool->npatch; i++)
         for (int dim = 0; dim < 3; dim++)
             for (int f = 0; f < NFACE; f++) flux_item<double>(k, P, pool->all[i], dim, f);
@@ -78,7 +86,7 @@ void hc_div_source(const bh_params* Pp, const bh_pool* pool, double* dv, double*
 void hc_ghosts(const bh_params* Pp, const bh_pool* pool, const int32_t* list, int n) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < n; i++)
-        for (int e = 0; e < 16 * N_STRIP; e++) ghost_copy_item(P, list[i], e);
+        for (int e = 0; e < 2 * N_STRIP; e++) ghost_copy_item(P, list[i], e);
     for (int i = 0; i < n; i++)
         for (int e = 0; e < N_STRIP; e++) ghost_prolong_item(k, P, list[i], e);
     for (int i = 0; i < n; i++)
@@ -92,7 +100,7 @@ void hc_prims(const bh_params* Pp, const bh_pool* pool, int ghost_first) {
 void hc_ghosts_prims(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < pool->nleaf; i++)
-        for (int e = 0; e < 16 * N_STRIP; e++) ghost_copy_item(P, pool->leaves[i], e);
+        for (int e = 0; e < 2 * N_STRIP; e++) ghost_copy_item(P, pool->leaves[i], e);
     for (int i = 0; i < pool->nleaf; i++)
         for (int e = 0; e < N_STRIP; e++) ghost_prolong_item(k, P, pool->leaves[i], e);
     if (pool->status && pool->leafmask) {

@@ -75,6 +75,11 @@ def test_kernel_items_bitwise(case):
         assert eq(L, Lc) and eq(R, Rc)
     hk.call("hc_fluxcomp", C.byref(pool)); orc.fluxcomp(hp)
     assert eq(hh.F, hp.F)
+    F_aux = hh.F.copy()                     # the same fluxes without the per-cell scratch
+    hh.F[:] = 0
+    hk.call("hc_fluxcomp", C.byref(hk.pool(hh, aux=False)))
+    assert eq(hh.F, F_aux)
+    pool = hk.pool(hh)
     dt = hk.L.hc_dtcomp(C.byref(hk.P), C.byref(pool), 0.4)
     assert dt == orc.dtcomp(hp, 0.4)
     hk.L.hc_emfcomp(C.byref(pool)); orc.emfcomp(hp)
