@@ -5,4 +5,5 @@
 // division/square root; logf/expf keep their full accuracy.
 #define BH_VARIANT vmixed
 #define BH_REAL float
+#define BH_MINB_FLUX 6   // the FP32 face computation needs fewer registers
 #include "bh_variant.cuh"

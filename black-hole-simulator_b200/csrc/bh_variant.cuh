@@ -32,12 +32,16 @@ constexpr int TPB = 128;
 // minimum resident CTAs per SM requested from ptxas for the heavy kernels
 // (caps their registers per thread); tuned on B200
 // (sweeps on the 128^3 box: con2prim and floors run fastest at 6 CTAs of
-// 128 threads per SM, the flux kernel at 5, the update at 4)
+// 128 threads per SM, the FP64 flux kernel at 4 -- the FP32 one of the
+// mixed variant at 6, set in bh_mixed.cu -- and the update at 4)
 #ifndef BH_MINB_PRIMS
 #define BH_MINB_PRIMS 6
 #endif
+#ifndef BH_MINB_GHOST
+#define BH_MINB_GHOST 6
+#endif
 #ifndef BH_MINB_FLUX
-#define BH_MINB_FLUX 5
+#define BH_MINB_FLUX 4
 #endif
 #ifndef BH_MINB_FLOORS
 #define BH_MINB_FLOORS 6
@@ -110,7 +114,7 @@ __global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_prims(KP kp, Pool P, con
 __global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_prims_interior(KP kp, Pool P, const int32_t* list) {
     ITEM(N_INT); prims_interior_item(kp, P, list[blockIdx.y], e);
 }
-__global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_prims_ghost(KP kp, Pool P, const int32_t* list) {
+__global__ void __launch_bounds__(TPB, BH_MINB_GHOST) k_prims_ghost(KP kp, Pool P, const int32_t* list) {
     ITEM(N_GHOST); prims_ghost_item(kp, P, list[blockIdx.y], e);
 }
 __global__ void __launch_bounds__(TPB, BH_MINB_FLOORS) k_floors(KP kp, Pool P, const int32_t* list) {
