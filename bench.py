@@ -163,9 +163,16 @@ def alg_bytes(call, npatch):
 E2E_DEPTH = 3      # device trees of the end-to-end pipeline
 STEP_BYTES = 296   # algorithmic HBM bytes per zone-update of a whole RK2 step
 
-# DRAM bytes (read + write) per launch from ncu captures of this workload,
-# keyed by (call, grid); see profiles/ for the captures they come from
-TRAFFIC = {}
+# DRAM bytes (read + write) per launch from the ncu capture of the 64^3 box
+# (profiles/kernels_magnetised_box_64cube.md, fp64-fma; stage 0 and stage 1
+# averaged; a call's kernels summed).  The 128^3 figures scale them by the
+# patch count (x8): every launch touches each patch's arrays once, so
+# traffic grows in proportion to the patches.
+_T64 = {"fluxcomp": (16.40 + 0.00 + 100.61 + 38.33) * 1e6,
+        "ghosts_prims": (46.79 + 5.29 + 36.53 + 1.37 + 65.64 + 19.73) * 1e6,
+        "update": (102.31 + 17.75) * 1e6,
+        "floors": (49.61 + 4.01) * 1e6}
+TRAFFIC = {**{(k, 64): v for k, v in _T64.items()}, **{(k, 128): 8 * v for k, v in _T64.items()}}
 
 
 def cpu_reference_sample(threads):
