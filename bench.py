@@ -285,6 +285,31 @@ def field_l1(a, b):
     return out
 
 
+def restart_ms(tree, prec, k, U0, W0, B0):
+    """ms per step of ``prec`` on ``tree``, each step restarted from (U0, W0,
+    B0) like the headline, CUDA events around k steps after 2 warm-up."""
+    import torch
+    import bhgpu
+    rk = bhgpu.RK2Integrator(CFL)
+    keep = tree.precision
+    tree.precision = prec
+
+    def one():
+        tree.U.copy_(U0); tree.W.copy_(W0); tree.Bf.copy_(B0)
+        rk.step(tree, sync=False, check_domain=False)
+    for _ in range(2):
+        one()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(k):
+        one()
+    b.record(); torch.cuda.synchronize()
+    tree.precision = keep
+    tree.clear_error()
+    return a.elapsed_time(b) / k
+
+
 def variant_accuracy(tree, prec, steps, U0, W0, B0):
     """``prec`` against the reference-faithful FP64 variant after ``steps``
     steps from the same state of ``tree``."""
@@ -469,6 +494,32 @@ def run_ours(args):
         if prec in variants:
             variants[prec]["accuracy_vs_fp64"] = acc
 
+    # ---- mixed against plain FP64 where the reference's answer is well
+    # conditioned: the unmagnetised box on the same 128^3 grid (B = 0), both
+    # variants timed the same way, the error after five steps
+    hyd = make_tree(nq, seed=1, precision="fp64", B0=(0.0, 0.0, 0.0), amp=0.0)
+    hU0, hW0, hB0 = hyd.U.clone(), hyd.W.clone(), hyd.Bf.clone()
+    k_h = max(10, args.steps // 4)
+    hyd_ms = {p_: restart_ms(hyd, p_, k_h, hU0, hW0, hB0) for p_ in ("fp64", "mixed")}
+    hyd_acc = variant_accuracy(hyd, "mixed", 5, hU0, hW0, hB0)
+    del hyd, hU0, hW0, hB0
+    l1_max = max(v_ for k_, v_ in hyd_acc.items() if k_ != "nan_mask")
+    mixed_vs_fp64 = {
+        "unmagnetised_box": {"workload": f"{args.grid}^3 box of the headline with B = 0",
+                             "fp64_ms_per_step": hyd_ms["fp64"], "mixed_ms_per_step": hyd_ms["mixed"],
+                             "speedup": hyd_ms["fp64"] / hyd_ms["mixed"], "l1_err_5_steps": hyd_acc,
+                             "within_1e-5": l1_max <= 1e-5},
+        "magnetised_box": {"workload": "the headline box",
+                           "fp64_ms_per_step": variants.get("fp64", {}).get("ms_per_step", ms_max / args.steps),
+                           "mixed_ms_per_step": variants["mixed"]["ms_per_step"] if "mixed" in variants
+                           else ms_max / args.steps,
+                           "l1_err_1_step": accuracy["mixed"]["magnetised_box_1_step"],
+                           "note": "the reference's own result moves by ~8e-3 (L1) under a 1e-7 input "
+                                   "perturbation on this state; the mixed error is of that size"},
+    }
+    mixed_vs_fp64["magnetised_box"]["speedup"] = (mixed_vs_fp64["magnetised_box"]["fp64_ms_per_step"] /
+                                                  mixed_vs_fp64["magnetised_box"]["mixed_ms_per_step"])
+
     # ---- end to end through the public API with host buffers --------------
     # bhgpu.HostPipeline over E2E_DEPTH device trees: every step uploads the
     # state from pinned host memory, steps it and downloads the result; the
@@ -523,6 +574,7 @@ def run_ours(args):
             "speedup_vs_plain_fp64": fp64_ms / (ms_max / args.steps),
             "accuracy_vs_fp64": accuracy.get(args.precision, "identical roundings (the reference-faithful form)"),
             "variants": variants,
+            "mixed_vs_plain_fp64": mixed_vs_fp64,
             "config": {"workload": f"magnetised box {args.grid}^3: flat metric, periodic, PLM-minmod + HLLD + CT, "
                                    f"RK2 CFL 0.4, {args.precision} arithmetic", "grid": f"{args.grid}^3",
                        "patches": tree.npatch, "patch": "16^3 + 2 ghosts", "parallelism": f"replicas x{world}",

@@ -47,6 +47,28 @@ class Patch:
         return e0, sp
 
 
+@dataclass
+class RegridPlan:
+    """What one regrid does to the pool, in the indices of the extended
+    quilt (the old patches, then the children appended by refinement):
+
+    refined:   (parent, [8 children]) per refined patch
+    flattened: (parent, [8 children]) per flattened patch
+    keep:      extended indices that remain, in the new quilt order
+    ext_pgeo:  [n_ext, 6] corners and spacings of the extended quilt
+    """
+    n_old: int
+    n_ext: int
+    ext_pgeo: np.ndarray
+    refined: list
+    flattened: list
+    keep: np.ndarray
+
+    @property
+    def changed(self) -> bool:
+        return bool(self.refined or self.flattened)
+
+
 class Quilt:
     """The patch list of ``amrtree`` (``quilt``, grid.hpp:119), in quilt order.
 
@@ -93,6 +115,56 @@ class Quilt:
             kids.append(len(self.patches) - 1)
         P.leaf = False
         return kids
+
+    # ------------------------------------------------------------------
+    def regrid(self, flags) -> "RegridPlan":
+        """Patch bookkeeping of amrtree::regrid (grid.cpp:722-835) given the
+        per-patch flags of its cell loop (bit 0: refine, bit 1: erase; the
+        flags of non-leaf patches are ignored).
+
+        Leaves flagged for refinement are refined in quilt order, their
+        children appended (refine, :574-600); then every leaf flagged for
+        erasure whose parent is not a leaf and whose siblings are all leaves
+        flattens that parent (:827-834).  The reference keeps raw pointers
+        to children that an earlier flatten of the same parent has already
+        destroyed; the only consistent reading of its loop is that each
+        parent is flattened at most once, which is what happens here.
+        Flattened children leave the quilt with the order of the others
+        kept (std::remove_if, :722-726).  Returns the plan the data
+        operations follow, in the indices of the quilt before removal."""
+        flags = np.asarray(flags)
+        n_old = len(self.patches)
+        rfn = [p for p in range(n_old) if self.patches[p].leaf and flags[p] & 1]
+        flt = [p for p in range(n_old) if self.patches[p].leaf and flags[p] & 2]
+        refined = [(p, self.refine(p)) for p in rfn]
+        ext_pgeo = self._pgeo()
+        flattened, removed = [], set()
+        for p in flt:
+            par = self.patches[p].parent
+            if par < 0 or self.patches[par].leaf:
+                continue
+            kids = self.patches[par].children
+            if any(c >= 0 and not self.patches[c].leaf for c in kids):
+                continue
+            flattened.append((par, list(kids)))
+            removed.update(c for c in kids if c >= 0)
+            self.patches[par].children = [-1] * 8
+            self.patches[par].leaf = True
+        keep = np.array([q for q in range(len(self.patches)) if q not in removed], np.int64)
+        new_of = {int(q): i for i, q in enumerate(keep)}
+        self.patches = [self.patches[q] for q in keep]
+        for P in self.patches:
+            P.parent = new_of.get(P.parent, -1) if P.parent >= 0 else -1
+            P.children = [new_of.get(c, -1) if c >= 0 else -1 for c in P.children]
+        return RegridPlan(n_old, len(ext_pgeo), ext_pgeo, refined, flattened, keep)
+
+    def _pgeo(self) -> np.ndarray:
+        pgeo = np.zeros((len(self.patches), 6), np.float64)
+        for p, P in enumerate(self.patches):
+            e0, sp = P.origin_spacing()
+            pgeo[p, :3] = e0
+            pgeo[p, 3:] = sp
+        return pgeo
 
     # ------------------------------------------------------------------
     def nbhd(self, p: int, dim: int, side: int) -> int:

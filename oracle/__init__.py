@@ -144,6 +144,12 @@ class Oracle:
         L.orc_dtcomp.argtypes = [PP, PO, C.c_double, _dp]
         L.orc_step.argtypes = [PP, PO, C.c_double, _dp]
         L.orc_maxdivb_all.argtypes = [PO, _dp]
+        L.orc_regrid_flags.argtypes = [PO, C.c_int, C.c_int]
+        L.orc_b_init.argtypes = [PO, C.c_int]
+        L.orc_refine_data.argtypes = [PP, PO, C.c_int, _ip]
+        L.orc_ccrstr.argtypes = [PP, PO, C.c_int, _ip]
+        for f in ("orc_regrid_flags", "orc_refine_data", "orc_ccrstr"):
+            getattr(L, f).restype = C.c_int
         for f in ("orc_ptoc_batch", "orc_fluxcomp_all", "orc_ghosts_all", "orc_prims", "orc_update",
                   "orc_rkstg", "orc_floors_all", "orc_dtcomp", "orc_step"):
             getattr(L, f).restype = C.c_int
@@ -251,6 +257,25 @@ class Oracle:
         self._chk(self.lib.orc_step(C.byref(self.P), C.byref(s), cfl, C.byref(dt)))
         return dt.value
 
+    # AMR regrid pieces (grid.cpp:573-835)
+    def regrid_flags(self, pool):
+        """Per-patch flags of amrtree::regrid's cell loop (bit 0 refine, bit 1
+        erase) for the leaf patches; 0 for the others."""
+        s = pool.cstruct()
+        return np.array([self.lib.orc_regrid_flags(C.byref(s), p, int(pool.lvl[p])) if pool.leaf[p] else 0
+                         for p in range(pool.npatch)], np.int32)
+
+    def b_init(self, pool, p):
+        s = pool.cstruct(); self.lib.orc_b_init(C.byref(s), p)
+
+    def refine_data(self, pool, p, kids):
+        k = np.ascontiguousarray(kids, np.int32); s = pool.cstruct()
+        self._chk(self.lib.orc_refine_data(C.byref(self.P), C.byref(s), p, _ptr(k, _ip)))
+
+    def ccrstr(self, pool, p, kids):
+        k = np.ascontiguousarray(kids, np.int32); s = pool.cstruct()
+        self._chk(self.lib.orc_ccrstr(C.byref(self.P), C.byref(s), p, _ptr(k, _ip)))
+
     def maxdivb(self, pool):
         out = np.zeros(pool.npatch); s = pool.cstruct()
         self.lib.orc_maxdivb_all(C.byref(s), _ptr(out))
@@ -284,6 +309,8 @@ class RefSolver:
             L.ref_put.argtypes = [v, _dp, _dp, _dp]
             L.ref_get.argtypes = [v, _dp, _dp, _dp, _dp, _dp, _dp]
             L.ref_refine.argtypes = [v, C.c_int]
+            L.ref_flatten.argtypes = [v, C.c_int]
+            L.ref_regrid.argtypes = [v]
             L.ref_metric_batch.argtypes = [C.c_double] * 3 + [_dp, _dp, C.c_int64, _dp]
             L.ref_ptoc_batch.argtypes = [C.c_double] * 4 + [_dp, _dp, _dp, C.c_int64, _dp, _dp]
             L.ref_ctop_batch.argtypes = [C.c_double] * 4 + [_dp, _dp, _dp, C.c_int64, _dp, _dp, _ip]
@@ -349,6 +376,13 @@ class RefSolver:
 
     def refine(self, p):
         self._chk(self.lib().ref_refine(self.h, p))
+
+    def flatten(self, p):
+        self._chk(self.lib().ref_flatten(self.h, p))
+
+    def regrid(self):
+        """amrtree::regrid; the patch count changes (npatch, patch_info)."""
+        self._chk(self.lib().ref_regrid(self.h))
 
     # stateless
     def metric(self, r, th):

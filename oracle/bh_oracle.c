@@ -1149,6 +1149,165 @@ int orc_ghosts(const orc_params *P, orc_pool *pool, int p) {          /* :524-57
 }
 
 /* ======================================================================
+ * L2: AMR regrid (grid/grid.cpp:573-835)
+ * ==================================================================== */
+
+/* refinement / flattening flags of leaf patch p at level lvl, from the cell
+ * loop of amrtree::regrid (:763-820): bit 0 = some cell asks for refinement
+ * (patch->refine), bit 1 = every cell allows flattening (patch->erase) */
+int orc_regrid_flags(const orc_pool *pool, int p, int lvl) {
+    const double lim_refine = 0.5, lim_flatten = 0.1, r0 = 3.0;   /* :765-768 */
+    const int max_lvl = 4;
+    const double *g = pool->pgeo + 6 * p;
+    double dx = g[3], dy = g[4], dz = g[5];
+    const double *rho = WP(pool, p, 0);
+    const double *B0 = WP(pool, p, 5), *B1 = WP(pool, p, 6), *B2 = WP(pool, p, 7);
+    int anyref = 0, allflt = 1;
+    for (int i = 0; i < BLK; i++)
+        for (int j = 0; j < BLK; j++)
+            for (int k = 0; k < BLK; k++) {
+                int l = lindx(i, j, k);
+                if (RP(pool, p)[l] < r0 && lvl < max_lvl) { anyref = 1; allflt = 0; continue; }
+                double chro = rho[l];
+                if (chro > 0.0) {
+                    double drho_dx = fabs(rho[lindx(i + 1, j, k)] - rho[lindx(i - 1, j, k)]) / (2 * dx);
+                    double drho_dy = fabs(rho[lindx(i, j + 1, k)] - rho[lindx(i, j - 1, k)]) / (2 * dy);
+                    double drho_dz = fabs(rho[lindx(i, j, k + 1)] - rho[lindx(i, j, k - 1)]) / (2 * dz);
+                    double drho = sqrt(drho_dx * drho_dx + drho_dy * drho_dy + drho_dz * drho_dz);
+                    double rgrh = drho * dx / chro;
+                    if (rgrh > lim_refine && lvl < max_lvl) { anyref = 1; allflt = 0; }
+                    if (rgrh > lim_flatten) allflt = 0;
+                }
+                double Bmag = sqrt(B0[l] * B0[l] + B1[l] * B1[l] + B2[l] * B2[l]);
+                if (Bmag > 1e-14) {
+                    double dB_dx = fabs(B0[lindx(i + 1, j, k)] - B0[lindx(i - 1, j, k)]) / (2 * dx);
+                    double dB_dy = fabs(B1[lindx(i, j + 1, k)] - B1[lindx(i, j - 1, k)]) / (2 * dy);
+                    double dB_dz = fabs(B2[lindx(i, j, k + 1)] - B2[lindx(i, j, k - 1)]) / (2 * dz);
+                    double rdB = (dB_dx * dx + dB_dy * dy + dB_dz * dz) / Bmag;
+                    if (rdB > lim_refine && lvl < max_lvl) { anyref = 1; allflt = 0; }
+                }
+            }
+    return ((anyref && lvl < max_lvl) ? 1 : 0) | ((allflt && lvl > 0) ? 2 : 0);
+}
+
+/* patch::B_init (:207-250): face B from the cells' W.B over all 20^3 cells.
+ * The z-face branch tests i (not k) against -ghost (quirk A19); its
+ * out-of-range cell indices k = -3 and k = 18 are used as the reference's
+ * linear index computes them (neighbouring cells in memory order). */
+void orc_b_init(orc_pool *pool, int p) {
+    const double *B0 = WP(pool, p, 5), *B1 = WP(pool, p, 6), *B2 = WP(pool, p, 7);
+    double *Bx = BFP(pool, p, 0), *By = BFP(pool, p, 1), *Bz = BFP(pool, p, 2);
+    for (int i = -GH; i < BLK + GH + 1; i++)
+        for (int j = -GH; j < BLK + GH; j++)
+            for (int k = -GH; k < BLK + GH; k++) {
+                if (i > -GH && i < BLK + GH) Bx[xfc(i, j, k)] = (B0[lindx(i - 1, j, k)] + B0[lindx(i, j, k)]) / 2;
+                else if (i == -GH) Bx[xfc(i, j, k)] = B0[lindx(i, j, k)];
+                else Bx[xfc(i, j, k)] = B0[lindx(i - 1, j, k)];
+            }
+    for (int i = -GH; i < BLK + GH; i++)
+        for (int j = -GH; j < BLK + GH + 1; j++)
+            for (int k = -GH; k < BLK + GH; k++) {
+                if (j > -GH && j < BLK + GH) By[yfc(i, j, k)] = (B1[lindx(i, j - 1, k)] + B1[lindx(i, j, k)]) / 2;
+                else if (j == -GH) By[yfc(i, j, k)] = B1[lindx(i, j, k)];
+                else By[yfc(i, j, k)] = B1[lindx(i, j - 1, k)];
+            }
+    for (int i = -GH; i < BLK + GH; i++)
+        for (int j = -GH; j < BLK + GH; j++)
+            for (int k = -GH; k < BLK + GH + 1; k++) {
+                if (k > -GH && k < BLK + GH) Bz[zfc(i, j, k)] = (B2[lindx(i, j, k - 1)] + B2[lindx(i, j, k)]) / 2;
+                else if (i == -GH) Bz[zfc(i, j, k)] = B2[lindx(i, j, k)];
+                else Bz[zfc(i, j, k)] = B2[lindx(i, j, k - 1)];
+            }
+}
+
+/* ctop of a regridded cell with the fallback of refine/ccrstr (:636-645,
+ * :694-703): on failure W = pvfs(r) with B = the cell's current W.B (zero
+ * in a newly created child), U = ptoc(W) */
+static int regrid_recover(const orc_params *P, orc_pool *pool, int p, int l) {
+    cons U; prim pv;
+    get_cons(pool, p, l, &U);
+    memset(&pv, 0, sizeof(pv));
+    int ok = ctop_(P, &U, RP(pool, p)[l], TP(pool, p)[l], &pv, P->maxiter, P->tol, 0, 0);
+    if (ok < 0) return ORC_EDOMAIN;
+    if (ok) { put_prim(pool, p, l, &pv); return 0; }
+    return floor_reset(P, pool, p, l);
+}
+
+/* the cell data of amrtree::refine (:603-648): child h of parent p takes a
+ * minmod-limited interpolation of the parent's conserved variables.  The
+ * reference's prolong lambda is declared (vc, vmx, vpx, ...) but called
+ * with the +x neighbour first, so each slope is minmod(vc - v[+1], v[-1] - vc).
+ * Then ctop with its fallback, and B_init of the child. */
+int orc_refine_data(const orc_params *P, orc_pool *pool, int p, const int32_t child[8]) {
+    for (int h = 0; h < 8; h++) {
+        int c = child[h];
+        int ix = (h >> 2) & 1, iy = (h >> 1) & 1, iz = h & 1;
+        for (int i = 0; i < BLK; i++)
+            for (int j = 0; j < BLK; j++)
+                for (int k = 0; k < BLK; k++) {
+                    int pi = (i + ix * BLK) / 2, pj = (j + iy * BLK) / 2, pk = (k + iz * BLK) / 2;
+                    double ox = (i % 2 == 0) ? -0.25 : 0.25;
+                    double oy = (j % 2 == 0) ? -0.25 : 0.25;
+                    double oz = (k % 2 == 0) ? -0.25 : 0.25;
+                    int lc = lindx(pi, pj, pk);
+                    int lpx = lindx(pi + 1, pj, pk), lmx = lindx(pi - 1, pj, pk);
+                    int lpy = lindx(pi, pj + 1, pk), lmy = lindx(pi, pj - 1, pk);
+                    int lpz = lindx(pi, pj, pk + 1), lmz = lindx(pi, pj, pk - 1);
+                    int lf = lindx(i, j, k);
+                    for (int v = 0; v < 8; v++) {
+                        const double *u = UP(pool, p, v);
+                        double vc = u[lc];
+                        double sx = minmod(vc - u[lpx], u[lmx] - vc);
+                        double sy = minmod(vc - u[lpy], u[lmy] - vc);
+                        double sz = minmod(vc - u[lpz], u[lmz] - vc);
+                        UP(pool, c, v)[lf] = vc + sx * ox + sy * oy + sz * oz;
+                    }
+                    if (regrid_recover(P, pool, c, lf)) return ORC_EDOMAIN;
+                }
+        orc_b_init(pool, c);
+    }
+    return 0;
+}
+
+/* amrtree::ccrstr (:651-712): each parent cell takes the volume-weighted
+ * mean of the eight child cells of its octant (cons() + vol * U, in the
+ * child-cell order di, dj, dk), then ctop with its fallback; then B_init */
+int orc_ccrstr(const orc_params *P, orc_pool *pool, int p, const int32_t child[8]) {
+    for (int pi = 0; pi < BLK; pi++)
+        for (int pj = 0; pj < BLK; pj++)
+            for (int pk = 0; pk < BLK; pk++) {
+                double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0}, volt = 0.0;
+                for (int h = 0; h < 8; h++) {
+                    int c = child[h];
+                    if (c < 0) continue;
+                    int ix = (h >> 2) & 1, iy = (h >> 1) & 1, iz = h & 1;
+                    const double *g = pool->pgeo + 6 * c;
+                    double vol = g[3] * g[4] * g[5];
+                    for (int di = 0; di < 2; di++)
+                        for (int dj = 0; dj < 2; dj++)
+                            for (int dk = 0; dk < 2; dk++) {
+                                int fi = 2 * (pi - ix * (BLK / 2)) + di;
+                                int fj = 2 * (pj - iy * (BLK / 2)) + dj;
+                                int fk = 2 * (pk - iz * (BLK / 2)) + dk;
+                                if (fi < 0 || fi >= BLK || fj < 0 || fj >= BLK || fk < 0 || fk >= BLK) continue;
+                                int lf = lindx(fi, fj, fk);
+                                volt += vol;
+                                for (int v = 0; v < 8; v++) acc[v] += vol * UP(pool, c, v)[lf];
+                            }
+                }
+                int l = lindx(pi, pj, pk);
+                if (volt > 0.0) {
+                    double inv = 1.0 / volt;
+                    for (int v = 0; v < 8; v++) acc[v] *= inv;
+                }
+                for (int v = 0; v < 8; v++) UP(pool, p, v)[l] = acc[v];
+                if (regrid_recover(P, pool, p, l)) return ORC_EDOMAIN;
+            }
+    orc_b_init(pool, p);
+    return 0;
+}
+
+/* ======================================================================
  * L2: floors, patch::floors (grid.cpp:331-358)
  * ==================================================================== */
 int orc_floors(const orc_params *P, orc_pool *pool, int p) {

@@ -109,6 +109,12 @@ int  orc_source(const orc_params *P, const orc_pool *pool, int p, int i, int j,
 int  orc_ghosts(const orc_params *P, orc_pool *pool, int p);
 int  orc_floors(const orc_params *P, orc_pool *pool, int p);
 
+/* ---- L2 AMR regrid (grid.cpp:573-835) ---------------------------------- */
+int  orc_regrid_flags(const orc_pool *pool, int p, int lvl);   /* bit 0 refine, bit 1 erase */
+void orc_b_init(orc_pool *pool, int p);
+int  orc_refine_data(const orc_params *P, orc_pool *pool, int p, const int32_t child[8]);
+int  orc_ccrstr(const orc_params *P, orc_pool *pool, int p, const int32_t child[8]);
+
 /* ---- L3 integrator ------------------------------------------------------ */
 int orc_dtcomp(const orc_params *P, const orc_pool *pool, double cfl, double *dt);
 int orc_prims(const orc_params *P, orc_pool *pool);          /* integrator.cpp:288-310 */

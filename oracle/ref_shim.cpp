@@ -353,7 +353,32 @@ void ref_get(void* h, double* U, double* W, double* dU, double* F, double* Bf, d
         }
     }
 }
-int ref_refine(void* h, int p) { GUARD(((Ref*)h)->tree.refine(((Ref*)h)->tree.quilt[p].get())); return 0; }
+// refine, ccrstr and regrid call conserved::ctop from their own cell loops.
+// Only the first call of a loop can see stack contents left by unrelated
+// earlier work (later calls see the previous cell's finite values, which the
+// a = 0 metric multiplies by an exact zero), so the stack is scrubbed on entry.
+int ref_refine(void* h, int p) {
+    scrub_stack();
+    GUARD(((Ref*)h)->tree.refine(((Ref*)h)->tree.quilt[p].get()));
+    return 0;
+}
+int ref_flatten(void* h, int p) {
+    scrub_stack();
+    GUARD(((Ref*)h)->tree.flatten(((Ref*)h)->tree.quilt[p].get()));
+    return 0;
+}
+// amrtree::regrid (grid.cpp:722-835), the reference's own flag loop, refinement and flattening.
+// patch::refine and patch::erase are never initialised (the constructor,
+// grid.cpp:19-48, leaves them out) and regrid only ever sets them to true
+// before it consumes and clears them; a patch built on recycled heap memory
+// can start with either flag set.  Clearing both first gives the reading in
+// which they start false, the one the flag loop's logic assumes.
+int ref_regrid(void* h) {
+    for (auto& p : ((Ref*)h)->tree.quilt) { p->refine = false; p->erase = false; }
+    scrub_stack();
+    GUARD(((Ref*)h)->tree.regrid());
+    return 0;
+}
 
 // ---- stateless physics ---------------------------------------------------
 void ref_metric_batch(double M, double a, double Q, const double* r, const double* th, int64_t n, double* out) {

@@ -104,6 +104,29 @@ def box_case(nq=2, seed=3, periodic=True, lim=0, M=0.0, a=0.0, lo=10.0, hi=12.0,
     return q, orc, hp
 
 
+def oracle_regrid(orc, hp, quilt):
+    """One amrtree::regrid on the oracle: flags, the quilt's plan, the data
+    operations on the extended pool, then the kept patches.  Returns the
+    new HostPool (quilt is updated in place) and the plan."""
+    flags = orc.regrid_flags(hp)
+    plan = quilt.regrid(flags)
+    T = quilt.tables()
+    ext = oracle.HostPool({"pgeo": plan.ext_pgeo, "lvl": np.zeros(plan.n_ext, np.int32),
+                           "ijk": np.zeros((plan.n_ext, 3), np.int32), "leaf": np.zeros(plan.n_ext, np.uint8),
+                           "nbr": np.zeros((plan.n_ext, 6, 2), np.int32)})
+    for name in ("U", "W", "dU", "F", "Bf", "EMF"):
+        getattr(ext, name)[:plan.n_old] = getattr(hp, name)
+    orc.geometry(ext)
+    for p, kids in plan.refined:
+        orc.refine_data(ext, p, kids)
+    for p, kids in plan.flattened:
+        orc.ccrstr(ext, p, kids)
+    new = oracle.HostPool(T)
+    for name in ("U", "W", "dU", "F", "Bf", "EMF", "rth"):
+        getattr(new, name)[:] = getattr(ext, name)[plan.keep]
+    return new, plan
+
+
 def gpu_tree(q, hp, M=0.0, a=0.0, lim=0, precision="fp64"):
     import bhgpu
     tree = bhgpu.AmrTree(q.dom_l, q.dom_h, q.nqlt, M=M, a=a, Q=0.0, gm=GAMMA, periodic=q.periodic,
