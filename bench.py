@@ -266,6 +266,43 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
 
 
 # ---------------------------------------------------------------------------
+# AMR regrid: one amrtree::regrid of the floor state around a Schwarzschild
+# hole (64^3 in 4^3 patches over [-16,16]^3: the 8 central patches hold
+# cells inside r = 3 and refine), and the refinement test alone on the
+# headline box, where nothing changes (the reference regrids after every step)
+def regrid_bench(tree):
+    import torch
+    import bhgpu
+    from bhgpu.mesh import Quilt
+    q = Quilt([-16.0] * 3, [16.0] * 3, 4)
+    t = bhgpu.AmrTree(q.dom_l, q.dom_h, 4, M=1.0, a=0.0, Q=0.0, gm=GAMMA, limiter="vanleer", quilt=q)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plan = t.regrid(check_domain=False)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    n_after = t.npatch
+    del t
+    flags = torch.zeros(tree.npatch, dtype=torch.uint8, device="cuda")
+    P = tree.params()
+    from bhgpu.solver import _p, _stream
+    L = bhgpu.lib
+    for _ in range(2):
+        L.bh_regrid_flags(C.byref(P), C.byref(tree.pool), _p(tree.lvl), _p(flags), _stream())
+    a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(10):
+        L.bh_regrid_flags(C.byref(P), C.byref(tree.pool), _p(tree.lvl), _p(flags), _stream())
+    b.record(); torch.cuda.synchronize()
+    return {"workload": "floor state around a Schwarzschild hole, 64^3 in 4^3 patches over [-16,16]^3, "
+                        "one amrtree::regrid (flags on the device, bookkeeping on the host, refine on the device)",
+            "patches_before": 64, "patches_after": n_after, "refined": len(plan.refined),
+            "ms_wall": (t1 - t0) * 1e3,
+            "refinement_test_ms": a.elapsed_time(b) / 10,
+            "refinement_test_workload": f"the headline box ({tree.npatch} patches), nothing refines"}
+
+
+# ---------------------------------------------------------------------------
 FIELDS = {"D": [0], "S": [1, 2, 3], "tau": [4], "B": [5, 6, 7]}
 
 
@@ -599,6 +636,7 @@ def run_ours(args):
             line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample}
             if args.con2prim_batch:
                 line["con2prim_batch"] = con2prim_batch()
+            line["regrid"] = regrid_bench(tree)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

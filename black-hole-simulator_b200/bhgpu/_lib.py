@@ -67,6 +67,10 @@ def _load():
         "bh_update": ([P, PP, _vp, i32, _vp], C.c_int),
         "bh_floors": ([P, PP, _vp], C.c_int),
         "bh_dtcomp": ([P, PP, dbl, _vp, _vp], C.c_int),
+        "bh_regrid_flags": ([P, PP, _vp, _vp, _vp], C.c_int),
+        "bh_refine": ([P, PP, _vp, i32, _vp], C.c_int),
+        "bh_ccrstr": ([P, PP, _vp, i32, _vp], C.c_int),
+        "bh_b_init": ([P, PP, _vp, i32, _vp], C.c_int),
         "bh_rkstg": ([P, PP, _vp, i32, _vp, _vp, i32, _vp], C.c_int),
         "bh_step": ([P, PP, dbl, _vp, _vp, _vp, i32, _vp], C.c_int),
     }

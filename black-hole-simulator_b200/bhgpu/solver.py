@@ -176,10 +176,7 @@ class AmrTree:
 
     # ------------------------------------------------------------------
     def _alloc(self):
-        T = self.quilt.tables()
-        self.tables = T
-        n = len(T["lvl"])
-        self.npatch = n
+        n = len(self.quilt)
         d, f64 = self.device, torch.float64
         self.U = torch.zeros((n, 8, NC), dtype=f64, device=d)
         self.W = torch.zeros((n, 8, NC), dtype=f64, device=d)
@@ -187,13 +184,25 @@ class AmrTree:
         self.F = torch.zeros((n, 3, 8, NF), dtype=f64, device=d)
         self.Bf = torch.zeros((n, 3, NF), dtype=f64, device=d)
         self.EMF = torch.zeros((n, 3, NE), dtype=f64, device=d)
+        self.err = torch.zeros(1, dtype=torch.int32, device=d)
+        self.dt = torch.zeros(1, dtype=f64, device=d)
+        self._bind()
+
+    def _bind(self):
+        """Per-patch tables, scratch and the bh_pool of the current quilt and
+        state arrays; cell geometry (patch::cell_init)."""
+        T = self.quilt.tables()
+        self.tables = T
+        n = len(T["lvl"])
+        self.npatch = n
+        d, f64 = self.device, torch.float64
         self.rth = torch.zeros((n, 2, NC), dtype=f64, device=d)
         self.pgeo = torch.as_tensor(T["pgeo"], device=d)
         self.nbr = torch.as_tensor(T["nbr"], device=d)
+        self.lvl = torch.as_tensor(T["lvl"], device=d)
         self.all = torch.arange(n, dtype=torch.int32, device=d)
         leaves = np.nonzero(T["leaf"])[0].astype(np.int32)
         self.leaves = torch.as_tensor(leaves, device=d)
-        self.err = torch.zeros(1, dtype=torch.int32, device=d)
         self.leafmask = torch.as_tensor(np.ascontiguousarray(T["leaf"], np.uint8), device=d)
         # scratch: con2prim outcome of every interior cell in the current stage
         self.status = torch.zeros((n, NC), dtype=torch.uint8, device=d)
@@ -206,11 +215,58 @@ class AmrTree:
             off[w + 1] = off[w] + len(lst)
         self._wave_off = off
         self.waves = torch.as_tensor(np.concatenate(waves) if waves else np.zeros(0, np.int32), device=d)
-        self.dt = torch.zeros(1, dtype=f64, device=d)
         self.pool = BhPool(n, _p(self.U), _p(self.W), _p(self.dU), _p(self.F), _p(self.Bf), _p(self.EMF),
                            _p(self.rth), _p(self.pgeo), _p(self.nbr), _p(self.all), _p(self.leaves),
                            len(leaves), _p(self.err), _p(self.leafmask), _p(self.status), _p(self.aux))
         check(lib.bh_geometry(C.byref(self.pool), _stream()), "patch::cell_init")
+
+    # ---- AMR -------------------------------------------------------------
+    def regrid(self, check_domain: bool = True, flags=None):
+        """amrtree::regrid (grid.cpp:722-835) on the device.
+
+        The refinement test of every leaf patch runs on the GPU
+        (bh_regrid_flags); the quilt bookkeeping -- which patches refine or
+        flatten and the order of the new quilt -- runs on the host from
+        those flags (Quilt.regrid); the pool is extended by the new children
+        (zeroed, as the reference value-initialises a new patch), refine
+        (bh_refine) and ccrstr (bh_ccrstr) fill them, and the flattened
+        children leave the pool.  ``flags`` (per patch, bit 0 refine, bit 1
+        erase) replaces the reference's refinement test with the caller's.
+        Returns the plan (bhgpu.mesh.RegridPlan)."""
+        P = self.params()
+        if flags is None:
+            fl = torch.zeros(self.npatch, dtype=torch.uint8, device=self.device)
+            check(lib.bh_regrid_flags(C.byref(P), C.byref(self.pool), _p(self.lvl), _p(fl), _stream()),
+                  "amrtree::regrid")
+            flags = fl.cpu().numpy()
+        plan = self.quilt.regrid(np.asarray(flags))
+        if not plan.changed:
+            return plan
+        d, grow = self.device, plan.n_ext - plan.n_old
+
+        def ext(t):
+            return torch.cat([t, t.new_zeros((grow,) + tuple(t.shape[1:]))]) if grow else t
+        U, W, dU, F, Bf, EMF = (ext(x) for x in (self.U, self.W, self.dU, self.F, self.Bf, self.EMF))
+        rth = torch.zeros((plan.n_ext, 2, NC), dtype=torch.float64, device=d)
+        pgeo = torch.as_tensor(plan.ext_pgeo, device=d)
+        all_ = torch.arange(plan.n_ext, dtype=torch.int32, device=d)
+        pool = BhPool(plan.n_ext, _p(U), _p(W), _p(dU), _p(F), _p(Bf), _p(EMF), _p(rth), _p(pgeo), None,
+                      _p(all_), None, 0, _p(self.err), None, None, None)
+        s = _stream()
+        check(lib.bh_geometry(C.byref(pool), s), "patch::cell_init")
+        if plan.refined:
+            rows = torch.as_tensor(np.array([[p] + kids for p, kids in plan.refined], np.int32), device=d)
+            check(lib.bh_refine(C.byref(P), C.byref(pool), _p(rows), len(plan.refined), s), "amrtree::refine")
+        if plan.flattened:
+            rows = torch.as_tensor(np.array([[p] + kids for p, kids in plan.flattened], np.int32), device=d)
+            check(lib.bh_ccrstr(C.byref(P), C.byref(pool), _p(rows), len(plan.flattened), s), "amrtree::ccrstr")
+        keep = torch.as_tensor(plan.keep, device=d)
+        self.U, self.W, self.dU, self.F, self.Bf, self.EMF = (
+            x.index_select(0, keep).contiguous() for x in (U, W, dU, F, Bf, EMF))
+        self._bind()
+        if check_domain:
+            self.check()
+        return plan
 
     def params(self, maxiter=500, tol=1e-10) -> BhParams:
         return _params(self.mtr, self.stt, self.limiter, maxiter, tol, self.precision)

@@ -107,6 +107,18 @@ int bh_update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int
     BH_DISPATCH(P, update(P, pool, dt_dev, stage, stream));
 }
 int bh_floors(const bh_params* P, const bh_pool* pool, void* stream) { BH_DISPATCH(P, floors(P, pool, stream)); }
+int bh_regrid_flags(const bh_params* P, const bh_pool* pool, const int32_t* lvl, uint8_t* flags, void* stream) {
+    BH_DISPATCH(P, regrid_flags(P, pool, lvl, flags, stream));
+}
+int bh_refine(const bh_params* P, const bh_pool* pool, const int32_t* plan, int32_t n, void* stream) {
+    BH_DISPATCH(P, refine(P, pool, plan, n, stream));
+}
+int bh_ccrstr(const bh_params* P, const bh_pool* pool, const int32_t* plan, int32_t n, void* stream) {
+    BH_DISPATCH(P, ccrstr(P, pool, plan, n, stream));
+}
+int bh_b_init(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
+    BH_DISPATCH(P, b_init(P, pool, patches, n, stream));
+}
 int bh_dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
     BH_DISPATCH(P, dtcomp(P, pool, cfl, dt_dev, stream));
 }

@@ -28,6 +28,10 @@
     int update(const bh_params*, const bh_pool*, const double*, int32_t, void*);                               \
     int floors(const bh_params*, const bh_pool*, void*);                                                       \
     int dtcomp(const bh_params*, const bh_pool*, double, double*, void*);                                      \
+    int regrid_flags(const bh_params*, const bh_pool*, const int32_t*, uint8_t*, void*);                       \
+    int refine(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
+    int ccrstr(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
+    int b_init(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
     int rkstg(const bh_params*, const bh_pool*, const double*, int32_t, const int32_t*, const int32_t*, int32_t, \
               void*);                                                                                           \
     int step(const bh_params*, const bh_pool*, double, double*, const int32_t*, const int32_t*, int32_t, void*); \

@@ -769,6 +769,147 @@ BH_HD inline void floors_item(const KP& kp, const Pool& P, int p, int c) {
     if (wrote) store_prim(P, p, l, w);
 }
 
+// ---- AMR regrid (grid.cpp:573-835) ---------------------------------------
+// One interior cell of amrtree::regrid's refinement test (:771-818): ref =
+// the cell asks for refinement, noflat = it forbids flattening its patch.
+constexpr int REGRID_MAX_LVL = 4;
+BH_HD inline void regrid_cell(const Pool& P, int p, int lvl, int c, bool& ref, bool& noflat) {
+    int i = c / 256, j = (c / 16) % 16, k = c % 16;
+    int l = lindx(i, j, k);
+    if (rr(P, p, l) < 3.0 && lvl < REGRID_MAX_LVL) { ref = true; noflat = true; return; }
+    const double* g = P.pgeo + 6 * p;
+    double dx = g[3], dy = g[4], dz = g[5];
+    const double* rho = Wv(P, p, 0);
+    double chro = rho[l];
+    if (chro > 0.0) {
+        double drho_dx = fabs(rho[lindx(i + 1, j, k)] - rho[lindx(i - 1, j, k)]) / (2 * dx);
+        double drho_dy = fabs(rho[lindx(i, j + 1, k)] - rho[lindx(i, j - 1, k)]) / (2 * dy);
+        double drho_dz = fabs(rho[lindx(i, j, k + 1)] - rho[lindx(i, j, k - 1)]) / (2 * dz);
+        double drho = sqrt(drho_dx * drho_dx + drho_dy * drho_dy + drho_dz * drho_dz);
+        double rgrh = drho * dx / chro;
+        if (rgrh > 0.5 && lvl < REGRID_MAX_LVL) { ref = true; noflat = true; }
+        if (rgrh > 0.1) noflat = true;
+    }
+    const double *B0 = Wv(P, p, 5), *B1 = Wv(P, p, 6), *B2 = Wv(P, p, 7);
+    double Bmag = sqrt(B0[l] * B0[l] + B1[l] * B1[l] + B2[l] * B2[l]);
+    if (Bmag > 1e-14) {
+        double dB_dx = fabs(B0[lindx(i + 1, j, k)] - B0[lindx(i - 1, j, k)]) / (2 * dx);
+        double dB_dy = fabs(B1[lindx(i, j + 1, k)] - B1[lindx(i, j - 1, k)]) / (2 * dy);
+        double dB_dz = fabs(B2[lindx(i, j, k + 1)] - B2[lindx(i, j, k - 1)]) / (2 * dz);
+        double rdB = (dB_dx * dx + dB_dy * dy + dB_dz * dz) / Bmag;
+        if (rdB > 0.5 && lvl < REGRID_MAX_LVL) { ref = true; noflat = true; }
+    }
+}
+// the patch's flags from the OR of its cells: bit 0 patch->refine, bit 1 patch->erase
+BH_HD inline uint8_t regrid_patch_flags(int lvl, bool anyref, bool anynoflat) {
+    return (uint8_t)(((anyref && lvl < REGRID_MAX_LVL) ? 1 : 0) | ((!anynoflat && lvl > 0) ? 2 : 0));
+}
+
+// patch::B_init (grid.cpp:207-250), face e of 3 x 8400: face B from the
+// cells' W.B.  The z-face branch tests i (not k) against -ghost; its cell
+// indices k = -3 and k = 18 are taken as the reference's linear index
+// computes them, i.e. neighbouring cells in memory order (all within the
+// patch's 8000 cells).
+BH_HD inline void b_init_item(const Pool& P, int p, int e) {
+    int d = e / NF, f = e % NF;
+    const double* Bc = Wv(P, p, 5 + d);
+    double v;
+    if (d == 0) {
+        int i = f / (CPN * CPN) - GH, j = (f / CPN) % CPN - GH, k = f % CPN - GH;
+        if (i > -GH && i < BLK + GH) v = (Bc[lindx(i - 1, j, k)] + Bc[lindx(i, j, k)]) / 2;
+        else if (i == -GH) v = Bc[lindx(i, j, k)];
+        else v = Bc[lindx(i - 1, j, k)];
+    } else if (d == 1) {
+        int i = f / ((CPN + 1) * CPN) - GH, j = (f / CPN) % (CPN + 1) - GH, k = f % CPN - GH;
+        if (j > -GH && j < BLK + GH) v = (Bc[lindx(i, j - 1, k)] + Bc[lindx(i, j, k)]) / 2;
+        else if (j == -GH) v = Bc[lindx(i, j, k)];
+        else v = Bc[lindx(i, j - 1, k)];
+    } else {
+        int i = f / (CPN * (CPN + 1)) - GH, j = (f / (CPN + 1)) % CPN - GH, k = f % (CPN + 1) - GH;
+        if (k > -GH && k < BLK + GH) v = (Bc[lindx(i, j, k - 1)] + Bc[lindx(i, j, k)]) / 2;
+        else if (i == -GH) v = Bc[lindx(i, j, k)];
+        else v = Bc[lindx(i, j, k - 1)];
+    }
+    Bfv(P, p, d)[f] = v;
+}
+
+// the cell data of amrtree::refine (:603-648) for interior cell c of child h
+// (patch `child`) of patch `parent`: a minmod-limited interpolation of the
+// parent's conserved variables, then ctop with its fallback (W = pvfs with
+// v = 0 and the cell's current B, zero in a new child; U = ptoc(W)).  The
+// reference's prolong lambda is declared (vc, vmx, vpx, ...) but called
+// with the +x neighbour first, so each slope is minmod(vc - v[+1], v[-1] - vc).
+BH_HD inline void refine_item(const KP& kp, const Pool& P, int parent, int child, int h, int c) {
+    int i = c / 256, j = (c / 16) % 16, k = c % 16;
+    int ix = (h >> 2) & 1, iy = (h >> 1) & 1, iz = h & 1;
+    int pi = (i + ix * BLK) / 2, pj = (j + iy * BLK) / 2, pk = (k + iz * BLK) / 2;
+    double ox = (i % 2 == 0) ? -0.25 : 0.25;
+    double oy = (j % 2 == 0) ? -0.25 : 0.25;
+    double oz = (k % 2 == 0) ? -0.25 : 0.25;
+    int lc = lindx(pi, pj, pk);
+    int lpx = lindx(pi + 1, pj, pk), lmx = lindx(pi - 1, pj, pk);
+    int lpy = lindx(pi, pj + 1, pk), lmy = lindx(pi, pj - 1, pk);
+    int lpz = lindx(pi, pj, pk + 1), lmz = lindx(pi, pj, pk - 1);
+    double u8[8];
+    for (int v = 0; v < 8; v++) {
+        const double* u = Uv(P, parent, v);
+        double vc = u[lc];
+        double sx = minmod(vc - u[lpx], u[lmx] - vc);
+        double sy = minmod(vc - u[lpy], u[lmy] - vc);
+        double sz = minmod(vc - u[lpz], u[lmz] - vc);
+        u8[v] = vc + sx * ox + sy * oy + sz * oz;
+    }
+    Cons cu;
+    cu.D = u8[0]; cu.tau = u8[4];
+    for (int d = 0; d < 3; d++) { cu.S[d] = u8[1 + d]; cu.B[d] = u8[5 + d]; }
+    int lf = lindx(i, j, k);
+    Prim w;
+    load_prim(P, child, lf, w);
+    bool dirty = false;
+    recover_cell(kp, P, child, lf, w, cu, dirty);
+    store_cons(P, child, lf, cu);
+    store_prim(P, child, lf, w);
+}
+
+// amrtree::ccrstr (:651-712) for interior cell c of `parent`: the
+// volume-weighted mean of the eight cells of its octant child (cons() +
+// vol * U, in the child-cell order di, dj, dk; the reference also visits
+// the other children, none of whose cells lies in range), then ctop with
+// the fallback keeping the parent cell's B
+BH_HD inline void ccrstr_item(const KP& kp, const Pool& P, int parent, const int32_t* kids, int c) {
+    int pi = c / 256, pj = (c / 16) % 16, pk = c % 16;
+    int ix = pi >= BLK / 2, iy = pj >= BLK / 2, iz = pk >= BLK / 2;
+    int ch = kids[ix * 4 + iy * 2 + iz];
+    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double volt = 0.0;
+    if (ch >= 0) {
+        const double* g = P.pgeo + 6 * ch;
+        double vol = g[3] * g[4] * g[5];
+        for (int di = 0; di < 2; di++)
+            for (int dj = 0; dj < 2; dj++)
+                for (int dk = 0; dk < 2; dk++) {
+                    int lf = lindx(2 * (pi - ix * (BLK / 2)) + di, 2 * (pj - iy * (BLK / 2)) + dj,
+                                   2 * (pk - iz * (BLK / 2)) + dk);
+                    volt += vol;
+                    for (int v = 0; v < 8; v++) acc[v] += vol * Uv(P, ch, v)[lf];
+                }
+    }
+    if (volt > 0.0) {
+        double inv = 1.0 / volt;
+        for (int v = 0; v < 8; v++) acc[v] *= inv;
+    }
+    Cons cu;
+    cu.D = acc[0]; cu.tau = acc[4];
+    for (int d = 0; d < 3; d++) { cu.S[d] = acc[1 + d]; cu.B[d] = acc[5 + d]; }
+    int l = lindx(pi, pj, pk);
+    Prim w;
+    load_prim(P, parent, l, w);
+    bool dirty = false;
+    recover_cell(kp, P, parent, l, w, cu, dirty);
+    store_cons(P, parent, l, cu);
+    store_prim(P, parent, l, w);
+}
+
 // ---- dtcomp (integrator.cpp:156-189): one cell's CFL candidate -----------
 constexpr double DBL_BIG = 1.7976931348623157e308;   // std::numeric_limits<double>::max()
 BH_HD inline double dt_item(const KP& kp, const Pool& P, int p, int c, double cfl) {

@@ -121,6 +121,36 @@ __global__ void __launch_bounds__(TPB, BH_MINB_FLOORS) k_floors(KP kp, Pool P, c
     ITEM(N_INT); floors_item(kp, P, list[blockIdx.y], e);
 }
 
+// ---- AMR regrid: flags (one CTA per leaf patch, OR-reduced over its
+// cells), refine and ccrstr (one thread per new cell; plan rows are
+// parent + 8 children), B_init (one thread per face) -----------------------
+__global__ void k_regrid_flags(Pool P, const int32_t* list, const int32_t* lvl, uint8_t* flags) {
+    int p = list[blockIdx.x];
+    int L = lvl[p];
+    bool ref = false, nf = false;
+    for (int c = threadIdx.x; c < N_INT; c += blockDim.x) regrid_cell(P, p, L, c, ref, nf);
+    int any_ref = __syncthreads_or(ref);
+    int any_nf = __syncthreads_or(nf);
+    if (threadIdx.x == 0) flags[p] = regrid_patch_flags(L, any_ref != 0, any_nf != 0);
+}
+__global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_refine(KP kp, Pool P, const int32_t* plan) {
+    ITEM(N_INT);
+    const int32_t* row = plan + (blockIdx.y / 8) * 9;
+    int h = blockIdx.y % 8;
+    refine_item(kp, P, row[0], row[1 + h], h, e);
+}
+__global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_ccrstr(KP kp, Pool P, const int32_t* plan) {
+    ITEM(N_INT);
+    const int32_t* row = plan + blockIdx.y * 9;
+    ccrstr_item(kp, P, row[0], row + 1, e);
+}
+__global__ void k_b_init(Pool P, const int32_t* list) { ITEM(3 * NF); b_init_item(P, list[blockIdx.y], e); }
+// B_init of the patches in columns [col0, col0 + ncol) of the plan rows
+__global__ void k_b_init_rows(Pool P, const int32_t* plan, int col0, int ncol) {
+    ITEM(3 * NF);
+    b_init_item(P, plan[(blockIdx.y / ncol) * 9 + col0 + blockIdx.y % ncol], e);
+}
+
 // constrans::maxdivB: one CTA per patch, max-reduction in shared memory
 __global__ void k_maxdivb(Pool P, double* out) {
     int p = blockIdx.x;
@@ -288,6 +318,35 @@ int update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_
 int floors(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     k_floors<<<grid2(N_INT, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    return launched();
+}
+int regrid_flags(const bh_params* P, const bh_pool* pool, const int32_t* lvl, uint8_t* flags, void* stream) {
+    if (!P || bad_pool(pool) || !lvl || !flags) return BH_EINVAL;
+    if (pool->nleaf == 0) return BH_OK;
+    k_regrid_flags<<<pool->nleaf, 256, 0, S(stream)>>>(pool_of(pool), pool->leaves, lvl, flags);
+    return launched();
+}
+int refine(const bh_params* P, const bh_pool* pool, const int32_t* plan, int32_t n, void* stream) {
+    if (!P || bad_pool(pool) || n < 0 || (n > 0 && !plan)) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    if (n > 65535 / 8) return BH_ERANGE;
+    k_refine<<<dim3(N_INT / TPB, n * 8), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), plan);
+    k_b_init_rows<<<dim3((3 * NF + TPB - 1) / TPB, n * 8), TPB, 0, S(stream)>>>(pool_of(pool), plan, 1, 8);
+    return launched();
+}
+int ccrstr(const bh_params* P, const bh_pool* pool, const int32_t* plan, int32_t n, void* stream) {
+    if (!P || bad_pool(pool) || n < 0 || (n > 0 && !plan)) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    if (n > 65535) return BH_ERANGE;
+    k_ccrstr<<<dim3(N_INT / TPB, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), plan);
+    k_b_init_rows<<<dim3((3 * NF + TPB - 1) / TPB, n), TPB, 0, S(stream)>>>(pool_of(pool), plan, 0, 1);
+    return launched();
+}
+int b_init(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
+    if (!P || bad_pool(pool) || n < 0 || (n > 0 && !patches)) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    if (n > 65535) return BH_ERANGE;
+    k_b_init<<<grid2(3 * NF, n), TPB, 0, S(stream)>>>(pool_of(pool), patches);
     return launched();
 }
 int dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {

@@ -184,6 +184,28 @@ int bh_update(const bh_params *P, const bh_pool *pool, const double *dt_dev, int
 /* patch::floors (grid/grid.cpp:331-358) on every patch */
 int bh_floors(const bh_params *P, const bh_pool *pool, void *stream);
 
+/* ---- L2 AMR regrid (grid/grid.cpp:573-835) ------------------------------ */
+/* The data operations of amrtree::regrid; the quilt bookkeeping (which
+ * patches refine or flatten, the order of the new quilt) is the caller's,
+ * from the flags below.  Plans are device arrays of rows
+ * (parent, child0 .. child7), children in octant order (grid.cpp:596-599). */
+/* the cell loop of amrtree::regrid (:763-820) on every leaf patch: flags[p]
+ * bit 0 = patch->refine, bit 1 = patch->erase; lvl[npatch] = patch levels.
+ * Entries of non-leaf patches are not written. */
+int bh_regrid_flags(const bh_params *P, const bh_pool *pool, const int32_t *lvl, uint8_t *flags,
+                    void *stream);
+/* the cell data of amrtree::refine (:603-648) for n refined patches: the
+ * children (already in the pool with zeroed arrays and geometry from
+ * bh_geometry) take the parent's prolonged U, con2prim with its fallback,
+ * and patch::B_init (:207-250).  n <= 8191 per call. */
+int bh_refine(const bh_params *P, const bh_pool *pool, const int32_t *plan, int32_t n, void *stream);
+/* amrtree::ccrstr (:651-712) + B_init for n flattened patches: each parent
+ * cell takes the volume-weighted mean of its octant child's cells and
+ * con2prim with its fallback.  n <= 65535 per call. */
+int bh_ccrstr(const bh_params *P, const bh_pool *pool, const int32_t *plan, int32_t n, void *stream);
+/* patch::B_init (:207-250) on the n listed patches */
+int bh_b_init(const bh_params *P, const bh_pool *pool, const int32_t *patches, int32_t n, void *stream);
+
 /* ---- L3 integrator ------------------------------------------------------ */
 /* rk2integrator::dtcomp (solver/integrator.cpp:156-189): *dt_dev = CFL step */
 int bh_dtcomp(const bh_params *P, const bh_pool *pool, double cfl, double *dt_dev, void *stream);

@@ -124,6 +124,34 @@ void hc_floors(const bh_params* Pp, const bh_pool* pool) {
     for (int i = 0; i < pool->npatch; i++)
         for (int c = 0; c < N_INT; c++) floors_item(k, P, pool->all[i], c);
 }
+// AMR regrid pieces, in the launch order of bh_regrid_flags / bh_refine /
+// bh_ccrstr (flags of the leaf patches; plan rows parent + 8 children)
+void hc_regrid_flags(const bh_params* Pp, const bh_pool* pool, const int32_t* lvl, uint8_t* flags) {
+    (void)Pp;
+    Pool P = pool_of(pool);
+    for (int i = 0; i < pool->nleaf; i++) {
+        int p = pool->leaves[i];
+        bool ref = false, nf = false;
+        for (int c = 0; c < N_INT; c++) regrid_cell(P, p, lvl[p], c, ref, nf);
+        flags[p] = regrid_patch_flags(lvl[p], ref, nf);
+    }
+}
+void hc_refine(const bh_params* Pp, const bh_pool* pool, const int32_t* plan, int n) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int r = 0; r < n; r++)
+        for (int h = 0; h < 8; h++)
+            for (int c = 0; c < N_INT; c++) refine_item(k, P, plan[r * 9], plan[r * 9 + 1 + h], h, c);
+    for (int r = 0; r < n; r++)
+        for (int h = 0; h < 8; h++)
+            for (int e = 0; e < 3 * NF; e++) b_init_item(P, plan[r * 9 + 1 + h], e);
+}
+void hc_ccrstr(const bh_params* Pp, const bh_pool* pool, const int32_t* plan, int n) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    for (int r = 0; r < n; r++)
+        for (int c = 0; c < N_INT; c++) ccrstr_item(k, P, plan[r * 9], plan + r * 9 + 1, c);
+    for (int r = 0; r < n; r++)
+        for (int e = 0; e < 3 * NF; e++) b_init_item(P, plan[r * 9], e);
+}
 double hc_dtcomp(const bh_params* Pp, const bh_pool* pool, double cfl) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     double best = DBL_BIG;

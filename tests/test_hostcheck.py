@@ -143,3 +143,90 @@ def test_refined_quilt_ghost_waves_bitwise():
     dt = hk.L.hc_step(C.byref(hk.P), C.byref(pool), 0.4, _d(flat), _d(off), len(waves))
     assert dt == orc.step(hp, 0.4)
     assert eq(hh.U, hp.U) and eq(hh.W, hp.W)
+
+
+def _hc_regrid(hk, hp, quilt, flags=None):
+    """bhgpu's device regrid sequence with the host-built kernel items:
+    flags, the quilt's plan, refine and ccrstr on the extended pool, the
+    kept patches."""
+    if flags is None:
+        pool = hk.pool(hp)
+        flags = np.zeros(hp.npatch, np.uint8)
+        hk.L.hc_regrid_flags(C.byref(hk.P), C.byref(pool), _d(np.ascontiguousarray(hp.lvl, np.int32)), _d(flags))
+    plan = quilt.regrid(flags)
+    ext = oracle.HostPool({"pgeo": plan.ext_pgeo, "lvl": np.zeros(plan.n_ext, np.int32),
+                           "ijk": np.zeros((plan.n_ext, 3), np.int32), "leaf": np.zeros(plan.n_ext, np.uint8),
+                           "nbr": np.zeros((plan.n_ext, 6, 2), np.int32)})
+    for name in ("U", "W", "dU", "F", "Bf", "EMF"):
+        getattr(ext, name)[:plan.n_old] = getattr(hp, name)
+    pool = hk.pool(ext)
+    hk.L.hc_geometry(C.byref(pool))
+    for rows, fn in ((plan.refined, "hc_refine"), (plan.flattened, "hc_ccrstr")):
+        if rows:
+            r = np.ascontiguousarray([[p] + kids for p, kids in rows], np.int32)
+            hk.call(fn, C.byref(pool), _d(r), C.c_int(len(rows)))
+    new = oracle.HostPool(quilt.tables())
+    for name in ("U", "W", "dU", "F", "Bf", "EMF", "rth"):
+        getattr(new, name)[:] = getattr(ext, name)[plan.keep]
+    return new, plan, flags
+
+
+def test_regrid_items_bitwise():
+    """The regrid kernels' items (flags, refine + B_init, ccrstr + B_init)
+    built for the host equal the oracle bit for bit: refinement of the
+    floor state around a Schwarzschild hole, and a refined patch of the
+    magnetised box flattened again."""
+    import copy
+    from helpers import oracle_regrid
+    lo, hi = [-6.0] * 3, [6.0] * 3
+    q = Quilt(lo, hi, 2)
+    orc = oracle.Oracle(1.0, 0.0, 0.0, GAMMA, limiter=1)
+    hk = HostKernels(1.0, 0.0, 0.0, GAMMA, 1)
+    hp = oracle.HostPool(q.tables())
+    orc.geometry(hp)
+    rf = 1.0 / np.power(np.sqrt(np.maximum(hp.rth[:, 0], 1e-10)), 3.0)    # amrtree::pvfs, the floor state
+    hp.W[:, 0] = 1e-7 * rf
+    hp.W[:, 1] = 1e-5 * rf
+    for p in range(hp.npatch):
+        hp.U[p] = orc.ptoc(hp.W[p], hp.rth[p, 0], hp.rth[p, 1])[0]
+    qh = copy.deepcopy(q)
+    ho, plan_o = oracle_regrid(orc, hp, q)
+    hh, plan_h, flags = _hc_regrid(hk, hp, qh)
+    assert plan_o.refined == plan_h.refined and len(plan_h.refined) == 8
+    assert eq(ho.U, hh.U) and eq(ho.W, hh.W) and eq(ho.Bf, hh.Bf)
+
+    q, orc, hp = box_case(2, seed=5, periodic=False, lim=1)
+    hk = HostKernels(0.0, 0.0, 0.0, GAMMA, 1)
+    f = np.zeros(8, np.uint8); f[5] = 1
+    qh = copy.deepcopy(q)
+    hh, _, _ = _hc_regrid(hk, hp, qh, f)
+    orig = orc.regrid_flags
+    orc.regrid_flags = lambda pool: f
+    ho, _ = oracle_regrid(orc, hp, q)
+    orc.regrid_flags = orig
+    assert eq(ho.U, hh.U) and eq(ho.W, hh.W) and eq(ho.Bf, hh.Bf)
+    orc.ghosts(ho); orc.ghosts(hh)
+    qh2 = copy.deepcopy(q)
+    ho2, plan_o = oracle_regrid(orc, ho, q)
+    hh2, plan_h, flags = _hc_regrid(hk, hh, qh2)
+    assert plan_o.flattened == plan_h.flattened == [(5, list(range(8, 16)))]
+    assert eq(ho2.U, hh2.U) and eq(ho2.W, hh2.W) and eq(ho2.Bf, hh2.Bf)
+
+
+def test_b_init_indices_stay_in_the_patch():
+    """patch::B_init's cell indices, including the out-of-range k = -3 and
+    k = 18 of its z-face branch, stay within a patch's 8000 cells."""
+    from bhgpu.mesh import cell_index
+    G, B = 2, 16
+    idx = []
+    for i in range(-G, B + G + 1):
+        for j in range(-G, B + G):
+            for k in range(-G, B + G):
+                idx += [cell_index(i - 1, j, k), cell_index(i, j, k)] if -G < i < B + G else \
+                       [cell_index(i, j, k)] if i == -G else [cell_index(i - 1, j, k)]
+    for i in range(-G, B + G):
+        for j in range(-G, B + G):
+            for k in range(-G, B + G + 1):
+                idx += [cell_index(i, j, k - 1), cell_index(i, j, k)] if -G < k < B + G else \
+                       [cell_index(i, j, k)] if i == -G else [cell_index(i, j, k - 1)]
+    assert min(idx) >= 0 and max(idx) < 8000
