@@ -162,7 +162,8 @@ class Oracle:
         seed = object.__getattribute__(self, "__dict__").get("noise_seed")
         if seed is not None and name in ("metric", "ptoc", "ctop", "hlld", "geometry", "reconfp_all", "fluxcomp",
                                          "emfcomp", "bfupdate", "f2cb", "ct", "div_source", "ghosts", "prims",
-                                         "update", "rkstg", "floors", "dtcomp", "step", "maxdivb"):
+                                         "update", "rkstg", "floors", "dtcomp", "step", "maxdivb",
+                                         "regrid_flags", "b_init", "refine_data", "ccrstr"):
             object.__getattribute__(self, "lib").orc_set_noise_seed(seed)
         return object.__getattribute__(self, name)
 

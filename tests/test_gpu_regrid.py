@@ -24,15 +24,36 @@ def tree_for(q, M, a, lim):
                          quilt=copy.deepcopy(q), init_floor=False)
 
 
-def check_same(tree, q, hp):
+def noise_envelope(hp_in, q_in, M, a, lim, ref_out, seeds=(1, 2, 3)):
+    """Per field, the largest relative L-infinity change of the oracle's
+    regrid result when every libm result carries one-ulp noise (three noise
+    patterns): the band in which the reference's own answer is defined.
+    Floor-state tau is a difference of terms ~1e5 times larger than itself,
+    so it moves by ~1e-11 under that noise."""
+    env = {}
+    for s in seeds:
+        orc = oracle.Oracle(M, a, 0.0, GAMMA, limiter=lim, noise=True, seed=s)
+        hp, _ = oracle_regrid(orc, hp_in.copy(), copy.deepcopy(q_in))
+        for name, arr, fields in (("U", hp.U, None), ("W", hp.W, PRIMS), ("Bf", hp.Bf, {"B": [0, 1, 2]})):
+            d = field_linf(arr, getattr(ref_out, name), fields) if fields else field_linf(arr, ref_out.U)
+            for k, v in d.items():
+                env[(name, k)] = max(env.get((name, k), 0.0), v)
+    return env
+
+
+def check_same(tree, q, hp, env=None):
+    """Same quilt; U, W, face B within 1e-12 per field, or within 8x the
+    noisy-libm envelope where that is wider."""
     T, G = q.tables(), tree.quilt.tables()
     for k in ("pgeo", "lvl", "ijk", "leaf", "nbr"):
         assert np.array_equal(T[k], G[k]), k
     U, W, Bf = (x.cpu().numpy() for x in (tree.U, tree.W, tree.Bf))
     assert same_nan(U, hp.U) and same_nan(W, hp.W)
-    assert max(field_linf(U, hp.U).values()) <= 1e-12
-    assert max(field_linf(W, hp.W, PRIMS).values()) <= 1e-12
-    assert max(field_linf(Bf, hp.Bf, {"B": [0, 1, 2]}).values()) <= 1e-12
+    for name, d in (("U", field_linf(U, hp.U)), ("W", field_linf(W, hp.W, PRIMS)),
+                    ("Bf", field_linf(Bf, hp.Bf, {"B": [0, 1, 2]}))):
+        for k, v in d.items():
+            bound = max(1e-12, 8 * env.get((name, k), 0.0)) if env else 1e-12
+            assert v <= bound, (name, k, v, bound)
 
 
 def floor_state(q, orc):
@@ -56,9 +77,10 @@ def test_regrid_refinement_near_the_horizon():
     for n_expect in (72, 584):
         tree.load(U=hp.U, W=hp.W, Bf=hp.Bf)
         plan = tree.regrid()
+        hp_in, q_in = hp.copy(), copy.deepcopy(q)
         hp, plan_o = oracle_regrid(orc, hp, q)
         assert plan.refined == plan_o.refined and len(q) == n_expect == tree.npatch
-        check_same(tree, q, hp)
+        check_same(tree, q, hp, noise_envelope(hp_in, q_in, 1.0, 0.0, 1, hp))
 
 
 def refined_box():
