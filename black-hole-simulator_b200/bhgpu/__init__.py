@@ -8,6 +8,7 @@ from .mesh import Quilt, BLOCK, GHOST, CPN, NC, NF, NE  # noqa: F401
 from .solver import (Metric, State, Conserved, hlld, AmrTree, RK2Integrator, StepGraph, DomainError,  # noqa: F401
                      BH_MINMOD, BH_VANLEER, BH_MC)
 from .pipeline import HostPipeline  # noqa: F401
+from .analysis import Analyser  # noqa: F401
 from . import configs  # noqa: F401
 
 __version__ = "0.1.0"

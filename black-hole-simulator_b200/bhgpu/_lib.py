@@ -29,7 +29,15 @@ class BhPool(C.Structure):
     _fields_ = [("npatch", C.c_int32), ("U", _vp), ("W", _vp), ("dU", _vp), ("F", _vp), ("Bf", _vp),
                 ("EMF", _vp), ("rth", _vp), ("pgeo", _vp), ("nbr", _vp), ("all", _vp),
                 ("leaves", _vp), ("nleaf", C.c_int32), ("err", _vp), ("leafmask", _vp), ("status", _vp),
-                ("aux", _vp)]
+                ("aux", _vp), ("Wd", _vp)]
+
+
+class BhAnalysisParams(C.Structure):
+    _fields_ = [("hrz", C.c_double), ("rs", C.c_double), ("rho_min_full", C.c_double),
+                ("rho_min_bundle", C.c_double)]
+
+
+BH_NQ = 20
 
 
 class BhError(RuntimeError):
@@ -68,6 +76,7 @@ def _load():
         "bh_floors": ([P, PP, _vp], C.c_int),
         "bh_dtcomp": ([P, PP, dbl, _vp, _vp], C.c_int),
         "bh_regrid_flags": ([P, PP, _vp, _vp, _vp], C.c_int),
+        "bh_analysis": ([P, PP, C.POINTER(BhAnalysisParams), _vp, _vp, _vp], C.c_int),
         "bh_refine": ([P, PP, _vp, i32, _vp], C.c_int),
         "bh_ccrstr": ([P, PP, _vp, i32, _vp], C.c_int),
         "bh_b_init": ([P, PP, _vp, i32, _vp], C.c_int),

@@ -184,6 +184,8 @@ class AmrTree:
         self.F = torch.zeros((n, 3, 8, NF), dtype=f64, device=d)
         self.Bf = torch.zeros((n, 3, NF), dtype=f64, device=d)
         self.EMF = torch.zeros((n, 3, NE), dtype=f64, device=d)
+        # derived fields (lor, p, h, b2) of the primitives floors and regrid leave
+        self.Wd = torch.zeros((n, 4, NC), dtype=f64, device=d)
         self.err = torch.zeros(1, dtype=torch.int32, device=d)
         self.dt = torch.zeros(1, dtype=f64, device=d)
         self._bind()
@@ -217,7 +219,8 @@ class AmrTree:
         self.waves = torch.as_tensor(np.concatenate(waves) if waves else np.zeros(0, np.int32), device=d)
         self.pool = BhPool(n, _p(self.U), _p(self.W), _p(self.dU), _p(self.F), _p(self.Bf), _p(self.EMF),
                            _p(self.rth), _p(self.pgeo), _p(self.nbr), _p(self.all), _p(self.leaves),
-                           len(leaves), _p(self.err), _p(self.leafmask), _p(self.status), _p(self.aux))
+                           len(leaves), _p(self.err), _p(self.leafmask), _p(self.status), _p(self.aux),
+                           _p(self.Wd))
         check(lib.bh_geometry(C.byref(self.pool), _stream()), "patch::cell_init")
 
     # ---- AMR -------------------------------------------------------------
@@ -246,12 +249,12 @@ class AmrTree:
 
         def ext(t):
             return torch.cat([t, t.new_zeros((grow,) + tuple(t.shape[1:]))]) if grow else t
-        U, W, dU, F, Bf, EMF = (ext(x) for x in (self.U, self.W, self.dU, self.F, self.Bf, self.EMF))
+        U, W, dU, F, Bf, EMF, Wd = (ext(x) for x in (self.U, self.W, self.dU, self.F, self.Bf, self.EMF, self.Wd))
         rth = torch.zeros((plan.n_ext, 2, NC), dtype=torch.float64, device=d)
         pgeo = torch.as_tensor(plan.ext_pgeo, device=d)
         all_ = torch.arange(plan.n_ext, dtype=torch.int32, device=d)
         pool = BhPool(plan.n_ext, _p(U), _p(W), _p(dU), _p(F), _p(Bf), _p(EMF), _p(rth), _p(pgeo), None,
-                      _p(all_), None, 0, _p(self.err), None, None, None)
+                      _p(all_), None, 0, _p(self.err), None, None, None, _p(Wd))
         s = _stream()
         check(lib.bh_geometry(C.byref(pool), s), "patch::cell_init")
         if plan.refined:
@@ -261,8 +264,8 @@ class AmrTree:
             rows = torch.as_tensor(np.array([[p] + kids for p, kids in plan.flattened], np.int32), device=d)
             check(lib.bh_ccrstr(C.byref(P), C.byref(pool), _p(rows), len(plan.flattened), s), "amrtree::ccrstr")
         keep = torch.as_tensor(plan.keep, device=d)
-        self.U, self.W, self.dU, self.F, self.Bf, self.EMF = (
-            x.index_select(0, keep).contiguous() for x in (U, W, dU, F, Bf, EMF))
+        self.U, self.W, self.dU, self.F, self.Bf, self.EMF, self.Wd = (
+            x.index_select(0, keep).contiguous() for x in (U, W, dU, F, Bf, EMF, Wd))
         self._bind()
         if check_domain:
             self.check()
@@ -391,8 +394,8 @@ class AmrTree:
         return t
 
     # ---- state exchange --------------------------------------------------
-    def load(self, U=None, W=None, Bf=None, dU=None):
-        for name, x in (("U", U), ("W", W), ("Bf", Bf), ("dU", dU)):
+    def load(self, U=None, W=None, Bf=None, dU=None, Wd=None):
+        for name, x in (("U", U), ("W", W), ("Bf", Bf), ("dU", dU), ("Wd", Wd)):
             if x is not None:
                 getattr(self, name).copy_(torch.as_tensor(np.asarray(x), dtype=torch.float64))
 

@@ -119,6 +119,10 @@ int bh_ccrstr(const bh_params* P, const bh_pool* pool, const int32_t* plan, int3
 int bh_b_init(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
     BH_DISPATCH(P, b_init(P, pool, patches, n, stream));
 }
+int bh_analysis(const bh_params* P, const bh_pool* pool, const bh_analysis_params* A, double* partial,
+                double* out, void* stream) {
+    BH_DISPATCH(P, analysis(P, pool, A, partial, out, stream));
+}
 int bh_dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
     BH_DISPATCH(P, dtcomp(P, pool, cfl, dt_dev, stream));
 }

@@ -31,9 +31,16 @@ struct Pool {               // kernel-side view of bh_pool
     const uint8_t* leafmask;
     uint8_t* status;
     double* aux;
+    double* Wd;
 };
 inline Pool pool_of(const bh_pool* p) {
-    return Pool{p->U, p->W, p->dU, p->F, p->Bf, p->EMF, p->rth, p->pgeo, p->nbr, p->err, p->leafmask, p->status, p->aux};
+    return Pool{p->U, p->W, p->dU, p->F, p->Bf, p->EMF, p->rth, p->pgeo, p->nbr, p->err, p->leafmask, p->status,
+                p->aux, p->Wd};
+}
+// the derived fields lor, p, h, b2 of a cell's primitives (pool->Wd)
+BH_HD inline void store_derived(const Pool& P, int p, int l, double lor, double pr, double h, double b2) {
+    double* d = P.Wd + (size_t)p * 4 * NC;
+    d[l] = lor; d[NC + l] = pr; d[2 * NC + l] = h; d[3 * NC + l] = b2;
 }
 
 BH_HD inline double* Uv(const Pool& P, int p, int v) { return P.U + ((size_t)p * 8 + v) * NC; }
@@ -101,13 +108,33 @@ static constexpr EdgeCells hEdgeCells = EdgeCells();      // host copy
 
 // W = pvfs(r) with the cell's B kept; U = ptoc(W) (integrator.cpp:211-218,
 // grid.cpp:484-487, grid.cpp:349-353)
-BH_HD inline void floor_reset(const KP& k, const Pool& P, int p, int l, Prim& w, Cons& u) {
+BH_HD inline void floor_reset(const KP& k, const Pool& P, int p, int l, Prim& w, Cons& u, PtocOut* po = nullptr) {
     double r = rr(P, p, l), th = tt(P, p, l);
     pvfs(r, w.rho, w.eps);
     w.v[0] = w.v[1] = w.v[2] = 0.0;
     Met mc;
     met_comp(k.tree, r, th, mc);
-    if (!ptoc(k.gamma, mc, w, u)) flag(P.err, BH_ERR_DOMAIN);
+    if (!ptoc(k.gamma, mc, w, u, po)) flag(P.err, BH_ERR_DOMAIN);
+}
+
+// ctop with the fallback of refine and ccrstr (grid.cpp:636-645, 694-703),
+// recording the derived fields of the primitives it leaves in pool->Wd
+BH_HD inline void recover_keep_derived(const KP& k, const Pool& P, int p, int l, Prim& w, Cons& u) {
+    Met mc;
+    met_comp(k.tree, rr(P, p, l), tt(P, p, l), mc);
+    Prim pv;
+    bool dom = false;
+    CtopOut co;
+    int ok = ctop(k.gamma, k.maxiter, k.tol, mc, u, pv, dom, P.Wd ? &co : nullptr);
+    if (dom) flag(P.err, BH_ERR_DOMAIN);
+    if (ok) {
+        w = pv;
+        if (P.Wd) store_derived(P, p, l, co.lor, co.p, co.h, co.b2);
+        return;
+    }
+    PtocOut po;
+    floor_reset(k, P, p, l, w, u, &po);
+    if (P.Wd) store_derived(P, p, l, po.lor, po.p, po.h, po.b2);
 }
 
 // ctop of one cell with the tree metric, rkstg's fallback on failure
@@ -749,24 +776,34 @@ BH_HD inline void floors_item(const KP& kp, const Pool& P, int p, int c) {
     Prim w;
     load_prim(P, p, l, w);
     bool wrote = false;
+    double d4[4];           // derived fields of the primitives written (pool->Wd)
     if (!bhl) {
         Met mc;
         met_comp(kp.tree, r, th, mc);
         Prim pv;
         bool dom = false;
-        int ok = ctop(kp.gamma, kp.maxiter, kp.tol, mc, u, pv, dom);
+        CtopOut co;
+        int ok = ctop(kp.gamma, kp.maxiter, kp.tol, mc, u, pv, dom, P.Wd ? &co : nullptr);
         if (dom) flag(P.err, BH_ERR_DOMAIN);
         bhl = !ok;
-        if (!bhl && !(pv.rho <= 0.0 || pv.eps <= 0.0)) { w = pv; wrote = true; }
+        if (!bhl && !(pv.rho <= 0.0 || pv.eps <= 0.0)) {
+            w = pv; wrote = true;
+            d4[0] = co.lor; d4[1] = co.p; d4[2] = co.h; d4[3] = co.b2;
+        }
     }
     double frho, feps;
     pvfs(r, frho, feps);
     if (bhl || w.rho <= frho) {
-        floor_reset(kp, P, p, l, w, u);
+        PtocOut po;
+        floor_reset(kp, P, p, l, w, u, P.Wd ? &po : nullptr);
         store_cons(P, p, l, u);
         wrote = true;
+        d4[0] = po.lor; d4[1] = po.p; d4[2] = po.h; d4[3] = po.b2;
     }
-    if (wrote) store_prim(P, p, l, w);
+    if (wrote) {
+        store_prim(P, p, l, w);
+        if (P.Wd) store_derived(P, p, l, d4[0], d4[1], d4[2], d4[3]);
+    }
 }
 
 // ---- AMR regrid (grid.cpp:573-835) ---------------------------------------
@@ -865,8 +902,7 @@ BH_HD inline void refine_item(const KP& kp, const Pool& P, int parent, int child
     int lf = lindx(i, j, k);
     Prim w;
     load_prim(P, child, lf, w);
-    bool dirty = false;
-    recover_cell(kp, P, child, lf, w, cu, dirty);
+    recover_keep_derived(kp, P, child, lf, w, cu);
     store_cons(P, child, lf, cu);
     store_prim(P, child, lf, w);
 }
@@ -904,10 +940,77 @@ BH_HD inline void ccrstr_item(const KP& kp, const Pool& P, int parent, const int
     int l = lindx(pi, pj, pk);
     Prim w;
     load_prim(P, parent, l, w);
-    bool dirty = false;
-    recover_cell(kp, P, parent, l, w, cu, dirty);
+    recover_keep_derived(kp, P, parent, l, w, cu);
     store_cons(P, parent, l, cu);
     store_prim(P, parent, l, w);
+}
+
+// ---- analysis::analyser (data/quantitatives.cpp:17-199) -------------------
+// The integrands of the diagnostics at interior cell c of leaf patch p,
+// times the cell volume, added to acc[BH_NQ]; surface integrals take the
+// cells within one cell diagonal of their radius (surf_int, :61-79).  The
+// cell's metric (the cell metric, cell.hpp:25) gives sqrt(-g), lapse, shift,
+// g_0mu and gamma_i2.
+struct AParams { double hrz, rs, rho_min_full, rho_min_bundle; };
+BH_HD inline void analysis_cell(const KP& kp, const Pool& P, int p, int c, const AParams& A, double acc[BH_NQ]) {
+    int i = c / 256, j = (c / 16) % 16, k = c % 16;
+    int l = lindx(i, j, k);
+    const double* g = P.pgeo + 6 * p;
+    double dx = g[3], dy = g[4], dz = g[5];
+    double xc = g[0] + (i + 0.5) * g[3], yc = g[1] + (j + 0.5) * g[4], zc = g[2] + (k + 0.5) * g[5];
+    double vol = dx * dy * dz;
+    double r = rr(P, p, l), th = tt(P, p, l);
+    Prim w;
+    load_prim(P, p, l, w);
+    const double* d = P.Wd + (size_t)p * 4 * NC;
+    double lor = d[l], pr = d[NC + l], h = d[2 * NC + l], b2 = d[3 * NC + l];
+    double D = Uv(P, p, 0)[l], tau = Uv(P, p, 4)[l], S0 = Uv(P, p, 1)[l], S1 = Uv(P, p, 2)[l];
+    MetSrc m;
+    met_src(kp.cell, r, th, m);
+    double sg = m.sqrtdetg;
+    double R = sqrt(xc * xc + yc * yc);
+    double vr = (xc * w.v[0] + yc * w.v[1] + zc * w.v[2]) / r;                    // val_vr :24-26
+    double vphi = (R < 1e-10) ? 0.0 : (xc * w.v[1] - yc * w.v[0]) / (R * R);     // val_vphi :27-31
+    double Br = (xc * w.B[0] + yc * w.B[1] + zc * w.B[2]) / r;                    // val_Br :33-35
+    double Bphi = (R < 1e-10) ? 0.0 : (xc * w.B[1] - yc * w.B[0]) / (R * R);     // val_Bphi :36-40
+    double shell = sqrt(dx * dx + dy * dy + dz * dz);
+    bool on_h = !(fabs(r - A.hrz) > shell), on_s = !(fabs(r - A.rs) > shell);
+    acc[BH_Q_MASS] += D * vol;
+    acc[BH_Q_ENERGY] += (tau + D) * vol;
+    acc[BH_Q_LPOL] += (xc * S1 - yc * S0) * vol;
+    if (on_h) {
+        acc[BH_Q_MDOT] += (-w.rho * lor * vr * sg) * vol;
+        acc[BH_Q_EDOT] += (-((tau + D) * (m.alpha * vr - (m.beta[0] * xc + m.beta[1] * yc + m.beta[2] * zc) / r))) * vol;
+        double wh = w.rho * h + b2;
+        acc[BH_Q_LDOT] += ((wh * lor * lor * vr * vphi - Br - Bphi) * sg) * vol;
+        acc[BH_Q_PHIB] += (fabs(Br) * sg) * vol;
+        // L_BZ (:135-155): Blow[i] is assigned inside the j loop, so gamma_i2 B_2 survives
+        double Blow[3] = {m.g[1][3] * w.B[2], m.g[2][3] * w.B[2], m.g[3][3] * w.B[2]};
+        double Bv = 0.0;
+        for (int a = 0; a < 3; a++) Bv += Blow[a] * w.v[a];
+        double bt = lor * Bv / m.alpha;
+        double br = (Br + m.alpha * bt * lor * vr) / lor;
+        double bt_ = m.g[0][0] * bt + m.g[0][1] * br + m.g[0][3] * (Bphi * lor);
+        double ur = lor * vr;
+        double ut_ = -m.alpha * lor;
+        acc[BH_Q_LBZ] += (-(b2 * ur * ut_ - br * bt_) * sg) * vol;
+    }
+    acc[BH_Q_MAGE] += (0.5 * b2 * sg) * vol;
+    acc[BH_Q_THERME] += (w.rho * w.eps * sg) * vol;
+    acc[BH_Q_PNUM] += (pr * sg) * vol;
+    acc[BH_Q_PDEN] += (0.5 * b2 * sg) * vol;
+    double stress = (w.rho * h * vr * vphi - Br * Bphi) * sg;
+    double ptot = (pr + 0.5 * b2) * sg;
+    acc[BH_Q_ASTRESS] += (w.rho < A.rho_min_full ? 0.0 : stress) * vol;
+    acc[BH_Q_APRESS] += (w.rho < A.rho_min_full ? 0.0 : ptot) * vol;
+    acc[BH_Q_ASTRESS_B] += (w.rho < A.rho_min_bundle ? 0.0 : stress) * vol;
+    acc[BH_Q_APRESS_B] += (w.rho < A.rho_min_bundle ? 0.0 : ptot) * vol;
+    acc[BH_Q_MAXW] += (w.rho < A.rho_min_full ? 0.0 : -Br * Bphi * sg) * vol;
+    acc[BH_Q_REYN] += (w.rho < A.rho_min_full ? 0.0 : w.rho * h * lor * lor * vr * vphi * sg) * vol;
+    if (on_s) {
+        acc[BH_Q_HNUM] += (fabs(zc) * w.rho * sg) * vol;
+        acc[BH_Q_HDEN] += (w.rho * sg) * vol;
+    }
 }
 
 // ---- dtcomp (integrator.cpp:156-189): one cell's CFL candidate -----------

@@ -151,6 +151,38 @@ __global__ void k_b_init_rows(Pool P, const int32_t* plan, int col0, int ncol) {
     b_init_item(P, plan[(blockIdx.y / ncol) * 9 + col0 + blockIdx.y % ncol], e);
 }
 
+// ---- analysis::analyser: one CTA per leaf patch sums its cells (each
+// thread a fixed stride of cells, then the warps in order), a second kernel
+// sums the patches in order: a fixed summation order, so reruns agree
+constexpr int ANL_TPB = 256;
+__global__ void __launch_bounds__(ANL_TPB) k_analysis(KP kp, Pool P, const int32_t* leaves, AParams A,
+                                                     double* partial) {
+    int p = leaves[blockIdx.x];
+    double acc[BH_NQ];
+    for (int q = 0; q < BH_NQ; q++) acc[q] = 0.0;
+    for (int c = threadIdx.x; c < N_INT; c += ANL_TPB) analysis_cell(kp, P, p, c, A, acc);
+    __shared__ double red[BH_NQ][ANL_TPB / 32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int q = 0; q < BH_NQ; q++) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[q][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < BH_NQ) {
+        double s = 0.0;
+        for (int w = 0; w < ANL_TPB / 32; w++) s += red[threadIdx.x][w];
+        partial[(size_t)blockIdx.x * BH_NQ + threadIdx.x] = s;
+    }
+}
+__global__ void k_analysis_sum(const double* partial, int n, double* out) {
+    int q = threadIdx.x;
+    if (q >= BH_NQ) return;
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += partial[(size_t)i * BH_NQ + q];
+    out[q] = s;
+}
+
 // constrans::maxdivB: one CTA per patch, max-reduction in shared memory
 __global__ void k_maxdivb(Pool P, double* out) {
     int p = blockIdx.x;
@@ -347,6 +379,15 @@ int b_init(const bh_params* P, const bh_pool* pool, const int32_t* patches, int3
     if (n == 0) return BH_OK;
     if (n > 65535) return BH_ERANGE;
     k_b_init<<<grid2(3 * NF, n), TPB, 0, S(stream)>>>(pool_of(pool), patches);
+    return launched();
+}
+int analysis(const bh_params* P, const bh_pool* pool, const bh_analysis_params* A, double* partial, double* out,
+             void* stream) {
+    if (!P || bad_pool(pool) || !A || !partial || !out || !pool->Wd) return BH_EINVAL;
+    if (pool->nleaf == 0) return BH_OK;
+    AParams ap{A->hrz, A->rs, A->rho_min_full, A->rho_min_bundle};
+    k_analysis<<<pool->nleaf, ANL_TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves, ap, partial);
+    k_analysis_sum<<<1, 32, 0, S(stream)>>>(partial, pool->nleaf, out);
     return launched();
 }
 int dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {

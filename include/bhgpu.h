@@ -96,6 +96,10 @@ typedef struct bh_pool {
                             computed once per cell instead of once per face that
                             reads the cell; NULL computes them per face.  Either
                             way the fluxes are the same bit for bit. */
+    double *Wd;          /* [np][4][8000] lor, p, h, b2 of the primitives as floors,
+                            refine and ccrstr leave them (the derived fields of the
+                            reference's prim, prim.hpp:21-25; read by bh_analysis);
+                            NULL: not kept */
 } bh_pool;
 
 /* ---- library --------------------------------------------------------------- */
@@ -205,6 +209,26 @@ int bh_refine(const bh_params *P, const bh_pool *pool, const int32_t *plan, int3
 int bh_ccrstr(const bh_params *P, const bh_pool *pool, const int32_t *plan, int32_t n, void *stream);
 /* patch::B_init (:207-250) on the n listed patches */
 int bh_b_init(const bh_params *P, const bh_pool *pool, const int32_t *patches, int32_t n, void *stream);
+
+/* ---- L3 analysis (data/quantitatives.cpp) ------------------------------- */
+/* Raw integrals of analysis::analyser over the leaf patches' interior cells:
+ * vol_int (:44-59) and surf_int (:61-79, cells within one cell diagonal of
+ * the radius) of each integrand times the cell volume, on the state a step
+ * (floors) or a regrid left -- the derived fields come from pool->Wd.  The
+ * sums run in a fixed order on the device (per patch, then over patches), not
+ * the reference's serial order.  out[BH_NQ] in this order: */
+enum { BH_Q_MASS, BH_Q_ENERGY, BH_Q_LPOL, BH_Q_MDOT, BH_Q_EDOT, BH_Q_LDOT, BH_Q_PHIB, BH_Q_MAGE,
+       BH_Q_THERME, BH_Q_LBZ, BH_Q_PNUM, BH_Q_PDEN, BH_Q_ASTRESS, BH_Q_APRESS, BH_Q_ASTRESS_B,
+       BH_Q_APRESS_B, BH_Q_MAXW, BH_Q_REYN, BH_Q_HNUM, BH_Q_HDEN, BH_NQ };
+typedef struct bh_analysis_params {
+    double hrz;             /* surface radius of the accretion integrals (r_horizon, :19-22) */
+    double rs;              /* surface radius of Hscal (batch_: 10 M)                   */
+    double rho_min_full;    /* density cut of alpha_ss / maxreyn in batch_ (0.01)        */
+    double rho_min_bundle;  /* density cut of alpha_ss in bundle_ (0.005)                */
+} bh_analysis_params;
+/* partial: device scratch [nleaf][BH_NQ]; out: device [BH_NQ]; needs pool->Wd */
+int bh_analysis(const bh_params *P, const bh_pool *pool, const bh_analysis_params *A, double *partial,
+                double *out, void *stream);
 
 /* ---- L3 integrator ------------------------------------------------------ */
 /* rk2integrator::dtcomp (solver/integrator.cpp:156-189): *dt_dev = CFL step */

@@ -21,6 +21,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 NC, NF, NE, NMC = 8000, 8400, 8820, 120
+NQ = 20   # raw integrals of orc_analysis (ORC_NQ)
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -43,7 +44,7 @@ class OrcParams(C.Structure):
 class OrcPool(C.Structure):
     _fields_ = [("npatch", C.c_int32), ("U", _dp), ("W", _dp), ("dU", _dp), ("F", _dp),
                 ("Bf", _dp), ("EMF", _dp), ("rth", _dp), ("pgeo", _dp), ("nbr", _ip),
-                ("leaf", _u8p), ("lvl", _ip), ("ijk", _ip)]
+                ("leaf", _u8p), ("lvl", _ip), ("ijk", _ip), ("Wd", _dp)]
 
 
 class HostPool:
@@ -59,6 +60,7 @@ class HostPool:
         self.Bf = np.zeros((n, 3, NF))
         self.EMF = np.zeros((n, 3, NE))
         self.rth = np.zeros((n, 2, NC))
+        self.Wd = np.zeros((n, 4, NC))      # lor, p, h, b2 as floors / regrid set them
         self.pgeo = np.ascontiguousarray(tables["pgeo"], np.float64)
         self.nbr = np.ascontiguousarray(tables["nbr"], np.int32)
         self.leaf = np.ascontiguousarray(tables["leaf"], np.uint8)
@@ -75,7 +77,7 @@ class HostPool:
         return OrcPool(self.npatch, _ptr(self.U), _ptr(self.W), _ptr(self.dU), _ptr(self.F),
                        _ptr(self.Bf), _ptr(self.EMF), _ptr(self.rth), _ptr(self.pgeo),
                        _ptr(self.nbr, _ip), _ptr(self.leaf, _u8p), _ptr(self.lvl, _ip),
-                       _ptr(self.ijk, _ip))
+                       _ptr(self.ijk, _ip), _ptr(self.Wd))
 
 
 class DomainError(ValueError):
@@ -145,6 +147,7 @@ class Oracle:
         L.orc_step.argtypes = [PP, PO, C.c_double, _dp]
         L.orc_maxdivb_all.argtypes = [PO, _dp]
         L.orc_regrid_flags.argtypes = [PO, C.c_int, C.c_int]
+        L.orc_analysis.argtypes = [PP, PO, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp]
         L.orc_b_init.argtypes = [PO, C.c_int]
         L.orc_refine_data.argtypes = [PP, PO, C.c_int, _ip]
         L.orc_ccrstr.argtypes = [PP, PO, C.c_int, _ip]
@@ -258,6 +261,15 @@ class Oracle:
         self._chk(self.lib.orc_step(C.byref(self.P), C.byref(s), cfl, C.byref(dt)))
         return dt.value
 
+    def analysis(self, pool, hrz, rs, rho_min_full=0.01, rho_min_bundle=0.005):
+        """Raw integrals of analysis::analyser (quantitatives.cpp), summed in
+        the reference's order, in the ORC_Q_* order of bh_oracle.h, and the
+        sums of the absolute values of their terms."""
+        out = np.zeros(NQ); absout = np.zeros(NQ); s = pool.cstruct()
+        self.lib.orc_analysis(C.byref(self.P), C.byref(s), hrz, rs, rho_min_full, rho_min_bundle, _ptr(out),
+                              _ptr(absout))
+        return out, absout
+
     # AMR regrid pieces (grid.cpp:573-835)
     def regrid_flags(self, pool):
         """Per-patch flags of amrtree::regrid's cell loop (bit 0 refine, bit 1
@@ -312,6 +324,9 @@ class RefSolver:
             L.ref_refine.argtypes = [v, C.c_int]
             L.ref_flatten.argtypes = [v, C.c_int]
             L.ref_regrid.argtypes = [v]
+            L.ref_derived.argtypes = [v, _dp]
+            L.ref_batch.argtypes = [v, C.c_double, _dp]
+            L.ref_bundle.argtypes = [v, C.c_double, _dp]
             L.ref_metric_batch.argtypes = [C.c_double] * 3 + [_dp, _dp, C.c_int64, _dp]
             L.ref_ptoc_batch.argtypes = [C.c_double] * 4 + [_dp, _dp, _dp, C.c_int64, _dp, _dp]
             L.ref_ctop_batch.argtypes = [C.c_double] * 4 + [_dp, _dp, _dp, C.c_int64, _dp, _dp, _ip]
@@ -384,6 +399,15 @@ class RefSolver:
     def regrid(self):
         """amrtree::regrid; the patch count changes (npatch, patch_info)."""
         self._chk(self.lib().ref_regrid(self.h))
+
+    def derived(self):
+        out = np.zeros((self.npatch, 4, NC)); self.lib().ref_derived(self.h, _ptr(out)); return out
+
+    def batch(self, t):
+        out = np.zeros(17); self.lib().ref_batch(self.h, t, _ptr(out)); return out
+
+    def bundle(self, t):
+        out = np.zeros(6); self.lib().ref_bundle(self.h, t, _ptr(out)); return out
 
     # stateless
     def metric(self, r, th):

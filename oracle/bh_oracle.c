@@ -1053,7 +1053,7 @@ static void gh_bndy(orc_pool *pool, int p, int dim, int side) {      /* :494-522
 }
 /* floor fallback used after a failed ctop in refine/prolong/rkstg:
  * W = pvfs with the cell's B kept, U = ptoc(W) */
-static int floor_reset(const orc_params *P, orc_pool *pool, int p, int l) {
+static int floor_reset_out(const orc_params *P, orc_pool *pool, int p, int l, prim *out) {
     double r = RP(pool, p)[l], th = TP(pool, p)[l];
     prim fl, cur;
     get_prim(pool, p, l, &cur);
@@ -1061,9 +1061,19 @@ static int floor_reset(const orc_params *P, orc_pool *pool, int p, int l) {
     for (int d = 0; d < 3; d++) fl.B[d] = cur.B[d];
     put_prim(pool, p, l, &fl);
     cons U;
-    if (ptoc_(P, &fl, r, th, &U)) return ORC_EDOMAIN;
+    if (ptoc_(P, &fl, r, th, &U)) return ORC_EDOMAIN;   /* ptoc sets fl's lor, p, h, b2 */
     put_cons(pool, p, l, &U);
+    if (out) *out = fl;
     return 0;
+}
+static int floor_reset(const orc_params *P, orc_pool *pool, int p, int l) {
+    return floor_reset_out(P, pool, p, l, 0);
+}
+/* the derived primitive fields a cell's W carries (prim.hpp:21-25) */
+static void put_derived(orc_pool *pool, int p, int l, const prim *pv) {
+    if (!pool->Wd) return;
+    double *d = pool->Wd + (size_t)p * 4 * NC;
+    d[l] = pv->lor; d[NC + l] = pv->p; d[2 * NC + l] = pv->h; d[3 * NC + l] = pv->b2;
 }
 static int gh_prolong(const orc_params *P, orc_pool *pool, int p, int nb, int dim, int side) { /* :427-492 */
     int pstart = (side == 1) ? BLK : -GH;
@@ -1229,8 +1239,11 @@ static int regrid_recover(const orc_params *P, orc_pool *pool, int p, int l) {
     memset(&pv, 0, sizeof(pv));
     int ok = ctop_(P, &U, RP(pool, p)[l], TP(pool, p)[l], &pv, P->maxiter, P->tol, 0, 0);
     if (ok < 0) return ORC_EDOMAIN;
-    if (ok) { put_prim(pool, p, l, &pv); return 0; }
-    return floor_reset(P, pool, p, l);
+    if (ok) { put_prim(pool, p, l, &pv); put_derived(pool, p, l, &pv); return 0; }
+    prim fl;
+    if (floor_reset_out(P, pool, p, l, &fl)) return ORC_EDOMAIN;
+    put_derived(pool, p, l, &fl);
+    return 0;
 }
 
 /* the cell data of amrtree::refine (:603-648): child h of parent p takes a
@@ -1327,16 +1340,132 @@ int orc_floors(const orc_params *P, orc_pool *pool, int p) {
                     bhl = !ok;
                     if (!bhl) {
                         int hl = !(pv.rho <= 0.0 || pv.eps <= 0.0);
-                        if (hl) put_prim(pool, p, l, &pv);
+                        if (hl) { put_prim(pool, p, l, &pv); put_derived(pool, p, l, &pv); }
                     }
                 }
                 prim fl;
                 pvfs_(P, r, &fl);
                 if (bhl || WP(pool, p, 0)[l] <= fl.rho) {
-                    if (floor_reset(P, pool, p, l)) return ORC_EDOMAIN;
+                    prim fo;
+                    if (floor_reset_out(P, pool, p, l, &fo)) return ORC_EDOMAIN;
+                    put_derived(pool, p, l, &fo);
                 }
             }
     return 0;
+}
+
+/* ======================================================================
+ * L3: analysis (data/quantitatives.cpp:17-247)
+ * ==================================================================== */
+typedef struct { double xc, yc, zc, r, th, dx, dy, dz, vol; prim W; cons U; } acell;
+static void acell_get(const orc_pool *pool, int p, int i, int j, int k, acell *c) {
+    const double *g = pool->pgeo + 6 * p;
+    int l = lindx(i, j, k);
+    c->dx = g[3]; c->dy = g[4]; c->dz = g[5];                 /* patch::cell_init, grid.cpp:154-157 */
+    c->xc = g[0] + (i + 0.5) * g[3]; c->yc = g[1] + (j + 0.5) * g[4]; c->zc = g[2] + (k + 0.5) * g[5];
+    c->vol = c->dx * c->dy * c->dz;
+    c->r = RP(pool, p)[l]; c->th = TP(pool, p)[l];
+    get_prim(pool, p, l, &c->W);
+    const double *d = pool->Wd + (size_t)p * 4 * NC;
+    c->W.lor = d[l]; c->W.p = d[NC + l]; c->W.h = d[2 * NC + l]; c->W.b2 = d[3 * NC + l];
+    get_cons(pool, p, l, &c->U);
+}
+static double val_vr(const acell *c) { return (c->xc * c->W.v[0] + c->yc * c->W.v[1] + c->zc * c->W.v[2]) / c->r; }
+static double val_vphi(const acell *c) {
+    double R = sqrt(c->xc * c->xc + c->yc * c->yc);
+    if (R < 1e-10) return 0.0;
+    return (c->xc * c->W.v[1] - c->yc * c->W.v[0]) / (R * R);
+}
+static double val_Br(const acell *c) { return (c->xc * c->W.B[0] + c->yc * c->W.B[1] + c->zc * c->W.B[2]) / c->r; }
+static double val_Bphi(const acell *c) {
+    double R = sqrt(c->xc * c->xc + c->yc * c->yc);
+    if (R < 1e-10) return 0.0;
+    return (c->xc * c->W.B[1] - c->yc * c->W.B[0]) / (R * R);
+}
+/* the integrand of quantity q at cell c, sg = sqrt(-g) of the cell's metric */
+static double aterm(int q, const acell *c, const mcomp *mc, double sg, double rho_min) {
+    switch (q) {
+    case ORC_Q_MASS: return c->U.D;                                               /* :83-87 */
+    case ORC_Q_ENERGY: return c->U.tau + c->U.D;                                  /* :88-92 */
+    case ORC_Q_LPOL: return c->xc * c->U.S[1] - c->yc * c->U.S[0];                /* :93-97 */
+    case ORC_Q_MDOT: return -c->W.rho * c->W.lor * val_vr(c) * sg;                /* :99-103 */
+    case ORC_Q_EDOT:                                                              /* :104-108 */
+        return -((c->U.tau + c->U.D) * (mc->alpha * val_vr(c) -
+                                        (mc->beta[0] * c->xc + mc->beta[1] * c->yc + mc->beta[2] * c->zc) / c->r));
+    case ORC_Q_LDOT: {                                                            /* :109-114 */
+        double w = c->W.rho * c->W.h + c->W.b2;
+        return (w * c->W.lor * c->W.lor * val_vr(c) * val_vphi(c) - val_Br(c) - val_Bphi(c)) * sg;
+    }
+    case ORC_Q_PHIB: return fabs(val_Br(c)) * sg;                                 /* :115-119 */
+    case ORC_Q_MAGE: return 0.5 * c->W.b2 * sg;                                   /* :125-129 */
+    case ORC_Q_THERME: return c->W.rho * c->W.eps * sg;                           /* :130-134 */
+    case ORC_Q_LBZ: {                                                             /* :135-155 */
+        double Blow[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) Blow[i] = mc->gam[i][j] * c->W.B[j];   /* assignment: j = 2 survives */
+        double Bv = 0.0;
+        for (int i = 0; i < 3; i++) Bv += Blow[i] * c->W.v[i];
+        double bt = c->W.lor * Bv / mc->alpha;
+        double br = (val_Br(c) + mc->alpha * bt * c->W.lor * val_vr(c)) / c->W.lor;
+        double bt_ = mc->g[0][0] * bt + mc->g[0][1] * br + mc->g[0][3] * (val_Bphi(c) * c->W.lor);
+        double ur = c->W.lor * val_vr(c);
+        double ut_ = -mc->alpha * c->W.lor;
+        return -(c->W.b2 * ur * ut_ - br * bt_) * sg;
+    }
+    case ORC_Q_PNUM: return c->W.p * sg;                                          /* :163-168 */
+    case ORC_Q_PDEN: return 0.5 * c->W.b2 * sg;
+    case ORC_Q_ASTRESS: case ORC_Q_ASTRESS_B:                                     /* :171-176 */
+        if (c->W.rho < rho_min) return 0.0;
+        return (c->W.rho * c->W.h * val_vr(c) * val_vphi(c) - val_Br(c) * val_Bphi(c)) * sg;
+    case ORC_Q_APRESS: case ORC_Q_APRESS_B:                                       /* :177-180 */
+        if (c->W.rho < rho_min) return 0.0;
+        return (c->W.p + 0.5 * c->W.b2) * sg;
+    case ORC_Q_MAXW:                                                              /* :184-187 */
+        if (c->W.rho < rho_min) return 0.0;
+        return -val_Br(c) * val_Bphi(c) * sg;
+    case ORC_Q_REYN:                                                              /* :188-191 */
+        if (c->W.rho < rho_min) return 0.0;
+        return c->W.rho * c->W.h * c->W.lor * c->W.lor * val_vr(c) * val_vphi(c) * sg;
+    case ORC_Q_HNUM: return fabs(c->zc) * c->W.rho * sg;                          /* :195-197 */
+    case ORC_Q_HDEN: return c->W.rho * sg;
+    default: return 0.0;
+    }
+}
+/* analyser::vol_int (:44-59) and surf_int (:61-79, r_surf >= 0): the sum of
+ * f * vol over the leaf patches' interior cells in quilt and i, j, k order */
+static double aint(const orc_params *P, const orc_pool *pool, int q, double r_surf, double rho_min,
+                   double *absint) {
+    double integral = 0.0, a = 0.0;
+    for (int p = 0; p < pool->npatch; p++) {
+        if (!pool->leaf[p]) continue;
+        for (int i = 0; i < BLK; i++)
+            for (int j = 0; j < BLK; j++)
+                for (int k = 0; k < BLK; k++) {
+                    acell c;
+                    acell_get(pool, p, i, j, k, &c);
+                    if (r_surf >= 0.0) {
+                        double shell = sqrt(c.dx * c.dx + c.dy * c.dy + c.dz * c.dz);
+                        if (fabs(c.r - r_surf) > shell) continue;
+                    }
+                    mcomp mc;
+                    mcomp_cell(P, c.r, c.th, &mc);
+                    double f = aterm(q, &c, &mc, mc.sqrtdetg, rho_min) * c.vol;
+                    integral += f;
+                    a += fabs(f);
+                }
+    }
+    if (absint) *absint = a;
+    return integral;
+}
+void orc_analysis(const orc_params *P, const orc_pool *pool, double hrz, double rs, double rho_min_full,
+                  double rho_min_bundle, double out[ORC_NQ], double out_abs[ORC_NQ]) {
+    for (int q = 0; q < ORC_NQ; q++) {
+        int surf = q == ORC_Q_MDOT || q == ORC_Q_EDOT || q == ORC_Q_LDOT || q == ORC_Q_PHIB || q == ORC_Q_LBZ ||
+                   q == ORC_Q_HNUM || q == ORC_Q_HDEN;
+        double rsurf = (q == ORC_Q_HNUM || q == ORC_Q_HDEN) ? rs : hrz;
+        double rmin = (q == ORC_Q_ASTRESS_B || q == ORC_Q_APRESS_B) ? rho_min_bundle : rho_min_full;
+        out[q] = aint(P, pool, q, surf ? rsurf : -1.0, rmin, out_abs ? out_abs + q : 0);
+    }
 }
 
 /* ======================================================================

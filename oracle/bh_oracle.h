@@ -75,6 +75,8 @@ typedef struct orc_pool {
     uint8_t *leaf;  /* [np]                                              */
     int32_t *lvl;   /* [np]                                              */
     int32_t *ijk;   /* [np][3]                                           */
+    double *Wd;     /* [np][4][NC] lor, p, h, b2 of the primitives that
+                       floors and regrid set (NULL: not kept)           */
 } orc_pool;
 
 /* ---- L0 physics ------------------------------------------------------ */
@@ -114,6 +116,17 @@ int  orc_regrid_flags(const orc_pool *pool, int p, int lvl);   /* bit 0 refine, 
 void orc_b_init(orc_pool *pool, int p);
 int  orc_refine_data(const orc_params *P, orc_pool *pool, int p, const int32_t child[8]);
 int  orc_ccrstr(const orc_params *P, orc_pool *pool, int p, const int32_t child[8]);
+
+/* ---- L3 analysis (data/quantitatives.cpp) ----------------------------- */
+/* the raw integrals of analysis::analyser over the leaf patches' interior
+ * cells, each summed in the reference's order; out[ORC_NQ] (ORC_Q_* below).
+ * hrz = horizon radius of surf_int, rs = Hscal's radius, rho_min_full and
+ * rho_min_bundle = the density cuts of batch_ (0.01) and bundle_ (0.005) */
+enum { ORC_Q_MASS, ORC_Q_ENERGY, ORC_Q_LPOL, ORC_Q_MDOT, ORC_Q_EDOT, ORC_Q_LDOT, ORC_Q_PHIB,
+       ORC_Q_MAGE, ORC_Q_THERME, ORC_Q_LBZ, ORC_Q_PNUM, ORC_Q_PDEN, ORC_Q_ASTRESS, ORC_Q_APRESS,
+       ORC_Q_ASTRESS_B, ORC_Q_APRESS_B, ORC_Q_MAXW, ORC_Q_REYN, ORC_Q_HNUM, ORC_Q_HDEN, ORC_NQ };
+void orc_analysis(const orc_params *P, const orc_pool *pool, double hrz, double rs, double rho_min_full,
+                  double rho_min_bundle, double out[ORC_NQ], double out_abs[ORC_NQ]);   /* out_abs: sum |f vol|, may be NULL */
 
 /* ---- L3 integrator ------------------------------------------------------ */
 int orc_dtcomp(const orc_params *P, const orc_pool *pool, double cfl, double *dt);

@@ -32,6 +32,7 @@
 #include "state.hpp"
 #include "hlld.hpp"
 #include "recon.hpp"
+#include "analysis.hpp"
 
 using namespace grid;
 
@@ -357,6 +358,31 @@ void ref_get(void* h, double* U, double* W, double* dU, double* F, double* Bf, d
 // Only the first call of a loop can see stack contents left by unrelated
 // earlier work (later calls see the previous cell's finite values, which the
 // a = 0 metric multiplies by an exact zero), so the stack is scrubbed on entry.
+// the derived fields of every cell's W (prim.hpp:21-25): [np][4][NC] lor, p, h, b2
+void ref_derived(void* h, double* Wd) {
+    Ref& R = *(Ref*)h;
+    for (int p = 0; p < R.np(); p++)
+        for (int l = 0; l < NC; l++) {
+            const prim& w = R.P(p).cells[l].W;
+            double* d = Wd + (size_t)p * 4 * NC;
+            d[l] = w.lor; d[NC + l] = w.p; d[2 * NC + l] = w.h; d[3 * NC + l] = w.b2;
+        }
+}
+// analysis::analyser::batch_ / bundle_ (data/quantitatives.cpp:201-247), the
+// struct members in declaration order after t (analysis.hpp:15-49)
+void ref_batch(void* h, double t, double* out) {
+    analysis::analyser anl;
+    analysis::batch b = anl.batch_(((Ref*)h)->tree, t);
+    double v[17] = {b.t, b.mass, b.energy, b.L_pol, b.Mdot, b.Edot, b.Ldot, b.Phi_B, b.MAD, b.magE, b.thermE,
+                    b.L_BZ, b.eta_BZ, b.Pbeta, b.alpha_ss, b.maxreyn, b.Hscal};
+    std::copy(v, v + 17, out);
+}
+void ref_bundle(void* h, double t, double* out) {
+    analysis::analyser anl;
+    analysis::bundle b = anl.bundle_(((Ref*)h)->tree, t);
+    double v[6] = {b.t, b.mass, b.Mdot, b.MAD, b.L_BZ, b.alpha_ss};
+    std::copy(v, v + 6, out);
+}
 int ref_refine(void* h, int p) {
     scrub_stack();
     GUARD(((Ref*)h)->tree.refine(((Ref*)h)->tree.quilt[p].get()));

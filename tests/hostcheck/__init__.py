@@ -64,7 +64,7 @@ class HostKernels:
         return self.BhPool(hp.npatch, _d(hp.U), _d(hp.W), _d(hp.dU), _d(hp.F), _d(hp.Bf), _d(hp.EMF), _d(hp.rth),
                            _d(hp.pgeo), _d(hp.nbr), _d(self._all), _d(self._leaves), len(self._leaves), _d(err),
                            _d(self._leafmask), _d(self._status) if reuse else None,
-                           _d(self._aux) if aux else None)
+                           _d(self._aux) if aux else None, _d(hp.Wd))
 
     def call(self, name, *args):
         return getattr(self.L, name)(C.byref(self.P), *args)

@@ -152,6 +152,15 @@ void hc_ccrstr(const bh_params* Pp, const bh_pool* pool, const int32_t* plan, in
     for (int r = 0; r < n; r++)
         for (int e = 0; e < 3 * NF; e++) b_init_item(P, plan[r * 9], e);
 }
+// analysis integrals with the cells visited and added in the reference's
+// serial order (quilt order, then i, j, k), so the sums equal the oracle's
+void hc_analysis(const bh_params* Pp, const bh_pool* pool, const bh_analysis_params* A, double* out) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    AParams ap{A->hrz, A->rs, A->rho_min_full, A->rho_min_bundle};
+    for (int q = 0; q < BH_NQ; q++) out[q] = 0.0;
+    for (int i = 0; i < pool->nleaf; i++)
+        for (int c = 0; c < N_INT; c++) analysis_cell(k, P, pool->leaves[i], c, ap, out);
+}
 double hc_dtcomp(const bh_params* Pp, const bh_pool* pool, double cfl) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     double best = DBL_BIG;

@@ -230,3 +230,18 @@ def test_b_init_indices_stay_in_the_patch():
                 idx += [cell_index(i, j, k - 1), cell_index(i, j, k)] if -G < k < B + G else \
                        [cell_index(i, j, k)] if i == -G else [cell_index(i, j, k - 1)]
     assert min(idx) >= 0 and max(idx) < 8000
+
+
+def test_analysis_items_bitwise():
+    """The analysis kernel's per-cell integrands built for the host, added in
+    the reference's order, equal the oracle's integrals bit for bit."""
+    from bhgpu._lib import BhAnalysisParams
+    q, orc, hp = box_case(2, seed=4, periodic=False, lim=1, M=1.0, a=0.0, lo=-6.0, hi=6.0)
+    orc.step(hp, 0.4)
+    hk = HostKernels(1.0, 0.0, 0.0, GAMMA, 1)
+    pool = hk.pool(hp)
+    out = np.zeros(20)
+    A = BhAnalysisParams(2.0, 10.0, 0.01, 0.005)
+    hk.L.hc_analysis(C.byref(hk.P), C.byref(pool), C.byref(A), _d(out))
+    raw, _ = orc.analysis(hp, 2.0, 10.0)
+    assert eq(out, raw)
