@@ -303,6 +303,51 @@ def regrid_bench(tree):
 
 
 # ---------------------------------------------------------------------------
+# diagnostics: analysis::analyser's bundle_ (what the reference's main()
+# prints after every step) and batch_ on the headline box after a step, and
+# the reference's own analyser on the 64^3 CPU sample
+def analysis_bench(tree):
+    import torch
+    import bhgpu
+    rk = bhgpu.RK2Integrator(CFL)
+    rk.step(tree, check_domain=False)      # floors records the derived fields
+    an = bhgpu.Analyser()
+    for _ in range(2):
+        an.bundle_(tree, 0.0)
+    torch.cuda.synchronize()
+    out = {"workload": f"analysis::analyser on the headline box ({tree.npatch} patches) after one step"}
+    for name, fn in (("bundle_ms", an.bundle_), ("batch_ms", an.batch_)):
+        t0 = time.perf_counter()
+        for _ in range(10):
+            fn(tree, 0.0)
+        out[name] = (time.perf_counter() - t0) * 100.0
+    tree.clear_error()
+    try:
+        import oracle
+        if oracle.ref_available():
+            from bhgpu import configs
+            from bhgpu.mesh import Quilt
+            q = Quilt([LO] * 3, [HI] * 3, 4, periodic=False)
+            W, Bf = configs.magnetised_box(q, seed=1, gamma=GAMMA)
+            orc = oracle.Oracle(0.0, 0.0, 0.0, GAMMA, limiter=1)
+            hp = oracle.HostPool(q.tables())
+            orc.geometry(hp)
+            hp.W[:] = W; hp.Bf[:] = Bf
+            for p in range(hp.npatch):
+                hp.U[p] = orc.ptoc(W[p], hp.rth[p, 0], hp.rth[p, 1])[0]
+            ref = oracle.RefSolver([LO] * 3, [HI] * 3, 4, 0.0, 0.0, 0.0, GAMMA)
+            ref.put(hp)
+            ref.step_native(CFL)
+            t0 = time.perf_counter(); ref.bundle(0.0); t1 = time.perf_counter(); ref.batch(0.0); t2 = time.perf_counter()
+            out["cpu_reference"] = {"bundle_ms": (t1 - t0) * 1e3, "batch_ms": (t2 - t1) * 1e3,
+                                    "sample": "the reference's analyser on the 64^3 box (64 patches) after its step, "
+                                              "one thread (the reference's analyser is serial)"}
+    except Exception as e:      # the CPU figure is informational
+        out["cpu_reference"] = {"error": str(e)}
+    return out
+
+
+# ---------------------------------------------------------------------------
 FIELDS = {"D": [0], "S": [1, 2, 3], "tau": [4], "B": [5, 6, 7]}
 
 
@@ -637,6 +682,7 @@ def run_ours(args):
             if args.con2prim_batch:
                 line["con2prim_batch"] = con2prim_batch()
             line["regrid"] = regrid_bench(tree)
+            line["analysis"] = analysis_bench(tree)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
