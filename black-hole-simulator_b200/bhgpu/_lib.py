@@ -29,7 +29,7 @@ class BhPool(C.Structure):
     _fields_ = [("npatch", C.c_int32), ("U", _vp), ("W", _vp), ("dU", _vp), ("F", _vp), ("Bf", _vp),
                 ("EMF", _vp), ("rth", _vp), ("pgeo", _vp), ("nbr", _vp), ("all", _vp),
                 ("leaves", _vp), ("nleaf", C.c_int32), ("err", _vp), ("leafmask", _vp), ("status", _vp),
-                ("aux", _vp), ("Wd", _vp)]
+                ("aux", _vp), ("Wd", _vp), ("nall", C.c_int32)]
 
 
 class BhAnalysisParams(C.Structure):

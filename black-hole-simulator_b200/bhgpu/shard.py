@@ -187,7 +187,7 @@ class ShardedStepper:
         t = tree
         self.pool = BhPool(t.npatch, _p(t.U), _p(t.W), _p(t.dU), _p(t.F), _p(t.Bf), _p(t.EMF), _p(t.rth),
                            _p(t.pgeo), _p(t.nbr), _p(self.all_mine), _p(self.leaves_mine), len(leaves), _p(t.err),
-                           _p(self.leafmask_mine), _p(t.status), _p(t.aux), _p(t.Wd))
+                           _p(self.leafmask_mine), _p(t.status), _p(t.aux), _p(t.Wd), len(self.all_mine))
         # waves restricted to owned leaves (one wave: the fused ghost fill + con2prim)
         off = t._wave_off
         lists = [t.waves[off[w]:off[w + 1]].cpu().numpy() for w in range(t.nwave)]

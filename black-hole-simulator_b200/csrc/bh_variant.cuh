@@ -225,7 +225,12 @@ __global__ void k_dtcomp(KP kp, Pool P, const int32_t* list, double cfl, double*
 // ==========================================================================
 inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 inline int launched() { return cudaGetLastError() == cudaSuccess ? BH_OK : BH_ECUDA; }
-inline bool bad_pool(const bh_pool* p) { return !p || p->npatch <= 0 || !p->all; }
+inline bool bad_pool(const bh_pool* p) {
+    return !p || p->npatch <= 0 || !p->all || p->nall < 0 || p->nall > p->npatch || p->nleaf < 0 ||
+           p->nleaf > p->npatch;
+}
+// entries of pool->all: the patches the flux/CT/update/floors kernels visit
+inline int nall(const bh_pool* p) { return p->nall > 0 ? p->nall : p->npatch; }
 inline dim3 grid2(int items, int npatch, int z = 1) { return dim3((items + TPB - 1) / TPB, npatch, z); }
 
 }  // namespace
@@ -261,7 +266,7 @@ int hlld(const bh_params* P, const double* WL, const double* WR, const double* U
 
 int geometry(const bh_pool* pool, void* stream) {
     if (bad_pool(pool)) return BH_EINVAL;
-    k_geometry<<<grid2(NC, pool->npatch), TPB, 0, S(stream)>>>(pool_of(pool), pool->all);
+    k_geometry<<<grid2(NC, nall(pool)), TPB, 0, S(stream)>>>(pool_of(pool), pool->all);
     return launched();
 }
 int reconfp(const bh_params* P, const bh_pool* pool, int32_t dim, int32_t limiter, double* L, double* R,
@@ -274,26 +279,26 @@ int reconfp(const bh_params* P, const bh_pool* pool, int32_t dim, int32_t limite
 int fluxcomp(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     if (pool->aux) {
-        k_aux<<<grid2(NC, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
-        k_flux_aux<<<grid2(NFACE, pool->npatch, 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+        k_aux<<<grid2(NC, nall(pool)), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+        k_flux_aux<<<grid2(NFACE, nall(pool), 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
     } else {
-        k_flux<<<grid2(NFACE, pool->npatch, 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+        k_flux<<<grid2(NFACE, nall(pool), 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
     }
     return launched();
 }
 int emfcomp(const bh_pool* pool, void* stream) {
     if (bad_pool(pool)) return BH_EINVAL;
-    k_emf<<<grid2(N_EDGE, pool->npatch), TPB, 0, S(stream)>>>(pool_of(pool), pool->all);
+    k_emf<<<grid2(N_EDGE, nall(pool)), TPB, 0, S(stream)>>>(pool_of(pool), pool->all);
     return launched();
 }
 int bfupdate(const bh_pool* pool, const double* dt_dev, void* stream) {
     if (bad_pool(pool) || !dt_dev) return BH_EINVAL;
-    k_bfupdate<<<grid2(N_BUP, pool->npatch), TPB, 0, S(stream)>>>(pool_of(pool), pool->all, dt_dev);
+    k_bfupdate<<<grid2(N_BUP, nall(pool)), TPB, 0, S(stream)>>>(pool_of(pool), pool->all, dt_dev);
     return launched();
 }
 int f2cb(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
-    k_f2cb<<<grid2(N_F2C, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    k_f2cb<<<grid2(N_F2C, nall(pool)), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
     return launched();
 }
 int maxdivb(const bh_pool* pool, double* out, void* stream) {
@@ -303,7 +308,7 @@ int maxdivb(const bh_pool* pool, double* out, void* stream) {
 }
 int div_source(const bh_params* P, const bh_pool* pool, double* div, double* src, void* stream) {
     if (!P || bad_pool(pool) || !div || !src) return BH_EINVAL;
-    k_div_source<<<grid2(N_INT, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, div,
+    k_div_source<<<grid2(N_INT, nall(pool)), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, div,
                                                                                src);
     return launched();
 }
@@ -343,13 +348,13 @@ int ghosts_prims(const bh_params* P, const bh_pool* pool, void* stream) {
 }
 int update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, void* stream) {
     if (!P || bad_pool(pool) || !dt_dev || (stage != 0 && stage != 1)) return BH_EINVAL;
-    k_update<<<dim3(UPD_BLOCKS, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, dt_dev,
+    k_update<<<dim3(UPD_BLOCKS, nall(pool)), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, dt_dev,
                                                                     stage);
     return launched();
 }
 int floors(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
-    k_floors<<<grid2(N_INT, pool->npatch), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    k_floors<<<grid2(N_INT, nall(pool)), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
     return launched();
 }
 int regrid_flags(const bh_params* P, const bh_pool* pool, const int32_t* lvl, uint8_t* flags, void* stream) {

@@ -84,7 +84,8 @@ typedef struct bh_pool {
     double *rth;         /* [np][2][8000]   written by bh_geometry               */
     const double *pgeo;  /* [np][6]  xedge[0], yedge[0], zedge[0], dx, dy, dz    */
     const int32_t *nbr;  /* [np][6][2] (neighbour, kind), slot dim*2 + (side>0)  */
-    const int32_t *all;  /* [npatch] patch indices 0..np-1 (flux/CT/update/floors) */
+    const int32_t *all;  /* [nall] patch indices the flux/CT/update/floors kernels
+                            visit (normally 0..npatch-1)                       */
     const int32_t *leaves; int32_t nleaf;  /* leaf patch indices (ghosts, prims, dt) */
     int32_t *err;        /* device error word (BH_ERR_* bits)                    */
     const uint8_t *leafmask; /* [npatch] 1 for leaf patches                       */
@@ -100,6 +101,8 @@ typedef struct bh_pool {
                             refine and ccrstr leave them (the derived fields of the
                             reference's prim, prim.hpp:21-25; read by bh_analysis);
                             NULL: not kept */
+    int32_t nall;        /* entries of `all` (0: npatch); a subset of the patches,
+                            e.g. those one rank owns when a domain is sharded */
 } bh_pool;
 
 /* ---- library --------------------------------------------------------------- */

@@ -10,6 +10,9 @@
 
 using namespace bh;
 
+// entries of pool->all, as the launchers count them
+static inline int NALL(const bh_pool* p) { return p->nall > 0 ? p->nall : p->npatch; }
+
 extern "C" {
 
 void hc_metric(const bh_params* P, const double* r, const double* th, int64_t n, double* out) {
@@ -32,7 +35,7 @@ void hc_hlld(const bh_params* P, const double* WL, const double* WR, const doubl
 }
 void hc_geometry(const bh_pool* pool) {
     Pool P = pool_of(pool);
-    for (int i = 0; i < pool->npatch; i++)
+    for (int i = 0; i < NALL(pool); i++)
         for (int l = 0; l < NC; l++) geometry_item(P, pool->all[i], l);
 }
 void hc_reconfp(const bh_params* Pp, const bh_pool* pool, int dim, int lim, double* L, double* R) {
@@ -44,30 +47,30 @@ void hc_reconfp(const bh_params* Pp, const bh_pool* pool, int dim, int lim, doub
 void hc_fluxcomp(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     if (pool->aux) {
-        for (int i = 0; i < pool->npatch; i++)
+        for (int i = 0; i < NALL(pool); i++)
             for (int l = 0; l < NC; l++) aux_item<double>(k, P, pool->all[i], l);
-        for (int i = 0; i < pool->npatch; i++)
+        for (int i = 0; i < NALL(pool); i++)
             for (int dim = 0; dim < 3; dim++)
                 for (int f = 0; f < NFACE; f++) flux_item<double, true>(k, P, pool->all[i], dim, f);
         return;
     }
-    for (int i = 0; i < pool->npatch; i++)
+    for (int i = 0; i < NALL(pool); i++)
         for (int dim = 0; dim < 3; dim++)
             for (int f = 0; f < NFACE; f++) flux_item<double>(k, P, pool->all[i], dim, f);
 }
 void hc_emfcomp(const bh_pool* pool) {
     Pool P = pool_of(pool);
-    for (int i = 0; i < pool->npatch; i++)
+    for (int i = 0; i < NALL(pool); i++)
         for (int e = 0; e < N_EDGE; e++) emf_item(P, pool->all[i], e);
 }
 void hc_bfupdate(const bh_pool* pool, double dt) {
     Pool P = pool_of(pool);
-    for (int i = 0; i < pool->npatch; i++)
+    for (int i = 0; i < NALL(pool); i++)
         for (int e = 0; e < N_BUP; e++) bfupdate_item(P, pool->all[i], e, dt);
 }
 void hc_f2cb(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
-    for (int i = 0; i < pool->npatch; i++)
+    for (int i = 0; i < NALL(pool); i++)
         for (int e = 0; e < N_F2C; e++) f2cb_item(k, P, pool->all[i], e);
 }
 void hc_maxdivb(const bh_pool* pool, double* out) {
@@ -80,7 +83,7 @@ void hc_maxdivb(const bh_pool* pool, double* out) {
 }
 void hc_div_source(const bh_params* Pp, const bh_pool* pool, double* dv, double* sv) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
-    for (int i = 0; i < pool->npatch; i++)
+    for (int i = 0; i < NALL(pool); i++)
         for (int c = 0; c < N_INT; c++) div_source_item<double>(k, P, pool->all[i], c, dv, sv);
 }
 void hc_ghosts(const bh_params* Pp, const bh_pool* pool, const int32_t* list, int n) {
@@ -114,14 +117,14 @@ void hc_ghosts_prims(const bh_params* Pp, const bh_pool* pool) {
 }
 void hc_update(const bh_params* Pp, const bh_pool* pool, double dt, int stage) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
-    for (int i = 0; i < pool->npatch; i++)
+    for (int i = 0; i < NALL(pool); i++)
         for (int c = 0; c < N_INT; c++) update_interior_item<double>(k, P, pool->all[i], c, dt, stage);
-    for (int i = 0; i < pool->npatch; i++)
+    for (int i = 0; i < NALL(pool); i++)
         for (int e = 0; e < N_SHELL; e++) update_shell_item(k, P, pool->all[i], e);
 }
 void hc_floors(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
-    for (int i = 0; i < pool->npatch; i++)
+    for (int i = 0; i < NALL(pool); i++)
         for (int c = 0; c < N_INT; c++) floors_item(k, P, pool->all[i], c);
 }
 // AMR regrid pieces, in the launch order of bh_regrid_flags / bh_refine /

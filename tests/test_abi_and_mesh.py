@@ -80,3 +80,19 @@ def test_ghost_waves_order_prolongation_sources_first():
                     assert where[nb] < where[p]
                 else:
                     assert where[p] < where[nb]
+
+
+def test_pool_lists_longer_than_the_pool_are_rejected():
+    """A pool whose `all` or `leaves` list claims more entries than it has
+    patches is refused before anything is launched (no device needed)."""
+    import ctypes as C
+    import numpy as np
+    from bhgpu._lib import BhParams, BhPool, lib
+    idx = np.arange(4, dtype=np.int32)
+    p = C.c_void_p(idx.ctypes.data)
+    P = BhParams(0.0, 0.0, 0.0, 4.0 / 3.0, 0, 500, 1e-10, 1.0, 0.0, 0.0, 0, 0)
+    too_many_all = BhPool(2, *([None] * 9), p, p, 0, *([None] * 5), 3)
+    too_many_leaves = BhPool(2, *([None] * 9), p, p, 3, *([None] * 5), 0)
+    for pool in (too_many_all, too_many_leaves):
+        assert lib.bh_fluxcomp(C.byref(P), C.byref(pool), None) == -1
+        assert lib.bh_floors(C.byref(P), C.byref(pool), None) == -1
