@@ -348,6 +348,38 @@ def analysis_bench(tree):
 
 
 # ---------------------------------------------------------------------------
+# initial data: the Fishbone-Moncrief torus of the Kerr box (a = 0.9375,
+# 128^3 over [-40,40]^3 in 8^3 patches) by bh_torus_init, and the
+# reference's own initialisation of the 64^3 version on the host
+def torus_bench():
+    import torch
+    import bhgpu
+    from bhgpu.mesh import Quilt
+    q = Quilt([-40.0] * 3, [40.0] * 3, 8)
+    t = bhgpu.AmrTree(q.dom_l, q.dom_h, 8, M=1.0, a=0.9375, Q=0.0, gm=GAMMA, quilt=q, init_floor=False)
+    t.torus_init()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s = t.torus_init()
+    torch.cuda.synchronize()
+    out = {"workload": "Fishbone-Moncrief torus initial data, Kerr a=0.9375, 128^3 over [-40,40]^3 (512 patches)",
+           "ms": (time.perf_counter() - t0) * 1e3, "l0": s["l0"], "rho_max": s["rho_max"]}
+    del t
+    try:
+        import oracle
+        if oracle.ref_available():
+            ref = oracle.RefSolver([-40.0] * 3, [40.0] * 3, 4, 1.0, 0.9375, 0.0, GAMMA)
+            t0 = time.perf_counter()
+            ref.torus_init()
+            out["cpu_reference"] = {"ms": (time.perf_counter() - t0) * 1e3,
+                                    "sample": "the reference's fm_init + B_pot_init + ptoc, 64^3 (64 patches), "
+                                              "one thread (serial loops)"}
+    except Exception as e:      # the CPU figure is informational
+        out["cpu_reference"] = {"error": str(e)}
+    return out
+
+
+# ---------------------------------------------------------------------------
 FIELDS = {"D": [0], "S": [1, 2, 3], "tau": [4], "B": [5, 6, 7]}
 
 
@@ -683,6 +715,7 @@ def run_ours(args):
                 line["con2prim_batch"] = con2prim_batch()
             line["regrid"] = regrid_bench(tree)
             line["analysis"] = analysis_bench(tree)
+            line["torus_init"] = torus_bench()
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

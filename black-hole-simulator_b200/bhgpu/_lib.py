@@ -77,6 +77,7 @@ def _load():
         "bh_dtcomp": ([P, PP, dbl, _vp, _vp], C.c_int),
         "bh_regrid_flags": ([P, PP, _vp, _vp, _vp], C.c_int),
         "bh_analysis": ([P, PP, C.POINTER(BhAnalysisParams), _vp, _vp, _vp], C.c_int),
+        "bh_torus_init": ([P, PP, dbl, dbl, _vp, _vp], C.c_int),
         "bh_refine": ([P, PP, _vp, i32, _vp], C.c_int),
         "bh_ccrstr": ([P, PP, _vp, i32, _vp], C.c_int),
         "bh_b_init": ([P, PP, _vp, i32, _vp], C.c_int),

@@ -223,6 +223,28 @@ class AmrTree:
                            _p(self.Wd))
         check(lib.bh_geometry(C.byref(self.pool), _stream()), "patch::cell_init")
 
+    # ---- initial data ----------------------------------------------------
+    def torus_init(self, r_max: float | None = None, r_in: float | None = None) -> dict:
+        """The initial data of the reference's main() (main.cpp:89-160) on the
+        device: floor state, Fishbone-Moncrief torus (init::fm_init,
+        initconds.cpp:228-591; the reference fixes r_max = 12 M, r_in = 4.5 M),
+        face B from the curl of A_phi (init::B_pot_init, :594-667), U = ptoc(W).
+        Returns l0, W_in, ln h at r_max, the torus density maximum before
+        normalisation and the interior density maximum; raises where main()
+        stops (no density above 1e-14)."""
+        M = self.mtr.M
+        r_max = 12.0 * M if r_max is None else float(r_max)
+        r_in = 4.5 * M if r_in is None else float(r_in)
+        out = np.zeros(5)
+        P = self.params()
+        rc = lib.bh_torus_init(C.byref(P), C.byref(self.pool), r_max, r_in, out.ctypes.data_as(C.c_void_p),
+                               _stream())
+        if rc == -3:
+            raise RuntimeError("Density initialisation threw back an error: rho_max is zero after "
+                               "Fishbone-Moncrief torus initialisation attempt!")
+        check(rc, "torus initial data")
+        return dict(zip(("l0", "W_in", "lnh_max", "rho_max_torus", "rho_max"), out.tolist()))
+
     # ---- AMR -------------------------------------------------------------
     def regrid(self, check_domain: bool = True, flags=None):
         """amrtree::regrid (grid.cpp:722-835) on the device.

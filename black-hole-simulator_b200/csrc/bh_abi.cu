@@ -123,6 +123,9 @@ int bh_analysis(const bh_params* P, const bh_pool* pool, const bh_analysis_param
                 double* out, void* stream) {
     BH_DISPATCH(P, analysis(P, pool, A, partial, out, stream));
 }
+int bh_torus_init(const bh_params* P, const bh_pool* pool, double r_max, double r_in, double* out, void* stream) {
+    BH_DISPATCH(P, torus_init(P, pool, r_max, r_in, out, stream));
+}
 int bh_dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
     BH_DISPATCH(P, dtcomp(P, pool, cfl, dt_dev, stream));
 }

@@ -30,6 +30,7 @@
     int dtcomp(const bh_params*, const bh_pool*, double, double*, void*);                                      \
     int regrid_flags(const bh_params*, const bh_pool*, const int32_t*, uint8_t*, void*);                       \
     int analysis(const bh_params*, const bh_pool*, const bh_analysis_params*, double*, double*, void*);       \
+    int torus_init(const bh_params*, const bh_pool*, double, double, double*, void*);                          \
     int refine(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
     int ccrstr(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
     int b_init(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \

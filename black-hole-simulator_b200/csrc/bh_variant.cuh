@@ -11,8 +11,10 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <cstring>
 #include "bhgpu.h"
 #include "bh_items.cuh"
+#include "bh_init.cuh"
 
 #ifndef BH_VARIANT
 #error "define BH_VARIANT before including bh_variant.cuh"
@@ -181,6 +183,36 @@ __global__ void k_analysis_sum(const double* partial, int n, double* out) {
     double s = 0.0;
     for (int i = 0; i < n; i++) s += partial[(size_t)i * BH_NQ + q];
     out[q] = s;
+}
+
+// ---- torus initial data: max-reductions on the bit patterns of
+// non-negative doubles (they order like the values), so they are exact ----
+__device__ inline void atomic_max_nonneg(unsigned long long* m, double v) {
+    if (v >= 0.0) atomicMax(m, (unsigned long long)__double_as_longlong(v));
+}
+__global__ void k_floor_all(KP kp, Pool P, const int32_t* list) { ITEM(NC); floor_cell(kp, P, list[blockIdx.y], e); }
+__global__ void k_fm_scalars(KP kp, double r_max, double r_in, TorusScalars* out) {
+    *out = fm_scalars(kp.tree, kp.gamma, r_max, r_in);
+}
+__global__ void k_fm_rho_max(KP kp, Pool P, const int32_t* list, const TorusScalars* s, unsigned long long* m) {
+    ITEM(N_INT);
+    atomic_max_nonneg(m, fm_cell_rho(kp, P, list[blockIdx.y], e, *s));
+}
+__global__ void k_fm_prims(KP kp, Pool P, const int32_t* list, const TorusScalars* s, const unsigned long long* m) {
+    ITEM(N_INT);
+    fm_cell_prims(kp, P, list[blockIdx.y], e, *s, 1.0 / __longlong_as_double((long long)*m));
+}
+__global__ void k_interior_rho_max(Pool P, const int32_t* list, unsigned long long* m) {
+    ITEM(N_INT);
+    int p = list[blockIdx.y];
+    atomic_max_nonneg(m, Wv(P, p, 0)[lindx(e / 256, (e / 16) % 16, e % 16)]);
+}
+__global__ void k_bpot(Pool P, const int32_t* list, const unsigned long long* m) {
+    ITEM(N_F2C);
+    bpot_item(P, list[blockIdx.y], e, __longlong_as_double((long long)*m));
+}
+__global__ void k_ptoc_interior(KP kp, Pool P, const int32_t* list) {
+    ITEM(N_INT); ptoc_interior_item(kp, P, list[blockIdx.y], e);
 }
 
 // constrans::maxdivB: one CTA per patch, max-reduction in shared memory
@@ -394,6 +426,62 @@ int analysis(const bh_params* P, const bh_pool* pool, const bh_analysis_params* 
     k_analysis<<<pool->nleaf, ANL_TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->leaves, ap, partial);
     k_analysis_sum<<<1, 32, 0, S(stream)>>>(partial, pool->nleaf, out);
     return launched();
+}
+// the initial-data sequence of main() (main.cpp:89-160) on every listed patch:
+// out[5] (host) = l0, W_in, ln h at r_max, the torus' rho_max before
+// normalisation, the global interior rho_max after fm_init
+int torus_init(const bh_params* P, const bh_pool* pool, double r_max, double r_in, double* out, void* stream) {
+    if (!P || bad_pool(pool) || !out) return BH_EINVAL;
+    cudaStream_t st = S(stream);
+    KP kp = kp_of(P);
+    Pool pv = pool_of(pool);
+    int n = nall(pool);
+    TorusScalars* ds = nullptr;
+    unsigned long long* dm = nullptr;
+    if (cudaMallocAsync((void**)&ds, sizeof(TorusScalars), st) != cudaSuccess) return BH_ECUDA;
+    if (cudaMallocAsync((void**)&dm, 2 * sizeof(unsigned long long), st) != cudaSuccess) {
+        cudaFreeAsync(ds, st);
+        return BH_ECUDA;
+    }
+    cudaMemsetAsync(dm, 0, 2 * sizeof(unsigned long long), st);
+    k_floor_all<<<grid2(NC, n), TPB, 0, st>>>(kp, pv, pool->all);          // amrtree::amrtree, grid.cpp:191-205
+    k_fm_scalars<<<1, 1, 0, st>>>(kp, r_max, r_in, ds);
+    TorusScalars hs;
+    cudaMemcpyAsync(&hs, ds, sizeof(hs), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    out[0] = hs.l0; out[1] = hs.W_in; out[2] = hs.lnh_max;
+    double rho_fm = 0.0;
+    if (hs.lnh_max > 0.0) {                                                   // initconds.cpp:425-429
+        k_fm_rho_max<<<grid2(N_INT, n), TPB, 0, st>>>(kp, pv, pool->all, ds, dm);
+        unsigned long long bits = 0;
+        cudaMemcpyAsync(&bits, dm, sizeof(bits), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        memcpy(&rho_fm, &bits, sizeof(double));
+        if (rho_fm >= 1e-14)                                                  // :481-484
+            k_fm_prims<<<grid2(N_INT, n), TPB, 0, st>>>(kp, pv, pool->all, ds, dm);
+    }
+    out[3] = rho_fm;
+    k_interior_rho_max<<<grid2(N_INT, n), TPB, 0, st>>>(pv, pool->all, dm + 1);   // main.cpp:99-108
+    unsigned long long gbits = 0;
+    cudaMemcpyAsync(&gbits, dm + 1, sizeof(gbits), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    double glmx;
+    memcpy(&glmx, &gbits, sizeof(double));
+    out[4] = glmx;
+    int rc = BH_OK;
+    if (glmx < 1e-14) {
+        rc = BH_ERANGE;                                                       // main.cpp:109-112
+    } else {
+        if (glmx > 1e-10) {                                                   // B_pot_init :598
+            k_bpot<<<grid2(N_F2C, n), TPB, 0, st>>>(pv, pool->all, dm + 1);
+            k_f2cb<<<grid2(N_F2C, n), TPB, 0, st>>>(kp, pv, pool->all);
+        }
+        k_ptoc_interior<<<grid2(N_INT, n), TPB, 0, st>>>(kp, pv, pool->all);
+    }
+    cudaFreeAsync(ds, st);
+    cudaFreeAsync(dm, st);
+    int lr = launched();
+    return lr ? lr : rc;
 }
 int dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
     if (!P || bad_pool(pool) || !dt_dev) return BH_EINVAL;

@@ -233,6 +233,23 @@ typedef struct bh_analysis_params {
 int bh_analysis(const bh_params *P, const bh_pool *pool, const bh_analysis_params *A, double *partial,
                 double *out, void *stream);
 
+/* ---- initial data (solver/initconds.cpp, main.cpp:89-160) --------------- */
+/* The initial-data sequence of the reference's main() on the patches of
+ * pool->all: the floor state of every cell (amrtree::amrtree, grid.cpp:
+ * 191-205); init::fm_init (:228-591), a Fishbone-Moncrief torus with pressure
+ * maximum at r_max and inner edge r_in (the reference: 12 M and 4.5 M),
+ * polytrope K = 0.001 M^(Gamma-1), normalised to rho_max = 1, in the
+ * interior cells; init::B_pot_init (:594-667) on every patch, face B from the
+ * curl of A_phi = max(rho / rho_max - 0.2, 0) sampled at cell edges, then
+ * f2cB; U = ptoc(W) in the interior cells.  Synchronises the stream and
+ * allocates (stream-ordered, freed before it returns) 64 bytes of scratch.
+ * out[5] (host): l0, W_in, ln h at r_max, the torus density maximum before
+ * normalisation (0 where fm_init gives up and leaves the floor state), the
+ * interior density maximum after it.  Returns BH_ERANGE where main() stops
+ * (that maximum below 1e-14; no field, no ptoc). */
+int bh_torus_init(const bh_params *P, const bh_pool *pool, double r_max, double r_in, double *out,
+                  void *stream);
+
 /* ---- L3 integrator ------------------------------------------------------ */
 /* rk2integrator::dtcomp (solver/integrator.cpp:156-189): *dt_dev = CFL step */
 int bh_dtcomp(const bh_params *P, const bh_pool *pool, double cfl, double *dt_dev, void *stream);

@@ -326,6 +326,7 @@ class RefSolver:
             L.ref_regrid.argtypes = [v]
             L.ref_derived.argtypes = [v, _dp]
             L.ref_batch.argtypes = [v, C.c_double, _dp]
+            L.ref_torus_init.argtypes = [v, _dp]
             L.ref_bundle.argtypes = [v, C.c_double, _dp]
             L.ref_metric_batch.argtypes = [C.c_double] * 3 + [_dp, _dp, C.c_int64, _dp]
             L.ref_ptoc_batch.argtypes = [C.c_double] * 4 + [_dp, _dp, _dp, C.c_int64, _dp, _dp]
@@ -402,6 +403,14 @@ class RefSolver:
 
     def derived(self):
         out = np.zeros((self.npatch, 4, NC)); self.lib().ref_derived(self.h, _ptr(out)); return out
+
+    def torus_init(self):
+        """main()'s initial data (Fishbone-Moncrief torus + A_phi field);
+        returns (status, interior rho_max after fm_init)."""
+        m = C.c_double(0)
+        rc = self.lib().ref_torus_init(self.h, C.byref(m))
+        self._chk(rc if rc < 0 else 0)
+        return rc, m.value
 
     def batch(self, t):
         out = np.zeros(17); self.lib().ref_batch(self.h, t, _ptr(out)); return out

@@ -33,6 +33,8 @@
 #include "hlld.hpp"
 #include "recon.hpp"
 #include "analysis.hpp"
+#include "initial.hpp"
+#include "ct.hpp"
 
 using namespace grid;
 
@@ -382,6 +384,31 @@ void ref_bundle(void* h, double t, double* out) {
     analysis::bundle b = anl.bundle_(((Ref*)h)->tree, t);
     double v[6] = {b.t, b.mass, b.Mdot, b.MAD, b.L_BZ, b.alpha_ss};
     std::copy(v, v + 6, out);
+}
+// the initial-data sequence of main() (main.cpp:89-160) after the amrtree
+// constructor: init::fm_init, the global interior rho_max, init::B_pot_init
+// on every patch, ptoc of the interior cells (the loops of main restated;
+// fm_init and B_pot_init are the reference's own).  The reference's fm_init
+// fixes r_max = 12 M and r_in = 4.5 M.  Returns 1 where main() stops.
+int ref_torus_init(void* h, double* rho_max_out) {
+    amrtree& tree = ((Ref*)h)->tree;
+    GUARD(torus::init::fm_init(tree));
+    double rho_max = 0.0;
+    for (const auto& p : tree.quilt)
+        for (int i = 0; i < block; i++)
+            for (int j = 0; j < block; j++)
+                for (int k = 0; k < block; k++) rho_max = std::max(rho_max, p->cell_(i, j, k).W.rho);
+    *rho_max_out = rho_max;
+    if (rho_max < 1e-14) return 1;
+    for (const auto& p : tree.quilt) torus::init::B_pot_init(*p, tree.mtr, rho_max);
+    for (const auto& p : tree.quilt)
+        for (int i = 0; i < block; i++)
+            for (int j = 0; j < block; j++)
+                for (int k = 0; k < block; k++) {
+                    cell& c = p->cell_(i, j, k);
+                    GUARD(c.U = tree.cnsv.ptoc(c.W, c.r, c.th));
+                }
+    return 0;
 }
 int ref_refine(void* h, int p) {
     scrub_stack();

@@ -7,6 +7,7 @@
 #include <stdint.h>
 #include "bhgpu.h"
 #include "bh_items.cuh"
+#include "bh_init.cuh"
 
 using namespace bh;
 
@@ -163,6 +164,37 @@ void hc_analysis(const bh_params* Pp, const bh_pool* pool, const bh_analysis_par
     for (int q = 0; q < BH_NQ; q++) out[q] = 0.0;
     for (int i = 0; i < pool->nleaf; i++)
         for (int c = 0; c < N_INT; c++) analysis_cell(k, P, pool->leaves[i], c, ap, out);
+}
+// the initial-data sequence of bh_torus_init, serially; out[5] as there
+int hc_torus_init(const bh_params* Pp, const bh_pool* pool, double r_max, double r_in, double* out) {
+    KP k = kp_of(Pp); Pool P = pool_of(pool);
+    int n = NALL(pool);
+    for (int i = 0; i < n; i++)
+        for (int l = 0; l < NC; l++) floor_cell(k, P, pool->all[i], l);
+    TorusScalars s = fm_scalars(k.tree, k.gamma, r_max, r_in);
+    out[0] = s.l0; out[1] = s.W_in; out[2] = s.lnh_max;
+    double rho_fm = 0.0;
+    if (s.lnh_max > 0.0) {
+        for (int i = 0; i < n; i++)
+            for (int c = 0; c < N_INT; c++) rho_fm = smax(rho_fm, fm_cell_rho(k, P, pool->all[i], c, s));
+        if (rho_fm >= 1e-14)
+            for (int i = 0; i < n; i++)
+                for (int c = 0; c < N_INT; c++) fm_cell_prims(k, P, pool->all[i], c, s, 1.0 / rho_fm);
+    }
+    out[3] = rho_fm;
+    double glmx = 0.0;
+    for (int i = 0; i < n; i++)
+        for (int c = 0; c < N_INT; c++) glmx = smax(glmx, Wv(P, pool->all[i], 0)[lindx(c / 256, (c / 16) % 16, c % 16)]);
+    out[4] = glmx;
+    if (glmx < 1e-14) return BH_ERANGE;
+    if (glmx > 1e-10)
+        for (int i = 0; i < n; i++) {
+            for (int e = 0; e < N_F2C; e++) bpot_item(P, pool->all[i], e, glmx);
+            for (int e = 0; e < N_F2C; e++) f2cb_item(k, P, pool->all[i], e);
+        }
+    for (int i = 0; i < n; i++)
+        for (int c = 0; c < N_INT; c++) ptoc_interior_item(k, P, pool->all[i], c);
+    return BH_OK;
 }
 double hc_dtcomp(const bh_params* Pp, const bh_pool* pool, double cfl) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
