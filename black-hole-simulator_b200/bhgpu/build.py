@@ -23,7 +23,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 # and mixed variants contract, and the mixed variant's FP32 arithmetic uses
 # flush-to-zero and the fast division/square root
 FMAD = {"bh_fp64fma.cu": ["--fmad=true"],
-        "bh_mixed.cu": ["--fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]}
+        "bh_mixed.cu": ["--fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+        "bh_mlp.cu": ["--fmad=true"]}
 
 
 def sources():

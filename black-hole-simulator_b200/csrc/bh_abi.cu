@@ -126,6 +126,15 @@ int bh_analysis(const bh_params* P, const bh_pool* pool, const bh_analysis_param
 int bh_torus_init(const bh_params* P, const bh_pool* pool, double r_max, double r_in, double* out, void* stream) {
     BH_DISPATCH(P, torus_init(P, pool, r_max, r_in, out, stream));
 }
+int bh_ctop_guess(const bh_params* P, const double* U, const double* r, const double* th, int64_t n,
+                  const double* xi0, double* W, double* Wd, int32_t* status, int32_t* iters, int32_t* path,
+                  void* stream) {
+    BH_DISPATCH(P, ctop_guess(P, U, r, th, n, xi0, W, Wd, status, iters, path, stream));
+}
+int bh_ctop_pre(const bh_params* P, const double* U, const double* r, const double* th, int64_t n, double* pre,
+                void* stream) {
+    BH_DISPATCH(P, ctop_pre(P, U, r, th, n, pre, stream));
+}
 int bh_dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
     BH_DISPATCH(P, dtcomp(P, pool, cfl, dt_dev, stream));
 }

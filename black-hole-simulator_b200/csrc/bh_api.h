@@ -31,6 +31,9 @@
     int regrid_flags(const bh_params*, const bh_pool*, const int32_t*, uint8_t*, void*);                       \
     int analysis(const bh_params*, const bh_pool*, const bh_analysis_params*, double*, double*, void*);       \
     int torus_init(const bh_params*, const bh_pool*, double, double, double*, void*);                          \
+    int ctop_guess(const bh_params*, const double*, const double*, const double*, int64_t, const double*,      \
+                   double*, double*, int32_t*, int32_t*, int32_t*, void*);                                     \
+    int ctop_pre(const bh_params*, const double*, const double*, const double*, int64_t, double*, void*);    \
     int refine(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
     int ccrstr(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
     int b_init(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \

@@ -1087,6 +1087,41 @@ BH_HD inline void ctop_item(const KP& k, const double* U, const double* r, const
     if (path) path[q] = co.path;
 }
 
+// ctop with Newton started from xi0[q] (bh_ctop_guess); the outputs of ctop_item
+BH_HD inline void ctop_guess_item(const KP& k, const double* U, const double* r, const double* th, int64_t n,
+                                  int64_t q, const double* xi0, double* W, double* Wd, int32_t* status, int32_t* iters,
+                                  int32_t* path) {
+    Cons c;
+    c.D = U[q]; c.tau = U[4 * n + q];
+    for (int d = 0; d < 3; d++) { c.S[d] = U[(1 + d) * n + q]; c.B[d] = U[(5 + d) * n + q]; }
+    Met mc;
+    met_comp(k.tree, r[q], th[q], mc);
+    Prim w = {0, 0, {0, 0, 0}, {0, 0, 0}};
+    CtopOut co = {0, 0, 0, 0, 0, 0, 0};
+    bool dom = false;
+    int ok = ctop(k.gamma, k.maxiter, k.tol, mc, c, w, dom, &co, xi0[q]);
+    W[q] = w.rho; W[n + q] = w.eps;
+    for (int d = 0; d < 3; d++) { W[(2 + d) * n + q] = w.v[d]; W[(5 + d) * n + q] = w.B[d]; }
+    if (Wd) { Wd[q] = co.p; Wd[n + q] = co.T; Wd[2 * n + q] = co.h; Wd[3 * n + q] = co.lor; Wd[4 * n + q] = co.b2; }
+    status[q] = dom ? -1 : ok;
+    if (iters) iters[q] = co.iters;
+    if (path) path[q] = co.path;
+}
+// the preamble quantities of ctop (D, tau, Ssq, Bsq, SB) of cell q, pre [5][n]
+BH_HD inline void ctop_pre_item(const KP& k, const double* U, const double* r, const double* th, int64_t n, int64_t q,
+                                double* pre) {
+    Cons c;
+    c.D = U[q]; c.tau = U[4 * n + q];
+    for (int d = 0; d < 3; d++) { c.S[d] = U[(1 + d) * n + q]; c.B[d] = U[(5 + d) * n + q]; }
+    Met mc;
+    met_comp(k.tree, r[q], th[q], mc);
+    Prim w;
+    bool dom = false;
+    double p5[5];
+    ctop(k.gamma, 0, k.tol, mc, c, w, dom, nullptr, NAN, p5);   // no Newton step: only the preamble is wanted
+    for (int i = 0; i < 5; i++) pre[i * n + q] = p5[i];
+}
+
 BH_HD inline void hlld_item(const KP& k, const double* WL, const double* WR, const double* UL, const double* UR,
                             const double* r, const double* th, int dim, int64_t n, int64_t q, double* F,
                             double* cts) {

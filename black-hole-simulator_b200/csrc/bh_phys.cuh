@@ -357,8 +357,11 @@ BH_HD inline bool cp_bd(double gamma, double xa, double xb, double Ssq, double B
 
 struct CtopOut { double p, T, h, lor, b2; int iters, path; };
 // returns 1 ok / 0 failed; *domain set where the reference throws
+// xi0: Newton's start where it lies strictly inside the bracket (the learned
+// guess; NaN, the default, keeps the reference's midpoint); pre[5] (may be
+// null) receives D, tau, Ssq, Bsq, SB of the preamble
 BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, const Cons& cv, Prim& pv,
-                           bool& domain, CtopOut* co = nullptr) {
+                           bool& domain, CtopOut* co = nullptr, double xi0 = NAN, double* pre = nullptr) {
     double sg = mc.sqrtdetgam;
     double D = cv.D / sg;
     double tau = cv.tau / sg;
@@ -386,6 +389,8 @@ BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, cons
         fl = fres(gamma, xi_h, Ssq, Bsq, SB, D, tau);
     }
     double xi = (xi_l + xi_h) / 2.0;
+    if (pre) { pre[0] = D; pre[1] = tau; pre[2] = Ssq; pre[3] = Bsq; pre[4] = SB; }
+    if (isfinite(xi0) && xi0 > xi_l && xi0 < xi_h) xi = xi0;
     bool nr_ok = true, conv = false;
     int it = 0;
     for (int i = 0; i < maxiter; i++) {

@@ -66,6 +66,13 @@ __global__ void k_ctop(KP k, const double* U, const double* r, const double* th,
                        int32_t* st, int32_t* it, int32_t* pa) {
     BATCH; ctop_item(k, U, r, th, n, q, W, Wd, st, it, pa);
 }
+__global__ void k_ctop_guess(KP k, const double* U, const double* r, const double* th, int64_t n, const double* xi0,
+                             double* W, double* Wd, int32_t* st, int32_t* it, int32_t* pa) {
+    BATCH; ctop_guess_item(k, U, r, th, n, q, xi0, W, Wd, st, it, pa);
+}
+__global__ void k_ctop_pre(KP k, const double* U, const double* r, const double* th, int64_t n, double* pre) {
+    BATCH; ctop_pre_item(k, U, r, th, n, q, pre);
+}
 __global__ void k_hlld(KP k, const double* WL, const double* WR, const double* UL, const double* UR, const double* r,
                        const double* th, int dim, int64_t n, double* F, double* cts) {
     BATCH; hlld_item(k, WL, WR, UL, UR, r, th, dim, n, q, F, cts);
@@ -387,6 +394,21 @@ int update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_
 int floors(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     k_floors<<<grid2(N_INT, nall(pool)), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    return launched();
+}
+int ctop_guess(const bh_params* P, const double* U, const double* r, const double* th, int64_t n, const double* xi0,
+               double* W, double* Wd, int32_t* status, int32_t* iters, int32_t* path, void* stream) {
+    if (!P || n < 0 || (n > 0 && (!U || !r || !th || !xi0 || !W || !status))) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    k_ctop_guess<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), U, r, th, n, xi0, W, Wd, status,
+                                                                      iters, path);
+    return launched();
+}
+int ctop_pre(const bh_params* P, const double* U, const double* r, const double* th, int64_t n, double* pre,
+             void* stream) {
+    if (!P || n < 0 || (n > 0 && (!U || !r || !th || !pre))) return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    k_ctop_pre<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), U, r, th, n, pre);
     return launched();
 }
 int regrid_flags(const bh_params* P, const bh_pool* pool, const int32_t* lvl, uint8_t* flags, void* stream) {

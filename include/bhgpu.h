@@ -250,6 +250,42 @@ int bh_analysis(const bh_params *P, const bh_pool *pool, const bh_analysis_param
 int bh_torus_init(const bh_params *P, const bh_pool *pool, double r_max, double r_in, double *out,
                   void *stream);
 
+/* ---- learned con2prim initial guess ------------------------------------- */
+/* No counterpart in the reference (its Newton iteration starts at the bracket
+ * midpoint, conserved.cpp:170): a 6 -> 64 -> 64 -> 2 network (tanh) maps
+ * features of a cell's conserved state to log(xi / D) and log W; con2prim
+ * then starts Newton there (inside the bracket; else at the midpoint) and
+ * keeps the reference's Newton, Brent fallback and acceptance tests.
+ * Parameters (FP32, flat): W1 [64][6], b1 [64], W2 [64][64], b2 [64],
+ * W3 [2][64], b3 [2], then 12 floats of feature normalisation (mean[6],
+ * 1/std[6]); inference reads their BF16 copy and accumulates in FP32. */
+#define BH_MLP_NPARAM 4738
+typedef struct bh_mlp {
+    float *w;                /* [BH_MLP_NPARAM + 12] device                 */
+    void *wb;                /* [BH_MLP_NPARAM] device, bf16                 */
+    float *adam_m, *adam_v;  /* [BH_MLP_NPARAM] device, training only        */
+    int64_t step;            /* Adam steps taken (host)                      */
+} bh_mlp;
+/* the preamble of conserved::ctop (conserved.cpp:135-168): pre [5][n] =
+ * D, tau, Ssq, Bsq, SB (with the reference's assignment loop, A2) */
+int bh_ctop_pre(const bh_params *P, const double *U, const double *r, const double *th, int64_t n, double *pre,
+                void *stream);
+/* bh_ctop with Newton started from xi0[n] where it lies strictly inside the
+ * bracket (NaN or outside: the reference's midpoint) */
+int bh_ctop_guess(const bh_params *P, const double *U, const double *r, const double *th, int64_t n,
+                  const double *xi0, double *W, double *Wd, int32_t *status, int32_t *iters, int32_t *path,
+                  void *stream);
+/* xi0[n] = D exp(y0) of the network (NaN where a feature is not finite) */
+int bh_mlp_guess(const bh_mlp *m, const double *pre, const double *r, int64_t n, double *xi0, void *stream);
+/* one Adam step (lr > 0; lr = 0 only computes) on the mean squared error of
+ * y against target [2][n]; scratch: (4 * 64 + 9) * n + BH_MLP_NPARAM floats,
+ * whose last BH_MLP_NPARAM hold the gradient; loss_out (device, may be NULL)
+ * receives the summed squared error */
+int bh_mlp_train_step(bh_mlp *m, const double *pre, const double *r, const float *target, int64_t n, float lr,
+                      float *scratch, float *loss_out, void *stream);
+/* refresh the BF16 copy from the FP32 weights */
+int bh_mlp_sync_bf16(bh_mlp *m, void *stream);
+
 /* ---- L3 integrator ------------------------------------------------------ */
 /* rk2integrator::dtcomp (solver/integrator.cpp:156-189): *dt_dev = CFL step */
 int bh_dtcomp(const bh_params *P, const bh_pool *pool, double cfl, double *dt_dev, void *stream);

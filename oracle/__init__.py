@@ -148,6 +148,7 @@ class Oracle:
         L.orc_maxdivb_all.argtypes = [PO, _dp]
         L.orc_regrid_flags.argtypes = [PO, C.c_int, C.c_int]
         L.orc_analysis.argtypes = [PP, PO, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp]
+        L.orc_ctop_guess_batch.argtypes = [PP, _dp, _dp, _dp, C.c_int64, _dp, _dp, _dp, _ip, _ip, _ip, _dp]
         L.orc_b_init.argtypes = [PO, C.c_int]
         L.orc_refine_data.argtypes = [PP, PO, C.c_int, _ip]
         L.orc_ccrstr.argtypes = [PP, PO, C.c_int, _ip]
@@ -260,6 +261,19 @@ class Oracle:
         dt = C.c_double(0); s = pool.cstruct()
         self._chk(self.lib.orc_step(C.byref(self.P), C.byref(s), cfl, C.byref(dt)))
         return dt.value
+
+    def ctop_guess(self, U, r, th, xi0=None):
+        """ctop with Newton started from xi0 [n] (None or NaN: the midpoint);
+        returns (W, Wd, status, iters, path, pre) with pre [7][n] = D, tau,
+        Ssq, Bsq, SB, xi_l, xi_h of the preamble."""
+        U = np.ascontiguousarray(U, np.float64); n = U.shape[1]
+        r = np.ascontiguousarray(r, np.float64); th = np.ascontiguousarray(th, np.float64)
+        x = None if xi0 is None else np.ascontiguousarray(xi0, np.float64)
+        W = np.zeros((8, n)); Wd = np.zeros((5, n)); pre = np.zeros((7, n))
+        st = np.zeros(n, np.int32); it = np.zeros(n, np.int32); pa = np.zeros(n, np.int32)
+        self.lib.orc_ctop_guess_batch(C.byref(self.P), _ptr(U), _ptr(r), _ptr(th), n, _ptr(x) if x is not None else None,
+                                      _ptr(W), _ptr(Wd), _ptr(st, _ip), _ptr(it, _ip), _ptr(pa, _ip), _ptr(pre))
+        return W, Wd, st, it, pa, pre
 
     def analysis(self, pool, hrz, rs, rho_min_full=0.01, rho_min_bundle=0.005):
         """Raw integrals of analysis::analyser (quantitatives.cpp), summed in

@@ -332,8 +332,17 @@ static int cp_bd(const orc_params *P, double xa, double xb, double Ssq, double B
 }
 /* ctop (:135-230).  Returns 1 / 0 like the reference's bool, or ORC_EDOMAIN
  * where the reference throws from the EOS. */
+/* ctop with Newton started from xi0 when xi0 lies strictly inside the bracket
+ * (the learned initial guess; NaN: the reference's bracket midpoint), and the
+ * preamble's quantities D, tau, Ssq, Bsq, SB, xi_l, xi_h in pre[7] (may be NULL) */
+static int ctop_g(const orc_params *P, const cons *cv, double r, double th, prim *pv,
+                  int maxiter, double tol, int32_t *iters, int32_t *path, double xi0, double *pre);
 static int ctop_(const orc_params *P, const cons *cv, double r, double th, prim *pv,
                  int maxiter, double tol, int32_t *iters, int32_t *path) {
+    return ctop_g(P, cv, r, th, pv, maxiter, tol, iters, path, NAN, 0);
+}
+static int ctop_g(const orc_params *P, const cons *cv, double r, double th, prim *pv,
+                  int maxiter, double tol, int32_t *iters, int32_t *path, double xi0, double *pre) {
     mcomp mc;
     mcomp_fill(P, r, th, &mc);
     double sg = mc.sqrtdetgam;
@@ -363,6 +372,8 @@ static int ctop_(const orc_params *P, const cons *cv, double r, double th, prim 
         fl = fres(P, xi_h, Ssq, Bsq, SB, D, tau);
     }
     xi = (xi_l + xi_h) / 2.0;
+    if (pre) { pre[0] = D; pre[1] = tau; pre[2] = Ssq; pre[3] = Bsq; pre[4] = SB; pre[5] = xi_l; pre[6] = xi_h; }
+    if (isfinite(xi0) && xi0 > xi_l && xi0 < xi_h) xi = xi0;
     int nr_ok = 1, it = 0, converged = 0;
     for (int i = 0; i < maxiter; i++) {
         double dF;
@@ -411,6 +422,29 @@ static int ctop_(const orc_params *P, const cons *cv, double r, double th, prim 
     pv->b2 = (Bv * Bv + Bsq) / ltz2;
     if (pv->rho <= 0.0 || pv->eps <= 0.0 || pv->p <= 0.0) return 0;
     return 1;
+}
+/* batched ctop with a per-cell Newton start xi0[n] (NaN: the midpoint) and
+ * the preamble quantities pre [7][n] (may be NULL) */
+void orc_ctop_guess_batch(const orc_params *P, const double *U, const double *r, const double *th, int64_t n,
+                          const double *xi0, double *W, double *Wd, int32_t *status, int32_t *iters,
+                          int32_t *path, double *pre) {
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t q = 0; q < n; q++) {
+        cons c; prim pv;
+        c.D = U[q]; c.tau = U[4 * n + q];
+        for (int d = 0; d < 3; d++) { c.S[d] = U[(1 + d) * n + q]; c.B[d] = U[(5 + d) * n + q]; }
+        memset(&pv, 0, sizeof(pv));
+        double pr[7];
+        int32_t it = 0, pa = 0;
+        int ok = ctop_g(P, &c, r[q], th[q], &pv, P->maxiter, P->tol, &it, &pa, xi0 ? xi0[q] : NAN, pr);
+        W[q] = pv.rho; W[n + q] = pv.eps;
+        for (int d = 0; d < 3; d++) { W[(2 + d) * n + q] = pv.v[d]; W[(5 + d) * n + q] = pv.B[d]; }
+        if (Wd) { Wd[q] = pv.p; Wd[n + q] = pv.T; Wd[2 * n + q] = pv.h; Wd[3 * n + q] = pv.lor; Wd[4 * n + q] = pv.b2; }
+        status[q] = ok;
+        if (iters) iters[q] = it;
+        if (path) path[q] = pa;
+        if (pre) for (int k = 0; k < 7; k++) pre[k * n + q] = pr[k];
+    }
 }
 int orc_ctop(const orc_params *P, const double U[8], double r, double th, double W[8],
              double Wd[5], int32_t *iters, int32_t *path) {

@@ -135,6 +135,11 @@ int orc_update(const orc_params *P, orc_pool *pool, double dt, int stage); /* :3
 int orc_rkstg(const orc_params *P, orc_pool *pool, double dt, int stage);
 int orc_step(const orc_params *P, orc_pool *pool, double cfl, double *dt);
 
+/* ctop with a learned Newton start (xi0 NaN: the reference's midpoint) */
+void orc_ctop_guess_batch(const orc_params *P, const double *U, const double *r, const double *th, int64_t n,
+                          const double *xi0, double *W, double *Wd, int32_t *status, int32_t *iters,
+                          int32_t *path, double *pre);
+
 /* batch helpers used by the tests (vectorised over n items, SoA [8][n]) */
 void orc_metric_batch(const orc_params *P, const double *r, const double *th,
                       int64_t n, double *mc);

@@ -1,0 +1,67 @@
+"""The learned con2prim guess on the device: the network's gradient
+(bh_mlp_train_step) against the CPU restatement (oracle/mlp.py), training on
+solver-generated pairs, and what the trained guess does to the reference's
+con2prim on held-out cells of the stress batch (Kerr a = 0.9375): fewer
+Newton iterations, no more failures, the same primitives where both
+succeed (both stop at |f(xi)| < 1e-10)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp
+
+pytestmark = pytest.mark.gpu
+
+
+def batch(n, seed):
+    import bhgpu
+    from bhgpu import configs
+    W, r, th = configs.con2prim_batch(n, seed=seed)
+    cn = bhgpu.Conserved(bhgpu.Metric(1.0, 0.9375, 0.0), bhgpu.State(4.0 / 3.0))
+    U, _ = cn.ptoc(W, r, th, check_domain=False)
+    return cn, U, torch.as_tensor(r, device="cuda"), torch.as_tensor(th, device="cuda")
+
+
+def test_gradient_matches_the_cpu_restatement():
+    import bhgpu
+    cn, U, r, th = batch(2048, 11)
+    g = bhgpu.C2PGuess(cn, seed=3)
+    pre = g.preamble(U, r, th)
+    x = g.features(pre, r)
+    ok = torch.isfinite(x).all(0) & torch.isfinite(pre).all(0)
+    idx = torch.nonzero(ok).flatten()
+    pre, rr, x = pre[:, idx].contiguous(), r[idx].contiguous(), x[:, idx]
+    g.w[mlp.NPARAM:mlp.NPARAM + 6] = x.mean(1)
+    g.w[mlp.NPARAM + 6:] = 1.0 / x.std(1)
+    import ctypes as C
+    from bhgpu.c2p_guess import lib
+    lib.bh_mlp_sync_bf16(C.byref(g.s), None)
+    rng = np.random.default_rng(0)
+    tgt = torch.as_tensor(rng.normal(size=(2, idx.numel())), dtype=torch.float32, device="cuda")
+    L, grad = g.gradient(pre, rr, tgt)
+    Lc, gc = mlp.loss_and_grad(g.w.double().cpu().numpy(), mlp.features(pre.cpu().numpy(), rr.cpu().numpy()),
+                               tgt.double().cpu().numpy().T)
+    assert abs(L - Lc) <= 1e-4 * abs(Lc)
+    assert np.abs(grad - gc).max() <= 1e-3 * np.abs(gc).max()
+
+
+def test_trained_guess_saves_newton_iterations():
+    import bhgpu
+    cn, U, r, th = batch(1 << 16, 5)
+    g = bhgpu.C2PGuess(cn, seed=0)
+    hist = g.train(U, r, th, steps=1500, batch=8192)
+    assert hist[-1] < 0.05 * hist[0]
+    cn2, U2, r2, th2 = batch(1 << 16, 6)             # held out
+    W0, Wd0, st0, it0, pa0 = cn.ctop(U2, r2, th2, check_domain=False)
+    W1, Wd1, st1, it1, pa1 = g.ctop(U2, r2, th2)
+    ok0, ok1 = st0 == 1, st1 == 1
+    both = ok0 & ok1
+    it_plain = it0[both].double().mean().item()
+    it_guess = it1[both].double().mean().item()
+    fail0, fail1 = 1 - ok0.double().mean().item(), 1 - ok1.double().mean().item()
+    rel = ((W1[0] - W0[0]).abs() / W0[0].abs())[both]
+    print(f"loss {hist[0]:.3g} -> {hist[-1]:.3g}; Newton iterations {it_plain:.2f} -> {it_guess:.2f}; "
+          f"failed {fail0:.4f} -> {fail1:.4f}; rho rel diff max {rel.max().item():.2e}")
+    assert it_guess < 0.95 * it_plain
+    assert fail1 <= fail0 + 2e-3
+    assert rel.max().item() <= 1e-6
