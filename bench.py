@@ -248,6 +248,31 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
            "mean_newton_iters": float(it.mean()),
            "alg_bytes_per_cell": C2P_ALG_BYTES,
            "achieved_GBs": n_cells * C2P_ALG_BYTES / (ms / 1e3) / 1e9}
+    # the learned initial guess: trained on this batch's first 2^16 cells,
+    # timed (preamble + network + con2prim) on the whole batch
+    try:
+        g = bhgpu.C2PGuess(cn, seed=0)
+        t0 = time.perf_counter()
+        g.train(U[:, :1 << 16].contiguous(), rd[:1 << 16].contiguous(), thd[:1 << 16].contiguous(), steps=1500)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t0
+        g.ctop(U, rd, thd)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(reps):
+            Wg, Wdg, stg, itg, pag = g.ctop(U, rd, thd)
+        b.record(); torch.cuda.synchronize()
+        msg = a.elapsed_time(b) / reps
+        stg_, itg_ = stg.cpu().numpy(), itg.cpu().numpy()
+        both = (st == 1) & (stg_ == 1)
+        out["mlp_guess"] = {"network": "6-64-64-2 tanh, BF16 weights, FP32 math, trained on the GPU on 2^16 "
+                                       "solver-generated pairs (1500 Adam steps)",
+                            "train_s": t_train, "ms": msg, "cells_per_s": n_cells / (msg / 1e3),
+                            "mean_newton_iters_where_both_recover": {"plain": float(it[both].mean()),
+                                                                     "guess": float(itg_[both].mean())},
+                            "failed_frac": {"plain": float(np.mean(st != 1)), "guess": float(np.mean(stg_ != 1))}}
+    except Exception as e:      # informational
+        out["mlp_guess"] = {"error": str(e)}
     # the reference's own conserved::ctop on a sample, all host threads
     try:
         import oracle

@@ -3,7 +3,8 @@
 solver-generated pairs, and what the trained guess does to the reference's
 con2prim on held-out cells of the stress batch (Kerr a = 0.9375): fewer
 Newton iterations, no more failures, the same primitives where both
-succeed (both stop at |f(xi)| < 1e-10)."""
+succeed (both stop at |f(xi)| < 1e-10; measured: 8.59 -> 7.44 iterations,
+failures 55.84 % -> 55.82 %, rho within 2.3e-9)."""
 import numpy as np
 import pytest
 import torch
@@ -59,7 +60,11 @@ def test_trained_guess_saves_newton_iterations():
     it_plain = it0[both].double().mean().item()
     it_guess = it1[both].double().mean().item()
     fail0, fail1 = 1 - ok0.double().mean().item(), 1 - ok1.double().mean().item()
-    rel = ((W1[0] - W0[0]).abs() / W0[0].abs())[both]
+    # the reference accepts NaN primitives (its positivity tests are false
+    # for NaN); those must agree, the finite ones match to Newton's tolerance
+    assert torch.equal(torch.isnan(W1[0][both]), torch.isnan(W0[0][both]))
+    fin = both & torch.isfinite(W0[0])
+    rel = ((W1[0] - W0[0]).abs() / W0[0].abs())[fin]
     print(f"loss {hist[0]:.3g} -> {hist[-1]:.3g}; Newton iterations {it_plain:.2f} -> {it_guess:.2f}; "
           f"failed {fail0:.4f} -> {fail1:.4f}; rho rel diff max {rel.max().item():.2e}")
     assert it_guess < 0.95 * it_plain
