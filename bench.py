@@ -238,6 +238,7 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
     b.record(); torch.cuda.synchronize()
     ms = a.elapsed_time(b) / reps
     st, it, pa = st.cpu().numpy(), it.cpu().numpy(), pa.cpu().numpy()
+    Wg0 = Wg.cpu().numpy()
     out = {"workload": f"con2prim stress batch: {n_cells} independent Kerr-Schild cells (a=0.9375, Gamma=4/3), "
                        "log-uniform rho, W in [1,20], log-uniform sigma, isotropic v and B, r in [1.5,50]",
            "cells": n_cells, "ms": ms, "cells_per_s": n_cells / (ms / 1e3),
@@ -270,7 +271,9 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
                             "train_s": t_train, "ms": msg, "cells_per_s": n_cells / (msg / 1e3),
                             "mean_newton_iters_where_both_recover": {"plain": float(it[both].mean()),
                                                                      "guess": float(itg_[both].mean())},
-                            "failed_frac": {"plain": float(np.mean(st != 1)), "guess": float(np.mean(stg_ != 1))}}
+                            "failed_frac": {"plain": float(np.mean(st != 1)), "guess": float(np.mean(stg_ != 1))},
+                            "other_root_frac": float(np.mean(np.abs(Wg[0].cpu().numpy()[both] - Wg0[0][both]) >
+                                                             1e-6 * np.abs(Wg0[0][both])))}
     except Exception as e:      # informational
         out["mlp_guess"] = {"error": str(e)}
     # the reference's own conserved::ctop on a sample, all host threads
