@@ -239,6 +239,7 @@ BH_HD inline void reconfp(const KP& kp, const Pool& P, int p, int i, int j, int 
         recon_scal(log(RT(We[lm])), log(RT(We[lc])), log(RT(We[lp])), log(RT(We[lpp])), lim, L.eps, R.eps);
         L.eps = exp(L.eps); R.eps = exp(R.eps);
     }
+#pragma unroll
     for (int d = 0; d < 3; d++) {
         const double* x = Wv(P, p, 2 + d);
         recon_scal(RT(x[lm]), RT(x[lc]), RT(x[lp]), RT(x[lpp]), lim, L.v[d], R.v[d]);
@@ -256,6 +257,7 @@ BH_HD inline void reconfp(const KP& kp, const Pool& P, int p, int i, int j, int 
         causalv(L.v, met_cast<RT>(mL));
         causalv(R.v, met_cast<RT>(mR));
     }
+#pragma unroll
     for (int d = 0; d < 3; d++) {
         const double* x = Wv(P, p, 5 + d);
         if (d == dim) { L.B[d] = RT(x[lc]); R.B[d] = RT(x[lp]); }
@@ -291,7 +293,10 @@ BH_HD inline void flux_item(const KP& kp, const Pool& P, int p, int dim, int f) 
     if (dim == 0) { bn = Bfv(P, p, 0)[xfc(i + 1, j, k)]; fi = xfc(i, j, k); }
     else if (dim == 1) { bn = Bfv(P, p, 1)[yfc(i, j + 1, k)]; fi = yfc(i, j, k); }
     else { bn = Bfv(P, p, 2)[zfc(i, j, k + 1)]; fi = zfc(i, j, k); }
-    L.B[dim] = RT(bn); R.B[dim] = RT(bn);
+    // constant indices keep L and R in registers (dim is a launch index)
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        if (d == dim) { L.B[d] = RT(bn); R.B[d] = RT(bn); }
     int lL = lindx(i, j, k), lR = lindx(i + (dim == 0), j + (dim == 1), k + (dim == 2));
     double rf = (rr(P, p, lL) + rr(P, p, lR)) / 2;
     double thf = (tt(P, p, lL) + tt(P, p, lR)) / 2;
@@ -370,9 +375,12 @@ BH_HD inline void div_flux(const Pool& P, int p, int i, int j, int k, double sg,
     int xr = xfc(i, j, k), xl = xfc(i - 1, j, k);
     int yr = yfc(i, j, k), yl = yfc(i, j - 1, k);
     int zr = zfc(i, j, k), zl = zfc(i, j, k - 1);
+    double idx = 1.0 / dx, idy = 1.0 / dy, idz = 1.0 / dz, isg = 1.0 / sg;
+#pragma unroll
     for (int v = 0; v < 5; v++) {
         const double *Fx = Fv(P, p, 0, v), *Fy = Fv(P, p, 1, v), *Fz = Fv(P, p, 2, v);
-        out[v] = -((Fx[xr] - Fx[xl]) / dx + (Fy[yr] - Fy[yl]) / dy + (Fz[zr] - Fz[zl]) / dz) / sg;
+        out[v] = -quo(quo(Fx[xr] - Fx[xl], dx, idx) + quo(Fy[yr] - Fy[yl], dy, idy) + quo(Fz[zr] - Fz[zl], dz, idz),
+                      sg, isg);
     }
     out[5] = out[6] = out[7] = 0.0;
 }
@@ -400,21 +408,22 @@ BH_HD inline bool source(const KP& kp, const MetSrc& mc, const Prim& Wd, RT out[
         v2 += vlow[m] * W.v[m];
     }
     v2 = smin(v2, RT(1) - RT(1e-10));
-    RT ltz2 = RT(1.0) / (RT(1.0) - v2);
+    RT om = RT(1.0) - v2;                 // 1 / ltz2 within an ulp
+    RT ltz2 = RT(1.0) / om;
     RT ltz = sqrt(ltz2);
     RT Bv = RT(0.0), Bsq = RT(0.0);
     for (int m = 0; m < 3; m++) { Bv += Blow[m] * W.v[m]; Bsq += Blow[m] * W.B[m]; }
-    RT b2 = Bv * Bv + Bsq / ltz2;
+    RT b2 = Bv * Bv + quo(Bsq, ltz2, om);
     bool ok = eos_ok(W.rho);
     RT g = RT(kp.gamma);
     RT px = press(g, W.rho, W.eps);
     RT h = enth(g, W.eps);
-    RT alpha = RT(mc.alpha);
+    RT alpha = RT(mc.alpha), ialpha = RT(1.0) / alpha, iltz = RT(1.0) / ltz;
     RT u4[4], b4[4];
-    u4[0] = ltz / alpha;
-    for (int m = 0; m < 3; m++) u4[m + 1] = ltz * (W.v[m] - RT(mc.beta[m]) / alpha);
-    b4[0] = ltz * Bv / alpha;
-    for (int m = 0; m < 3; m++) b4[m + 1] = (W.B[m] + alpha * b4[0] * u4[m + 1]) / ltz;
+    u4[0] = quo(ltz, alpha, ialpha);
+    for (int m = 0; m < 3; m++) u4[m + 1] = ltz * (W.v[m] - quo(RT(mc.beta[m]), alpha, ialpha));
+    b4[0] = quo(ltz * Bv, alpha, ialpha);
+    for (int m = 0; m < 3; m++) b4[m + 1] = quo(W.B[m] + alpha * b4[0] * u4[m + 1], ltz, iltz);
     RT T44[4][4];
     RT rhohb2 = W.rho * h + b2;
     for (int m = 0; m < 4; m++)

@@ -4,6 +4,8 @@
 // con2prim stay FP64.  Compiled with FMA contraction and fast FP32
 // division/square root; logf/expf keep their full accuracy.
 #define BH_VARIANT vmixed
+#define BH_RCP   // reciprocals formed once for repeated divisors (quo)
 #define BH_REAL float
 #define BH_MINB_FLUX 6   // the FP32 face computation needs fewer registers
+#define BH_FLUX_ALT 4, 8
 #include "bh_variant.cuh"

@@ -37,6 +37,24 @@ BH_HD inline double pow_3(double x) { return pow(x, 3.0); }
 BH_HD inline double pow_4(double x) { return pow(x, 4); }
 #endif
 
+// ---- quotients ---------------------------------------------------------
+// quo(a, b, rb) is the reference's a / b.  Variants compiled with BH_RCP
+// (the FMA-contracted FP64 one and the mixed one) multiply by rb, a
+// reciprocal of b the caller forms once for several quotients with the same
+// divisor: each quotient moves by an ulp or two, as a contracted multiply-add
+// does, and a multiply replaces the multi-instruction IEEE division.  In the
+// reference-faithful build rb is never read and its computation is dead.
+template <typename T>
+BH_HD inline T quo(T a, T b, T rb) {
+#ifdef BH_RCP
+    (void)b;
+    return a * rb;
+#else
+    (void)rb;
+    return a / b;
+#endif
+}
+
 constexpr int BLK = 16, GH = 2, CPN = 20;
 constexpr int NC = CPN * CPN * CPN;                 // 8000 cells / patch
 constexpr int NF = (CPN + 1) * CPN * CPN;           // 8400 faces / direction
@@ -252,7 +270,8 @@ BH_HD inline bool ptoc(RT gamma, const MetT<RT>& mc, const PrimT<RT>& pv, ConsT<
         v2 += vlow[i] * pv.v[i];
     }
     v2 = smin(v2, RT(1.0) - RT(1e-10));
-    RT lor = RT(1.0) / sqrt(RT(1.0) - v2);
+    RT sq1v = sqrt(RT(1.0) - v2);
+    RT lor = RT(1.0) / sq1v;              // 1 / lor = sq1v within an ulp
     bool ok = eos_ok(pv.rho);
     RT p = press(gamma, pv.rho, pv.eps);
     RT h = enth(gamma, pv.eps);
@@ -269,7 +288,7 @@ BH_HD inline bool ptoc(RT gamma, const MetT<RT>& mc, const PrimT<RT>& pv, ConsT<
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) Bsq += Blow[i] * mc.gam[i][j] * pv.B[j];
-    RT b2 = (Bv * Bv + Bsq) / (lor);
+    RT b2 = quo(Bv * Bv + Bsq, lor, sq1v);
     RT bt = lor * Bv / mc.alpha;
     RT pstar = p + b2 / 2;
     RT w = pv.rho * h + b2;
@@ -277,7 +296,7 @@ BH_HD inline bool ptoc(RT gamma, const MetT<RT>& mc, const PrimT<RT>& pv, ConsT<
     CV.tau = sg * (w * lor * lor - pstar - bt * bt) - CV.D;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        RT bi = (Blow[i] + mc.alpha * bt * lor * vlow[i]) / lor;
+        RT bi = quo(Blow[i] + mc.alpha * bt * lor * vlow[i], lor, sq1v);
         CV.S[i] = sg * (w * lor * lor * vlow[i] - mc.alpha * bt * bi);
         CV.B[i] = sg * pv.B[i];
     }
@@ -300,23 +319,28 @@ BH_HD inline double f_df(double gamma, double xi, double Ssq, double Bsq, double
     double xipK = xi + K;
     double vsq = (Ssq * X + Yi * (2.0 * xi + K)) / (X + xipK * xipK);
     if (vsq >= 1.0) { df = 0.0; return 1e30; }
-    double ltz2 = 1.0 / (1.0 - vsq);
+    double om = 1.0 - vsq;                // 1 / ltz2 within an ulp
+    double ltz2 = 1.0 / om;
     double ltz = sqrt(ltz2);
-    double rho = Dn / ltz;
+    // reciprocals for quo: 1 / ltz = sqrt(om) within two ulps; with them the
+    // residual alone (fres) needs neither ltz2 nor ltz
+    double il = sqrt(om), iX = 1.0 / X;
+    double rho = quo(Dn, ltz, il);
     double G = gamma - 1.0;
-    double p = (G / gamma) * (xi / ltz2 - Dn / ltz);
-    double pstar = p + K / (2 * ltz2) + Yi / (2 * X);
+    double p = (G / gamma) * (quo(xi, ltz2, om) - quo(Dn, ltz, il));
+    double pstar = p + quo(K, 2 * ltz2, 0.5 * om) + quo(Yi, 2 * X, 0.5 * iX);
     if (p < 0.0 || rho < 0.0) { df = 0.0; return 1e32; }
     double f = xi - taun - Dn - pstar;
     double N = Ssq * X + Yi * (2.0 * xi + K);
     double Mq = X * xipK * xipK;
     double dN = 2.0 * Ssq * xi + 2.0 * Yi;
     double dM = 2.0 * xi * xipK * xipK + 2.0 * X * X;
-    double dvv = (dN * Mq - dM * N) / (Mq * Mq);
+    double iMq = 1.0 / Mq;
+    double dvv = quo(dN * Mq - dM * N, Mq * Mq, iMq * iMq);
     double dltz2 = ltz2 * ltz2 * dvv;
-    double dltz = dltz2 / (2.0 * ltz);
-    double dp = (G / gamma) * ((1.0 / ltz2) - (xi * dltz2) / (ltz2 * ltz2) + Dn * dltz / ltz2);
-    double dpstar = dp - (K * dltz2) / (2.0 * ltz2 * ltz2) - Yi / (xi * X);
+    double dltz = quo(dltz2, 2.0 * ltz, 0.5 * il);
+    double dp = (G / gamma) * (quo(1.0, ltz2, om) - quo(xi * dltz2, ltz2 * ltz2, om * om) + quo(Dn * dltz, ltz2, om));
+    double dpstar = dp - quo(K * dltz2, 2.0 * ltz2 * ltz2, 0.5 * om * om) - quo(Yi, xi * X, xi * iX * iX);
     df = 1 - dpstar;
     return f;
 }
@@ -362,9 +386,9 @@ struct CtopOut { double p, T, h, lor, b2; int iters, path; };
 // null) receives D, tau, Ssq, Bsq, SB of the preamble
 BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, const Cons& cv, Prim& pv,
                            bool& domain, CtopOut* co = nullptr, double xi0 = NAN, double* pre = nullptr) {
-    double sg = mc.sqrtdetgam;
-    double D = cv.D / sg;
-    double tau = cv.tau / sg;
+    double sg = mc.sqrtdetgam, isg = 1.0 / sg;
+    double D = quo(cv.D, sg, isg);
+    double tau = quo(cv.tau, sg, isg);
     // conserved.cpp:144-150 reads B[j], S[j] for j > i before they are
     // assigned; those reads are zero here (the reference's value on a clean stack)
     double B[3] = {0.0, 0.0, 0.0}, S[3] = {0.0, 0.0, 0.0};
@@ -372,8 +396,8 @@ BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, cons
     double Bsq = 0.0, Ssq = 0.0, SB = 0.0;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        B[i] = cv.B[i] / sg;
-        S[i] = cv.S[i] / sg;
+        B[i] = quo(cv.B[i], sg, isg);
+        S[i] = quo(cv.S[i], sg, isg);
         Bu[i] = mc.gam_inv[i][2] * B[2];     // the inner j-loop assigns; j = 2 survives
         Su[i] = mc.gam_inv[i][2] * S[2];
         Ssq += S[i] * Su[i];
@@ -426,9 +450,10 @@ BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, cons
     double p = press(gamma, pv.rho, pv.eps);
     double hh = enth(gamma, pv.eps);
     double T = p / pv.rho;
+    double ixpQ = 1.0 / xpQ;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        pv.v[i] = (Su[i] + (SB / xi) * Bu[i]) / xpQ;
+        pv.v[i] = quo(Su[i] + (SB / xi) * Bu[i], xpQ, ixpQ);
         pv.B[i] = B[i];
     }
     if (co) {
@@ -460,7 +485,7 @@ BH_HD inline void pvfs(double r, double& rho, double& eps) {
 // HLLD (solver/hlld.cpp)
 // ======================================================================
 template <typename RT> struct SideT {
-    RT rho, eps, p, h, vn, vt1, vt2, Bn, Bt1, Bt2, ltz2, b2, pt, cf, D, tau, Sn, St1, St2, Bc, E;
+    RT rho, eps, p, h, vn, vt1, vt2, Bn, Bt1, Bt2, ltz2, iltz2, b2, pt, cf, D, tau, Sn, St1, St2, Bc, E;
 };
 template <typename RT> struct CstT { RT D, Sn, St1, St2, tau, Bn, Bt1, Bt2; };
 
@@ -480,6 +505,7 @@ BH_HD inline bool side_(RT gamma, const PrimT<RT>& W, const ConsT<RT>& U, const 
     s.p = press(gamma, W.rho, W.eps);
     s.h = enth(gamma, W.eps);
     RT v2 = RT(0.0), vlow[3] = {0, 0, 0}, Blow[3] = {0, 0, 0};
+    RT isg = RT(1.0) / sqrtg;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
 #pragma unroll
@@ -490,22 +516,23 @@ BH_HD inline bool side_(RT gamma, const PrimT<RT>& W, const ConsT<RT>& U, const 
         v2 += vlow[i] * W.v[i];
     }
     v2 = smin(v2, 1 - RT(1e-10));
-    s.ltz2 = RT(1.0) / (RT(1.0) - v2);
+    s.iltz2 = RT(1.0) - v2;               // 1 / ltz2 within an ulp
+    s.ltz2 = RT(1.0) / s.iltz2;
     RT Bv = RT(0.0);
 #pragma unroll
     for (int i = 0; i < 3; i++) Bv += Blow[i] * W.v[i];
     RT Bsq = RT(0.0);
 #pragma unroll
     for (int i = 0; i < 3; i++) Bsq += Blow[i] * W.B[i];
-    s.b2 = Bv * Bv + Bsq / s.ltz2;
+    s.b2 = Bv * Bv + quo(Bsq, s.ltz2, s.iltz2);
     s.vn = W.v[dim]; s.vt1 = W.v[t1]; s.vt2 = W.v[t2];
     s.Bn = W.B[dim]; s.Bt1 = W.B[t1]; s.Bt2 = W.B[t2];
     s.pt = s.p + s.b2 / 2;
     RT cs2 = cs2f(gamma, W.rho, W.eps);
     s.cf = fastspeed(s.rho, s.h, s.b2, cs2);
-    s.D = U.D / sqrtg; s.tau = U.tau / sqrtg;
-    s.Sn = U.S[dim] / sqrtg; s.St1 = U.S[t1] / sqrtg; s.St2 = U.S[t2] / sqrtg;
-    s.Bc = U.B[dim] / sqrtg;
+    s.D = quo(U.D, sqrtg, isg); s.tau = quo(U.tau, sqrtg, isg);
+    s.Sn = quo(U.S[dim], sqrtg, isg); s.St1 = quo(U.S[t1], sqrtg, isg); s.St2 = quo(U.S[t2], sqrtg, isg);
+    s.Bc = quo(U.B[dim], sqrtg, isg);
     s.E = s.tau + s.D;
     return ok;
 }
@@ -514,10 +541,10 @@ BH_HD inline CstT<RT> physflux(const SideT<RT>& s, RT a, RT btn) {     // :97-12
     CstT<RT> F;
     RT vn = s.vn;
     F.D = s.D * vn;
-    F.tau = (s.E + s.pt) * vn - s.Bn * (s.Bn * vn + s.Bt1 * s.vt1 + s.Bt2 * s.vt2) / s.ltz2;
-    F.Sn = s.Sn * vn - s.Bn * s.Bn / s.ltz2 + s.pt;
-    F.St1 = s.St1 * vn - s.Bt1 * s.Bn / s.ltz2;
-    F.St2 = s.St2 * vn - s.Bt2 * s.Bn / s.ltz2;
+    F.tau = (s.E + s.pt) * vn - quo(s.Bn * (s.Bn * vn + s.Bt1 * s.vt1 + s.Bt2 * s.vt2), s.ltz2, s.iltz2);
+    F.Sn = s.Sn * vn - quo(s.Bn * s.Bn, s.ltz2, s.iltz2) + s.pt;
+    F.St1 = s.St1 * vn - quo(s.Bt1 * s.Bn, s.ltz2, s.iltz2);
+    F.St2 = s.St2 * vn - quo(s.Bt2 * s.Bn, s.ltz2, s.iltz2);
     F.Bn = RT(0.0);
     F.Bt1 = s.Bt1 * vn - s.Bn * s.vt1;
     F.Bt2 = s.Bt2 * vn - s.Bn * s.vt2;
@@ -534,32 +561,34 @@ BH_HD inline CstT<RT> physflux(const SideT<RT>& s, RT a, RT btn) {     // :97-12
 template <typename RT>
 BH_HD inline CstT<RT> hll_flux(const SideT<RT>& L, const SideT<RT>& R, const CstT<RT>& FL, const CstT<RT>& FR, RT SL,
                                         RT SR) {                            // :124-137
-    RT dS = SR - SL;
+    RT dS = SR - SL, idS = RT(1.0) / dS;
     CstT<RT> F;
-    F.D = (SR * FL.D - SL * FR.D + SL * SR * (R.D - L.D)) / dS;
-    F.tau = (SR * FL.tau - SL * FR.tau + SL * SR * (R.tau - L.tau)) / dS;
-    F.Sn = (SR * FL.Sn - SL * FR.Sn + SL * SR * (R.Sn - L.Sn)) / dS;
-    F.St1 = (SR * FL.St1 - SL * FR.St1 + SL * SR * (R.St1 - L.St1)) / dS;
-    F.St2 = (SR * FL.St2 - SL * FR.St2 + SL * SR * (R.St2 - L.St2)) / dS;
-    F.Bn = (SR * FL.Bn - SL * FR.Bn + SL * SR * (R.Bn - L.Bn)) / dS;
-    F.Bt1 = (SR * FL.Bt1 - SL * FR.Bt1 + SL * SR * (R.Bt1 - L.Bt1)) / dS;
-    F.Bt2 = (SR * FL.Bt2 - SL * FR.Bt2 + SL * SR * (R.Bt2 - L.Bt2)) / dS;
+    F.D = quo(SR * FL.D - SL * FR.D + SL * SR * (R.D - L.D), dS, idS);
+    F.tau = quo(SR * FL.tau - SL * FR.tau + SL * SR * (R.tau - L.tau), dS, idS);
+    F.Sn = quo(SR * FL.Sn - SL * FR.Sn + SL * SR * (R.Sn - L.Sn), dS, idS);
+    F.St1 = quo(SR * FL.St1 - SL * FR.St1 + SL * SR * (R.St1 - L.St1), dS, idS);
+    F.St2 = quo(SR * FL.St2 - SL * FR.St2 + SL * SR * (R.St2 - L.St2), dS, idS);
+    F.Bn = quo(SR * FL.Bn - SL * FR.Bn + SL * SR * (R.Bn - L.Bn), dS, idS);
+    F.Bt1 = quo(SR * FL.Bt1 - SL * FR.Bt1 + SL * SR * (R.Bt1 - L.Bt1), dS, idS);
+    F.Bt2 = quo(SR * FL.Bt2 - SL * FR.Bt2 + SL * SR * (R.Bt2 - L.Bt2), dS, idS);
     return F;
 }
 template <typename RT>
 BH_HD inline CstT<RT> star_stt(const SideT<RT>& s, RT SK, RT SM, RT pt_x) {  // :140-159
     CstT<RT> Ux;
-    Ux.D = s.D * (SK - s.vn) / (SK - SM);
-    Ux.tau = (s.E * (SK - s.vn) - s.pt * s.vn + pt_x * SM) / (SK - SM) - Ux.D;
-    Ux.Sn = (s.Sn * (SK - s.vn) - s.pt + pt_x) / (SK - SM);
-    Ux.St1 = s.St1 * (SK - s.vn) / (SK - SM);
-    Ux.St2 = s.St2 * (SK - s.vn) / (SK - SM);
+    RT dK = SK - SM, idK = RT(1.0) / dK;
+    Ux.D = quo(s.D * (SK - s.vn), dK, idK);
+    Ux.tau = quo(s.E * (SK - s.vn) - s.pt * s.vn + pt_x * SM, dK, idK) - Ux.D;
+    Ux.Sn = quo(s.Sn * (SK - s.vn) - s.pt + pt_x, dK, idK);
+    Ux.St1 = quo(s.St1 * (SK - s.vn), dK, idK);
+    Ux.St2 = quo(s.St2 * (SK - s.vn), dK, idK);
     Ux.Bn = s.Bc;
     RT den = s.D * (SK - s.vn) * (SK - SM) - s.Bn * s.Bn;
     if (fabs(den) > RT(1e-14)) {
         RT k = s.Bn * (SM - s.vn) / den;
-        Ux.Bt1 = s.Bt1 - s.Bn * (s.vt1 * (SK - s.vn) + s.Bn * s.Bt1 / s.D) * k;
-        Ux.Bt2 = s.Bt2 - s.Bn * (s.vt2 * (SK - s.vn) + s.Bn * s.Bt2 / s.D) * k;
+        RT iD = RT(1.0) / s.D;
+        Ux.Bt1 = s.Bt1 - s.Bn * (s.vt1 * (SK - s.vn) + quo(s.Bn * s.Bt1, s.D, iD)) * k;
+        Ux.Bt2 = s.Bt2 - s.Bn * (s.vt2 * (SK - s.vn) + quo(s.Bn * s.Bt2, s.D, iD)) * k;
     } else {
         Ux.Bt1 = s.Bt1; Ux.Bt2 = s.Bt2;
     }
@@ -576,20 +605,25 @@ BH_HD inline void alfstar_stt(const CstT<RT>& UxL, const CstT<RT>& UxR, RT Bn, R
     RT sq_DL = sqrt(fabs(UxL.D));
     RT sq_DR = sqrt(fabs(UxR.D));
     RT den = sq_DL + sq_DR;
+    RT iden = RT(1.0) / den, iDL = RT(1.0) / UxL.D, iDR = RT(1.0) / UxR.D;
     RT sgnBn = (Bn >= RT(0.0)) ? RT(1.0) : -RT(1.0);
-    RT vt1xx = (sq_DL * UxL.St1 / UxL.D + sq_DR * UxR.St1 / UxR.D + sgnBn * (UxR.Bt1 - UxL.Bt1)) / den;
-    RT vt2xx = (sq_DL * UxL.St2 / UxL.D + sq_DR * UxR.St2 / UxR.D + sgnBn * (UxR.Bt2 - UxL.Bt2)) / den;
-    RT Bt1xx = (sq_DL * UxL.Bt1 / UxL.D + sq_DR * UxR.Bt1 / UxR.D +
-                    sgnBn * sq_DL * sq_DR * (UxR.St1 / UxR.D - UxL.St1 / UxL.D)) / den;
-    RT Bt2xx = (sq_DL * UxL.Bt2 / UxL.D + sq_DR * UxR.Bt2 / UxR.D +
-                    sgnBn * sq_DL * sq_DR * (UxR.St2 / UxR.D - UxL.St2 / UxL.D)) / den;
+    RT vt1xx = quo(quo(sq_DL * UxL.St1, UxL.D, iDL) + quo(sq_DR * UxR.St1, UxR.D, iDR) + sgnBn * (UxR.Bt1 - UxL.Bt1),
+                   den, iden);
+    RT vt2xx = quo(quo(sq_DL * UxL.St2, UxL.D, iDL) + quo(sq_DR * UxR.St2, UxR.D, iDR) + sgnBn * (UxR.Bt2 - UxL.Bt2),
+                   den, iden);
+    RT Bt1xx = quo(quo(sq_DL * UxL.Bt1, UxL.D, iDL) + quo(sq_DR * UxR.Bt1, UxR.D, iDR) +
+                       sgnBn * sq_DL * sq_DR * (quo(UxR.St1, UxR.D, iDR) - quo(UxL.St1, UxL.D, iDL)),
+                   den, iden);
+    RT Bt2xx = quo(quo(sq_DL * UxL.Bt2, UxL.D, iDL) + quo(sq_DR * UxR.Bt2, UxR.D, iDR) +
+                       sgnBn * sq_DL * sq_DR * (quo(UxR.St2, UxR.D, iDR) - quo(UxL.St2, UxL.D, iDL)),
+                   den, iden);
     UxxL.St1 = UxL.D * vt1xx; UxxR.St1 = UxR.D * vt1xx;
     UxxL.St2 = UxL.D * vt2xx; UxxR.St2 = UxR.D * vt2xx;
     UxxL.Bt1 = Bt1xx; UxxR.Bt1 = Bt1xx;
     UxxL.Bt2 = Bt2xx; UxxR.Bt2 = Bt2xx;
     UxxL.Sn = UxL.D * SM; UxxR.Sn = UxR.D * SM;
-    const RT vt1xL = UxL.St1 / UxL.D, vt2xL = UxL.St2 / UxL.D;
-    const RT vt1xR = UxR.St1 / UxR.D, vt2xR = UxR.St2 / UxR.D;
+    const RT vt1xL = quo(UxL.St1, UxL.D, iDL), vt2xL = quo(UxL.St2, UxL.D, iDL);
+    const RT vt1xR = quo(UxR.St1, UxR.D, iDR), vt2xR = quo(UxR.St2, UxR.D, iDR);
     RT dE_L = sq_DL * sgnBn * (vt1xx * Bt1xx + vt2xx * Bt2xx - vt1xL * UxL.Bt1 - vt2xL * UxL.Bt2);
     RT dE_R = sq_DR * sgnBn * (vt1xx * Bt1xx + vt2xx * Bt2xx - vt1xR * UxR.Bt1 - vt2xR * UxR.Bt2);
     UxxL.tau = UxL.tau - dE_L;

@@ -11,21 +11,26 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 LIB = os.path.join(HERE, "libhostcheck.so")
+# the same items with the reciprocal-reuse quotients of the FMA and mixed
+# variants (BH_RCP), still without contraction
+LIB_RCP = os.path.join(HERE, "libhostcheck_rcp.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 
-def build():
+def build(rcp: bool = False):
+    lib = LIB_RCP if rcp else LIB
     src = os.path.join(HERE, "hostcheck.cu")
     csrc = os.path.join(REPO, "black-hole-simulator_b200", "csrc")
     deps = [src] + [os.path.join(csrc, f) for f in os.listdir(csrc)] + [os.path.join(REPO, "include", "bhgpu.h")]
-    if os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(d) for d in deps):
-        return
+    if os.path.exists(lib) and all(os.path.getmtime(lib) >= os.path.getmtime(d) for d in deps):
+        return lib
     cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O2",
            "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", "-I" + os.path.join(REPO, "include"),
-           "-I" + csrc, src, "-o", LIB]
+           "-I" + csrc] + (["-DBH_RCP"] if rcp else []) + [src, "-o", lib]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(r.stderr)
+    return lib
 
 
 def _d(a):
@@ -34,13 +39,13 @@ def _d(a):
 
 
 class HostKernels:
-    def __init__(self, M, a, Q, gamma, limiter, maxiter=500, tol=1e-10):
-        build()
+    def __init__(self, M, a, Q, gamma, limiter, maxiter=500, tol=1e-10, rcp=False):
+        lib = build(rcp)
         import sys
         sys.path.insert(0, os.path.join(REPO, "black-hole-simulator_b200"))
         from bhgpu._lib import BhParams, BhPool
         self.BhPool = BhPool
-        self.L = C.CDLL(LIB)
+        self.L = C.CDLL(lib)
         self.P = BhParams(M, a, Q, gamma, limiter, maxiter, tol, 1.0, 0.0, 0.0)
         self.L.hc_dtcomp.restype = C.c_double
         self.L.hc_step.restype = C.c_double

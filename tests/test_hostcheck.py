@@ -245,3 +245,76 @@ def test_analysis_items_bitwise():
     hk.L.hc_analysis(C.byref(hk.P), C.byref(pool), C.byref(A), _d(out))
     raw, _ = orc.analysis(hp, 2.0, 10.0)
     assert eq(out, raw)
+
+
+# ---- the reciprocal-reuse quotients (BH_RCP) of the FMA and mixed variants
+
+def _rel(a, b):
+    m = np.isfinite(a) & np.isfinite(b)
+    scale = np.abs(b[m]).max()
+    return float(np.abs(a[m] - b[m]).max() / scale) if scale > 0 else 0.0
+
+
+@pytest.mark.parametrize("M,a,Q", [(0.0, 0.0, 0.0), (1.0, 0.9375, 0.0)])
+def test_reciprocal_form_physics_close(M, a, Q):
+    """ptoc and HLLD with reciprocals in place of repeated divisions stay
+    within a few ulps of the reference's quotients (relative to each output
+    row's magnitude); con2prim's outcome changes on no more cells than the
+    reference's own changes on a one-ulp move of its input, and where both
+    recover, the primitives agree to the Newton tolerance's width."""
+    rng = np.random.default_rng(2)
+    W, r, th = random_prims(5000, rng)
+    orc = oracle.Oracle(M, a, Q, GAMMA)
+    hk = HostKernels(M, a, Q, GAMMA, 1, rcp=True)
+    n = W.shape[1]
+    U = np.zeros((8, n)); Wd = np.zeros((4, n))
+    hk.call("hc_ptoc", _d(W), _d(r), _d(th), C.c_int64(n), _d(U), _d(Wd))
+    Uc, Wdc = orc.ptoc(W, r, th)
+    assert np.array_equal(np.isfinite(U), np.isfinite(Uc))
+    for v in range(8):
+        assert _rel(U[v], Uc[v]) <= 1e-14, v
+    WR = W.copy(); WR[0] *= 1.07; WR[2:5] += 0.01
+    UR, _ = orc.ptoc(WR, r, th)
+    for dim in range(3):
+        F = np.zeros((8, n)); cts = np.zeros(n)
+        hk.call("hc_hlld", _d(W), _d(WR), _d(Uc), _d(UR), _d(r), _d(th), C.c_int(dim), C.c_int64(n), _d(F), _d(cts))
+        Fc, cc, _ = orc.hlld(W, WR, Uc, UR, r, th, dim)
+        assert _rel(cts, cc) <= 1e-14
+        for v in range(8):
+            assert _rel(F[v], Fc[v]) <= 1e-13, (dim, v)
+    Wo = np.zeros((8, n)); Wdo = np.zeros((5, n))
+    st = np.zeros(n, np.int32); it = np.zeros(n, np.int32); pa = np.zeros(n, np.int32)
+    hk.call("hc_ctop", _d(Uc), _d(r), _d(th), C.c_int64(n), _d(Wo), _d(Wdo), _d(st), _d(it), _d(pa))
+    Wc, _, stc, _, _ = orc.ctop(Uc, r, th)
+    # Brent's success within its 100 iterations is knife-edge for many of
+    # these cells: the reference's own outcome flips on a one-ulp move of U
+    r2 = np.random.default_rng(5)
+    Up = np.where(r2.random(Uc.shape) < 0.5, np.nextafter(Uc, np.inf), np.nextafter(Uc, -np.inf))
+    stp = orc.ctop(Up, r, th)[2]
+    assert np.mean(st != stc) <= max(1e-3, np.mean(stp != stc))
+    ok = (st == 1) & (stc == 1)
+    for v in range(8):
+        assert _rel(Wo[v, ok], Wc[v, ok]) <= 1e-8, v
+
+
+@pytest.mark.parametrize("case", [CASES[0], CASES[2]])
+def test_reciprocal_form_first_step(case):
+    """One step with the reciprocal quotients meets the first-step gate the
+    FMA-contracted GPU variant meets against the oracle: 1e-12 relative L-inf
+    per conserved field, or 8x the oracle's own response to a one-ulp change
+    of its input."""
+    from helpers import field_linf, rel_linf, ulp_sensitivity
+    q, orc, hp = box_case(2, seed=4, **case)
+    sens = ulp_sensitivity(orc, hp, steps=1)
+    hk = HostKernels(case["M"], case["a"], 0.0, GAMMA, case["lim"], rcp=True)
+    hh = hp.copy()
+    pool = hk.pool(hh)
+    off = np.array([0, hp.npatch], np.int32)
+    waves = np.arange(hp.npatch, dtype=np.int32)
+    dt = hk.L.hc_step(C.byref(hk.P), C.byref(pool), 0.4, _d(waves), _d(off), 1)
+    dtc = orc.step(hp, 0.4)
+    assert abs(dt - dtc) <= 1e-12 * dtc
+    assert np.array_equal(np.isfinite(hh.U), np.isfinite(hp.U))
+    assert max(field_linf(hh.U, hp.U).values()) <= 1e-12
+    for v in range(8):
+        assert rel_linf(hh.U[:, v], hp.U[:, v]) <= max(1e-12, 8 * sens[v]), v
