@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--con2prim-batch", type=int, default=1, help="also measure the 2^24-cell con2prim batch")
+    ap.add_argument("--con2prim-cells", type=int, default=1 << 24, help="cells of the con2prim batch")
     ap.add_argument("--precision", default="fp64-fma", choices=["fp64", "fp64-fma", "mixed"],
                     help="arithmetic variant of the headline value; the other variants are timed beside it")
     return ap.parse_args()
@@ -274,6 +275,37 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
                             "failed_frac": {"plain": float(np.mean(st != 1)), "guess": float(np.mean(stg_ != 1))},
                             "other_root_frac": float(np.mean(np.abs(Wg[0].cpu().numpy()[both] - Wg0[0][both]) >
                                                              1e-6 * np.abs(Wg0[0][both])))}
+        # the same with the network on the tensor cores (bh_ctop_learned)
+        g.ctop_learned(U, rd, thd)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(reps):
+            Wt, Wdt, stt_, itt, pat = g.ctop_learned(U, rd, thd)
+        b.record(); torch.cuda.synchronize()
+        mst = a.elapsed_time(b) / reps
+        # its second kernel alone (Newton / Brent from the same starting points)
+        xi0t = g.ctop_learned(U, rd, thd, want_xi0=True)[5]
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(reps):
+            g.ctop_from(U, rd, thd, xi0t)
+        b.record(); torch.cuda.synchronize()
+        ms_newton = a.elapsed_time(b) / reps
+        stt_, itt = stt_.cpu().numpy(), itt.cpu().numpy()
+        both_t = (st == 1) & (stt_ == 1)
+        fail_t = (st != 1) & (stt_ != 1)
+        out["mlp_guess"]["tensor_core"] = {
+            "kernels": "k_guess_tc (metric, preamble, network as tcgen05.mma BF16 -> FP32 in TMEM, 128-cell "
+                       "tiles, persistent CTAs) + k_ctop_guess (Newton / Brent, one thread per cell)",
+            "ms": mst, "guess_kernel_ms": mst - ms_newton, "newton_kernel_ms": ms_newton,
+            "cells_per_s": n_cells / (mst / 1e3), "speedup_vs_plain": ms / mst,
+            "mean_newton_iters_where_both_recover": {"plain": float(it[both_t].mean()),
+                                                     "guess": float(itt[both_t].mean())},
+            "mean_newton_iters_all_cells": {"plain": float(it.mean()), "guess": float(itt.mean())},
+            "mean_newton_iters_where_both_fail": {"plain": float(it[fail_t].mean()),
+                                                  "guess": float(itt[fail_t].mean())},
+            "failed_frac": float(np.mean(stt_ != 1)),
+            "status_equal_to_three_kernel_form": float(np.mean(stt_ == stg_))}
     except Exception as e:      # informational
         out["mlp_guess"] = {"error": str(e)}
     # the reference's own conserved::ctop on a sample, all host threads
@@ -740,7 +772,7 @@ def run_ours(args):
             v, kind, sample = cpu_reference_sample(threads)
             line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample}
             if args.con2prim_batch:
-                line["con2prim_batch"] = con2prim_batch()
+                line["con2prim_batch"] = con2prim_batch(args.con2prim_cells)
             line["regrid"] = regrid_bench(tree)
             line["analysis"] = analysis_bench(tree)
             line["torus_init"] = torus_bench()

@@ -9,7 +9,7 @@ from .solver import (Metric, State, Conserved, hlld, AmrTree, RK2Integrator, Ste
                      BH_MINMOD, BH_VANLEER, BH_MC)
 from .pipeline import HostPipeline  # noqa: F401
 from .analysis import Analyser  # noqa: F401
-from .c2p_guess import C2PGuess  # noqa: F401
+from .c2p_guess import C2PGuess, wait_selftest  # noqa: F401
 from . import configs  # noqa: F401
 
 __version__ = "0.1.0"

@@ -38,11 +38,22 @@ def _sig():
     lib.bh_mlp_guess.argtypes = [C.POINTER(BhMlp), vp, vp, i64, vp, vp]
     lib.bh_mlp_train_step.argtypes = [C.POINTER(BhMlp), vp, vp, vp, i64, C.c_float, vp, vp, vp]
     lib.bh_mlp_sync_bf16.argtypes = [C.POINTER(BhMlp), vp]
-    for f in ("bh_ctop_pre", "bh_ctop_guess", "bh_mlp_guess", "bh_mlp_train_step", "bh_mlp_sync_bf16"):
+    lib.bh_ctop_learned.argtypes = [P, C.POINTER(BhMlp), vp, vp, vp, i64, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.bh_wait_selftest.argtypes = [vp, vp]
+    for f in ("bh_ctop_pre", "bh_ctop_guess", "bh_mlp_guess", "bh_mlp_train_step", "bh_mlp_sync_bf16",
+              "bh_ctop_learned", "bh_wait_selftest"):
         getattr(lib, f).restype = C.c_int
 
 
 _sig()
+
+
+def wait_selftest() -> int:
+    """Run the tensor-core kernels' bounded wait on an mbarrier nothing
+    arrives on; returns the device error word it leaves (BH_ERR_TIMEOUT = 2)."""
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    check(lib.bh_wait_selftest(_p(err), _stream()), "bh_wait_selftest")
+    return int(err.item())
 
 
 class C2PGuess:
@@ -136,8 +147,12 @@ class C2PGuess:
         """conserved::ctop started from the network's guess: (W, Wd, status,
         iters, path) as Conserved.ctop."""
         U, r, th = _dev(U, "cuda"), _dev(r, "cuda"), _dev(th, "cuda")
+        return self.ctop_from(U, r, th, self.guess(self.preamble(U, r, th), r))
+
+    def ctop_from(self, U, r, th, xi0):
+        """conserved::ctop with Newton started from the given xi0 (bh_ctop_guess)."""
+        U, r, th, xi0 = _dev(U, "cuda"), _dev(r, "cuda"), _dev(th, "cuda"), _dev(xi0, "cuda")
         n = U.shape[1]
-        xi0 = self.guess(self.preamble(U, r, th), r)
         W = torch.empty((8, n), dtype=torch.float64, device=self.device)
         Wd = torch.empty((5, n), dtype=torch.float64, device=self.device)
         st = torch.empty(n, dtype=torch.int32, device=self.device)
@@ -147,3 +162,26 @@ class C2PGuess:
         check(lib.bh_ctop_guess(C.byref(P), _p(U), _p(r), _p(th), n, _p(xi0), _p(W), _p(Wd), _p(st), _p(it), _p(pa),
                                 _stream()), "ctop with guess")
         return W, Wd, st, it, pa
+
+    def ctop_learned(self, U, r, th, want_xi0: bool = False):
+        """The same as ctop() with the network on the tensor cores: one
+        kernel for the metric, the preamble and the network, one for Newton
+        (bh_ctop_learned).  Returns (W, Wd, status, iters, path) and, with
+        want_xi0, the starting points."""
+        U, r, th = _dev(U, "cuda"), _dev(r, "cuda"), _dev(th, "cuda")
+        n = U.shape[1]
+        W = torch.empty((8, n), dtype=torch.float64, device=self.device)
+        Wd = torch.empty((5, n), dtype=torch.float64, device=self.device)
+        st = torch.empty(n, dtype=torch.int32, device=self.device)
+        it = torch.empty(n, dtype=torch.int32, device=self.device)
+        pa = torch.empty(n, dtype=torch.int32, device=self.device)
+        xi0 = torch.empty(n, dtype=torch.float64, device=self.device)
+        err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        P = self._P()
+        check(lib.bh_ctop_learned(C.byref(P), C.byref(self.s), _p(U), _p(r), _p(th), n,
+                                  _p(xi0), _p(W), _p(Wd), _p(st), _p(it), _p(pa),
+                                  _p(err), _stream()), "ctop with the tensor-core guess")
+        if int(err.item()) != 0:
+            raise RuntimeError(f"bh_ctop_learned: device error word {int(err.item())} (tensor-core wait ran out)")
+        out = (W, Wd, st, it, pa)
+        return out + (xi0,) if want_xi0 else out

@@ -135,6 +135,11 @@ int bh_ctop_pre(const bh_params* P, const double* U, const double* r, const doub
                 void* stream) {
     BH_DISPATCH(P, ctop_pre(P, U, r, th, n, pre, stream));
 }
+int bh_ctop_learned(const bh_params* P, const bh_mlp* m, const double* U, const double* r, const double* th,
+                    int64_t n, double* xi0, double* W, double* Wd, int32_t* status, int32_t* iters, int32_t* path,
+                    int32_t* err, void* stream) {
+    BH_DISPATCH(P, ctop_learned(P, m, U, r, th, n, xi0, W, Wd, status, iters, path, err, stream));
+}
 int bh_dtcomp(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, void* stream) {
     BH_DISPATCH(P, dtcomp(P, pool, cfl, dt_dev, stream));
 }

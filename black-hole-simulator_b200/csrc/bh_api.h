@@ -34,6 +34,8 @@
     int ctop_guess(const bh_params*, const double*, const double*, const double*, int64_t, const double*,      \
                    double*, double*, int32_t*, int32_t*, int32_t*, void*);                                     \
     int ctop_pre(const bh_params*, const double*, const double*, const double*, int64_t, double*, void*);    \
+    int ctop_learned(const bh_params*, const bh_mlp*, const double*, const double*, const double*, int64_t,   \
+                     double*, double*, double*, int32_t*, int32_t*, int32_t*, int32_t*, void*);               \
     int refine(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
     int ccrstr(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \
     int b_init(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \

@@ -16,6 +16,7 @@
 #include <stdint.h>
 #include <math.h>
 #include "bhgpu.h"
+#include "bh_tc.cuh"
 
 namespace {
 
@@ -28,15 +29,10 @@ constexpr int TPB = 128;
 inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 inline int launched() { return cudaGetLastError() == cudaSuccess ? BH_OK : BH_ECUDA; }
 
-// features of a cell from the con2prim preamble (D, tau, Ssq, Bsq, SB) and r
+// features of cell q from the con2prim preamble pre [5][n] and r
 __device__ inline void features(const double* pre, const double* r, int64_t n, int64_t q, float x[NI]) {
-    double D = pre[q], tau = pre[n + q], Ssq = pre[2 * n + q], Bsq = pre[3 * n + q], SB = pre[4 * n + q];
-    x[0] = (float)log(D);
-    x[1] = (float)asinh(tau / D);
-    x[2] = (float)log1p(Ssq / (D * D));
-    x[3] = (float)log1p(Bsq / D);
-    x[4] = (float)asinh(SB / (D * sqrt(D)));
-    x[5] = (float)log(r[q]);
+    double p5[5] = {pre[q], pre[n + q], pre[2 * n + q], pre[3 * n + q], pre[4 * n + q]};
+    bh_tc::features(p5, r[q], x);
 }
 
 __device__ inline float bf(__nv_bfloat16 v) { return __bfloat162float(v); }
@@ -169,9 +165,25 @@ __global__ void k_sum(const float* x, int64_t n, float* out) {
     if (threadIdx.x == 0) *out = red[0];
 }
 
+// the bounded wait of the tensor-core kernels on an mbarrier that nothing
+// arrives on: it must give up and report, never hang
+__global__ void k_wait_selftest(int32_t* err) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) bh_tc::mbar_init(&bar);
+    __syncthreads();
+    bool ok = bh_tc::mbar_wait(&bar, 0);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(err, BH_ERR_TIMEOUT);
+}
+
 }  // namespace
 
 extern "C" {
+
+int bh_wait_selftest(int32_t* err, void* stream) {
+    if (!err) return BH_EINVAL;
+    k_wait_selftest<<<1, 32, 0, S(stream)>>>(err);
+    return launched();
+}
 
 int bh_mlp_sync_bf16(bh_mlp* m, void* stream) {
     if (!m || !m->w || !m->wb) return BH_EINVAL;

@@ -383,7 +383,8 @@ struct CtopOut { double p, T, h, lor, b2; int iters, path; };
 // returns 1 ok / 0 failed; *domain set where the reference throws
 // xi0: Newton's start where it lies strictly inside the bracket (the learned
 // guess; NaN, the default, keeps the reference's midpoint); pre[5] (may be
-// null) receives D, tau, Ssq, Bsq, SB of the preamble
+// null) receives D, tau, Ssq, Bsq, SB of the preamble, and with maxiter = 0
+// ctop returns right after it (pv and co are then not written)
 BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, const Cons& cv, Prim& pv,
                            bool& domain, CtopOut* co = nullptr, double xi0 = NAN, double* pre = nullptr) {
     double sg = mc.sqrtdetgam, isg = 1.0 / sg;
@@ -404,6 +405,10 @@ BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, cons
         Bsq += B[i] * Bu[i];
         SB += S[i] * Bu[i];
     }
+    if (pre) {
+        pre[0] = D; pre[1] = tau; pre[2] = Ssq; pre[3] = Bsq; pre[4] = SB;
+        if (maxiter == 0) return 0;   // only the preamble was asked for
+    }
     double xi_l = D;
     double xi_h = tau + D + Bsq / 2.0 + 1e3;
     double fl = fres(gamma, xi_l, Ssq, Bsq, SB, D, tau);
@@ -413,7 +418,6 @@ BH_HD inline int ctop(double gamma, int maxiter, double tol, const Met& mc, cons
         fl = fres(gamma, xi_h, Ssq, Bsq, SB, D, tau);
     }
     double xi = (xi_l + xi_h) / 2.0;
-    if (pre) { pre[0] = D; pre[1] = tau; pre[2] = Ssq; pre[3] = Bsq; pre[4] = SB; }
     if (isfinite(xi0) && xi0 > xi_l && xi0 < xi_h) xi = xi0;
     bool nr_ok = true, conv = false;
     int it = 0;

@@ -15,6 +15,7 @@
 #include "bhgpu.h"
 #include "bh_items.cuh"
 #include "bh_init.cuh"
+#include "bh_tc.cuh"
 
 #ifndef BH_VARIANT
 #error "define BH_VARIANT before including bh_variant.cuh"
@@ -72,6 +73,68 @@ __global__ void k_ctop_guess(KP k, const double* U, const double* r, const doubl
 }
 __global__ void k_ctop_pre(KP k, const double* U, const double* r, const double* th, int64_t n, double* pre) {
     BATCH; ctop_pre_item(k, U, r, th, n, q, pre);
+}
+// the learned con2prim start for every cell, the network on the tensor
+// cores (bh_tc.cuh): one tile of 128 cells per pass, the CTAs persistent
+// over the tiles (grid = the resident CTAs, at most 8 per SM so that their
+// tensor memory always fits).  Per cell: the metric, con2prim's preamble
+// (conserved.cpp:135-150), the features and the network; xi0 = D exp(y0),
+// NaN where a feature is not finite.  The work per cell is nearly uniform,
+// so the CTA-wide steps of the network cost little; con2prim's own
+// iterations, whose count varies from cell to cell, run afterwards in
+// k_ctop_guess (one thread per cell, no barriers).
+__global__ void __launch_bounds__(bh_tc::ROWS, 4)
+    k_guess_tc(KP k, const __nv_bfloat16* wb, const float* norm, const double* U, const double* r,
+               const double* th, int64_t n, double* xi0_out, int32_t* err) {
+    __shared__ bh_tc::Smem s;
+    const int t = threadIdx.x;
+    bh_tc::stage_weights(s, wb, norm);
+    if (t == 0) bh_tc::mbar_init(&s.mbar);
+    if (t < 32) bh_tc::tmem_alloc(&s.tmem);
+    bh_tc::fence_before();
+    __syncthreads();
+    bh_tc::fence_after();
+    const uint32_t tmem = s.tmem;
+    uint32_t phase = 0;
+    bool ok = true;
+    const int64_t ntile = (n + bh_tc::ROWS - 1) / bh_tc::ROWS;
+    for (int64_t tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const int64_t q = tile * bh_tc::ROWS + t;
+        const bool in = q < n;
+        double p5[5] = {NAN, NAN, NAN, NAN, NAN};
+        float xn[bh_tc::NI];
+        bool valid = false;
+        if (in) {
+            Cons c;
+            c.D = U[q]; c.tau = U[4 * n + q];
+            for (int d = 0; d < 3; d++) { c.S[d] = U[(1 + d) * n + q]; c.B[d] = U[(5 + d) * n + q]; }
+            Met mc;
+            met_comp(k.tree, r[q], th[q], mc);
+            Prim w0;
+            bool dom0 = false;
+            ctop(k.gamma, 0, k.tol, mc, c, w0, dom0, nullptr, NAN, p5);   // the preamble only
+            float x[bh_tc::NI];
+            bh_tc::features(p5, r[q], x);
+            valid = true;
+            for (int i = 0; i < bh_tc::NI; i++) {
+                valid &= isfinite(x[i]);
+                xn[i] = (x[i] - s.norm[i]) * s.norm[bh_tc::NI + i];
+            }
+        }
+        float y0 = 0.0f;
+        if (!bh_tc::network(s, tmem, phase, xn, valid, y0)) { ok = false; break; }
+        if (in) xi0_out[q] = valid ? p5[0] * exp((double)y0) : NAN;
+    }
+    if (!ok) {
+        // an MMA did not complete in time: record it, give it one more bounded
+        // wait, then release the tensor memory all the same
+        bh_tc::mbar_wait(&s.mbar, phase ^ 1u);
+        if (t == 0) atomicOr(err, BH_ERR_TIMEOUT);
+    }
+    bh_tc::fence_before();
+    __syncthreads();
+    bh_tc::fence_after();
+    if (t < 32) bh_tc::tmem_free(tmem);
 }
 __global__ void k_hlld(KP k, const double* WL, const double* WR, const double* UL, const double* UR, const double* r,
                        const double* th, int dim, int64_t n, double* F, double* cts) {
@@ -400,6 +463,30 @@ int ctop_guess(const bh_params* P, const double* U, const double* r, const doubl
                double* W, double* Wd, int32_t* status, int32_t* iters, int32_t* path, void* stream) {
     if (!P || n < 0 || (n > 0 && (!U || !r || !th || !xi0 || !W || !status))) return BH_EINVAL;
     if (n == 0) return BH_OK;
+    k_ctop_guess<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), U, r, th, n, xi0, W, Wd, status,
+                                                                      iters, path);
+    return launched();
+}
+int ctop_learned(const bh_params* P, const bh_mlp* m, const double* U, const double* r, const double* th,
+                 int64_t n, double* xi0, double* W, double* Wd, int32_t* status, int32_t* iters, int32_t* path,
+                 int32_t* err, void* stream) {
+    if (!P || !m || !m->w || !m->wb || !err || n < 0 ||
+        (n > 0 && (!U || !r || !th || !xi0 || !W || !status)))
+        return BH_EINVAL;
+    if (n == 0) return BH_OK;
+    int dev = 0, nsm = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_guess_tc, bh_tc::ROWS, 0) != cudaSuccess || occ < 1)
+        return BH_ECUDA;
+    // every CTA resident at once, and never more per SM than the tensor
+    // memory holds: no CTA ever waits in tcgen05.alloc
+    if (occ > bh_tc::MAX_CTAS_PER_SM) occ = bh_tc::MAX_CTAS_PER_SM;
+    const int64_t ntile = (n + bh_tc::ROWS - 1) / bh_tc::ROWS;
+    const int64_t grid = ntile < (int64_t)nsm * occ ? ntile : (int64_t)nsm * occ;
+    k_guess_tc<<<(unsigned)grid, bh_tc::ROWS, 0, S(stream)>>>(kp_of(P), (const __nv_bfloat16*)m->wb,
+                                                            m->w + BH_MLP_NPARAM, U, r, th, n, xi0, err);
+    if (cudaGetLastError() != cudaSuccess) return BH_ECUDA;
     k_ctop_guess<<<(unsigned)((n + TPB - 1) / TPB), TPB, 0, S(stream)>>>(kp_of(P), U, r, th, n, xi0, W, Wd, status,
                                                                       iters, path);
     return launched();

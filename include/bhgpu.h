@@ -47,7 +47,8 @@ enum {
 };
 /* bits of the device error word */
 enum {
-    BH_ERR_DOMAIN = 1   /* density <= 0 reached the EOS (reference throws) */
+    BH_ERR_DOMAIN = 1,  /* density <= 0 reached the EOS (reference throws) */
+    BH_ERR_TIMEOUT = 2  /* a bounded on-device wait ran out (bh_ctop_learned) */
 };
 
 /* arithmetic variant (bh_params.precision) */
@@ -275,6 +276,17 @@ int bh_ctop_pre(const bh_params *P, const double *U, const double *r, const doub
 int bh_ctop_guess(const bh_params *P, const double *U, const double *r, const double *th, int64_t n,
                   const double *xi0, double *W, double *Wd, int32_t *status, int32_t *iters, int32_t *path,
                   void *stream);
+/* bh_ctop_guess started from the network's guess, the network on the
+ * tensor cores (tcgen05, BF16 weights, FP32 accumulation in tensor memory;
+ * activations as BF16 hi + lo halves): one kernel computes per cell the
+ * metric, the preamble, the features and the network and writes the
+ * starting points to xi0 [n] (caller's buffer, required); a second runs the
+ * reference's Newton / Brent from them.  *err (device word) gets
+ * BH_ERR_TIMEOUT if a tensor-core wait ran out.  Replaces the sequence
+ * bh_ctop_pre, bh_mlp_guess, bh_ctop_guess. */
+int bh_ctop_learned(const bh_params *P, const bh_mlp *m, const double *U, const double *r, const double *th,
+                    int64_t n, double *xi0, double *W, double *Wd, int32_t *status, int32_t *iters, int32_t *path,
+                    int32_t *err, void *stream);
 /* xi0[n] = D exp(y0) of the network (NaN where a feature is not finite) */
 int bh_mlp_guess(const bh_mlp *m, const double *pre, const double *r, int64_t n, double *xi0, void *stream);
 /* one Adam step (lr > 0; lr = 0 only computes) on the mean squared error of
@@ -285,6 +297,11 @@ int bh_mlp_train_step(bh_mlp *m, const double *pre, const double *r, const float
                       float *scratch, float *loss_out, void *stream);
 /* refresh the BF16 copy from the FP32 weights */
 int bh_mlp_sync_bf16(bh_mlp *m, void *stream);
+/* failure-detection self test (no counterpart in the reference): one CTA
+ * waits, with the bounded wait of bh_ctop_learned, on an mbarrier that nothing
+ * arrives on; after about a second it gives up and sets BH_ERR_TIMEOUT in
+ * *err (device word) */
+int bh_wait_selftest(int32_t *err, void *stream);
 
 /* ---- L3 integrator ------------------------------------------------------ */
 /* rk2integrator::dtcomp (solver/integrator.cpp:156-189): *dt_dev = CFL step */

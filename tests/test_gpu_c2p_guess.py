@@ -85,3 +85,47 @@ def test_trained_guess_saves_newton_iterations():
     # than one root in the bracket, and another start may settle on another
     assert other_root <= 5e-3                      # measured 1.2e-3
     assert rel.median().item() <= 1e-9
+
+
+@pytest.mark.parametrize("n", [(1 << 16) + 77, 100])
+def test_tensor_core_network_is_the_trained_network(n):
+    """bh_ctop_learned evaluates the network on the tensor cores (BF16
+    weights, activations as BF16 hi + lo halves, FP32 accumulation in
+    tensor memory) in the kernel that also forms con2prim's preamble.  Its
+    starting points equal the CUDA-core network's (bh_mlp_guess) up to FP32
+    summation order, with the same NaN pattern, on a ragged last tile too;
+    the con2prim outcomes then agree with the three-kernel sequence
+    bh_ctop_pre, bh_mlp_guess, bh_ctop_guess."""
+    import bhgpu
+    cn, U, r, th = batch(1 << 16, 5)
+    g = bhgpu.C2PGuess(cn, seed=0)
+    g.train(U, r, th, steps=500, batch=8192)
+    cn2, U2, r2, th2 = batch(n, 6)
+    xi_cc = g.guess(g.preamble(U2, r2, th2), r2)
+    W1, Wd1, st1, it1, pa1 = g.ctop(U2, r2, th2)
+    W2, Wd2, st2, it2, pa2, xi_tc = g.ctop_learned(U2, r2, th2, want_xi0=True)
+    torch.cuda.synchronize()
+    assert torch.equal(torch.isnan(xi_cc), torch.isnan(xi_tc))
+    fin = torch.isfinite(xi_cc)
+    assert fin.double().mean().item() > 0.9
+    rel = ((xi_tc - xi_cc).abs() / xi_cc.abs())[fin]
+    print(f"n={n}: start points, max relative difference {rel.max().item():.2e}, "
+          f"median {rel.median().item():.2e}")
+    assert rel.max().item() <= 1e-3
+    same = (st1 == st2).double().mean().item()
+    assert same >= 0.999, same
+    ok = (st1 == 1) & (st2 == 1)
+    if ok.any():
+        d = abs(it1[ok].double().mean().item() - it2[ok].double().mean().item())
+        assert d <= 0.01 * it1[ok].double().mean().item() + 0.05
+
+
+def test_bounded_wait_reports_a_timeout():
+    """The tensor-core kernel's bounded mbarrier wait, run on a barrier
+    nothing arrives on: it gives up after its limit (about a second) and
+    sets BH_ERR_TIMEOUT in the error word; the context stays usable."""
+    import bhgpu
+    err = bhgpu.wait_selftest()
+    assert err == 2
+    x = torch.ones(4, device="cuda")
+    assert float(x.sum().item()) == 4.0
