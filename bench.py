@@ -169,10 +169,10 @@ STEP_BYTES = 296   # algorithmic HBM bytes per zone-update of a whole RK2 step
 # averaged; a call's kernels summed).  The 128^3 figures scale them by the
 # patch count (x8): every launch touches each patch's arrays once, so
 # traffic grows in proportion to the patches.
-_T64 = {"fluxcomp": (16.40 + 0.00 + 100.61 + 38.33) * 1e6,
-        "ghosts_prims": (46.79 + 5.29 + 36.53 + 1.37 + 65.64 + 19.73) * 1e6,
-        "update": (102.31 + 17.75) * 1e6,
-        "floors": (49.61 + 4.01) * 1e6}
+_T64 = {"fluxcomp": (16.40 + 0.00 + 95.60 + 34.74) * 1e6,
+        "ghosts_prims": (46.74 + 6.01 + 36.53 + 1.27 + 65.04 + 14.74) * 1e6,
+        "update": (102.38 + 17.20) * 1e6,
+        "floors": (49.86 + 5.34) * 1e6}
 TRAFFIC = {**{(k, 64): v for k, v in _T64.items()}, **{(k, 128): 8 * v for k, v in _T64.items()}}
 
 
