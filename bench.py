@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--con2prim-batch", type=int, default=1, help="also measure the 2^24-cell con2prim batch")
     ap.add_argument("--con2prim-cells", type=int, default=1 << 24, help="cells of the con2prim batch")
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="tune the launch bounds of the heavy kernels on the box first (bhgpu.tune)")
     ap.add_argument("--precision", default="fp64-fma", choices=["fp64", "fp64-fma", "mixed"],
                     help="arithmetic variant of the headline value; the other variants are timed beside it")
     return ap.parse_args()
@@ -426,6 +428,10 @@ def torus_bench():
            "ms": (time.perf_counter() - t0) * 1e3, "l0": s["l0"], "rho_max": s["rho_max"]}
     del t
     try:
+        out["step"] = torus_step_bench()
+    except Exception as e:      # informational
+        out["step"] = {"error": str(e)}
+    try:
         import oracle
         if oracle.ref_available():
             ref = oracle.RefSolver([-40.0] * 3, [40.0] * 3, 4, 1.0, 0.9375, 0.0, GAMMA)
@@ -436,6 +442,81 @@ def torus_bench():
                                               "one thread (serial loops)"}
     except Exception as e:      # the CPU figure is informational
         out["cpu_reference"] = {"error": str(e)}
+    return out
+
+
+def torus_step_bench(steps=20, free_steps=100):
+    """RK2 steps of the reference's scheme on the torus geometry of the
+    128^3 Kerr box (a = 0.9375, r_in = 6, r_max = 12, Gamma = 4/3, outflow,
+    van Leer), per arithmetic variant: each step from the initial data, and
+    a free run of free_steps steps compared with the faithful FP64 one.  The
+    reference itself stops in the first step (std::domain_error from its
+    EOS); the device records that in its error word and continues with the
+    fallback the reference's code reaches, so the steps run in full."""
+    import torch
+    import bhgpu
+    from bhgpu.mesh import Quilt
+    q = Quilt([-40.0] * 3, [40.0] * 3, 8)
+    t = bhgpu.AmrTree(q.dom_l, q.dom_h, 8, M=1.0, a=0.9375, Q=0.0, gm=GAMMA, quilt=q, init_floor=False)
+    t.torus_init(r_max=12.0, r_in=6.0)
+    torch.cuda.synchronize()
+    U0, W0, B0 = t.U.clone(), t.W.clone(), t.Bf.clone()
+    integ = bhgpu.RK2Integrator(CFL)
+    a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+    out = {"workload": "reference scheme on the Kerr torus, a=0.9375, r_in=6, r_max=12, Gamma=4/3, 128^3 over "
+                       "[-40,40]^3 (512 patches), outflow, van Leer, CFL 0.4 (no beta normalisation, "
+                       "perturbation or excision: the reference has none)",
+           "zones": 128 ** 3}
+    res = {}
+    for prec in ("fp64", "fp64-fma", "mixed"):
+        t.precision = prec
+
+        def one():
+            t.U.copy_(U0); t.W.copy_(W0); t.Bf.copy_(B0)
+            integ.step(t, sync=False, check_domain=False)
+        for _ in range(3):
+            one()
+        torch.cuda.synchronize()
+        t.clear_error()
+        a.record()
+        for _ in range(steps):
+            one()
+        b.record(); torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / steps
+        res[prec] = {"ms_per_step": ms, "value": 128 ** 3 / (ms / 1e3), "dt": float(t.dt.item()),
+                     "domain_error_flagged": bool(t.read_error() & 1),
+                     "nan_frac_U": float((~torch.isfinite(t.U)).double().mean().item()), "U": t.U.clone()}
+    for prec in ("fp64-fma", "mixed"):
+        res[prec]["l1_vs_fp64_1_step"] = field_l1(res[prec]["U"], res["fp64"]["U"])
+        res[prec]["speedup_vs_plain_fp64"] = res["fp64"]["ms_per_step"] / res[prec]["ms_per_step"]
+    for prec in res:
+        del res[prec]["U"]
+    out["restarted_steps"] = res
+    free = {}
+    for prec in ("fp64", "fp64-fma", "mixed"):
+        t.precision = prec
+        t.U.copy_(U0); t.W.copy_(W0); t.Bf.copy_(B0)
+        t.clear_error()
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(free_steps):
+            integ.step(t, sync=False, check_domain=False)
+        b.record(); torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / free_steps
+        divb = t.maxdivb()
+        fin = torch.isfinite(divb)
+        free[prec] = {"ms_per_step": ms, "value": 128 ** 3 / (ms / 1e3),
+                      "max_divB": float(divb[fin].max().item()) if fin.any() else None,
+                      "nan_frac_U": float((~torch.isfinite(t.U)).double().mean().item()),
+                      "domain_error_flagged": bool(t.read_error() & 1), "U": t.U.clone()}
+    for prec in ("fp64-fma", "mixed"):
+        free[prec][f"l1_vs_fp64_{free_steps}_steps"] = field_l1(free[prec]["U"], free["fp64"]["U"])
+        free[prec]["speedup_vs_plain_fp64"] = free["fp64"]["ms_per_step"] / free[prec]["ms_per_step"]
+    for prec in free:
+        del free[prec]["U"]
+    out[f"free_run_{free_steps}_steps"] = free
+    t.precision = "fp64"
+    del t
     return out
 
 
@@ -572,6 +653,15 @@ def run_ours(args):
     nq = args.grid // 16
     tree = make_tree(nq, seed=1, precision=args.precision)
     zones = (nq * 16) ** 3
+    # launch bounds of the heavy kernels: timed on this box, per variant
+    tuning = {}
+    if args.autotune:
+        integ = bhgpu.RK2Integrator(CFL)
+        for prec in ("fp64", "fp64-fma", "mixed"):
+            tree.precision = prec
+            tuning[prec] = bhgpu.tune.autotune(tree, integ, reps=2)
+        tree.precision = args.precision
+        tree.clear_error()
     U0, W0, B0 = tree.U.clone(), tree.W.clone(), tree.Bf.clone()
     L = bhgpu.lib
     P = tree.params()
@@ -766,6 +856,10 @@ def run_ours(args):
                          "step_frac": value / world * STEP_BYTES / (peak * 1e9)},
             "clocks": ck,
             "device_error_word": err,
+            "autotune": ({prec: {"choice_ctas_per_sm": t["choice"],
+                                 "step_ms_per_candidate": {k: {str(c): round(m, 4) for c, m in v.items()}
+                                                           for k, v in t["ms"].items()}}
+                          for prec, t in tuning.items()} if tuning else "off (compiled-in launch bounds)"),
         }
         if world == 1:
             threads = os.cpu_count() or 1

@@ -38,18 +38,23 @@ def build(verbose: bool = False) -> str:
     deps.append(os.path.join(REPO, "include", "bhgpu.h"))
     if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
         return out
-    objs = []
     bdir = os.path.join(PKG, "_build")
     os.makedirs(bdir, exist_ok=True)
+    jobs = []
     for src in srcs:
         obj = os.path.join(bdir, os.path.basename(src).replace(".cu", ".o"))
         cmd = [NVCC] + ARCH + COMMON + FMAD.get(os.path.basename(src), ["--fmad=false"]) + ["-c", src, "-o", obj]
+        jobs.append((cmd, obj))
         if verbose:
             print(" ".join(cmd))
-        r = subprocess.run(cmd, capture_output=True, text=True)
+    # the translation units compile independently: in parallel
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(lambda j: subprocess.run(j[0], capture_output=True, text=True), jobs))
+    for (cmd, obj), r in zip(jobs, results):
         if r.returncode != 0:
             raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-        objs.append(obj)
+    objs = [obj for _, obj in jobs]
     cmd = [NVCC] + ARCH + ["-shared", "-o", out] + objs
     if verbose:
         print(" ".join(cmd))

@@ -135,6 +135,23 @@ int bh_ctop_pre(const bh_params* P, const double* U, const double* r, const doub
                 void* stream) {
     BH_DISPATCH(P, ctop_pre(P, U, r, th, n, pre, stream));
 }
+int bh_tune_candidates(int32_t kernel, int32_t* out, int32_t max) {
+    if (kernel < 0 || kernel >= BH_TUNE_NKERNEL || (max > 0 && !out) || max < 0) return BH_EINVAL;
+    int n = 0;
+    while (n < 5 && bh_tune_cands[kernel][n]) n++;
+    for (int i = 0; i < n && i < max; i++) out[i] = bh_tune_cands[kernel][i];
+    return n;
+}
+int bh_tune_set(int32_t precision, int32_t kernel, int32_t ctas) {
+    bh_params P = {};
+    P.precision = precision;
+    BH_DISPATCH(&P, tune_set(kernel, ctas));
+}
+int bh_tune_get(int32_t precision, int32_t kernel, int32_t* ctas) {
+    bh_params P = {};
+    P.precision = precision;
+    BH_DISPATCH(&P, tune_get(kernel, ctas));
+}
 int bh_ctop_learned(const bh_params* P, const bh_mlp* m, const double* U, const double* r, const double* th,
                     int64_t n, double* xi0, double* W, double* Wd, int32_t* status, int32_t* iters, int32_t* path,
                     int32_t* err, void* stream) {

@@ -5,6 +5,17 @@
 #include <stdint.h>
 #include "bhgpu.h"
 
+// launch-bound candidates of the tuned kernels (BH_TUNE_*), zero-terminated;
+// bh_variant.cuh instantiates each kernel for exactly its list
+constexpr int32_t bh_tune_cands[BH_TUNE_NKERNEL][5] = {
+    {3, 4, 5, 6, 0}, {3, 4, 5, 6, 0}, {4, 6, 8, 0, 0}, {4, 6, 8, 0, 0}, {4, 6, 8, 0, 0}};
+inline bool bh_tune_valid(int32_t kernel, int32_t ctas) {
+    if (kernel < 0 || kernel >= BH_TUNE_NKERNEL) return false;
+    for (int i = 0; i < 5 && bh_tune_cands[kernel][i]; i++)
+        if (bh_tune_cands[kernel][i] == ctas) return true;
+    return false;
+}
+
 #define BH_VARIANT_API(NS)                                                                                       \
     namespace NS {                                                                                              \
     int metric_comp(const bh_params*, const double*, const double*, int64_t, double*, void*);                  \
@@ -34,6 +45,8 @@
     int ctop_guess(const bh_params*, const double*, const double*, const double*, int64_t, const double*,      \
                    double*, double*, int32_t*, int32_t*, int32_t*, void*);                                     \
     int ctop_pre(const bh_params*, const double*, const double*, const double*, int64_t, double*, void*);    \
+    int tune_set(int32_t, int32_t);                                                                         \
+    int tune_get(int32_t, int32_t*);                                                                        \
     int ctop_learned(const bh_params*, const bh_mlp*, const double*, const double*, const double*, int64_t,   \
                      double*, double*, double*, int32_t*, int32_t*, int32_t*, int32_t*, void*);               \
     int refine(const bh_params*, const bh_pool*, const int32_t*, int32_t, void*);                              \

@@ -553,39 +553,60 @@ BH_HD inline void strip_ijk(int dim, int pos, int t1, int t2, int& i, int& j, in
     else { i = t1; j = t2; k = pos; }
 }
 
-// ghost-strip copy (gh_copy :390-425, gh_bndy :494-522) of one state
-// vector: item e of patch p copies U (a = 0) or W (a = 1), a = e / N_STRIP,
-// of strip cell e % N_STRIP -- eight independent loads, then eight stores.
-// The cells of a slot are ordered so that neighbouring items are neighbours
-// in memory (k fastest; for the k-strips of dim 2 the two layers gg first).
-// The 128 items of a CTA share one array and one slot, so the neighbour
-// kind is uniform.
+// ghost-strip copy (gh_copy :390-425, gh_bndy :494-522) of two cells' state
+// vectors: item e of patch p copies U (a = 0) or W (a = 1), a = e / N_COPY,
+// of the strip-cell pair e % N_COPY.  A pair is two cells adjacent in k --
+// the same row for the x- and y-strips, the two layers of a k-strip -- so
+// the eight variables move as eight aligned 16-byte loads and stores (the
+// per-patch linear index of an even k is even, grid.cpp:51-53).  Pairs are
+// ordered so that neighbouring items are neighbours in memory.  The 128
+// items of a CTA share one array and one slot, so the neighbour kind is
+// uniform.
+constexpr int N_COPY = N_STRIP / 2;
 BH_HD inline void ghost_copy_item(const Pool& P, int p, int e) {
-    int a = e / N_STRIP, c = e % N_STRIP;
-    int s = c / 512, rem = c % 512;
+    int a = e / N_COPY, c = e % N_COPY;
+    int s = c / 256, rem = c % 256;
     int dim = s / 2, side = (s & 1) ? 1 : -1;
     int nb = P.nbr[(p * 6 + s) * 2], kind = P.nbr[(p * 6 + s) * 2 + 1];
     if (kind != BH_NB_COPY && kind != BH_NB_BNDY) return;
-    int gg, t1, t2;
-    if (dim == 2) { gg = rem & 1; t2 = (rem >> 1) & 15; t1 = rem >> 5; }
-    else { gg = rem >> 8; t1 = (rem >> 4) & 15; t2 = rem & 15; }
+    // the first cell of the pair: ghost (gi, gj, gk), source (ai, aj, ak);
+    // the second is k + 1 in both, except an outflow k-strip on the +k side,
+    // whose layers mirror the interior (ghost 16, 17 <- 15, 14)
     int gi, gj, gk, ai, aj, ak, src_p;
-    strip_ijk(dim, (side == 1 ? BLK : -GH) + gg, t1, t2, gi, gj, gk);
-    if (kind == BH_NB_COPY) {
-        src_p = nb;
-        strip_ijk(dim, (side == 1 ? 0 : BLK - GH) + gg, t1, t2, ai, aj, ak);
+    bool swap = false;
+    if (dim == 2) {
+        int t1 = rem >> 4, t2 = rem & 15;
+        strip_ijk(2, side == 1 ? BLK : -GH, t1, t2, gi, gj, gk);
+        if (kind == BH_NB_COPY) {
+            src_p = nb;
+            strip_ijk(2, side == 1 ? 0 : BLK - GH, t1, t2, ai, aj, ak);
+        } else {
+            src_p = p;
+            strip_ijk(2, side == 1 ? BLK - 2 : 0, t1, t2, ai, aj, ak);
+            swap = side == 1;
+        }
     } else {
-        src_p = p;
-        strip_ijk(dim, side == 1 ? BLK - 1 - gg : gg, t1, t2, ai, aj, ak);
+        int gg = rem >> 7, t1 = (rem >> 3) & 15, t2 = (rem & 7) * 2;
+        strip_ijk(dim, (side == 1 ? BLK : -GH) + gg, t1, t2, gi, gj, gk);
+        if (kind == BH_NB_COPY) {
+            src_p = nb;
+            strip_ijk(dim, (side == 1 ? 0 : BLK - GH) + gg, t1, t2, ai, aj, ak);
+        } else {
+            src_p = p;
+            strip_ijk(dim, side == 1 ? BLK - 1 - gg : gg, t1, t2, ai, aj, ak);
+        }
     }
     double* dst = a == 0 ? Uv(P, p, 0) : Wv(P, p, 0);
     const double* src = a == 0 ? Uv(P, src_p, 0) : Wv(P, src_p, 0);
     int lg = lindx(gi, gj, gk), la = lindx(ai, aj, ak);
-    double x[8];
+    double2 x[8];
 #pragma unroll
-    for (int v = 0; v < 8; v++) x[v] = src[(size_t)v * NC + la];
+    for (int v = 0; v < 8; v++) x[v] = *reinterpret_cast<const double2*>(src + (size_t)v * NC + la);
 #pragma unroll
-    for (int v = 0; v < 8; v++) dst[(size_t)v * NC + lg] = x[v];
+    for (int v = 0; v < 8; v++) {
+        double2 y = swap ? make_double2(x[v].y, x[v].x) : x[v];
+        *reinterpret_cast<double2*>(dst + (size_t)v * NC + lg) = y;
+    }
 }
 
 // ghost-strip prolongation from a coarser neighbour, strip cell e of patch p

@@ -7,5 +7,4 @@
 #define BH_RCP   // reciprocals formed once for repeated divisors (quo)
 #define BH_REAL float
 #define BH_MINB_FLUX 6   // the FP32 face computation needs fewer registers
-#define BH_FLUX_ALT 4, 8
 #include "bh_variant.cuh"

@@ -16,6 +16,7 @@
 #include "bh_items.cuh"
 #include "bh_init.cuh"
 #include "bh_tc.cuh"
+#include "bh_api.h"
 
 #ifndef BH_VARIANT
 #error "define BH_VARIANT before including bh_variant.cuh"
@@ -149,7 +150,10 @@ __global__ void __launch_bounds__(TPB, BH_MINB_FLUX) k_flux(KP kp, Pool P, const
     ITEM(NFACE); flux_item<BH_REAL>(kp, P, list[blockIdx.y], blockIdx.z, e);
 }
 __global__ void k_aux(KP kp, Pool P, const int32_t* list) { ITEM(NC); aux_item<BH_REAL>(kp, P, list[blockIdx.y], e); }
-__global__ void __launch_bounds__(TPB, BH_MINB_FLUX) k_flux_aux(KP kp, Pool P, const int32_t* list) {
+// the kernels the autotuner sets: one instantiation per candidate number
+// of resident CTAs per SM (MB), which caps their registers per thread
+template <int MB>
+__global__ void __launch_bounds__(TPB, MB) k_flux_aux(KP kp, Pool P, const int32_t* list) {
     ITEM(NFACE); flux_item<BH_REAL, true>(kp, P, list[blockIdx.y], blockIdx.z, e);
 }
 __global__ void k_emf(Pool P, const int32_t* list) { ITEM(N_EDGE); emf_item(P, list[blockIdx.y], e); }
@@ -164,7 +168,8 @@ __global__ void k_div_source(KP kp, Pool P, const int32_t* list, double* dv, dou
 // the shell cells, so no warp mixes the two
 constexpr int UPD_INT = N_INT / TPB;
 constexpr int UPD_BLOCKS = UPD_INT + (N_SHELL + TPB - 1) / TPB;
-__global__ void __launch_bounds__(TPB, BH_MINB_UPDATE) k_update(KP kp, Pool P, const int32_t* list, const double* dtp, int stage) {
+template <int MB>
+__global__ void __launch_bounds__(TPB, MB) k_update(KP kp, Pool P, const int32_t* list, const double* dtp, int stage) {
     int p = list[blockIdx.y];
     if ((int)blockIdx.x < UPD_INT) {
         update_interior_item<BH_REAL>(kp, P, p, blockIdx.x * TPB + threadIdx.x, *dtp, stage);
@@ -175,7 +180,7 @@ __global__ void __launch_bounds__(TPB, BH_MINB_UPDATE) k_update(KP kp, Pool P, c
 }
 // amrtree::ghosts strip fill: one copied double per thread, then the
 // prolonged cells (CTAs whose slot has another neighbour kind exit at once)
-__global__ void k_ghost_copy(Pool P, const int32_t* list) { ITEM(2 * N_STRIP); ghost_copy_item(P, list[blockIdx.y], e); }
+__global__ void k_ghost_copy(Pool P, const int32_t* list) { ITEM(2 * N_COPY); ghost_copy_item(P, list[blockIdx.y], e); }
 __global__ void k_ghost_prolong(KP kp, Pool P, const int32_t* list) {
     ITEM(N_STRIP); ghost_prolong_item(kp, P, list[blockIdx.y], e);
 }
@@ -183,13 +188,16 @@ __global__ void k_ghost_ctop(KP kp, Pool P, const int32_t* list) { ITEM(NC); gho
 __global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_prims(KP kp, Pool P, const int32_t* list, int ghost_first) {
     ITEM(NC); prims_item(kp, P, list[blockIdx.y], e, ghost_first);
 }
-__global__ void __launch_bounds__(TPB, BH_MINB_PRIMS) k_prims_interior(KP kp, Pool P, const int32_t* list) {
+template <int MB>
+__global__ void __launch_bounds__(TPB, MB) k_prims_interior(KP kp, Pool P, const int32_t* list) {
     ITEM(N_INT); prims_interior_item(kp, P, list[blockIdx.y], e);
 }
-__global__ void __launch_bounds__(TPB, BH_MINB_GHOST) k_prims_ghost(KP kp, Pool P, const int32_t* list) {
+template <int MB>
+__global__ void __launch_bounds__(TPB, MB) k_prims_ghost(KP kp, Pool P, const int32_t* list) {
     ITEM(N_GHOST); prims_ghost_item(kp, P, list[blockIdx.y], e);
 }
-__global__ void __launch_bounds__(TPB, BH_MINB_FLOORS) k_floors(KP kp, Pool P, const int32_t* list) {
+template <int MB>
+__global__ void __launch_bounds__(TPB, MB) k_floors(KP kp, Pool P, const int32_t* list) {
     ITEM(N_INT); floors_item(kp, P, list[blockIdx.y], e);
 }
 
@@ -335,7 +343,42 @@ inline bool bad_pool(const bh_pool* p) {
 inline int nall(const bh_pool* p) { return p->nall > 0 ? p->nall : p->npatch; }
 inline dim3 grid2(int items, int npatch, int z = 1) { return dim3((items + TPB - 1) / TPB, npatch, z); }
 
+// ---- launch bounds chosen by the autotuner --------------------------------
+// The current choice per tuned kernel (resident 128-thread CTAs per SM asked
+// of ptxas), per process and per variant, initially the compiled-in
+// default; launches made after bh_tune_set (and graphs captured after it)
+// use the new choice.  The candidate lists are bh_tune_cands (bh_api.h);
+// each switch below instantiates exactly those.
+int g_minb[BH_TUNE_NKERNEL] = {BH_MINB_FLUX, BH_MINB_UPDATE, BH_MINB_PRIMS, BH_MINB_GHOST, BH_MINB_FLOORS};
+
+#define BH_TUNED_CASE(K, MB, GRID, ST, ...) \
+    case MB: K<MB><<<GRID, TPB, 0, ST>>>(__VA_ARGS__); break;
+// flux and update: 3, 4, 5, 6; con2prim (interior, ghost) and floors: 4, 6, 8
+#define BH_LAUNCH_3456(K, WHICH, GRID, ST, ...)                                                            \
+    switch (g_minb[WHICH]) {                                                                             \
+        BH_TUNED_CASE(K, 3, GRID, ST, __VA_ARGS__) BH_TUNED_CASE(K, 4, GRID, ST, __VA_ARGS__)            \
+        BH_TUNED_CASE(K, 5, GRID, ST, __VA_ARGS__) BH_TUNED_CASE(K, 6, GRID, ST, __VA_ARGS__)            \
+        default: return BH_EINVAL;                                                                       \
+    }
+#define BH_LAUNCH_468(K, WHICH, GRID, ST, ...)                                                             \
+    switch (g_minb[WHICH]) {                                                                             \
+        BH_TUNED_CASE(K, 4, GRID, ST, __VA_ARGS__) BH_TUNED_CASE(K, 6, GRID, ST, __VA_ARGS__)            \
+        BH_TUNED_CASE(K, 8, GRID, ST, __VA_ARGS__)                                                       \
+        default: return BH_EINVAL;                                                                       \
+    }
+
 }  // namespace
+
+int tune_set(int32_t kernel, int32_t ctas) {
+    if (!bh_tune_valid(kernel, ctas)) return BH_EINVAL;
+    g_minb[kernel] = ctas;
+    return BH_OK;
+}
+int tune_get(int32_t kernel, int32_t* ctas) {
+    if (kernel < 0 || kernel >= BH_TUNE_NKERNEL || !ctas) return BH_EINVAL;
+    *ctas = g_minb[kernel];
+    return BH_OK;
+}
 
 int metric_comp(const bh_params* P, const double* r, const double* th, int64_t n, double* out, void* stream) {
     if (!P || n < 0) return BH_EINVAL;
@@ -382,7 +425,8 @@ int fluxcomp(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
     if (pool->aux) {
         k_aux<<<grid2(NC, nall(pool)), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
-        k_flux_aux<<<grid2(NFACE, nall(pool), 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+        BH_LAUNCH_3456(k_flux_aux, BH_TUNE_FLUX, grid2(NFACE, nall(pool), 3), S(stream), kp_of(P), pool_of(pool),
+                       pool->all)
     } else {
         k_flux<<<grid2(NFACE, nall(pool), 3), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
     }
@@ -417,7 +461,7 @@ int div_source(const bh_params* P, const bh_pool* pool, double* div, double* src
 int ghosts(const bh_params* P, const bh_pool* pool, const int32_t* patches, int32_t n, void* stream) {
     if (!P || bad_pool(pool) || n < 0 || (n > 0 && !patches)) return BH_EINVAL;
     if (n == 0) return BH_OK;
-    k_ghost_copy<<<grid2(2 * N_STRIP, n), TPB, 0, S(stream)>>>(pool_of(pool), patches);
+    k_ghost_copy<<<grid2(2 * N_COPY, n), TPB, 0, S(stream)>>>(pool_of(pool), patches);
     k_ghost_prolong<<<grid2(N_STRIP, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
     k_ghost_ctop<<<grid2(NC, n), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), patches);
     return launched();
@@ -435,11 +479,13 @@ int ghosts_prims_status(const bh_params* P, const bh_pool* pool, uint8_t* status
     if (pool->nleaf == 0) return BH_OK;
     Pool pv = pool_of(pool);
     pv.status = status;
-    k_ghost_copy<<<grid2(2 * N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(pv, pool->leaves);
+    k_ghost_copy<<<grid2(2 * N_COPY, pool->nleaf), TPB, 0, S(stream)>>>(pv, pool->leaves);
     k_ghost_prolong<<<grid2(N_STRIP, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
     if (status && pool->leafmask) {
-        k_prims_interior<<<grid2(N_INT, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
-        k_prims_ghost<<<grid2(N_GHOST, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves);
+        BH_LAUNCH_468(k_prims_interior, BH_TUNE_PRIMS_INTERIOR, grid2(N_INT, pool->nleaf), S(stream), kp_of(P), pv,
+                      pool->leaves)
+        BH_LAUNCH_468(k_prims_ghost, BH_TUNE_PRIMS_GHOST, grid2(N_GHOST, pool->nleaf), S(stream), kp_of(P), pv,
+                      pool->leaves)
     } else {
         k_prims<<<grid2(NC, pool->nleaf), TPB, 0, S(stream)>>>(kp_of(P), pv, pool->leaves, 1);
     }
@@ -450,13 +496,13 @@ int ghosts_prims(const bh_params* P, const bh_pool* pool, void* stream) {
 }
 int update(const bh_params* P, const bh_pool* pool, const double* dt_dev, int32_t stage, void* stream) {
     if (!P || bad_pool(pool) || !dt_dev || (stage != 0 && stage != 1)) return BH_EINVAL;
-    k_update<<<dim3(UPD_BLOCKS, nall(pool)), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all, dt_dev,
-                                                                    stage);
+    BH_LAUNCH_3456(k_update, BH_TUNE_UPDATE, dim3(UPD_BLOCKS, nall(pool)), S(stream), kp_of(P), pool_of(pool),
+                   pool->all, dt_dev, stage)
     return launched();
 }
 int floors(const bh_params* P, const bh_pool* pool, void* stream) {
     if (!P || bad_pool(pool)) return BH_EINVAL;
-    k_floors<<<grid2(N_INT, nall(pool)), TPB, 0, S(stream)>>>(kp_of(P), pool_of(pool), pool->all);
+    BH_LAUNCH_468(k_floors, BH_TUNE_FLOORS, grid2(N_INT, nall(pool)), S(stream), kp_of(P), pool_of(pool), pool->all)
     return launched();
 }
 int ctop_guess(const bh_params* P, const double* U, const double* r, const double* th, int64_t n, const double* xi0,

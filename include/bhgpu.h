@@ -303,6 +303,27 @@ int bh_mlp_sync_bf16(bh_mlp *m, void *stream);
  * *err (device word) */
 int bh_wait_selftest(int32_t *err, void *stream);
 
+/* ---- launch-bound autotuning (no counterpart in the reference) ----------
+ * The heaviest kernels are compiled for several numbers of resident
+ * 128-thread CTAs per SM (which caps their registers per thread); which one
+ * runs is chosen per process and per arithmetic variant, initially the
+ * compiled-in default.  bhgpu.tune.autotune times the candidates on a
+ * caller's pool and sets the fastest.  Launches made after bh_tune_set, and
+ * CUDA graphs captured after it, use the new choice. */
+enum {
+    BH_TUNE_FLUX = 0,            /* fluxcomp face kernel (3, 4, 5, 6)          */
+    BH_TUNE_UPDATE = 1,          /* f2cB + RK update (3, 4, 5, 6)              */
+    BH_TUNE_PRIMS_INTERIOR = 2,  /* con2prim of interior cells (4, 6, 8)       */
+    BH_TUNE_PRIMS_GHOST = 3,     /* con2prim of ghost cells (4, 6, 8)          */
+    BH_TUNE_FLOORS = 4,          /* patch::floors (4, 6, 8)                    */
+    BH_TUNE_NKERNEL = 5
+};
+/* the candidates of `kernel` into out[max]; returns their number, or BH_EINVAL */
+int bh_tune_candidates(int32_t kernel, int32_t *out, int32_t max);
+/* the CTAs per SM `kernel` of variant `precision` launches with */
+int bh_tune_set(int32_t precision, int32_t kernel, int32_t ctas_per_sm);
+int bh_tune_get(int32_t precision, int32_t kernel, int32_t *ctas_per_sm);
+
 /* ---- L3 integrator ------------------------------------------------------ */
 /* rk2integrator::dtcomp (solver/integrator.cpp:156-189): *dt_dev = CFL step */
 int bh_dtcomp(const bh_params *P, const bh_pool *pool, double cfl, double *dt_dev, void *stream);

@@ -90,7 +90,7 @@ void hc_div_source(const bh_params* Pp, const bh_pool* pool, double* dv, double*
 void hc_ghosts(const bh_params* Pp, const bh_pool* pool, const int32_t* list, int n) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < n; i++)
-        for (int e = 0; e < 2 * N_STRIP; e++) ghost_copy_item(P, list[i], e);
+        for (int e = 0; e < 2 * N_COPY; e++) ghost_copy_item(P, list[i], e);
     for (int i = 0; i < n; i++)
         for (int e = 0; e < N_STRIP; e++) ghost_prolong_item(k, P, list[i], e);
     for (int i = 0; i < n; i++)
@@ -104,7 +104,7 @@ void hc_prims(const bh_params* Pp, const bh_pool* pool, int ghost_first) {
 void hc_ghosts_prims(const bh_params* Pp, const bh_pool* pool) {
     KP k = kp_of(Pp); Pool P = pool_of(pool);
     for (int i = 0; i < pool->nleaf; i++)
-        for (int e = 0; e < 2 * N_STRIP; e++) ghost_copy_item(P, pool->leaves[i], e);
+        for (int e = 0; e < 2 * N_COPY; e++) ghost_copy_item(P, pool->leaves[i], e);
     for (int i = 0; i < pool->nleaf; i++)
         for (int e = 0; e < N_STRIP; e++) ghost_prolong_item(k, P, pool->leaves[i], e);
     if (pool->status && pool->leafmask) {

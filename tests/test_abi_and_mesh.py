@@ -6,6 +6,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from bhgpu import mesh
 
@@ -96,3 +97,22 @@ def test_pool_lists_longer_than_the_pool_are_rejected():
     for pool in (too_many_all, too_many_leaves):
         assert lib.bh_fluxcomp(C.byref(P), C.byref(pool), None) == -1
         assert lib.bh_floors(C.byref(P), C.byref(pool), None) == -1
+
+
+def test_tuning_table_host_side():
+    """The autotuner's launch-bound table: candidates per kernel, the
+    compiled-in defaults among them, settable per variant, invalid values
+    refused (host calls only, no device needed)."""
+    from bhgpu import tune, BhError
+    assert tune.candidates("flux") == [3, 4, 5, 6]
+    assert tune.candidates("floors") == [4, 6, 8]
+    for prec in ("fp64", "fp64-fma", "mixed"):
+        for k, c in tune.current(prec).items():
+            assert c in tune.candidates(k)
+    assert tune.get("mixed", "flux") == 6 and tune.get("fp64", "flux") == 4
+    tune.set("fp64", "update", 5)
+    assert tune.get("fp64", "update") == 5 and tune.get("fp64-fma", "update") == 4
+    tune.set("fp64", "update", 4)
+    with pytest.raises(BhError):
+        tune.set("fp64", "update", 7)
+    assert tune.get("fp64", "update") == 4
