@@ -521,7 +521,12 @@ int ctop_learned(const bh_params* P, const bh_mlp* m, const double* U, const dou
         return BH_EINVAL;
     if (n == 0) return BH_OK;
     int dev = 0, nsm = 0, occ = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
+    // the kernel's 44 KB of static shared memory: ask for the largest
+    // shared-memory carveout, or the default one leaves room for a single
+    // CTA per SM (measured: 148 CTAs, 6 % of warps active)
+    if (cudaFuncSetAttribute(k_guess_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
+        cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_guess_tc, bh_tc::ROWS, 0) != cudaSuccess || occ < 1)
         return BH_ECUDA;
