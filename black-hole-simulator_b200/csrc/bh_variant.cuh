@@ -520,19 +520,20 @@ int ctop_learned(const bh_params* P, const bh_mlp* m, const double* U, const dou
         (n > 0 && (!U || !r || !th || !xi0 || !W || !status)))
         return BH_EINVAL;
     if (n == 0) return BH_OK;
-    int dev = 0, nsm = 0, occ = 0;
-    // the kernel's 44 KB of static shared memory: ask for the largest
-    // shared-memory carveout, or the default one leaves room for a single
-    // CTA per SM (measured: 148 CTAs, 6 % of warps active)
+    int dev = 0, nsm = 0;
+    // 44 KB of static shared memory per CTA: ask for the largest carveout
     if (cudaFuncSetAttribute(k_guess_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
         cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_guess_tc, bh_tc::ROWS, 0) != cudaSuccess || occ < 1)
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return BH_ECUDA;
-    // every CTA resident at once, and never more per SM than the tensor
-    // memory holds: no CTA ever waits in tcgen05.alloc
-    if (occ > bh_tc::MAX_CTAS_PER_SM) occ = bh_tc::MAX_CTAS_PER_SM;
+    // CTAs per SM: the launch bounds (128 threads, 4 CTAs) cap the registers
+    // so that 4 fit, 4 x 45 KB of shared memory fit, and 4 x 64 tensor-memory
+    // columns fit in 512, so no CTA ever waits in tcgen05.alloc.  (The
+    // occupancy calculator answered 1 for this kernel on B200, which left 3
+    // of 4 slots idle; CTAs beyond the resident ones would only queue.)
+    const int occ = 4;
+    static_assert(4 <= bh_tc::MAX_CTAS_PER_SM, "tensor memory of the resident CTAs");
     const int64_t ntile = (n + bh_tc::ROWS - 1) / bh_tc::ROWS;
     const int64_t grid = ntile < (int64_t)nsm * occ ? ntile : (int64_t)nsm * occ;
     k_guess_tc<<<(unsigned)grid, bh_tc::ROWS, 0, S(stream)>>>(kp_of(P), (const __nv_bfloat16*)m->wb,
