@@ -30,9 +30,14 @@ e2e   : same metric through the public API with host buffers
         with consecutive steps on three device trees so that the copies of
         neighbouring steps overlap the step; the one-tree (serial) figure
         is reported beside it.
-roofline : the flux kernel (k_flux, the largest share of the step),
-        algorithmic bytes per launch / its CUDA-event duration inside the
-        timed region, against the measured HBM copy bandwidth.
+roofline : the call with the largest share of the step (ghost fill +
+        con2prim, or the face fluxes), its algorithmic bytes per launch / its
+        CUDA-event duration inside the timed region, against the measured HBM
+        copy bandwidth (the fallback figure when MEASURED_PEAKS.json is
+        absent).
+autotune : before timing, the launch bounds of the heavy kernels are tuned
+        on the box for every variant (bhgpu.tune; --autotune 0 keeps the
+        compiled-in ones).
 cpu_baseline : the reference solver's own rk2integrator::step compiled from
         its sources (oracle/_ref), on all host cores, on a 64^3 sample.
 """
