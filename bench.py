@@ -72,8 +72,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--con2prim-batch", type=int, default=1, help="also measure the 2^24-cell con2prim batch")
     ap.add_argument("--con2prim-cells", type=int, default=1 << 24, help="cells of the con2prim batch")
-    ap.add_argument("--autotune", type=int, default=1,
-                    help="tune the launch bounds of the heavy kernels on the box first (bhgpu.tune)")
+    ap.add_argument("--autotune", type=int, default=1, choices=[0, 1, 2],
+                    help="launch bounds of the heavy kernels: 1 tune them on the box first and save the choice "
+                         "(bhgpu.tune), 2 apply the saved choice without timing (for profiler runs), 0 keep "
+                         "the compiled-in ones")
     ap.add_argument("--precision", default="fp64-fma", choices=["fp64", "fp64-fma", "mixed"],
                     help="arithmetic variant of the headline value; the other variants are timed beside it")
     return ap.parse_args()
@@ -668,13 +670,19 @@ def run_ours(args):
     zones = (nq * 16) ** 3
     # launch bounds of the heavy kernels: timed on this box, per variant
     tuning = {}
-    if args.autotune:
+    if args.autotune == 1:
         integ = bhgpu.RK2Integrator(CFL)
         for prec in ("fp64", "fp64-fma", "mixed"):
             tree.precision = prec
-            tuning[prec] = bhgpu.tune.autotune(tree, integ, reps=2)
+            tuning[prec] = bhgpu.tune.autotune(tree, integ, reps=2, save=True)
         tree.precision = args.precision
         tree.clear_error()
+    elif args.autotune == 2:
+        for prec in ("fp64", "fp64-fma", "mixed"):
+            choice = bhgpu.tune.load_tuning(prec)
+            if choice is None:
+                raise SystemExit(f"--autotune 2: no saved launch bounds for {prec} on this GPU")
+            tuning[prec] = {"choice": choice, "ms": {}}
     U0, W0, B0 = tree.U.clone(), tree.W.clone(), tree.Bf.clone()
     L = bhgpu.lib
     P = tree.params()
@@ -865,7 +873,7 @@ def run_ours(args):
                          "step_frac": value / world * STEP_BYTES / (peak * 1e9)},
             "clocks": ck,
             "device_error_word": err,
-            "autotune": ({prec: {"choice_ctas_per_sm": t["choice"],
+            "autotune": ({prec: {"choice_ctas_per_sm": t["choice"], "timed": bool(t["ms"]),
                                  "step_ms_per_candidate": {k: {str(c): round(m, 4) for c, m in v.items()}
                                                            for k, v in t["ms"].items()}}
                           for prec, t in tuning.items()} if tuning else "off (compiled-in launch bounds)"),
