@@ -12,5 +12,6 @@ from .analysis import Analyser  # noqa: F401
 from .c2p_guess import C2PGuess, wait_selftest  # noqa: F401
 from . import configs  # noqa: F401
 from . import tune  # noqa: F401
+from . import snapshot  # noqa: F401
 
 __version__ = "0.1.0"

@@ -421,6 +421,14 @@ class AmrTree:
             if x is not None:
                 getattr(self, name).copy_(torch.as_tensor(np.asarray(x), dtype=torch.float64))
 
+    def data_write(self, path: str, t: float = 0.0, step: int = 0, derived: bool = False):
+        """Grid data for the renderer (the reference's data_write switch,
+        main.cpp:40-43, whose writer data.hpp never defines): the leaf
+        patches' interior primitives and geometry in one snapshot file
+        (bhgpu.snapshot)."""
+        from . import snapshot
+        snapshot.from_tree(self, path, t=t, step=step, derived=derived)
+
     def host(self, names=("U", "W", "Bf")):
         return {k: getattr(self, k).cpu().numpy() for k in names}
 

@@ -92,3 +92,21 @@ def test_first_step_of_the_torus_matches_the_oracle():
     torus_step_gate(tree.U.cpu().numpy(), tree.Bf.cpu().numpy(), hp, orc, 1.0, 0.9375, tree.limiter)
     dtc = orc.dtcomp(hp, 0.4)
     assert abs(dtg - dtc) <= 1e-12 * dtc
+
+
+def test_snapshot_of_the_torus(tmp_path):
+    """data_write after torus_init: the file holds the leaf patches'
+    interior primitives bit for bit, with their origins and spacings."""
+    import bhgpu
+    from bhgpu import snapshot
+    q = Quilt([-40.0] * 3, [40.0] * 3, 2)
+    tree = bhgpu.AmrTree(q.dom_l, q.dom_h, 2, M=1.0, a=0.9375, Q=0.0, gm=4.0 / 3.0, quilt=q, init_floor=False)
+    tree.torus_init(r_max=12.0, r_in=6.0)
+    path = str(tmp_path / "torus.bhsnap")
+    tree.data_write(path, t=0.0, step=0, derived=True)
+    h, a = snapshot.read(path)
+    W = tree.W.cpu().numpy().reshape(-1, 8, 20, 20, 20)[:, :, 2:18, 2:18, 2:18]
+    leaves = tree.leaves.cpu().numpy()
+    assert np.array_equal(a["W"].view(np.uint64), np.ascontiguousarray(W[leaves]).view(np.uint64))
+    assert np.array_equal(a["origin"], tree.tables["pgeo"][leaves, :3])
+    assert h["metric"]["a"] == 0.9375 and a["Wd"].shape == (len(leaves), 4, 16, 16, 16)
