@@ -674,7 +674,7 @@ def run_ours(args):
         integ = bhgpu.RK2Integrator(CFL)
         for prec in ("fp64", "fp64-fma", "mixed"):
             tree.precision = prec
-            tuning[prec] = bhgpu.tune.autotune(tree, integ, reps=2, save=True)
+            tuning[prec] = bhgpu.tune.autotune(tree, integ, reps=2, save=(rank == 0))
         tree.precision = args.precision
         tree.clear_error()
     elif args.autotune == 2:

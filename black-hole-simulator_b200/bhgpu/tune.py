@@ -115,25 +115,36 @@ def autotune(tree, integrator, reps: int = 3, cache: str | None = None, save: bo
     torch.cuda.synchronize()
     choice = current(prec)
     if save:
-        path = _cache_path(cache)
-        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
-        data = {}
-        if os.path.exists(path):
-            with open(path) as f:
-                data = json.load(f)
-        data[_key(prec)] = choice
-        with open(path, "w") as f:
-            json.dump(data, f, indent=1, sort_keys=True)
+        _save(_cache_path(cache), _key(prec), choice)
     return {"choice": choice, "ms": timings}
+
+
+def _save(path: str, key: str, choice: dict) -> None:
+    """Merge one choice into the cache file; the file is replaced whole
+    (write to a temporary name, then rename), so a reader never sees half
+    of it, and an unreadable old file is started afresh."""
+    os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+    data = {}
+    try:
+        with open(path) as f:
+            data = json.load(f)
+    except (OSError, ValueError):
+        data = {}
+    data[key] = choice
+    tmp = f"{path}.{os.getpid()}.tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
 
 
 def load_tuning(precision: str, cache: str | None = None) -> dict | None:
     """Apply the cached choice for this GPU and variant, if there is one."""
     path = _cache_path(cache)
-    if not os.path.exists(path):
+    try:
+        with open(path) as f:
+            choice = json.load(f).get(_key(precision))
+    except (OSError, ValueError):
         return None
-    with open(path) as f:
-        choice = json.load(f).get(_key(precision))
     if not choice:
         return None
     for k, c in choice.items():

@@ -116,3 +116,21 @@ def test_tuning_table_host_side():
     with pytest.raises(BhError):
         tune.set("fp64", "update", 7)
     assert tune.get("fp64", "update") == 4
+
+
+def test_tuning_cache_file(tmp_path):
+    """The tuner's cache: merged per key, replaced whole, a damaged file
+    started afresh and read as absent (host only)."""
+    import json
+    from bhgpu import tune
+    path = str(tmp_path / "t.json")
+    tune._save(path, "GPU|fp64", {"flux": 4})
+    tune._save(path, "GPU|mixed", {"flux": 6})
+    with open(path) as f:
+        assert json.load(f) == {"GPU|fp64": {"flux": 4}, "GPU|mixed": {"flux": 6}}
+    with open(path, "w") as f:
+        f.write("{not json")
+    assert tune.load_tuning("fp64", cache=path) is None
+    tune._save(path, "GPU|fp64", {"flux": 5})
+    with open(path) as f:
+        assert json.load(f) == {"GPU|fp64": {"flux": 5}}
