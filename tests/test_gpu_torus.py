@@ -114,21 +114,25 @@ def test_snapshot_of_the_torus(tmp_path):
 
 def test_mixed_first_step_of_the_torus_within_1e_5_of_fp64():
     """The mixed FP32/FP64 variant against the faithful FP64 variant on the
-    torus (same initial data, one step): relative L1 per conserved
-    component at most 1e-5 (the accuracy bound the mixed form is held to),
-    NaN masks within 1e-3 of each other."""
+    torus at its configuration's resolution (128^3 over [-40,40]^3, same
+    initial data, one step): relative L1 per conserved component at most
+    1e-5 (the accuracy bound the mixed form is held to), NaN masks within
+    1e-3 of each other.  (On a 32^3 grid the first step is already as
+    chaotic as the reference's own response to one-ulp noise, so the bound
+    is checked where the configuration is defined.)"""
     import bhgpu
     from helpers import mask_disagreement, rel_l1
-    q = Quilt([-40.0] * 3, [40.0] * 3, 2)
+    q = Quilt([-40.0] * 3, [40.0] * 3, 8)
     out = {}
     for prec in ("fp64", "mixed"):
-        tree = bhgpu.AmrTree(q.dom_l, q.dom_h, 2, M=1.0, a=0.9375, Q=0.0, gm=4.0 / 3.0, quilt=q, init_floor=False,
+        tree = bhgpu.AmrTree(q.dom_l, q.dom_h, 8, M=1.0, a=0.9375, Q=0.0, gm=4.0 / 3.0, quilt=q, init_floor=False,
                              precision=prec)
         tree.torus_init(r_max=12.0, r_in=6.0)
         bhgpu.RK2Integrator(0.4).step(tree, check_domain=False)
         out[prec] = tree.U.cpu().numpy()
+        del tree
     l1 = rel_l1(out["mixed"], out["fp64"])
     mask = mask_disagreement(out["mixed"], out["fp64"])
-    print("mixed vs fp64 on the torus, one step: L1", ["%.1e" % x for x in l1], "mask", mask)
+    print("mixed vs fp64 on the 128^3 torus, one step: L1", ["%.1e" % x for x in l1], "mask", mask)
     assert mask <= 1e-3
     assert max(l1) <= 1e-5, l1
