@@ -743,6 +743,16 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     err = tree.read_error()
+    # constrained transport keeps div B at roundoff: the face-centred
+    # divergence (constrans::maxdivB) of the state the timed steps left (one
+    # step from the seeded state) and of the seeded state itself, raw and
+    # relative to max|B| / dx
+    divb_after = float(torch.nan_to_num(tree.maxdivb(), nan=0.0).max().item())
+    tree.U.copy_(U0); tree.W.copy_(W0); tree.Bf.copy_(B0)
+    divb_before = float(torch.nan_to_num(tree.maxdivb(), nan=0.0).max().item())
+    bscale = float(B0.abs().max().item()) / float(tree.tables["pgeo"][0, 3])
+    divb = {"max_initial": divb_before, "max_after_step": divb_after,
+            "relative_initial": divb_before / bscale, "relative_after_step": divb_after / bscale}
 
     # ---- the other arithmetic variants, same workload, for comparison --------
     variants = {}
@@ -873,6 +883,7 @@ def run_ours(args):
                          "step_frac": value / world * STEP_BYTES / (peak * 1e9)},
             "clocks": ck,
             "device_error_word": err,
+            "div_B": divb,
             "autotune": ({prec: {"choice_ctas_per_sm": t["choice"], "timed": bool(t["ms"]),
                                  "step_ms_per_candidate": {k: {str(c): round(m, 4) for c, m in v.items()}
                                                            for k, v in t["ms"].items()}}
