@@ -523,8 +523,24 @@ def torus_step_bench(steps=20, free_steps=100):
     for prec in free:
         del free[prec]["U"]
     out[f"free_run_{free_steps}_steps"] = free
+    # the divergence timeline: fp64 and mixed stepped side by side from the
+    # same initial data (untimed), NaN fraction of U and mixed-vs-fp64
+    # relative L1 on the entries finite in both, at checkpoints
     t.precision = "fp64"
-    del t
+    m = bhgpu.AmrTree(q.dom_l, q.dom_h, 8, M=1.0, a=0.9375, Q=0.0, gm=GAMMA, quilt=q, init_floor=False,
+                      precision="mixed")
+    t.U.copy_(U0); t.W.copy_(W0); t.Bf.copy_(B0)
+    m.U.copy_(U0); m.W.copy_(W0); m.Bf.copy_(B0)
+    timeline = []
+    for k in range(1, free_steps + 1):
+        integ.step(t, sync=False, check_domain=False)
+        integ.step(m, sync=False, check_domain=False)
+        if k in (1, 2, 3, 5, 10, 20, 50, 100):
+            l1 = field_l1(m.U, t.U)
+            timeline.append({"step": k, "nan_frac_U_fp64": float((~torch.isfinite(t.U)).double().mean().item()),
+                             "mixed_vs_fp64": l1})
+    out["divergence_timeline"] = timeline
+    del t, m
     return out
 
 
