@@ -41,6 +41,21 @@ __host__ __device__ constexpr uint32_t kmaj(int row, int k, int K) {
     return (uint32_t)((row >> 3) * (K / 8) * 128 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
+// the operand layouts the descriptors below assume: every element inside
+// its buffer, the layer-1 operand inside the first 4 KB of the shared one,
+// and each K = 16 step 256 bytes (two 128-byte core-matrix columns) on
+static_assert(kmaj(ROWS - 1, K2 - 1, K2) + 2 <= ROWS * K2 * 2, "layer-2 A in its buffer");
+static_assert(kmaj(ROWS - 1, K1 - 1, K1) + 2 <= ROWS * K1 * 2, "layer-1 A in the first 4 KB");
+static_assert(kmaj(NH - 1, K1 - 1, K1) + 2 <= NH * K1 * 2, "layer-1 B in its buffer");
+static_assert(kmaj(NH - 1, NH - 1, NH) + 2 <= NH * NH * 2, "layer-2 B in its buffer");
+static_assert(kmaj(0, 16, K2) == 256 && kmaj(0, 48, NH) == 3 * 256, "K-step stride of the descriptors");
+static_assert(kmaj(8, 0, K2) == (K2 / 8) * 128 && kmaj(8, 0, K1) == (K1 / 8) * 128, "8-row group stride (SBO)");
+static_assert(kmaj(0, 8, K2) == 128, "core-matrix column stride (LBO)");
+// kind::f16 with M = 128: N a multiple of 16 in [16, 256]; the fields fit
+static_assert(ROWS == 128 && NH % 16 == 0 && NH >= 16 && NH <= 256, "MMA shape");
+static_assert((NH >> 3) < 64 && (ROWS >> 4) < 32, "instruction-descriptor fields");
+static_assert(2 * NI + 1 <= K1, "features, their low halves and the bias column fit layer 1's K");
+
 struct Smem {
     alignas(128) uint8_t a[ROWS * K2 * 2];   // 32 KB: layer-1 A (K = 16, first 4 KB) or layer-2 A (K = 128)
     alignas(128) uint8_t b1[NH * K1 * 2];    // 2 KB
