@@ -358,13 +358,18 @@ BH_HD inline bool cp_bd(double gamma, double xa, double xb, double Ssq, double B
     double xc = xa, fc = fa;
     bool mflag = true;
     double s = 0.0, d = 0.0;
+    // fa and fb change only by the swap at the end of an iteration (A7: they
+    // are never updated from fs), so fb - fa is loop-invariant until a swap;
+    // its reciprocal is formed here and again after a swap (used by the
+    // variants that multiply by reciprocals; the faithful one divides)
+    double idfba = 1.0 / (fb - fa);
     for (int i = 0; i < 100; i++) {
         if (fabs(xb - xa) < tol) { root = xb; return true; }
         if (fa != fc && fb != fc)
             s = (xa * fb * fc) / ((fa - fb) - (fa - fc)) + (xb * fa * fc) / ((fb - fa) - (fb - fc)) +
                 (xc * fa * fb) / ((fc - fa) - (fc - fb));
         else
-            s = xb - fb * (xb - xa) / (fb - fa);
+            s = xb - quo(fb * (xb - xa), fb - fa, idfba);
         bool c1 = !((3 * xa + 4) / 4 < s && s < xb);
         bool c2 = mflag && fabs(s - xb) >= fabs(xb - xc) / 2;
         bool c3 = !mflag && fabs(s - xb) >= fabs(xc - d) / 2;
@@ -374,7 +379,10 @@ BH_HD inline bool cp_bd(double gamma, double xa, double xb, double Ssq, double B
         d = xc; xc = xb; fc = fb;
         if (fa * fs < 0.0) xb = s;
         else xa = s;
-        if (fabs(fa) < fabs(fb)) { double t = xa; xa = xb; xb = t; t = fa; fa = fb; fb = t; }
+        if (fabs(fa) < fabs(fb)) {
+            double t = xa; xa = xb; xb = t; t = fa; fa = fb; fb = t;
+            idfba = 1.0 / (fb - fa);
+        }
     }
     return false;
 }
