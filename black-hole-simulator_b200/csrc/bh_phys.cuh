@@ -317,14 +317,24 @@ BH_HD inline double f_df(double gamma, double xi, double Ssq, double Bsq, double
     double K = Bsq;
     double X = xi * xi;
     double xipK = xi + K;
+#ifdef BH_RCP
+    // one division for both divisors of the residual, X + (xi + K)^2 and X:
+    // their reciprocals from that of the product (an ulp or two each)
+    double Dv = X + xipK * xipK;
+    double rXD = 1.0 / (X * Dv);
+    double vsq = (Ssq * X + Yi * (2.0 * xi + K)) * (X * rXD);
+    double iX = Dv * rXD;
+#else
     double vsq = (Ssq * X + Yi * (2.0 * xi + K)) / (X + xipK * xipK);
+    double iX = 1.0 / X;                  // read only by the reciprocal variants' quo
+#endif
     if (vsq >= 1.0) { df = 0.0; return 1e30; }
     double om = 1.0 - vsq;                // 1 / ltz2 within an ulp
     double ltz2 = 1.0 / om;
     double ltz = sqrt(ltz2);
     // reciprocals for quo: 1 / ltz = sqrt(om) within two ulps; with them the
     // residual alone (fres) needs neither ltz2 nor ltz
-    double il = sqrt(om), iX = 1.0 / X;
+    double il = sqrt(om);
     double rho = quo(Dn, ltz, il);
     double G = gamma - 1.0;
     double p = (G / gamma) * (quo(xi, ltz2, om) - quo(Dn, ltz, il));
