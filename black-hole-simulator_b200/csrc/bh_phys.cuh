@@ -326,7 +326,6 @@ BH_HD inline double f_df(double gamma, double xi, double Ssq, double Bsq, double
     double iX = Dv * rXD;
 #else
     double vsq = (Ssq * X + Yi * (2.0 * xi + K)) / (X + xipK * xipK);
-    double iX = 1.0 / X;                  // read only by the reciprocal variants' quo
 #endif
     if (vsq >= 1.0) { df = 0.0; return 1e30; }
     double om = 1.0 - vsq;                // 1 / ltz2 within an ulp
@@ -334,7 +333,11 @@ BH_HD inline double f_df(double gamma, double xi, double Ssq, double Bsq, double
     double ltz = sqrt(ltz2);
     // reciprocals for quo: 1 / ltz = sqrt(om) within two ulps; with them the
     // residual alone (fres) needs neither ltz2 nor ltz
+#ifdef BH_RCP
     double il = sqrt(om);
+#else
+    double il = sqrt(om), iX = 1.0 / X;   // read only by the reciprocal variants' quo
+#endif
     double rho = quo(Dn, ltz, il);
     double G = gamma - 1.0;
     double p = (G / gamma) * (quo(xi, ltz2, om) - quo(Dn, ltz, il));
