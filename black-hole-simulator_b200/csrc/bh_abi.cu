@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <mutex>
+#include <new>
 #include "bhgpu.h"
 #include "bh_api.h"
 #include "bh_phys.cuh"
@@ -167,6 +168,51 @@ int bh_rkstg(const bh_params* P, const bh_pool* pool, const double* dt_dev, int3
 int bh_step(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, const int32_t* waves,
             const int32_t* wave_off, int32_t nwave, void* stream) {
     BH_DISPATCH(P, step(P, pool, cfl, dt_dev, waves, wave_off, nwave, stream));
+}
+
+struct bh_step_graph {
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+};
+
+int bh_step_graph_create(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev,
+                         const int32_t* waves, const int32_t* wave_off, int32_t nwave, void* stream,
+                         bh_step_graph** out) {
+    if (!P || !out || !stream) return BH_EINVAL;
+    *out = nullptr;
+    cudaStream_t st = S(stream);
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return BH_ECUDA;
+    int rc = bh_step(P, pool, cfl, dt_dev, waves, wave_off, nwave, stream);
+    cudaGraph_t graph = nullptr;
+    // the capture is always ended, also when the step refused its arguments
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (rc != BH_OK || e != cudaSuccess || !graph) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc != BH_OK ? rc : BH_ECUDA;
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return BH_ECUDA;
+    }
+    bh_step_graph* g = new (std::nothrow) bh_step_graph{graph, exec};
+    if (!g) {
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        return BH_ECUDA;
+    }
+    *out = g;
+    return BH_OK;
+}
+int bh_step_graph_replay(bh_step_graph* g, void* stream) {
+    if (!g || !stream) return BH_EINVAL;
+    return cudaGraphLaunch(g->exec, S(stream)) == cudaSuccess ? BH_OK : BH_ECUDA;
+}
+int bh_step_graph_destroy(bh_step_graph* g) {
+    if (!g) return BH_EINVAL;
+    cudaError_t a = cudaGraphExecDestroy(g->exec), b = cudaGraphDestroy(g->graph);
+    delete g;
+    return a == cudaSuccess && b == cudaSuccess ? BH_OK : BH_ECUDA;
 }
 
 }  // extern "C"

@@ -337,6 +337,23 @@ int bh_rkstg(const bh_params *P, const bh_pool *pool, const double *dt_dev, int3
 int bh_step(const bh_params *P, const bh_pool *pool, double cfl, double *dt_dev,
             const int32_t *waves, const int32_t *wave_off_host, int32_t nwave, void *stream);
 
+/* rk2integrator::step recorded once as a CUDA graph and replayed: the step
+ * never synchronises with the host (dt stays in *dt_dev), so its launches
+ * form one graph.  bh_step_graph_create captures bh_step with these
+ * arguments on `stream` (required, not the legacy default stream) and
+ * instantiates it; the pool's arrays, dt_dev and waves must stay valid and
+ * at the same addresses while the graph lives.  The graph keeps the launch
+ * bounds chosen when it was captured (bh_tune_set).  The CUDA graph objects
+ * are host-side handles the CUDA runtime allocates; no device memory is
+ * allocated.  (The reference has no counterpart: its step is a host loop.) */
+typedef struct bh_step_graph bh_step_graph;
+int bh_step_graph_create(const bh_params *P, const bh_pool *pool, double cfl, double *dt_dev,
+                         const int32_t *waves, const int32_t *wave_off_host, int32_t nwave, void *stream,
+                         bh_step_graph **out);
+/* one step: a replay of the captured graph on `stream` */
+int bh_step_graph_replay(bh_step_graph *g, void *stream);
+int bh_step_graph_destroy(bh_step_graph *g);
+
 #ifdef __cplusplus
 }
 #endif

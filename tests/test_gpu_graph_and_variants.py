@@ -86,3 +86,46 @@ def test_host_pipeline_equals_stepping_alone():
     for o, w in zip(outs, want):
         for a, b in zip(o, w):
             assert torch.equal(a.nan_to_num(7.0), b.nan_to_num(7.0))
+
+
+def test_c_abi_step_graph_equals_direct_steps():
+    """bh_step_graph_create / _replay / _destroy (the step as a CUDA graph for
+    C callers): two replays on a non-default stream equal two direct bh_step
+    calls bit for bit (faithful variant), and the legacy default stream is
+    refused."""
+    import ctypes as C
+    import bhgpu
+    from bhgpu._lib import BhParams, BhPool, lib
+    from bhgpu.solver import _p
+    vp = C.c_void_p
+    lib.bh_step_graph_create.argtypes = [C.POINTER(BhParams), C.POINTER(BhPool), C.c_double, vp, vp, vp, C.c_int32,
+                                         vp, C.POINTER(vp)]
+    lib.bh_step_graph_replay.argtypes = [vp, vp]
+    lib.bh_step_graph_destroy.argtypes = [vp]
+    for f in ("bh_step_graph_create", "bh_step_graph_replay", "bh_step_graph_destroy"):
+        getattr(lib, f).restype = C.c_int
+    q, orc, hp = box_case(2, seed=9, periodic=True, lim=0)
+    direct = gpu_tree(q, hp, 0.0, 0.0, 0)
+    rk = bhgpu.RK2Integrator(0.4)
+    rk.step(direct, check_domain=False)
+    rk.step(direct, check_domain=False)
+    torch.cuda.synchronize()
+    g_tree = gpu_tree(q, hp, 0.0, 0.0, 0)
+    P = g_tree.params()
+    off = g_tree._wave_off
+    s = torch.cuda.Stream()
+    h = vp()
+    args = (C.byref(P), C.byref(g_tree.pool), 0.4, _p(g_tree.dt), _p(g_tree.waves), off.ctypes.data_as(vp),
+            g_tree.nwave)
+    assert lib.bh_step_graph_create(*args, None, C.byref(h)) != 0      # legacy default stream refused
+    assert lib.bh_step_graph_create(*args, vp(s.cuda_stream), C.byref(h)) == 0 and h.value
+    try:
+        for _ in range(2):
+            assert lib.bh_step_graph_replay(h, vp(s.cuda_stream)) == 0
+        s.synchronize()
+    finally:
+        assert lib.bh_step_graph_destroy(h) == 0
+    for name in ("U", "W", "Bf"):
+        a, b = getattr(direct, name), getattr(g_tree, name)
+        assert torch.equal(a.contiguous().view(torch.int64), b.contiguous().view(torch.int64)), name
+    assert torch.equal(direct.dt.view(torch.int64), g_tree.dt.view(torch.int64))
