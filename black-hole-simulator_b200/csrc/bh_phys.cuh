@@ -147,9 +147,12 @@ BH_HD inline void met_comp(const MP& m, double r, double th, Met& o) {
     o.gam_inv[2][0] = gi13; o.gam_inv[2][1] = 0.0; o.gam_inv[2][2] = gi33;
     o.sqrtdetg = (r * r + a * a * s2) * t.s;                // gdet :52-54
     o.alpha = pow_mhalf(1 + H);                             // lapse :93-95
-    o.beta[0] = -gi01 / gi00;                               // shift :96-100
-    o.beta[1] = -0.0 / gi00;
-    o.beta[2] = -0.0 / gi00;
+    // shift :96-100, three quotients by g^00 (one reciprocal in the
+    // reciprocal variants; the sign of -0.0 / g^00 is kept by the product)
+    double igi00 = 1.0 / gi00;
+    o.beta[0] = quo(-gi01, gi00, igi00);
+    o.beta[1] = quo(-0.0, gi00, igi00);
+    o.beta[2] = quo(-0.0, gi00, igi00);
     o.sqrtdetgam = o.alpha * o.sqrtdetg;                    // :117-119
 }
 
@@ -183,7 +186,8 @@ BH_HD inline void met_src(const MP& m, double r, double th, MetSrc& o) {
     o.gi[3][3] = pow_m1(Sig * t.s * t.s);
     o.sqrtdetg = (r * r + a * a * s2) * t.s;
     o.alpha = pow_mhalf(1 + H);
-    for (int i = 0; i < 3; i++) o.beta[i] = -o.gi[0][i + 1] / o.gi[0][0];
+    double igi00 = 1.0 / o.gi[0][0];
+    for (int i = 0; i < 3; i++) o.beta[i] = quo(-o.gi[0][i + 1], o.gi[0][0], igi00);
     // metric derivatives (:72-80)
     double sig = r * r + a * a * c2;
     double isig = pow_m1(sig), isig2 = pow_m2(sig);
@@ -318,10 +322,13 @@ BH_HD inline double f_df(double gamma, double xi, double Ssq, double Bsq, double
     double X = xi * xi;
     double xipK = xi + K;
 #ifdef BH_RCP
-    // one division for both divisors of the residual, X + (xi + K)^2 and X:
-    // their reciprocals from that of the product (an ulp or two each)
-    double Dv = X + xipK * xipK;
-    double rXD = 1.0 / (X * Dv);
+    // one division for the divisors of the residual, X + (xi + K)^2 and X,
+    // and of its derivative, X (xi + K)^2: their reciprocals from that of
+    // the product (an ulp or two each)
+    double xipK2 = xipK * xipK;
+    double Dv = X + xipK2;
+    double r3 = 1.0 / (X * Dv * xipK2);
+    double rXD = xipK2 * r3;
     double vsq = (Ssq * X + Yi * (2.0 * xi + K)) * (X * rXD);
     double iX = Dv * rXD;
 #else
@@ -348,7 +355,11 @@ BH_HD inline double f_df(double gamma, double xi, double Ssq, double Bsq, double
     double Mq = X * xipK * xipK;
     double dN = 2.0 * Ssq * xi + 2.0 * Yi;
     double dM = 2.0 * xi * xipK * xipK + 2.0 * X * X;
-    double iMq = 1.0 / Mq;
+#ifdef BH_RCP
+    double iMq = Dv * r3;
+#else
+    double iMq = 1.0 / Mq;               // read only by the reciprocal variants' quo
+#endif
     double dvv = quo(dN * Mq - dM * N, Mq * Mq, iMq * iMq);
     double dltz2 = ltz2 * ltz2 * dvv;
     double dltz = quo(dltz2, 2.0 * ltz, 0.5 * il);
