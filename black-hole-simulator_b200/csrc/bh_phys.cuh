@@ -96,6 +96,7 @@ template <typename RT>
 struct MetT {
     RT gam[3][3], gam_inv[3][3];
     RT alpha, beta[3], sqrtdetg, sqrtdetgam;
+    RT ialpha;   // 1 / alpha, for the reciprocal variants' quo
 };
 using Met = MetT<double>;
 // the spatial metric at reduced precision (values computed in FP64)
@@ -104,7 +105,7 @@ BH_HD inline MetT<RT> met_cast(const Met& m) {
     MetT<RT> o;
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) { o.gam[i][j] = RT(m.gam[i][j]); o.gam_inv[i][j] = RT(m.gam_inv[i][j]); }
-    o.alpha = RT(m.alpha); o.sqrtdetg = RT(m.sqrtdetg); o.sqrtdetgam = RT(m.sqrtdetgam);
+    o.alpha = RT(m.alpha); o.sqrtdetg = RT(m.sqrtdetg); o.sqrtdetgam = RT(m.sqrtdetgam); o.ialpha = RT(m.ialpha);
     for (int i = 0; i < 3; i++) o.beta[i] = RT(m.beta[i]);
     return o;
 }
@@ -146,7 +147,15 @@ BH_HD inline void met_comp(const MP& m, double r, double th, Met& o) {
     o.gam_inv[1][0] = 0.0;  o.gam_inv[1][1] = gi22; o.gam_inv[1][2] = 0.0;
     o.gam_inv[2][0] = gi13; o.gam_inv[2][1] = 0.0; o.gam_inv[2][2] = gi33;
     o.sqrtdetg = (r * r + a * a * s2) * t.s;                // gdet :52-54
+#if defined(BH_RCP) && defined(__CUDA_ARCH__)
+    // the reciprocal variants on the device: the lapse from the hardware
+    // reciprocal square root (within an ulp), its inverse without a division
+    o.alpha = rsqrt(1 + H);                                 // lapse :93-95
+    o.ialpha = (1 + H) * o.alpha;
+#else
     o.alpha = pow_mhalf(1 + H);                             // lapse :93-95
+    o.ialpha = 1.0 / o.alpha;
+#endif
     // shift :96-100, three quotients by g^00 (one reciprocal in the
     // reciprocal variants; the sign of -0.0 / g^00 is kept by the product)
     double igi00 = 1.0 / gi00;
@@ -293,7 +302,7 @@ BH_HD inline bool ptoc(RT gamma, const MetT<RT>& mc, const PrimT<RT>& pv, ConsT<
 #pragma unroll
         for (int j = 0; j < 3; j++) Bsq += Blow[i] * mc.gam[i][j] * pv.B[j];
     RT b2 = quo(Bv * Bv + Bsq, lor, sq1v);
-    RT bt = lor * Bv / mc.alpha;
+    RT bt = quo(lor * Bv, mc.alpha, mc.ialpha);
     RT pstar = p + b2 / 2;
     RT w = pv.rho * h + b2;
     CV.D = sg * pv.rho * lor;
