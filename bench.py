@@ -76,7 +76,7 @@ def parse():
                     help="launch bounds of the heavy kernels: 1 tune them on the box first and save the choice "
                          "(bhgpu.tune), 2 apply the saved choice without timing (for profiler runs), 0 keep "
                          "the compiled-in ones")
-    ap.add_argument("--precision", default="fp64-fma", choices=["fp64", "fp64-fma", "mixed"],
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64-fma", "mixed"],
                     help="arithmetic variant of the headline value; the other variants are timed beside it")
     return ap.parse_args()
 
@@ -191,8 +191,8 @@ def cpu_reference_sample(threads):
     all host threads; returns (zone-updates/s, kind, sample)."""
     import numpy as np
     import oracle
-    from bhgpu import configs
-    from bhgpu.mesh import Quilt
+    from bhgrid import configs
+    from bhgrid.mesh import Quilt
     os.environ["OMP_NUM_THREADS"] = str(threads)
     q = Quilt([LO] * 3, [HI] * 3, 4, periodic=False)
     W, Bf = configs.magnetised_box(q, seed=1, gamma=GAMMA)
@@ -614,8 +614,8 @@ def run_reference(args):
         return 0
     import numpy as np
     import oracle
-    from bhgpu import configs
-    from bhgpu.mesh import Quilt
+    from bhgrid import configs
+    from bhgrid.mesh import Quilt
     threads = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(threads)
     nq = 4

@@ -15,22 +15,30 @@ constexpr int NC_ = bh::NC;
 // ---- library-owned scratch for bh_ghosts_prims_static ---------------------
 // The con2prim outcome of every interior cell, BH_STATIC_MAX_PATCHES x 8000
 // bytes, held by every GPU that loads the library until the process exits.
-// Host code cannot use the array's name as a device address: each device's
-// address is looked up once (cudaGetSymbolAddress, on the first call made
-// with that device current) and handed to the kernels.
+// Host code cannot use the array's name as a device address: the current
+// device's address is looked up (cudaGetSymbolAddress) and handed to the
+// kernels.  The lookup is repeated on every call made while the stream is
+// not being captured, so the address follows the module when a device reset
+// (cudaDeviceReset) or a new primary context reloads it; a call made during
+// a capture cannot look it up and takes the address the last uncaptured
+// call on that device found.
 __device__ __align__(256) uint8_t g_static_status[(size_t)BH_STATIC_MAX_PATCHES * NC_];
 constexpr int kMaxDevices = 64;
 void* g_static_status_ptr[kMaxDevices] = {nullptr};
 std::mutex g_static_status_mu;
 
-int static_status_ptr(uint8_t** out) {
+int static_status_ptr(cudaStream_t st, uint8_t** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BH_ECUDA;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return BH_ECUDA;
     std::lock_guard<std::mutex> lock(g_static_status_mu);
-    if (!g_static_status_ptr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_static_status) != cudaSuccess || !p) return BH_ECUDA;
         g_static_status_ptr[dev] = p;
+    } else if (!g_static_status_ptr[dev]) {
+        return BH_ECUDA;   // no uncaptured call has looked the address up on this device
     }
     *out = (uint8_t*)g_static_status_ptr[dev];
     return BH_OK;
@@ -99,7 +107,7 @@ int bh_ghosts_prims_static(const bh_params* P, const bh_pool* pool, void* stream
     if (pool->npatch > BH_STATIC_MAX_PATCHES) return BH_ERANGE;
     if (pool->nleaf == 0) return BH_OK;
     uint8_t* status = nullptr;
-    int rc = static_status_ptr(&status);
+    int rc = static_status_ptr(S(stream), &status);
     if (rc) return rc;
     // every entry read is written by the interior pass of the same call first
     BH_DISPATCH(P, ghosts_prims_status(P, pool, status, stream));

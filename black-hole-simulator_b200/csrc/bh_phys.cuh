@@ -194,7 +194,13 @@ BH_HD inline void met_src(const MP& m, double r, double th, MetSrc& o) {
     o.gi[1][3] = o.gi[3][1] = a * pow_m1(Sig);
     o.gi[3][3] = pow_m1(Sig * t.s * t.s);
     o.sqrtdetg = (r * r + a * a * s2) * t.s;
+#if defined(BH_RCP) && defined(__CUDA_ARCH__)
+    // the same lapse as met_comp's in the reciprocal variants, so that the
+    // face/ptoc metric and the source metric of a cell agree to the bit
+    o.alpha = rsqrt(1 + H);
+#else
     o.alpha = pow_mhalf(1 + H);
+#endif
     double igi00 = 1.0 / o.gi[0][0];
     for (int i = 0; i < 3; i++) o.beta[i] = quo(-o.gi[0][i + 1], o.gi[0][0], igi00);
     // metric derivatives (:72-80)

@@ -84,11 +84,22 @@ class DomainError(ValueError):
     """The reference throws std::domain_error from its EOS (thermo.cpp:11-31)."""
 
 
+def reference_root() -> str:
+    """Root of the reference checkout: $BH_REFERENCE if set, else the
+    Makefile's default (REF ?=), which is the only place that names one."""
+    env = os.environ.get("BH_REFERENCE")
+    if env:
+        return env
+    out = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True)
+    return out.stdout.strip() if out.returncode == 0 else ""
+
+
 def build(ref: bool = True, quiet: bool = True):
     """Compile the checkers (the reference harness only if its sources exist)."""
     targets = ["all"]
-    if ref and os.path.isdir("/root/reference/src/fluid"):
-        targets.append("ref")
+    root = reference_root() if ref else ""
+    if root and os.path.isdir(os.path.join(root, "src", "fluid")):
+        targets += ["ref", "REF=" + root]
     out = subprocess.run(["make", "-C", HERE] + targets, capture_output=quiet, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + (out.stderr or ""))

@@ -102,6 +102,34 @@ def test_ctop(M, a, Q):
         assert rel_linf(Wg[v, same], Wc[v, same]) <= TOL, v
 
 
+def test_ctop_stress_batch_distribution():
+    """The con2prim stress batch's own distribution (log-uniform rho in
+    [1e-8, 1], W up to 20, sigma up to 100, Kerr a = 0.9375 at r in
+    [1.5, 50]) on a 2^16-cell sample: the same gates as test_ctop
+    (conserved.cpp:135-285)."""
+    import bhgpu
+    from bhgpu import configs
+    a = 0.9375
+    W, r, th = configs.con2prim_batch(1 << 16, seed=4, gamma=GAMMA, a=a)
+    orc = oracle.Oracle(1.0, a, 0.0, GAMMA)
+    Uc, _ = orc.ptoc(W, r, th)
+    cn = bhgpu.Conserved(bhgpu.Metric(1.0, a, 0.0), bhgpu.State(GAMMA))
+    Wg, _, stg, itg, pag = [_np(x) for x in cn.ctop(Uc, r, th, check_domain=False)]
+    Wc, _, stc, itc, pac = orc.ctop(Uc, r, th)
+    newton = pac == 0
+    assert newton.sum() > 1000 and (pac >= 2).sum() > 1000, "both routes exercised"
+    assert np.array_equal(pag[newton], pac[newton]) and np.array_equal(itg[newton], itc[newton])
+    assert np.array_equal(stg[newton], stc[newton])
+    _, _, st1, _, _ = orc.ctop(Uc, r, np.nextafter(th, 10.0))
+    own = np.mean(st1 != stc)
+    assert np.mean(stg != stc) <= 1.5 * own + 1e-3, (np.mean(stg != stc), own)
+    same = (stg == 1) & (stc == 1) & (pag == pac)
+    assert same.sum() > 1000
+    assert same_nan(Wg[:, same], Wc[:, same])
+    for v in range(8):
+        assert rel_linf(Wg[v, same], Wc[v, same]) <= TOL, v
+
+
 def test_ctop_brent_route_exact_metric():
     """theta = pi/2 and a flat metric make every metric entry exact on both
     sides; the Brent fallback then gives identical outcomes."""
