@@ -1,0 +1,298 @@
+"""The corrected ("fixed") scheme: Valencia GRMHD in Cartesian Kerr-Schild.
+
+The reference's own scheme (``src/fluid``) stops in the first step of a Kerr
+torus (``physics/thermo.cpp:10-11`` reached from ``conserved.cpp:205``); this
+mode keeps its structure -- ``rk2integrator::step`` = dt, two RK stages of
+con2prim, ghost fill, face fluxes, constrained transport and update
+(``solver/integrator.cpp:191-275``) -- with the defects corrected (listed in
+``csrc/bh_fixed_phys.cuh``).  Host side only: the block table, the
+27-neighbour table and the work lists are built here in numpy; the device
+buffers are torch tensors; every computation runs in ``libbhgpu.so``.
+
+Layout (``include/bhgpu.h``, bh_fx_grid): cubic blocks of n^3 interior cells,
+each stored per array as an (n+5)^3 box (cells -2 .. n+2 per axis).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from bhgrid.blocks import BLOCK_DTYPE, CHUNK, box_size, interior as _interior, uniform_blocks, work_items  # noqa: F401
+
+from ._lib import BH_FP64, BH_FP64_FMA, BH_MIXED, BH_MC, BH_MINMOD, BH_VANLEER, BhError, check, lib
+
+_vp, _d, _i32, _i64 = C.c_void_p, C.c_double, C.c_int32, C.c_int64
+GHOST = 2
+PRECISIONS = {"fp64": BH_FP64, "fp64-fma": BH_FP64_FMA, "mixed": BH_MIXED}
+LIMITERS = {"minmod": BH_MINMOD, "vanleer": BH_VANLEER, "mc": BH_MC}
+
+
+class BhFxParams(C.Structure):
+    _fields_ = [("M", _d), ("a", _d), ("gamma", _d), ("cfl", _d), ("rho_floor", _d), ("u_floor", _d),
+                ("sigma_max", _d), ("W_max", _d), ("r_exc", _d), ("tol", _d), ("maxiter", _i32),
+                ("limiter", _i32), ("precision", _i32), ("reserved", _i32)]
+
+
+class BhFxGrid(C.Structure):
+    _fields_ = [("nblock", _i32), ("blocks", _vp), ("nbr", _vp), ("items_cell", _vp), ("nitem_cell", _i32),
+                ("items_pos", _vp), ("nitem_pos", _i32), ("items_ghost", _vp), ("nitem_ghost", _i32),
+                ("ncell", _i64), ("U", _vp), ("U1", _vp), ("W", _vp), ("Bf", _vp), ("Bf1", _vp), ("F", _vp),
+                ("dt", _vp), ("count", _vp), ("err", _vp)]
+
+
+class BhFxTorus(C.Structure):
+    _fields_ = [("r_in", _d), ("r_max", _d), ("kappa", _d), ("beta", _d), ("noise", _d), ("seed", C.c_uint64)]
+
+
+_sig = {
+    "bh_fx_step": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _vp],
+    "bh_fx_prims": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _i32, _vp],
+    "bh_fx_ghosts": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
+    "bh_fx_fluxes": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
+    "bh_fx_update": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
+    "bh_fx_divb": [C.POINTER(BhFxGrid), _vp, _vp],
+    "bh_fx_torus_init": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), C.POINTER(BhFxTorus), _vp, _vp, _vp],
+}
+for _name, _args in _sig.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = C.c_int
+
+
+def horizon_radius(M: float, a: float) -> float:
+    return M + math.sqrt(M * M - a * a)
+
+
+@dataclass
+class FxParams:
+    """Physics and numerics of the corrected scheme (bh_fx_params)."""
+    M: float = 1.0
+    a: float = 0.9375
+    gamma: float = 4.0 / 3.0
+    cfl: float = 0.4
+    rho_floor: float = 1e-6        # rho >= rho_floor r^-3/2
+    u_floor: float = 1e-8          # p / (Gamma - 1) >= u_floor r^-5/2
+    sigma_max: float = 100.0
+    W_max: float = 50.0
+    r_exc: float | None = None     # default: 1.2 r_H
+    tol: float = 1e-12
+    maxiter: int = 30
+    limiter: str = "vanleer"
+    precision: str = "fp64"
+
+    def cstruct(self) -> BhFxParams:
+        r_exc = self.r_exc if self.r_exc is not None else (
+            1.2 * horizon_radius(self.M, self.a) if self.M > 0 else 0.0)
+        return BhFxParams(self.M, self.a, self.gamma, self.cfl, self.rho_floor, self.u_floor, self.sigma_max,
+                          self.W_max, r_exc, self.tol, self.maxiter, LIMITERS[self.limiter],
+                          PRECISIONS[self.precision], 0)
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class FxGrid:
+    """Device buffers of the corrected scheme on a list of blocks.
+
+    ``FxGrid.uniform(lo, hi, N, block)`` builds the uniform N^3 grid over
+    [lo, hi]^3; ``block`` = N gives one block (no interior ghost exchange).
+    """
+
+    def __init__(self, blocks: np.ndarray, nbr: np.ndarray, params: FxParams, device="cuda"):
+        self.params = params
+        self.blocks_np = blocks
+        self.nbr_np = nbr
+        self.device = torch.device(device)
+        self.ncell = int(sum(box_size(int(n)) for n in blocks["n"]))
+        dev = self.device
+        self.blocks = torch.from_numpy(blocks.view(np.uint8).copy()).to(dev)
+        self.nbr = torch.from_numpy(nbr.copy()).to(dev)
+        self.items = {k: torch.from_numpy(work_items(blocks, k)).to(dev) for k in ("cell", "pos", "ghost")}
+        wdt = torch.float32 if params.precision == "mixed" else torch.float64
+        N = self.ncell
+        self.U = torch.zeros((8, N), dtype=torch.float64, device=dev)
+        self.U1 = torch.zeros_like(self.U)
+        self.W = torch.zeros((8, N), dtype=wdt, device=dev)
+        self.Bf = torch.zeros((3, N), dtype=torch.float64, device=dev)
+        self.Bf1 = torch.zeros_like(self.Bf)
+        self.F = torch.zeros((3, 8, N), dtype=wdt, device=dev)
+        self.dt = torch.zeros(2, dtype=torch.float64, device=dev)
+        self.count = torch.zeros(4, dtype=torch.int32, device=dev)
+        self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.scratch = torch.zeros(4, dtype=torch.float64, device=dev)
+        self._refresh()
+
+    @classmethod
+    def uniform(cls, lo: float, hi: float, N: int, block: int, params: FxParams, periodic=False, device="cuda"):
+        blocks, nbr = uniform_blocks(lo, hi, N, block, periodic)
+        return cls(blocks, nbr, params, device)
+
+    def _refresh(self):
+        it = self.items
+        self._g = BhFxGrid(len(self.blocks_np), _ptr(self.blocks), _ptr(self.nbr),
+                           _ptr(it["cell"]), it["cell"].shape[0], _ptr(it["pos"]), it["pos"].shape[0],
+                           _ptr(it["ghost"]), it["ghost"].shape[0], self.ncell,
+                           _ptr(self.U), _ptr(self.U1), _ptr(self.W), _ptr(self.Bf), _ptr(self.Bf1), _ptr(self.F),
+                           _ptr(self.dt), _ptr(self.count), _ptr(self.err))
+        self._p = self.params.cstruct()
+
+    @property
+    def precision(self):
+        return self.params.precision
+
+    @property
+    def zones(self) -> int:
+        return int(sum(int(n) ** 3 for n in self.blocks_np["n"]))
+
+    # ---- the step (rk2integrator::step, solver/integrator.cpp:262-275) ----
+    def step(self):
+        check(lib.bh_fx_step(C.byref(self._p), C.byref(self._g), _stream()), "bh_fx_step")
+
+    def prims(self, stage=0, with_dt=False):
+        check(lib.bh_fx_prims(C.byref(self._p), C.byref(self._g), stage, int(with_dt), _stream()), "bh_fx_prims")
+
+    def ghosts(self, stage=0):
+        check(lib.bh_fx_ghosts(C.byref(self._p), C.byref(self._g), stage, _stream()), "bh_fx_ghosts")
+
+    def fluxes(self, stage=0):
+        check(lib.bh_fx_fluxes(C.byref(self._p), C.byref(self._g), stage, _stream()), "bh_fx_fluxes")
+
+    def update(self, stage=0):
+        check(lib.bh_fx_update(C.byref(self._p), C.byref(self._g), stage, _stream()), "bh_fx_update")
+
+    def time_step(self) -> float:
+        """dt of the last step (device value, synchronises)."""
+        return float(self.dt[1].item())
+
+    def divb(self) -> float:
+        """max over interior cells of |div B~| / max|B~| of the cell's faces."""
+        out = torch.zeros(len(self.blocks_np), dtype=torch.float64, device=self.device)
+        check(lib.bh_fx_divb(C.byref(self._g), _ptr(out), _stream()), "bh_fx_divb")
+        return float(out.max().item())
+
+    def torus_init(self, r_in=6.0, r_max=12.0, kappa=1e-3, beta=100.0, noise=0.04, seed=1):
+        T = BhFxTorus(r_in, r_max, kappa, beta, noise, seed)
+        out = (C.c_double * 4)()
+        check(lib.bh_fx_torus_init(C.byref(self._p), C.byref(self._g), C.byref(T), _ptr(self.scratch), out,
+                                   _stream()), "bh_fx_torus_init")
+        return {"ell": out[0], "rho_max_raw": out[1], "field_scale": out[2], "beta": out[3]}
+
+    # ---- host views ----------------------------------------------------
+    def interior(self, arr: torch.Tensor) -> np.ndarray:
+        """[..., nblock, n, n, n] interior cells of a [..., ncell] array (numpy,
+        float64); all blocks must have the same n."""
+        return _interior(self.blocks_np, arr.detach().double().cpu().numpy())
+
+    def counters(self) -> dict:
+        c = self.count.cpu().numpy()
+        return {"c2p_failures": int(c[0]), "floored": int(c[1])}
+
+    def reset_counters(self):
+        self.count.zero_()
+
+    def copy_state_from(self, other: "FxGrid"):
+        """U, W (cast), Bf of another grid with the same blocks."""
+        self.U.copy_(other.U)
+        self.W.copy_(other.W.to(self.W.dtype))
+        self.Bf.copy_(other.Bf)
+
+    # ---- the step as one CUDA graph -----------------------------------------
+    def capture(self):
+        """Record one step (9 launches) as a CUDA graph on a side stream
+        (bh_fx_graph_create); ``replay()`` then runs a step with one launch
+        of the graph.  The grid's buffers must not be reallocated while the
+        graph lives."""
+        self.release_graph()
+        s = torch.cuda.Stream(self.device)
+        h = C.c_void_p()
+        check(lib.bh_fx_graph_create(C.byref(self._p), C.byref(self._g), C.c_void_p(s.cuda_stream), C.byref(h)),
+              "bh_fx_graph_create")
+        self._graph = h
+
+    def replay(self):
+        check(lib.bh_step_graph_replay(self._graph, _stream()), "bh_step_graph_replay")
+
+    def release_graph(self):
+        if getattr(self, "_graph", None):
+            lib.bh_step_graph_destroy(self._graph)
+        self._graph = None
+
+    def __del__(self):
+        try:
+            self.release_graph()
+        except Exception:
+            pass
+
+
+lib.bh_fx_graph_create.argtypes = [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _vp, C.POINTER(_vp)]
+lib.bh_fx_graph_create.restype = C.c_int
+lib.bh_step_graph_replay.argtypes = [_vp, _vp]
+lib.bh_step_graph_replay.restype = C.c_int
+lib.bh_step_graph_destroy.argtypes = [_vp]
+lib.bh_step_graph_destroy.restype = C.c_int
+
+
+class FxHostPipeline:
+    """Host-resident torus states stepped through the GPU, copies overlapped.
+
+    Each ``submit`` uploads a state (U, W, Bf in the grid layout, pinned
+    host tensors) into one of the pipeline's device grids on a copy stream,
+    advances it ``steps`` RK2 steps on a compute stream and downloads it on
+    a second copy stream; consecutive submissions use different grids, so
+    the upload of one state, the step of the previous one and the download
+    of the one before overlap.  Each result is bit-identical to stepping the
+    state alone.  The returned event marks the end of the download.
+    """
+
+    def __init__(self, grids: list[FxGrid], steps: int = 1):
+        if not grids:
+            raise ValueError("FxHostPipeline needs at least one device grid")
+        if any(g.ncell != grids[0].ncell or g.precision != grids[0].precision for g in grids):
+            raise ValueError("the grids of a pipeline must share one layout and variant")
+        self.grids, self.steps = list(grids), int(steps)
+        dev = grids[0].device
+        self.s_in, self.s_run, self.s_out = (torch.cuda.Stream(dev) for _ in range(3))
+        self._freed: list[torch.cuda.Event | None] = [None] * len(self.grids)
+        self._k = 0
+
+    def submit(self, U, W, Bf, out_U, out_W, out_Bf) -> torch.cuda.Event:
+        slot = self._k % len(self.grids)
+        self._k += 1
+        g = self.grids[slot]
+        with torch.cuda.stream(self.s_in):
+            if self._freed[slot] is not None:
+                self.s_in.wait_event(self._freed[slot])
+            g.U.copy_(U, non_blocking=True)
+            g.W.copy_(W, non_blocking=True)
+            g.Bf.copy_(Bf, non_blocking=True)
+            loaded = torch.cuda.Event()
+            loaded.record(self.s_in)
+        with torch.cuda.stream(self.s_run):
+            self.s_run.wait_event(loaded)
+            for _ in range(self.steps):
+                g.step()
+            done = torch.cuda.Event()
+            done.record(self.s_run)
+        with torch.cuda.stream(self.s_out):
+            self.s_out.wait_event(done)
+            out_U.copy_(g.U, non_blocking=True)
+            out_W.copy_(g.W, non_blocking=True)
+            out_Bf.copy_(g.Bf, non_blocking=True)
+            freed = torch.cuda.Event()
+            freed.record(self.s_out)
+        self._freed[slot] = freed
+        return freed
+
+    def synchronize(self):
+        for e in self._freed:
+            if e is not None:
+                e.synchronize()

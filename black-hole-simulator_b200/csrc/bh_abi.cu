@@ -178,19 +178,90 @@ int bh_step(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev,
     BH_DISPATCH(P, step(P, pool, cfl, dt_dev, waves, wave_off, nwave, stream));
 }
 
+// ---- the corrected scheme ----------------------------------------------
+namespace {
+int fx_bad(const bh_fx_params* P, const bh_fx_grid* g) {
+    if (!P || !g || g->nblock <= 0 || !g->blocks || !g->nbr || !g->U || !g->U1 || !g->W || !g->Bf || !g->Bf1 ||
+        !g->F || !g->dt || !g->count || g->ncell <= 0)
+        return 1;
+    if ((g->nitem_cell > 0 && !g->items_cell) || (g->nitem_pos > 0 && !g->items_pos) ||
+        (g->nitem_ghost > 0 && !g->items_ghost) || g->nitem_cell < 0 || g->nitem_pos < 0 || g->nitem_ghost < 0)
+        return 1;
+    if (P->precision < BH_FP64 || P->precision > BH_MIXED || P->maxiter <= 0 || !(P->gamma > 1.0)) return 1;
+    return 0;
+}
+}  // namespace
+#define FX_DISPATCH(P, call)                                 \
+    switch ((P)->precision) {                                \
+    case BH_FP64: return vfp64::call;                        \
+    case BH_FP64_FMA: return vfma::call;                     \
+    case BH_MIXED: return vmixed::call;                      \
+    default: return BH_EINVAL;                               \
+    }
+
+int bh_fx_step(const bh_fx_params* P, const bh_fx_grid* g, void* stream) {
+    if (fx_bad(P, g)) return BH_EINVAL;
+    FX_DISPATCH(P, fx_step(P, g, stream));
+}
+int bh_fx_prims(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t with_dt, void* stream) {
+    if (fx_bad(P, g) || stage < 0 || stage > 1) return BH_EINVAL;
+    FX_DISPATCH(P, fx_prims(P, g, stage, with_dt, stream));
+}
+int bh_fx_ghosts(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* stream) {
+    if (fx_bad(P, g) || stage < 0 || stage > 1) return BH_EINVAL;
+    FX_DISPATCH(P, fx_ghosts(P, g, stage, stream));
+}
+int bh_fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* stream) {
+    if (fx_bad(P, g) || stage < 0 || stage > 1) return BH_EINVAL;
+    FX_DISPATCH(P, fx_fluxes(P, g, stage, stream));
+}
+int bh_fx_update(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* stream) {
+    if (fx_bad(P, g) || stage < 0 || stage > 1) return BH_EINVAL;
+    FX_DISPATCH(P, fx_update(P, g, stage, stream));
+}
+int bh_fx_divb(const bh_fx_grid* g, double* out, void* stream) {
+    if (!g || g->nblock <= 0 || !g->blocks || !g->Bf || !out || (g->nitem_cell > 0 && !g->items_cell)) return BH_EINVAL;
+    return vfp64::fx_divb(g, out, stream);
+}
+int bh_fx_torus_init(const bh_fx_params* P, const bh_fx_grid* g, const bh_fx_torus* T, double* scratch, double* out,
+                     void* stream) {
+    if (fx_bad(P, g) || !T || !scratch || !(T->r_max > T->r_in) || !(T->r_in > 0.0) || !(T->kappa > 0.0)) return BH_EINVAL;
+    FX_DISPATCH(P, fx_torus_init(P, g, T, scratch, out, stream));
+}
+
 struct bh_step_graph {
     cudaGraph_t graph;
     cudaGraphExec_t exec;
 };
 
+extern "C++" {
+namespace {
+// capture fn(stream) on stream into an instantiated graph
+template <typename Fn>
+int capture_graph(void* stream, bh_step_graph** out, Fn fn);
+}  // namespace
+}
+
 int bh_step_graph_create(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev,
                          const int32_t* waves, const int32_t* wave_off, int32_t nwave, void* stream,
                          bh_step_graph** out) {
     if (!P || !out || !stream) return BH_EINVAL;
+    return capture_graph(stream, out, [&](void* s) { return bh_step(P, pool, cfl, dt_dev, waves, wave_off, nwave, s); });
+}
+int bh_fx_graph_create(const bh_fx_params* P, const bh_fx_grid* g, void* stream, bh_step_graph** out) {
+    if (!P || !out || !stream) return BH_EINVAL;
+    if (fx_bad(P, g)) return BH_EINVAL;
+    return capture_graph(stream, out, [&](void* s) { return bh_fx_step(P, g, s); });
+}
+
+extern "C++" {
+namespace {
+template <typename Fn>
+int capture_graph(void* stream, bh_step_graph** out, Fn fn) {
     *out = nullptr;
     cudaStream_t st = S(stream);
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return BH_ECUDA;
-    int rc = bh_step(P, pool, cfl, dt_dev, waves, wave_off, nwave, stream);
+    int rc = fn(stream);
     cudaGraph_t graph = nullptr;
     // the capture is always ended, also when the step refused its arguments
     cudaError_t e = cudaStreamEndCapture(st, &graph);
@@ -212,6 +283,9 @@ int bh_step_graph_create(const bh_params* P, const bh_pool* pool, double cfl, do
     *out = g;
     return BH_OK;
 }
+}  // namespace
+}
+
 int bh_step_graph_replay(bh_step_graph* g, void* stream) {
     if (!g || !stream) return BH_EINVAL;
     return cudaGraphLaunch(g->exec, S(stream)) == cudaSuccess ? BH_OK : BH_ECUDA;

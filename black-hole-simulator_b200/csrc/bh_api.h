@@ -55,6 +55,13 @@ inline bool bh_tune_valid(int32_t kernel, int32_t ctas) {
     int rkstg(const bh_params*, const bh_pool*, const double*, int32_t, const int32_t*, const int32_t*, int32_t, \
               void*);                                                                                           \
     int step(const bh_params*, const bh_pool*, double, double*, const int32_t*, const int32_t*, int32_t, void*); \
+    int fx_prims(const bh_fx_params*, const bh_fx_grid*, int32_t, int32_t, void*);                           \
+    int fx_ghosts(const bh_fx_params*, const bh_fx_grid*, int32_t, void*);                                    \
+    int fx_fluxes(const bh_fx_params*, const bh_fx_grid*, int32_t, void*);                                    \
+    int fx_update(const bh_fx_params*, const bh_fx_grid*, int32_t, void*);                                    \
+    int fx_step(const bh_fx_params*, const bh_fx_grid*, void*);                                               \
+    int fx_divb(const bh_fx_grid*, double*, void*);                                                           \
+    int fx_torus_init(const bh_fx_params*, const bh_fx_grid*, const bh_fx_torus*, double*, double*, void*);   \
     }
 
 BH_VARIANT_API(vfp64)

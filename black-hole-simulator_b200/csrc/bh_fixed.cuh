@@ -1,0 +1,682 @@
+// bh_fixed.cuh -- kernels and launch sequences of the corrected ("fixed")
+// scheme (bh_fixed_phys.cuh), compiled once per arithmetic variant inside
+// the variant's namespace (bh_variant.cuh includes this file):
+//   RT  arithmetic type of reconstruction, face fluxes and sources
+//       (double; float in the mixed variant)
+//   WT  storage type of the primitives (the face work's input) and FT of
+//       the face fluxes: RT as well, so the mixed variant moves half the
+//       bytes of the face work
+// Conserved state, face field, con2prim, the CT update and dt stay FP64.
+//
+// Data: a list of cubic blocks, each n^3 interior cells with two ghost
+// layers, stored per array as a (n+5)^3 box (cells -2..n+2 per axis; the
+// extra layer holds the upper faces): index ((i+2) S + (j+2)) S + (k+2) with
+// S = n + 5 -- the reference's per-patch order (grid.cpp:51-53: i slowest,
+// k fastest).  The x-face (i-1/2, j, k), the y-face (i, j-1/2, k) and the
+// z-face (i, j, k-1/2) share the index of cell (i, j, k); so do the edges
+// E_x (i, j-1/2, k-1/2), E_y (i-1/2, j, k-1/2) and E_z (i-1/2, j-1/2, k).
+//
+// Work: every kernel walks a list of items (block, first index); item t of
+// a launch is CTA t, and its threads take consecutive indices of that
+// block's index space (interior cells, flux positions or ghost cells), so
+// blocks of different sizes share one launch with equal work per CTA.
+#pragma once
+#include "bh_fixed_phys.cuh"
+
+namespace fx {
+namespace {   // internal linkage: every arithmetic variant compiles its own copy
+using namespace bhfx;
+
+constexpr int FX_TPB = BH_FX_CHUNK;
+
+struct Grid {
+    const bh_fx_block* blk;
+    const int32_t* nbr;
+    double *U, *U1, *Bf, *Bf1;
+    void *W, *F;
+    int64_t ncell;
+    double* dt;
+    int32_t* count;
+    int32_t* err;
+};
+inline Grid grid_of(const bh_fx_grid* g) {
+    return Grid{g->blocks, g->nbr, g->U, g->U1, g->Bf, g->Bf1, g->W, g->F, g->ncell, g->dt, g->count, g->err};
+}
+inline FxPar par_of(const bh_fx_params* p) {
+    FxPar q;
+    q.M = p->M; q.a = p->a; q.gamma = p->gamma;
+    q.rho_fl = p->rho_floor; q.u_fl = p->u_floor; q.sigma_max = p->sigma_max; q.W_max = p->W_max;
+    q.r_exc = p->r_exc; q.tol = p->tol; q.maxiter = p->maxiter; q.limiter = p->limiter;
+    return q;
+}
+
+__device__ inline int64_t bidx(const bh_fx_block& b, int i, int j, int k) {
+    const int S = b.n + 5;
+    return b.off + ((int64_t)(i + 2) * S + (j + 2)) * S + (k + 2);
+}
+__device__ inline int bstride_i(const bh_fx_block& b) { return (b.n + 5) * (b.n + 5); }
+__device__ inline int bstride_j(const bh_fx_block& b) { return b.n + 5; }
+
+// ---- positions ---------------------------------------------------------
+__device__ inline void cell_centre(const bh_fx_block& b, int i, int j, int k, double* x) {
+    x[0] = b.x0[0] + (i + 0.5) * b.dx;
+    x[1] = b.x0[1] + (j + 0.5) * b.dx;
+    x[2] = b.x0[2] + (k + 0.5) * b.dx;
+}
+
+template <typename T>
+__device__ inline T* arr(void* base, int64_t ncell, int v) { return (T*)base + (int64_t)v * ncell; }
+
+// ======================================================================
+// CFL reduction on the bit patterns of non-negative doubles
+// ======================================================================
+__device__ inline void atomic_min_pos(double* slot, double v) {
+    atomicMin((unsigned long long*)slot, (unsigned long long)__double_as_longlong(v));
+}
+__device__ inline void atomic_max_pos(double* slot, double v) {
+    atomicMax((unsigned long long*)slot, (unsigned long long)__double_as_longlong(v));
+}
+__global__ void k_fx_dt_init(double* dt) {
+    dt[0] = __longlong_as_double(0x7FF0000000000000LL);   // +inf
+}
+
+// ======================================================================
+// con2prim + floors + excision on every interior cell of the stage buffer
+// (U, Bf for stage 0; U1, Bf1 for stage 1); stage 0 also reduces the CFL
+// limit into dt[0]
+// ======================================================================
+template <typename WT>
+__global__ void __launch_bounds__(FX_TPB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage, int with_dt) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    double dtc = 1e300;
+    if (e < n * n * n) {
+        const int i = e / (n * n), j = (e / n) % n, k = e % n;
+        const int64_t c = bidx(B, i, j, k);
+        double* U = stage ? G.U1 : G.U;
+        const double* Bf = stage ? G.Bf1 : G.Bf;
+        const int64_t N = G.ncell;
+        double x[3];
+        cell_centre(B, i, j, k, x);
+        KS m;
+        ks_metric(P, x[0], x[1], x[2], m);
+        // cell field: mean of the two faces (the role of f2cB, transport.cpp:60-75)
+        const int si = bstride_i(B), sj = bstride_j(B);
+        double Bt[3] = {0.5 * (Bf[c] + Bf[c + si]), 0.5 * (Bf[N + c] + Bf[N + c + sj]),
+                        0.5 * (Bf[2 * N + c] + Bf[2 * N + c + 1])};
+        double isg = 1.0 / m.sqrtgam;
+        double Bc[3] = {Bt[0] * isg, Bt[1] * isg, Bt[2] * isg};
+        double u[8], wo[8], w[8];
+        for (int v = 0; v < 5; v++) u[v] = U[v * N + c];
+        WT* W = (WT*)G.W;
+        for (int v = 0; v < 5; v++) wo[v] = (double)W[v * N + c];
+        int iters = 0;
+        int st = con2prim(P, m, u, Bc, wo, w, iters);
+        int rewrite = 0;
+        if (st != 0) {
+            // keep the previous primitives with the new field
+            for (int v = 0; v < 5; v++) w[v] = wo[v];
+            for (int d = 0; d < 3; d++) w[P_B + d] = Bc[d];
+            atomicAdd(&G.count[0], 1);
+            rewrite = 1;
+        }
+        if (apply_floors(P, m, w)) {
+            rewrite = 1;
+            atomicAdd(&G.count[1], 1);
+        }
+        if (rewrite) {
+            KSm<double> mm;
+            ks_cast(m, mm);
+            Derived<double> d;
+            derive(mm, P.gamma, w, d);
+            prim2cons(mm, P.gamma, w, d, u);
+            for (int v = 0; v < 5; v++) U[v * N + c] = u[v];
+        }
+        for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
+        for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];
+        if (with_dt) {
+            double dx[3] = {B.dx, B.dx, B.dx};
+            dtc = cell_dt(P, m, w, dx);
+        }
+    }
+    if (with_dt) {
+        for (int o = 16; o > 0; o >>= 1) dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+        if ((threadIdx.x & 31) == 0 && dtc < 1e300) atomic_min_pos(G.dt, dtc);
+    }
+}
+
+// ======================================================================
+// ghost fill: cells of the two ghost layers (edges and corners included)
+// take the primitives of the cell they image -- in a neighbour block
+// (same size and level) or, across the outer boundary, the nearest
+// interior cell (outflow: copy, the role of gh_bndy, grid.cpp:494-522) --
+// and the face field of their faces outside the block's own range.
+// ======================================================================
+__device__ inline int shell_decode(int n, int e, int& i, int& j, int& k) {
+    const int m = n + 4;
+    const int s1 = 4 * m * m, s2 = 4 * n * m, s3 = 4 * n * n;
+    if (e < s1) {   // i in {-2,-1,n,n+1}, j,k in [-2, n+1]
+        int q = e / (m * m), r = e % (m * m);
+        i = q < 2 ? q - 2 : n + q - 2; j = r / m - 2; k = r % m - 2;
+        return 1;
+    }
+    e -= s1;
+    if (e < s2) {   // i in [0,n), j in {-2,-1,n,n+1}, k in [-2, n+1]
+        int q = e / (n * m), r = e % (n * m);
+        i = r / m; k = r % m - 2;
+        j = q < 2 ? q - 2 : n + q - 2;
+        return 1;
+    }
+    e -= s2;
+    if (e < s3) {   // i, j in [0,n), k in {-2,-1,n,n+1}
+        int q = e / (n * n), r = e % (n * n);
+        i = r / n; j = r % n;
+        k = q < 2 ? q - 2 : n + q - 2;
+        return 1;
+    }
+    return 0;
+}
+
+// the source of ghost position (i, j, k) (cell, or face of normal fdim
+// when fdim >= 0): block and in-block coordinates
+__device__ inline int ghost_source(const Grid& G, int b, int n, int fdim, int& i, int& j, int& k) {
+    int c[3] = {i, j, k};
+    int o[3];
+    const int32_t* nb = G.nbr + (int64_t)b * 27;
+    for (int d = 0; d < 3; d++) {
+        int hi = (d == fdim) ? n : n - 1;   // a face's normal index runs to n
+        o[d] = c[d] < 0 ? -1 : (c[d] > hi ? 1 : 0);
+        if (o[d] != 0) {
+            int face_nb = nb[(d == 0 ? (o[d] + 1) * 9 + 4 : d == 1 ? 9 + (o[d] + 1) * 3 + 1 : 12 + o[d] + 1)];
+            if (face_nb < 0) {   // outer boundary: outflow
+                c[d] = c[d] < 0 ? 0 : hi;
+                o[d] = 0;
+            }
+        }
+    }
+    int src = nb[(o[0] + 1) * 9 + (o[1] + 1) * 3 + (o[2] + 1)];
+    if (src < 0) src = b;
+    i = c[0] - o[0] * n; j = c[1] - o[1] * n; k = c[2] - o[2] * n;
+    return src;
+}
+
+template <typename WT>
+__global__ void __launch_bounds__(FX_TPB) k_fx_ghost(Grid G, const int32_t* items, int stage) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    int i, j, k;
+    if (!shell_decode(n, e, i, j, k)) return;
+    const int64_t N = G.ncell;
+    WT* W = (WT*)G.W;
+    double* Bf = stage ? G.Bf1 : G.Bf;
+    const int64_t c = bidx(B, i, j, k);
+    {
+        int si = i, sj = j, sk = k;
+        int s = ghost_source(G, b, n, -1, si, sj, sk);
+        const int64_t sc = bidx(G.blk[s], si, sj, sk);
+        for (int v = 0; v < 8; v++) W[v * N + c] = W[v * N + sc];
+    }
+    // the lower faces of this ghost cell that the flux kernel reads: normal
+    // index 0..n, transverse index -1..n, outside the block's own faces
+    // (transverse 0..n-1)
+    for (int d = 0; d < 3; d++) {
+        int cc[3] = {i, j, k};
+        if (cc[d] < 0 || cc[d] > n) continue;
+        bool need = true;
+        for (int q = 0; q < 3; q++)
+            if (q != d && (cc[q] < -1 || cc[q] > n)) need = false;
+        if (!need) continue;
+        int si = i, sj = j, sk = k;
+        int s = ghost_source(G, b, n, d, si, sj, sk);
+        Bf[d * N + c] = Bf[d * N + bidx(G.blk[s], si, sj, sk)];
+    }
+}
+
+// ======================================================================
+// face fluxes: one thread per position (i, j, k) in [-1, n]^3 computes the
+// HLL flux at the lower x-, y- and z-face of that position where the face
+// is needed: normal index 0..n and transverse index -1..n (the transverse
+// layer feeds the EMFs of the block's boundary edges)
+// ======================================================================
+template <typename RT, typename WT, typename FT>
+__device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_block& B, int i, int j, int k, int d,
+                                 const double* Bfs) {
+    const int64_t N = G.ncell;
+    const int64_t c = bidx(B, i, j, k);
+    const int st = d == 0 ? bstride_i(B) : (d == 1 ? bstride_j(B) : 1);
+    const WT* W = (const WT*)G.W;
+    double x[3];
+    cell_centre(B, i, j, k, x);
+    x[d] -= 0.5 * B.dx;
+    KS mk;
+    ks_metric(P, x[0], x[1], x[2], mk);
+    KSm<RT> m;
+    ks_cast(mk, m);
+    RT wL[8], wR[8];
+    for (int v = 0; v < 8; v++) {
+        if (v == P_B + d) continue;
+        RT a = RT(W[v * N + c - 2 * st]), bb = RT(W[v * N + c - st]);
+        RT cc = RT(W[v * N + c]), dd = RT(W[v * N + c + st]);
+        plm_face(a, bb, cc, dd, P.limiter, wL[v], wR[v]);
+    }
+    // (the limiters keep every face value between its two cells' values, so
+    // face densities and pressures stay positive)
+    RT Bn = RT(Bfs[d * N + c] / mk.sqrtgam);
+    wL[P_B + d] = Bn;
+    wR[P_B + d] = Bn;
+    RT F[8];
+    hll_face(m, RT(P.gamma), d, wL, wR, F);
+    FT* Fo = (FT*)G.F;
+    for (int v = 0; v < 8; v++) Fo[((int64_t)d * 8 + v) * N + c] = (FT)F[v];
+}
+
+template <typename RT, typename WT, typename FT>
+__global__ void __launch_bounds__(FX_TPB) k_fx_flux(FxPar P, Grid G, const int32_t* items, int stage) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n, m = n + 2;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    if (e >= m * m * m) return;
+    const int i = e / (m * m) - 1, j = (e / m) % m - 1, k = e % m - 1;
+    const double* Bfs = stage ? G.Bf1 : G.Bf;
+    if (i >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 0, Bfs);
+    if (j >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 1, Bfs);
+    if (k >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 2, Bfs);
+}
+
+// ======================================================================
+// update: flux divergence + geometric source + RK2 (Heun) combine of the
+// conserved state; constrained transport of the face field with edge EMFs
+// averaged from the face fluxes (emfcomp's stencil, transport.cpp:11-36)
+// and the Heun average of the two stages (stage 0: U1 = U + dt L(U),
+// Bf1 = Bf - dt curl E; stage 1: U = (U + U1 + dt L(U1)) / 2, Bf = (Bf +
+// Bf1 - dt curl E) / 2)
+// ======================================================================
+template <typename FT>
+__device__ inline double fget(const Grid& G, int d, int v, int64_t c) {
+    return (double)((const FT*)G.F)[((int64_t)d * 8 + v) * G.ncell + c];
+}
+// EMF components at the edges indexed like cell c
+template <typename FT>
+__device__ inline double emf_x(const Grid& G, int64_t c, int sj, int sk) {   // (i, j-1/2, k-1/2)
+    return 0.25 * (fget<FT>(G, 2, C_B + 1, c) + fget<FT>(G, 2, C_B + 1, c - sj) - fget<FT>(G, 1, C_B + 2, c) -
+                   fget<FT>(G, 1, C_B + 2, c - sk));
+}
+template <typename FT>
+__device__ inline double emf_y(const Grid& G, int64_t c, int si, int sk) {   // (i-1/2, j, k-1/2)
+    return 0.25 * (fget<FT>(G, 0, C_B + 2, c) + fget<FT>(G, 0, C_B + 2, c - sk) - fget<FT>(G, 2, C_B + 0, c) -
+                   fget<FT>(G, 2, C_B + 0, c - si));
+}
+template <typename FT>
+__device__ inline double emf_z(const Grid& G, int64_t c, int si, int sj) {   // (i-1/2, j-1/2, k)
+    return 0.25 * (fget<FT>(G, 1, C_B + 0, c) + fget<FT>(G, 1, C_B + 0, c - si) - fget<FT>(G, 0, C_B + 1, c) -
+                   fget<FT>(G, 0, C_B + 1, c - sj));
+}
+template <typename FT>
+__device__ inline void face_update(const Grid& G, int d, int64_t c, int si, int sj, int sk, double idx, double dt,
+                                   int stage) {
+    const int64_t N = G.ncell;
+    double curl;
+    if (d == 0)
+        curl = (emf_z<FT>(G, c + sj, si, sj) - emf_z<FT>(G, c, si, sj)) * idx -
+               (emf_y<FT>(G, c + sk, si, sk) - emf_y<FT>(G, c, si, sk)) * idx;
+    else if (d == 1)
+        curl = (emf_x<FT>(G, c + sk, sj, sk) - emf_x<FT>(G, c, sj, sk)) * idx -
+               (emf_z<FT>(G, c + si, si, sj) - emf_z<FT>(G, c, si, sj)) * idx;
+    else
+        curl = (emf_y<FT>(G, c + si, si, sk) - emf_y<FT>(G, c, si, sk)) * idx -
+               (emf_x<FT>(G, c + sj, sj, sk) - emf_x<FT>(G, c, sj, sk)) * idx;
+    if (stage == 0)
+        G.Bf1[d * N + c] = G.Bf[d * N + c] - dt * curl;
+    else
+        G.Bf[d * N + c] = 0.5 * (G.Bf[d * N + c] + G.Bf1[d * N + c] - dt * curl);
+}
+
+template <typename RT, typename WT, typename FT>
+__global__ void __launch_bounds__(FX_TPB) k_fx_update(FxPar P, Grid G, const int32_t* items, int stage,
+                                                      double cfl) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    if (e >= n * n * n) return;
+    const int i = e / (n * n), j = (e / n) % n, k = e % n;
+    const int64_t N = G.ncell;
+    const int64_t c = bidx(B, i, j, k);
+    const int si = bstride_i(B), sj = bstride_j(B), sk = 1;
+    const double dt = cfl * G.dt[0];
+    if (stage == 0 && blockIdx.x == 0 && threadIdx.x == 0) G.dt[1] = dt;
+    const double idx = 1.0 / B.dx;
+    // source at the cell centre from the stage's primitives
+    double x[3];
+    cell_centre(B, i, j, k, x);
+    KS mk;
+    ks_metric(P, x[0], x[1], x[2], mk);
+    KSD dk;
+    ks_deriv(P, x[0], x[1], x[2], mk, dk);
+    const WT* W = (const WT*)G.W;
+    RT w[8];
+    for (int v = 0; v < 8; v++) w[v] = RT(W[v * N + c]);
+    RT S[8];
+    source<RT>(mk, dk, RT(P.gamma), w, S);
+    for (int v = 0; v < 5; v++) {
+        double div = (fget<FT>(G, 0, v, c + si) - fget<FT>(G, 0, v, c)) * idx +
+                     (fget<FT>(G, 1, v, c + sj) - fget<FT>(G, 1, v, c)) * idx +
+                     (fget<FT>(G, 2, v, c + sk) - fget<FT>(G, 2, v, c)) * idx;
+        double L = (double)S[v] - div;
+        if (stage == 0)
+            G.U1[v * N + c] = G.U[v * N + c] + dt * L;
+        else
+            G.U[v * N + c] = 0.5 * (G.U[v * N + c] + G.U1[v * N + c] + dt * L);
+    }
+    // face field: this cell's three lower faces, and the upper boundary faces
+    face_update<FT>(G, 0, c, si, sj, sk, idx, dt, stage);
+    face_update<FT>(G, 1, c, si, sj, sk, idx, dt, stage);
+    face_update<FT>(G, 2, c, si, sj, sk, idx, dt, stage);
+    if (i == n - 1) face_update<FT>(G, 0, c + si, si, sj, sk, idx, dt, stage);
+    if (j == n - 1) face_update<FT>(G, 1, c + sj, si, sj, sk, idx, dt, stage);
+    if (k == n - 1) face_update<FT>(G, 2, c + sk, si, sj, sk, idx, dt, stage);
+}
+
+// ======================================================================
+// divergence of the face field: per interior cell |div B| dx / max(|B~|)
+// of its six faces; max over each block into out[b] (non-negative doubles)
+// ======================================================================
+__global__ void __launch_bounds__(FX_TPB) k_fx_divb(Grid G, const int32_t* items, double* out) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    double v = 0.0;
+    if (e < n * n * n) {
+        const int i = e / (n * n), j = (e / n) % n, k = e % n;
+        const int64_t N = G.ncell, c = bidx(B, i, j, k);
+        const int si = bstride_i(B), sj = bstride_j(B);
+        double f[6] = {G.Bf[c], G.Bf[c + si], G.Bf[N + c], G.Bf[N + c + sj], G.Bf[2 * N + c], G.Bf[2 * N + c + 1]};
+        double div = (f[1] - f[0]) + (f[3] - f[2]) + (f[5] - f[4]);
+        double mx = 0.0;
+        for (int q = 0; q < 6; q++) mx = fmax(mx, fabs(f[q]));
+        v = mx > 0.0 ? fabs(div) / mx : 0.0;
+    }
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0 && v > 0.0) atomic_max_pos(out + b, v);
+}
+
+
+// ======================================================================
+// initial data (bh_fx_torus_init)
+// ======================================================================
+struct TorusK {
+    FMTorus t;
+    double noise;
+    uint64_t seed;
+};
+__global__ void __launch_bounds__(FX_TPB) k_fxi_rho(Grid G, const int32_t* items, TorusK T, double* scratch) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    double rho = 0.0;
+    if (e < n * n * n) {
+        const int i = e / (n * n), j = (e / n) % n, k = e % n;
+        double x[3];
+        cell_centre(B, i, j, k, x);
+        rho = fm_rho(T.t, x[0], x[1], x[2], nullptr);
+    }
+    for (int o = 16; o > 0; o >>= 1) rho = fmax(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+    if ((threadIdx.x & 31) == 0 && rho > 0.0) atomic_max_pos(scratch, rho);
+}
+// primitives of the interior cells (no field yet); max p_gas of the torus
+template <typename WT>
+__global__ void __launch_bounds__(FX_TPB) k_fxi_prims(FxPar P, Grid G, const int32_t* items, TorusK T,
+                                                      double* scratch) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    double pg = 0.0;
+    if (e < n * n * n) {
+        const int i = e / (n * n), j = (e / n) % n, k = e % n;
+        const int64_t N = G.ncell, c = bidx(B, i, j, k);
+        double x[3];
+        cell_centre(B, i, j, k, x);
+        KS m;
+        ks_metric(P, x[0], x[1], x[2], m);
+        const double rmax = scratch[0];
+        double rho = fm_rho(T.t, x[0], x[1], x[2], nullptr);
+        double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (rho > 0.0 && rmax > 0.0) {
+            double p = T.t.kappa * pow(rho, T.t.gamma) / rmax;
+            double u = hash_uniform(T.seed, cell_key(B.x0, B.dx, i, j, k));
+            p = p * (1.0 + T.noise * (2.0 * u - 1.0));
+            double ut, ux, uy;
+            fm_velocity(T.t, x[0], x[1], x[2], ut, ux, uy);
+            // ut^i = u^i + u^t beta^i
+            w[P_RHO] = rho / rmax;
+            w[P_PRS] = p;
+            w[P_UT] = ux + ut * m.beta[0];
+            w[P_UT + 1] = uy + ut * m.beta[1];
+            w[P_UT + 2] = ut * m.beta[2];
+        } else {
+            floor_state(P, m.r, w[P_RHO], w[P_PRS]);
+        }
+        apply_floors(P, m, w);
+        if (rho > 0.0 && rmax > 0.0) pg = w[P_PRS];
+        WT* W = (WT*)G.W;
+        for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];
+    }
+    for (int o = 16; o > 0; o >>= 1) pg = fmax(pg, __shfl_xor_sync(0xffffffffu, pg, o));
+    if ((threadIdx.x & 31) == 0 && pg > 0.0) atomic_max_pos(scratch + 1, pg);
+}
+// A_phi = max(rho / rho_max - 0.2, 0) at a point, as Cartesian (A_x, A_y)
+__device__ inline void apot(const TorusK& T, double rmax, double x, double y, double z, double& ax, double& ay) {
+    double rho = fm_rho(T.t, x, y, z, nullptr);
+    double A = rho / rmax - 0.2;
+    ax = ay = 0.0;
+    if (A > 0.0) {
+        double iw = 1.0 / (x * x + y * y);
+        ax = -A * y * iw;
+        ay = A * x * iw;
+    }
+}
+// face field = curl of the edge potential (A_z = 0), unscaled
+__global__ void __launch_bounds__(FX_TPB) k_fxi_faces(Grid G, const int32_t* items, TorusK T, double* scratch) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n, m = n + 2;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    if (e >= m * m * m) return;
+    const int i = e / (m * m) - 1, j = (e / m) % m - 1, k = e % m - 1;
+    const int64_t N = G.ncell, c = bidx(B, i, j, k);
+    const double rmax = scratch[0], h = B.dx;
+    const double X = B.x0[0], Y = B.x0[1], Z = B.x0[2];
+    double ax0, ay0, ax1, ay1, d0, d1;
+    if (i >= 0) {   // x-face (i-1/2, j, k): -(A_y(k+1/2) - A_y(k-1/2)) / dz, y-edges at (i-1/2, j, k -+ 1/2)
+        apot(T, rmax, X + i * h, Y + (j + 0.5) * h, Z + k * h, d0, ay0);
+        apot(T, rmax, X + i * h, Y + (j + 0.5) * h, Z + (k + 1) * h, d1, ay1);
+        G.Bf[c] = -(ay1 - ay0) / h;
+    }
+    if (j >= 0) {   // y-face (i, j-1/2, k): (A_x(k+1/2) - A_x(k-1/2)) / dz, x-edges at (i, j-1/2, k -+ 1/2)
+        apot(T, rmax, X + (i + 0.5) * h, Y + j * h, Z + k * h, ax0, d0);
+        apot(T, rmax, X + (i + 0.5) * h, Y + j * h, Z + (k + 1) * h, ax1, d1);
+        G.Bf[N + c] = (ax1 - ax0) / h;
+    }
+    if (k >= 0) {   // z-face (i, j, k-1/2): dA_y/dx - dA_x/dy
+        double ayl, ayr, axl, axr;
+        apot(T, rmax, X + i * h, Y + (j + 0.5) * h, Z + k * h, d0, ayl);
+        apot(T, rmax, X + (i + 1) * h, Y + (j + 0.5) * h, Z + k * h, d1, ayr);
+        apot(T, rmax, X + (i + 0.5) * h, Y + j * h, Z + k * h, axl, d0);
+        apot(T, rmax, X + (i + 0.5) * h, Y + (j + 1) * h, Z + k * h, axr, d1);
+        G.Bf[2 * N + c] = (ayr - ayl) / h - (axr - axl) / h;
+    }
+}
+// max b^2 / 2 of the interior cells with the unscaled field
+template <typename WT>
+__global__ void __launch_bounds__(FX_TPB) k_fxi_pmag(FxPar P, Grid G, const int32_t* items, double* scratch) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    double pm = 0.0;
+    if (e < n * n * n) {
+        const int i = e / (n * n), j = (e / n) % n, k = e % n;
+        const int64_t N = G.ncell, c = bidx(B, i, j, k);
+        const int si = bstride_i(B), sj = bstride_j(B);
+        double x[3];
+        cell_centre(B, i, j, k, x);
+        KS mk;
+        ks_metric(P, x[0], x[1], x[2], mk);
+        double isg = 1.0 / mk.sqrtgam;
+        const WT* W = (const WT*)G.W;
+        double w[8];
+        for (int v = 0; v < 5; v++) w[v] = (double)W[v * N + c];
+        w[P_B] = 0.5 * (G.Bf[c] + G.Bf[c + si]) * isg;
+        w[P_B + 1] = 0.5 * (G.Bf[N + c] + G.Bf[N + c + sj]) * isg;
+        w[P_B + 2] = 0.5 * (G.Bf[2 * N + c] + G.Bf[2 * N + c + 1]) * isg;
+        KSm<double> m;
+        ks_cast(mk, m);
+        Derived<double> d;
+        derive(m, P.gamma, w, d);
+        pm = 0.5 * d.b2;
+    }
+    for (int o = 16; o > 0; o >>= 1) pm = fmax(pm, __shfl_xor_sync(0xffffffffu, pm, o));
+    if ((threadIdx.x & 31) == 0 && pm > 0.0) atomic_max_pos(scratch + 2, pm);
+}
+__device__ inline double field_scale(const double* scratch, double beta) {
+    return (scratch[2] > 0.0 && beta > 0.0) ? sqrt(scratch[1] / (beta * scratch[2])) : 0.0;
+}
+__global__ void __launch_bounds__(FX_TPB) k_fxi_scale(Grid G, const int32_t* items, double beta, double* scratch) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n, m = n + 2;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    const double s = field_scale(scratch, beta);
+    if (blockIdx.x == 0 && threadIdx.x == 0) scratch[3] = s;
+    if (e >= m * m * m) return;
+    const int i = e / (m * m) - 1, j = (e / m) % m - 1, k = e % m - 1;
+    const int64_t N = G.ncell, c = bidx(B, i, j, k);
+    if (i >= 0) G.Bf[c] *= s;
+    if (j >= 0) G.Bf[N + c] *= s;
+    if (k >= 0) G.Bf[2 * N + c] *= s;
+}
+// cell field and conserved state of the interior cells
+template <typename WT>
+__global__ void __launch_bounds__(FX_TPB) k_fxi_cons(FxPar P, Grid G, const int32_t* items) {
+    const int32_t b = items[2 * blockIdx.x];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n;
+    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
+    if (e >= n * n * n) return;
+    const int i = e / (n * n), j = (e / n) % n, k = e % n;
+    const int64_t N = G.ncell, c = bidx(B, i, j, k);
+    const int si = bstride_i(B), sj = bstride_j(B);
+    double x[3];
+    cell_centre(B, i, j, k, x);
+    KS mk;
+    ks_metric(P, x[0], x[1], x[2], mk);
+    double Bt[3] = {0.5 * (G.Bf[c] + G.Bf[c + si]), 0.5 * (G.Bf[N + c] + G.Bf[N + c + sj]),
+                    0.5 * (G.Bf[2 * N + c] + G.Bf[2 * N + c + 1])};
+    double isg = 1.0 / mk.sqrtgam;
+    WT* W = (WT*)G.W;
+    double w[8], u[8];
+    for (int v = 0; v < 5; v++) w[v] = (double)W[v * N + c];
+    for (int d = 0; d < 3; d++) w[P_B + d] = Bt[d] * isg;
+    KSm<double> m;
+    ks_cast(mk, m);
+    Derived<double> d;
+    derive(m, P.gamma, w, d);
+    prim2cons(m, P.gamma, w, d, u);
+    for (int v = 0; v < 5; v++) G.U[v * N + c] = u[v];
+    for (int q = 0; q < 3; q++) G.U[(5 + q) * N + c] = Bt[q];
+    for (int v = 5; v < 8; v++) W[v * N + c] = (WT)w[v];
+}
+
+}  // namespace
+}  // namespace fx
+
+// ---- launch sequences of this variant (bh_api.h) -------------------------
+namespace BH_VARIANT {
+namespace {
+using FRT = BH_REAL;
+inline cudaStream_t fxs(void* s) { return (cudaStream_t)s; }
+inline int fx_launched() { return cudaGetLastError() == cudaSuccess ? BH_OK : BH_ECUDA; }
+}  // namespace
+
+int fx_prims(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t with_dt, void* s) {
+    fx::FxPar p = fx::par_of(P);
+    fx::Grid G = fx::grid_of(g);
+    if (with_dt) fx::k_fx_dt_init<<<1, 1, 0, fxs(s)>>>(g->dt);
+    if (g->nitem_cell)
+        fx::k_fx_c2p<FRT><<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt);
+    return fx_launched();
+}
+int fx_ghosts(const bh_fx_params*, const bh_fx_grid* g, int32_t stage, void* s) {
+    fx::Grid G = fx::grid_of(g);
+    if (g->nitem_ghost) fx::k_fx_ghost<FRT><<<g->nitem_ghost, fx::FX_TPB, 0, fxs(s)>>>(G, g->items_ghost, stage);
+    return fx_launched();
+}
+int fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
+    fx::FxPar p = fx::par_of(P);
+    fx::Grid G = fx::grid_of(g);
+    if (g->nitem_pos)
+        fx::k_fx_flux<FRT, FRT, FRT><<<g->nitem_pos, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_pos, stage);
+    return fx_launched();
+}
+int fx_update(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
+    fx::FxPar p = fx::par_of(P);
+    fx::Grid G = fx::grid_of(g);
+    if (g->nitem_cell)
+        fx::k_fx_update<FRT, FRT, FRT><<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, P->cfl);
+    return fx_launched();
+}
+int fx_step(const bh_fx_params* P, const bh_fx_grid* g, void* s) {
+    for (int stage = 0; stage < 2; stage++) {
+        int rc = fx_prims(P, g, stage, stage == 0, s);
+        if (!rc) rc = fx_ghosts(P, g, stage, s);
+        if (!rc) rc = fx_fluxes(P, g, stage, s);
+        if (!rc) rc = fx_update(P, g, stage, s);
+        if (rc) return rc;
+    }
+    return BH_OK;
+}
+int fx_divb(const bh_fx_grid* g, double* out, void* s) {
+    fx::Grid G = fx::grid_of(g);
+    if (cudaMemsetAsync(out, 0, sizeof(double) * g->nblock, fxs(s)) != cudaSuccess) return BH_ECUDA;
+    if (g->nitem_cell) fx::k_fx_divb<<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(G, g->items_cell, out);
+    return fx_launched();
+}
+int fx_torus_init(const bh_fx_params* P, const bh_fx_grid* g, const bh_fx_torus* T, double* scratch, double* out,
+                  void* s) {
+    fx::FxPar p = fx::par_of(P);
+    fx::Grid G = fx::grid_of(g);
+    fx::TorusK tk;
+    tk.t = bhfx::fm_torus(P->a, P->gamma, T->kappa, T->r_in, T->r_max);
+    tk.noise = T->noise;
+    tk.seed = T->seed;
+    cudaStream_t st = fxs(s);
+    if (cudaMemsetAsync(scratch, 0, 4 * sizeof(double), st) != cudaSuccess) return BH_ECUDA;
+    if (cudaMemsetAsync(g->Bf, 0, 3 * sizeof(double) * g->ncell, st) != cudaSuccess) return BH_ECUDA;
+    fx::k_fxi_rho<<<g->nitem_cell, fx::FX_TPB, 0, st>>>(G, g->items_cell, tk, scratch);
+    fx::k_fxi_prims<FRT><<<g->nitem_cell, fx::FX_TPB, 0, st>>>(p, G, g->items_cell, tk, scratch);
+    fx::k_fxi_faces<<<g->nitem_pos, fx::FX_TPB, 0, st>>>(G, g->items_pos, tk, scratch);
+    fx::k_fxi_pmag<FRT><<<g->nitem_cell, fx::FX_TPB, 0, st>>>(p, G, g->items_cell, scratch);
+    fx::k_fxi_scale<<<g->nitem_pos, fx::FX_TPB, 0, st>>>(G, g->items_pos, T->beta, scratch);
+    fx::k_fxi_cons<FRT><<<g->nitem_cell, fx::FX_TPB, 0, st>>>(p, G, g->items_cell);
+    int rc = fx_launched();
+    if (rc) return rc;
+    if (out) {
+        double h[4];
+        if (cudaMemcpyAsync(h, scratch, sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess) return BH_ECUDA;
+        if (cudaStreamSynchronize(st) != cudaSuccess) return BH_ECUDA;
+        out[0] = tk.t.ell;
+        out[1] = h[0];
+        out[2] = h[3];
+        out[3] = h[3] > 0.0 ? h[1] / (h[3] * h[3] * h[2]) : 0.0;
+    }
+    return BH_OK;
+}
+}  // namespace BH_VARIANT

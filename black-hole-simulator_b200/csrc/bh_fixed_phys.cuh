@@ -1,0 +1,642 @@
+// bh_fixed_phys.cuh -- device physics of the corrected ("fixed") scheme:
+// textbook Valencia GRMHD in Cartesian Kerr-Schild coordinates.
+//
+// The reference's scheme (src/fluid) cannot carry a Kerr torus through one
+// step: its EOS throws in the first stage (physics/thermo.cpp:10-11 reached
+// from conserved.cpp:205), its Newton derivative is wrong
+// (conserved.cpp:114), its Brent fallback never updates fa/fb
+// (conserved.cpp:261,272-282), its y and z faces call hlld(..., dim = 0)
+// (grid.cpp:298,322), its metric is the (t,r,theta,phi) form applied to
+// Cartesian vectors (spacetime.cpp:20-54), and its face field takes the full
+// dt in both RK stages (transport.cpp:38-58, integrator.cpp:233-234).  This
+// header keeps the reference's structure -- metric at cell and face centres,
+// ptoc, a Newton con2prim, PLM face states, a two-wave HLL flux (the
+// reference's own fallback, hlld.cpp:124-137), edge EMFs averaged from face
+// fluxes (transport.cpp:11-36), the RK2 combine (integrator.cpp:238-259) --
+// with each of those defects corrected:
+//
+//   metric    Kerr-Schild in Cartesian form, g = eta + 2 H l (x) l with
+//             H = M r^3 / (r^4 + a^2 z^2) and the null covector
+//             l = (1, (r x + a y)/(r^2+a^2), (r y - a x)/(r^2+a^2), z/r):
+//             alpha = (1+2H)^-1/2, beta^i = 2H l_i/(1+2H),
+//             gamma_ij = delta_ij + 2H l_i l_j, sqrt(gamma) = (1+2H)^1/2,
+//             sqrt(-g) = 1; its first derivatives are analytic.
+//   con2prim  Newton on Z = rho h W^2 with the exact derivative of the
+//             energy residual (Noble et al. 2006, the "1D" scheme), raised
+//             indices with the full inverse spatial metric.
+//   fluxes    Valencia fluxes in the face's own normal direction; wave
+//             speeds from the fast magnetosonic estimate in the GR
+//             eigenvalue formula (Banyuls et al. 1997); HLL (Harten, Lax,
+//             van Leer; Einfeldt's speed bounds).
+//   sources   S(S_j) = 1/2 T^{mu nu} d_j g_{mu nu} and
+//             S(tau) = alpha (T^{mu 0} d_mu ln alpha - T^{mu nu} Gamma^0_{mu nu}),
+//             both evaluated from the analytic metric derivatives.
+//   CT        face B advanced by a Heun average of the two stages' EMFs.
+//
+// Every operation of the time step is +, -, *, / or sqrt, so a build with
+// --fmad=false and IEEE division equals a C restatement with the same
+// operation order bit for bit.  RT is the arithmetic type of the face work
+// (reconstruction, fluxes, sources): double, or float in the mixed variant;
+// the metric is always evaluated in double.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#ifndef BH_HD
+#define BH_HD __host__ __device__
+#endif
+
+namespace bhfx {
+
+// primitive slots: rho, p, ut^x, ut^y, ut^z (ut^i = W v^i, the spatial
+// velocity of the fluid measured by normal observers times its Lorentz
+// factor), B^x, B^y, B^z (Eulerian field, not densitised)
+enum { P_RHO = 0, P_PRS = 1, P_UT = 2, P_B = 5 };
+// conserved slots (the reference's cons order, cons.hpp:14-60), densitised
+// by sqrt(gamma): D, S_x, S_y, S_z, tau, B^x, B^y, B^z
+enum { C_D = 0, C_S = 1, C_TAU = 4, C_B = 5 };
+
+struct FxPar {
+    double M, a, gamma;
+    double rho_fl, u_fl;      // floors rho >= rho_fl r^-3/2, u = p/(Gamma-1) >= u_fl r^-5/2
+    double sigma_max, W_max;  // b^2/rho <= sigma_max, Lorentz factor <= W_max
+    double r_exc;             // cells with r < r_exc are reset to the floor state
+    double tol;               // con2prim: |dZ| <= tol Z
+    int maxiter, limiter;
+};
+
+template <typename T>
+BH_HD inline T fmin_(T a, T b) { return b < a ? b : a; }
+template <typename T>
+BH_HD inline T fmax_(T a, T b) { return a < b ? b : a; }
+template <typename T>
+BH_HD inline T fabs_(T a) { return a < T(0) ? -a : a; }
+BH_HD inline double sqrt_(double x) { return sqrt(x); }
+BH_HD inline float sqrt_(float x) { return sqrtf(x); }
+
+// ======================================================================
+// metric
+// ======================================================================
+// Kerr-Schild radius of a Cartesian point: the positive root of
+// r^4 - (R^2 - a^2) r^2 - a^2 z^2 = 0
+BH_HD inline double ks_r2(double a, double x, double y, double z) {
+    double a2 = a * a;
+    double d = x * x + y * y + z * z - a2;
+    return 0.5 * (d + sqrt(d * d + 4.0 * a2 * z * z));
+}
+
+struct KS {
+    double H, l[3];            // H and the spatial part of l_mu (l_0 = 1)
+    double alpha, sqrtgam;     // lapse, sqrt(det gamma)
+    double beta[3];            // shift beta^i
+    double g[6], gi[6];        // gamma_ij and gamma^ij: xx, xy, xz, yy, yz, zz
+    double r;
+};
+BH_HD inline int sym(int i, int j) {   // index into the 6-entry symmetric storage
+    int a = i < j ? i : j, b = i < j ? j : i;
+    return a == 0 ? b : (a == 1 ? 2 + b : 5);
+}
+
+BH_HD inline void ks_metric(const FxPar& P, double x, double y, double z, KS& m) {
+    const double a = P.a, a2 = a * a;
+    double r2 = ks_r2(a, x, y, z);
+    double r = sqrt(r2);
+    double q = r2 * r2 + a2 * z * z;
+    // on the disc z = 0, x^2 + y^2 <= a^2 (r = 0) the metric is flat
+    double H = q > 0.0 ? P.M * r * r2 / q : 0.0;
+    double ir2a = 1.0 / (r2 + a2);
+    m.r = r;
+    m.H = H;
+    m.l[0] = (r * x + a * y) * ir2a;
+    m.l[1] = (r * y - a * x) * ir2a;
+    m.l[2] = r > 0.0 ? z / r : 0.0;
+    double h2 = 2.0 * H, f = 1.0 + h2;
+    m.sqrtgam = sqrt(f);
+    m.alpha = 1.0 / m.sqrtgam;
+    double hf = h2 / f;
+    for (int i = 0; i < 3; i++) m.beta[i] = hf * m.l[i];
+    for (int i = 0; i < 3; i++)
+        for (int j = i; j < 3; j++) {
+            double ll = m.l[i] * m.l[j];
+            m.g[sym(i, j)] = (i == j ? 1.0 : 0.0) + h2 * ll;
+            m.gi[sym(i, j)] = (i == j ? 1.0 : 0.0) - hf * ll;
+        }
+}
+
+// first derivatives: dH[k] = d_k H, dl[k][i] = d_k l_i (d_k l_0 = 0)
+struct KSD {
+    double dH[3], dl[3][3];
+};
+BH_HD inline void ks_deriv(const FxPar& P, double x, double y, double z, const KS& m, KSD& d) {
+    const double a = P.a, a2 = a * a, r = m.r, r2 = r * r;
+    double q = r2 * r2 + a2 * z * z;
+    if (!(q > 0.0) || !(r > 0.0)) {
+        for (int k = 0; k < 3; k++) {
+            d.dH[k] = 0.0;
+            for (int i = 0; i < 3; i++) d.dl[k][i] = 0.0;
+        }
+        return;
+    }
+    double iq = 1.0 / q, r3 = r2 * r;
+    double dr[3] = {x * r3 * iq, y * r3 * iq, z * r * (r2 + a2) * iq};
+    double ir2a = 1.0 / (r2 + a2);
+    for (int k = 0; k < 3; k++) {
+        double dq = 4.0 * r3 * dr[k] + (k == 2 ? 2.0 * a2 * z : 0.0);
+        d.dH[k] = P.M * (3.0 * r2 * dr[k] * q - r3 * dq) * iq * iq;
+        double t = 2.0 * r * dr[k];
+        d.dl[k][0] = (dr[k] * x + (k == 0 ? r : 0.0) + (k == 1 ? a : 0.0) - m.l[0] * t) * ir2a;
+        d.dl[k][1] = (dr[k] * y + (k == 1 ? r : 0.0) - (k == 0 ? a : 0.0) - m.l[1] * t) * ir2a;
+        d.dl[k][2] = ((k == 2 ? 1.0 : 0.0) - m.l[2] * dr[k]) / r;
+    }
+}
+
+// the spatial metric at the arithmetic type of the face work
+template <typename RT>
+struct KSm {
+    RT alpha, sqrtgam, beta[3], g[6], gi[6];
+};
+template <typename RT>
+BH_HD inline void ks_cast(const KS& m, KSm<RT>& o) {
+    o.alpha = RT(m.alpha); o.sqrtgam = RT(m.sqrtgam);
+    for (int i = 0; i < 3; i++) o.beta[i] = RT(m.beta[i]);
+    for (int i = 0; i < 6; i++) { o.g[i] = RT(m.g[i]); o.gi[i] = RT(m.gi[i]); }
+}
+template <typename RT>
+BH_HD inline void lower(const RT* g, const RT* v, RT* o) {
+    o[0] = g[0] * v[0] + g[1] * v[1] + g[2] * v[2];
+    o[1] = g[1] * v[0] + g[3] * v[1] + g[4] * v[2];
+    o[2] = g[2] * v[0] + g[4] * v[1] + g[5] * v[2];
+}
+
+// ======================================================================
+// primitive -> conserved (the role of conserved::ptoc, conserved.cpp:17-73)
+// ======================================================================
+// Derived quantities of a primitive state at a point.
+template <typename RT>
+struct Derived {
+    RT W, v[3], vl[3], Bl[3], B2, Bv, b2, rhohW2, ptot;
+};
+template <typename RT>
+BH_HD inline void derive(const KSm<RT>& m, RT gamma, const RT* w, Derived<RT>& d) {
+    RT ut[3] = {w[P_UT], w[P_UT + 1], w[P_UT + 2]};
+    RT B[3] = {w[P_B], w[P_B + 1], w[P_B + 2]};
+    RT utl[3];
+    lower(m.g, ut, utl);
+    RT u2 = utl[0] * ut[0] + utl[1] * ut[1] + utl[2] * ut[2];
+    d.W = sqrt_(RT(1) + u2);
+    RT iW = RT(1) / d.W;
+    for (int i = 0; i < 3; i++) { d.v[i] = ut[i] * iW; d.vl[i] = utl[i] * iW; }
+    lower(m.g, B, d.Bl);
+    d.B2 = d.Bl[0] * B[0] + d.Bl[1] * B[1] + d.Bl[2] * B[2];
+    d.Bv = d.Bl[0] * d.v[0] + d.Bl[1] * d.v[1] + d.Bl[2] * d.v[2];
+    d.b2 = d.B2 * iW * iW + d.Bv * d.Bv;
+    RT rhoh = w[P_RHO] + gamma / (gamma - RT(1)) * w[P_PRS];
+    d.rhohW2 = rhoh * d.W * d.W;
+    d.ptot = w[P_PRS] + RT(0.5) * d.b2;
+}
+// densitised conserved state of primitives w (B slots: sqrt(gamma) B)
+template <typename RT>
+BH_HD inline void prim2cons(const KSm<RT>& m, RT gamma, const RT* w, const Derived<RT>& d, RT* u) {
+    const RT sg = m.sqrtgam;
+    RT v2 = RT(1) - RT(1) / (d.W * d.W);
+    u[C_D] = sg * w[P_RHO] * d.W;
+    RT e = d.rhohW2 + d.B2;
+    for (int i = 0; i < 3; i++) u[C_S + i] = sg * (e * d.vl[i] - d.Bv * d.Bl[i]);
+    RT E = d.rhohW2 - w[P_PRS] + RT(0.5) * d.B2 * (RT(1) + v2) - RT(0.5) * d.Bv * d.Bv;
+    u[C_TAU] = sg * E - u[C_D];
+    for (int i = 0; i < 3; i++) u[C_B + i] = sg * w[P_B + i];
+}
+
+// ======================================================================
+// fluxes in direction dd (Valencia, densitised: sqrt(-g) F^dd with
+// sqrt(-g) = alpha sqrt(gamma))
+// ======================================================================
+template <typename RT>
+BH_HD inline void phys_flux(const KSm<RT>& m, int dd, const RT* w, const Derived<RT>& d, const RT* u, RT* F) {
+    RT vt = m.alpha * d.v[dd] - m.beta[dd];       // coordinate transport velocity
+    RT ag = m.alpha * m.sqrtgam;
+    RT iW2 = RT(1) / (d.W * d.W);
+    RT Bd = w[P_B + dd];
+    F[C_D] = u[C_D] * vt;
+    for (int j = 0; j < 3; j++) {
+        RT bjB = (d.Bl[j] * iW2 + d.Bv * d.vl[j]) * Bd;   // b_j B^dd / W
+        F[C_S + j] = u[C_S + j] * vt + ag * ((j == dd ? d.ptot : RT(0)) - bjB);
+    }
+    F[C_TAU] = u[C_TAU] * vt + ag * (d.ptot * d.v[dd] - d.Bv * Bd);
+    for (int k = 0; k < 3; k++) {
+        RT vtk = m.alpha * d.v[k] - m.beta[k];
+        F[C_B + k] = k == dd ? RT(0) : m.sqrtgam * (w[P_B + k] * vt - Bd * vtk);
+    }
+}
+
+// fast magnetosonic signal speeds lambda-, lambda+ in direction dd
+template <typename RT>
+BH_HD inline void signal_speeds(const KSm<RT>& m, RT gamma, int dd, const RT* w, const Derived<RT>& d, RT& lm,
+                                RT& lp) {
+    RT rhoh = w[P_RHO] + gamma / (gamma - RT(1)) * w[P_PRS];
+    RT cs2 = gamma * w[P_PRS] / rhoh;
+    RT va2 = d.b2 / (rhoh + d.b2);
+    RT c2 = cs2 + va2 - cs2 * va2;
+    c2 = fmin_(fmax_(c2, RT(0)), RT(1));
+    RT v2 = RT(1) - RT(1) / (d.W * d.W);
+    RT vd = d.v[dd];
+    RT gdd = m.gi[dd == 0 ? 0 : (dd == 1 ? 3 : 5)];
+    RT den = RT(1) / (RT(1) - v2 * c2);
+    RT disc = (RT(1) - v2) * (gdd * (RT(1) - v2 * c2) - vd * vd * (RT(1) - c2));
+    RT rt = sqrt_(fmax_(c2 * disc, RT(0)));
+    RT base = vd * (RT(1) - c2);
+    lm = m.alpha * (base - rt) * den - m.beta[dd];
+    lp = m.alpha * (base + rt) * den - m.beta[dd];
+}
+
+// ======================================================================
+// PLM (reconfp's role, reconstruction.cpp:40-97): limited slopes
+// ======================================================================
+enum { FX_MINMOD = 0, FX_VANLEER = 1, FX_MC = 2 };
+template <typename RT>
+BH_HD inline RT lim_slope(RT dl, RT dr, int lim) {
+    if (dl * dr <= RT(0)) return RT(0);
+    if (lim == FX_VANLEER) return RT(2) * dl * dr / (dl + dr);
+    RT al = fabs_(dl), ar = fabs_(dr);
+    RT s = dl > RT(0) ? RT(1) : RT(-1);
+    if (lim == FX_MC) {
+        RT c = RT(0.5) * (al + ar);
+        return s * fmin_(c, RT(2) * fmin_(al, ar));
+    }
+    return s * fmin_(al, ar);
+}
+// face values at i-1/2 from cells i-2, i-1 (left) and i-1, i (right)
+template <typename RT>
+BH_HD inline void plm_face(RT wmm, RT wm, RT wp, RT wpp, int lim, RT& L, RT& R) {
+    L = wm + RT(0.5) * lim_slope(wm - wmm, wp - wm, lim);
+    R = wp - RT(0.5) * lim_slope(wp - wm, wpp - wp, lim);
+}
+
+// ======================================================================
+// HLL flux at a face from reconstructed left/right primitives.  The normal
+// field comes from the face (wL[P_B+dd] = wR[P_B+dd]).  Returns the larger
+// signal speed magnitude.
+// ======================================================================
+template <typename RT>
+BH_HD inline RT hll_face(const KSm<RT>& m, RT gamma, int dd, const RT* wL, const RT* wR, RT* F) {
+    Derived<RT> dL, dR;
+    derive(m, gamma, wL, dL);
+    derive(m, gamma, wR, dR);
+    RT uL[8], uR[8], FL[8], FR[8];
+    prim2cons(m, gamma, wL, dL, uL);
+    prim2cons(m, gamma, wR, dR, uR);
+    phys_flux(m, dd, wL, dL, uL, FL);
+    phys_flux(m, dd, wR, dR, uR, FR);
+    RT lmL, lpL, lmR, lpR;
+    signal_speeds(m, gamma, dd, wL, dL, lmL, lpL);
+    signal_speeds(m, gamma, dd, wR, dR, lmR, lpR);
+    RT sl = fmin_(fmin_(lmL, lmR), RT(0));
+    RT sr = fmax_(fmax_(lpL, lpR), RT(0));
+    RT ds = sr - sl;
+    if (ds > RT(0)) {
+        RT ids = RT(1) / ds, ss = sr * sl;
+        for (int v = 0; v < 8; v++) F[v] = (sr * FL[v] - sl * FR[v] + ss * (uR[v] - uL[v])) * ids;
+    } else {
+        for (int v = 0; v < 8; v++) F[v] = RT(0.5) * (FL[v] + FR[v]);
+    }
+    F[C_B + dd] = RT(0);
+    return fmax_(sr, -sl);
+}
+
+// ======================================================================
+// geometric source of a cell (densitised: sqrt(-g) S = S here)
+// ======================================================================
+template <typename RT>
+BH_HD inline void source(const KS& mk, const KSD& dk, RT gamma, const RT* w, RT* S) {
+    KSm<RT> m;
+    ks_cast(mk, m);
+    Derived<RT> d;
+    derive(m, gamma, w, d);
+    const RT H = RT(mk.H);
+    RT l[4] = {RT(1), RT(mk.l[0]), RT(mk.l[1]), RT(mk.l[2])};
+    // four-velocity and magnetic four-vector
+    RT ia = RT(1) / m.alpha;
+    RT u[4], b[4];
+    u[0] = d.W * ia;
+    for (int i = 0; i < 3; i++) u[1 + i] = w[P_UT + i] - u[0] * m.beta[i];
+    b[0] = d.W * d.Bv * ia;
+    RT iW = RT(1) / d.W;
+    for (int i = 0; i < 3; i++) b[1 + i] = (w[P_B + i] + m.alpha * b[0] * u[1 + i]) * iW;
+    RT rhoh = w[P_RHO] + gamma / (gamma - RT(1)) * w[P_PRS];
+    RT e = rhoh + d.b2;
+    // inverse four-metric g^{mu nu} = eta^{mu nu} - 2H l^mu l^nu, l^mu = (-1, l_i)
+    RT lu[4] = {RT(-1), l[1], l[2], l[3]};
+    RT T[4][4];
+    for (int mu = 0; mu < 4; mu++)
+        for (int nu = mu; nu < 4; nu++) {
+            RT eta = mu == nu ? (mu == 0 ? RT(-1) : RT(1)) : RT(0);
+            RT gi = eta - RT(2) * H * lu[mu] * lu[nu];
+            T[mu][nu] = e * u[mu] * u[nu] + d.ptot * gi - b[mu] * b[nu];
+            T[nu][mu] = T[mu][nu];
+        }
+    // Tl^mu = T^{mu nu} l_nu
+    RT Tl[4];
+    for (int mu = 0; mu < 4; mu++) Tl[mu] = T[mu][0] * l[0] + T[mu][1] * l[1] + T[mu][2] * l[2] + T[mu][3] * l[3];
+    RT Tll = Tl[0] * l[0] + Tl[1] * l[1] + Tl[2] * l[2] + Tl[3] * l[3];
+    RT dH[3], dl[3][3];
+    for (int k = 0; k < 3; k++) {
+        dH[k] = RT(dk.dH[k]);
+        for (int i = 0; i < 3; i++) dl[k][i] = RT(dk.dl[k][i]);
+    }
+    // S(S_j) = 1/2 T^{mu nu} d_j g_{mu nu} = dH_j Tl.l + 2H Tl^i d_j l_i
+    RT s[3];
+    for (int j = 0; j < 3; j++)
+        s[j] = dH[j] * Tll + RT(2) * H * (Tl[1] * dl[j][0] + Tl[2] * dl[j][1] + Tl[3] * dl[j][2]);
+    // T^{mu nu} Gamma^0_{mu nu} = -2A + 4H^2 (l.Bv) - 2H C - 2H (l.s) with
+    // A = Tl^k d_k H, Bv_i = Tl^k d_k l_i, C = T^{kj} d_k l_j
+    RT A = Tl[1] * dH[0] + Tl[2] * dH[1] + Tl[3] * dH[2];
+    RT lB = RT(0), Cc = RT(0);
+    for (int i = 0; i < 3; i++) {
+        RT Bi = Tl[1] * dl[0][i] + Tl[2] * dl[1][i] + Tl[3] * dl[2][i];
+        lB += l[1 + i] * Bi;
+        Cc += T[1][1 + i] * dl[0][i] + T[2][1 + i] * dl[1][i] + T[3][1 + i] * dl[2][i];
+    }
+    RT ls = l[1] * s[0] + l[2] * s[1] + l[3] * s[2];
+    RT TG = RT(-2) * A + RT(4) * H * H * lB - RT(2) * H * Cc - RT(2) * H * ls;
+    // d_i ln alpha = -alpha^2 d_i H
+    RT a2 = m.alpha * m.alpha;
+    RT T0dH = T[0][1] * dH[0] + T[0][2] * dH[1] + T[0][3] * dH[2];
+    RT ag = m.alpha * m.sqrtgam;
+    S[C_D] = RT(0);
+    for (int j = 0; j < 3; j++) S[C_S + j] = ag * s[j];
+    S[C_TAU] = ag * m.alpha * (-a2 * T0dH - TG);
+    for (int k = 0; k < 3; k++) S[C_B + k] = RT(0);
+}
+
+// ======================================================================
+// floors (the atmosphere of amrtree::pvfs, grid.cpp:133-146, as the
+// configuration asks: rho_fl r^-3/2, u_fl r^-5/2), evaluated at max(r, 1)
+// ======================================================================
+BH_HD inline void floor_state(const FxPar& P, double r, double& rho, double& p) {
+    double re = r > 1.0 ? r : 1.0;
+    double s = sqrt(re);
+    rho = P.rho_fl / (re * s);
+    p = (P.gamma - 1.0) * P.u_fl / (re * re * s);
+}
+
+// ======================================================================
+// con2prim: Newton on Z = rho h W^2 (FP64).  U densitised, B^i the cell's
+// Eulerian field (not densitised), wo the previous primitives (initial
+// guess).  Returns 0 on success (w filled), 1 if the root was not found,
+// 2 if the recovered state is unphysical; iters receives the residual
+// evaluations.
+//
+// Phase 1: Newton from the previous primitives' Z (a step's change of the
+// state is small, so this converges in two or three iterations).  It stops
+// at the first iterate where v^2(Z) reaches the Lorentz-factor ceiling (the
+// derivative is not that of the clamped residual there).  Phase 2: the
+// residual is negative as Z -> 0 and positive for large Z; a bracket
+// [0, Z_hi] (Z_hi doubled until f > 0) is narrowed by safeguarded Newton
+// steps, each replaced by bisection when it would leave the bracket.
+// ======================================================================
+struct C2P {
+    double D, S2, B2, SB2, B4, E, gf, v2max;
+};
+// residual f(Z) and its derivative; v2 is clamped to v2max (clamped = 1)
+BH_HD inline void c2p_eval(const C2P& q, double Z, double& f, double& df, double& v2, int& clamped) {
+    double iZ = 1.0 / Z, ZB = Z + q.B2, iZB = 1.0 / ZB;
+    double iZB2 = iZB * iZB, iZ2 = iZ * iZ;
+    v2 = q.S2 * iZB2 + q.SB2 * (q.B2 + 2.0 * Z) * iZ2 * iZB2;
+    clamped = v2 > q.v2max;
+    if (clamped) v2 = q.v2max;
+    double W2i = 1.0 - v2, Wi = sqrt(W2i);
+    double p = q.gf * (Z * W2i - q.D * Wi);
+    f = Z - p + 0.5 * (1.0 + v2) * q.B2 - 0.5 * q.SB2 * iZ2 - q.E;
+    double dv2 = clamped ? 0.0
+                         : -2.0 * q.S2 * iZB2 * iZB -
+                               2.0 * q.SB2 * (3.0 * Z * Z + 3.0 * Z * q.B2 + q.B4) * iZ2 * iZ * iZB2 * iZB;
+    double dp = q.gf * (W2i - Z * dv2 + 0.5 * q.D * dv2 / Wi);
+    df = 1.0 - dp + 0.5 * q.B2 * dv2 + q.SB2 * iZ2 * iZ;
+}
+
+BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const double* B, const double* wo,
+                          double* w, int& iters) {
+    const double gm = P.gamma;
+    const double isg = 1.0 / m.sqrtgam;
+    C2P q;
+    q.gf = (gm - 1.0) / gm;
+    q.D = U[C_D] * isg;
+    double tau = U[C_TAU] * isg;
+    double S[3] = {U[C_S] * isg, U[C_S + 1] * isg, U[C_S + 2] * isg};
+    double Su[3];
+    lower(m.gi, S, Su);   // S^i = gamma^ij S_j
+    double Bl[3];
+    lower(m.g, B, Bl);
+    q.S2 = Su[0] * S[0] + Su[1] * S[1] + Su[2] * S[2];
+    q.B2 = Bl[0] * B[0] + Bl[1] * B[1] + Bl[2] * B[2];
+    double SB = S[0] * B[0] + S[1] * B[1] + S[2] * B[2];
+    q.SB2 = SB * SB;
+    q.B4 = q.B2 * q.B2;
+    q.E = tau + q.D;
+    q.v2max = 1.0 - 1.0 / (P.W_max * P.W_max);
+    // initial guess from the previous primitives
+    double uto[3] = {wo[P_UT], wo[P_UT + 1], wo[P_UT + 2]}, utl[3];
+    lower(m.g, uto, utl);
+    double W2o = 1.0 + utl[0] * uto[0] + utl[1] * uto[1] + utl[2] * uto[2];
+    double Z = (wo[P_RHO] + gm / (gm - 1.0) * wo[P_PRS]) * W2o;
+    if (!(Z > 0.0) || !(Z < 1e300)) Z = q.E > q.D ? q.E : q.D;
+    int it = 0, ok = 0;
+    double f, df, v2;
+    int clamped;
+    // phase 1
+    for (; it < P.maxiter; it++) {
+        c2p_eval(q, Z, f, df, v2, clamped);
+        if (clamped || !(df != 0.0)) break;
+        double Zn = Z - f / df;
+        if (!(Zn > 0.0)) break;
+        double err = fabs_(Zn - Z);
+        Z = Zn;
+        if (err <= P.tol * Z) { ok = 1; it++; break; }
+    }
+    // phase 2
+    if (!ok) {
+        double lo = 0.0, hi = Z > q.E ? Z : q.E;
+        if (!(hi > 0.0)) hi = 1.0;
+        int k = 0;
+        for (; k < 64; k++) {
+            c2p_eval(q, hi, f, df, v2, clamped);
+            it++;
+            if (f > 0.0) break;
+            lo = hi;
+            hi = 2.0 * hi;
+        }
+        if (f > 0.0 && hi < 1e300) {
+            Z = hi;
+            for (k = 0; k < 2 * P.maxiter + 60; k++) {
+                double Zn = (df > 0.0) ? Z - f / df : 0.5 * (lo + hi);
+                if (!(Zn > lo && Zn < hi)) Zn = 0.5 * (lo + hi);
+                double err = fabs_(Zn - Z);
+                Z = Zn;
+                if (err <= P.tol * Z) { ok = 1; break; }
+                c2p_eval(q, Z, f, df, v2, clamped);
+                it++;
+                if (f > 0.0) hi = Z; else lo = Z;
+            }
+        }
+    }
+    iters = it;
+    if (!ok) return 1;
+    double iZ = 1.0 / Z, ZB = Z + q.B2, iZB = 1.0 / ZB;
+    v2 = q.S2 * iZB * iZB + q.SB2 * (q.B2 + 2.0 * Z) * iZ * iZ * iZB * iZB;
+    if (!(v2 < q.v2max)) v2 = q.v2max;
+    double Wl = 1.0 / sqrt(1.0 - v2);
+    double rho = q.D / Wl;
+    double p = q.gf * (Z * (1.0 - v2) - q.D / Wl);
+    // v_i = (S_i + (S.B / Z) B_i) / (Z + B^2), raised with gamma^ij
+    double vl[3], vu[3];
+    for (int i = 0; i < 3; i++) vl[i] = (S[i] + SB * iZ * Bl[i]) * iZB;
+    lower(m.gi, vl, vu);
+    w[P_RHO] = rho;
+    w[P_PRS] = p;
+    for (int i = 0; i < 3; i++) { w[P_UT + i] = Wl * vu[i]; w[P_B + i] = B[i]; }
+    if (!(rho > 0.0) || !(p == p) || !(Wl == Wl)) return 2;
+    return 0;
+}
+
+// ======================================================================
+// floors and excision on a recovered state: returns 1 if w was changed
+// (the caller then rewrites U = prim2cons(w))
+// ======================================================================
+BH_HD inline int apply_floors(const FxPar& P, const KS& m, double* w) {
+    double rf, pf;
+    floor_state(P, m.r, rf, pf);
+    int changed = 0;
+    if (m.r < P.r_exc) {
+        w[P_RHO] = rf; w[P_PRS] = pf;
+        w[P_UT] = w[P_UT + 1] = w[P_UT + 2] = 0.0;
+        return 1;
+    }
+    // Lorentz factor ceiling
+    double ut[3] = {w[P_UT], w[P_UT + 1], w[P_UT + 2]}, utl[3];
+    lower(m.g, ut, utl);
+    double u2 = utl[0] * ut[0] + utl[1] * ut[1] + utl[2] * ut[2];
+    double umax2 = P.W_max * P.W_max - 1.0;
+    if (u2 > umax2) {
+        double s = sqrt(umax2 / u2);
+        for (int i = 0; i < 3; i++) w[P_UT + i] = ut[i] * s;
+        u2 = umax2;
+        changed = 1;
+    }
+    // magnetisation ceiling b^2 / rho <= sigma_max
+    double W2 = 1.0 + u2, W = sqrt(W2);
+    double B[3] = {w[P_B], w[P_B + 1], w[P_B + 2]}, Bl[3];
+    lower(m.g, B, Bl);
+    double B2 = Bl[0] * B[0] + Bl[1] * B[1] + Bl[2] * B[2];
+    double Bu = (Bl[0] * w[P_UT] + Bl[1] * w[P_UT + 1] + Bl[2] * w[P_UT + 2]) / W;
+    double b2 = B2 / W2 + Bu * Bu;
+    double rs = b2 / P.sigma_max;
+    if (rs > rf) rf = rs;
+    if (!(w[P_RHO] >= rf)) { w[P_RHO] = rf; changed = 1; }
+    if (!(w[P_PRS] >= pf)) { w[P_PRS] = pf; changed = 1; }
+    return changed;
+}
+
+// ======================================================================
+// CFL limit of a cell: the smallest dx_d / max|lambda_d|
+// ======================================================================
+BH_HD inline double cell_dt(const FxPar& P, const KS& mk, const double* w, const double* dx) {
+    KSm<double> m;
+    ks_cast(mk, m);
+    Derived<double> d;
+    derive(m, P.gamma, w, d);
+    double best = 1e300;
+    for (int dd = 0; dd < 3; dd++) {
+        double lm, lp;
+        signal_speeds(m, P.gamma, dd, w, d, lm, lp);
+        double c = fmax_(fabs_(lm), fabs_(lp));
+        if (c > 0.0) best = fmin_(best, dx[dd] / c);
+    }
+    return best;
+}
+
+
+// ======================================================================
+// initial data: Fishbone & Moncrief (1976) torus in Boyer-Lindquist form,
+// carried to Cartesian Kerr-Schild (the role of init::fm_init,
+// initconds.cpp:228-591, with the configuration's parameters)
+// ======================================================================
+// u^t u_phi of the prograde circular equatorial orbit at r (M = 1 units):
+// the torus's conserved angular momentum when its pressure peaks at r
+BH_HD inline double fm_ell(double a, double r) {
+    double sr = sqrt(r), r32 = r * sr;
+    return (r * r - 2.0 * a * sr + a * a) * (r32 + a) / (r32 * (r32 - 3.0 * sr + 2.0 * a));
+}
+struct FMPoint {
+    double Sig, Del, A, e2;   // Sigma, Delta, A and e^{2 nu - 2 psi} = Sigma^2 Delta / (A^2 sin^2)
+};
+BH_HD inline FMPoint fm_point(double a, double r, double s2, double c2) {
+    FMPoint f;
+    f.Sig = r * r + a * a * c2;
+    f.Del = r * r - 2.0 * r + a * a;
+    double ra = r * r + a * a;
+    f.A = ra * ra - f.Del * a * a * s2;
+    f.e2 = f.Sig * f.Sig * f.Del / (f.A * f.A * s2);
+    return f;
+}
+// the FM enthalpy potential W(r, theta); ln h = W(r, theta) - W(r_in, pi/2)
+BH_HD inline double fm_potential(double a, double ell, double r, double s2, double c2) {
+    FMPoint f = fm_point(a, r, s2, c2);
+    double X = sqrt(1.0 + 4.0 * ell * ell * f.e2);
+    return 0.5 * log((1.0 + X) * f.A / (f.Sig * f.Del)) - 0.5 * X - 2.0 * a * r * ell / f.A;
+}
+struct FMTorus {
+    double a, gamma, kappa, r_in, ell, w_in;
+};
+BH_HD inline FMTorus fm_torus(double a, double gamma, double kappa, double r_in, double r_max) {
+    FMTorus t;
+    t.a = a; t.gamma = gamma; t.kappa = kappa; t.r_in = r_in;
+    t.ell = fm_ell(a, r_max);
+    t.w_in = fm_potential(a, t.ell, r_in, 1.0, 0.0);
+    return t;
+}
+// density (before normalisation) at a Cartesian KS point; 0 outside the torus
+BH_HD inline double fm_rho(const FMTorus& t, double x, double y, double z, double* lnh_out) {
+    double r = sqrt(ks_r2(t.a, x, y, z));
+    if (!(r >= t.r_in)) return 0.0;
+    double c = z / r, c2 = c * c, s2 = 1.0 - c2;
+    if (!(s2 > 0.0)) return 0.0;
+    double lnh = fm_potential(t.a, t.ell, r, s2, c2) - t.w_in;
+    if (lnh_out) *lnh_out = lnh;
+    if (!(lnh > 0.0)) return 0.0;
+    double h = exp(lnh);
+    return pow((h - 1.0) * (t.gamma - 1.0) / (t.kappa * t.gamma), 1.0 / (t.gamma - 1.0));
+}
+// four-velocity of the torus at a Cartesian KS point inside it:
+// u^t and the Cartesian u^x, u^y (u^r = u^theta = 0, u^z = 0)
+BH_HD inline void fm_velocity(const FMTorus& t, double x, double y, double z, double& ut, double& ux, double& uy) {
+    const double a = t.a;
+    double r = sqrt(ks_r2(a, x, y, z));
+    double c = z / r, c2 = c * c, s2 = 1.0 - c2;
+    FMPoint f = fm_point(a, r, s2, c2);
+    // velocity in the locally non-rotating frame, u_(phi)^2 (1 + u_(phi)^2) = ell^2 e2
+    double U = sqrt(0.5 * (-1.0 + sqrt(1.0 + 4.0 * t.ell * t.ell * f.e2)));
+    ut = sqrt((1.0 + U * U) * f.A / (f.Sig * f.Del));
+    double uphi = 2.0 * a * r * ut / f.A + U * sqrt(f.Sig / (f.A * s2));
+    // x + i y = (r + i a) e^{i phi} sin(theta): d x / d phi = -y, d y / d phi = x
+    ux = -y * uphi;
+    uy = x * uphi;
+}
+// key of a cell from its global integer coordinates (x / dx - 1/2 rounded),
+// so that the seeded perturbation does not depend on how the grid is cut
+// into blocks; 21 bits per axis
+BH_HD inline uint64_t cell_key(const double* x0, double dx, int i, int j, int k) {
+    const int64_t off = 1 << 20;
+    int64_t g0 = llround(x0[0] / dx) + i + off, g1 = llround(x0[1] / dx) + j + off, g2 = llround(x0[2] / dx) + k + off;
+    return ((uint64_t)g0 << 42) | ((uint64_t)g1 << 21) | (uint64_t)g2;
+}
+// uniform deviate in [0, 1) from a 64-bit counter hash (SplitMix64 finaliser)
+BH_HD inline double hash_uniform(uint64_t seed, uint64_t id) {
+    uint64_t z = seed * 0x100000001B3ULL + id + 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+}  // namespace bhfx

@@ -681,3 +681,6 @@ int step(const bh_params* P, const bh_pool* pool, double cfl, double* dt_dev, co
 }
 
 }  // namespace BH_VARIANT
+
+// the corrected scheme's kernels, compiled in this variant's arithmetic
+#include "bh_fixed.cuh"

@@ -178,9 +178,12 @@ int bh_ghosts_prims(const bh_params *P, const bh_pool *pool, void *stream);
  * the library holds until the process exits; pool->status is ignored.
  * Nothing is allocated or freed; pools of more than BH_STATIC_MAX_PATCHES
  * patches are rejected with BH_ERANGE before anything is launched.
- * The first call on each device, with that device current, looks up the
- * array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  Every call uses the same array and leaves its
+ * Every call made while its stream is not being captured looks up the
+ * array's device address on the current device (cudaGetSymbolAddress), so
+ * the address stays right after a device reset; a call made during a stream
+ * capture reuses the address the last such call found on that device, so
+ * make a first call on each device before any stream capture (BH_ECUDA
+ * otherwise).  Every call uses the same array and leaves its
  * contents behind; each call writes every entry it later reads, so nothing
  * needs clearing, but calls that overlap on the GPU (concurrent streams)
  * race on the array.  Results equal bh_ghosts_prims bit for bit. */
@@ -353,6 +356,114 @@ int bh_step_graph_create(const bh_params *P, const bh_pool *pool, double cfl, do
 /* one step: a replay of the captured graph on `stream` */
 int bh_step_graph_replay(bh_step_graph *g, void *stream);
 int bh_step_graph_destroy(bh_step_graph *g);
+
+/* ==========================================================================
+ * The corrected scheme ("fixed" physics mode).  No counterpart in the
+ * reference: its own scheme stops in the first step of a Kerr torus
+ * (physics/thermo.cpp:10-11 reached from conserved.cpp:205) and has several
+ * defects listed in csrc/bh_fixed_phys.cuh.  This is textbook Valencia GRMHD
+ * in Cartesian Kerr-Schild coordinates (M, a) with the reference's structure:
+ * PLM face states, two-wave HLL fluxes in each face's own normal direction,
+ * geometric sources from the analytic metric derivatives, constrained
+ * transport with a Heun-averaged face field, an exact-derivative Newton
+ * con2prim started from the previous primitives, floors
+ * (rho >= rho_floor r^-3/2, p/(Gamma-1) >= u_floor r^-5/2, b^2/rho <=
+ * sigma_max, W <= W_max) and excision (cells with r < r_exc are reset to
+ * the floor state at rest every stage).
+ *
+ * Layout: a list of cubic blocks of n^3 interior cells (n a multiple of 8)
+ * with two ghost layers; every array stores each block as a (n+5)^3 box
+ * (cells -2 .. n+2 per axis) at offset blocks[b].off, index
+ * ((i+2) S + (j+2)) S + (k+2), S = n + 5 (i slowest, k fastest, as the
+ * reference's patches).  The x-face (i-1/2, j, k), y-face (i, j-1/2, k) and
+ * z-face (i, j, k-1/2) share the index of cell (i, j, k).
+ *   U, U1  [8][ncell] conserved D, S_x, S_y, S_z, tau, B^x, B^y, B^z
+ *                     densitised by sqrt(gamma) (U1: the RK stage state)
+ *   W      [8][ncell] primitives rho, p, ut^x, ut^y, ut^z (ut = W v, the
+ *                     Eulerian velocity times its Lorentz factor), B^x, B^y,
+ *                     B^z; double, or float when precision is BH_MIXED
+ *   Bf, Bf1 [3][ncell] face field sqrt(gamma) B^d (Bf1: the stage's)
+ *   F      [3][8][ncell] face fluxes (double, or float for BH_MIXED)
+ * Work lists: items_* are device arrays of int32 pairs (block, first index)
+ * of BH_FX_CHUNK consecutive indices of the block's index space: interior
+ * cells (n^3, index (i n + j) n + k), flux positions ((n+2)^3, positions
+ * -1 .. n per axis) and ghost cells ((n+4)^3 - n^3, the ghost shell).
+ * ========================================================================== */
+#define BH_FX_CHUNK 128
+typedef struct bh_fx_params {
+    double M, a, gamma;
+    double cfl;
+    double rho_floor, u_floor;   /* floor coefficients                             */
+    double sigma_max, W_max;     /* magnetisation and Lorentz-factor ceilings       */
+    double r_exc;                /* excision radius                                 */
+    double tol;                  /* con2prim: stop when |dZ| <= tol Z (1e-12)       */
+    int32_t maxiter;             /* con2prim Newton cap (30)                        */
+    int32_t limiter;             /* BH_MINMOD / BH_VANLEER / BH_MC                  */
+    int32_t precision;           /* BH_FP64 / BH_FP64_FMA / BH_MIXED                */
+    int32_t reserved;
+} bh_fx_params;
+
+typedef struct bh_fx_block {
+    int32_t n, level;
+    int64_t off;                 /* offset of the block's box in every array        */
+    double x0[3];                /* lower corner of the interior                    */
+    double dx;                   /* cell size                                       */
+} bh_fx_block;
+
+typedef struct bh_fx_grid {
+    int32_t nblock;
+    const bh_fx_block *blocks;   /* device [nblock]                                  */
+    const int32_t *nbr;          /* device [nblock][27]: the block at offset
+                                    (ox, oy, oz) in {-1,0,1}^3, index
+                                    (ox+1)*9 + (oy+1)*3 + (oz+1); -1 = outside the
+                                    domain (outflow)                               */
+    const int32_t *items_cell; int32_t nitem_cell;
+    const int32_t *items_pos;  int32_t nitem_pos;
+    const int32_t *items_ghost; int32_t nitem_ghost;
+    int64_t ncell;               /* entries per array (sum of (n+5)^3)               */
+    double *U, *U1;
+    void *W;
+    double *Bf, *Bf1;
+    void *F;
+    double *dt;                  /* device [2]: dt[0] min over cells of dx / |signal
+                                    speed|, dt[1] the step's time step cfl dt[0]    */
+    int32_t *count;              /* device [4]: con2prim failures, floored cells     */
+    int32_t *err;                /* device error word                                */
+} bh_fx_grid;
+
+/* one RK2 step: con2prim (+ CFL reduction), ghost fill, fluxes, update, twice */
+int bh_fx_step(const bh_fx_params *P, const bh_fx_grid *g, void *stream);
+/* bh_fx_step recorded once as a CUDA graph (9 launches; dt stays on the
+ * device): replay and release it with bh_step_graph_replay / _destroy.
+ * stream is required (not the legacy default stream); the grid's arrays
+ * must stay valid at the same addresses while the graph lives. */
+int bh_fx_graph_create(const bh_fx_params *P, const bh_fx_grid *g, void *stream, bh_step_graph **out);
+/* the pieces of a stage (stage 0 works on U/Bf, stage 1 on U1/Bf1) */
+int bh_fx_prims(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, int32_t with_dt, void *stream);
+int bh_fx_ghosts(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
+int bh_fx_fluxes(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
+int bh_fx_update(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
+/* max over each block's interior cells of |div B~| / max |B~| of the cell's
+ * faces (a relative divergence, 0 up to roundoff under CT): out [nblock]
+ * device, cleared by the call */
+int bh_fx_divb(const bh_fx_grid *g, double *out, void *stream);
+
+/* Fishbone-Moncrief torus (pressure maximum at r_max, inner edge r_in,
+ * polytrope p = kappa rho^Gamma normalised to rho_max = 1) in the atmosphere
+ * of the floors, pressure perturbed by (1 + noise (2 u - 1)) with u uniform
+ * from a hash of the seed and the cell's global integer coordinates (the
+ * same for any cutting of the grid into blocks), and a single field loop from
+ * A_phi = max(rho / rho_max - 0.2, 0) scaled so that max p_gas / max p_mag
+ * = beta over the interior cells.  Fills W, U (every cell of every box), Bf.
+ * scratch: device [4] doubles.  out (host, may be NULL) [4]: the torus's
+ * specific angular momentum u^t u_phi, the density maximum before
+ * normalisation, the field scale applied, max p_gas / max p_mag after it. */
+typedef struct bh_fx_torus {
+    double r_in, r_max, kappa, beta, noise;
+    uint64_t seed;
+} bh_fx_torus;
+int bh_fx_torus_init(const bh_fx_params *P, const bh_fx_grid *g, const bh_fx_torus *T, double *scratch,
+                     double *out, void *stream);
 
 #ifdef __cplusplus
 }

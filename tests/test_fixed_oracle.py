@@ -1,0 +1,377 @@
+"""The corrected scheme's CPU oracle (oracle/bh_fixed.c) pinned to physics.
+
+The reference has no such scheme, so these tests pin the restatement to
+identities computed independently here in numpy:
+
+* the Kerr-Schild metric: l null, det g = -1, lapse/shift/spatial metric
+  from the inverted 4-metric; its derivatives against finite differences;
+* conserved variables and fluxes against projections of the stress-energy
+  tensor T^{mu nu} = (rho h + b^2) u u + (p + b^2/2) g^-1 - b b built from
+  the four-velocity and the magnetic four-vector;
+* geometric sources against the Valencia source terms evaluated with
+  Christoffel symbols from finite differences of the metric;
+* signal speeds against relativistic velocity addition in flat space;
+* con2prim: primitives -> conserved -> primitives round trips, from good
+  and from poor initial guesses;
+* the Fishbone-Moncrief torus: pressure maximum at r_max, normalised
+  four-velocity, conserved u^t u_phi;
+* the scheme: a uniform state is preserved, the face field's divergence
+  stays at roundoff, and a sound wave converges at second order.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import fixed as ofx
+from bhgrid.blocks import interior, uniform_blocks
+
+
+class Prm:
+    def __init__(self, **kw):
+        self.M, self.a, self.gamma, self.cfl = 1.0, 0.9375, 4.0 / 3.0, 0.4
+        self.rho_floor, self.u_floor, self.sigma_max, self.W_max = 1e-6, 1e-8, 100.0, 50.0
+        self.r_exc, self.tol, self.maxiter, self.limiter = None, 1e-12, 30, "vanleer"
+        self.__dict__.update(kw)
+
+
+ETA = np.diag([-1.0, 1.0, 1.0, 1.0])
+
+
+def np_metric(M, a, x, y, z):
+    """4-metric g_{mu nu} and inverse at one Cartesian Kerr-Schild point"""
+    R2 = x * x + y * y + z * z
+    r2 = 0.5 * (R2 - a * a) + math.sqrt(0.25 * (R2 - a * a) ** 2 + a * a * z * z)
+    r = math.sqrt(r2)
+    H = M * r ** 3 / (r ** 4 + a * a * z * z)
+    l = np.array([1.0, (r * x + a * y) / (r2 + a * a), (r * y - a * x) / (r2 + a * a), z / r])
+    g = ETA + 2 * H * np.outer(l, l)
+    return g, np.linalg.inv(g), r, H, l
+
+
+def sample_points(rng, n, rmin=2.0, rmax=40.0):
+    r = rng.uniform(rmin, rmax, n)
+    v = rng.normal(size=(3, n))
+    v /= np.linalg.norm(v, axis=0)
+    return r * v[0], r * v[1], r * v[2]
+
+
+def sample_prims(rng, n, umax=3.0, sigma=5.0):
+    w = np.zeros((8, n))
+    w[0] = 10 ** rng.uniform(-4, 0, n)
+    w[1] = w[0] * 10 ** rng.uniform(-3, 0, n)
+    w[2:5] = rng.normal(size=(3, n)) * rng.uniform(0, umax, n) / math.sqrt(3)
+    w[5:8] = rng.normal(size=(3, n)) * np.sqrt(sigma * w[0] * rng.uniform(0, 1, n))
+    return w
+
+
+def four_vectors(gam, g, gi, w):
+    """u^mu, b^mu from (rho, p, ut^i, B^i) with the spatial metric of g"""
+    alpha = 1.0 / math.sqrt(-gi[0, 0])
+    beta = -gi[0, 1:] / gi[0, 0]
+    gs = g[1:, 1:]
+    ut, B = w[2:5], w[5:8]
+    W = math.sqrt(1 + ut @ gs @ ut)
+    v = ut / W
+    u = np.zeros(4)
+    u[0] = W / alpha
+    u[1:] = W * (v - beta / alpha)
+    Bv = B @ gs @ v
+    b = np.zeros(4)
+    b[0] = W * Bv / alpha
+    b[1:] = (B + alpha * b[0] * u[1:]) / W
+    return u, b, alpha, beta, W
+
+
+def stress(gam, gi, w, u, b, g):
+    bl = g @ b
+    b2 = b @ bl
+    rhoh = w[0] + gam / (gam - 1) * w[1]
+    return (rhoh + b2) * np.outer(u, u) + (w[1] + 0.5 * b2) * gi - np.outer(b, b)
+
+
+def test_metric_identities():
+    prm = ofx.params(Prm())
+    rng = np.random.default_rng(1)
+    x, y, z = sample_points(rng, 200, 1.2, 60.0)
+    out = ofx.metric(prm, x, y, z)
+    for q in range(len(x)):
+        g, gi, r, H, l = np_metric(1.0, 0.9375, x[q], y[q], z[q])
+        assert abs(l @ np.linalg.inv(ETA) @ l) < 1e-13
+        assert abs(np.linalg.det(g) + 1.0) < 1e-10
+        alpha = 1 / math.sqrt(-gi[0, 0])
+        beta = -gi[0, 1:] / gi[0, 0]
+        o = out[q]
+        assert abs(o[0] - H) <= 1e-14 * max(H, 1) and np.allclose(o[1:4], l[1:], rtol=0, atol=1e-14)
+        assert abs(o[4] - alpha) < 1e-14 and np.allclose(o[6:9], beta, rtol=0, atol=1e-14)
+        assert abs(o[5] - math.sqrt(np.linalg.det(g[1:, 1:]))) < 1e-12
+        gs, gsi = g[1:, 1:], np.linalg.inv(g[1:, 1:])
+        idx = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]
+        assert np.allclose([o[9 + t] for t in range(6)], [gs[i, j] for i, j in idx], rtol=0, atol=1e-13)
+        assert np.allclose([o[15 + t] for t in range(6)], [gsi[i, j] for i, j in idx], rtol=0, atol=1e-12)
+        assert abs(o[21] - r) < 1e-13 * r
+
+
+def test_metric_derivatives_finite_difference():
+    prm = ofx.params(Prm())
+    rng = np.random.default_rng(2)
+    x, y, z = sample_points(rng, 200, 1.3, 50.0)
+    d = ofx.deriv(prm, x, y, z)
+    h = 1e-4
+    for k in range(3):
+        dx = [np.zeros_like(x) for _ in range(3)]
+        dx[k][:] = h
+        mp = [ofx.metric(prm, x + s * dx[0], y + s * dx[1], z + s * dx[2]) for s in (-2, -1, 1, 2)]
+        fd = (mp[0] - 8 * mp[1] + 8 * mp[2] - mp[3]) / (12 * h)
+        assert np.allclose(d[:, k], fd[:, 0], rtol=1e-7, atol=1e-10)
+        for i in range(3):
+            assert np.allclose(d[:, 3 + 3 * k + i], fd[:, 1 + i], rtol=1e-7, atol=1e-10)
+
+
+def test_conserved_and_fluxes_from_stress_tensor():
+    prm = ofx.params(Prm())
+    gam = prm.gamma
+    rng = np.random.default_rng(3)
+    n = 300
+    x, y, z = sample_points(rng, n)
+    w = sample_prims(rng, n)
+    for dd in range(3):
+        U, F, lm, lp = ofx.cons_flux(prm, x, y, z, dd, w)
+        for q in range(n):
+            g, gi, r, H, l = np_metric(1.0, 0.9375, x[q], y[q], z[q])
+            u, b, alpha, beta, W = four_vectors(gam, g, gi, w[:, q])
+            T = stress(gam, gi, w[:, q], u, b, g)
+            sg = math.sqrt(np.linalg.det(g[1:, 1:]))
+            smg = math.sqrt(-np.linalg.det(g))
+            Tmix = T @ g                      # T^mu_nu
+            D = sg * w[0, q] * W
+            exp_u = np.zeros(8)
+            exp_u[0] = D
+            exp_u[1:4] = smg * Tmix[0, 1:]
+            exp_u[4] = sg * alpha ** 2 * T[0, 0] - D
+            exp_u[5:8] = sg * w[5:8, q]
+            i = 1 + dd
+            exp_F = np.zeros(8)
+            exp_F[0] = smg * w[0, q] * u[i]
+            exp_F[1:4] = smg * Tmix[i, 1:]
+            exp_F[4] = smg * (alpha * T[0, i] - w[0, q] * u[i])
+            for k in range(3):
+                exp_F[5 + k] = smg * (b[1 + k] * u[i] - b[i] * u[1 + k])
+            scale_u = np.abs(exp_u[:5]).max()
+            assert np.allclose(U[:, q], exp_u, rtol=1e-11, atol=1e-12 * scale_u), (dd, q)
+            scale_f = max(np.abs(exp_F).max(), 1e-300)
+            assert np.allclose(F[:, q], exp_F, rtol=1e-10, atol=1e-11 * scale_f), (dd, q)
+
+
+def test_signal_speeds_flat_boost():
+    """flat space, motion along the face normal: (v -+ c)/(1 -+ v c)"""
+    prm = ofx.params(Prm(M=0.0, a=0.0))
+    gam = prm.gamma
+    rng = np.random.default_rng(4)
+    n = 100
+    x, y, z = sample_points(rng, n)
+    for dd in range(3):
+        w = np.zeros((8, n))
+        w[0] = rng.uniform(0.1, 1, n)
+        w[1] = rng.uniform(0.01, 1, n)
+        v = rng.uniform(-0.9, 0.9, n)
+        w[2 + dd] = v / np.sqrt(1 - v * v)
+        w[5 + dd] = rng.uniform(0, 1, n)         # field along the motion: b^2 = B^2 / W^2 ... kept general
+        _, _, lm, lp = ofx.cons_flux(prm, x, y, z, dd, w)
+        W = 1 / np.sqrt(1 - v * v)
+        rhoh = w[0] + gam / (gam - 1) * w[1]
+        B2 = w[5 + dd] ** 2
+        Bv = w[5 + dd] * v
+        b2 = B2 / W ** 2 + Bv ** 2
+        cs2 = gam * w[1] / rhoh
+        va2 = b2 / (rhoh + b2)
+        c = np.sqrt(cs2 + va2 - cs2 * va2)
+        assert np.allclose(lm, (v - c) / (1 - v * c), rtol=1e-12, atol=1e-14)
+        assert np.allclose(lp, (v + c) / (1 + v * c), rtol=1e-12, atol=1e-14)
+
+
+def test_sources_from_christoffels():
+    prm = ofx.params(Prm())
+    gam = prm.gamma
+    rng = np.random.default_rng(5)
+    n = 60
+    x, y, z = sample_points(rng, n, 1.8, 30.0)
+    w = sample_prims(rng, n)
+    S = ofx.source(prm, x, y, z, w)
+    h = 1e-4
+    for q in range(n):
+        p = np.array([x[q], y[q], z[q]])
+        g, gi, r, H, l = np_metric(1.0, 0.9375, *p)
+        dg = np.zeros((4, 4, 4))   # dg[k] = d_k g, k = 0 (time) stays 0
+        for k in range(3):
+            e = np.zeros(3); e[k] = h
+            gs = [np_metric(1.0, 0.9375, *(p + s * e))[0] for s in (-2, -1, 1, 2)]
+            dg[1 + k] = (gs[0] - 8 * gs[1] + 8 * gs[2] - gs[3]) / (12 * h)
+        Gam = 0.5 * (np.einsum("ls,msn->lmn", gi, dg) + np.einsum("ls,nsm->lmn", gi, dg)
+                     - np.einsum("ls,smn->lmn", gi, dg))
+        u, b, alpha, beta, W = four_vectors(gam, g, gi, w[:, q])
+        T = stress(gam, gi, w[:, q], u, b, g)
+        smg = math.sqrt(-np.linalg.det(g))
+        exp = np.zeros(8)
+        for j in range(3):
+            J = 1 + j
+            exp[1 + j] = smg * (np.einsum("mn,mn->", T, dg[:, :, J])
+                                - np.einsum("mn,dnm,d->", T, Gam, g[:, J]))
+        dlna = np.zeros(4)
+        for k in range(3):
+            e = np.zeros(3); e[k] = h
+            al = [1 / math.sqrt(-np_metric(1.0, 0.9375, *(p + s * e))[1][0, 0]) for s in (-2, -1, 1, 2)]
+            dlna[1 + k] = (al[0] - 8 * al[1] + 8 * al[2] - al[3]) / (12 * h) / alpha
+        exp[4] = smg * alpha * (T[:, 0] @ dlna - np.einsum("mn,nm->", T, Gam[0]))
+        scale = np.abs(exp).max()
+        assert np.allclose(S[:, q], exp, rtol=1e-6, atol=1e-8 * scale), (q, S[:, q], exp)
+
+
+@pytest.mark.parametrize("guess", ["near", "poor"])
+def test_con2prim_round_trip(guess):
+    prm = ofx.params(Prm())
+    rng = np.random.default_rng(6)
+    n = 4000
+    x, y, z = sample_points(rng, n, 1.8, 40.0)
+    w = sample_prims(rng, n, umax=5.0, sigma=20.0)
+    U, _, _, _ = ofx.cons_flux(prm, x, y, z, 0, w)
+    wo = w.copy()
+    if guess == "near":
+        wo[:5] *= 1 + 1e-3 * rng.normal(size=(5, n))
+    else:
+        wo[0] *= 1e-4; wo[1] *= 1e3; wo[2:5] = 0.0
+    wr, st, it = ofx.con2prim(prm, x, y, z, U, w[5:8], wo)
+    assert (st == 0).all(), np.bincount(st)
+    for v in range(5):
+        scale = np.abs(w[v]) + (np.abs(w[2:5]).max(0) if v >= 2 else 0) + 1e-300
+        err = np.abs(wr[v] - w[v]) / scale
+        assert err.max() <= 1e-8, (v, err.max())
+    if guess == "near":
+        assert np.median(it) <= 4
+
+
+def test_fishbone_moncrief_torus():
+    a, gam, r_in, r_max = 0.9375, 4.0 / 3.0, 6.0, 12.0
+    ell = ofx.fm_ell(a, r_max)
+    # independent: u^t u_phi of the circular equatorial geodesic at r_max (BL)
+    r = r_max
+    Om = 1 / (r ** 1.5 + a)
+    Sig, Del = r * r, r * r - 2 * r + a * a
+    A = (r * r + a * a) ** 2 - Del * a * a
+    gtt, gtp, gpp = -(1 - 2 * r / Sig), -2 * a * r / Sig, A / Sig
+    ut = 1 / math.sqrt(-(gtt + 2 * gtp * Om + gpp * Om * Om))
+    uphi_low = (gtp + gpp * Om) * ut
+    assert abs(ell - ut * uphi_low) < 1e-12 * ell
+    # pressure maximum at r_max in the equatorial plane: d ln h / dr = 0
+    h = 1e-4
+    dW = (ofx.fm_potential(a, ell, r_max + h, 1.0, 0.0) - ofx.fm_potential(a, ell, r_max - h, 1.0, 0.0)) / (2 * h)
+    dW_in = (ofx.fm_potential(a, ell, r_in + h, 1.0, 0.0) - ofx.fm_potential(a, ell, r_in - h, 1.0, 0.0)) / (2 * h)
+    assert abs(dW) < 1e-8 and abs(dW_in) > 1e-3
+    # four-velocity at torus points: normalised, conserved u^t u_phi
+    rng = np.random.default_rng(7)
+    rr = rng.uniform(7, 20, 300); th = rng.uniform(1.2, 1.9, 300); ph = rng.uniform(0, 2 * np.pi, 300)
+    x = (rr * np.cos(ph) - a * np.sin(ph)) * np.sin(th)
+    y = (rr * np.sin(ph) + a * np.cos(ph)) * np.sin(th)
+    z = rr * np.cos(th)
+    out = ofx.fm(a, gam, 1e-3, r_in, r_max, x, y, z)
+    inside = out[:, 0] > 0
+    assert inside.sum() > 50
+    for q in np.where(inside)[0]:
+        g, gi, r_, H, l = np_metric(1.0, a, x[q], y[q], z[q])
+        assert abs(r_ - rr[q]) < 1e-10 * rr[q]
+        u = np.array([out[q, 2], out[q, 3], out[q, 4], 0.0])
+        assert abs(u @ g @ u + 1) < 1e-11
+        ul = g @ u
+        assert abs(u[0] * (-y[q] * ul[1] + x[q] * ul[2]) - ell) < 1e-10 * ell
+
+
+def _flat_grid(N, block, prm, periodic=True, lo=0.0, hi=1.0):
+    blocks, nbr = uniform_blocks(lo, hi, N, block, periodic)
+    return ofx.FxHost(blocks, nbr, ofx.params(prm))
+
+
+def _set_cells(h, fn):
+    """W, U of every interior cell from fn(x, y, z) -> w[8]; face field from
+    the cell values (uniform field only)"""
+    for b in h.blocks:
+        n, S, off, dx = int(b["n"]), int(b["n"]) + 5, int(b["off"]), b["dx"]
+        idx = off + ((np.arange(n)[:, None, None] + 2) * S + (np.arange(n)[None, :, None] + 2)) * S + (
+            np.arange(n)[None, None, :] + 2)
+        c = (np.arange(n) + 0.5) * dx
+        X = b["x0"][0] + c[:, None, None] + 0 * c[None, :, None] + 0 * c[None, None, :]
+        Y = b["x0"][1] + 0 * c[:, None, None] + c[None, :, None] + 0 * c[None, None, :]
+        Z = b["x0"][2] + 0 * c[:, None, None] + 0 * c[None, :, None] + c[None, None, :]
+        w = fn(X.ravel(), Y.ravel(), Z.ravel())
+        h.W[:, idx.ravel()] = w
+        U, _, _, _ = ofx.cons_flux(h.prm, X.ravel(), Y.ravel(), Z.ravel(), 0, w)
+        h.U[:, idx.ravel()] = U
+        all_idx = off + np.arange(S ** 3)
+        for d in range(3):
+            h.Bf[d, all_idx] = w[5 + d, 0]
+
+
+def test_uniform_state_preserved():
+    prm = Prm(M=0.0, a=0.0, r_exc=-1.0, rho_floor=1e-12, u_floor=1e-14)
+    h = _flat_grid(16, 8, prm)
+    w0 = np.array([1.0, 0.3, 0.2, -0.1, 0.05, 0.4, 0.1, -0.2])
+    _set_cells(h, lambda X, Y, Z: np.repeat(w0[:, None], X.size, 1))
+    U0 = h.interior(h.U).copy()
+    for _ in range(2):
+        h.step()
+    U1 = h.interior(h.U)
+    for v in range(8):
+        assert np.abs(U1[v] - U0[v]).max() <= 1e-14 * max(np.abs(U0[v]).max(), 1.0), v
+    assert h.divb() == 0.0
+
+
+def _sound_wave_error(N, gam=4.0 / 3.0, eps=1e-4, t_end=0.25):
+    prm = Prm(M=0.0, a=0.0, r_exc=-1.0, rho_floor=1e-12, u_floor=1e-14, cfl=0.3, limiter="mc")
+    h = _flat_grid(N, 8, prm)
+    rho0, p0 = 1.0, 0.6
+    rhoh = rho0 + gam / (gam - 1) * p0
+    cs = math.sqrt(gam * p0 / rhoh)
+
+    def wave(X, t):
+        ph = np.sin(2 * np.pi * (X - cs * t))
+        dp = eps * p0 * ph
+        w = np.zeros((8, X.size))
+        w[0] = rho0 + rho0 * dp / (gam * p0)
+        w[1] = p0 + dp
+        v = dp / (rhoh * cs)
+        w[2] = v / np.sqrt(1 - v * v)
+        return w
+
+    _set_cells(h, lambda X, Y, Z: wave(X, 0.0))
+    t = 0.0
+    while t < t_end - 1e-12:
+        h.step()
+        t += h.dt[1]
+    err = 0.0
+    for b in h.blocks:
+        n = int(b["n"])
+        c = b["x0"][0] + (np.arange(n) + 0.5) * b["dx"]
+        exact = wave(np.repeat(c, n * n), t)[1].reshape(n, n, n)
+        S = n + 5
+        box = h.W[1, int(b["off"]):int(b["off"]) + S ** 3].reshape(S, S, S)[2:2 + n, 2:2 + n, 2:2 + n]
+        err += np.abs(box - exact).sum()
+    return err / N ** 3
+
+
+def test_sound_wave_second_order():
+    e16 = _sound_wave_error(16)
+    e32 = _sound_wave_error(32)
+    assert e32 < e16 / 2.8, (e16, e32)
+
+
+def test_divergence_stays_at_roundoff_on_torus():
+    blocks, nbr = uniform_blocks(-40.0, 40.0, 32, 16)
+    h = ofx.FxHost(blocks, nbr, ofx.params(Prm()))
+    h.torus_init()
+    assert h.divb() <= 1e-14
+    for _ in range(3):
+        h.step()
+    assert h.divb() <= 1e-13
+    assert h.count[0] == 0
+    assert np.isfinite(interior(blocks, h.U)).all()
