@@ -1,50 +1,45 @@
 #!/usr/bin/env python
-"""Benchmark of the GPU GRMHD block update (one JSON line on rank 0).
+"""Benchmark of the GPU GRMHD update (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--grid 128|64] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload: the uniform magnetised box -- rho = 1, p = 0.1 (1 + 0.01 N(0,1)),
-v = 0, B = (0.5, 0.3, 0) + curl of a random vector potential (|k| <= 4,
-RMS 1e-2), flat tree metric (M = a = Q = 0), Gamma = 4/3, periodic,
-PLM-minmod + HLLD + constrained transport, RK2 at CFL 0.4 -- on a 128^3
-grid of 8^3 patches of 16^3 cells (``--grid 64``: the 64^3 box of 4^3
-patches).  Synthetic seeded data.
+Workload (the torus configuration the metric is quoted on): a Kerr black
+hole (M = 1, a = 0.9375) on a uniform Cartesian 128^3 grid over
+[-40, 40]^3, excision inside r = 1.2 r_H; a Fishbone-Moncrief torus with
+r_in = 6, r_max = 12, Gamma = 4/3, atmosphere rho = 1e-6 r^-3/2, a seeded 4 %
+pressure perturbation and a single field loop from A_phi ~ max(rho/rho_max -
+0.2, 0) normalised to plasma beta = 100 -- stepped with RK2 at CFL 0.4 by the
+corrected Valencia scheme (bhgpu.fixed: PLM van Leer, HLL fluxes in each
+face's normal, analytic Kerr-Schild sources, constrained transport, Newton
+con2prim).  The reference's own scheme cannot run this configuration: it
+throws std::domain_error in its first stage (src/fluid/physics/thermo.cpp:11).
+Synthetic seeded data.
 
-Arithmetic: the headline runs the FP64 kernels with fused multiply-add
-(``--precision``, default fp64-fma); the reference-faithful FP64 form and
-the mixed FP32/FP64 variant are timed beside it on the same workload, with
-the mixed variant's accuracy against FP64 (the magnetised box after one
-step, the unmagnetised box after five).
-
-A step is one full rk2integrator::step (dtcomp, two RK stages with ghost
-fill, con2prim, fluxes, CT and update, floors) over the whole grid,
-restarted every step from the seeded initial state (a device-to-device
-copy inside the timed region), so every step does the same work.
-
-value : zone-updates/s, inputs resident in HBM, device-timed with CUDA
-        events, max over ranks.  N > 1 runs one independent box per GPU
-        (weak scaling, no data-path collective).
-e2e   : same metric through the public API with host buffers
-        (bhgpu.HostPipeline): per step the H2D copy of the state (U, W, Bf)
-        from pinned memory, the step, and the D2H copy of the new state,
-        with consecutive steps on three device trees so that the copies of
-        neighbouring steps overlap the step; the one-tree (serial) figure
-        is reported beside it.
-roofline : the call with the largest share of the step (ghost fill +
-        con2prim, or the face fluxes), its algorithmic bytes per launch / its
-        CUDA-event duration inside the timed region, against the measured HBM
-        copy bandwidth (the fallback figure when MEASURED_PEAKS.json is
-        absent).
-autotune : before timing, the launch bounds of the heavy kernels are tuned
-        on the box for every variant (bhgpu.tune; --autotune 0 keeps the
-        compiled-in ones).
-cpu_baseline : the reference solver's own rk2integrator::step compiled from
-        its sources (oracle/_ref), on all host cores, on a 64^3 sample.
+value : zone-updates/s of the mixed-precision form (reconstruction, fluxes
+        and sources in FP32; conserved state, constrained transport,
+        con2prim and dt in FP64), the step replayed as one CUDA graph,
+        free-running from the initial data, device-timed with CUDA events,
+        max over ranks; N > 1 runs one independent torus per GPU (weak
+        scaling, no data-path collective).  The plain FP64 form (and the
+        FMA-contracted FP64 form) are timed the same way beside it, and the
+        mixed form's relative L1/Linf error against plain FP64 after 100
+        steps from the same initial data is reported per conserved field
+        with the face field's divergence.
+e2e   : the same metric through the public API with host buffers
+        (bhgpu.fixed.FxHostPipeline): per step the state (U, W, Bf) goes up
+        from pinned host memory, is stepped, and comes back down; three
+        device grids overlap the copies of neighbouring steps.
+roofline : the kernel with the largest share of the step, its algorithmic
+        bytes per launch over its CUDA-event duration, against the measured
+        HBM copy bandwidth (MEASURED_PEAKS.json; fallback 6650 GB/s); the
+        FP64/FP32 pipe peaks measured here by bh_peak_fma are reported beside
+        it, since these kernels are instruction-bound.
+cpu_baseline : the CPU port of the same scheme (oracle/bh_fixed.c,
+        OpenMP over all host cores) on the same 128^3 torus.
 """
 from __future__ import annotations
 
 import argparse
-import ctypes as C
 import json
 import os
 import statistics
@@ -59,7 +54,11 @@ sys.path.insert(0, REPO)
 METRIC = "zone-updates/s"
 GAMMA = 4.0 / 3.0
 CFL = 0.4
-LO, HI = 10.0, 12.0
+LO, HI = -40.0, 40.0
+TORUS = dict(r_in=6.0, r_max=12.0, kappa=1e-3, beta=100.0, noise=0.04, seed=1)
+STEP_BYTES = 296          # algorithmic HBM bytes per zone-update of an RK2 step
+LAUNCHES_PER_STEP = 9     # dt init, then con2prim, ghosts, fluxes, update per stage
+E2E_DEPTH = 3
 
 
 def parse():
@@ -67,17 +66,14 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--grid", type=int, default=128, choices=[64, 128])
+    ap.add_argument("--grid", type=int, default=128)
+    ap.add_argument("--block", type=int, default=128, help="cells per block edge (the grid is one block by default)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-steps", type=int, default=2, help="steps of the CPU port in cpu_baseline")
+    ap.add_argument("--faithful", type=int, default=1, help="also time the reference-faithful FP64 path")
     ap.add_argument("--con2prim-batch", type=int, default=1, help="also measure the 2^24-cell con2prim batch")
-    ap.add_argument("--con2prim-cells", type=int, default=1 << 24, help="cells of the con2prim batch")
-    ap.add_argument("--autotune", type=int, default=1, choices=[0, 1, 2],
-                    help="launch bounds of the heavy kernels: 1 tune them on the box first and save the choice "
-                         "(bhgpu.tune), 2 apply the saved choice without timing (for profiler runs), 0 keep "
-                         "the compiled-in ones")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64-fma", "mixed"],
-                    help="arithmetic variant of the headline value; the other variants are timed beside it")
     return ap.parse_args()
 
 
@@ -87,17 +83,14 @@ def env_rank():
 
 
 def measured_peaks():
-    path = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
-        with open(path) as f:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
 
 
-# ---------------------------------------------------------------------------
-# clock sampling during the timed region
 class Clocks:
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -135,94 +128,248 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def arm_config(args, world):
+    return {"workload": f"Kerr-Schild torus {args.grid}^3 (configuration 2): a=0.9375 over [-40,40]^3, "
+                        "Fishbone-Moncrief r_in=6 r_max=12, Gamma=4/3, beta=100 single loop, 4% pressure noise, "
+                        "excision r<1.2 r_H; corrected Valencia scheme, PLM van Leer + HLL + CT, RK2 CFL 0.4",
+            "grid": f"{args.grid}^3", "blocks": (args.grid // args.block) ** 3,
+            "block": f"{args.block}^3 + 2 ghosts", "parallelism": f"replicas x{world}",
+            "l2": "working set > L2 (the 128^3 state, primitives and fluxes exceed 126 MB)",
+            "run": "free-running from the torus initial data (every step continues the last)"}
+
+
 # ---------------------------------------------------------------------------
-def make_tree(nq, seed, precision="fp64", **box):
-    import bhgpu
-    from bhgpu import configs
-    from bhgpu.mesh import Quilt
-    q = Quilt([LO] * 3, [HI] * 3, nq, periodic=True)
-    tree = bhgpu.AmrTree(q.dom_l, q.dom_h, nq, M=0.0, a=0.0, Q=0.0, gm=GAMMA, periodic=True,
-                         limiter="minmod", quilt=q, init_floor=False, precision=precision)
-    W, Bf = configs.magnetised_box(q, seed=seed, gamma=GAMMA, **box)
-    tree.load(W=W, Bf=Bf)
-    tree.prim_to_cons()
-    return tree
+def torus_grid(args, precision):
+    from bhgpu.fixed import FxGrid, FxParams
+    g = FxGrid.uniform(LO, HI, args.grid, args.block, FxParams(precision=precision))
+    info = g.torus_init(**TORUS)
+    return g, info
 
 
-# Algorithmic HBM bytes of one launch of each stage call over the whole pool
-# (the data the computation must read and write once, nothing re-read):
-#   ghosts_prims: per leaf patch, the ghost-strip copy (3072 cells x U and W,
-#       read and written) and con2prim of all 20^3 cells (U and r, theta in,
-#       W out)
-#   fluxcomp: per direction, the primitives and (r, theta) of the 20x16x16
-#       stencil cells, the normal face B and the 8 flux components of the
-#       17x16x16 faces
-#   update: per interior cell, 3 faces x 8 flux components, W, U and dU read,
-#       U and dU written, 3 face B, (r, theta); per shell cell W.B and U.B
-#   floors: per interior cell U, W, (r, theta) read, W written
-def alg_bytes(call, npatch):
-    per = {
-        "ghosts_prims": 3072 * 16 * 8 * 2 + 8000 * (8 + 2 + 8) * 8,
-        "fluxcomp": 3 * ((20 * 16 * 16) * (8 + 2) * 8 + (17 * 16 * 16) * 8 + (17 * 16 * 16) * 8 * 8),
-        "update": 4096 * (24 + 8 + 8 + 8 + 8 + 8 + 3 + 2) * 8 + (6859 - 4096) * (3 + 6) * 8,
-        "floors": 4096 * (8 + 8 + 2 + 8) * 8,
-    }
-    return per[call] * npatch
+def timed_steps(g, K, W, dist, clocks_bus=None):
+    """ms per step of K graph replays after W warm-up replays (max over ranks)."""
+    import torch
+    g.capture()
+    for _ in range(W):
+        g.replay()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ck = Clocks(clocks_bus) if clocks_bus is not None else None
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(K):
+        g.replay()
+    b.record()
+    torch.cuda.synchronize()
+    clocks = ck.stop() if ck else None
+    t = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    g.release_graph()
+    return float(t.item()) / K, clocks
 
 
-E2E_DEPTH = 3      # device trees of the end-to-end pipeline
-STEP_BYTES = 296   # algorithmic HBM bytes per zone-update of a whole RK2 step
+def piece_ms(g, reps=5):
+    """CUDA-event ms of each launch of a stage (stage 0 and 1 averaged)."""
+    import torch
+    out = {}
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name in ("prims", "ghosts", "fluxes", "update"):
+        ts = []
+        for stage in (0, 1):
+            fn = {"prims": lambda: g.prims(stage, stage == 0), "ghosts": lambda: g.ghosts(stage),
+                  "fluxes": lambda: g.fluxes(stage), "update": lambda: g.update(stage)}[name]
+            fn()
+            torch.cuda.synchronize()
+            a.record()
+            for _ in range(reps):
+                fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b) / reps)
+        out[name] = sum(ts) / 2
+    return out
 
-# DRAM bytes (read + write) per launch from the ncu capture of the 64^3 box
-# (profiles/kernels_magnetised_box_64cube.md, fp64-fma; stage 0 and stage 1
-# averaged; a call's kernels summed; the flux kernel at the launch bound the
-# tuner picks on B200, whose register spills add traffic).  The 128^3 figures scale them by the
-# patch count (x8): every launch touches each patch's arrays once, so
-# traffic grows in proportion to the patches.
-_T64 = {"fluxcomp": (16.40 + 0.00 + 128.76 + 69.04) * 1e6,   # k_flux_aux at 6 CTAs/SM, the tuner's choice
-        "ghosts_prims": (46.74 + 6.01 + 36.53 + 1.27 + 65.04 + 14.74) * 1e6,
-        "update": (102.38 + 17.20) * 1e6,
-        "floors": (49.86 + 5.34) * 1e6}
-TRAFFIC = {**{(k, 64): v for k, v in _T64.items()}, **{(k, 128): 8 * v for k, v in _T64.items()}}
+
+def alg_bytes(piece, n, wb):
+    """Algorithmic HBM bytes of one launch over one n^3 block (each value the
+    launch must read or write, once); wb = bytes per primitive/flux value:
+      prims:  U (5) and the face field (3) in, the previous primitives (5)
+              in, primitives (8) and the cell field of U (3) out
+      ghosts: 8 primitives and 3 face values per ghost cell, in and out
+      fluxes: primitives of the (n+4)^3 stencil box; per face of the
+              3 (n+1)(n+2)^2 the normal face field in and 8 flux components out
+      update: 24 flux components, 8 primitives, U (and U1 at stage 1: 7.5
+              values on average) in, 5 conserved out; 3 face values in and
+              out"""
+    cells, ghost = n ** 3, (n + 4) ** 3 - n ** 3
+    faces = 3 * (n + 1) * (n + 2) ** 2
+    if piece == "prims":
+        return cells * ((5 + 3 + 3) * 8 + (5 + 8) * wb)
+    if piece == "ghosts":
+        return ghost * 2 * (8 * wb + 3 * 8)
+    if piece == "fluxes":
+        return (n + 4) ** 3 * 8 * wb + faces * (8 + 8 * wb)
+    if piece == "update":
+        return cells * (24 * wb + 8 * wb + 7.5 * 8 + 5 * 8 + 6 * 8)
+    raise KeyError(piece)
 
 
-def cpu_reference_sample(threads):
-    """The reference's own rk2integrator::step on a 64^3 box (4^3 patches),
-    all host threads; returns (zone-updates/s, kind, sample)."""
+def accuracy(args, steps):
+    """plain FP64 and mixed from the same initial data, `steps` steps each"""
     import numpy as np
+    import torch
+    from bhgpu.fixed import FxGrid, FxParams
+    ref, _ = torus_grid(args, "fp64")
+    mix = FxGrid(ref.blocks_np, ref.nbr_np, FxParams(precision="mixed"))
+    mix.copy_state_from(ref)
+    ref.capture()
+    mix.capture()
+    for _ in range(steps):
+        ref.replay()
+        mix.replay()
+    torch.cuda.synchronize()
+    ref.release_graph()
+    mix.release_graph()
+    a, b = mix.interior(mix.U), ref.interior(ref.U)
+    fields = {"D": [0], "S": [1, 2, 3], "tau": [4], "B": [5, 6, 7]}
+    out = {"steps": steps, "finite": bool(np.isfinite(a).all() and np.isfinite(b).all()),
+           "rel_l1": {k: float(np.abs(a[c] - b[c]).sum() / np.abs(b[c]).sum()) for k, c in fields.items()},
+           "rel_linf": {k: float(np.abs(a[c] - b[c]).max() / np.abs(b[c]).max()) for k, c in fields.items()},
+           "div_B_rel": {"fp64": ref.divb(), "mixed": mix.divb()},
+           "c2p_failures": {"fp64": ref.counters()["c2p_failures"], "mixed": mix.counters()["c2p_failures"]},
+           "torus_rho_max": float(ref.interior(ref.W)[0].max())}
+    out["max_rel_l1"] = max(out["rel_l1"].values())
+    out["within_1e-5"] = out["max_rel_l1"] <= 1e-5
+    del ref, mix
+    torch.cuda.empty_cache()
+    return out
+
+
+def e2e_measure(args, g0, dist):
+    import torch
+    from bhgpu.fixed import FxGrid, FxHostPipeline
+    pin = lambda x: x.cpu().pin_memory()
+    hU, hW, hB = pin(g0.U), pin(g0.W), pin(g0.Bf)
+    grids = [g0] + [FxGrid(g0.blocks_np, g0.nbr_np, g0.params) for _ in range(E2E_DEPTH - 1)]
+    outs = [tuple(torch.empty_like(x).pin_memory() for x in (hU, hW, hB)) for _ in range(E2E_DEPTH)]
+
+    def run(pipe, nstep):
+        for i in range(len(pipe.grids)):
+            pipe.submit(hU, hW, hB, *outs[i])
+        pipe.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(pipe.s_in)
+        for i in range(nstep):
+            pipe.submit(hU, hW, hB, *outs[i % len(pipe.grids)])
+        b.record(pipe.s_out)
+        torch.cuda.synchronize()
+        t = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()) / nstep
+
+    ms = run(FxHostPipeline(grids), args.e2e_steps)
+    ms_serial = run(FxHostPipeline(grids[:1]), max(3, args.e2e_steps // 3))
+    nbytes = sum(x.numel() * x.element_size() for x in (hU, hW, hB))
+    del grids
+    return ms, ms_serial, nbytes
+
+
+def cpu_port_sample(args, threads, steps):
+    """The CPU port of the scheme (oracle/bh_fixed.c, OpenMP) on the same
+    torus: zone-updates/s over `steps` steps after one warm-up step."""
+    import oracle
+    from oracle import fixed as ofx
+    from bhgrid.blocks import uniform_blocks
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    oracle.build(ref=False)
+
+    class _P:
+        M, a, gamma, cfl, rho_floor, u_floor, sigma_max, W_max = 1.0, 0.9375, GAMMA, CFL, 1e-6, 1e-8, 100.0, 50.0
+        r_exc, tol, maxiter, limiter = None, 1e-12, 30, "vanleer"
+    blocks, nbr = uniform_blocks(LO, HI, args.grid, args.block)
+    h = ofx.FxHost(blocks, nbr, ofx.params(_P))
+    h.torus_init(**TORUS)
+    h.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        h.step()
+    t = time.perf_counter() - t0
+    return args.grid ** 3 * steps / t, t / steps
+
+
+def reference_scheme_cpu(threads):
+    """The reference's own rk2integrator::step (oracle/_ref, its OpenMP
+    loops) on the 64^3 magnetised box it can run (outflow, van Leer)."""
     import oracle
     from bhgrid import configs
     from bhgrid.mesh import Quilt
+    if not oracle.ref_available():
+        return {"unavailable": "the reference harness (oracle/_ref) is not built on this host"}
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    q = Quilt([LO] * 3, [HI] * 3, 4, periodic=False)
+    q = Quilt([10.0] * 3, [12.0] * 3, 4, periodic=False)
     W, Bf = configs.magnetised_box(q, seed=1, gamma=GAMMA)
     orc = oracle.Oracle(0.0, 0.0, 0.0, GAMMA, limiter=1)
     hp = oracle.HostPool(q.tables())
     orc.geometry(hp)
-    hp.W[:] = W; hp.Bf[:] = Bf
+    hp.W[:] = W
+    hp.Bf[:] = Bf
     for p in range(hp.npatch):
         hp.U[p] = orc.ptoc(W[p], hp.rth[p, 0], hp.rth[p, 1])[0]
-    zones = 64 ** 3
-    if oracle.ref_available():
-        ref = oracle.RefSolver([LO] * 3, [HI] * 3, 4, 0.0, 0.0, 0.0, GAMMA)
-        times = []
-        for _ in range(3):
-            ref.put(hp)
-            t0 = time.perf_counter()
-            ref.step_native(CFL)
-            times.append(time.perf_counter() - t0)
-        t = statistics.median(times)
-        return zones / t, "reference", ("reference rk2integrator::step (its own OpenMP loops, outflow ghosts, "
-                                        f"van Leer) on the 64^3 box, median of 3 steps from the initial state, "
-                                        f"{t:.2f} s/step")
+    ref = oracle.RefSolver([10.0] * 3, [12.0] * 3, 4, 0.0, 0.0, 0.0, GAMMA)
     times = []
     for _ in range(3):
-        h = hp.copy()
+        ref.put(hp)
         t0 = time.perf_counter()
-        orc.step(h, CFL)
+        ref.step_native(CFL)
         times.append(time.perf_counter() - t0)
     t = statistics.median(times)
-    return zones / t, "port", f"C restatement step on the 64^3 box, median of 3 steps, {t:.2f} s/step"
+    return {"value": 64 ** 3 / t, "unit": METRIC, "cores": threads, "kind": "reference",
+            "sample": "the reference's own rk2integrator::step on the 64^3 magnetised box it can run "
+                      f"(outflow, van Leer), median of 3 steps from the initial state, {t:.2f} s/step"}
+
+
+def faithful_gpu(steps=20):
+    """The reference-faithful FP64 path (bhgpu.RK2Integrator, the reference's
+    own arithmetic) on the 128^3 magnetised box, each step restarted."""
+    import torch
+    import bhgpu
+    from bhgrid import configs
+    from bhgrid.mesh import Quilt
+    q = Quilt([10.0] * 3, [12.0] * 3, 8, periodic=True)
+    tree = bhgpu.AmrTree(q.dom_l, q.dom_h, 8, M=0.0, a=0.0, Q=0.0, gm=GAMMA, periodic=True, limiter="minmod",
+                         quilt=q, init_floor=False, precision="fp64")
+    W, Bf = configs.magnetised_box(q, seed=1, gamma=GAMMA)
+    tree.load(W=W, Bf=Bf)
+    tree.prim_to_cons()
+    U0, W0, B0 = tree.U.clone(), tree.W.clone(), tree.Bf.clone()
+    rk = bhgpu.RK2Integrator(CFL)
+
+    def one():
+        tree.U.copy_(U0)
+        tree.W.copy_(W0)
+        tree.Bf.copy_(B0)
+        rk.step(tree, sync=False, check_domain=False)
+    for _ in range(3):
+        one()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        one()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    tree.clear_error()
+    return {"workload": "magnetised box 128^3 (flat, periodic, PLM minmod + the reference's HLLD + CT), "
+                        "reference-faithful FP64 (the reference's roundings), each step restarted",
+            "ms_per_step": ms, "zone_updates_per_s": 128 ** 3 / (ms / 1e3)}
 
 
 # ---------------------------------------------------------------------------
@@ -234,7 +381,7 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
     import numpy as np
     import torch
     import bhgpu
-    from bhgpu import configs
+    from bhgrid import configs
     W, r, th = configs.con2prim_batch(n_cells, seed=4, gamma=GAMMA, a=0.9375)
     mtr, stt = bhgpu.Metric(1.0, 0.9375, 0.0), bhgpu.State(GAMMA)
     cn = bhgpu.Conserved(mtr, stt)
@@ -323,7 +470,7 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
         import oracle
         if oracle.ref_available():
             ns = 1 << 16
-            ref = oracle.RefSolver([LO] * 3, [HI] * 3, 1, 1.0, 0.9375, 0.0, GAMMA)
+            ref = oracle.RefSolver([10.0] * 3, [12.0] * 3, 1, 1.0, 0.9375, 0.0, GAMMA)
             Us = U[:, :ns].cpu().numpy()
             t0 = time.perf_counter()
             ref.ctop(Us, r[:ns], th[:ns])
@@ -334,342 +481,35 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
         out["cpu_reference"] = {"error": str(e)}
     return out
 
-
-# ---------------------------------------------------------------------------
-# AMR regrid: one amrtree::regrid of the floor state around a Schwarzschild
-# hole (64^3 in 4^3 patches over [-16,16]^3: the 8 central patches hold
-# cells inside r = 3 and refine), and the refinement test alone on the
-# headline box, where nothing changes (the reference regrids after every step)
-def regrid_bench(tree):
-    import torch
-    import bhgpu
-    from bhgpu.mesh import Quilt
-    q = Quilt([-16.0] * 3, [16.0] * 3, 4)
-    t = bhgpu.AmrTree(q.dom_l, q.dom_h, 4, M=1.0, a=0.0, Q=0.0, gm=GAMMA, limiter="vanleer", quilt=q)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    plan = t.regrid(check_domain=False)
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    n_after = t.npatch
-    del t
-    flags = torch.zeros(tree.npatch, dtype=torch.uint8, device="cuda")
-    P = tree.params()
-    from bhgpu.solver import _p, _stream
-    L = bhgpu.lib
-    for _ in range(2):
-        L.bh_regrid_flags(C.byref(P), C.byref(tree.pool), _p(tree.lvl), _p(flags), _stream())
-    a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(10):
-        L.bh_regrid_flags(C.byref(P), C.byref(tree.pool), _p(tree.lvl), _p(flags), _stream())
-    b.record(); torch.cuda.synchronize()
-    return {"workload": "floor state around a Schwarzschild hole, 64^3 in 4^3 patches over [-16,16]^3, "
-                        "one amrtree::regrid (flags on the device, bookkeeping on the host, refine on the device)",
-            "patches_before": 64, "patches_after": n_after, "refined": len(plan.refined),
-            "ms_wall": (t1 - t0) * 1e3,
-            "refinement_test_ms": a.elapsed_time(b) / 10,
-            "refinement_test_workload": f"the headline box ({tree.npatch} patches), nothing refines"}
-
-
-# ---------------------------------------------------------------------------
-# diagnostics: analysis::analyser's bundle_ (what the reference's main()
-# prints after every step) and batch_ on the headline box after a step, and
-# the reference's own analyser on the 64^3 CPU sample
-def analysis_bench(tree):
-    import torch
-    import bhgpu
-    rk = bhgpu.RK2Integrator(CFL)
-    rk.step(tree, check_domain=False)      # floors records the derived fields
-    an = bhgpu.Analyser()
-    for _ in range(2):
-        an.bundle_(tree, 0.0)
-    torch.cuda.synchronize()
-    out = {"workload": f"analysis::analyser on the headline box ({tree.npatch} patches) after one step"}
-    for name, fn in (("bundle_ms", an.bundle_), ("batch_ms", an.batch_)):
-        t0 = time.perf_counter()
-        for _ in range(10):
-            fn(tree, 0.0)
-        out[name] = (time.perf_counter() - t0) * 100.0
-    tree.clear_error()
-    try:
-        import oracle
-        if oracle.ref_available():
-            from bhgpu import configs
-            from bhgpu.mesh import Quilt
-            q = Quilt([LO] * 3, [HI] * 3, 4, periodic=False)
-            W, Bf = configs.magnetised_box(q, seed=1, gamma=GAMMA)
-            orc = oracle.Oracle(0.0, 0.0, 0.0, GAMMA, limiter=1)
-            hp = oracle.HostPool(q.tables())
-            orc.geometry(hp)
-            hp.W[:] = W; hp.Bf[:] = Bf
-            for p in range(hp.npatch):
-                hp.U[p] = orc.ptoc(W[p], hp.rth[p, 0], hp.rth[p, 1])[0]
-            ref = oracle.RefSolver([LO] * 3, [HI] * 3, 4, 0.0, 0.0, 0.0, GAMMA)
-            ref.put(hp)
-            ref.step_native(CFL)
-            t0 = time.perf_counter(); ref.bundle(0.0); t1 = time.perf_counter(); ref.batch(0.0); t2 = time.perf_counter()
-            out["cpu_reference"] = {"bundle_ms": (t1 - t0) * 1e3, "batch_ms": (t2 - t1) * 1e3,
-                                    "sample": "the reference's analyser on the 64^3 box (64 patches) after its step, "
-                                              "one thread (the reference's analyser is serial)"}
-    except Exception as e:      # the CPU figure is informational
-        out["cpu_reference"] = {"error": str(e)}
-    return out
-
-
-# ---------------------------------------------------------------------------
-# initial data: the Fishbone-Moncrief torus of the Kerr box (a = 0.9375,
-# 128^3 over [-40,40]^3 in 8^3 patches) by bh_torus_init, and the
-# reference's own initialisation of the 64^3 version on the host
-def torus_bench():
-    import torch
-    import bhgpu
-    from bhgpu.mesh import Quilt
-    q = Quilt([-40.0] * 3, [40.0] * 3, 8)
-    t = bhgpu.AmrTree(q.dom_l, q.dom_h, 8, M=1.0, a=0.9375, Q=0.0, gm=GAMMA, quilt=q, init_floor=False)
-    t.torus_init()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    s = t.torus_init()
-    torch.cuda.synchronize()
-    out = {"workload": "Fishbone-Moncrief torus initial data, Kerr a=0.9375, 128^3 over [-40,40]^3 (512 patches)",
-           "ms": (time.perf_counter() - t0) * 1e3, "l0": s["l0"], "rho_max": s["rho_max"]}
-    del t
-    try:
-        out["step"] = torus_step_bench()
-    except Exception as e:      # informational
-        out["step"] = {"error": str(e)}
-    try:
-        import oracle
-        if oracle.ref_available():
-            ref = oracle.RefSolver([-40.0] * 3, [40.0] * 3, 4, 1.0, 0.9375, 0.0, GAMMA)
-            t0 = time.perf_counter()
-            ref.torus_init()
-            out["cpu_reference"] = {"ms": (time.perf_counter() - t0) * 1e3,
-                                    "sample": "the reference's fm_init + B_pot_init + ptoc, 64^3 (64 patches), "
-                                              "one thread (serial loops)"}
-    except Exception as e:      # the CPU figure is informational
-        out["cpu_reference"] = {"error": str(e)}
-    return out
-
-
-def torus_step_bench(steps=20, free_steps=100):
-    """RK2 steps of the reference's scheme on the torus geometry of the
-    128^3 Kerr box (a = 0.9375, r_in = 6, r_max = 12, Gamma = 4/3, outflow,
-    van Leer), per arithmetic variant: each step from the initial data, and
-    a free run of free_steps steps compared with the faithful FP64 one.  The
-    reference itself stops in the first step (std::domain_error from its
-    EOS); the device records that in its error word and continues with the
-    fallback the reference's code reaches, so the steps run in full."""
-    import torch
-    import bhgpu
-    from bhgpu.mesh import Quilt
-    q = Quilt([-40.0] * 3, [40.0] * 3, 8)
-    t = bhgpu.AmrTree(q.dom_l, q.dom_h, 8, M=1.0, a=0.9375, Q=0.0, gm=GAMMA, quilt=q, init_floor=False)
-    t.torus_init(r_max=12.0, r_in=6.0)
-    torch.cuda.synchronize()
-    U0, W0, B0 = t.U.clone(), t.W.clone(), t.Bf.clone()
-    integ = bhgpu.RK2Integrator(CFL)
-    a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
-    out = {"workload": "reference scheme on the Kerr torus, a=0.9375, r_in=6, r_max=12, Gamma=4/3, 128^3 over "
-                       "[-40,40]^3 (512 patches), outflow, van Leer, CFL 0.4 (no beta normalisation, "
-                       "perturbation or excision: the reference has none)",
-           "zones": 128 ** 3}
-    res = {}
-    for prec in ("fp64", "fp64-fma", "mixed"):
-        t.precision = prec
-
-        def one():
-            t.U.copy_(U0); t.W.copy_(W0); t.Bf.copy_(B0)
-            integ.step(t, sync=False, check_domain=False)
-        for _ in range(3):
-            one()
-        torch.cuda.synchronize()
-        t.clear_error()
-        a.record()
-        for _ in range(steps):
-            one()
-        b.record(); torch.cuda.synchronize()
-        ms = a.elapsed_time(b) / steps
-        res[prec] = {"ms_per_step": ms, "value": 128 ** 3 / (ms / 1e3), "dt": float(t.dt.item()),
-                     "domain_error_flagged": bool(t.read_error() & 1),
-                     "nan_frac_U": float((~torch.isfinite(t.U)).double().mean().item()), "U": t.U.clone()}
-    for prec in ("fp64-fma", "mixed"):
-        res[prec]["l1_vs_fp64_1_step"] = field_l1(res[prec]["U"], res["fp64"]["U"])
-        res[prec]["speedup_vs_plain_fp64"] = res["fp64"]["ms_per_step"] / res[prec]["ms_per_step"]
-    for prec in res:
-        del res[prec]["U"]
-    out["restarted_steps"] = res
-    free = {}
-    for prec in ("fp64", "fp64-fma", "mixed"):
-        t.precision = prec
-        t.U.copy_(U0); t.W.copy_(W0); t.Bf.copy_(B0)
-        t.clear_error()
-        torch.cuda.synchronize()
-        a.record()
-        for _ in range(free_steps):
-            integ.step(t, sync=False, check_domain=False)
-        b.record(); torch.cuda.synchronize()
-        ms = a.elapsed_time(b) / free_steps
-        divb = t.maxdivb()
-        fin = torch.isfinite(divb)
-        free[prec] = {"ms_per_step": ms, "value": 128 ** 3 / (ms / 1e3),
-                      "max_divB": float(divb[fin].max().item()) if fin.any() else None,
-                      "nan_frac_U": float((~torch.isfinite(t.U)).double().mean().item()),
-                      "domain_error_flagged": bool(t.read_error() & 1), "U": t.U.clone()}
-    for prec in ("fp64-fma", "mixed"):
-        free[prec][f"l1_vs_fp64_{free_steps}_steps"] = field_l1(free[prec]["U"], free["fp64"]["U"])
-        free[prec]["speedup_vs_plain_fp64"] = free["fp64"]["ms_per_step"] / free[prec]["ms_per_step"]
-    for prec in free:
-        del free[prec]["U"]
-    out[f"free_run_{free_steps}_steps"] = free
-    # the divergence timeline: fp64 and mixed stepped side by side from the
-    # same initial data (untimed), NaN fraction of U and mixed-vs-fp64
-    # relative L1 on the entries finite in both, at checkpoints
-    t.precision = "fp64"
-    m = bhgpu.AmrTree(q.dom_l, q.dom_h, 8, M=1.0, a=0.9375, Q=0.0, gm=GAMMA, quilt=q, init_floor=False,
-                      precision="mixed")
-    t.U.copy_(U0); t.W.copy_(W0); t.Bf.copy_(B0)
-    m.U.copy_(U0); m.W.copy_(W0); m.Bf.copy_(B0)
-    timeline = []
-    for k in range(1, free_steps + 1):
-        integ.step(t, sync=False, check_domain=False)
-        integ.step(m, sync=False, check_domain=False)
-        if k in (1, 2, 3, 5, 10, 20, 50, 100):
-            l1 = field_l1(m.U, t.U)
-            timeline.append({"step": k, "nan_frac_U_fp64": float((~torch.isfinite(t.U)).double().mean().item()),
-                             "mixed_vs_fp64": l1})
-    out["divergence_timeline"] = timeline
-    del t, m
-    return out
-
-
-# ---------------------------------------------------------------------------
-FIELDS = {"D": [0], "S": [1, 2, 3], "tau": [4], "B": [5, 6, 7]}
-
-
-def field_l1(a, b):
-    """Relative L1 difference per conserved field of two [np][8][NC] states
-    (entries finite in both) and the fraction of entries whose NaN masks
-    disagree."""
-    import torch
-    out = {}
-    for name, comps in FIELDS.items():
-        x, y = a[:, comps], b[:, comps]
-        m = torch.isfinite(x) & torch.isfinite(y)
-        den = y[m].abs().mean().item() if m.any() else 0.0
-        num = (x[m] - y[m]).abs().mean().item() if m.any() else 0.0
-        out[name] = num / den if den > 0 else num
-    out["nan_mask"] = (torch.isfinite(a) != torch.isfinite(b)).double().mean().item()
-    return out
-
-
-def restart_ms(tree, prec, k, U0, W0, B0):
-    """ms per step of ``prec`` on ``tree``, each step restarted from (U0, W0,
-    B0) like the headline, CUDA events around k steps after 2 warm-up."""
-    import torch
-    import bhgpu
-    rk = bhgpu.RK2Integrator(CFL)
-    keep = tree.precision
-    tree.precision = prec
-
-    def one():
-        tree.U.copy_(U0); tree.W.copy_(W0); tree.Bf.copy_(B0)
-        rk.step(tree, sync=False, check_domain=False)
-    for _ in range(2):
-        one()
-    torch.cuda.synchronize()
-    a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(k):
-        one()
-    b.record(); torch.cuda.synchronize()
-    tree.precision = keep
-    tree.clear_error()
-    return a.elapsed_time(b) / k
-
-
-def variant_accuracy(tree, prec, steps, U0, W0, B0):
-    """``prec`` against the reference-faithful FP64 variant after ``steps``
-    steps from the same state of ``tree``."""
-    import bhgpu
-    rk = bhgpu.RK2Integrator(CFL)
-    res = {}
-    keep = tree.precision
-    for p in ("fp64", prec):
-        tree.precision = p
-        tree.U.copy_(U0); tree.W.copy_(W0); tree.Bf.copy_(B0)
-        for _ in range(steps):
-            rk.step(tree, check_domain=False)
-        res[p] = tree.U.clone()
-    tree.precision = keep
-    tree.clear_error()
-    return field_l1(res[prec], res["fp64"])
-
-
 # ---------------------------------------------------------------------------
 def run_reference(args):
+    """The reference arm: the same torus on the host cores.  The reference's
+    own scheme cannot step it (std::domain_error in its first stage), so the
+    timed implementation is the CPU port of the scheme this repository runs
+    on the GPU (oracle/bh_fixed.c), OpenMP over all host threads."""
     rank, _, world = env_rank()
     if rank != 0:
         return 0
-    import numpy as np
-    import oracle
-    from bhgrid import configs
-    from bhgrid.mesh import Quilt
     threads = os.cpu_count() or 1
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    nq = 4
-    q = Quilt([LO] * 3, [HI] * 3, nq, periodic=False)
-    W, Bf = configs.magnetised_box(q, seed=1, gamma=GAMMA)
-    orc = oracle.Oracle(0.0, 0.0, 0.0, GAMMA, limiter=1)
-    hp = oracle.HostPool(q.tables())
-    orc.geometry(hp)
-    hp.W[:] = W; hp.Bf[:] = Bf
-    for p in range(hp.npatch):
-        hp.U[p] = orc.ptoc(W[p], hp.rth[p, 0], hp.rth[p, 1])[0]
-    zones = (nq * 16) ** 3
-    if oracle.ref_available():
-        ref = oracle.RefSolver([LO] * 3, [HI] * 3, nq, 0.0, 0.0, 0.0, GAMMA)
-        kind = "reference"
-
-        def one():
-            ref.put(hp)
-            ref.step_native(CFL)
-    else:
-        kind = "port"
-
-        def one():
-            orc.step(hp.copy(), CFL)
-    for _ in range(args.warmup):
-        one()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        one()
-    t = time.perf_counter() - t0
-    value = zones * args.steps / t
-    sample = (f"each step: the {'reference rk2integrator::step' if kind == 'reference' else 'C restatement step'} "
-              f"on a 64^3 sample of the box (4^3 patches of 16^3, outflow ghosts, van Leer: the reference's "
-              f"own loop), restarted from the initial state")
+    nsteps = max(1, min(args.steps, 10))
+    value, s_per_step = cpu_port_sample(args, threads, nsteps)
+    sample = (f"each step: one RK2 step of the {args.grid}^3 torus by the CPU port of the corrected scheme "
+              f"(oracle/bh_fixed.c, {threads} OpenMP threads); {nsteps} of the {args.steps} steps timed "
+              f"after 1 warm-up step, {s_per_step:.2f} s/step")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)", "config": arm_config(args.grid, world),
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample},
-            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * s_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": arm_config(args, world),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's own rk2integrator::step cannot run this configuration (its EOS throws "
+                    "std::domain_error in the first stage, src/fluid/physics/thermo.cpp:11); "
+                    "reference_scheme times it on the box it can run",
+            "reference_scheme": reference_scheme_cpu(threads)}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def arm_config(grid, world):
-    """The workload both arms name (the reference arm times a bounded sample
-    of it, described in its cpu_baseline)."""
-    return {"workload": f"magnetised box {grid}^3: flat metric, periodic, PLM-minmod + HLLD + CT, RK2 CFL 0.4",
-            "grid": f"{grid}^3", "patches": (grid // 16) ** 3, "patch": "16^3 + 2 ghosts",
-            "parallelism": f"replicas x{world}", "l2": "working set > L2 (inputs and outputs larger than 126 MB)",
-            "restart": "each step restarts from the seeded state (D2D copy inside the timed region)"}
-
-
-# ---------------------------------------------------------------------------
 def run_ours(args):
     import torch
     rank, local_rank, world = env_rank()
@@ -679,245 +519,86 @@ def run_ours(args):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
-    import bhgpu
-    from bhgpu.solver import _p, _stream
+    from bhgpu import peaks
+    warm = max(args.warmup, 3)
+    props = torch.cuda.get_device_properties(local_rank)
+    bus = getattr(props, "pci_bus_id", None)
 
-    nq = args.grid // 16
-    tree = make_tree(nq, seed=1, precision=args.precision)
-    zones = (nq * 16) ** 3
-    # launch bounds of the heavy kernels: timed on this box, per variant
-    tuning = {}
-    if args.autotune == 1:
-        integ = bhgpu.RK2Integrator(CFL)
-        for prec in ("fp64", "fp64-fma", "mixed"):
-            tree.precision = prec
-            tuning[prec] = bhgpu.tune.autotune(tree, integ, reps=2, save=(rank == 0))
-        tree.precision = args.precision
-        tree.clear_error()
-    elif args.autotune == 2:
-        for prec in ("fp64", "fp64-fma", "mixed"):
-            choice = bhgpu.tune.load_tuning(prec)
-            if choice is None:
-                raise SystemExit(f"--autotune 2: no saved launch bounds for {prec} on this GPU")
-            tuning[prec] = {"choice": choice, "ms": {}}
-    U0, W0, B0 = tree.U.clone(), tree.W.clone(), tree.Bf.clone()
-    L = bhgpu.lib
-    P = tree.params()
-    pool = C.byref(tree.pool)
-    dtp = _p(tree.dt)
-    ev = {k: [] for k in ("ghosts_prims", "fluxcomp", "update", "floors")}
-    # my kernels per step: dt_init, dtcomp, 2 x (ghost_copy, ghost_prolong,
-    # prims_interior, prims_ghost, aux, flux, emf, bfupdate, update), floors
-    KL_PER_STEP = 21
-
-    def timed(name, record, fn):
-        if record:
-            a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
-            a.record(); fn(); b.record()
-            ev[name].append((a, b))
-        else:
-            fn()
-
-    def step(record=False):
-        s = _stream()
-        tree.U.copy_(U0); tree.W.copy_(W0); tree.Bf.copy_(B0)
-        L.bh_dtcomp(P, pool, CFL, dtp, s)
-        for stage in (0, 1):
-            timed("ghosts_prims", record, lambda: L.bh_ghosts_prims(P, pool, s))
-            timed("fluxcomp", record, lambda: L.bh_fluxcomp(P, pool, s))
-            L.bh_emfcomp(pool, s)
-            L.bh_bfupdate(pool, dtp, s)
-            timed("update", record, lambda: L.bh_update(P, pool, dtp, stage, s))
-        timed("floors", record, lambda: L.bh_floors(P, pool, s))
-
-    for _ in range(max(args.warmup, 3)):
-        step()
-    torch.cuda.synchronize()
-    tree.clear_error()
-    bus = None
-    try:
-        u = str(torch.cuda.get_device_properties(local_rank).uuid)
-        bus = u if u.startswith("GPU-") else "GPU-" + u
-    except Exception:
-        pass
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = Clocks(bus)
-    t_start = torch.cuda.Event(enable_timing=True); t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record()
-    for _ in range(args.steps):
-        step(record=True)
-    t_end.record()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ck = clocks.stop()
-    ms = t_start.elapsed_time(t_end)
-    call_ms = {k: [a.elapsed_time(b) for a, b in v] for k, v in ev.items()}
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    err = tree.read_error()
-    # constrained transport keeps div B at roundoff: the face-centred
-    # divergence (constrans::maxdivB) of the state the timed steps left (one
-    # step from the seeded state) and of the seeded state itself, raw and
-    # relative to max|B| / dx
-    divb_after = float(torch.nan_to_num(tree.maxdivb(), nan=0.0).max().item())
-    tree.U.copy_(U0); tree.W.copy_(W0); tree.Bf.copy_(B0)
-    divb_before = float(torch.nan_to_num(tree.maxdivb(), nan=0.0).max().item())
-    bscale = float(B0.abs().max().item()) / float(tree.tables["pgeo"][0, 3])
-    divb = {"max_initial": divb_before, "max_after_step": divb_after,
-            "relative_initial": divb_before / bscale, "relative_after_step": divb_after / bscale}
-
-    # ---- the other arithmetic variants, same workload, for comparison --------
+    # the headline: the mixed form
+    g, info = torus_grid(args, "mixed")
+    ms_mixed, clocks = timed_steps(g, args.steps, warm, dist, clocks_bus=bus or "")
+    counters = g.counters()
+    divb_after = g.divb()
+    pieces = {"mixed": piece_ms(g)}
+    ms_e2e, ms_e2e_serial, nbytes = e2e_measure(args, g, dist)
+    del g
+    torch.cuda.empty_cache()
     variants = {}
-    for prec in [p for p in ("fp64", "fp64-fma", "mixed") if p != args.precision]:
-        tree.precision = prec
-        P = tree.params()
-        for _ in range(2):
-            step()
-        torch.cuda.synchronize()
-        a0 = torch.cuda.Event(enable_timing=True); b0 = torch.cuda.Event(enable_timing=True)
-        k_other = max(10, args.steps // 4)
-        a0.record()
-        for _ in range(k_other):
-            step()
-        b0.record(); torch.cuda.synchronize()
-        vms = a0.elapsed_time(b0) / k_other
-        variants[prec] = {"ms_per_step": vms, "value": world * zones / (vms / 1e3),
-                          "dtype": "f32+f64" if prec == "mixed" else "f64"}
-    tree.precision = args.precision
-    P = tree.params()
-    fp64_ms = variants["fp64"]["ms_per_step"] if "fp64" in variants else ms_max / args.steps
-    for prec, v in variants.items():
-        v["speedup_vs_plain_fp64"] = fp64_ms / v["ms_per_step"]
-    # accuracy of the non-faithful variants against the faithful FP64 one
-    accuracy = {}
-    for prec in ("fp64-fma", "mixed"):
-        acc = {"magnetised_box_1_step": variant_accuracy(tree, prec, 1, U0, W0, B0)}
-        if prec == "mixed":
-            hyd = make_tree(4, seed=1, precision="fp64", B0=(0.0, 0.0, 0.0), amp=0.0)
-            acc["unmagnetised_box_64cube_5_steps"] = variant_accuracy(
-                hyd, prec, 5, hyd.U.clone(), hyd.W.clone(), hyd.Bf.clone())
-            del hyd
-        accuracy[prec] = acc
-        if prec in variants:
-            variants[prec]["accuracy_vs_fp64"] = acc
-
-    # ---- mixed against plain FP64 where the reference's answer is well
-    # conditioned: the unmagnetised box on the same 128^3 grid (B = 0), both
-    # variants timed the same way, the error after five steps
-    hyd = make_tree(nq, seed=1, precision="fp64", B0=(0.0, 0.0, 0.0), amp=0.0)
-    hU0, hW0, hB0 = hyd.U.clone(), hyd.W.clone(), hyd.Bf.clone()
-    k_h = max(10, args.steps // 4)
-    hyd_ms = {p_: restart_ms(hyd, p_, k_h, hU0, hW0, hB0) for p_ in ("fp64", "mixed")}
-    hyd_acc = variant_accuracy(hyd, "mixed", 5, hU0, hW0, hB0)
-    del hyd, hU0, hW0, hB0
-    l1_max = max(v_ for k_, v_ in hyd_acc.items() if k_ != "nan_mask")
-    mixed_vs_fp64 = {
-        "unmagnetised_box": {"workload": f"{args.grid}^3 box of the headline with B = 0",
-                             "fp64_ms_per_step": hyd_ms["fp64"], "mixed_ms_per_step": hyd_ms["mixed"],
-                             "speedup": hyd_ms["fp64"] / hyd_ms["mixed"], "l1_err_5_steps": hyd_acc,
-                             "within_1e-5": l1_max <= 1e-5},
-        "magnetised_box": {"workload": "the headline box",
-                           "fp64_ms_per_step": variants.get("fp64", {}).get("ms_per_step", ms_max / args.steps),
-                           "mixed_ms_per_step": variants["mixed"]["ms_per_step"] if "mixed" in variants
-                           else ms_max / args.steps,
-                           "l1_err_1_step": accuracy["mixed"]["magnetised_box_1_step"],
-                           "note": "the reference's own result moves by ~8e-3 (L1) under a 1e-7 input "
-                                   "perturbation on this state; the mixed error is of that size"},
-    }
-    mixed_vs_fp64["magnetised_box"]["speedup"] = (mixed_vs_fp64["magnetised_box"]["fp64_ms_per_step"] /
-                                                  mixed_vs_fp64["magnetised_box"]["mixed_ms_per_step"])
-
-    # ---- end to end through the public API with host buffers --------------
-    # bhgpu.HostPipeline over E2E_DEPTH device trees: every step uploads the
-    # state from pinned host memory, steps it and downloads the result; the
-    # upload of step n+1 and the download of step n-1 overlap the step n.
-    # The same API with one tree (each upload waits for the previous
-    # download) is timed beside it as the serial figure.
-    pin = lambda x: x.cpu().pin_memory()
-    hU, hW, hB = pin(U0), pin(W0), pin(B0)
-    rk = bhgpu.RK2Integrator(CFL)
-    trees = [tree] + [make_tree(nq, seed=1, precision=args.precision) for _ in range(E2E_DEPTH - 1)]
-    outs = [tuple(torch.empty_like(x).pin_memory() for x in (hU, hW, hB)) for _ in range(E2E_DEPTH)]
-
-    def e2e_run(pipe, nstep):
-        for i in range(len(pipe.trees)):          # warm-up: every tree once
-            pipe.submit(hU, hW, hB, *outs[i])
-        pipe.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
-        a.record(pipe.s_in)
-        for i in range(nstep):
-            pipe.submit(hU, hW, hB, *outs[i % len(pipe.trees)])
-        b.record(pipe.s_out)
-        torch.cuda.synchronize()
-        te = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        return float(te.item()) / nstep
-
-    e2e_ms = e2e_run(bhgpu.HostPipeline(trees, rk), args.e2e_steps)
-    e2e_serial_ms = e2e_run(bhgpu.HostPipeline(trees[:1], rk), max(3, args.e2e_steps // 3))
-    for t_ in trees:
-        t_.clear_error()
-    del trees
-    h2d = (hU.numel() + hW.numel() + hB.numel()) * 8
-    d2h = h2d
+    for prec in ("fp64", "fp64-fma"):
+        gv, _ = torus_grid(args, prec)
+        ms_v, _ = timed_steps(gv, args.steps, warm, dist)
+        variants[prec] = {"ms_per_step": ms_v, "zone_updates_per_s": world * args.grid ** 3 / (ms_v / 1e3)}
+        if prec == "fp64":
+            pieces["fp64"] = piece_ms(gv)
+        del gv
+        torch.cuda.empty_cache()
+    acc = accuracy(args, args.accuracy_steps)
+    if dist:
+        dist.barrier()
 
     if rank == 0:
-        value = world * zones * args.steps / (ms_max / 1e3)
+        zones = args.grid ** 3
+        value = world * zones / (ms_mixed / 1e3)
         peak, peak_kind = measured_peaks()
-        share = {k: sum(v) / ms for k, v in call_ms.items()}
-        # the dominant kernel: k_flux_aux, the largest single kernel of the
-        # step (its call adds k_aux, 6 % of it); the ghost-fill call has a
-        # similar share but is four kernels
-        top = "fluxcomp"
-        top_avg = statistics.mean(call_ms[top]) / 1e3
-        achieved = alg_bytes(top, tree.npatch) / top_avg / 1e9
+        fp64_tf, fp32_tf = peaks.fma_peak("fp64"), peaks.fma_peak("fp32")
+        nblk = (args.grid // args.block) ** 3
+        share = {k: v * 2 / ms_mixed for k, v in pieces["mixed"].items()}
+        top = max(pieces["mixed"], key=lambda k: pieces["mixed"][k])
+        top_ms = pieces["mixed"][top]
+        byts = alg_bytes(top, args.block, 4) * nblk
+        achieved = byts / (top_ms * 1e-3) / 1e9
+        kname = {"prims": "k_fx_c2p<float>", "ghosts": "k_fx_ghost<float>", "fluxes": "k_fx_flux<float,float,float>",
+                 "update": "k_fx_update<float,float,float>"}[top]
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
-            "data": "synthetic (seeded)",
-            "precision": args.precision,
-            "speedup_vs_plain_fp64": fp64_ms / (ms_max / args.steps),
-            "accuracy_vs_fp64": accuracy.get(args.precision, "identical roundings (the reference-faithful form)"),
+            "warmup": warm, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+            "precision": "mixed (reconstruction, fluxes, sources FP32; state, CT, con2prim, dt FP64)",
+            "config": arm_config(args, world),
+            "mixed_vs_plain_fp64": {"speedup": variants["fp64"]["ms_per_step"] / ms_mixed,
+                                    "speedup_vs_fp64_fma": variants["fp64-fma"]["ms_per_step"] / ms_mixed,
+                                    "accuracy_after_steps": acc},
             "variants": variants,
-            "mixed_vs_plain_fp64": mixed_vs_fp64,
-            "config": arm_config(args.grid, world),
-            "e2e": {"value": world * zones / (e2e_ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                    "api": f"bhgpu.HostPipeline, {E2E_DEPTH} device trees, pinned host U/W/Bf in and out every step",
-                    "serial_value": world * zones / (e2e_serial_ms / 1e3), "serial_ms_per_step": e2e_serial_ms},
-            "gpu_launches": KL_PER_STEP * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "k_flux_aux (+ k_aux): the fluxcomp call", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": TRAFFIC.get((top, args.grid)), "peak_source": peak_kind,
-                         "ms_per_launch": top_avg * 1e3,
+            "torus": {"ell": info["ell"], "field_scale": info["field_scale"], "beta": info["beta"],
+                      "div_B_rel_after_timed_steps": divb_after, "counters_after_timed_steps": counters},
+            "e2e": {"value": world * zones / (ms_e2e / 1e3), "unit": METRIC, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "ms_per_step": ms_e2e,
+                    "api": f"bhgpu.fixed.FxHostPipeline, {E2E_DEPTH} device grids, pinned host U/W/Bf in and "
+                           "out every step",
+                    "serial_value": world * zones / (ms_e2e_serial / 1e3), "serial_ms_per_step": ms_e2e_serial},
+            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "roofline": {"bound": "hbm", "kernel": f"{kname} ({top})", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "ms_per_launch": top_ms, "alg_bytes_per_launch": byts,
+                         "launch_ms": {k: {p: round(v, 5) for p, v in d.items()} for k, d in pieces.items()},
                          "step_share": {k: round(v, 4) for k, v in share.items()},
-                         "step_frac": value / world * STEP_BYTES / (peak * 1e9)},
-            "clocks": ck,
-            "device_error_word": err,
-            "div_B": divb,
-            "autotune": ({prec: {"choice_ctas_per_sm": t["choice"], "timed": bool(t["ms"]),
-                                 "step_ms_per_candidate": {k: {str(c): round(m, 4) for c, m in v.items()}
-                                                           for k, v in t["ms"].items()}}
-                          for prec, t in tuning.items()} if tuning else "off (compiled-in launch bounds)"),
+                         "step_frac": value / world * STEP_BYTES / (peak * 1e9),
+                         "fp_pipe_peaks_tflops": {"fp64": fp64_tf, "fp32": fp32_tf,
+                                                  "source": "bh_peak_fma on this GPU"}},
+            "clocks": clocks,
         }
         if world == 1:
             threads = os.cpu_count() or 1
-            v, kind, sample = cpu_reference_sample(threads)
-            line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample}
+            v, s_per = cpu_port_sample(args, threads, args.cpu_steps)
+            line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+                                    "sample": f"{args.cpu_steps} RK2 steps of the same {args.grid}^3 torus by the "
+                                              f"CPU port of the scheme (oracle/bh_fixed.c, OpenMP), "
+                                              f"{s_per:.2f} s/step"}
+            line["reference_scheme_cpu"] = reference_scheme_cpu(threads)
+            if args.faithful:
+                line["reference_faithful_gpu"] = faithful_gpu()
             if args.con2prim_batch:
-                line["con2prim_batch"] = con2prim_batch(args.con2prim_cells)
-            line["regrid"] = regrid_bench(tree)
-            line["analysis"] = analysis_bench(tree)
-            line["torus_init"] = torus_bench()
+                line["con2prim_batch"] = con2prim_batch()
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

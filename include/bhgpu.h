@@ -465,6 +465,14 @@ typedef struct bh_fx_torus {
 int bh_fx_torus_init(const bh_fx_params *P, const bh_fx_grid *g, const bh_fx_torus *T, double *scratch,
                      double *out, void *stream);
 
+/* ---- FMA throughput (no counterpart in the reference) -------------------
+ * n threads each run `iters` rounds of independent multiply-add chains in
+ * FP64 (precision BH_FP64, 8 chains) or FP32 (BH_MIXED, 16 chains) and
+ * write one value to out[n] (device, caller-allocated); *flops receives the
+ * floating-point operations issued (2 per multiply-add).  Timed by the
+ * caller, it gives the pipe peaks that bound the compute-heavy kernels. */
+int bh_peak_fma(int32_t precision, int32_t iters, void *out, int64_t n, int64_t *flops, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
