@@ -9,7 +9,7 @@ hole (M = 1, a = 0.9375) on a uniform Cartesian 128^3 grid over
 r_in = 6, r_max = 12, Gamma = 4/3, atmosphere rho = 1e-6 r^-3/2, a seeded 4 %
 pressure perturbation and a single field loop from A_phi ~ max(rho/rho_max -
 0.2, 0) normalised to plasma beta = 100 -- stepped with RK2 at CFL 0.4 by the
-corrected Valencia scheme (bhgpu.fixed: PLM van Leer, HLL fluxes in each
+corrected Valencia scheme (bhgpu.fixed: PLM with the MC limiter, HLL fluxes in each
 face's normal, analytic Kerr-Schild sources, constrained transport, Newton
 con2prim).  The reference's own scheme cannot run this configuration: it
 throws std::domain_error in its first stage (src/fluid/physics/thermo.cpp:11).
@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2, help="steps of the CPU port in cpu_baseline")
     ap.add_argument("--faithful", type=int, default=1, help="also time the reference-faithful FP64 path")
     ap.add_argument("--con2prim-batch", type=int, default=1, help="also measure the 2^24-cell con2prim batch")
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="choose the launch bounds of the heavy kernels on the torus first (bhgpu.fixed.autotune)")
     return ap.parse_args()
 
 
@@ -92,46 +94,61 @@ def measured_peaks():
 
 
 class Clocks:
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+    """nvidia-smi sampling of SM clocks and throttle reasons (every 50 ms);
+    summary() keeps the samples time-stamped inside a host-time window."""
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, bus_id: str | None):
-        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"]
-        if bus_id:
-            cmd += ["-i", bus_id]
+    def __init__(self, gpu_uuid: str | None):
+        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "50"]
+        if gpu_uuid:
+            cmd += ["-i", gpu_uuid]
         try:
             self.p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except Exception:
-            self.p = None
+        except Exception as e:
+            self.p, self.err = None, str(e)
 
-    def stop(self):
+    def stop(self, t0=None, t1=None):
         if self.p is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [f"nvidia-smi unavailable: {self.err}"]}
+        time.sleep(0.1)
         self.p.terminate()
         out, _ = self.p.communicate(timeout=10)
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in out.strip().splitlines():
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 7:
+            if len(f) < 8:
                 continue
             try:
-                sm.append(float(f[0])); mx.append(float(f[1]))
+                ts = time.mktime(time.strptime(f[0].split(".")[0], "%Y/%m/%d %H:%M:%S")) + float(
+                    "0." + f[0].split(".")[1]) if "." in f[0] else 0.0
+                rows.append((ts, float(f[1]), float(f[2]), f[4:8]))
             except ValueError:
                 continue
-            for n, v in zip(names, f[3:7]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [r for r in rows if t0 is not None and t0 - 0.05 <= r[0] <= t1 + 0.05]
+        window = "timed region" if inside else "whole sampling span (no sample inside the timed region)"
+        use = inside or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in use for n, v in zip(names, r[3]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median([r[1] for r in use]) if use else None,
+                "sm_max_mhz": max(r[2] for r in use) if use else None, "reasons": reasons,
+                "samples": len(use), "window": window}
+
+
+def gpu_uuid(dev):
+    import torch
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
 
 
 def arm_config(args, world):
     return {"workload": f"Kerr-Schild torus {args.grid}^3 (configuration 2): a=0.9375 over [-40,40]^3, "
                         "Fishbone-Moncrief r_in=6 r_max=12, Gamma=4/3, beta=100 single loop, 4% pressure noise, "
-                        "excision r<1.2 r_H; corrected Valencia scheme, PLM van Leer + HLL + CT, RK2 CFL 0.4",
+                        "excision r<1.2 r_H; corrected Valencia scheme, PLM MC + HLL + CT, RK2 CFL 0.4",
             "grid": f"{args.grid}^3", "blocks": (args.grid // args.block) ** 3,
             "block": f"{args.block}^3 + 2 ghosts", "parallelism": f"replicas x{world}",
             "l2": "working set > L2 (the 128^3 state, primitives and fluxes exceed 126 MB)",
@@ -146,23 +163,32 @@ def torus_grid(args, precision):
     return g, info
 
 
-def timed_steps(g, K, W, dist, clocks_bus=None):
-    """ms per step of K graph replays after W warm-up replays (max over ranks)."""
+def timed_steps(g, K, W, dist, clocks_uuid=False):
+    """ms per step of K graph replays after W warm-up replays (max over
+    ranks); with clocks_uuid the SM clocks are sampled during the K steps."""
     import torch
     g.capture()
+    ck = Clocks(clocks_uuid or None) if clocks_uuid is not False else None
     for _ in range(W):
         g.replay()
+    if ck is not None:       # let the sampler come up while the GPU keeps stepping
+        torch.cuda.synchronize()
+        t_w = time.time()
+        while time.time() - t_w < 0.4:
+            g.replay()
+            torch.cuda.synchronize()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    ck = Clocks(clocks_bus) if clocks_bus is not None else None
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.time()
     a.record()
     for _ in range(K):
         g.replay()
     b.record()
     torch.cuda.synchronize()
-    clocks = ck.stop() if ck else None
+    t1 = time.time()
+    clocks = ck.stop(t0, t1) if ck else None
     t = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -292,7 +318,7 @@ def cpu_port_sample(args, threads, steps):
 
     class _P:
         M, a, gamma, cfl, rho_floor, u_floor, sigma_max, W_max = 1.0, 0.9375, GAMMA, CFL, 1e-6, 1e-8, 100.0, 50.0
-        r_exc, tol, maxiter, limiter = None, 1e-12, 30, "vanleer"
+        r_exc, tol, maxiter, limiter = None, 1e-12, 30, "mc"
     blocks, nbr = uniform_blocks(LO, HI, args.grid, args.block)
     h = ofx.FxHost(blocks, nbr, ofx.params(_P))
     h.torus_init(**TORUS)
@@ -521,12 +547,15 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
     from bhgpu import peaks
     warm = max(args.warmup, 3)
-    props = torch.cuda.get_device_properties(local_rank)
-    bus = getattr(props, "pci_bus_id", None)
+    uuid = gpu_uuid(local_rank)
 
+    from bhgpu.fixed import autotune
+    tuning = {}
     # the headline: the mixed form
     g, info = torus_grid(args, "mixed")
-    ms_mixed, clocks = timed_steps(g, args.steps, warm, dist, clocks_bus=bus or "")
+    if args.autotune:
+        tuning["mixed"] = autotune(g)
+    ms_mixed, clocks = timed_steps(g, args.steps, warm, dist, clocks_uuid=uuid or "")
     counters = g.counters()
     divb_after = g.divb()
     pieces = {"mixed": piece_ms(g)}
@@ -536,6 +565,8 @@ def run_ours(args):
     variants = {}
     for prec in ("fp64", "fp64-fma"):
         gv, _ = torus_grid(args, prec)
+        if args.autotune:
+            tuning[prec] = autotune(gv)
         ms_v, _ = timed_steps(gv, args.steps, warm, dist)
         variants[prec] = {"ms_per_step": ms_v, "zone_updates_per_s": world * args.grid ** 3 / (ms_v / 1e3)}
         if prec == "fp64":
@@ -586,6 +617,10 @@ def run_ours(args):
                          "fp_pipe_peaks_tflops": {"fp64": fp64_tf, "fp32": fp32_tf,
                                                   "source": "bh_peak_fma on this GPU"}},
             "clocks": clocks,
+            "autotune": ({p: {"choice_ctas_per_sm": t["choice"],
+                              "step_ms_per_candidate": {k: {str(c): round(m, 4) for c, m in v.items()}
+                                                        for k, v in t["ms"].items()}}
+                          for p, t in tuning.items()} if tuning else "off (ptxas's own register choice)"),
         }
         if world == 1:
             threads = os.cpu_count() or 1

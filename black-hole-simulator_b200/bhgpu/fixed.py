@@ -81,7 +81,7 @@ class FxParams:
     r_exc: float | None = None     # default: 1.2 r_H
     tol: float = 1e-12
     maxiter: int = 30
-    limiter: str = "vanleer"
+    limiter: str = "mc"           # monotonized central: no division per slope
     precision: str = "fp64"
 
     def cstruct(self) -> BhFxParams:
@@ -296,3 +296,60 @@ class FxHostPipeline:
         for e in self._freed:
             if e is not None:
                 e.synchronize()
+
+
+# ---------------------------------------------------------------------------
+# launch-bound autotuning of the scheme's heavy kernels (bh_fx_tune_*)
+TUNE_KERNELS = ("c2p", "flux", "update")
+TUNE_CANDIDATES = (1, 3, 4, 5, 6)
+lib.bh_fx_tune_set.argtypes = [_i32, _i32, _i32]
+lib.bh_fx_tune_get.argtypes = [_i32, _i32, C.POINTER(_i32)]
+lib.bh_fx_tune_set.restype = C.c_int
+lib.bh_fx_tune_get.restype = C.c_int
+
+
+def tune_set(precision: str, kernel: str, ctas: int):
+    check(lib.bh_fx_tune_set(PRECISIONS[precision], TUNE_KERNELS.index(kernel), ctas), "bh_fx_tune_set")
+
+
+def tune_get(precision: str, kernel: str) -> int:
+    v = _i32()
+    check(lib.bh_fx_tune_get(PRECISIONS[precision], TUNE_KERNELS.index(kernel), C.byref(v)), "bh_fx_tune_get")
+    return int(v.value)
+
+
+def autotune(grid: FxGrid, reps: int = 4, candidates=TUNE_CANDIDATES) -> dict:
+    """Choose the launch bounds of con2prim, fluxes and update for the
+    grid's variant: for one kernel at a time (the others held), every
+    candidate times `reps` RK2 steps (CUDA events) from the same saved state;
+    the fastest is kept.  The grid's state is restored.  In the FP64 variant
+    every choice gives the same bits (no contraction); in the contracted
+    variants ptxas may pair multiply-adds differently under another register
+    budget, which moves results by ulps.  Returns {"choice": {kernel: ctas},
+    "ms": {kernel: {ctas: ms per step}}}."""
+    saved = [t.clone() for t in (grid.U, grid.W, grid.Bf)]
+    prec = grid.precision
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"choice": {}, "ms": {}}
+    for k in TUNE_KERNELS:
+        times = {}
+        for c in candidates:
+            tune_set(prec, k, c)
+            for t, s in zip((grid.U, grid.W, grid.Bf), saved):
+                t.copy_(s)
+            grid.step()
+            torch.cuda.synchronize()
+            a.record()
+            for _ in range(reps):
+                grid.step()
+            b.record()
+            torch.cuda.synchronize()
+            times[c] = a.elapsed_time(b) / reps
+        best = min(times, key=times.get)
+        tune_set(prec, k, best)
+        out["choice"][k] = best
+        out["ms"][k] = times
+    for t, s in zip((grid.U, grid.W, grid.Bf), saved):
+        t.copy_(s)
+    grid.reset_counters()
+    return out

@@ -219,6 +219,22 @@ int bh_fx_update(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void
     if (fx_bad(P, g) || stage < 0 || stage > 1) return BH_EINVAL;
     FX_DISPATCH(P, fx_update(P, g, stage, stream));
 }
+int bh_fx_tune_set(int32_t precision, int32_t kernel, int32_t ctas) {
+    switch (precision) {
+    case BH_FP64: return vfp64::fx_tune_set(kernel, ctas);
+    case BH_FP64_FMA: return vfma::fx_tune_set(kernel, ctas);
+    case BH_MIXED: return vmixed::fx_tune_set(kernel, ctas);
+    default: return BH_EINVAL;
+    }
+}
+int bh_fx_tune_get(int32_t precision, int32_t kernel, int32_t* ctas) {
+    switch (precision) {
+    case BH_FP64: return vfp64::fx_tune_get(kernel, ctas);
+    case BH_FP64_FMA: return vfma::fx_tune_get(kernel, ctas);
+    case BH_MIXED: return vmixed::fx_tune_get(kernel, ctas);
+    default: return BH_EINVAL;
+    }
+}
 int bh_fx_divb(const bh_fx_grid* g, double* out, void* stream) {
     if (!g || g->nblock <= 0 || !g->blocks || !g->Bf || !out || (g->nitem_cell > 0 && !g->items_cell)) return BH_EINVAL;
     return vfp64::fx_divb(g, out, stream);
@@ -287,7 +303,7 @@ int capture_graph(void* stream, bh_step_graph** out, Fn fn) {
 }
 
 int bh_step_graph_replay(bh_step_graph* g, void* stream) {
-    if (!g || !stream) return BH_EINVAL;
+    if (!g) return BH_EINVAL;
     return cudaGraphLaunch(g->exec, S(stream)) == cudaSuccess ? BH_OK : BH_ECUDA;
 }
 int bh_step_graph_destroy(bh_step_graph* g) {

@@ -62,6 +62,8 @@ inline bool bh_tune_valid(int32_t kernel, int32_t ctas) {
     int fx_step(const bh_fx_params*, const bh_fx_grid*, void*);                                               \
     int fx_divb(const bh_fx_grid*, double*, void*);                                                           \
     int fx_torus_init(const bh_fx_params*, const bh_fx_grid*, const bh_fx_torus*, double*, double*, void*);   \
+    int fx_tune_set(int32_t, int32_t);                                                                        \
+    int fx_tune_get(int32_t, int32_t*);                                                                       \
     }
 
 BH_VARIANT_API(vfp64)

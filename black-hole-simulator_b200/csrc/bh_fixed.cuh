@@ -85,8 +85,8 @@ __global__ void k_fx_dt_init(double* dt) {
 // (U, Bf for stage 0; U1, Bf1 for stage 1); stage 0 also reduces the CFL
 // limit into dt[0]
 // ======================================================================
-template <typename WT>
-__global__ void __launch_bounds__(FX_TPB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage, int with_dt) {
+template <typename RT, typename WT, int MINB>
+__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage, int with_dt) {
     const int32_t b = items[2 * blockIdx.x];
     const bh_fx_block B = G.blk[b];
     const int n = B.n;
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_c2p(FxPar P, Grid G, const int32_
         WT* W = (WT*)G.W;
         for (int v = 0; v < 5; v++) wo[v] = (double)W[v * N + c];
         int iters = 0;
-        int st = con2prim(P, m, u, Bc, wo, w, iters);
+        int st = con2prim<sizeof(RT) < sizeof(double)>(P, m, u, Bc, wo, w, iters);
         int rewrite = 0;
         if (st != 0) {
             // keep the previous primitives with the new field
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_c2p(FxPar P, Grid G, const int32_
         for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];
         if (with_dt) {
             double dx[3] = {B.dx, B.dx, B.dx};
-            dtc = cell_dt(P, m, w, dx);
+            dtc = cell_dt<RT>(P, m, w, dx);
         }
     }
     if (with_dt) {
@@ -252,10 +252,8 @@ __device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_bloc
     double x[3];
     cell_centre(B, i, j, k, x);
     x[d] -= 0.5 * B.dx;
-    KS mk;
-    ks_metric(P, x[0], x[1], x[2], mk);
     KSm<RT> m;
-    ks_cast(mk, m);
+    face_geometry<RT>(P, x, m);
     RT wL[8], wR[8];
     for (int v = 0; v < 8; v++) {
         if (v == P_B + d) continue;
@@ -265,7 +263,7 @@ __device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_bloc
     }
     // (the limiters keep every face value between its two cells' values, so
     // face densities and pressures stay positive)
-    RT Bn = RT(Bfs[d * N + c] / mk.sqrtgam);
+    RT Bn = RT(Bfs[d * N + c]) / m.sqrtgam;
     wL[P_B + d] = Bn;
     wR[P_B + d] = Bn;
     RT F[8];
@@ -274,8 +272,8 @@ __device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_bloc
     for (int v = 0; v < 8; v++) Fo[((int64_t)d * 8 + v) * N + c] = (FT)F[v];
 }
 
-template <typename RT, typename WT, typename FT>
-__global__ void __launch_bounds__(FX_TPB) k_fx_flux(FxPar P, Grid G, const int32_t* items, int stage) {
+template <typename RT, typename WT, typename FT, int MINB>
+__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux(FxPar P, Grid G, const int32_t* items, int stage) {
     const int32_t b = items[2 * blockIdx.x];
     const bh_fx_block B = G.blk[b];
     const int n = B.n, m = n + 2;
@@ -336,8 +334,8 @@ __device__ inline void face_update(const Grid& G, int d, int64_t c, int si, int 
         G.Bf[d * N + c] = 0.5 * (G.Bf[d * N + c] + G.Bf1[d * N + c] - dt * curl);
 }
 
-template <typename RT, typename WT, typename FT>
-__global__ void __launch_bounds__(FX_TPB) k_fx_update(FxPar P, Grid G, const int32_t* items, int stage,
+template <typename RT, typename WT, typename FT, int MINB>
+__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, const int32_t* items, int stage,
                                                       double cfl) {
     const int32_t b = items[2 * blockIdx.x];
     const bh_fx_block B = G.blk[b];
@@ -354,10 +352,9 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_update(FxPar P, Grid G, const int
     // source at the cell centre from the stage's primitives
     double x[3];
     cell_centre(B, i, j, k, x);
-    KS mk;
-    ks_metric(P, x[0], x[1], x[2], mk);
-    KSD dk;
-    ks_deriv(P, x[0], x[1], x[2], mk, dk);
+    KSb<RT> mk;
+    KSDb<RT> dk;
+    cell_geometry<RT>(P, x, mk, dk);
     const WT* W = (const WT*)G.W;
     RT w[8];
     for (int v = 0; v < 8; v++) w[v] = RT(W[v * N + c]);
@@ -606,12 +603,39 @@ inline cudaStream_t fxs(void* s) { return (cudaStream_t)s; }
 inline int fx_launched() { return cudaGetLastError() == cudaSuccess ? BH_OK : BH_ECUDA; }
 }  // namespace
 
+// launch bounds of the heavy kernels: resident 128-thread CTAs per SM asked
+// of ptxas (which caps registers per thread); 1 leaves the choice to ptxas.
+// Chosen per process and variant (bh_fx_tune_set), initially 1.
+int fx_tune_tab[BH_FX_TUNE_N] = {1, 1, 1};
+#define FX_TUNED(kernel, LAUNCH)                                                  \
+    switch (fx_tune_tab[kernel]) {                                                \
+    case 3: LAUNCH(3); break;                                                     \
+    case 4: LAUNCH(4); break;                                                     \
+    case 5: LAUNCH(5); break;                                                     \
+    case 6: LAUNCH(6); break;                                                     \
+    default: LAUNCH(1); break;                                                    \
+    }
+
+int fx_tune_set(int32_t kernel, int32_t ctas) {
+    if (kernel < 0 || kernel >= BH_FX_TUNE_N || !(ctas == 1 || (ctas >= 3 && ctas <= 6))) return BH_EINVAL;
+    fx_tune_tab[kernel] = ctas;
+    return BH_OK;
+}
+int fx_tune_get(int32_t kernel, int32_t* ctas) {
+    if (kernel < 0 || kernel >= BH_FX_TUNE_N || !ctas) return BH_EINVAL;
+    *ctas = fx_tune_tab[kernel];
+    return BH_OK;
+}
+
 int fx_prims(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t with_dt, void* s) {
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
     if (with_dt) fx::k_fx_dt_init<<<1, 1, 0, fxs(s)>>>(g->dt);
-    if (g->nitem_cell)
-        fx::k_fx_c2p<FRT><<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt);
+    if (g->nitem_cell) {
+#define L_(M) fx::k_fx_c2p<FRT, FRT, M><<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt)
+        FX_TUNED(BH_FX_TUNE_C2P, L_)
+#undef L_
+    }
     return fx_launched();
 }
 int fx_ghosts(const bh_fx_params*, const bh_fx_grid* g, int32_t stage, void* s) {
@@ -622,15 +646,21 @@ int fx_ghosts(const bh_fx_params*, const bh_fx_grid* g, int32_t stage, void* s) 
 int fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
-    if (g->nitem_pos)
-        fx::k_fx_flux<FRT, FRT, FRT><<<g->nitem_pos, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_pos, stage);
+    if (g->nitem_pos) {
+#define L_(M) fx::k_fx_flux<FRT, FRT, FRT, M><<<g->nitem_pos, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_pos, stage)
+        FX_TUNED(BH_FX_TUNE_FLUX, L_)
+#undef L_
+    }
     return fx_launched();
 }
 int fx_update(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
-    if (g->nitem_cell)
-        fx::k_fx_update<FRT, FRT, FRT><<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, P->cfl);
+    if (g->nitem_cell) {
+#define L_(M) fx::k_fx_update<FRT, FRT, FRT, M><<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, P->cfl)
+        FX_TUNED(BH_FX_TUNE_UPDATE, L_)
+#undef L_
+    }
     return fx_launched();
 }
 int fx_step(const bh_fx_params* P, const bh_fx_grid* g, void* s) {

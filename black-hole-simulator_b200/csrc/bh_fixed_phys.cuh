@@ -80,74 +80,83 @@ BH_HD inline float sqrt_(float x) { return sqrtf(x); }
 // ======================================================================
 // Kerr-Schild radius of a Cartesian point: the positive root of
 // r^4 - (R^2 - a^2) r^2 - a^2 z^2 = 0
-BH_HD inline double ks_r2(double a, double x, double y, double z) {
-    double a2 = a * a;
-    double d = x * x + y * y + z * z - a2;
-    return 0.5 * (d + sqrt(d * d + 4.0 * a2 * z * z));
+template <typename T>
+BH_HD inline T ks_r2(T a, T x, T y, T z) {
+    T a2 = a * a;
+    T d = x * x + y * y + z * z - a2;
+    return T(0.5) * (d + sqrt_(d * d + T(4) * a2 * z * z));
 }
 
-struct KS {
-    double H, l[3];            // H and the spatial part of l_mu (l_0 = 1)
-    double alpha, sqrtgam;     // lapse, sqrt(det gamma)
-    double beta[3];            // shift beta^i
-    double g[6], gi[6];        // gamma_ij and gamma^ij: xx, xy, xz, yy, yz, zz
-    double r;
+// The metric at a point, in the arithmetic type T (double everywhere but in
+// the mixed variant's face and source work away from the horizon)
+template <typename T>
+struct KSb {
+    T H, l[3];              // H and the spatial part of l_mu (l_0 = 1)
+    T alpha, sqrtgam;       // lapse, sqrt(det gamma)
+    T beta[3];              // shift beta^i
+    T g[6], gi[6];          // gamma_ij and gamma^ij: xx, xy, xz, yy, yz, zz
+    T r;
 };
+using KS = KSb<double>;
 BH_HD inline int sym(int i, int j) {   // index into the 6-entry symmetric storage
     int a = i < j ? i : j, b = i < j ? j : i;
     return a == 0 ? b : (a == 1 ? 2 + b : 5);
 }
 
-BH_HD inline void ks_metric(const FxPar& P, double x, double y, double z, KS& m) {
-    const double a = P.a, a2 = a * a;
-    double r2 = ks_r2(a, x, y, z);
-    double r = sqrt(r2);
-    double q = r2 * r2 + a2 * z * z;
+template <typename T>
+BH_HD inline void ks_metric(const FxPar& P, T x, T y, T z, KSb<T>& m) {
+    const T a = T(P.a), a2 = a * a;
+    T r2 = ks_r2(a, x, y, z);
+    T r = sqrt_(r2);
+    T q = r2 * r2 + a2 * z * z;
     // on the disc z = 0, x^2 + y^2 <= a^2 (r = 0) the metric is flat
-    double H = q > 0.0 ? P.M * r * r2 / q : 0.0;
-    double ir2a = 1.0 / (r2 + a2);
+    T H = q > T(0) ? T(P.M) * r * r2 / q : T(0);
+    T ir2a = T(1) / (r2 + a2);
     m.r = r;
     m.H = H;
     m.l[0] = (r * x + a * y) * ir2a;
     m.l[1] = (r * y - a * x) * ir2a;
-    m.l[2] = r > 0.0 ? z / r : 0.0;
-    double h2 = 2.0 * H, f = 1.0 + h2;
-    m.sqrtgam = sqrt(f);
-    m.alpha = 1.0 / m.sqrtgam;
-    double hf = h2 / f;
+    m.l[2] = r > T(0) ? z / r : T(0);
+    T h2 = T(2) * H, f = T(1) + h2;
+    m.sqrtgam = sqrt_(f);
+    m.alpha = T(1) / m.sqrtgam;
+    T hf = h2 / f;
     for (int i = 0; i < 3; i++) m.beta[i] = hf * m.l[i];
     for (int i = 0; i < 3; i++)
         for (int j = i; j < 3; j++) {
-            double ll = m.l[i] * m.l[j];
-            m.g[sym(i, j)] = (i == j ? 1.0 : 0.0) + h2 * ll;
-            m.gi[sym(i, j)] = (i == j ? 1.0 : 0.0) - hf * ll;
+            T ll = m.l[i] * m.l[j];
+            m.g[sym(i, j)] = (i == j ? T(1) : T(0)) + h2 * ll;
+            m.gi[sym(i, j)] = (i == j ? T(1) : T(0)) - hf * ll;
         }
 }
 
 // first derivatives: dH[k] = d_k H, dl[k][i] = d_k l_i (d_k l_0 = 0)
-struct KSD {
-    double dH[3], dl[3][3];
+template <typename T>
+struct KSDb {
+    T dH[3], dl[3][3];
 };
-BH_HD inline void ks_deriv(const FxPar& P, double x, double y, double z, const KS& m, KSD& d) {
-    const double a = P.a, a2 = a * a, r = m.r, r2 = r * r;
-    double q = r2 * r2 + a2 * z * z;
-    if (!(q > 0.0) || !(r > 0.0)) {
+using KSD = KSDb<double>;
+template <typename T>
+BH_HD inline void ks_deriv(const FxPar& P, T x, T y, T z, const KSb<T>& m, KSDb<T>& d) {
+    const T a = T(P.a), a2 = a * a, r = m.r, r2 = r * r;
+    T q = r2 * r2 + a2 * z * z;
+    if (!(q > T(0)) || !(r > T(0))) {
         for (int k = 0; k < 3; k++) {
-            d.dH[k] = 0.0;
-            for (int i = 0; i < 3; i++) d.dl[k][i] = 0.0;
+            d.dH[k] = T(0);
+            for (int i = 0; i < 3; i++) d.dl[k][i] = T(0);
         }
         return;
     }
-    double iq = 1.0 / q, r3 = r2 * r;
-    double dr[3] = {x * r3 * iq, y * r3 * iq, z * r * (r2 + a2) * iq};
-    double ir2a = 1.0 / (r2 + a2);
+    T iq = T(1) / q, r3 = r2 * r;
+    T dr[3] = {x * r3 * iq, y * r3 * iq, z * r * (r2 + a2) * iq};
+    T ir2a = T(1) / (r2 + a2);
     for (int k = 0; k < 3; k++) {
-        double dq = 4.0 * r3 * dr[k] + (k == 2 ? 2.0 * a2 * z : 0.0);
-        d.dH[k] = P.M * (3.0 * r2 * dr[k] * q - r3 * dq) * iq * iq;
-        double t = 2.0 * r * dr[k];
-        d.dl[k][0] = (dr[k] * x + (k == 0 ? r : 0.0) + (k == 1 ? a : 0.0) - m.l[0] * t) * ir2a;
-        d.dl[k][1] = (dr[k] * y + (k == 1 ? r : 0.0) - (k == 0 ? a : 0.0) - m.l[1] * t) * ir2a;
-        d.dl[k][2] = ((k == 2 ? 1.0 : 0.0) - m.l[2] * dr[k]) / r;
+        T dq = T(4) * r3 * dr[k] + (k == 2 ? T(2) * a2 * z : T(0));
+        d.dH[k] = T(P.M) * (T(3) * r2 * dr[k] * q - r3 * dq) * iq * iq;
+        T t = T(2) * r * dr[k];
+        d.dl[k][0] = (dr[k] * x + (k == 0 ? r : T(0)) + (k == 1 ? a : T(0)) - m.l[0] * t) * ir2a;
+        d.dl[k][1] = (dr[k] * y + (k == 1 ? r : T(0)) - (k == 0 ? a : T(0)) - m.l[1] * t) * ir2a;
+        d.dl[k][2] = ((k == 2 ? T(1) : T(0)) - m.l[2] * dr[k]) / r;
     }
 }
 
@@ -156,8 +165,8 @@ template <typename RT>
 struct KSm {
     RT alpha, sqrtgam, beta[3], g[6], gi[6];
 };
-template <typename RT>
-BH_HD inline void ks_cast(const KS& m, KSm<RT>& o) {
+template <typename RT, typename T>
+BH_HD inline void ks_cast(const KSb<T>& m, KSm<RT>& o) {
     o.alpha = RT(m.alpha); o.sqrtgam = RT(m.sqrtgam);
     for (int i = 0; i < 3; i++) o.beta[i] = RT(m.beta[i]);
     for (int i = 0; i < 6; i++) { o.g[i] = RT(m.g[i]); o.gi[i] = RT(m.gi[i]); }
@@ -175,7 +184,7 @@ BH_HD inline void lower(const RT* g, const RT* v, RT* o) {
 // Derived quantities of a primitive state at a point.
 template <typename RT>
 struct Derived {
-    RT W, v[3], vl[3], Bl[3], B2, Bv, b2, rhohW2, ptot;
+    RT W, iW, rhoh, v[3], vl[3], Bl[3], B2, Bv, b2, rhohW2, ptot;
 };
 template <typename RT>
 BH_HD inline void derive(const KSm<RT>& m, RT gamma, const RT* w, Derived<RT>& d) {
@@ -186,12 +195,14 @@ BH_HD inline void derive(const KSm<RT>& m, RT gamma, const RT* w, Derived<RT>& d
     RT u2 = utl[0] * ut[0] + utl[1] * ut[1] + utl[2] * ut[2];
     d.W = sqrt_(RT(1) + u2);
     RT iW = RT(1) / d.W;
+    d.iW = iW;
     for (int i = 0; i < 3; i++) { d.v[i] = ut[i] * iW; d.vl[i] = utl[i] * iW; }
     lower(m.g, B, d.Bl);
     d.B2 = d.Bl[0] * B[0] + d.Bl[1] * B[1] + d.Bl[2] * B[2];
     d.Bv = d.Bl[0] * d.v[0] + d.Bl[1] * d.v[1] + d.Bl[2] * d.v[2];
     d.b2 = d.B2 * iW * iW + d.Bv * d.Bv;
     RT rhoh = w[P_RHO] + gamma / (gamma - RT(1)) * w[P_PRS];
+    d.rhoh = rhoh;
     d.rhohW2 = rhoh * d.W * d.W;
     d.ptot = w[P_PRS] + RT(0.5) * d.b2;
 }
@@ -199,7 +210,7 @@ BH_HD inline void derive(const KSm<RT>& m, RT gamma, const RT* w, Derived<RT>& d
 template <typename RT>
 BH_HD inline void prim2cons(const KSm<RT>& m, RT gamma, const RT* w, const Derived<RT>& d, RT* u) {
     const RT sg = m.sqrtgam;
-    RT v2 = RT(1) - RT(1) / (d.W * d.W);
+    RT v2 = RT(1) - d.iW * d.iW;
     u[C_D] = sg * w[P_RHO] * d.W;
     RT e = d.rhohW2 + d.B2;
     for (int i = 0; i < 3; i++) u[C_S + i] = sg * (e * d.vl[i] - d.Bv * d.Bl[i]);
@@ -216,7 +227,7 @@ template <typename RT>
 BH_HD inline void phys_flux(const KSm<RT>& m, int dd, const RT* w, const Derived<RT>& d, const RT* u, RT* F) {
     RT vt = m.alpha * d.v[dd] - m.beta[dd];       // coordinate transport velocity
     RT ag = m.alpha * m.sqrtgam;
-    RT iW2 = RT(1) / (d.W * d.W);
+    RT iW2 = d.iW * d.iW;
     RT Bd = w[P_B + dd];
     F[C_D] = u[C_D] * vt;
     for (int j = 0; j < 3; j++) {
@@ -234,12 +245,11 @@ BH_HD inline void phys_flux(const KSm<RT>& m, int dd, const RT* w, const Derived
 template <typename RT>
 BH_HD inline void signal_speeds(const KSm<RT>& m, RT gamma, int dd, const RT* w, const Derived<RT>& d, RT& lm,
                                 RT& lp) {
-    RT rhoh = w[P_RHO] + gamma / (gamma - RT(1)) * w[P_PRS];
-    RT cs2 = gamma * w[P_PRS] / rhoh;
-    RT va2 = d.b2 / (rhoh + d.b2);
-    RT c2 = cs2 + va2 - cs2 * va2;
+    RT rhoh = d.rhoh;
+    // c_s^2 + v_A^2 - c_s^2 v_A^2 with c_s^2 = Gamma p / (rho h), v_A^2 = b^2 / (rho h + b^2)
+    RT c2 = (gamma * w[P_PRS] + d.b2) / (rhoh + d.b2);
     c2 = fmin_(fmax_(c2, RT(0)), RT(1));
-    RT v2 = RT(1) - RT(1) / (d.W * d.W);
+    RT v2 = RT(1) - d.iW * d.iW;
     RT vd = d.v[dd];
     RT gdd = m.gi[dd == 0 ? 0 : (dd == 1 ? 3 : 5)];
     RT den = RT(1) / (RT(1) - v2 * c2);
@@ -307,8 +317,8 @@ BH_HD inline RT hll_face(const KSm<RT>& m, RT gamma, int dd, const RT* wL, const
 // ======================================================================
 // geometric source of a cell (densitised: sqrt(-g) S = S here)
 // ======================================================================
-template <typename RT>
-BH_HD inline void source(const KS& mk, const KSD& dk, RT gamma, const RT* w, RT* S) {
+template <typename RT, typename MT>
+BH_HD inline void source(const KSb<MT>& mk, const KSDb<MT>& dk, RT gamma, const RT* w, RT* S) {
     KSm<RT> m;
     ks_cast(mk, m);
     Derived<RT> d;
@@ -323,8 +333,7 @@ BH_HD inline void source(const KS& mk, const KSD& dk, RT gamma, const RT* w, RT*
     b[0] = d.W * d.Bv * ia;
     RT iW = RT(1) / d.W;
     for (int i = 0; i < 3; i++) b[1 + i] = (w[P_B + i] + m.alpha * b[0] * u[1 + i]) * iW;
-    RT rhoh = w[P_RHO] + gamma / (gamma - RT(1)) * w[P_PRS];
-    RT e = rhoh + d.b2;
+    RT e = d.rhoh + d.b2;
     // inverse four-metric g^{mu nu} = eta^{mu nu} - 2H l^mu l^nu, l^mu = (-1, l_i)
     RT lu[4] = {RT(-1), l[1], l[2], l[3]};
     RT T[4][4];
@@ -395,26 +404,33 @@ BH_HD inline void floor_state(const FxPar& P, double r, double& rho, double& p) 
 // [0, Z_hi] (Z_hi doubled until f > 0) is narrowed by safeguarded Newton
 // steps, each replaced by bisection when it would leave the bracket.
 // ======================================================================
-struct C2P {
-    double D, S2, B2, SB2, B4, E, gf, v2max;
+template <typename T>
+struct C2Pb {
+    T D, S2, B2, SB2, B4, E, gf, v2max;
 };
+using C2P = C2Pb<double>;
 // residual f(Z) and its derivative; v2 is clamped to v2max (clamped = 1)
-BH_HD inline void c2p_eval(const C2P& q, double Z, double& f, double& df, double& v2, int& clamped) {
-    double iZ = 1.0 / Z, ZB = Z + q.B2, iZB = 1.0 / ZB;
-    double iZB2 = iZB * iZB, iZ2 = iZ * iZ;
-    v2 = q.S2 * iZB2 + q.SB2 * (q.B2 + 2.0 * Z) * iZ2 * iZB2;
+template <typename T>
+BH_HD inline void c2p_eval(const C2Pb<T>& q, T Z, T& f, T& df, T& v2, int& clamped) {
+    T iZ = T(1) / Z, ZB = Z + q.B2, iZB = T(1) / ZB;
+    T iZB2 = iZB * iZB, iZ2 = iZ * iZ;
+    v2 = q.S2 * iZB2 + q.SB2 * (q.B2 + T(2) * Z) * iZ2 * iZB2;
     clamped = v2 > q.v2max;
     if (clamped) v2 = q.v2max;
-    double W2i = 1.0 - v2, Wi = sqrt(W2i);
-    double p = q.gf * (Z * W2i - q.D * Wi);
-    f = Z - p + 0.5 * (1.0 + v2) * q.B2 - 0.5 * q.SB2 * iZ2 - q.E;
-    double dv2 = clamped ? 0.0
-                         : -2.0 * q.S2 * iZB2 * iZB -
-                               2.0 * q.SB2 * (3.0 * Z * Z + 3.0 * Z * q.B2 + q.B4) * iZ2 * iZ * iZB2 * iZB;
-    double dp = q.gf * (W2i - Z * dv2 + 0.5 * q.D * dv2 / Wi);
-    df = 1.0 - dp + 0.5 * q.B2 * dv2 + q.SB2 * iZ2 * iZ;
+    T W2i = T(1) - v2, Wi = sqrt_(W2i);
+    T p = q.gf * (Z * W2i - q.D * Wi);
+    f = Z - p + T(0.5) * (T(1) + v2) * q.B2 - T(0.5) * q.SB2 * iZ2 - q.E;
+    T dv2 = clamped ? T(0)
+                    : T(-2) * q.S2 * iZB2 * iZB -
+                          T(2) * q.SB2 * (T(3) * Z * Z + T(3) * Z * q.B2 + q.B4) * iZ2 * iZ * iZB2 * iZB;
+    T dp = q.gf * (W2i - Z * dv2 + T(0.5) * q.D * dv2 / Wi);
+    df = T(1) - dp + T(0.5) * q.B2 * dv2 + q.SB2 * iZ2 * iZ;
 }
 
+// PRE32 (the mixed variant): up to four FP32 Newton iterations move the
+// previous primitives' Z towards the root before the FP64 iterations, which
+// alone decide convergence and give the recovered state.
+template <bool PRE32 = false>
 BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const double* B, const double* wo,
                           double* w, int& iters) {
     const double gm = P.gamma;
@@ -441,10 +457,29 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
     double W2o = 1.0 + utl[0] * uto[0] + utl[1] * uto[1] + utl[2] * uto[2];
     double Z = (wo[P_RHO] + gm / (gm - 1.0) * wo[P_PRS]) * W2o;
     if (!(Z > 0.0) || !(Z < 1e300)) Z = q.E > q.D ? q.E : q.D;
-    int it = 0, ok = 0;
+    int it = 0, ok = 0, it32 = 0;
     double f, df, v2;
     int clamped;
-    // phase 1
+    if (PRE32) {
+        C2Pb<float> qf;
+        qf.D = float(q.D); qf.S2 = float(q.S2); qf.B2 = float(q.B2); qf.SB2 = float(q.SB2);
+        qf.B4 = float(q.B4); qf.E = float(q.E); qf.gf = float(q.gf); qf.v2max = float(q.v2max);
+        float Zf = float(Z), ff, dff, v2f;
+        int cl;
+        for (; it32 < 4; it32++) {
+            c2p_eval(qf, Zf, ff, dff, v2f, cl);
+            if (cl || !(dff != 0.0f)) break;
+            float Zn = Zf - ff / dff;
+            if (!(Zn > 0.0f)) break;
+            float e = fabs_(Zn - Zf);
+            Zf = Zn;
+            if (e <= 1e-6f * Zf) { it32++; break; }
+        }
+        if (Zf > 0.0f && Zf < 1e30f) Z = double(Zf);
+    }
+    // phase 1; a step of at most sqrt(tol) Z is accepted as the last one:
+    // Newton's quadratic convergence leaves an error of order tol Z after it
+    const double qtol = sqrt(P.tol);
     for (; it < P.maxiter; it++) {
         c2p_eval(q, Z, f, df, v2, clamped);
         if (clamped || !(df != 0.0)) break;
@@ -452,7 +487,7 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
         if (!(Zn > 0.0)) break;
         double err = fabs_(Zn - Z);
         Z = Zn;
-        if (err <= P.tol * Z) { ok = 1; it++; break; }
+        if (err <= qtol * Z) { ok = 1; it++; break; }
     }
     // phase 2
     if (!ok) {
@@ -480,7 +515,7 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
             }
         }
     }
-    iters = it;
+    iters = it + it32;
     if (!ok) return 1;
     double iZ = 1.0 / Z, ZB = Z + q.B2, iZB = 1.0 / ZB;
     v2 = q.S2 * iZB * iZB + q.SB2 * (q.B2 + 2.0 * Z) * iZ * iZ * iZB * iZB;
@@ -540,21 +575,76 @@ BH_HD inline int apply_floors(const FxPar& P, const KS& m, double* w) {
 // ======================================================================
 // CFL limit of a cell: the smallest dx_d / max|lambda_d|
 // ======================================================================
-BH_HD inline double cell_dt(const FxPar& P, const KS& mk, const double* w, const double* dx) {
-    KSm<double> m;
+template <typename A, typename B>
+BH_HD inline void copy_geometry(const KSb<A>& m, const KSDb<A>& d, KSb<B>& mo, KSDb<B>& dout) {
+    mo.H = B(m.H); mo.alpha = B(m.alpha); mo.sqrtgam = B(m.sqrtgam); mo.r = B(m.r);
+    for (int i = 0; i < 3; i++) { mo.l[i] = B(m.l[i]); mo.beta[i] = B(m.beta[i]); dout.dH[i] = B(d.dH[i]); }
+    for (int i = 0; i < 6; i++) { mo.g[i] = B(m.g[i]); mo.gi[i] = B(m.gi[i]); }
+    for (int k = 0; k < 3; k++)
+        for (int i = 0; i < 3; i++) dout.dl[k][i] = B(d.dl[k][i]);
+}
+
+template <typename RT = double>
+BH_HD inline double cell_dt(const FxPar& P, const KS& mk, const double* w64, const double* dx) {
+    KSm<RT> m;
     ks_cast(mk, m);
-    Derived<double> d;
-    derive(m, P.gamma, w, d);
+    RT w[8];
+    for (int v = 0; v < 8; v++) w[v] = RT(w64[v]);
+    Derived<RT> d;
+    derive(m, RT(P.gamma), w, d);
     double best = 1e300;
     for (int dd = 0; dd < 3; dd++) {
-        double lm, lp;
-        signal_speeds(m, P.gamma, dd, w, d, lm, lp);
-        double c = fmax_(fabs_(lm), fabs_(lp));
+        RT lm, lp;
+        signal_speeds(m, RT(P.gamma), dd, w, d, lm, lp);
+        double c = fmax_(fabs_(double(lm)), fabs_(double(lp)));
         if (c > 0.0) best = fmin_(best, dx[dd] / c);
     }
     return best;
 }
 
+// ======================================================================
+// geometry for the face and source work.  FP64 everywhere in the FP64
+// variants; in the mixed variant (RT = float) the metric and its
+// derivatives are evaluated in FP32 beyond r ~ FX_R_FP64 (Euclidean
+// radius), and in FP64 and rounded inside it, where the horizon's steep
+// gradients are.
+// ======================================================================
+constexpr double FX_R_FP64 = 4.0;
+template <typename RT>
+BH_HD inline bool fp32_geometry(const double* x) {
+    if (sizeof(RT) == sizeof(double)) return false;
+    return x[0] * x[0] + x[1] * x[1] + x[2] * x[2] > FX_R_FP64 * FX_R_FP64;
+}
+// spatial metric at a face centre
+template <typename RT>
+BH_HD inline void face_geometry(const FxPar& P, const double* x, KSm<RT>& m) {
+    if (fp32_geometry<RT>(x)) {
+        KSb<float> mf;
+        ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
+        ks_cast(mf, m);
+    } else {
+        KS mk;
+        ks_metric(P, x[0], x[1], x[2], mk);
+        ks_cast(mk, m);
+    }
+}
+// metric and derivatives at a cell centre, in RT
+template <typename RT>
+BH_HD inline void cell_geometry(const FxPar& P, const double* x, KSb<RT>& m, KSDb<RT>& d) {
+    if (fp32_geometry<RT>(x)) {
+        KSb<float> mf;
+        KSDb<float> df;
+        ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
+        ks_deriv<float>(P, float(x[0]), float(x[1]), float(x[2]), mf, df);
+        copy_geometry(mf, df, m, d);
+    } else {
+        KS mk;
+        KSD dk;
+        ks_metric(P, x[0], x[1], x[2], mk);
+        ks_deriv(P, x[0], x[1], x[2], mk, dk);
+        copy_geometry(mk, dk, m, d);
+    }
+}
 
 // ======================================================================
 // initial data: Fishbone & Moncrief (1976) torus in Boyer-Lindquist form,

@@ -353,7 +353,8 @@ typedef struct bh_step_graph bh_step_graph;
 int bh_step_graph_create(const bh_params *P, const bh_pool *pool, double cfl, double *dt_dev,
                          const int32_t *waves, const int32_t *wave_off_host, int32_t nwave, void *stream,
                          bh_step_graph **out);
-/* one step: a replay of the captured graph on `stream` */
+/* one step: a replay of the captured graph on `stream` (NULL: the legacy
+ * default stream) */
 int bh_step_graph_replay(bh_step_graph *g, void *stream);
 int bh_step_graph_destroy(bh_step_graph *g);
 
@@ -430,6 +431,15 @@ typedef struct bh_fx_grid {
     int32_t *count;              /* device [4]: con2prim failures, floored cells     */
     int32_t *err;                /* device error word                                */
 } bh_fx_grid;
+
+/* Launch bounds of the scheme's three heavy kernels (no counterpart in the
+ * reference): each is compiled for 1 (no register cap), 3, 4, 5 and 6
+ * resident 128-thread CTAs per SM; the choice is per process and variant,
+ * initially 1.  bhgpu.fixed.autotune times the candidates on a grid and sets
+ * the fastest.  Launches (and graphs captured) after the call use it. */
+enum { BH_FX_TUNE_C2P = 0, BH_FX_TUNE_FLUX = 1, BH_FX_TUNE_UPDATE = 2, BH_FX_TUNE_N = 3 };
+int bh_fx_tune_set(int32_t precision, int32_t kernel, int32_t ctas_per_sm);
+int bh_fx_tune_get(int32_t precision, int32_t kernel, int32_t *ctas_per_sm);
 
 /* one RK2 step: con2prim (+ CFL reduction), ghost fill, fluxes, update, twice */
 int bh_fx_step(const bh_fx_params *P, const bh_fx_grid *g, void *stream);

@@ -125,7 +125,7 @@ static void lower3(const double* g, const double* v, double* o) {
 
 /* ------------------------------------------------------- prim -> cons */
 typedef struct {
-    double W, v[3], vl[3], Bl[3], B2, Bv, b2, rhohW2, ptot;
+    double W, iW, rhoh, v[3], vl[3], Bl[3], B2, Bv, b2, rhohW2, ptot;
 } drv;
 
 static void derive(const ksm* m, double gamma, const double* w, drv* d) {
@@ -136,6 +136,7 @@ static void derive(const ksm* m, double gamma, const double* w, drv* d) {
     double u2 = utl[0] * ut[0] + utl[1] * ut[1] + utl[2] * ut[2];
     d->W = sqrt(1.0 + u2);
     double iW = 1.0 / d->W;
+    d->iW = iW;
     for (int i = 0; i < 3; i++) {
         d->v[i] = ut[i] * iW;
         d->vl[i] = utl[i] * iW;
@@ -145,13 +146,14 @@ static void derive(const ksm* m, double gamma, const double* w, drv* d) {
     d->Bv = d->Bl[0] * d->v[0] + d->Bl[1] * d->v[1] + d->Bl[2] * d->v[2];
     d->b2 = d->B2 * iW * iW + d->Bv * d->Bv;
     double rhoh = w[RHO] + gamma / (gamma - 1.0) * w[PRS];
+    d->rhoh = rhoh;
     d->rhohW2 = rhoh * d->W * d->W;
     d->ptot = w[PRS] + 0.5 * d->b2;
 }
 
 static void p2c(const ksm* m, const double* w, const drv* d, double* u) {
     double sg = m->sqrtgam;
-    double v2 = 1.0 - 1.0 / (d->W * d->W);
+    double v2 = 1.0 - d->iW * d->iW;
     u[CD] = sg * w[RHO] * d->W;
     double e = d->rhohW2 + d->B2;
     for (int i = 0; i < 3; i++) u[CS + i] = sg * (e * d->vl[i] - d->Bv * d->Bl[i]);
@@ -163,7 +165,7 @@ static void p2c(const ksm* m, const double* w, const drv* d, double* u) {
 static void pflux(const ksm* m, int dd, const double* w, const drv* d, const double* u, double* F) {
     double vt = m->alpha * d->v[dd] - m->beta[dd];
     double ag = m->alpha * m->sqrtgam;
-    double iW2 = 1.0 / (d->W * d->W);
+    double iW2 = d->iW * d->iW;
     double Bd = w[BB + dd];
     F[CD] = u[CD] * vt;
     for (int j = 0; j < 3; j++) {
@@ -178,12 +180,10 @@ static void pflux(const ksm* m, int dd, const double* w, const drv* d, const dou
 }
 
 static void speeds(const ksm* m, double gamma, int dd, const double* w, const drv* d, double* lm, double* lp) {
-    double rhoh = w[RHO] + gamma / (gamma - 1.0) * w[PRS];
-    double cs2 = gamma * w[PRS] / rhoh;
-    double va2 = d->b2 / (rhoh + d->b2);
-    double c2 = cs2 + va2 - cs2 * va2;
+    double rhoh = d->rhoh;
+    double c2 = (gamma * w[PRS] + d->b2) / (rhoh + d->b2);
     c2 = dmin(dmax(c2, 0.0), 1.0);
-    double v2 = 1.0 - 1.0 / (d->W * d->W);
+    double v2 = 1.0 - d->iW * d->iW;
     double vd = d->v[dd];
     double gdd = m->gi[dd == 0 ? 0 : (dd == 1 ? 3 : 5)];
     double den = 1.0 / (1.0 - v2 * c2);
@@ -245,8 +245,7 @@ static void source(const ksm* m, const ksd* dk, double gamma, const double* w, d
     b[0] = d.W * d.Bv * ia;
     double iW = 1.0 / d.W;
     for (int i = 0; i < 3; i++) b[1 + i] = (w[BB + i] + m->alpha * b[0] * u[1 + i]) * iW;
-    double rhoh = w[RHO] + gamma / (gamma - 1.0) * w[PRS];
-    double e = rhoh + d.b2;
+    double e = d.rhoh + d.b2;
     double lu[4] = {-1.0, l[1], l[2], l[3]};
     double T[4][4];
     for (int mu = 0; mu < 4; mu++)
@@ -339,6 +338,9 @@ static int c2p(const fxo_params* P, const ksm* m, const double* U, const double*
     int it = 0, ok = 0;
     double f = 0.0, df = 0.0, v2 = 0.0;
     int clamped = 0;
+    /* a step of at most sqrt(tol) Z is the last: Newton's quadratic
+     * convergence leaves an error of order tol Z after it */
+    double qtol = sqrt(P->tol);
     for (; it < P->maxiter; it++) {
         c2p_eval(&q, Z, &f, &df, &v2, &clamped);
         if (clamped || !(df != 0.0)) break;
@@ -346,7 +348,7 @@ static int c2p(const fxo_params* P, const ksm* m, const double* U, const double*
         if (!(Zn > 0.0)) break;
         double err = dabs(Zn - Z);
         Z = Zn;
-        if (err <= P->tol * Z) {
+        if (err <= qtol * Z) {
             ok = 1;
             it++;
             break;

@@ -244,10 +244,14 @@ def test_con2prim_round_trip(guess):
         wo[0] *= 1e-4; wo[1] *= 1e3; wo[2:5] = 0.0
     wr, st, it = ofx.con2prim(prm, x, y, z, U, w[5:8], wo)
     assert (st == 0).all(), np.bincount(st)
+    # rho and ut to 1e-8 relative; the pressure comes from p = (Gamma-1)/Gamma
+    # (Z / W^2 - rho / W), a difference that cancels in cold gas, so its error
+    # follows Z's (about 1e-12 relative) times rho h, not p itself
+    rhoh = w[0] + 4.0 * w[1]
     for v in range(5):
-        scale = np.abs(w[v]) + (np.abs(w[2:5]).max(0) if v >= 2 else 0) + 1e-300
+        scale = (rhoh if v == 1 else np.abs(w[v]) + (np.abs(w[2:5]).max(0) if v >= 2 else 0)) + 1e-300
         err = np.abs(wr[v] - w[v]) / scale
-        assert err.max() <= 1e-8, (v, err.max())
+        assert err.max() <= (1e-10 if v == 1 else 1e-8), (v, err.max())
     if guess == "near":
         assert np.median(it) <= 4
 
