@@ -21,12 +21,14 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from bhgrid.blocks import BLOCK_DTYPE, CHUNK, box_size, interior as _interior, uniform_blocks, work_items  # noqa: F401
+from bhgrid.blocks import (BLOCK_DTYPE, CHUNK, box_size, interior as _interior, leveled_blocks,  # noqa: F401
+                           uniform_blocks, work_items)
 
 from ._lib import BH_FP64, BH_FP64_FMA, BH_MIXED, BH_MC, BH_MINMOD, BH_VANLEER, BhError, check, lib
 
 _vp, _d, _i32, _i64 = C.c_void_p, C.c_double, C.c_int32, C.c_int64
 GHOST = 2
+QSLOTS = 6           # BH_FX_QSLOTS
 PRECISIONS = {"fp64": BH_FP64, "fp64-fma": BH_FP64_FMA, "mixed": BH_MIXED}
 LIMITERS = {"minmod": BH_MINMOD, "vanleer": BH_VANLEER, "mc": BH_MC}
 
@@ -41,7 +43,7 @@ class BhFxGrid(C.Structure):
     _fields_ = [("nblock", _i32), ("blocks", _vp), ("nbr", _vp), ("items_cell", _vp), ("nitem_cell", _i32),
                 ("items_pos", _vp), ("nitem_pos", _i32), ("items_ghost", _vp), ("nitem_ghost", _i32),
                 ("ncell", _i64), ("U", _vp), ("U1", _vp), ("W", _vp), ("Bf", _vp), ("Bf1", _vp), ("F", _vp),
-                ("dt", _vp), ("count", _vp), ("err", _vp)]
+                ("dt", _vp), ("count", _vp), ("err", _vp), ("E", _vp), ("maxlevel", _i32), ("queue_ctas", _i32), ("queue", _vp)]
 
 
 class BhFxTorus(C.Structure):
@@ -107,7 +109,12 @@ class FxGrid:
     [lo, hi]^3; ``block`` = N gives one block (no interior ghost exchange).
     """
 
-    def __init__(self, blocks: np.ndarray, nbr: np.ndarray, params: FxParams, device="cuda"):
+    def __init__(self, blocks: np.ndarray, nbr: np.ndarray, params: FxParams, device="cuda", emf_arrays=None,
+                 persistent=False):
+        """emf_arrays: keep the edge EMFs in arrays (required, and the
+        default, when blocks have different levels; otherwise they are
+        computed on the fly by the update).  persistent: launch the step
+        kernels as persistent CTAs fed by a device work queue."""
         self.params = params
         self.blocks_np = blocks
         self.nbr_np = nbr
@@ -129,12 +136,26 @@ class FxGrid:
         self.count = torch.zeros(4, dtype=torch.int32, device=dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.scratch = torch.zeros(4, dtype=torch.float64, device=dev)
+        self.maxlevel = int(blocks["level"].max())
+        if emf_arrays is None:
+            emf_arrays = self.maxlevel > 0
+        self.E = torch.zeros((3, N), dtype=torch.float64, device=dev) if emf_arrays else None
+        self.queue = torch.zeros(2 * QSLOTS, dtype=torch.int32, device=dev) if persistent else None
         self._refresh()
 
     @classmethod
-    def uniform(cls, lo: float, hi: float, N: int, block: int, params: FxParams, periodic=False, device="cuda"):
+    def uniform(cls, lo: float, hi: float, N: int, block: int, params: FxParams, periodic=False, device="cuda",
+                emf_arrays=None, persistent=False):
         blocks, nbr = uniform_blocks(lo, hi, N, block, periodic)
-        return cls(blocks, nbr, params, device)
+        return cls(blocks, nbr, params, device, emf_arrays, persistent)
+
+    @classmethod
+    def leveled(cls, lo: float, hi: float, level: np.ndarray, n0: int, params: FxParams, device="cuda",
+                persistent=False):
+        """Equal cubes over [lo, hi]^3 with per-cube levels (n0 2^level cells
+        per axis), e.g. bhgrid.blocks.torus_levels()."""
+        blocks, nbr = leveled_blocks(lo, hi, level, n0)
+        return cls(blocks, nbr, params, device, persistent=persistent)
 
     def _refresh(self):
         it = self.items
@@ -142,7 +163,7 @@ class FxGrid:
                            _ptr(it["cell"]), it["cell"].shape[0], _ptr(it["pos"]), it["pos"].shape[0],
                            _ptr(it["ghost"]), it["ghost"].shape[0], self.ncell,
                            _ptr(self.U), _ptr(self.U1), _ptr(self.W), _ptr(self.Bf), _ptr(self.Bf1), _ptr(self.F),
-                           _ptr(self.dt), _ptr(self.count), _ptr(self.err))
+                           _ptr(self.dt), _ptr(self.count), _ptr(self.err), _ptr(self.E), self.maxlevel, 0, _ptr(self.queue))
         self._p = self.params.cstruct()
 
     @property

@@ -77,3 +77,76 @@ def interior(blocks: np.ndarray, arr: np.ndarray) -> np.ndarray:
         box = arr[..., int(b["off"]):int(b["off"]) + S ** 3].reshape(arr.shape[:-1] + (S, S, S))
         out.append(box[..., 2:2 + n, 2:2 + n, 2:2 + n])
     return np.stack(out, axis=-4)
+
+
+def balanced_levels(level: np.ndarray) -> np.ndarray:
+    """Raise cube levels until every pair of cubes that touch (faces, edges
+    or corners) differ by at most one level (2:1 balance)."""
+    lv = level.copy()
+    nb = lv.shape[0]
+    changed = True
+    while changed:
+        changed = False
+        for i in range(nb):
+            for j in range(nb):
+                for k in range(nb):
+                    m = lv[max(i - 1, 0):i + 2, max(j - 1, 0):j + 2, max(k - 1, 0):k + 2].max()
+                    if lv[i, j, k] < m - 1:
+                        lv[i, j, k] = m - 1
+                        changed = True
+    return lv
+
+
+def leveled_blocks(lo: float, hi: float, level: np.ndarray, n0: int, periodic: bool = False):
+    """Block table and 27-neighbour table of equal cubes over [lo, hi]^3, one
+    block per cube, cube (i, j, k) holding (n0 2^level)^3 cells: a
+    refinement level changes a cube's resolution, not its extent, so each
+    block has exactly one neighbour per offset; levels must be 2:1 balanced."""
+    nb = level.shape[0]
+    if n0 % 8:
+        raise ValueError("block sizes must be multiples of 8")
+    L = (hi - lo) / nb
+    blocks = np.zeros(nb ** 3, BLOCK_DTYPE)
+    nbr = np.full((nb ** 3, 27), -1, np.int32)
+    off = 0
+    for bi in range(nb):
+        for bj in range(nb):
+            for bk in range(nb):
+                b = (bi * nb + bj) * nb + bk
+                n = n0 << int(level[bi, bj, bk])
+                blocks[b]["n"] = n
+                blocks[b]["level"] = level[bi, bj, bk]
+                blocks[b]["off"] = off
+                blocks[b]["x0"] = (lo + bi * L, lo + bj * L, lo + bk * L)
+                blocks[b]["dx"] = L / n
+                off += box_size(n)
+                for ox in (-1, 0, 1):
+                    for oy in (-1, 0, 1):
+                        for oz in (-1, 0, 1):
+                            q = [bi + ox, bj + oy, bk + oz]
+                            if periodic:
+                                q = [v % nb for v in q]
+                            elif not all(0 <= v < nb for v in q):
+                                continue
+                            s = (q[0] * nb + q[1]) * nb + q[2]
+                            if abs(int(level[q[0], q[1], q[2]]) - int(level[bi, bj, bk])) > 1:
+                                raise ValueError("levels are not 2:1 balanced")
+                            nbr[b, (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1)] = s
+    return blocks, nbr
+
+
+def torus_levels(nb: int = 8, lo: float = -40.0, hi: float = 40.0, r_fine=(14.0, 26.0), seed: int = 3,
+                 jitter: float = 0.25):
+    """Seeded uneven level map concentrated near the hole: level 2 for cubes
+    whose centre lies within r_fine[0], 1 within r_fine[1], 0 beyond; a
+    fraction `jitter` of the cubes moves one level up or down at random;
+    then 2:1 balanced."""
+    rng = np.random.default_rng(seed)
+    L = (hi - lo) / nb
+    c = lo + (np.arange(nb) + 0.5) * L
+    R = np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2)
+    lv = np.where(R < r_fine[0], 2, np.where(R < r_fine[1], 1, 0))
+    move = rng.random(lv.shape) < jitter
+    step = rng.choice([-1, 1], size=lv.shape)
+    lv = np.clip(np.where(move, lv + step, lv), 0, 2)
+    return balanced_levels(lv)

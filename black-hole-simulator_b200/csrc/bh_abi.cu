@@ -188,6 +188,7 @@ int fx_bad(const bh_fx_params* P, const bh_fx_grid* g) {
         (g->nitem_ghost > 0 && !g->items_ghost) || g->nitem_cell < 0 || g->nitem_pos < 0 || g->nitem_ghost < 0)
         return 1;
     if (P->precision < BH_FP64 || P->precision > BH_MIXED || P->maxiter <= 0 || !(P->gamma > 1.0)) return 1;
+    if (g->maxlevel < 0 || g->maxlevel > 8 || (g->maxlevel > 0 && !g->E)) return 1;
     return 0;
 }
 }  // namespace

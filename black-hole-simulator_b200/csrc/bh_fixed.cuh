@@ -38,9 +38,10 @@ struct Grid {
     double* dt;
     int32_t* count;
     int32_t* err;
+    double* E;
 };
 inline Grid grid_of(const bh_fx_grid* g) {
-    return Grid{g->blocks, g->nbr, g->U, g->U1, g->Bf, g->Bf1, g->W, g->F, g->ncell, g->dt, g->count, g->err};
+    return Grid{g->blocks, g->nbr, g->U, g->U1, g->Bf, g->Bf1, g->W, g->F, g->ncell, g->dt, g->count, g->err, g->E};
 }
 inline FxPar par_of(const bh_fx_params* p) {
     FxPar q;
@@ -76,6 +77,43 @@ __device__ inline void atomic_min_pos(double* slot, double v) {
 __device__ inline void atomic_max_pos(double* slot, double v) {
     atomicMax((unsigned long long*)slot, (unsigned long long)__double_as_longlong(v));
 }
+// ======================================================================
+// the item loop.  Without a queue, CTA t takes item t of the launch's work
+// list.  With one (the persistent form: a grid of resident CTAs), each CTA
+// takes items from a device counter until none is left; the last CTA to
+// finish resets the counter for the next launch of the slot, so a step
+// needs no extra launch or memset and records into a CUDA graph as is.
+// ======================================================================
+struct Queue {
+    int32_t* head;   // next item (NULL: one CTA per item)
+    int32_t* done;   // CTAs finished
+    int32_t nitem;
+};
+template <typename Body>
+__device__ __forceinline__ void for_items(const Queue& q, Body body) {
+    if (!q.head) {
+        body((int)blockIdx.x);
+        return;
+    }
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(q.head, 1);
+        __syncthreads();
+        const int t = s_item;
+        __syncthreads();
+        if (t >= q.nitem) break;
+        body(t);
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(q.done, 1) == (int)gridDim.x - 1) {
+            *q.head = 0;
+            *q.done = 0;
+            __threadfence();
+        }
+    }
+}
+
 __global__ void k_fx_dt_init(double* dt) {
     dt[0] = __longlong_as_double(0x7FF0000000000000LL);   // +inf
 }
@@ -86,65 +124,67 @@ __global__ void k_fx_dt_init(double* dt) {
 // limit into dt[0]
 // ======================================================================
 template <typename RT, typename WT, int MINB>
-__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage, int with_dt) {
-    const int32_t b = items[2 * blockIdx.x];
-    const bh_fx_block B = G.blk[b];
-    const int n = B.n;
-    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
-    double dtc = 1e300;
-    if (e < n * n * n) {
-        const int i = e / (n * n), j = (e / n) % n, k = e % n;
-        const int64_t c = bidx(B, i, j, k);
-        double* U = stage ? G.U1 : G.U;
-        const double* Bf = stage ? G.Bf1 : G.Bf;
-        const int64_t N = G.ncell;
-        double x[3];
-        cell_centre(B, i, j, k, x);
-        KS m;
-        ks_metric(P, x[0], x[1], x[2], m);
-        // cell field: mean of the two faces (the role of f2cB, transport.cpp:60-75)
-        const int si = bstride_i(B), sj = bstride_j(B);
-        double Bt[3] = {0.5 * (Bf[c] + Bf[c + si]), 0.5 * (Bf[N + c] + Bf[N + c + sj]),
-                        0.5 * (Bf[2 * N + c] + Bf[2 * N + c + 1])};
-        double isg = 1.0 / m.sqrtgam;
-        double Bc[3] = {Bt[0] * isg, Bt[1] * isg, Bt[2] * isg};
-        double u[8], wo[8], w[8];
-        for (int v = 0; v < 5; v++) u[v] = U[v * N + c];
-        WT* W = (WT*)G.W;
-        for (int v = 0; v < 5; v++) wo[v] = (double)W[v * N + c];
-        int iters = 0;
-        int st = con2prim<sizeof(RT) < sizeof(double)>(P, m, u, Bc, wo, w, iters);
-        int rewrite = 0;
-        if (st != 0) {
-            // keep the previous primitives with the new field
-            for (int v = 0; v < 5; v++) w[v] = wo[v];
-            for (int d = 0; d < 3; d++) w[P_B + d] = Bc[d];
-            atomicAdd(&G.count[0], 1);
-            rewrite = 1;
+__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage, int with_dt, Queue Q) {
+    for_items(Q, [&](int t) {
+        const int32_t b = items[2 * t];
+        const bh_fx_block B = G.blk[b];
+        const int n = B.n;
+        const int e = items[2 * t + 1] + threadIdx.x;
+        double dtc = 1e300;
+        if (e < n * n * n) {
+            const int i = e / (n * n), j = (e / n) % n, k = e % n;
+            const int64_t c = bidx(B, i, j, k);
+            double* U = stage ? G.U1 : G.U;
+            const double* Bf = stage ? G.Bf1 : G.Bf;
+            const int64_t N = G.ncell;
+            double x[3];
+            cell_centre(B, i, j, k, x);
+            KS m;
+            ks_metric(P, x[0], x[1], x[2], m);
+            // cell field: mean of the two faces (the role of f2cB, transport.cpp:60-75)
+            const int si = bstride_i(B), sj = bstride_j(B);
+            double Bt[3] = {0.5 * (Bf[c] + Bf[c + si]), 0.5 * (Bf[N + c] + Bf[N + c + sj]),
+                            0.5 * (Bf[2 * N + c] + Bf[2 * N + c + 1])};
+            double isg = 1.0 / m.sqrtgam;
+            double Bc[3] = {Bt[0] * isg, Bt[1] * isg, Bt[2] * isg};
+            double u[8], wo[8], w[8];
+            for (int v = 0; v < 5; v++) u[v] = U[v * N + c];
+            WT* W = (WT*)G.W;
+            for (int v = 0; v < 5; v++) wo[v] = (double)W[v * N + c];
+            int iters = 0;
+            int st = con2prim<sizeof(RT) < sizeof(double)>(P, m, u, Bc, wo, w, iters);
+            int rewrite = 0;
+            if (st != 0) {
+                // keep the previous primitives with the new field
+                for (int v = 0; v < 5; v++) w[v] = wo[v];
+                for (int d = 0; d < 3; d++) w[P_B + d] = Bc[d];
+                atomicAdd(&G.count[0], 1);
+                rewrite = 1;
+            }
+            if (apply_floors(P, m, w)) {
+                rewrite = 1;
+                atomicAdd(&G.count[1], 1);
+            }
+            if (rewrite) {
+                KSm<double> mm;
+                ks_cast(m, mm);
+                Derived<double> d;
+                derive(mm, P.gamma, w, d);
+                prim2cons(mm, P.gamma, w, d, u);
+                for (int v = 0; v < 5; v++) U[v * N + c] = u[v];
+            }
+            for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
+            for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];
+            if (with_dt) {
+                double dx[3] = {B.dx, B.dx, B.dx};
+                dtc = cell_dt<RT>(P, m, w, dx);
+            }
         }
-        if (apply_floors(P, m, w)) {
-            rewrite = 1;
-            atomicAdd(&G.count[1], 1);
-        }
-        if (rewrite) {
-            KSm<double> mm;
-            ks_cast(m, mm);
-            Derived<double> d;
-            derive(mm, P.gamma, w, d);
-            prim2cons(mm, P.gamma, w, d, u);
-            for (int v = 0; v < 5; v++) U[v * N + c] = u[v];
-        }
-        for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
-        for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];
         if (with_dt) {
-            double dx[3] = {B.dx, B.dx, B.dx};
-            dtc = cell_dt<RT>(P, m, w, dx);
+            for (int o = 16; o > 0; o >>= 1) dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+            if ((threadIdx.x & 31) == 0 && dtc < 1e300) atomic_min_pos(G.dt, dtc);
         }
-    }
-    if (with_dt) {
-        for (int o = 16; o > 0; o >>= 1) dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
-        if ((threadIdx.x & 31) == 0 && dtc < 1e300) atomic_min_pos(G.dt, dtc);
-    }
+    });
 }
 
 // ======================================================================
@@ -202,38 +242,111 @@ __device__ inline int ghost_source(const Grid& G, int b, int n, int fdim, int& i
     return src;
 }
 
+// Where the image lies in a block of another level (blocks are equal cubes,
+// one level apart at most): a finer source is averaged (restriction, the 8
+// cells or 4 faces that cover the ghost), a coarser one is interpolated
+// (prolongation: the covering coarse cell plus a quarter of its
+// minmod-limited slope towards the ghost cell in each direction; a face
+// takes the coarse face it lies on, or the mean of the two it lies between).
+// Pass 0 fills the copies and restrictions; pass l > 0 the prolongations
+// into the blocks of level l, whose coarse sources' ghosts earlier passes
+// have filled.
+__device__ inline double mm_slope(double a, double b, double c) {   // minmod of the two differences
+    double l = b - a, r = c - b;
+    if (l * r <= 0.0) return 0.0;
+    return fabs(l) < fabs(r) ? l : r;
+}
 template <typename WT>
-__global__ void __launch_bounds__(FX_TPB) k_fx_ghost(Grid G, const int32_t* items, int stage) {
-    const int32_t b = items[2 * blockIdx.x];
-    const bh_fx_block B = G.blk[b];
-    const int n = B.n;
-    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
-    int i, j, k;
-    if (!shell_decode(n, e, i, j, k)) return;
-    const int64_t N = G.ncell;
-    WT* W = (WT*)G.W;
-    double* Bf = stage ? G.Bf1 : G.Bf;
-    const int64_t c = bidx(B, i, j, k);
-    {
-        int si = i, sj = j, sk = k;
-        int s = ghost_source(G, b, n, -1, si, sj, sk);
-        const int64_t sc = bidx(G.blk[s], si, sj, sk);
-        for (int v = 0; v < 8; v++) W[v * N + c] = W[v * N + sc];
-    }
-    // the lower faces of this ghost cell that the flux kernel reads: normal
-    // index 0..n, transverse index -1..n, outside the block's own faces
-    // (transverse 0..n-1)
-    for (int d = 0; d < 3; d++) {
-        int cc[3] = {i, j, k};
-        if (cc[d] < 0 || cc[d] > n) continue;
-        bool need = true;
-        for (int q = 0; q < 3; q++)
-            if (q != d && (cc[q] < -1 || cc[q] > n)) need = false;
-        if (!need) continue;
-        int si = i, sj = j, sk = k;
-        int s = ghost_source(G, b, n, d, si, sj, sk);
-        Bf[d * N + c] = Bf[d * N + bidx(G.blk[s], si, sj, sk)];
-    }
+__global__ void __launch_bounds__(FX_TPB) k_fx_ghost(Grid G, const int32_t* items, int stage, int pass, Queue Q) {
+    for_items(Q, [&](int t) {
+        const int32_t b = items[2 * t];
+        const bh_fx_block B = G.blk[b];
+        if (pass > 0 && B.level != pass) return;
+        const int n = B.n;
+        const int e = items[2 * t + 1] + threadIdx.x;
+        int i, j, k;
+        if (!shell_decode(n, e, i, j, k)) return;
+        const int64_t N = G.ncell;
+        WT* W = (WT*)G.W;
+        double* Bf = stage ? G.Bf1 : G.Bf;
+        const int64_t c = bidx(B, i, j, k);
+        {
+            int si = i, sj = j, sk = k;
+            int s = ghost_source(G, b, n, -1, si, sj, sk);
+            const bh_fx_block S = G.blk[s];
+            const int kind = S.n == n ? 0 : (S.n > n ? 1 : 2);   // copy, restrict, prolong
+            if ((kind == 2) == (pass > 0)) {
+                if (kind == 0) {
+                    const int64_t sc = bidx(S, si, sj, sk);
+                    for (int v = 0; v < 8; v++) W[v * N + c] = W[v * N + sc];
+                } else if (kind == 1) {
+                    for (int v = 0; v < 8; v++) {
+                        double sum = 0.0;
+                        for (int a = 0; a < 2; a++)
+                            for (int q = 0; q < 2; q++)
+                                for (int r = 0; r < 2; r++)
+                                    sum += (double)W[v * N + bidx(S, 2 * si + a, 2 * sj + q, 2 * sk + r)];
+                        W[v * N + c] = (WT)(0.125 * sum);
+                    }
+                } else {
+                    const int ic = si >> 1, jc = sj >> 1, kc = sk >> 1;
+                    const double gx = (si & 1) ? 0.25 : -0.25, gy = (sj & 1) ? 0.25 : -0.25, gz = (sk & 1) ? 0.25 : -0.25;
+                    for (int v = 0; v < 8; v++) {
+                        const WT* Wv = W + v * N;
+                        double w0 = (double)Wv[bidx(S, ic, jc, kc)];
+                        double sx = mm_slope((double)Wv[bidx(S, ic - 1, jc, kc)], w0, (double)Wv[bidx(S, ic + 1, jc, kc)]);
+                        double sy = mm_slope((double)Wv[bidx(S, ic, jc - 1, kc)], w0, (double)Wv[bidx(S, ic, jc + 1, kc)]);
+                        double sz = mm_slope((double)Wv[bidx(S, ic, jc, kc - 1)], w0, (double)Wv[bidx(S, ic, jc, kc + 1)]);
+                        W[v * N + c] = (WT)(w0 + gx * sx + gy * sy + gz * sz);
+                    }
+                }
+            }
+        }
+        // the lower faces of this ghost cell that the flux kernel reads: normal
+        // index 0..n, transverse index -1..n, outside the block's own faces
+        // (transverse 0..n-1)
+        for (int d = 0; d < 3; d++) {
+            int cc[3] = {i, j, k};
+            if (cc[d] < 0 || cc[d] > n) continue;
+            bool need = true;
+            for (int q = 0; q < 3; q++)
+                if (q != d && (cc[q] < -1 || cc[q] > n)) need = false;
+            if (!need) continue;
+            int t[3] = {i, j, k};
+            int s = ghost_source(G, b, n, d, t[0], t[1], t[2]);
+            const bh_fx_block S = G.blk[s];
+            const int kind = S.n == n ? 0 : (S.n > n ? 1 : 2);
+            if ((kind == 2) != (pass > 0)) continue;
+            const double* Bd = Bf + d * N;
+            double v;
+            if (kind == 0) {
+                v = Bd[bidx(S, t[0], t[1], t[2])];
+            } else if (kind == 1) {
+                // the 4 fine faces on this coarse face
+                int f[3] = {2 * t[0], 2 * t[1], 2 * t[2]};
+                const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+                double sum = 0.0;
+                for (int a = 0; a < 2; a++)
+                    for (int q = 0; q < 2; q++) {
+                        int g[3] = {f[0], f[1], f[2]};
+                        g[t1] += a;
+                        g[t2] += q;
+                        sum += Bd[bidx(S, g[0], g[1], g[2])];
+                    }
+                v = 0.25 * sum;
+            } else {
+                int g[3] = {t[0] >> 1, t[1] >> 1, t[2] >> 1};
+                if (t[d] & 1) {   // between two coarse faces
+                    int h[3] = {g[0], g[1], g[2]};
+                    h[d] += 1;
+                    v = 0.5 * (Bd[bidx(S, g[0], g[1], g[2])] + Bd[bidx(S, h[0], h[1], h[2])]);
+                } else {
+                    v = Bd[bidx(S, g[0], g[1], g[2])];
+                }
+            }
+            Bf[d * N + c] = v;
+        }
+    });
 }
 
 // ======================================================================
@@ -273,17 +386,19 @@ __device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_bloc
 }
 
 template <typename RT, typename WT, typename FT, int MINB>
-__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux(FxPar P, Grid G, const int32_t* items, int stage) {
-    const int32_t b = items[2 * blockIdx.x];
-    const bh_fx_block B = G.blk[b];
-    const int n = B.n, m = n + 2;
-    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
-    if (e >= m * m * m) return;
-    const int i = e / (m * m) - 1, j = (e / m) % m - 1, k = e % m - 1;
-    const double* Bfs = stage ? G.Bf1 : G.Bf;
-    if (i >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 0, Bfs);
-    if (j >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 1, Bfs);
-    if (k >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 2, Bfs);
+__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux(FxPar P, Grid G, const int32_t* items, int stage, Queue Q) {
+    for_items(Q, [&](int t) {
+        const int32_t b = items[2 * t];
+        const bh_fx_block B = G.blk[b];
+        const int n = B.n, m = n + 2;
+        const int e = items[2 * t + 1] + threadIdx.x;
+        if (e >= m * m * m) return;
+        const int i = e / (m * m) - 1, j = (e / m) % m - 1, k = e % m - 1;
+        const double* Bfs = stage ? G.Bf1 : G.Bf;
+        if (i >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 0, Bfs);
+        if (j >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 1, Bfs);
+        if (k >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 2, Bfs);
+    });
 }
 
 // ======================================================================
@@ -319,7 +434,15 @@ __device__ inline void face_update(const Grid& G, int d, int64_t c, int si, int 
                                    int stage) {
     const int64_t N = G.ncell;
     double curl;
-    if (d == 0)
+    if (G.E) {   // the edge EMFs of the grid (corrected at level changes)
+        const double *Ex = G.E, *Ey = G.E + N, *Ez = G.E + 2 * N;
+        if (d == 0)
+            curl = (Ez[c + sj] - Ez[c]) * idx - (Ey[c + sk] - Ey[c]) * idx;
+        else if (d == 1)
+            curl = (Ex[c + sk] - Ex[c]) * idx - (Ez[c + si] - Ez[c]) * idx;
+        else
+            curl = (Ey[c + si] - Ey[c]) * idx - (Ex[c + sj] - Ex[c]) * idx;
+    } else if (d == 0)
         curl = (emf_z<FT>(G, c + sj, si, sj) - emf_z<FT>(G, c, si, sj)) * idx -
                (emf_y<FT>(G, c + sk, si, sk) - emf_y<FT>(G, c, si, sk)) * idx;
     else if (d == 1)
@@ -334,49 +457,117 @@ __device__ inline void face_update(const Grid& G, int d, int64_t c, int si, int 
         G.Bf[d * N + c] = 0.5 * (G.Bf[d * N + c] + G.Bf1[d * N + c] - dt * curl);
 }
 
+// edge EMFs of every block (the edges its face updates read: E_x at
+// i in [0,n), j, k in [0,n], and alike), from the face fluxes
+template <typename FT>
+__global__ void __launch_bounds__(FX_TPB) k_fx_emf(Grid G, const int32_t* items, Queue Q) {
+    for_items(Q, [&](int t) {
+        const int32_t b = items[2 * t];
+        const bh_fx_block B = G.blk[b];
+        const int n = B.n, m = n + 2;
+        const int e = items[2 * t + 1] + threadIdx.x;
+        if (e >= m * m * m) return;
+        const int i = e / (m * m) - 1, j = (e / m) % m - 1, k = e % m - 1;
+        if (i < 0 || j < 0 || k < 0) return;
+        const int64_t N = G.ncell, c = bidx(B, i, j, k);
+        const int si = bstride_i(B), sj = bstride_j(B), sk = 1;
+        if (i < n) G.E[c] = emf_x<FT>(G, c, sj, sk);
+        if (j < n) G.E[N + c] = emf_y<FT>(G, c, si, sk);
+        if (k < n) G.E[2 * N + c] = emf_z<FT>(G, c, si, sj);
+    });
+}
+
+// EMF correction at level changes: an edge on a block's boundary that a
+// finer block also touches takes the mean of that block's two EMFs along it,
+// so every copy of a shared face sees the same circulation and the face
+// field of the coarse side stays the mean of the fine faces (div B at
+// roundoff).  Levels differ by one at most, so one pass suffices.
+__global__ void __launch_bounds__(FX_TPB) k_fx_emf_fix(Grid G, const int32_t* items, Queue Q) {
+    for_items(Q, [&](int t) {
+        const int32_t b = items[2 * t];
+        const bh_fx_block B = G.blk[b];
+        const int n = B.n, m = n + 2;
+        const int e = items[2 * t + 1] + threadIdx.x;
+        if (e >= m * m * m) return;
+        const int p[3] = {e / (m * m) - 1, (e / m) % m - 1, e % m - 1};
+        if (p[0] < 0 || p[1] < 0 || p[2] < 0) return;
+        const int64_t N = G.ncell;
+        const int32_t* nb = G.nbr + (int64_t)b * 27;
+        for (int d = 0; d < 3; d++) {          // edge direction
+            if (p[d] >= n) continue;
+            const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+            const int o1 = p[t1] == 0 ? -1 : (p[t1] == n ? 1 : 0);
+            const int o2 = p[t2] == 0 ? -1 : (p[t2] == n ? 1 : 0);
+            if (o1 == 0 && o2 == 0) continue;  // not on the boundary
+            // the cubes sharing the edge: offsets (a1 o1, a2 o2), (a1, a2) != (0, 0)
+            for (int a1 = 0; a1 <= (o1 != 0); a1++)
+                for (int a2 = 0; a2 <= (o2 != 0); a2++) {
+                    if (!a1 && !a2) continue;
+                    int o[3] = {0, 0, 0};
+                    o[t1] = a1 * o1;
+                    o[t2] = a2 * o2;
+                    const int s = nb[(o[0] + 1) * 9 + (o[1] + 1) * 3 + (o[2] + 1)];
+                    if (s < 0) continue;
+                    const bh_fx_block S = G.blk[s];
+                    if (S.n != 2 * n) continue;
+                    // the two fine edges along this one, in the finer block's frame
+                    int f[3] = {2 * (p[0] - o[0] * n), 2 * (p[1] - o[1] * n), 2 * (p[2] - o[2] * n)};
+                    int g[3] = {f[0], f[1], f[2]};
+                    g[d] += 1;
+                    const double* Es = G.E + d * N;
+                    G.E[d * N + bidx(B, p[0], p[1], p[2])] = 0.5 * (Es[bidx(S, f[0], f[1], f[2])] + Es[bidx(S, g[0], g[1], g[2])]);
+                    a1 = 2;   // done with this edge
+                    break;
+                }
+        }
+    });
+}
+
 template <typename RT, typename WT, typename FT, int MINB>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, const int32_t* items, int stage,
-                                                      double cfl) {
-    const int32_t b = items[2 * blockIdx.x];
-    const bh_fx_block B = G.blk[b];
-    const int n = B.n;
-    const int e = items[2 * blockIdx.x + 1] + threadIdx.x;
-    if (e >= n * n * n) return;
-    const int i = e / (n * n), j = (e / n) % n, k = e % n;
-    const int64_t N = G.ncell;
-    const int64_t c = bidx(B, i, j, k);
-    const int si = bstride_i(B), sj = bstride_j(B), sk = 1;
-    const double dt = cfl * G.dt[0];
-    if (stage == 0 && blockIdx.x == 0 && threadIdx.x == 0) G.dt[1] = dt;
-    const double idx = 1.0 / B.dx;
-    // source at the cell centre from the stage's primitives
-    double x[3];
-    cell_centre(B, i, j, k, x);
-    KSb<RT> mk;
-    KSDb<RT> dk;
-    cell_geometry<RT>(P, x, mk, dk);
-    const WT* W = (const WT*)G.W;
-    RT w[8];
-    for (int v = 0; v < 8; v++) w[v] = RT(W[v * N + c]);
-    RT S[8];
-    source<RT>(mk, dk, RT(P.gamma), w, S);
-    for (int v = 0; v < 5; v++) {
-        double div = (fget<FT>(G, 0, v, c + si) - fget<FT>(G, 0, v, c)) * idx +
-                     (fget<FT>(G, 1, v, c + sj) - fget<FT>(G, 1, v, c)) * idx +
-                     (fget<FT>(G, 2, v, c + sk) - fget<FT>(G, 2, v, c)) * idx;
-        double L = (double)S[v] - div;
-        if (stage == 0)
-            G.U1[v * N + c] = G.U[v * N + c] + dt * L;
-        else
-            G.U[v * N + c] = 0.5 * (G.U[v * N + c] + G.U1[v * N + c] + dt * L);
-    }
-    // face field: this cell's three lower faces, and the upper boundary faces
-    face_update<FT>(G, 0, c, si, sj, sk, idx, dt, stage);
-    face_update<FT>(G, 1, c, si, sj, sk, idx, dt, stage);
-    face_update<FT>(G, 2, c, si, sj, sk, idx, dt, stage);
-    if (i == n - 1) face_update<FT>(G, 0, c + si, si, sj, sk, idx, dt, stage);
-    if (j == n - 1) face_update<FT>(G, 1, c + sj, si, sj, sk, idx, dt, stage);
-    if (k == n - 1) face_update<FT>(G, 2, c + sk, si, sj, sk, idx, dt, stage);
+                                                      double cfl, Queue Q) {
+    for_items(Q, [&](int t) {
+        const int32_t b = items[2 * t];
+        const bh_fx_block B = G.blk[b];
+        const int n = B.n;
+        const int e = items[2 * t + 1] + threadIdx.x;
+        if (e >= n * n * n) return;
+        const int i = e / (n * n), j = (e / n) % n, k = e % n;
+        const int64_t N = G.ncell;
+        const int64_t c = bidx(B, i, j, k);
+        const int si = bstride_i(B), sj = bstride_j(B), sk = 1;
+        const double dt = cfl * G.dt[0];
+        if (stage == 0 && t == 0 && threadIdx.x == 0) G.dt[1] = dt;
+        const double idx = 1.0 / B.dx;
+        // source at the cell centre from the stage's primitives
+        double x[3];
+        cell_centre(B, i, j, k, x);
+        KSb<RT> mk;
+        KSDb<RT> dk;
+        cell_geometry<RT>(P, x, mk, dk);
+        const WT* W = (const WT*)G.W;
+        RT w[8];
+        for (int v = 0; v < 8; v++) w[v] = RT(W[v * N + c]);
+        RT S[8];
+        source<RT>(mk, dk, RT(P.gamma), w, S);
+        for (int v = 0; v < 5; v++) {
+            double div = (fget<FT>(G, 0, v, c + si) - fget<FT>(G, 0, v, c)) * idx +
+                         (fget<FT>(G, 1, v, c + sj) - fget<FT>(G, 1, v, c)) * idx +
+                         (fget<FT>(G, 2, v, c + sk) - fget<FT>(G, 2, v, c)) * idx;
+            double L = (double)S[v] - div;
+            if (stage == 0)
+                G.U1[v * N + c] = G.U[v * N + c] + dt * L;
+            else
+                G.U[v * N + c] = 0.5 * (G.U[v * N + c] + G.U1[v * N + c] + dt * L);
+        }
+        // face field: this cell's three lower faces, and the upper boundary faces
+        face_update<FT>(G, 0, c, si, sj, sk, idx, dt, stage);
+        face_update<FT>(G, 1, c, si, sj, sk, idx, dt, stage);
+        face_update<FT>(G, 2, c, si, sj, sk, idx, dt, stage);
+        if (i == n - 1) face_update<FT>(G, 0, c + si, si, sj, sk, idx, dt, stage);
+        if (j == n - 1) face_update<FT>(G, 1, c + sj, si, sj, sk, idx, dt, stage);
+        if (k == n - 1) face_update<FT>(G, 2, c + sk, si, sj, sk, idx, dt, stage);
+    });
 }
 
 // ======================================================================
@@ -480,8 +671,27 @@ __device__ inline void apot(const TorusK& T, double rmax, double x, double y, do
         ay = A * x * iw;
     }
 }
-// face field = curl of the edge potential (A_z = 0), unscaled
-__global__ void __launch_bounds__(FX_TPB) k_fxi_faces(Grid G, const int32_t* items, TorusK T, double* scratch) {
+// face field = curl of the edge potential (A_z = 0), unscaled.  An edge's
+// A is the mean of A at the midpoints of its sub-edges at the finest level
+// of the grid (2^(maxlevel - level) of them), so that a coarse face's
+// circulation equals the mean of the finer faces that cover it.
+__device__ inline void apot_edge(const TorusK& T, double rmax, double x, double y, double z, int d, double h, int K,
+                                 double& ax, double& ay) {
+    double sx = 0.0, sy = 0.0, p[3] = {x, y, z};
+    const double hk = h / K;
+    for (int q = 0; q < K; q++) {
+        double r[3] = {p[0], p[1], p[2]};
+        r[d] = p[d] + (q + 0.5) * hk;
+        double a, b;
+        apot(T, rmax, r[0], r[1], r[2], a, b);
+        sx += a;
+        sy += b;
+    }
+    ax = sx / K;
+    ay = sy / K;
+}
+__global__ void __launch_bounds__(FX_TPB) k_fxi_faces(Grid G, const int32_t* items, TorusK T, double* scratch,
+                                                      int maxlevel) {
     const int32_t b = items[2 * blockIdx.x];
     const bh_fx_block B = G.blk[b];
     const int n = B.n, m = n + 2;
@@ -491,23 +701,24 @@ __global__ void __launch_bounds__(FX_TPB) k_fxi_faces(Grid G, const int32_t* ite
     const int64_t N = G.ncell, c = bidx(B, i, j, k);
     const double rmax = scratch[0], h = B.dx;
     const double X = B.x0[0], Y = B.x0[1], Z = B.x0[2];
+    const int K = 1 << (maxlevel - B.level);
     double ax0, ay0, ax1, ay1, d0, d1;
     if (i >= 0) {   // x-face (i-1/2, j, k): -(A_y(k+1/2) - A_y(k-1/2)) / dz, y-edges at (i-1/2, j, k -+ 1/2)
-        apot(T, rmax, X + i * h, Y + (j + 0.5) * h, Z + k * h, d0, ay0);
-        apot(T, rmax, X + i * h, Y + (j + 0.5) * h, Z + (k + 1) * h, d1, ay1);
+        apot_edge(T, rmax, X + i * h, Y + j * h, Z + k * h, 1, h, K, d0, ay0);
+        apot_edge(T, rmax, X + i * h, Y + j * h, Z + (k + 1) * h, 1, h, K, d1, ay1);
         G.Bf[c] = -(ay1 - ay0) / h;
     }
     if (j >= 0) {   // y-face (i, j-1/2, k): (A_x(k+1/2) - A_x(k-1/2)) / dz, x-edges at (i, j-1/2, k -+ 1/2)
-        apot(T, rmax, X + (i + 0.5) * h, Y + j * h, Z + k * h, ax0, d0);
-        apot(T, rmax, X + (i + 0.5) * h, Y + j * h, Z + (k + 1) * h, ax1, d1);
+        apot_edge(T, rmax, X + i * h, Y + j * h, Z + k * h, 0, h, K, ax0, d0);
+        apot_edge(T, rmax, X + i * h, Y + j * h, Z + (k + 1) * h, 0, h, K, ax1, d1);
         G.Bf[N + c] = (ax1 - ax0) / h;
     }
     if (k >= 0) {   // z-face (i, j, k-1/2): dA_y/dx - dA_x/dy
         double ayl, ayr, axl, axr;
-        apot(T, rmax, X + i * h, Y + (j + 0.5) * h, Z + k * h, d0, ayl);
-        apot(T, rmax, X + (i + 1) * h, Y + (j + 0.5) * h, Z + k * h, d1, ayr);
-        apot(T, rmax, X + (i + 0.5) * h, Y + j * h, Z + k * h, axl, d0);
-        apot(T, rmax, X + (i + 0.5) * h, Y + (j + 1) * h, Z + k * h, axr, d1);
+        apot_edge(T, rmax, X + i * h, Y + j * h, Z + k * h, 1, h, K, d0, ayl);
+        apot_edge(T, rmax, X + (i + 1) * h, Y + j * h, Z + k * h, 1, h, K, d1, ayr);
+        apot_edge(T, rmax, X + i * h, Y + j * h, Z + k * h, 0, h, K, axl, d0);
+        apot_edge(T, rmax, X + i * h, Y + (j + 1) * h, Z + k * h, 0, h, K, axr, d1);
         G.Bf[2 * N + c] = (ayr - ayl) / h - (axr - axl) / h;
     }
 }
@@ -601,6 +812,39 @@ namespace {
 using FRT = BH_REAL;
 inline cudaStream_t fxs(void* s) { return (cudaStream_t)s; }
 inline int fx_launched() { return cudaGetLastError() == cudaSuccess ? BH_OK : BH_ECUDA; }
+// work-queue slots of the step kernels
+enum { QS_C2P = 0, QS_GHOST = 1, QS_FLUX = 2, QS_EMF = 3, QS_EMF_FIX = 4, QS_UPDATE = 5 };
+static_assert(QS_UPDATE + 1 == BH_FX_QSLOTS, "queue slots");
+inline fx::Queue fx_q(const bh_fx_grid* g, int slot, int nitem) {
+    if (!g->queue) return fx::Queue{nullptr, nullptr, nitem};
+    return fx::Queue{g->queue + 2 * slot, g->queue + 2 * slot + 1, nitem};
+}
+// CTAs of a launch: one per item, or (persistent) the resident CTAs of the
+// kernel on this device, from the occupancy calculator (cached per kernel)
+inline int fx_grid(const void* fn, int nitem, const bh_fx_grid* g) {
+    if (!g->queue) return nitem;
+    int ctas = g->queue_ctas;
+    if (ctas <= 0) {
+        static const void* keys[96];
+        static int vals[96];
+        static int nkeys = 0;
+        int occ = 0;
+        for (int i = 0; i < nkeys; i++)
+            if (keys[i] == fn) occ = vals[i];
+        if (!occ) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, fx::FX_TPB, 0) != cudaSuccess || occ < 1) occ = 1;
+            if (nkeys < 96) { keys[nkeys] = fn; vals[nkeys] = occ; nkeys++; }
+        }
+        static int sms = 0;
+        if (!sms) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+        }
+        ctas = sms * occ;
+    }
+    return nitem < ctas ? nitem : ctas;
+}
 }  // namespace
 
 // launch bounds of the heavy kernels: resident 128-thread CTAs per SM asked
@@ -632,7 +876,7 @@ int fx_prims(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t 
     fx::Grid G = fx::grid_of(g);
     if (with_dt) fx::k_fx_dt_init<<<1, 1, 0, fxs(s)>>>(g->dt);
     if (g->nitem_cell) {
-#define L_(M) fx::k_fx_c2p<FRT, FRT, M><<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt)
+#define L_(M) fx::k_fx_c2p<FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_c2p<FRT, FRT, M>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt, fx_q(g, QS_C2P, g->nitem_cell))
         FX_TUNED(BH_FX_TUNE_C2P, L_)
 #undef L_
     }
@@ -640,14 +884,18 @@ int fx_prims(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t 
 }
 int fx_ghosts(const bh_fx_params*, const bh_fx_grid* g, int32_t stage, void* s) {
     fx::Grid G = fx::grid_of(g);
-    if (g->nitem_ghost) fx::k_fx_ghost<FRT><<<g->nitem_ghost, fx::FX_TPB, 0, fxs(s)>>>(G, g->items_ghost, stage);
+    // pass 0: copies and restrictions; pass l: prolongations into level l
+    for (int pass = 0; pass <= g->maxlevel; pass++)
+        if (g->nitem_ghost)
+            fx::k_fx_ghost<FRT><<<fx_grid((const void*)fx::k_fx_ghost<FRT>, g->nitem_ghost, g), fx::FX_TPB, 0, fxs(s)>>>(
+                G, g->items_ghost, stage, pass, fx_q(g, QS_GHOST, g->nitem_ghost));
     return fx_launched();
 }
 int fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
     if (g->nitem_pos) {
-#define L_(M) fx::k_fx_flux<FRT, FRT, FRT, M><<<g->nitem_pos, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_pos, stage)
+#define L_(M) fx::k_fx_flux<FRT, FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_flux<FRT, FRT, FRT, M>, g->nitem_pos, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_pos, stage, fx_q(g, QS_FLUX, g->nitem_pos))
         FX_TUNED(BH_FX_TUNE_FLUX, L_)
 #undef L_
     }
@@ -656,8 +904,15 @@ int fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s
 int fx_update(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
+    if (g->E && g->nitem_pos) {
+        fx::k_fx_emf<FRT><<<fx_grid((const void*)fx::k_fx_emf<FRT>, g->nitem_pos, g), fx::FX_TPB, 0, fxs(s)>>>(
+            G, g->items_pos, fx_q(g, QS_EMF, g->nitem_pos));
+        if (g->maxlevel > 0)
+            fx::k_fx_emf_fix<<<fx_grid((const void*)fx::k_fx_emf_fix, g->nitem_pos, g), fx::FX_TPB, 0, fxs(s)>>>(
+                G, g->items_pos, fx_q(g, QS_EMF_FIX, g->nitem_pos));
+    }
     if (g->nitem_cell) {
-#define L_(M) fx::k_fx_update<FRT, FRT, FRT, M><<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, P->cfl)
+#define L_(M) fx::k_fx_update<FRT, FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_update<FRT, FRT, FRT, M>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, P->cfl, fx_q(g, QS_UPDATE, g->nitem_cell))
         FX_TUNED(BH_FX_TUNE_UPDATE, L_)
 #undef L_
     }
@@ -692,7 +947,7 @@ int fx_torus_init(const bh_fx_params* P, const bh_fx_grid* g, const bh_fx_torus*
     if (cudaMemsetAsync(g->Bf, 0, 3 * sizeof(double) * g->ncell, st) != cudaSuccess) return BH_ECUDA;
     fx::k_fxi_rho<<<g->nitem_cell, fx::FX_TPB, 0, st>>>(G, g->items_cell, tk, scratch);
     fx::k_fxi_prims<FRT><<<g->nitem_cell, fx::FX_TPB, 0, st>>>(p, G, g->items_cell, tk, scratch);
-    fx::k_fxi_faces<<<g->nitem_pos, fx::FX_TPB, 0, st>>>(G, g->items_pos, tk, scratch);
+    fx::k_fxi_faces<<<g->nitem_pos, fx::FX_TPB, 0, st>>>(G, g->items_pos, tk, scratch, g->maxlevel);
     fx::k_fxi_pmag<FRT><<<g->nitem_cell, fx::FX_TPB, 0, st>>>(p, G, g->items_cell, scratch);
     fx::k_fxi_scale<<<g->nitem_pos, fx::FX_TPB, 0, st>>>(G, g->items_pos, T->beta, scratch);
     fx::k_fxi_cons<FRT><<<g->nitem_cell, fx::FX_TPB, 0, st>>>(p, G, g->items_cell);

@@ -373,7 +373,11 @@ int bh_step_graph_destroy(bh_step_graph *g);
  * the floor state at rest every stage).
  *
  * Layout: a list of cubic blocks of n^3 interior cells (n a multiple of 8)
- * with two ghost layers; every array stores each block as a (n+5)^3 box
+ * with two ghost layers.  Blocks are equal cubes of space; a block of level
+ * l holds twice the cells per axis of level l-1 (the 27-neighbour table
+ * links equal cubes, whose levels differ by one at most): ghost cells of a
+ * coarser or finer neighbour are prolonged or restricted, and the edge EMFs
+ * of a coarse block along a finer one take the finer block's values; every array stores each block as a (n+5)^3 box
  * (cells -2 .. n+2 per axis) at offset blocks[b].off, index
  * ((i+2) S + (j+2)) S + (k+2), S = n + 5 (i slowest, k fastest, as the
  * reference's patches).  The x-face (i-1/2, j, k), y-face (i, j-1/2, k) and
@@ -430,7 +434,19 @@ typedef struct bh_fx_grid {
                                     speed|, dt[1] the step's time step cfl dt[0]    */
     int32_t *count;              /* device [4]: con2prim failures, floored cells     */
     int32_t *err;                /* device error word                                */
+    double *E;                   /* [3][ncell] edge EMFs, or NULL: computed on the fly
+                                    (allowed only when every block has one level)  */
+    int32_t maxlevel;            /* highest block level (0: one level)               */
+    int32_t queue_ctas;          /* CTAs of a persistent launch (0: the SMs times the
+                                    CTAs the kernel keeps resident per SM)          */
+    int32_t *queue;              /* device [2 * BH_FX_QSLOTS], zeroed once before the
+                                    first launch, or NULL.  Set: every step kernel is
+                                    launched persistent, its CTAs taking work items
+                                    from a counter in this array (the counters reset
+                                    themselves at the end of each launch).  NULL: one
+                                    CTA per work item.  Both give the same results. */
 } bh_fx_grid;
+#define BH_FX_QSLOTS 6
 
 /* Launch bounds of the scheme's three heavy kernels (no counterpart in the
  * reference): each is compiled for 1 (no register cap), 3, 4, 5 and 6

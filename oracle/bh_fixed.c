@@ -566,34 +566,104 @@ static int gsrc(const int32_t* nbr, int b, int n, int fdim, int* c) {
     return s;
 }
 
+/* minmod of the two differences around b */
+static double mm_slope(double a, double b, double c) {
+    double l = b - a, r = c - b;
+    if (l * r <= 0.0) return 0.0;
+    return dabs(l) < dabs(r) ? l : r;
+}
+
+/* Ghost fill over blocks of several levels (equal cubes, levels one apart
+ * at most): a same-level image is copied, a finer one averaged (8 cells or
+ * 4 faces), a coarser one interpolated (the covering cell plus a quarter of
+ * its minmod slope per direction; a face takes the coarse face it lies on
+ * or the mean of the two it lies between).  Pass 0: copies and
+ * restrictions; pass l: prolongations into level-l blocks. */
 void fxo_ghosts(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, double* W, double* Bf,
-                double* Bf1, int stage) {
+                double* Bf1, int stage, int maxlevel) {
     double* F = stage ? Bf1 : Bf;
-    for (int b = 0; b < nblock; b++) {
-        int n = blk[b].n;
+    for (int pass = 0; pass <= maxlevel; pass++)
+        for (int b = 0; b < nblock; b++) {
+            int n = blk[b].n;
+            if (pass > 0 && blk[b].level != pass) continue;
 #pragma omp parallel for schedule(static)
-        for (int i = -2; i < n + 2; i++)
-            for (int j = -2; j < n + 2; j++)
-                for (int k = -2; k < n + 2; k++) {
-                    if (i >= 0 && i < n && j >= 0 && j < n && k >= 0 && k < n) continue;
-                    int64_t c = bx(&blk[b], i, j, k);
-                    int q[3] = {i, j, k};
-                    int s = gsrc(nbr, b, n, -1, q);
-                    int64_t sc = bx(&blk[s], q[0], q[1], q[2]);
-                    for (int v = 0; v < 8; v++) W[v * N + c] = W[v * N + sc];
-                    for (int d = 0; d < 3; d++) {
-                        int cc[3] = {i, j, k};
-                        if (cc[d] < 0 || cc[d] > n) continue;
-                        int need = 1;
-                        for (int e = 0; e < 3; e++)
-                            if (e != d && (cc[e] < -1 || cc[e] > n)) need = 0;
-                        if (!need) continue;
-                        int fq[3] = {i, j, k};
-                        int fs = gsrc(nbr, b, n, d, fq);
-                        F[d * N + c] = F[d * N + bx(&blk[fs], fq[0], fq[1], fq[2])];
+            for (int i = -2; i < n + 2; i++)
+                for (int j = -2; j < n + 2; j++)
+                    for (int k = -2; k < n + 2; k++) {
+                        if (i >= 0 && i < n && j >= 0 && j < n && k >= 0 && k < n) continue;
+                        int64_t c = bx(&blk[b], i, j, k);
+                        int q[3] = {i, j, k};
+                        int s = gsrc(nbr, b, n, -1, q);
+                        const fxo_block* S = &blk[s];
+                        int kind = S->n == n ? 0 : (S->n > n ? 1 : 2);
+                        if ((kind == 2) == (pass > 0)) {
+                            if (kind == 0) {
+                                int64_t sc = bx(S, q[0], q[1], q[2]);
+                                for (int v = 0; v < 8; v++) W[v * N + c] = W[v * N + sc];
+                            } else if (kind == 1) {
+                                for (int v = 0; v < 8; v++) {
+                                    double sum = 0.0;
+                                    for (int a = 0; a < 2; a++)
+                                        for (int e = 0; e < 2; e++)
+                                            for (int r = 0; r < 2; r++)
+                                                sum += W[v * N + bx(S, 2 * q[0] + a, 2 * q[1] + e, 2 * q[2] + r)];
+                                    W[v * N + c] = 0.125 * sum;
+                                }
+                            } else {
+                                int ic = q[0] >> 1, jc = q[1] >> 1, kc = q[2] >> 1;
+                                double gx = (q[0] & 1) ? 0.25 : -0.25, gy = (q[1] & 1) ? 0.25 : -0.25,
+                                       gz = (q[2] & 1) ? 0.25 : -0.25;
+                                for (int v = 0; v < 8; v++) {
+                                    const double* Wv = W + v * N;
+                                    double w0 = Wv[bx(S, ic, jc, kc)];
+                                    double sx = mm_slope(Wv[bx(S, ic - 1, jc, kc)], w0, Wv[bx(S, ic + 1, jc, kc)]);
+                                    double sy = mm_slope(Wv[bx(S, ic, jc - 1, kc)], w0, Wv[bx(S, ic, jc + 1, kc)]);
+                                    double sz = mm_slope(Wv[bx(S, ic, jc, kc - 1)], w0, Wv[bx(S, ic, jc, kc + 1)]);
+                                    W[v * N + c] = w0 + gx * sx + gy * sy + gz * sz;
+                                }
+                            }
+                        }
+                        for (int d = 0; d < 3; d++) {
+                            int cc[3] = {i, j, k};
+                            if (cc[d] < 0 || cc[d] > n) continue;
+                            int need = 1;
+                            for (int e = 0; e < 3; e++)
+                                if (e != d && (cc[e] < -1 || cc[e] > n)) need = 0;
+                            if (!need) continue;
+                            int t[3] = {i, j, k};
+                            int fs = gsrc(nbr, b, n, d, t);
+                            const fxo_block* T = &blk[fs];
+                            int fk = T->n == n ? 0 : (T->n > n ? 1 : 2);
+                            if ((fk == 2) != (pass > 0)) continue;
+                            const double* Bd = F + d * N;
+                            double v;
+                            if (fk == 0) {
+                                v = Bd[bx(T, t[0], t[1], t[2])];
+                            } else if (fk == 1) {
+                                int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+                                double sum = 0.0;
+                                for (int a = 0; a < 2; a++)
+                                    for (int e = 0; e < 2; e++) {
+                                        int g[3] = {2 * t[0], 2 * t[1], 2 * t[2]};
+                                        g[t1] += a;
+                                        g[t2] += e;
+                                        sum += Bd[bx(T, g[0], g[1], g[2])];
+                                    }
+                                v = 0.25 * sum;
+                            } else {
+                                int g[3] = {t[0] >> 1, t[1] >> 1, t[2] >> 1};
+                                if (t[d] & 1) {
+                                    int h[3] = {g[0], g[1], g[2]};
+                                    h[d] += 1;
+                                    v = 0.5 * (Bd[bx(T, g[0], g[1], g[2])] + Bd[bx(T, h[0], h[1], h[2])]);
+                                } else {
+                                    v = Bd[bx(T, g[0], g[1], g[2])];
+                                }
+                            }
+                            F[d * N + c] = v;
+                        }
                     }
-                }
-    }
+        }
 }
 
 static void face(const fxo_params* P, const fxo_block* B, int64_t N, const double* W, const double* Bfs, double* F,
@@ -646,18 +716,73 @@ static double ey_(const double* F, int64_t N, int64_t c, int si, int sk) {
 static double ez_(const double* F, int64_t N, int64_t c, int si, int sj) {
     return 0.25 * (FG(1, CB + 0, c) + FG(1, CB + 0, c - si) - FG(0, CB + 1, c) - FG(0, CB + 1, c - sj));
 }
-static void fupd(const double* F, int64_t N, double* Bf, double* Bf1, int d, int64_t c, int si, int sj, int sk,
+/* edge EMFs of every block (E_x at i in [0,n), j, k in [0,n], alike for y,
+ * z) from the face fluxes; then, where a finer block touches a boundary
+ * edge, the mean of its two EMFs along that edge */
+void fxo_emf(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, const double* F, double* E,
+             int maxlevel) {
+    for (int b = 0; b < nblock; b++) {
+        const fxo_block* B = &blk[b];
+        int n = B->n, si = (n + 5) * (n + 5), sj = n + 5, sk = 1;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i <= n; i++)
+            for (int j = 0; j <= n; j++)
+                for (int k = 0; k <= n; k++) {
+                    int64_t c = bx(B, i, j, k);
+                    if (i < n) E[c] = ex_(F, N, c, sj, sk);
+                    if (j < n) E[N + c] = ey_(F, N, c, si, sk);
+                    if (k < n) E[2 * N + c] = ez_(F, N, c, si, sj);
+                }
+    }
+    if (maxlevel == 0) return;
+    for (int b = 0; b < nblock; b++) {
+        const fxo_block* B = &blk[b];
+        int n = B->n;
+        const int32_t* nb = nbr + (int64_t)b * 27;
+        for (int i = 0; i <= n; i++)
+            for (int j = 0; j <= n; j++)
+                for (int k = 0; k <= n; k++) {
+                    int p[3] = {i, j, k};
+                    for (int d = 0; d < 3; d++) {
+                        if (p[d] >= n) continue;
+                        int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+                        int o1 = p[t1] == 0 ? -1 : (p[t1] == n ? 1 : 0);
+                        int o2 = p[t2] == 0 ? -1 : (p[t2] == n ? 1 : 0);
+                        if (o1 == 0 && o2 == 0) continue;
+                        int done = 0;
+                        for (int a1 = 0; a1 <= (o1 != 0) && !done; a1++)
+                            for (int a2 = 0; a2 <= (o2 != 0) && !done; a2++) {
+                                if (!a1 && !a2) continue;
+                                int o[3] = {0, 0, 0};
+                                o[t1] = a1 * o1;
+                                o[t2] = a2 * o2;
+                                int s = nb[(o[0] + 1) * 9 + (o[1] + 1) * 3 + (o[2] + 1)];
+                                if (s < 0) continue;
+                                const fxo_block* S = &blk[s];
+                                if (S->n != 2 * n) continue;
+                                int f[3] = {2 * (p[0] - o[0] * n), 2 * (p[1] - o[1] * n), 2 * (p[2] - o[2] * n)};
+                                int g[3] = {f[0], f[1], f[2]};
+                                g[d] += 1;
+                                const double* Es = E + d * N;
+                                E[d * N + bx(B, p[0], p[1], p[2])] =
+                                    0.5 * (Es[bx(S, f[0], f[1], f[2])] + Es[bx(S, g[0], g[1], g[2])]);
+                                done = 1;
+                            }
+                    }
+                }
+    }
+}
+
+static void fupd(const double* E, int64_t N, double* Bf, double* Bf1, int d, int64_t c, int si, int sj, int sk,
                  double idx, double dt, int stage) {
+    const double *Ex = E, *Ey = E + N, *Ez = E + 2 * N;
     double curl;
     if (d == 0)
-        curl = (ez_(F, N, c + sj, si, sj) - ez_(F, N, c, si, sj)) * idx -
-               (ey_(F, N, c + sk, si, sk) - ey_(F, N, c, si, sk)) * idx;
+        curl = (Ez[c + sj] - Ez[c]) * idx - (Ey[c + sk] - Ey[c]) * idx;
     else if (d == 1)
-        curl = (ex_(F, N, c + sk, sj, sk) - ex_(F, N, c, sj, sk)) * idx -
-               (ez_(F, N, c + si, si, sj) - ez_(F, N, c, si, sj)) * idx;
+        curl = (Ex[c + sk] - Ex[c]) * idx - (Ez[c + si] - Ez[c]) * idx;
     else
-        curl = (ey_(F, N, c + si, si, sk) - ey_(F, N, c, si, sk)) * idx -
-               (ex_(F, N, c + sj, sj, sk) - ex_(F, N, c, sj, sk)) * idx;
+        curl = (Ey[c + si] - Ey[c]) * idx - (Ex[c + sj] - Ex[c]) * idx;
     if (stage == 0)
         Bf1[d * N + c] = Bf[d * N + c] - dt * curl;
     else
@@ -665,7 +790,7 @@ static void fupd(const double* F, int64_t N, double* Bf, double* Bf1, int d, int
 }
 
 void fxo_update(const fxo_params* P, int32_t nblock, const fxo_block* blk, int64_t N, double* U, double* U1,
-                const double* W, double* Bf, double* Bf1, const double* F, double* dt, int stage) {
+                const double* W, double* Bf, double* Bf1, const double* F, const double* E, double* dt, int stage) {
     double dtv = P->cfl * dt[0];
     if (stage == 0) dt[1] = dtv;
     for (int b = 0; b < nblock; b++) {
@@ -695,23 +820,25 @@ void fxo_update(const fxo_params* P, int32_t nblock, const fxo_block* blk, int64
                         else
                             U[v * N + c] = 0.5 * (U[v * N + c] + U1[v * N + c] + dtv * L);
                     }
-                    fupd(F, N, Bf, Bf1, 0, c, si, sj, sk, idx, dtv, stage);
-                    fupd(F, N, Bf, Bf1, 1, c, si, sj, sk, idx, dtv, stage);
-                    fupd(F, N, Bf, Bf1, 2, c, si, sj, sk, idx, dtv, stage);
-                    if (i == n - 1) fupd(F, N, Bf, Bf1, 0, c + si, si, sj, sk, idx, dtv, stage);
-                    if (j == n - 1) fupd(F, N, Bf, Bf1, 1, c + sj, si, sj, sk, idx, dtv, stage);
-                    if (k == n - 1) fupd(F, N, Bf, Bf1, 2, c + sk, si, sj, sk, idx, dtv, stage);
+                    fupd(E, N, Bf, Bf1, 0, c, si, sj, sk, idx, dtv, stage);
+                    fupd(E, N, Bf, Bf1, 1, c, si, sj, sk, idx, dtv, stage);
+                    fupd(E, N, Bf, Bf1, 2, c, si, sj, sk, idx, dtv, stage);
+                    if (i == n - 1) fupd(E, N, Bf, Bf1, 0, c + si, si, sj, sk, idx, dtv, stage);
+                    if (j == n - 1) fupd(E, N, Bf, Bf1, 1, c + sj, si, sj, sk, idx, dtv, stage);
+                    if (k == n - 1) fupd(E, N, Bf, Bf1, 2, c + sk, si, sj, sk, idx, dtv, stage);
                 }
     }
 }
 
 void fxo_step(const fxo_params* P, int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, double* U,
-              double* U1, double* W, double* Bf, double* Bf1, double* F, double* dt, int32_t* count) {
+              double* U1, double* W, double* Bf, double* Bf1, double* F, double* E, double* dt, int32_t* count,
+              int maxlevel) {
     for (int stage = 0; stage < 2; stage++) {
         fxo_prims(P, nblock, blk, nbr, N, U, U1, W, Bf, Bf1, F, dt, count, stage, stage == 0);
-        fxo_ghosts(nblock, blk, nbr, N, W, Bf, Bf1, stage);
+        fxo_ghosts(nblock, blk, nbr, N, W, Bf, Bf1, stage, maxlevel);
         fxo_fluxes(P, nblock, blk, N, W, Bf, Bf1, F, stage);
-        fxo_update(P, nblock, blk, N, U, U1, W, Bf, Bf1, F, dt, stage);
+        fxo_emf(nblock, blk, nbr, N, F, E, maxlevel);
+        fxo_update(P, nblock, blk, N, U, U1, W, Bf, Bf1, F, E, dt, stage);
     }
 }
 
@@ -923,10 +1050,27 @@ static void apot(const fmt* t, double rmax, double x, double y, double z, double
     }
 }
 
+/* A along an edge: the mean over its K finest-level sub-edge midpoints */
+static void apot_edge(const fmt* t, double rmax, double x, double y, double z, int d, double h, int K, double* ax,
+                      double* ay) {
+    double sx = 0.0, sy = 0.0, p[3] = {x, y, z};
+    double hk = h / K;
+    for (int q = 0; q < K; q++) {
+        double r[3] = {p[0], p[1], p[2]};
+        r[d] = p[d] + (q + 0.5) * hk;
+        double a, b;
+        apot(t, rmax, r[0], r[1], r[2], &a, &b);
+        sx += a;
+        sy += b;
+    }
+    *ax = sx / K;
+    *ay = sy / K;
+}
+
 /* the torus initial data of bh_fx_torus_init; out[4] as there */
 void fxo_torus_init(const fxo_params* P, int32_t nblock, const fxo_block* blk, int64_t N, double* U, double* W,
                     double* Bf, double r_in, double r_max, double kappa, double beta, double noise, uint64_t seed,
-                    double* out) {
+                    double* out, int maxlevel) {
     fmt t = {P->a, P->gamma, kappa, r_in, fm_ell(P->a, r_max), 0.0};
     t.w_in = fm_pot(P->a, t.ell, r_in, 1.0, 0.0);
     memset(Bf, 0, sizeof(double) * 3 * N);
@@ -978,27 +1122,28 @@ void fxo_torus_init(const fxo_params* P, int32_t nblock, const fxo_block* blk, i
         const fxo_block* B = &blk[b];
         int n = B->n;
         double h = B->dx, X = B->x0[0], Y = B->x0[1], Z = B->x0[2];
+        int K = 1 << (maxlevel - B->level);
         for (int i = -1; i <= n; i++)
             for (int j = -1; j <= n; j++)
                 for (int k = -1; k <= n; k++) {
                     int64_t c = bx(B, i, j, k);
                     double ax0, ay0, ax1, ay1, d0, d1;
                     if (i >= 0) {
-                        apot(&t, rmax, X + i * h, Y + (j + 0.5) * h, Z + k * h, &d0, &ay0);
-                        apot(&t, rmax, X + i * h, Y + (j + 0.5) * h, Z + (k + 1) * h, &d1, &ay1);
+                        apot_edge(&t, rmax, X + i * h, Y + j * h, Z + k * h, 1, h, K, &d0, &ay0);
+                        apot_edge(&t, rmax, X + i * h, Y + j * h, Z + (k + 1) * h, 1, h, K, &d1, &ay1);
                         Bf[c] = -(ay1 - ay0) / h;
                     }
                     if (j >= 0) {
-                        apot(&t, rmax, X + (i + 0.5) * h, Y + j * h, Z + k * h, &ax0, &d0);
-                        apot(&t, rmax, X + (i + 0.5) * h, Y + j * h, Z + (k + 1) * h, &ax1, &d1);
+                        apot_edge(&t, rmax, X + i * h, Y + j * h, Z + k * h, 0, h, K, &ax0, &d0);
+                        apot_edge(&t, rmax, X + i * h, Y + j * h, Z + (k + 1) * h, 0, h, K, &ax1, &d1);
                         Bf[N + c] = (ax1 - ax0) / h;
                     }
                     if (k >= 0) {
                         double ayl, ayr, axl, axr;
-                        apot(&t, rmax, X + i * h, Y + (j + 0.5) * h, Z + k * h, &d0, &ayl);
-                        apot(&t, rmax, X + (i + 1) * h, Y + (j + 0.5) * h, Z + k * h, &d1, &ayr);
-                        apot(&t, rmax, X + (i + 0.5) * h, Y + j * h, Z + k * h, &axl, &d0);
-                        apot(&t, rmax, X + (i + 0.5) * h, Y + (j + 1) * h, Z + k * h, &axr, &d1);
+                        apot_edge(&t, rmax, X + i * h, Y + j * h, Z + k * h, 1, h, K, &d0, &ayl);
+                        apot_edge(&t, rmax, X + (i + 1) * h, Y + j * h, Z + k * h, 1, h, K, &d1, &ayr);
+                        apot_edge(&t, rmax, X + i * h, Y + j * h, Z + k * h, 0, h, K, &axl, &d0);
+                        apot_edge(&t, rmax, X + i * h, Y + (j + 1) * h, Z + k * h, 0, h, K, &axr, &d1);
                         Bf[2 * N + c] = (ayr - ayl) / h - (axr - axl) / h;
                     }
                 }

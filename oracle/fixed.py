@@ -35,11 +35,12 @@ def lib():
         L = C.CDLL(path)
         P = C.POINTER(FxoParams)
         v, i32, i64, d = C.c_void_p, C.c_int32, C.c_int64, C.c_double
-        L.fxo_step.argtypes = [P, i32, v, v, i64] + [v] * 8
+        L.fxo_step.argtypes = [P, i32, v, v, i64] + [v] * 9 + [C.c_int]
         L.fxo_prims.argtypes = [P, i32, v, v, i64] + [v] * 8 + [C.c_int, C.c_int]
-        L.fxo_ghosts.argtypes = [i32, v, v, i64, v, v, v, C.c_int]
+        L.fxo_ghosts.argtypes = [i32, v, v, i64, v, v, v, C.c_int, C.c_int]
+        L.fxo_emf.argtypes = [i32, v, v, i64, v, v, C.c_int]
         L.fxo_fluxes.argtypes = [P, i32, v, i64, v, v, v, v, C.c_int]
-        L.fxo_update.argtypes = [P, i32, v, i64, v, v, v, v, v, v, v, C.c_int]
+        L.fxo_update.argtypes = [P, i32, v, i64, v, v, v, v, v, v, v, v, C.c_int]
         L.fxo_divb.argtypes = [i32, v, i64, v, v]
         L.fxo_metric_batch.argtypes = [P, i64, v, v, v, v]
         L.fxo_deriv_batch.argtypes = [P, i64, v, v, v, v]
@@ -52,7 +53,7 @@ def lib():
         L.fxo_fm_potential.restype = d
         L.fxo_fm_ell.argtypes = [d, d]
         L.fxo_fm_ell.restype = d
-        L.fxo_torus_init.argtypes = [P, i32, v, i64, v, v, v, d, d, d, d, d, C.c_uint64, v]
+        L.fxo_torus_init.argtypes = [P, i32, v, i64, v, v, v, d, d, d, d, d, C.c_uint64, v, C.c_int]
         _lib = L
     return _lib
 
@@ -87,6 +88,8 @@ class FxHost:
         self.Bf = np.zeros((3, N))
         self.Bf1 = np.zeros((3, N))
         self.F = np.zeros((3, 8, N))
+        self.E = np.zeros((3, N))
+        self.maxlevel = int(self.blocks["level"].max())
         self.dt = np.zeros(2)
         self.count = np.zeros(4, np.int32)
 
@@ -95,7 +98,7 @@ class FxHost:
 
     def step(self):
         lib().fxo_step(*self._g(), _p(self.U), _p(self.U1), _p(self.W), _p(self.Bf), _p(self.Bf1), _p(self.F),
-                       _p(self.dt), _p(self.count))
+                       _p(self.E), _p(self.dt), _p(self.count), self.maxlevel)
 
     def prims(self, stage=0, with_dt=False):
         lib().fxo_prims(*self._g(), _p(self.U), _p(self.U1), _p(self.W), _p(self.Bf), _p(self.Bf1), _p(self.F),
@@ -103,15 +106,21 @@ class FxHost:
 
     def ghosts(self, stage=0):
         lib().fxo_ghosts(len(self.blocks), _p(self.blocks), _p(self.nbr), self.N, _p(self.W), _p(self.Bf),
-                         _p(self.Bf1), stage)
+                         _p(self.Bf1), stage, self.maxlevel)
 
     def fluxes(self, stage=0):
         lib().fxo_fluxes(C.byref(self.prm), len(self.blocks), _p(self.blocks), self.N, _p(self.W), _p(self.Bf),
                          _p(self.Bf1), _p(self.F), stage)
 
+    def emf(self):
+        lib().fxo_emf(len(self.blocks), _p(self.blocks), _p(self.nbr), self.N, _p(self.F), _p(self.E),
+                      self.maxlevel)
+
     def update(self, stage=0):
+        """edge EMFs from the fluxes (corrected at level changes), then the update"""
+        self.emf()
         lib().fxo_update(C.byref(self.prm), len(self.blocks), _p(self.blocks), self.N, _p(self.U), _p(self.U1),
-                         _p(self.W), _p(self.Bf), _p(self.Bf1), _p(self.F), _p(self.dt), stage)
+                         _p(self.W), _p(self.Bf), _p(self.Bf1), _p(self.F), _p(self.E), _p(self.dt), stage)
 
     def divb(self) -> float:
         out = np.zeros(len(self.blocks))
@@ -121,7 +130,7 @@ class FxHost:
     def torus_init(self, r_in=6.0, r_max=12.0, kappa=1e-3, beta=100.0, noise=0.04, seed=1):
         out = np.zeros(4)
         lib().fxo_torus_init(C.byref(self.prm), len(self.blocks), _p(self.blocks), self.N, _p(self.U), _p(self.W),
-                             _p(self.Bf), r_in, r_max, kappa, beta, noise, seed, _p(out))
+                             _p(self.Bf), r_in, r_max, kappa, beta, noise, seed, _p(out), self.maxlevel)
         return {"ell": out[0], "rho_max_raw": out[1], "field_scale": out[2], "beta": out[3]}
 
     def interior(self, arr: np.ndarray) -> np.ndarray:

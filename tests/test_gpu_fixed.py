@@ -161,3 +161,99 @@ def test_mixed_torus_100_steps_128():
         assert e <= 1e-5, (name, errs)
     assert ref.divb() <= 1e-12 and mix.divb() <= 1e-12
     assert ref.counters()["c2p_failures"] == 0
+
+
+# ---- blocks of several levels (equal cubes at 8^3, 16^3, 32^3 cells) ------
+def _leveled(precision="fp64", nb=8, r_fine=(14.0, 26.0), seed=3):
+    from bhgpu.fixed import FxGrid, FxParams
+    from bhgrid.blocks import torus_levels
+    lv = torus_levels(nb=nb, r_fine=r_fine, seed=seed)
+    return FxGrid.leveled(-40.0, 40.0, lv, 8, FxParams(precision=precision))
+
+
+def test_leveled_grid_has_three_levels():
+    g = _leveled()
+    assert sorted(set(int(v) for v in g.blocks_np["level"])) == [0, 1, 2]
+    assert g.E is not None and g.maxlevel == 2
+
+
+def test_leveled_init_matches_oracle():
+    g = _leveled()
+    g.torus_init()
+    torch.cuda.synchronize()
+    h = _host(g)
+    h.torus_init()
+    for name in ("U", "W", "Bf"):
+        a, b = getattr(g, name).cpu().numpy(), getattr(h, name)
+        for v in range(a.shape[0]):
+            assert _rel_linf(a[v], b[v]) <= 1e-13, (name, v)
+    assert g.divb() <= 1e-14
+
+
+def test_leveled_steps_bitwise():
+    """ghost fill across levels (copies, restrictions, prolongations), the
+    EMF correction at level changes and the update: FP64 = oracle, bit for bit"""
+    g = _leveled()
+    g.torus_init()
+    h = _host(g)
+    _load(h, g)
+    for _ in range(2):
+        g.step()
+        h.step()
+    torch.cuda.synchronize()
+    for name in ("U", "Bf", "W", "E"):
+        assert np.array_equal(getattr(g, name).cpu().numpy(), getattr(h, name)), name
+    assert g.time_step() == h.dt[1]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_leveled_divergence_at_roundoff(precision):
+    g = _leveled(precision)
+    g.torus_init()
+    for _ in range(10):
+        g.step()
+    torch.cuda.synchronize()
+    assert g.divb() <= 1e-13
+    assert np.isfinite(g.U.cpu().numpy()).all()
+    assert g.counters()["c2p_failures"] == 0
+
+
+def test_emf_arrays_equal_on_the_fly():
+    """edge EMFs kept in arrays (the leveled path) = EMFs formed inside the
+    update (the one-level path), bit for bit"""
+    from bhgpu.fixed import FxGrid, FxParams
+    a = FxGrid.uniform(-40.0, 40.0, 32, 16, FxParams(precision="fp64"), emf_arrays=True)
+    b = FxGrid.uniform(-40.0, 40.0, 32, 16, FxParams(precision="fp64"), emf_arrays=False)
+    a.torus_init()
+    b.torus_init()
+    for _ in range(2):
+        a.step()
+        b.step()
+    torch.cuda.synchronize()
+    for name in ("U", "Bf", "W"):
+        assert np.array_equal(getattr(a, name).cpu().numpy(), getattr(b, name).cpu().numpy()), name
+
+
+@pytest.mark.parametrize("leveled", [False, True])
+def test_persistent_queue_equals_item_launches(leveled):
+    """the step kernels as persistent CTAs fed by the device work queue give
+    the same bits as one CTA per work item; the queue counters reset
+    themselves after every launch"""
+    from bhgpu.fixed import FxGrid, FxParams
+    from bhgrid.blocks import torus_levels
+    if leveled:
+        lv = torus_levels(nb=8, r_fine=(14.0, 26.0), seed=3)
+        a = FxGrid.leveled(-40.0, 40.0, lv, 8, FxParams(precision="fp64"), persistent=True)
+        b = FxGrid.leveled(-40.0, 40.0, lv, 8, FxParams(precision="fp64"), persistent=False)
+    else:
+        a = FxGrid.uniform(-40.0, 40.0, 32, 16, FxParams(precision="fp64"), persistent=True)
+        b = FxGrid.uniform(-40.0, 40.0, 32, 16, FxParams(precision="fp64"), persistent=False)
+    a.torus_init()
+    b.torus_init()
+    for _ in range(3):
+        a.step()
+        b.step()
+    torch.cuda.synchronize()
+    for name in ("U", "Bf", "W"):
+        assert np.array_equal(getattr(a, name).cpu().numpy(), getattr(b, name).cpu().numpy()), name
+    assert int(a.queue.abs().sum().item()) == 0
