@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=2, help="steps of the CPU port in cpu_baseline")
     ap.add_argument("--faithful", type=int, default=1, help="also time the reference-faithful FP64 path")
     ap.add_argument("--con2prim-batch", type=int, default=1, help="also measure the 2^24-cell con2prim batch")
+    ap.add_argument("--amr", type=int, default=1, help="also measure the block-AMR configurations 3 and 5")
     ap.add_argument("--autotune", type=int, default=1,
                     help="choose the launch bounds of the heavy kernels on the torus first (bhgpu.fixed.autotune)")
     return ap.parse_args()
@@ -508,6 +509,69 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
     return out
 
 # ---------------------------------------------------------------------------
+# block AMR: equal cubes (8 per axis over [-40, 40]^3) at several levels, all
+# blocks of all sizes in one launch per kernel (persistent CTAs fed by the
+# device work queue), the step replayed as a CUDA graph
+AMR_CONFIGS = {
+    "config3": {"n0": 8, "r_fine": (14.0, 26.0), "seed": 3, "accuracy_steps": 100,
+                "what": "3 levels: blocks of 8^3, 16^3 and 32^3 cells (+2 ghosts), seeded uneven mix "
+                        "concentrated near the hole"},
+    "config5": {"n0": 4, "r_fine": (10.0, 18.0, 28.0), "seed": 5, "accuracy_steps": 200,
+                "what": "4 levels: blocks of 4^3 to 32^3 cells, effective 256^3 at the finest level"},
+}
+
+
+def amr_bench(warm, steps, autotuned=None):
+    import numpy as np
+    import torch
+    from bhgpu.fixed import FxGrid, FxParams
+    from bhgrid.blocks import torus_levels
+    peak, _ = measured_peaks()
+    out = {}
+    for name, c in AMR_CONFIGS.items():
+        lv = torus_levels(nb=8, r_fine=c["r_fine"], seed=c["seed"])
+        n_of = {l: c["n0"] << l for l in range(int(lv.max()) + 1)}
+        zones = int(sum((n_of[int(l)] ** 3) for l in lv.ravel()))
+        res = {"workload": f"Kerr-Schild torus on 512 equal cubes over [-40,40]^3, {c['what']}",
+               "blocks_per_size": {f"{n_of[l]}^3": int((lv == l).sum()) for l in n_of},
+               "zones": zones, "torus": dict(TORUS)}
+        for prec, persistent in (("mixed", True), ("mixed", False), ("fp64", True)):
+            g = FxGrid.leveled(LO, HI, lv, c["n0"], FxParams(precision=prec), persistent=persistent)
+            g.torus_init(**TORUS)
+            ms, _ = timed_steps(g, steps, warm, None)
+            key = f"{prec}{'' if persistent else '_one_cta_per_item'}"
+            res[key] = {"ms_per_step": ms, "zone_updates_per_s": zones / (ms / 1e3),
+                        "hbm_frac_296B": zones / (ms / 1e3) * STEP_BYTES / (peak * 1e9)}
+            del g
+            torch.cuda.empty_cache()
+        res["mixed_vs_plain_fp64_speedup"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
+        # accuracy after the configuration's step count
+        ref = FxGrid.leveled(LO, HI, lv, c["n0"], FxParams(precision="fp64"), persistent=True)
+        ref.torus_init(**TORUS)
+        mix = FxGrid(ref.blocks_np, ref.nbr_np, FxParams(precision="mixed"), persistent=True)
+        mix.copy_state_from(ref)
+        ref.capture()
+        mix.capture()
+        for _ in range(c["accuracy_steps"]):
+            ref.replay()
+            mix.replay()
+        torch.cuda.synchronize()
+        ref.release_graph()
+        mix.release_graph()
+        a, b = mix.U.cpu().numpy(), ref.U.cpu().numpy()
+        fields = {"D": [0], "S": [1, 2, 3], "tau": [4], "B": [5, 6, 7]}
+        res["accuracy"] = {"steps": c["accuracy_steps"], "finite": bool(np.isfinite(a).all()),
+                           "rel_l1": {k: float(np.abs(a[f] - b[f]).sum() / np.abs(b[f]).sum()) for k, f in fields.items()},
+                           "div_B_rel": {"fp64": ref.divb(), "mixed": mix.divb()},
+                           "c2p_failures": {"fp64": ref.counters()["c2p_failures"],
+                                            "mixed": mix.counters()["c2p_failures"]}}
+        del ref, mix
+        torch.cuda.empty_cache()
+        out[name] = res
+    return out
+
+
+# ---------------------------------------------------------------------------
 def run_reference(args):
     """The reference arm: the same torus on the host cores.  The reference's
     own scheme cannot step it (std::domain_error in its first stage), so the
@@ -630,6 +694,8 @@ def run_ours(args):
                                               f"CPU port of the scheme (oracle/bh_fixed.c, OpenMP), "
                                               f"{s_per:.2f} s/step"}
             line["reference_scheme_cpu"] = reference_scheme_cpu(threads)
+            if args.amr:
+                line["block_amr"] = amr_bench(warm, min(args.steps, 20))
             if args.faithful:
                 line["reference_faithful_gpu"] = faithful_gpu()
             if args.con2prim_batch:

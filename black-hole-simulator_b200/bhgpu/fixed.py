@@ -322,7 +322,7 @@ class FxHostPipeline:
 # ---------------------------------------------------------------------------
 # launch-bound autotuning of the scheme's heavy kernels (bh_fx_tune_*)
 TUNE_KERNELS = ("c2p", "flux", "update")
-TUNE_CANDIDATES = (1, 3, 4, 5, 6)
+TUNE_CANDIDATES = (1, 3, 4, 5, 6, 7, 8)
 lib.bh_fx_tune_set.argtypes = [_i32, _i32, _i32]
 lib.bh_fx_tune_get.argtypes = [_i32, _i32, C.POINTER(_i32)]
 lib.bh_fx_tune_set.restype = C.c_int

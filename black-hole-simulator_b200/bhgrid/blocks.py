@@ -103,8 +103,8 @@ def leveled_blocks(lo: float, hi: float, level: np.ndarray, n0: int, periodic: b
     refinement level changes a cube's resolution, not its extent, so each
     block has exactly one neighbour per offset; levels must be 2:1 balanced."""
     nb = level.shape[0]
-    if n0 % 8:
-        raise ValueError("block sizes must be multiples of 8")
+    if n0 % 2 or n0 < 4:
+        raise ValueError("block sizes must be even and at least 4")
     L = (hi - lo) / nb
     blocks = np.zeros(nb ** 3, BLOCK_DTYPE)
     nbr = np.full((nb ** 3, 27), -1, np.int32)
@@ -137,16 +137,20 @@ def leveled_blocks(lo: float, hi: float, level: np.ndarray, n0: int, periodic: b
 
 def torus_levels(nb: int = 8, lo: float = -40.0, hi: float = 40.0, r_fine=(14.0, 26.0), seed: int = 3,
                  jitter: float = 0.25):
-    """Seeded uneven level map concentrated near the hole: level 2 for cubes
-    whose centre lies within r_fine[0], 1 within r_fine[1], 0 beyond; a
-    fraction `jitter` of the cubes moves one level up or down at random;
-    then 2:1 balanced."""
+    """Seeded uneven level map concentrated near the hole: with radii
+    r_fine = (r_1, ..., r_L) in increasing order, a cube whose centre lies
+    within r_l gets level L - l + 1 (the innermost the highest), beyond all
+    of them level 0; a fraction `jitter` of the cubes moves one level up or
+    down at random; then 2:1 balanced."""
     rng = np.random.default_rng(seed)
     L = (hi - lo) / nb
     c = lo + (np.arange(nb) + 0.5) * L
     R = np.sqrt(c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2)
-    lv = np.where(R < r_fine[0], 2, np.where(R < r_fine[1], 1, 0))
+    top = len(r_fine)
+    lv = np.zeros(R.shape, np.int64)
+    for l, r in enumerate(sorted(r_fine, reverse=True)):
+        lv = np.where(R < r, l + 1, lv)
     move = rng.random(lv.shape) < jitter
     step = rng.choice([-1, 1], size=lv.shape)
-    lv = np.clip(np.where(move, lv + step, lv), 0, 2)
+    lv = np.clip(np.where(move, lv + step, lv), 0, top)
     return balanced_levels(lv)

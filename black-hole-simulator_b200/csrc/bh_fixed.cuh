@@ -857,11 +857,13 @@ int fx_tune_tab[BH_FX_TUNE_N] = {1, 1, 1};
     case 4: LAUNCH(4); break;                                                     \
     case 5: LAUNCH(5); break;                                                     \
     case 6: LAUNCH(6); break;                                                     \
+    case 7: LAUNCH(7); break;                                                     \
+    case 8: LAUNCH(8); break;                                                     \
     default: LAUNCH(1); break;                                                    \
     }
 
 int fx_tune_set(int32_t kernel, int32_t ctas) {
-    if (kernel < 0 || kernel >= BH_FX_TUNE_N || !(ctas == 1 || (ctas >= 3 && ctas <= 6))) return BH_EINVAL;
+    if (kernel < 0 || kernel >= BH_FX_TUNE_N || !(ctas == 1 || (ctas >= 3 && ctas <= 8))) return BH_EINVAL;
     fx_tune_tab[kernel] = ctas;
     return BH_OK;
 }

@@ -372,7 +372,7 @@ int bh_step_graph_destroy(bh_step_graph *g);
  * sigma_max, W <= W_max) and excision (cells with r < r_exc are reset to
  * the floor state at rest every stage).
  *
- * Layout: a list of cubic blocks of n^3 interior cells (n a multiple of 8)
+ * Layout: a list of cubic blocks of n^3 interior cells (n even, at least 4)
  * with two ghost layers.  Blocks are equal cubes of space; a block of level
  * l holds twice the cells per axis of level l-1 (the 27-neighbour table
  * links equal cubes, whose levels differ by one at most): ghost cells of a
@@ -449,7 +449,7 @@ typedef struct bh_fx_grid {
 #define BH_FX_QSLOTS 6
 
 /* Launch bounds of the scheme's three heavy kernels (no counterpart in the
- * reference): each is compiled for 1 (no register cap), 3, 4, 5 and 6
+ * reference): each is compiled for 1 (no register cap) and 3 to 8
  * resident 128-thread CTAs per SM; the choice is per process and variant,
  * initially 1.  bhgpu.fixed.autotune times the candidates on a grid and sets
  * the fastest.  Launches (and graphs captured) after the call use it. */
