@@ -139,8 +139,17 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
             const int64_t N = G.ncell;
             double x[3];
             cell_centre(B, i, j, k, x);
+            // the mixed variant beyond r ~ FX_R_FP64: geometry, floors and the
+            // floor rewrite in FP32; the Newton iterations in FP64 throughout
+            const bool g32 = fp32_geometry<RT>(x);
             KS m;
-            ks_metric(P, x[0], x[1], x[2], m);
+            KSb<float> mf;
+            if (g32) {
+                ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
+                copy_metric(mf, m);
+            } else {
+                ks_metric(P, x[0], x[1], x[2], m);
+            }
             // cell field: mean of the two faces (the role of f2cB, transport.cpp:60-75)
             const int si = bstride_i(B), sj = bstride_j(B);
             double Bt[3] = {0.5 * (Bf[c] + Bf[c + si]), 0.5 * (Bf[N + c] + Bf[N + c + sj]),
@@ -161,17 +170,36 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
                 atomicAdd(&G.count[0], 1);
                 rewrite = 1;
             }
-            if (apply_floors(P, m, w)) {
-                rewrite = 1;
-                atomicAdd(&G.count[1], 1);
-            }
-            if (rewrite) {
-                KSm<double> mm;
-                ks_cast(m, mm);
-                Derived<double> d;
-                derive(mm, P.gamma, w, d);
-                prim2cons(mm, P.gamma, w, d, u);
-                for (int v = 0; v < 5; v++) U[v * N + c] = u[v];
+            if (g32) {
+                float wf[8];
+                for (int v = 0; v < 8; v++) wf[v] = float(w[v]);
+                if (apply_floors(P, mf, wf)) {
+                    rewrite = 1;
+                    atomicAdd(&G.count[1], 1);
+                }
+                if (rewrite) {
+                    KSm<float> mm;
+                    ks_cast(mf, mm);
+                    Derived<float> d;
+                    float uf[8];
+                    derive(mm, float(P.gamma), wf, d);
+                    prim2cons(mm, float(P.gamma), wf, d, uf);
+                    for (int v = 0; v < 5; v++) U[v * N + c] = (double)uf[v];
+                    for (int v = 0; v < 5; v++) w[v] = (double)wf[v];
+                }
+            } else {
+                if (apply_floors(P, m, w)) {
+                    rewrite = 1;
+                    atomicAdd(&G.count[1], 1);
+                }
+                if (rewrite) {
+                    KSm<double> mm;
+                    ks_cast(m, mm);
+                    Derived<double> d;
+                    derive(mm, P.gamma, w, d);
+                    prim2cons(mm, P.gamma, w, d, u);
+                    for (int v = 0; v < 5; v++) U[v * N + c] = u[v];
+                }
             }
             for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
             for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];

@@ -382,11 +382,13 @@ BH_HD inline void source(const KSb<MT>& mk, const KSDb<MT>& dk, RT gamma, const 
 // floors (the atmosphere of amrtree::pvfs, grid.cpp:133-146, as the
 // configuration asks: rho_fl r^-3/2, u_fl r^-5/2), evaluated at max(r, 1)
 // ======================================================================
-BH_HD inline void floor_state(const FxPar& P, double r, double& rho, double& p) {
-    double re = r > 1.0 ? r : 1.0;
-    double s = sqrt(re);
-    rho = P.rho_fl / (re * s);
-    p = (P.gamma - 1.0) * P.u_fl / (re * re * s);
+template <typename T>
+BH_HD inline void floor_state(const FxPar& P, T r, T& rho, T& p) {
+    T re = r > T(1) ? r : T(1);
+    T s = sqrt_(re);
+    T ir = T(1) / (re * re * s);          // r^-5/2
+    rho = T(P.rho_fl) * re * ir;
+    p = (T(P.gamma) - T(1)) * T(P.u_fl) * ir;
 }
 
 // ======================================================================
@@ -520,9 +522,10 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
     double iZ = 1.0 / Z, ZB = Z + q.B2, iZB = 1.0 / ZB;
     v2 = q.S2 * iZB * iZB + q.SB2 * (q.B2 + 2.0 * Z) * iZ * iZ * iZB * iZB;
     if (!(v2 < q.v2max)) v2 = q.v2max;
-    double Wl = 1.0 / sqrt(1.0 - v2);
-    double rho = q.D / Wl;
-    double p = q.gf * (Z * (1.0 - v2) - q.D / Wl);
+    double W2i = 1.0 - v2, Wi = sqrt(W2i);
+    double Wl = 1.0 / Wi;
+    double rho = q.D * Wi;
+    double p = q.gf * (Z * W2i - rho);
     // v_i = (S_i + (S.B / Z) B_i) / (Z + B^2), raised with gamma^ij
     double vl[3], vu[3];
     for (int i = 0; i < 3; i++) vl[i] = (S[i] + SB * iZ * Bl[i]) * iZB;
@@ -538,34 +541,35 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
 // floors and excision on a recovered state: returns 1 if w was changed
 // (the caller then rewrites U = prim2cons(w))
 // ======================================================================
-BH_HD inline int apply_floors(const FxPar& P, const KS& m, double* w) {
-    double rf, pf;
+template <typename T>
+BH_HD inline int apply_floors(const FxPar& P, const KSb<T>& m, T* w) {
+    T rf, pf;
     floor_state(P, m.r, rf, pf);
     int changed = 0;
-    if (m.r < P.r_exc) {
+    if (m.r < T(P.r_exc)) {
         w[P_RHO] = rf; w[P_PRS] = pf;
-        w[P_UT] = w[P_UT + 1] = w[P_UT + 2] = 0.0;
+        w[P_UT] = w[P_UT + 1] = w[P_UT + 2] = T(0);
         return 1;
     }
     // Lorentz factor ceiling
-    double ut[3] = {w[P_UT], w[P_UT + 1], w[P_UT + 2]}, utl[3];
+    T ut[3] = {w[P_UT], w[P_UT + 1], w[P_UT + 2]}, utl[3];
     lower(m.g, ut, utl);
-    double u2 = utl[0] * ut[0] + utl[1] * ut[1] + utl[2] * ut[2];
-    double umax2 = P.W_max * P.W_max - 1.0;
+    T u2 = utl[0] * ut[0] + utl[1] * ut[1] + utl[2] * ut[2];
+    T umax2 = T(P.W_max) * T(P.W_max) - T(1);
     if (u2 > umax2) {
-        double s = sqrt(umax2 / u2);
-        for (int i = 0; i < 3; i++) w[P_UT + i] = ut[i] * s;
+        T sc = sqrt_(umax2 / u2);
+        for (int i = 0; i < 3; i++) w[P_UT + i] = ut[i] * sc;
         u2 = umax2;
         changed = 1;
     }
     // magnetisation ceiling b^2 / rho <= sigma_max
-    double W2 = 1.0 + u2, W = sqrt(W2);
-    double B[3] = {w[P_B], w[P_B + 1], w[P_B + 2]}, Bl[3];
+    T W2 = T(1) + u2, iW2 = T(1) / W2;
+    T B[3] = {w[P_B], w[P_B + 1], w[P_B + 2]}, Bl[3];
     lower(m.g, B, Bl);
-    double B2 = Bl[0] * B[0] + Bl[1] * B[1] + Bl[2] * B[2];
-    double Bu = (Bl[0] * w[P_UT] + Bl[1] * w[P_UT + 1] + Bl[2] * w[P_UT + 2]) / W;
-    double b2 = B2 / W2 + Bu * Bu;
-    double rs = b2 / P.sigma_max;
+    T B2 = Bl[0] * B[0] + Bl[1] * B[1] + Bl[2] * B[2];
+    T Bu2 = Bl[0] * w[P_UT] + Bl[1] * w[P_UT + 1] + Bl[2] * w[P_UT + 2];   // W (B.v)
+    T b2 = (B2 + Bu2 * Bu2) * iW2;
+    T rs = b2 * (T(1) / T(P.sigma_max));
     if (rs > rf) rf = rs;
     if (!(w[P_RHO] >= rf)) { w[P_RHO] = rf; changed = 1; }
     if (!(w[P_PRS] >= pf)) { w[P_PRS] = pf; changed = 1; }
@@ -575,6 +579,12 @@ BH_HD inline int apply_floors(const FxPar& P, const KS& m, double* w) {
 // ======================================================================
 // CFL limit of a cell: the smallest dx_d / max|lambda_d|
 // ======================================================================
+template <typename A, typename B>
+BH_HD inline void copy_metric(const KSb<A>& m, KSb<B>& mo) {
+    mo.H = B(m.H); mo.alpha = B(m.alpha); mo.sqrtgam = B(m.sqrtgam); mo.r = B(m.r);
+    for (int i = 0; i < 3; i++) { mo.l[i] = B(m.l[i]); mo.beta[i] = B(m.beta[i]); }
+    for (int i = 0; i < 6; i++) { mo.g[i] = B(m.g[i]); mo.gi[i] = B(m.gi[i]); }
+}
 template <typename A, typename B>
 BH_HD inline void copy_geometry(const KSb<A>& m, const KSDb<A>& d, KSb<B>& mo, KSDb<B>& dout) {
     mo.H = B(m.H); mo.alpha = B(m.alpha); mo.sqrtgam = B(m.sqrtgam); mo.r = B(m.r);

@@ -283,8 +283,9 @@ static void source(const ksm* m, const ksd* dk, double gamma, const double* w, d
 static void floor_state(const fxo_params* P, double r, double* rho, double* p) {
     double re = r > 1.0 ? r : 1.0;
     double s = sqrt(re);
-    *rho = P->rho_floor / (re * s);
-    *p = (P->gamma - 1.0) * P->u_floor / (re * re * s);
+    double ir = 1.0 / (re * re * s); /* r^-5/2 */
+    *rho = P->rho_floor * re * ir;
+    *p = (P->gamma - 1.0) * P->u_floor * ir;
 }
 
 typedef struct {
@@ -387,9 +388,10 @@ static int c2p(const fxo_params* P, const ksm* m, const double* U, const double*
     double iZ = 1.0 / Z, ZB = Z + q.B2, iZB = 1.0 / ZB;
     v2 = q.S2 * iZB * iZB + q.SB2 * (q.B2 + 2.0 * Z) * iZ * iZ * iZB * iZB;
     if (!(v2 < q.v2max)) v2 = q.v2max;
-    double Wl = 1.0 / sqrt(1.0 - v2);
-    double rho = q.D / Wl;
-    double p = q.gf * (Z * (1.0 - v2) - q.D / Wl);
+    double W2i = 1.0 - v2, Wi = sqrt(W2i);
+    double Wl = 1.0 / Wi;
+    double rho = q.D * Wi;
+    double p = q.gf * (Z * W2i - rho);
     double vl[3], vu[3];
     for (int i = 0; i < 3; i++) vl[i] = (S[i] + SB * iZ * Bl[i]) * iZB;
     lower3(m->gi, vl, vu);
@@ -423,13 +425,13 @@ static int floors(const fxo_params* P, const ksm* m, double* w) {
         u2 = umax2;
         changed = 1;
     }
-    double W2 = 1.0 + u2, W = sqrt(W2);
+    double W2 = 1.0 + u2, iW2 = 1.0 / W2;
     double B[3] = {w[BB], w[BB + 1], w[BB + 2]}, Bl[3];
     lower3(m->g, B, Bl);
     double B2 = Bl[0] * B[0] + Bl[1] * B[1] + Bl[2] * B[2];
-    double Bu = (Bl[0] * w[UT] + Bl[1] * w[UT + 1] + Bl[2] * w[UT + 2]) / W;
-    double b2 = B2 / W2 + Bu * Bu;
-    double rs = b2 / P->sigma_max;
+    double Bu2 = Bl[0] * w[UT] + Bl[1] * w[UT + 1] + Bl[2] * w[UT + 2]; /* W (B.v) */
+    double b2 = (B2 + Bu2 * Bu2) * iW2;
+    double rs = b2 * (1.0 / P->sigma_max);
     if (rs > rf) rf = rs;
     if (!(w[RHO] >= rf)) {
         w[RHO] = rf;
