@@ -21,8 +21,8 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from bhgrid.blocks import (BLOCK_DTYPE, CHUNK, box_size, interior as _interior, leveled_blocks,  # noqa: F401
-                           uniform_blocks, work_items)
+from bhgrid.blocks import (BLOCK_DTYPE, CHUNK, TILE_MIN, box_size, flux_items, interior as _interior,  # noqa: F401
+                           leveled_blocks, uniform_blocks, work_items)
 
 from ._lib import BH_FP64, BH_FP64_FMA, BH_MIXED, BH_MC, BH_MINMOD, BH_VANLEER, BhError, check, lib
 
@@ -43,7 +43,8 @@ class BhFxGrid(C.Structure):
     _fields_ = [("nblock", _i32), ("blocks", _vp), ("nbr", _vp), ("items_cell", _vp), ("nitem_cell", _i32),
                 ("items_pos", _vp), ("nitem_pos", _i32), ("items_ghost", _vp), ("nitem_ghost", _i32),
                 ("ncell", _i64), ("U", _vp), ("U1", _vp), ("W", _vp), ("Bf", _vp), ("Bf1", _vp), ("F", _vp),
-                ("dt", _vp), ("count", _vp), ("err", _vp), ("E", _vp), ("maxlevel", _i32), ("queue_ctas", _i32), ("queue", _vp)]
+                ("dt", _vp), ("count", _vp), ("err", _vp), ("E", _vp), ("maxlevel", _i32), ("queue_ctas", _i32), ("queue", _vp),
+                ("items_flux", _vp), ("nitem_flux", _i32)]
 
 
 class BhFxTorus(C.Structure):
@@ -124,6 +125,7 @@ class FxGrid:
         self.blocks = torch.from_numpy(blocks.view(np.uint8).copy()).to(dev)
         self.nbr = torch.from_numpy(nbr.copy()).to(dev)
         self.items = {k: torch.from_numpy(work_items(blocks, k)).to(dev) for k in ("cell", "pos", "ghost")}
+        self.items["flux"] = torch.from_numpy(flux_items(blocks)).to(dev)
         wdt = torch.float32 if params.precision == "mixed" else torch.float64
         N = self.ncell
         self.U = torch.zeros((8, N), dtype=torch.float64, device=dev)
@@ -163,7 +165,8 @@ class FxGrid:
                            _ptr(it["cell"]), it["cell"].shape[0], _ptr(it["pos"]), it["pos"].shape[0],
                            _ptr(it["ghost"]), it["ghost"].shape[0], self.ncell,
                            _ptr(self.U), _ptr(self.U1), _ptr(self.W), _ptr(self.Bf), _ptr(self.Bf1), _ptr(self.F),
-                           _ptr(self.dt), _ptr(self.count), _ptr(self.err), _ptr(self.E), self.maxlevel, 0, _ptr(self.queue))
+                           _ptr(self.dt), _ptr(self.count), _ptr(self.err), _ptr(self.E), self.maxlevel, 0, _ptr(self.queue),
+                           _ptr(it["flux"]), it["flux"].shape[0])
         self._p = self.params.cstruct()
 
     @property
@@ -322,6 +325,7 @@ class FxHostPipeline:
 # ---------------------------------------------------------------------------
 # launch-bound autotuning of the scheme's heavy kernels (bh_fx_tune_*)
 TUNE_KERNELS = ("c2p", "flux", "update")
+TUNE_KNOBS = TUNE_KERNELS + ("stage",)   # "stage": 1 = the staged flux kernel
 TUNE_CANDIDATES = (1, 3, 4, 5, 6, 7, 8)
 lib.bh_fx_tune_set.argtypes = [_i32, _i32, _i32]
 lib.bh_fx_tune_get.argtypes = [_i32, _i32, C.POINTER(_i32)]
@@ -330,45 +334,65 @@ lib.bh_fx_tune_get.restype = C.c_int
 
 
 def tune_set(precision: str, kernel: str, ctas: int):
-    check(lib.bh_fx_tune_set(PRECISIONS[precision], TUNE_KERNELS.index(kernel), ctas), "bh_fx_tune_set")
+    """kernel in TUNE_KERNELS: resident CTAs per SM (1, 3..8); "stage": 0/1."""
+    check(lib.bh_fx_tune_set(PRECISIONS[precision], TUNE_KNOBS.index(kernel), ctas), "bh_fx_tune_set")
 
 
 def tune_get(precision: str, kernel: str) -> int:
     v = _i32()
-    check(lib.bh_fx_tune_get(PRECISIONS[precision], TUNE_KERNELS.index(kernel), C.byref(v)), "bh_fx_tune_get")
+    check(lib.bh_fx_tune_get(PRECISIONS[precision], TUNE_KNOBS.index(kernel), C.byref(v)), "bh_fx_tune_get")
     return int(v.value)
 
 
 def autotune(grid: FxGrid, reps: int = 4, candidates=TUNE_CANDIDATES) -> dict:
-    """Choose the launch bounds of con2prim, fluxes and update for the
-    grid's variant: for one kernel at a time (the others held), every
-    candidate times `reps` RK2 steps (CUDA events) from the same saved state;
-    the fastest is kept.  The grid's state is restored.  In the FP64 variant
-    every choice gives the same bits (no contraction); in the contracted
-    variants ptxas may pair multiply-adds differently under another register
-    budget, which moves results by ulps.  Returns {"choice": {kernel: ctas},
-    "ms": {kernel: {ctas: ms per step}}}."""
+    """Choose the launch bounds of con2prim, fluxes and update, and whether
+    the flux stencil is staged in shared memory, for the grid's variant: for
+    one kernel at a time (the others held), every candidate times `reps` RK2
+    steps (CUDA events) from the same saved state; the fastest is kept (the
+    flux candidates are the pairs (staged, launch bound); staging is tried
+    only where the grid has blocks of TILE_MIN cells per axis or more).  The
+    grid's state is restored.  In the FP64 variant every choice gives the
+    same bits (no contraction); in the contracted variants ptxas may pair
+    multiply-adds differently under another register budget, which moves
+    results by ulps.  Returns {"choice": {knob: value}, "ms": {kernel:
+    {candidate: ms per step}}} (flux candidates keyed "s<stage>/<ctas>")."""
     saved = [t.clone() for t in (grid.U, grid.W, grid.Bf)]
     prec = grid.precision
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {"choice": {}, "ms": {}}
+    tiled = bool((grid.blocks_np["n"] >= TILE_MIN).any())
+
+    def timed(set_fn):
+        set_fn()
+        for t, s in zip((grid.U, grid.W, grid.Bf), saved):
+            t.copy_(s)
+        grid.step()
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(reps):
+            grid.step()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
     for k in TUNE_KERNELS:
         times = {}
-        for c in candidates:
-            tune_set(prec, k, c)
-            for t, s in zip((grid.U, grid.W, grid.Bf), saved):
-                t.copy_(s)
-            grid.step()
-            torch.cuda.synchronize()
-            a.record()
-            for _ in range(reps):
-                grid.step()
-            b.record()
-            torch.cuda.synchronize()
-            times[c] = a.elapsed_time(b) / reps
-        best = min(times, key=times.get)
-        tune_set(prec, k, best)
-        out["choice"][k] = best
+        if k == "flux":
+            for st in ((0, 1) if tiled else (0,)):
+                for c in candidates:
+                    times[f"s{st}/{c}"] = timed(lambda: (tune_set(prec, "stage", st), tune_set(prec, k, c)))
+            best = min(times, key=times.get)
+            st, c = best[1:].split("/")
+            tune_set(prec, "stage", int(st))
+            tune_set(prec, k, int(c))
+            out["choice"]["stage"] = int(st)
+            out["choice"][k] = int(c)
+        else:
+            for c in candidates:
+                times[c] = timed(lambda: tune_set(prec, k, c))
+            best = min(times, key=times.get)
+            tune_set(prec, k, best)
+            out["choice"][k] = best
         out["ms"][k] = times
     for t, s in zip((grid.U, grid.W, grid.Bf), saved):
         t.copy_(s)

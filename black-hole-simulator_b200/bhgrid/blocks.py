@@ -67,6 +67,44 @@ def work_items(blocks: np.ndarray, kind: str) -> np.ndarray:
     return np.concatenate(out).astype(np.int32)
 
 
+# tiles of the staged flux kernel: TILE positions (i, j, k) per tile; blocks
+# below TILE_MIN cells per axis keep chunks of positions (a tile box of n + 2
+# positions per axis wastes up to (ceil((n+2)/T) T / (n+2)) of its threads)
+TILE = (4, 4, 8)
+TILE_MIN = 64
+
+
+def flux_items(blocks: np.ndarray, tile_min: int = TILE_MIN) -> np.ndarray:
+    """(block, e) work items of the staged flux kernel: e >= 0 is tile e of a
+    block with n >= tile_min (tile (ti, tj, tk) -> (ti nj + tj) nk + tk over
+    the position box [-1, n]^3), e < 0 the CHUNK positions from -(e + 1) on
+    of a smaller block."""
+    out = []
+    for b, n in enumerate(blocks["n"]):
+        n = int(n)
+        m = n + 2
+        if n >= tile_min:
+            nt = -(-m // TILE[0]) * -(-m // TILE[1]) * -(-m // TILE[2])
+            e = np.arange(nt, dtype=np.int32)
+        else:
+            e = -np.arange(0, m ** 3, CHUNK, dtype=np.int32) - 1
+        out.append(np.stack([np.full_like(e, b), e], 1))
+    return np.concatenate(out).astype(np.int32)
+
+
+def flux_item_positions(n: int, e: int) -> np.ndarray:
+    """Positions (i, j, k) in [-1, n]^3 that item e of a block of n cells
+    covers (the kernel's decode; positions beyond n are masked)."""
+    m = n + 2
+    if e < 0:
+        idx = np.arange(-(e + 1), min(-(e + 1) + CHUNK, m ** 3))
+        return np.stack([idx // (m * m) - 1, (idx // m) % m - 1, idx % m - 1], 1)
+    nj, nk = -(-m // TILE[1]), -(-m // TILE[2])
+    o = (-1 + (e // (nj * nk)) * TILE[0], -1 + ((e // nk) % nj) * TILE[1], -1 + (e % nk) * TILE[2])
+    g = np.stack(np.meshgrid(*[np.arange(o[d], o[d] + TILE[d]) for d in range(3)], indexing="ij"), -1).reshape(-1, 3)
+    return g[(g <= n).all(1)]
+
+
 def interior(blocks: np.ndarray, arr: np.ndarray) -> np.ndarray:
     """[..., nblock, n, n, n] interior cells of a [..., ncell] array (all
     blocks of one size)."""

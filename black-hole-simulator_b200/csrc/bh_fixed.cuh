@@ -89,6 +89,9 @@ struct Queue {
     int32_t* done;   // CTAs finished
     int32_t nitem;
 };
+// the item bodies are inlined into the kernel: an outlined body would take
+// the kernel's parameter structs by address and copy them to local memory
+#define FX_INLINE __attribute__((always_inline))
 template <typename Body>
 __device__ __forceinline__ void for_items(const Queue& q, Body body) {
     if (!q.head) {
@@ -125,7 +128,7 @@ __global__ void k_fx_dt_init(double* dt) {
 // ======================================================================
 template <typename RT, typename WT, int MINB>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage, int with_dt, Queue Q) {
-    for_items(Q, [&](int t) {
+    for_items(Q, [&](int t) FX_INLINE {
         const int32_t b = items[2 * t];
         const bh_fx_block B = G.blk[b];
         const int n = B.n;
@@ -142,30 +145,47 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
             // the mixed variant beyond r ~ FX_R_FP64: geometry, floors and the
             // floor rewrite in FP32; the Newton iterations in FP64 throughout
             const bool g32 = fp32_geometry<RT>(x);
-            KS m;
-            KSb<float> mf;
-            if (g32) {
-                ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
-                copy_metric(mf, m);
-            } else {
-                ks_metric(P, x[0], x[1], x[2], m);
-            }
             // cell field: mean of the two faces (the role of f2cB, transport.cpp:60-75)
             const int si = bstride_i(B), sj = bstride_j(B);
-            double Bt[3] = {0.5 * (Bf[c] + Bf[c + si]), 0.5 * (Bf[N + c] + Bf[N + c + sj]),
-                            0.5 * (Bf[2 * N + c] + Bf[2 * N + c + 1])};
-            double isg = 1.0 / m.sqrtgam;
-            double Bc[3] = {Bt[0] * isg, Bt[1] * isg, Bt[2] * isg};
-            double u[8], wo[8], w[8];
-            for (int v = 0; v < 5; v++) u[v] = U[v * N + c];
+            const double Bt[3] = {0.5 * (Bf[c] + Bf[c + si]), 0.5 * (Bf[N + c] + Bf[N + c + sj]),
+                                  0.5 * (Bf[2 * N + c] + Bf[2 * N + c + 1])};
             WT* W = (WT*)G.W;
-            for (int v = 0; v < 5; v++) wo[v] = (double)W[v * N + c];
+            constexpr bool MIXED = sizeof(RT) < sizeof(double);
+            C2PS cs;
+            KS m;
+            cell_metric(P, x, g32, m);
+            {
+                const double isg = 1.0 / m.sqrtgam;
+                const double Bc[3] = {Bt[0] * isg, Bt[1] * isg, Bt[2] * isg};
+                double u[5], wo[5];
+                for (int v = 0; v < 5; v++) u[v] = U[v * N + c];
+                for (int v = 0; v < 5; v++) wo[v] = (double)W[v * N + c];
+                c2p_setup(P, m, u, Bc, wo, cs);
+            }
             int iters = 0;
-            int st = con2prim<sizeof(RT) < sizeof(double)>(P, m, u, Bc, wo, w, iters);
+            int st = c2p_solve<MIXED>(P, cs, iters);
+            KSb<float> mf;
+            if (MIXED) {
+                // the metric again (FP32 over most of the grid), so that it is
+                // not kept through the iterations; the opaque copy of the
+                // centre keeps the compiler from reusing the first
+                double xr[3] = {x[0], x[1], x[2]};
+                asm("" : "+d"(xr[0]), "+d"(xr[1]), "+d"(xr[2]));
+                if (g32) {
+                    ks_metric<float>(P, float(xr[0]), float(xr[1]), float(xr[2]), mf);
+                    copy_metric(mf, m);
+                } else {
+                    ks_metric(P, xr[0], xr[1], xr[2], m);
+                }
+            }
+            const double isg = 1.0 / m.sqrtgam;
+            const double Bc[3] = {Bt[0] * isg, Bt[1] * isg, Bt[2] * isg};
+            double w[8];
+            if (st == 0) st = c2p_finish(m.gi, cs, Bc, w);
             int rewrite = 0;
             if (st != 0) {
                 // keep the previous primitives with the new field
-                for (int v = 0; v < 5; v++) w[v] = wo[v];
+                for (int v = 0; v < 5; v++) w[v] = (double)W[v * N + c];
                 for (int d = 0; d < 3; d++) w[P_B + d] = Bc[d];
                 atomicAdd(&G.count[0], 1);
                 rewrite = 1;
@@ -196,6 +216,7 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
                     KSm<double> mm;
                     ks_cast(m, mm);
                     Derived<double> d;
+                    double u[8];
                     derive(mm, P.gamma, w, d);
                     prim2cons(mm, P.gamma, w, d, u);
                     for (int v = 0; v < 5; v++) U[v * N + c] = u[v];
@@ -286,7 +307,7 @@ __device__ inline double mm_slope(double a, double b, double c) {   // minmod of
 }
 template <typename WT>
 __global__ void __launch_bounds__(FX_TPB) k_fx_ghost(Grid G, const int32_t* items, int stage, int pass, Queue Q) {
-    for_items(Q, [&](int t) {
+    for_items(Q, [&](int t) FX_INLINE {
         const int32_t b = items[2 * t];
         const bh_fx_block B = G.blk[b];
         if (pass > 0 && B.level != pass) return;
@@ -383,13 +404,13 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_ghost(Grid G, const int32_t* item
 // is needed: normal index 0..n and transverse index -1..n (the transverse
 // layer feeds the EMFs of the block's boundary edges)
 // ======================================================================
-template <typename RT, typename WT, typename FT>
-__device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_block& B, int i, int j, int k, int d,
-                                 const double* Bfs) {
+// the face computation; sten(v, o) is variable v of the cell o = -2..1
+// steps along d from (i, j, k) (the face lies between o = -1 and o = 0)
+template <typename RT, typename FT, typename Sten>
+__device__ __forceinline__ void face_flux_at(const FxPar& P, const Grid& G, const bh_fx_block& B, int i, int j, int k,
+                                             int d, const double* Bfs, const Sten& sten) {
     const int64_t N = G.ncell;
     const int64_t c = bidx(B, i, j, k);
-    const int st = d == 0 ? bstride_i(B) : (d == 1 ? bstride_j(B) : 1);
-    const WT* W = (const WT*)G.W;
     double x[3];
     cell_centre(B, i, j, k, x);
     x[d] -= 0.5 * B.dx;
@@ -398,9 +419,7 @@ __device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_bloc
     RT wL[8], wR[8];
     for (int v = 0; v < 8; v++) {
         if (v == P_B + d) continue;
-        RT a = RT(W[v * N + c - 2 * st]), bb = RT(W[v * N + c - st]);
-        RT cc = RT(W[v * N + c]), dd = RT(W[v * N + c + st]);
-        plm_face(a, bb, cc, dd, P.limiter, wL[v], wR[v]);
+        plm_face(sten(v, -2), sten(v, -1), sten(v, 0), sten(v, 1), P.limiter, wL[v], wR[v]);
     }
     // (the limiters keep every face value between its two cells' values, so
     // face densities and pressures stay positive)
@@ -413,9 +432,19 @@ __device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_bloc
     for (int v = 0; v < 8; v++) Fo[((int64_t)d * 8 + v) * N + c] = (FT)F[v];
 }
 
+// the stencil read from the primitives in global memory
+template <typename RT, typename WT, typename FT>
+__device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_block& B, int i, int j, int k, int d,
+                                 const double* Bfs) {
+    const int64_t N = G.ncell;
+    const WT* Wc = (const WT*)G.W + bidx(B, i, j, k);
+    const int st = d == 0 ? bstride_i(B) : (d == 1 ? bstride_j(B) : 1);
+    face_flux_at<RT, FT>(P, G, B, i, j, k, d, Bfs, [&](int v, int o) { return RT(Wc[v * N + o * st]); });
+}
+
 template <typename RT, typename WT, typename FT, int MINB>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux(FxPar P, Grid G, const int32_t* items, int stage, Queue Q) {
-    for_items(Q, [&](int t) {
+    for_items(Q, [&](int t) FX_INLINE {
         const int32_t b = items[2 * t];
         const bh_fx_block B = G.blk[b];
         const int n = B.n, m = n + 2;
@@ -426,6 +455,93 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux(FxPar P, Grid G, const
         if (i >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 0, Bfs);
         if (j >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 1, Bfs);
         if (k >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 2, Bfs);
+    });
+}
+
+// ----------------------------------------------------------------------
+// face fluxes with the stencil staged in shared memory.  A tile of
+// FX_TI x FX_TJ x FX_TK positions (i, j, k; 128 threads) first loads the
+// primitives its faces read -- the tile's cells and the cross-shaped halo
+// of two cells below and one above along each axis (the stencil of PLM) --
+// into shared memory with coalesced loads along k, then computes the
+// x-, y- and z-faces of every position from there: each primitive is read
+// from L2 once per tile instead of once per face that uses it.  The work
+// items (block, e) are tiles (e >= 0, tile e of the block's position box
+// [-1, n]^3) or, for blocks too small to tile well, chunks of 128
+// positions starting at -(e + 1) as in k_fx_flux.  The arithmetic is that
+// of k_fx_flux: the same bits.
+// ----------------------------------------------------------------------
+constexpr int FX_TI = 4, FX_TJ = 4, FX_TK = 8;
+constexpr int FX_HI = FX_TI + 3, FX_HJ = FX_TJ + 3, FX_HK = FX_TK + 3;   // -2 .. T per axis
+constexpr int FX_HBOX = FX_HI * FX_HJ * FX_HK;
+constexpr int FX_NX = FX_HI * FX_TJ * FX_TK;   // the tile and its x-halo
+constexpr int FX_NY = FX_TI * 3 * FX_TK;       // y-halo: j = -2, -1, TJ
+constexpr int FX_NZ = FX_TI * FX_TJ * 3;       // z-halo: k = -2, -1, TK
+constexpr int FX_NCROSS = FX_NX + FX_NY + FX_NZ;
+static_assert(FX_TI * FX_TJ * FX_TK == FX_TPB, "one thread per tile position");
+
+// offsets (a, b, c) in [-2, T] of the q-th cell of the cross-shaped halo
+__device__ inline void cross_cell(int q, int& a, int& b, int& c) {
+    if (q < FX_NX) {
+        a = q / (FX_TJ * FX_TK) - 2; b = (q / FX_TK) % FX_TJ; c = q % FX_TK;
+    } else if ((q -= FX_NX) < FX_NY) {
+        const int h = (q / FX_TK) % 3;
+        a = q / (3 * FX_TK); b = h < 2 ? h - 2 : FX_TJ; c = q % FX_TK;
+    } else {
+        q -= FX_NY;
+        const int h = q % 3;
+        a = q / (FX_TJ * 3); b = (q / 3) % FX_TJ; c = h < 2 ? h - 2 : FX_TK;
+    }
+}
+__device__ inline int box_at(int a, int b, int c) { return ((a + 2) * FX_HJ + (b + 2)) * FX_HK + (c + 2); }
+
+template <typename RT, typename WT, typename FT, int MINB>
+__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux_tile(FxPar P, Grid G, const int32_t* items, int stage,
+                                                             Queue Q) {
+    __shared__ WT sW[8][FX_HBOX];
+    for_items(Q, [&](int t) FX_INLINE {
+        const int32_t b = items[2 * t];
+        const bh_fx_block B = G.blk[b];
+        const int n = B.n, m = n + 2;
+        const double* Bfs = stage ? G.Bf1 : G.Bf;
+        const int32_t e0 = items[2 * t + 1];
+        if (e0 < 0) {   // a chunk of positions, as in k_fx_flux
+            const int e = -(e0 + 1) + threadIdx.x;
+            if (e >= m * m * m) return;
+            const int i = e / (m * m) - 1, j = (e / m) % m - 1, k = e % m - 1;
+            if (i >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 0, Bfs);
+            if (j >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 1, Bfs);
+            if (k >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 2, Bfs);
+            return;
+        }
+        const int nj = (m + FX_TJ - 1) / FX_TJ, nk = (m + FX_TK - 1) / FX_TK;
+        const int i0 = -1 + (e0 / (nj * nk)) * FX_TI, j0 = -1 + ((e0 / nk) % nj) * FX_TJ,
+                  k0 = -1 + (e0 % nk) * FX_TK;
+        const int64_t N = G.ncell;
+        const WT* W = (const WT*)G.W;
+        __syncthreads();   // the previous tile's reads of sW are done
+        for (int q = threadIdx.x; q < FX_NCROSS; q += FX_TPB) {
+            int a, bb, c;
+            cross_cell(q, a, bb, c);
+            const int i = i0 + a, j = j0 + bb, k = k0 + c;
+            // cells of the box -2 .. n+2 only (those outside feed no face)
+            if (i < -2 || i > n + 2 || j < -2 || j > n + 2 || k < -2 || k > n + 2) continue;
+            const WT* Wc = W + bidx(B, i, j, k);
+            const int o = box_at(a, bb, c);
+#pragma unroll
+            for (int v = 0; v < 8; v++) sW[v][o] = Wc[v * N];
+        }
+        __syncthreads();
+        const int a = threadIdx.x / (FX_TJ * FX_TK), bb = (threadIdx.x / FX_TK) % FX_TJ, c = threadIdx.x % FX_TK;
+        const int i = i0 + a, j = j0 + bb, k = k0 + c;
+        if (i > n || j > n || k > n) return;
+        const int o = box_at(a, bb, c);
+        if (i >= 0)
+            face_flux_at<RT, FT>(P, G, B, i, j, k, 0, Bfs,
+                                 [&](int v, int s) { return RT(sW[v][o + s * (FX_HJ * FX_HK)]); });
+        if (j >= 0)
+            face_flux_at<RT, FT>(P, G, B, i, j, k, 1, Bfs, [&](int v, int s) { return RT(sW[v][o + s * FX_HK]); });
+        if (k >= 0) face_flux_at<RT, FT>(P, G, B, i, j, k, 2, Bfs, [&](int v, int s) { return RT(sW[v][o + s]); });
     });
 }
 
@@ -489,7 +605,7 @@ __device__ inline void face_update(const Grid& G, int d, int64_t c, int si, int 
 // i in [0,n), j, k in [0,n], and alike), from the face fluxes
 template <typename FT>
 __global__ void __launch_bounds__(FX_TPB) k_fx_emf(Grid G, const int32_t* items, Queue Q) {
-    for_items(Q, [&](int t) {
+    for_items(Q, [&](int t) FX_INLINE {
         const int32_t b = items[2 * t];
         const bh_fx_block B = G.blk[b];
         const int n = B.n, m = n + 2;
@@ -511,7 +627,7 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_emf(Grid G, const int32_t* items,
 // field of the coarse side stays the mean of the fine faces (div B at
 // roundoff).  Levels differ by one at most, so one pass suffices.
 __global__ void __launch_bounds__(FX_TPB) k_fx_emf_fix(Grid G, const int32_t* items, Queue Q) {
-    for_items(Q, [&](int t) {
+    for_items(Q, [&](int t) FX_INLINE {
         const int32_t b = items[2 * t];
         const bh_fx_block B = G.blk[b];
         const int n = B.n, m = n + 2;
@@ -554,7 +670,7 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_emf_fix(Grid G, const int32_t* it
 template <typename RT, typename WT, typename FT, int MINB>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, const int32_t* items, int stage,
                                                       double cfl, Queue Q) {
-    for_items(Q, [&](int t) {
+    for_items(Q, [&](int t) FX_INLINE {
         const int32_t b = items[2 * t];
         const bh_fx_block B = G.blk[b];
         const int n = B.n;
@@ -878,7 +994,7 @@ inline int fx_grid(const void* fn, int nitem, const bh_fx_grid* g) {
 // launch bounds of the heavy kernels: resident 128-thread CTAs per SM asked
 // of ptxas (which caps registers per thread); 1 leaves the choice to ptxas.
 // Chosen per process and variant (bh_fx_tune_set), initially 1.
-int fx_tune_tab[BH_FX_TUNE_N] = {1, 1, 1};
+int fx_tune_tab[BH_FX_TUNE_N] = {1, 1, 1, 0};
 #define FX_TUNED(kernel, LAUNCH)                                                  \
     switch (fx_tune_tab[kernel]) {                                                \
     case 3: LAUNCH(3); break;                                                     \
@@ -891,7 +1007,11 @@ int fx_tune_tab[BH_FX_TUNE_N] = {1, 1, 1};
     }
 
 int fx_tune_set(int32_t kernel, int32_t ctas) {
-    if (kernel < 0 || kernel >= BH_FX_TUNE_N || !(ctas == 1 || (ctas >= 3 && ctas <= 8))) return BH_EINVAL;
+    if (kernel == BH_FX_TUNE_STAGE) {
+        if (ctas != 0 && ctas != 1) return BH_EINVAL;
+    } else if (kernel < 0 || kernel >= BH_FX_TUNE_N || !(ctas == 1 || (ctas >= 3 && ctas <= 8))) {
+        return BH_EINVAL;
+    }
     fx_tune_tab[kernel] = ctas;
     return BH_OK;
 }
@@ -924,7 +1044,11 @@ int fx_ghosts(const bh_fx_params*, const bh_fx_grid* g, int32_t stage, void* s) 
 int fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
-    if (g->nitem_pos) {
+    if (fx_tune_tab[BH_FX_TUNE_STAGE] && g->nitem_flux) {
+#define L_(M) fx::k_fx_flux_tile<FRT, FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_flux_tile<FRT, FRT, FRT, M>, g->nitem_flux, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_flux, stage, fx_q(g, QS_FLUX, g->nitem_flux))
+        FX_TUNED(BH_FX_TUNE_FLUX, L_)
+#undef L_
+    } else if (g->nitem_pos) {
 #define L_(M) fx::k_fx_flux<FRT, FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_flux<FRT, FRT, FRT, M>, g->nitem_pos, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_pos, stage, fx_q(g, QS_FLUX, g->nitem_pos))
         FX_TUNED(BH_FX_TUNE_FLUX, L_)
 #undef L_

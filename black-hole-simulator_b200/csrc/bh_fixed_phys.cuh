@@ -429,27 +429,33 @@ BH_HD inline void c2p_eval(const C2Pb<T>& q, T Z, T& f, T& df, T& v2, int& clamp
     df = T(1) - dp + T(0.5) * q.B2 * dv2 + q.SB2 * iZ2 * iZ;
 }
 
-// PRE32 (the mixed variant): up to four FP32 Newton iterations move the
-// previous primitives' Z towards the root before the FP64 iterations, which
-// alone decide convergence and give the recovered state.
-template <bool PRE32 = false>
-BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const double* B, const double* wo,
-                          double* w, int& iters) {
+// PRE32 (the mixed variant): up to four FP32 Newton iterations from the
+// previous primitives' Z.  Where they converge on a well-conditioned
+// residual the FP32 root is the result; elsewhere the FP64 iterations start
+// from it and alone decide convergence.
+// The solver in three parts -- setup (the metric's invariants into q),
+// solve (q and Z alone), finish (raise v with gamma^ij) -- so that a caller
+// can let the metric go while it iterates.
+struct C2PS {
+    C2P q;
+    double S[3], Bl[3], SB, Z;
+};
+BH_HD inline void c2p_setup(const FxPar& P, const KS& m, const double* U, const double* B, const double* wo,
+                            C2PS& s) {
     const double gm = P.gamma;
     const double isg = 1.0 / m.sqrtgam;
-    C2P q;
+    C2P& q = s.q;
     q.gf = (gm - 1.0) / gm;
     q.D = U[C_D] * isg;
     double tau = U[C_TAU] * isg;
-    double S[3] = {U[C_S] * isg, U[C_S + 1] * isg, U[C_S + 2] * isg};
+    for (int i = 0; i < 3; i++) s.S[i] = U[C_S + i] * isg;
     double Su[3];
-    lower(m.gi, S, Su);   // S^i = gamma^ij S_j
-    double Bl[3];
-    lower(m.g, B, Bl);
-    q.S2 = Su[0] * S[0] + Su[1] * S[1] + Su[2] * S[2];
-    q.B2 = Bl[0] * B[0] + Bl[1] * B[1] + Bl[2] * B[2];
-    double SB = S[0] * B[0] + S[1] * B[1] + S[2] * B[2];
-    q.SB2 = SB * SB;
+    lower(m.gi, s.S, Su);   // S^i = gamma^ij S_j
+    lower(m.g, B, s.Bl);
+    q.S2 = Su[0] * s.S[0] + Su[1] * s.S[1] + Su[2] * s.S[2];
+    q.B2 = s.Bl[0] * B[0] + s.Bl[1] * B[1] + s.Bl[2] * B[2];
+    s.SB = s.S[0] * B[0] + s.S[1] * B[1] + s.S[2] * B[2];
+    q.SB2 = s.SB * s.SB;
     q.B4 = q.B2 * q.B2;
     q.E = tau + q.D;
     q.v2max = 1.0 - 1.0 / (P.W_max * P.W_max);
@@ -459,6 +465,13 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
     double W2o = 1.0 + utl[0] * uto[0] + utl[1] * uto[1] + utl[2] * uto[2];
     double Z = (wo[P_RHO] + gm / (gm - 1.0) * wo[P_PRS]) * W2o;
     if (!(Z > 0.0) || !(Z < 1e300)) Z = q.E > q.D ? q.E : q.D;
+    s.Z = Z;
+}
+// returns 0 with s.Z the root, 1 if it was not found
+template <bool PRE32 = false>
+BH_HD inline int c2p_solve(const FxPar& P, C2PS& s, int& iters) {
+    const C2P& q = s.q;
+    double Z = s.Z;
     int it = 0, ok = 0, it32 = 0;
     double f, df, v2;
     int clamped;
@@ -467,7 +480,7 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
         qf.D = float(q.D); qf.S2 = float(q.S2); qf.B2 = float(q.B2); qf.SB2 = float(q.SB2);
         qf.B4 = float(q.B4); qf.E = float(q.E); qf.gf = float(q.gf); qf.v2max = float(q.v2max);
         float Zf = float(Z), ff, dff, v2f;
-        int cl;
+        int cl, conv = 0;
         for (; it32 < 4; it32++) {
             c2p_eval(qf, Zf, ff, dff, v2f, cl);
             if (cl || !(dff != 0.0f)) break;
@@ -475,9 +488,24 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
             if (!(Zn > 0.0f)) break;
             float e = fabs_(Zn - Zf);
             Zf = Zn;
-            if (e <= 1e-6f * Zf) { it32++; break; }
+            if (e <= 1e-6f * Zf) { it32++; conv = 1; break; }
         }
-        if (Zf > 0.0f && Zf < 1e30f) Z = double(Zf);
+        if (Zf > 0.0f && Zf < 1e30f) {
+            Z = double(Zf);
+            // The FP32 root is kept (the primitives it gives are stored in
+            // FP32) where the residual is well conditioned: its rounding
+            // error, 2^-24 times its largest term (E, B^2, (S.B)^2 / Z^2),
+            // moves the root by at most 2^-24 * 16 Z / f'(Z), f' >= 1/2 here
+            if (conv && dff >= 0.5f) {
+                float iz = 1.0f / Zf;
+                float big = qf.E + qf.B2 + qf.SB2 * iz * iz;
+                if (big <= 16.0f * Zf) {
+                    iters = it32;
+                    s.Z = Z;
+                    return 0;
+                }
+            }
+        }
     }
     // phase 1; a step of at most sqrt(tol) Z is accepted as the last one:
     // Newton's quadratic convergence leaves an error of order tol Z after it
@@ -518,9 +546,15 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
         }
     }
     iters = it + it32;
-    if (!ok) return 1;
+    s.Z = Z;
+    return ok ? 0 : 1;
+}
+// the primitives at the root; returns 0, or 2 if the state is unphysical
+BH_HD inline int c2p_finish(const double* gi, const C2PS& s, const double* B, double* w) {
+    const C2P& q = s.q;
+    const double Z = s.Z;
     double iZ = 1.0 / Z, ZB = Z + q.B2, iZB = 1.0 / ZB;
-    v2 = q.S2 * iZB * iZB + q.SB2 * (q.B2 + 2.0 * Z) * iZ * iZ * iZB * iZB;
+    double v2 = q.S2 * iZB * iZB + q.SB2 * (q.B2 + 2.0 * Z) * iZ * iZ * iZB * iZB;
     if (!(v2 < q.v2max)) v2 = q.v2max;
     double W2i = 1.0 - v2, Wi = sqrt(W2i);
     double Wl = 1.0 / Wi;
@@ -528,13 +562,21 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
     double p = q.gf * (Z * W2i - rho);
     // v_i = (S_i + (S.B / Z) B_i) / (Z + B^2), raised with gamma^ij
     double vl[3], vu[3];
-    for (int i = 0; i < 3; i++) vl[i] = (S[i] + SB * iZ * Bl[i]) * iZB;
-    lower(m.gi, vl, vu);
+    for (int i = 0; i < 3; i++) vl[i] = (s.S[i] + s.SB * iZ * s.Bl[i]) * iZB;
+    lower(gi, vl, vu);
     w[P_RHO] = rho;
     w[P_PRS] = p;
     for (int i = 0; i < 3; i++) { w[P_UT + i] = Wl * vu[i]; w[P_B + i] = B[i]; }
     if (!(rho > 0.0) || !(p == p) || !(Wl == Wl)) return 2;
     return 0;
+}
+template <bool PRE32 = false>
+BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const double* B, const double* wo,
+                          double* w, int& iters) {
+    C2PS s;
+    c2p_setup(P, m, U, B, wo, s);
+    if (c2p_solve<PRE32>(P, s, iters)) return 1;
+    return c2p_finish(m.gi, s, B, w);
 }
 
 // ======================================================================
@@ -584,6 +626,16 @@ BH_HD inline void copy_metric(const KSb<A>& m, KSb<B>& mo) {
     mo.H = B(m.H); mo.alpha = B(m.alpha); mo.sqrtgam = B(m.sqrtgam); mo.r = B(m.r);
     for (int i = 0; i < 3; i++) { mo.l[i] = B(m.l[i]); mo.beta[i] = B(m.beta[i]); }
     for (int i = 0; i < 6; i++) { mo.g[i] = B(m.g[i]); mo.gi[i] = B(m.gi[i]); }
+}
+// the cell-centre metric in FP64; from the FP32 metric where g32
+BH_HD inline void cell_metric(const FxPar& P, const double* x, bool g32, KS& m) {
+    if (g32) {
+        KSb<float> mf;
+        ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
+        copy_metric(mf, m);
+    } else {
+        ks_metric(P, x[0], x[1], x[2], m);
+    }
 }
 template <typename A, typename B>
 BH_HD inline void copy_geometry(const KSb<A>& m, const KSDb<A>& d, KSb<B>& mo, KSDb<B>& dout) {

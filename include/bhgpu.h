@@ -445,15 +445,26 @@ typedef struct bh_fx_grid {
                                     from a counter in this array (the counters reset
                                     themselves at the end of each launch).  NULL: one
                                     CTA per work item.  Both give the same results. */
+    const int32_t *items_flux;   /* device [nitem_flux][2] (block, e), or NULL/0: the work
+                                    of the staged flux kernel.  e >= 0: tile e of the
+                                    block's position box [-1, n]^3, tiles of 4 x 4 x 8
+                                    positions (i, j, k), tile index (ti * nj + tj) * nk
+                                    + tk with nj = ceil((n+2)/4), nk = ceil((n+2)/8);
+                                    e < 0: the 128 positions from -(e+1) on, as in
+                                    items_pos (bhgrid.blocks.flux_items builds it)  */
+    int32_t nitem_flux;
 } bh_fx_grid;
 #define BH_FX_QSLOTS 6
 
 /* Launch bounds of the scheme's three heavy kernels (no counterpart in the
  * reference): each is compiled for 1 (no register cap) and 3 to 8
  * resident 128-thread CTAs per SM; the choice is per process and variant,
- * initially 1.  bhgpu.fixed.autotune times the candidates on a grid and sets
- * the fastest.  Launches (and graphs captured) after the call use it. */
-enum { BH_FX_TUNE_C2P = 0, BH_FX_TUNE_FLUX = 1, BH_FX_TUNE_UPDATE = 2, BH_FX_TUNE_N = 3 };
+ * initially 1.  BH_FX_TUNE_STAGE (0 or 1, initially 0) selects the flux
+ * kernel: 1 = the stencil staged in shared memory per tile (items_flux; grids
+ * without items_flux keep the unstaged kernel), with the launch bounds of
+ * BH_FX_TUNE_FLUX.  bhgpu.fixed.autotune times the candidates on a grid and
+ * sets the fastest.  Launches (and graphs captured) after the call use it. */
+enum { BH_FX_TUNE_C2P = 0, BH_FX_TUNE_FLUX = 1, BH_FX_TUNE_UPDATE = 2, BH_FX_TUNE_STAGE = 3, BH_FX_TUNE_N = 4 };
 int bh_fx_tune_set(int32_t precision, int32_t kernel, int32_t ctas_per_sm);
 int bh_fx_tune_get(int32_t precision, int32_t kernel, int32_t *ctas_per_sm);
 

@@ -186,7 +186,12 @@ def test_leveled_init_matches_oracle():
     for name in ("U", "W", "Bf"):
         a, b = getattr(g, name).cpu().numpy(), getattr(h, name)
         for v in range(a.shape[0]):
-            assert _rel_linf(a[v], b[v]) <= 1e-13, (name, v)
+            # the field is a difference quotient of the vector potential (CUDA's
+            # and libm's transcendentals differ by an ulp of A): on the finest
+            # level, dx = 80/256, the ulp of A grows by |A| / (dx |B|) in B
+            field = name == "Bf" or (name == "U" and v >= 5) or (name == "W" and v >= 5)
+            tol = 1e-12 if field else 1e-13
+            assert _rel_linf(a[v], b[v]) <= tol, (name, v, _rel_linf(a[v], b[v]))
     assert g.divb() <= 1e-14
 
 
@@ -257,3 +262,72 @@ def test_persistent_queue_equals_item_launches(leveled):
     for name in ("U", "Bf", "W"):
         assert np.array_equal(getattr(a, name).cpu().numpy(), getattr(b, name).cpu().numpy()), name
     assert int(a.queue.abs().sum().item()) == 0
+
+
+def _staged(prec, on):
+    from bhgpu import fixed as fxm
+    fxm.tune_set(prec, "stage", 1 if on else 0)
+
+
+def test_staged_fluxes_bitwise_against_oracle():
+    """the flux stencil staged in shared memory per 4 x 4 x 8 tile (a 64^3
+    block): fluxes and two steps of the FP64 variant equal the oracle bit
+    for bit"""
+    g = _grid(64, 64)
+    g.torus_init()
+    h = _host(g)
+    _load(h, g)
+    assert int((g.items["flux"][:, 1] >= 0).sum().item()) == g.items["flux"].shape[0]
+    _staged("fp64", True)
+    try:
+        g.prims(0, with_dt=True); h.prims(0, with_dt=True)
+        g.ghosts(0); h.ghosts(0)
+        g.fluxes(0); h.fluxes(0)
+        torch.cuda.synchronize()
+        assert np.array_equal(g.F.cpu().numpy(), h.F)
+        g.update(0); h.update(0)
+        g.prims(1); h.prims(1)
+        g.ghosts(1); h.ghosts(1)
+        g.fluxes(1); h.fluxes(1)
+        g.update(1); h.update(1)
+        g.step(); h.step()
+        torch.cuda.synchronize()
+        for name in ("U", "Bf", "W"):
+            assert np.array_equal(g.interior(getattr(g, name)), h.interior(getattr(h, name))), name
+    finally:
+        _staged("fp64", False)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("persistent", [False, True])
+def test_staged_equals_unstaged_on_blocks_of_three_sizes(precision, persistent):
+    """tiles (blocks of 16^3 and 32^3 here) and position chunks (8^3) in one
+    staged launch, one CTA per item or persistent: the same bits as the
+    unstaged kernel in FP64; in the contracted mixed variant the two kernels
+    may pair multiply-adds differently (relative L-infinity <= 1e-6 per
+    array after three steps)"""
+    from bhgpu.fixed import FxGrid, FxParams
+    from bhgrid.blocks import flux_items, torus_levels
+    lv = torus_levels(nb=8, r_fine=(14.0, 26.0), seed=3)
+    grids = [FxGrid.leveled(-40.0, 40.0, lv, 8, FxParams(precision=precision), persistent=persistent)
+             for _ in range(2)]
+    a, b = grids
+    a.items["flux"] = torch.from_numpy(flux_items(a.blocks_np, tile_min=16)).to(a.U.device)
+    a._refresh()
+    kinds = a.items["flux"][:, 1].cpu().numpy()
+    assert (kinds >= 0).any() and (kinds < 0).any()
+    a.torus_init()
+    b.torus_init()
+    for _ in range(3):
+        _staged(precision, True)
+        a.step()
+        _staged(precision, False)
+        b.step()
+    torch.cuda.synchronize()
+    for name in ("U", "Bf", "W"):
+        x, y = getattr(a, name).double().cpu().numpy(), getattr(b, name).double().cpu().numpy()
+        if precision == "fp64":
+            assert np.array_equal(x, y), name
+        else:
+            for v in range(x.shape[0]):
+                assert _rel_linf(x[v], y[v]) <= 1e-6, (name, v)
