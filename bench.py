@@ -157,9 +157,9 @@ def arm_config(args, world):
 
 
 # ---------------------------------------------------------------------------
-def torus_grid(args, precision):
+def torus_grid(args, precision, limiter="mc"):
     from bhgpu.fixed import FxGrid, FxParams
-    g = FxGrid.uniform(LO, HI, args.grid, args.block, FxParams(precision=precision))
+    g = FxGrid.uniform(LO, HI, args.grid, args.block, FxParams(precision=precision, limiter=limiter))
     info = g.torus_init(**TORUS)
     return g, info
 
@@ -637,6 +637,15 @@ def run_ours(args):
             pieces["fp64"] = piece_ms(gv)
         del gv
         torch.cuda.empty_cache()
+    # PPM reconstruction (three ghost layers, unstaged flux kernel) beside it
+    ppm = {}
+    for prec in ("mixed", "fp64"):
+        gv, _ = torus_grid(args, prec, "ppm")
+        ms_v, _ = timed_steps(gv, args.steps, warm, dist)
+        ppm[prec] = {"ms_per_step": ms_v, "zone_updates_per_s": world * args.grid ** 3 / (ms_v / 1e3)}
+        del gv
+        torch.cuda.empty_cache()
+    ppm["mixed_vs_plain_fp64"] = ppm["fp64"]["ms_per_step"] / ppm["mixed"]["ms_per_step"]
     acc = accuracy(args, args.accuracy_steps)
     if dist:
         dist.barrier()
@@ -652,7 +661,9 @@ def run_ours(args):
         top_ms = pieces["mixed"][top]
         byts = alg_bytes(top, args.block, 4) * nblk
         achieved = byts / (top_ms * 1e-3) / 1e9
-        kname = {"prims": "k_fx_c2p<float>", "ghosts": "k_fx_ghost<float>", "fluxes": "k_fx_flux<float,float,float>",
+        from bhgpu.fixed import tune_get
+        flux_k = "k_fx_flux_tile" if tune_get("mixed", "stage") else "k_fx_flux"
+        kname = {"prims": "k_fx_c2p<float>", "ghosts": "k_fx_ghost<float>", "fluxes": f"{flux_k}<float,float,float>",
                  "update": "k_fx_update<float,float,float>"}[top]
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -664,6 +675,7 @@ def run_ours(args):
                                     "speedup_vs_fp64_fma": variants["fp64-fma"]["ms_per_step"] / ms_mixed,
                                     "accuracy_after_steps": acc},
             "variants": variants,
+            "ppm": ppm,
             "torus": {"ell": info["ell"], "field_scale": info["field_scale"], "beta": info["beta"],
                       "div_B_rel_after_timed_steps": divb_after, "counters_after_timed_steps": counters},
             "e2e": {"value": world * zones / (ms_e2e / 1e3), "unit": METRIC, "h2d_bytes_per_step": nbytes,

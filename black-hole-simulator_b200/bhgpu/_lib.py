@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libbhgpu.so")
 
 BH_OK, BH_EINVAL, BH_ECUDA, BH_ERANGE = 0, -1, -2, -3
 BH_ERR_DOMAIN = 1
-BH_MINMOD, BH_VANLEER, BH_MC = 0, 1, 2
+BH_MINMOD, BH_VANLEER, BH_MC, BH_PPM = 0, 1, 2, 3
 BH_FP64, BH_FP64_FMA, BH_MIXED = 0, 1, 2
 _vp = C.c_void_p
 

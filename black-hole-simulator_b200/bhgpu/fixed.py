@@ -10,7 +10,7 @@ con2prim, ghost fill, face fluxes, constrained transport and update
 buffers are torch tensors; every computation runs in ``libbhgpu.so``.
 
 Layout (``include/bhgpu.h``, bh_fx_grid): cubic blocks of n^3 interior cells,
-each stored per array as an (n+5)^3 box (cells -2 .. n+2 per axis).
+each stored per array as an (n+7)^3 box (cells -3 .. n+3 per axis).
 """
 from __future__ import annotations
 
@@ -21,16 +21,16 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from bhgrid.blocks import (BLOCK_DTYPE, CHUNK, TILE_MIN, box_size, flux_items, interior as _interior,  # noqa: F401
-                           leveled_blocks, uniform_blocks, work_items)
+from bhgrid.blocks import (BLOCK_DTYPE, CHUNK, TILE_MIN, box_size, flux_items, ghost_depth,  # noqa: F401
+                           interior as _interior, leveled_blocks, uniform_blocks, work_items)
 
-from ._lib import BH_FP64, BH_FP64_FMA, BH_MIXED, BH_MC, BH_MINMOD, BH_VANLEER, BhError, check, lib
+from ._lib import BH_FP64, BH_FP64_FMA, BH_MIXED, BH_MC, BH_MINMOD, BH_PPM, BH_VANLEER, BhError, check, lib
 
 _vp, _d, _i32, _i64 = C.c_void_p, C.c_double, C.c_int32, C.c_int64
 GHOST = 2
 QSLOTS = 6           # BH_FX_QSLOTS
 PRECISIONS = {"fp64": BH_FP64, "fp64-fma": BH_FP64_FMA, "mixed": BH_MIXED}
-LIMITERS = {"minmod": BH_MINMOD, "vanleer": BH_VANLEER, "mc": BH_MC}
+LIMITERS = {"minmod": BH_MINMOD, "vanleer": BH_VANLEER, "mc": BH_MC, "ppm": BH_PPM}
 
 
 class BhFxParams(C.Structure):
@@ -44,7 +44,7 @@ class BhFxGrid(C.Structure):
                 ("items_pos", _vp), ("nitem_pos", _i32), ("items_ghost", _vp), ("nitem_ghost", _i32),
                 ("ncell", _i64), ("U", _vp), ("U1", _vp), ("W", _vp), ("Bf", _vp), ("Bf1", _vp), ("F", _vp),
                 ("dt", _vp), ("count", _vp), ("err", _vp), ("E", _vp), ("maxlevel", _i32), ("queue_ctas", _i32), ("queue", _vp),
-                ("items_flux", _vp), ("nitem_flux", _i32)]
+                ("items_flux", _vp), ("nitem_flux", _i32), ("ghost_depth", _i32)]
 
 
 class BhFxTorus(C.Structure):
@@ -124,7 +124,9 @@ class FxGrid:
         dev = self.device
         self.blocks = torch.from_numpy(blocks.view(np.uint8).copy()).to(dev)
         self.nbr = torch.from_numpy(nbr.copy()).to(dev)
-        self.items = {k: torch.from_numpy(work_items(blocks, k)).to(dev) for k in ("cell", "pos", "ghost")}
+        self.ghost_depth = ghost_depth(params.limiter)
+        self.items = {k: torch.from_numpy(work_items(blocks, k, self.ghost_depth)).to(dev)
+                      for k in ("cell", "pos", "ghost")}
         self.items["flux"] = torch.from_numpy(flux_items(blocks)).to(dev)
         wdt = torch.float32 if params.precision == "mixed" else torch.float64
         N = self.ncell
@@ -166,7 +168,7 @@ class FxGrid:
                            _ptr(it["ghost"]), it["ghost"].shape[0], self.ncell,
                            _ptr(self.U), _ptr(self.U1), _ptr(self.W), _ptr(self.Bf), _ptr(self.Bf1), _ptr(self.F),
                            _ptr(self.dt), _ptr(self.count), _ptr(self.err), _ptr(self.E), self.maxlevel, 0, _ptr(self.queue),
-                           _ptr(it["flux"]), it["flux"].shape[0])
+                           _ptr(it["flux"]), it["flux"].shape[0], self.ghost_depth)
         self._p = self.params.cstruct()
 
     @property

@@ -1,6 +1,6 @@
 """Block tables of the corrected scheme's grid (include/bhgpu.h, bh_fx_grid).
 
-Pure numpy: the block table (n, level, offset of the block's (n+5)^3 box,
+Pure numpy: the block table (n, level, offset of the block's (n+7)^3 box,
 lower corner, spacing), the 27-neighbour table used by the ghost fill and the
 work lists (block, first index) the kernels walk.  The CPU oracle and the GPU
 path build their grids from the same tables.
@@ -10,14 +10,20 @@ from __future__ import annotations
 import numpy as np
 
 CHUNK = 128          # BH_FX_CHUNK: indices per work item (threads per CTA)
+GB = 3               # ghost layers of every block's box
 
 BLOCK_DTYPE = np.dtype([("n", "<i4"), ("level", "<i4"), ("off", "<i8"), ("x0", "<f8", 3), ("dx", "<f8")])
 assert BLOCK_DTYPE.itemsize == 48
 
 
 def box_size(n: int) -> int:
-    """Entries of one block's box per array: cells -2 .. n+2 per axis."""
-    return (n + 5) ** 3
+    """Entries of one block's box per array: cells -3 .. n+3 per axis."""
+    return (n + 2 * GB + 1) ** 3
+
+
+def ghost_depth(limiter) -> int:
+    """Ghost layers the fill covers: 3 for PPM's stencil, else 2."""
+    return 3 if limiter in ("ppm", 3) else 2
 
 
 def uniform_blocks(lo: float, hi: float, ncell: int, nblk: int, periodic: bool = False):
@@ -53,16 +59,17 @@ def uniform_blocks(lo: float, hi: float, ncell: int, nblk: int, periodic: bool =
     return blocks, nbr
 
 
-def index_count(n: int, kind: str) -> int:
-    return {"cell": n ** 3, "pos": (n + 2) ** 3, "ghost": (n + 4) ** 3 - n ** 3}[kind]
+def index_count(n: int, kind: str, depth: int = 2) -> int:
+    return {"cell": n ** 3, "pos": (n + 2) ** 3, "ghost": (n + 2 * depth) ** 3 - n ** 3}[kind]
 
 
-def work_items(blocks: np.ndarray, kind: str) -> np.ndarray:
+def work_items(blocks: np.ndarray, kind: str, depth: int = 2) -> np.ndarray:
     """(block, first index) pairs of CHUNK consecutive indices of each
-    block's index space: 'cell' n^3, 'pos' (n+2)^3, 'ghost' (n+4)^3 - n^3."""
+    block's index space: 'cell' n^3, 'pos' (n+2)^3, 'ghost' (n+2 depth)^3 -
+    n^3 (the shell of the depth ghost layers the fill covers)."""
     out = []
     for b, n in enumerate(blocks["n"]):
-        starts = np.arange(0, index_count(int(n), kind), CHUNK, dtype=np.int32)
+        starts = np.arange(0, index_count(int(n), kind, depth), CHUNK, dtype=np.int32)
         out.append(np.stack([np.full_like(starts, b), starts], 1))
     return np.concatenate(out).astype(np.int32)
 
@@ -109,11 +116,11 @@ def interior(blocks: np.ndarray, arr: np.ndarray) -> np.ndarray:
     """[..., nblock, n, n, n] interior cells of a [..., ncell] array (all
     blocks of one size)."""
     n = int(blocks["n"][0])
-    S = n + 5
+    S = n + 2 * GB + 1
     out = []
     for b in blocks:
         box = arr[..., int(b["off"]):int(b["off"]) + S ** 3].reshape(arr.shape[:-1] + (S, S, S))
-        out.append(box[..., 2:2 + n, 2:2 + n, 2:2 + n])
+        out.append(box[..., GB:GB + n, GB:GB + n, GB:GB + n])
     return np.stack(out, axis=-4)
 
 

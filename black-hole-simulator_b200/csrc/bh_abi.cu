@@ -189,6 +189,9 @@ int fx_bad(const bh_fx_params* P, const bh_fx_grid* g) {
         return 1;
     if (P->precision < BH_FP64 || P->precision > BH_MIXED || P->maxiter <= 0 || !(P->gamma > 1.0)) return 1;
     if (g->maxlevel < 0 || g->maxlevel > 8 || (g->maxlevel > 0 && !g->E)) return 1;
+    if (P->limiter < BH_MINMOD || P->limiter > BH_PPM || (g->ghost_depth != 0 && g->ghost_depth != 2 && g->ghost_depth != 3) ||
+        (P->limiter == BH_PPM && g->ghost_depth != 3) || (g->nitem_flux > 0 && !g->items_flux))
+        return 1;
     return 0;
 }
 }  // namespace

@@ -8,12 +8,14 @@
 //       bytes of the face work
 // Conserved state, face field, con2prim, the CT update and dt stay FP64.
 //
-// Data: a list of cubic blocks, each n^3 interior cells with two ghost
-// layers, stored per array as a (n+5)^3 box (cells -2..n+2 per axis; the
-// extra layer holds the upper faces): index ((i+2) S + (j+2)) S + (k+2) with
-// S = n + 5 -- the reference's per-patch order (grid.cpp:51-53: i slowest,
-// k fastest).  The x-face (i-1/2, j, k), the y-face (i, j-1/2, k) and the
-// z-face (i, j, k-1/2) share the index of cell (i, j, k); so do the edges
+// Data: a list of cubic blocks, each n^3 interior cells with FX_GB = 3
+// ghost layers, stored per array as a (n+7)^3 box (cells -3..n+3 per axis;
+// the extra layer holds the upper faces): index ((i+3) S + (j+3)) S + (k+3)
+// with S = n + 7 -- the reference's per-patch order (grid.cpp:51-53: i
+// slowest, k fastest).  The ghost fill covers the two layers PLM reads, or
+// all three for PPM (Grid::gdepth).  The x-face (i-1/2, j, k), the y-face
+// (i, j-1/2, k) and the z-face (i, j, k-1/2) share the index of cell
+// (i, j, k); so do the edges
 // E_x (i, j-1/2, k-1/2), E_y (i-1/2, j, k-1/2) and E_z (i-1/2, j-1/2, k).
 //
 // Work: every kernel walks a list of items (block, first index); item t of
@@ -39,9 +41,11 @@ struct Grid {
     int32_t* count;
     int32_t* err;
     double* E;
+    int gdepth;   // ghost layers filled: 2, or 3 (PPM)
 };
 inline Grid grid_of(const bh_fx_grid* g) {
-    return Grid{g->blocks, g->nbr, g->U, g->U1, g->Bf, g->Bf1, g->W, g->F, g->ncell, g->dt, g->count, g->err, g->E};
+    return Grid{g->blocks, g->nbr, g->U,     g->U1,  g->Bf, g->Bf1, g->W, g->F, g->ncell, g->dt, g->count, g->err,
+                g->E,      g->ghost_depth > 2 ? 3 : 2};
 }
 inline FxPar par_of(const bh_fx_params* p) {
     FxPar q;
@@ -51,12 +55,13 @@ inline FxPar par_of(const bh_fx_params* p) {
     return q;
 }
 
+constexpr int FX_GB = 3;
 __device__ inline int64_t bidx(const bh_fx_block& b, int i, int j, int k) {
-    const int S = b.n + 5;
-    return b.off + ((int64_t)(i + 2) * S + (j + 2)) * S + (k + 2);
+    const int S = b.n + 2 * FX_GB + 1;
+    return b.off + ((int64_t)(i + FX_GB) * S + (j + FX_GB)) * S + (k + FX_GB);
 }
-__device__ inline int bstride_i(const bh_fx_block& b) { return (b.n + 5) * (b.n + 5); }
-__device__ inline int bstride_j(const bh_fx_block& b) { return b.n + 5; }
+__device__ inline int bstride_i(const bh_fx_block& b) { return (b.n + 2 * FX_GB + 1) * (b.n + 2 * FX_GB + 1); }
+__device__ inline int bstride_j(const bh_fx_block& b) { return b.n + 2 * FX_GB + 1; }
 
 // ---- positions ---------------------------------------------------------
 __device__ inline void cell_centre(const bh_fx_block& b, int i, int j, int k, double* x) {
@@ -237,32 +242,34 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
 }
 
 // ======================================================================
-// ghost fill: cells of the two ghost layers (edges and corners included)
+// ghost fill: cells of the g ghost layers (edges and corners included)
 // take the primitives of the cell they image -- in a neighbour block
 // (same size and level) or, across the outer boundary, the nearest
 // interior cell (outflow: copy, the role of gh_bndy, grid.cpp:494-522) --
 // and the face field of their faces outside the block's own range.
 // ======================================================================
-__device__ inline int shell_decode(int n, int e, int& i, int& j, int& k) {
-    const int m = n + 4;
-    const int s1 = 4 * m * m, s2 = 4 * n * m, s3 = 4 * n * n;
-    if (e < s1) {   // i in {-2,-1,n,n+1}, j,k in [-2, n+1]
+// ghost cell e of the g layers around n^3 cells: i in the 2g ghost planes
+// first (all j, k), then j (interior i), then k (interior i, j)
+__device__ inline int shell_decode(int n, int g, int e, int& i, int& j, int& k) {
+    const int m = n + 2 * g, h = 2 * g;
+    const int s1 = h * m * m, s2 = h * n * m, s3 = h * n * n;
+    if (e < s1) {   // i in {-g..-1, n..n+g-1}, j, k in [-g, n+g)
         int q = e / (m * m), r = e % (m * m);
-        i = q < 2 ? q - 2 : n + q - 2; j = r / m - 2; k = r % m - 2;
+        i = q < g ? q - g : n + q - g; j = r / m - g; k = r % m - g;
         return 1;
     }
     e -= s1;
-    if (e < s2) {   // i in [0,n), j in {-2,-1,n,n+1}, k in [-2, n+1]
+    if (e < s2) {   // i in [0,n), j in the ghost planes, k in [-g, n+g)
         int q = e / (n * m), r = e % (n * m);
-        i = r / m; k = r % m - 2;
-        j = q < 2 ? q - 2 : n + q - 2;
+        i = r / m; k = r % m - g;
+        j = q < g ? q - g : n + q - g;
         return 1;
     }
     e -= s2;
-    if (e < s3) {   // i, j in [0,n), k in {-2,-1,n,n+1}
+    if (e < s3) {   // i, j in [0,n), k in the ghost planes
         int q = e / (n * n), r = e % (n * n);
         i = r / n; j = r % n;
-        k = q < 2 ? q - 2 : n + q - 2;
+        k = q < g ? q - g : n + q - g;
         return 1;
     }
     return 0;
@@ -314,7 +321,7 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_ghost(Grid G, const int32_t* item
         const int n = B.n;
         const int e = items[2 * t + 1] + threadIdx.x;
         int i, j, k;
-        if (!shell_decode(n, e, i, j, k)) return;
+        if (!shell_decode(n, G.gdepth, e, i, j, k)) return;
         const int64_t N = G.ncell;
         WT* W = (WT*)G.W;
         double* Bf = stage ? G.Bf1 : G.Bf;
@@ -405,8 +412,9 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_ghost(Grid G, const int32_t* item
 // layer feeds the EMFs of the block's boundary edges)
 // ======================================================================
 // the face computation; sten(v, o) is variable v of the cell o = -2..1
-// steps along d from (i, j, k) (the face lies between o = -1 and o = 0)
-template <typename RT, typename FT, typename Sten>
+// (PLM) or -3..2 (PPM, where PPM6) steps along d from (i, j, k) (the face
+// lies between o = -1 and o = 0)
+template <typename RT, typename FT, bool PPM6, typename Sten>
 __device__ __forceinline__ void face_flux_at(const FxPar& P, const Grid& G, const bh_fx_block& B, int i, int j, int k,
                                              int d, const double* Bfs, const Sten& sten) {
     const int64_t N = G.ncell;
@@ -419,7 +427,12 @@ __device__ __forceinline__ void face_flux_at(const FxPar& P, const Grid& G, cons
     RT wL[8], wR[8];
     for (int v = 0; v < 8; v++) {
         if (v == P_B + d) continue;
-        plm_face(sten(v, -2), sten(v, -1), sten(v, 0), sten(v, 1), P.limiter, wL[v], wR[v]);
+        if (PPM6 && P.limiter == FX_PPM) {
+            const RT a[6] = {sten(v, -3), sten(v, -2), sten(v, -1), sten(v, 0), sten(v, 1), sten(v, 2)};
+            ppm_face(a, wL[v], wR[v]);
+        } else {
+            plm_face(sten(v, -2), sten(v, -1), sten(v, 0), sten(v, 1), P.limiter, wL[v], wR[v]);
+        }
     }
     // (the limiters keep every face value between its two cells' values, so
     // face densities and pressures stay positive)
@@ -439,7 +452,7 @@ __device__ inline void face_flux(const FxPar& P, const Grid& G, const bh_fx_bloc
     const int64_t N = G.ncell;
     const WT* Wc = (const WT*)G.W + bidx(B, i, j, k);
     const int st = d == 0 ? bstride_i(B) : (d == 1 ? bstride_j(B) : 1);
-    face_flux_at<RT, FT>(P, G, B, i, j, k, d, Bfs, [&](int v, int o) { return RT(Wc[v * N + o * st]); });
+    face_flux_at<RT, FT, true>(P, G, B, i, j, k, d, Bfs, [&](int v, int o) { return RT(Wc[v * N + o * st]); });
 }
 
 template <typename RT, typename WT, typename FT, int MINB>
@@ -536,12 +549,15 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux_tile(FxPar P, Grid G, 
         const int i = i0 + a, j = j0 + bb, k = k0 + c;
         if (i > n || j > n || k > n) return;
         const int o = box_at(a, bb, c);
+        // (PLM only: the launch keeps PPM's wider stencil on k_fx_flux)
         if (i >= 0)
-            face_flux_at<RT, FT>(P, G, B, i, j, k, 0, Bfs,
-                                 [&](int v, int s) { return RT(sW[v][o + s * (FX_HJ * FX_HK)]); });
+            face_flux_at<RT, FT, false>(P, G, B, i, j, k, 0, Bfs,
+                                        [&](int v, int s) { return RT(sW[v][o + s * (FX_HJ * FX_HK)]); });
         if (j >= 0)
-            face_flux_at<RT, FT>(P, G, B, i, j, k, 1, Bfs, [&](int v, int s) { return RT(sW[v][o + s * FX_HK]); });
-        if (k >= 0) face_flux_at<RT, FT>(P, G, B, i, j, k, 2, Bfs, [&](int v, int s) { return RT(sW[v][o + s]); });
+            face_flux_at<RT, FT, false>(P, G, B, i, j, k, 1, Bfs,
+                                        [&](int v, int s) { return RT(sW[v][o + s * FX_HK]); });
+        if (k >= 0)
+            face_flux_at<RT, FT, false>(P, G, B, i, j, k, 2, Bfs, [&](int v, int s) { return RT(sW[v][o + s]); });
     });
 }
 
@@ -1044,7 +1060,7 @@ int fx_ghosts(const bh_fx_params*, const bh_fx_grid* g, int32_t stage, void* s) 
 int fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
-    if (fx_tune_tab[BH_FX_TUNE_STAGE] && g->nitem_flux) {
+    if (fx_tune_tab[BH_FX_TUNE_STAGE] && g->nitem_flux && P->limiter != fx::FX_PPM) {
 #define L_(M) fx::k_fx_flux_tile<FRT, FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_flux_tile<FRT, FRT, FRT, M>, g->nitem_flux, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_flux, stage, fx_q(g, QS_FLUX, g->nitem_flux))
         FX_TUNED(BH_FX_TUNE_FLUX, L_)
 #undef L_

@@ -263,7 +263,7 @@ BH_HD inline void signal_speeds(const KSm<RT>& m, RT gamma, int dd, const RT* w,
 // ======================================================================
 // PLM (reconfp's role, reconstruction.cpp:40-97): limited slopes
 // ======================================================================
-enum { FX_MINMOD = 0, FX_VANLEER = 1, FX_MC = 2 };
+enum { FX_MINMOD = 0, FX_VANLEER = 1, FX_MC = 2, FX_PPM = 3 };
 template <typename RT>
 BH_HD inline RT lim_slope(RT dl, RT dr, int lim) {
     if (dl * dr <= RT(0)) return RT(0);
@@ -281,6 +281,50 @@ template <typename RT>
 BH_HD inline void plm_face(RT wmm, RT wm, RT wp, RT wpp, int lim, RT& L, RT& R) {
     L = wm + RT(0.5) * lim_slope(wm - wmm, wp - wm, lim);
     R = wp - RT(0.5) * lim_slope(wp - wm, wpp - wp, lim);
+}
+
+// ======================================================================
+// PPM (Colella & Woodward 1984, J. Comput. Phys. 54, 174, eqs. 1.6-1.8 and
+// 1.10; no contact steepening, no flattening).  The face p-1/2 from the
+// cells a[0..5] = p-3 .. p+2: limited slopes of cells p-2 .. p+1, the
+// fourth-order interface values a_{p-3/2}, a_{p-1/2}, a_{p+1/2}, and the
+// monotonised parabolas of cells p-1 (its right value is L) and p (its left
+// value is R).  Every interface value lies between its two cells' values,
+// so face densities and pressures stay positive as with PLM.
+// ======================================================================
+template <typename RT>
+BH_HD inline RT ppm_dm(RT am, RT a0, RT ap) {
+    RT dl = a0 - am, dr = ap - a0;
+    if (dl * dr <= RT(0)) return RT(0);
+    RT da = RT(0.5) * (ap - am);
+    RT m = fmin_(fabs_(da), RT(2) * fmin_(fabs_(dl), fabs_(dr)));
+    return da > RT(0) ? m : -m;
+}
+template <typename RT>
+BH_HD inline void ppm_parabola(RT a, RT& l, RT& r) {
+    if ((r - a) * (a - l) <= RT(0)) {
+        l = a;
+        r = a;
+    } else {
+        RT d = r - l, c = a - RT(0.5) * (l + r), d2 = d * d * (RT(1) / RT(6));
+        if (d * c > d2)
+            l = RT(3) * a - RT(2) * r;
+        else if (-d2 > d * c)
+            r = RT(3) * a - RT(2) * l;
+    }
+}
+template <typename RT>
+BH_HD inline void ppm_face(const RT* a, RT& L, RT& R) {
+    RT dm[4];
+    for (int q = 0; q < 4; q++) dm[q] = ppm_dm(a[q], a[q + 1], a[q + 2]);
+    RT f[3];
+    for (int q = 0; q < 3; q++)
+        f[q] = a[q + 1] + RT(0.5) * (a[q + 2] - a[q + 1]) - (RT(1) / RT(6)) * (dm[q + 1] - dm[q]);
+    RT lL = f[0], lR = f[1], rL = f[1], rR = f[2];
+    ppm_parabola(a[2], lL, lR);
+    ppm_parabola(a[3], rL, rR);
+    L = lR;
+    R = rL;
 }
 
 // ======================================================================

@@ -59,8 +59,9 @@ enum {
                          source in FP32; metric, constrained transport, flux
                          divergence, RK combine, con2prim, floors and dt in FP64  */
 };
-/* reconstruction limiter (recon.hpp:36) */
-enum { BH_MINMOD = 0, BH_VANLEER = 1, BH_MC = 2 };
+/* reconstruction limiter (recon.hpp:36); BH_PPM (the corrected scheme only):
+ * the piecewise-parabolic method of Colella & Woodward (1984) */
+enum { BH_MINMOD = 0, BH_VANLEER = 1, BH_MC = 2, BH_PPM = 3 };
 /* neighbour kinds of the ghost fill (grid.cpp:528-534) */
 enum { BH_NB_BNDY = 0, BH_NB_COPY = 1, BH_NB_PROLONG = 2 };
 
@@ -373,14 +374,14 @@ int bh_step_graph_destroy(bh_step_graph *g);
  * the floor state at rest every stage).
  *
  * Layout: a list of cubic blocks of n^3 interior cells (n even, at least 4)
- * with two ghost layers.  Blocks are equal cubes of space; a block of level
+ * with three ghost layers (the fill covers two, or three with BH_PPM).  Blocks are equal cubes of space; a block of level
  * l holds twice the cells per axis of level l-1 (the 27-neighbour table
  * links equal cubes, whose levels differ by one at most): ghost cells of a
  * coarser or finer neighbour are prolonged or restricted, and the edge EMFs
- * of a coarse block along a finer one take the finer block's values; every array stores each block as a (n+5)^3 box
- * (cells -2 .. n+2 per axis) at offset blocks[b].off, index
- * ((i+2) S + (j+2)) S + (k+2), S = n + 5 (i slowest, k fastest, as the
- * reference's patches).  The x-face (i-1/2, j, k), y-face (i, j-1/2, k) and
+ * of a coarse block along a finer one take the finer block's values; every
+ * array stores each block as a (n+7)^3 box (cells -3 .. n+3 per axis) at
+ * offset blocks[b].off, index ((i+3) S + (j+3)) S + (k+3), S = n + 7 (i
+ * slowest, k fastest, as the reference's patches).  The x-face (i-1/2, j, k), y-face (i, j-1/2, k) and
  * z-face (i, j, k-1/2) share the index of cell (i, j, k).
  *   U, U1  [8][ncell] conserved D, S_x, S_y, S_z, tau, B^x, B^y, B^z
  *                     densitised by sqrt(gamma) (U1: the RK stage state)
@@ -392,7 +393,8 @@ int bh_step_graph_destroy(bh_step_graph *g);
  * Work lists: items_* are device arrays of int32 pairs (block, first index)
  * of BH_FX_CHUNK consecutive indices of the block's index space: interior
  * cells (n^3, index (i n + j) n + k), flux positions ((n+2)^3, positions
- * -1 .. n per axis) and ghost cells ((n+4)^3 - n^3, the ghost shell).
+ * -1 .. n per axis) and ghost cells ((n+2g)^3 - n^3, the shell of the g =
+ * ghost_depth layers the fill covers).
  * ========================================================================== */
 #define BH_FX_CHUNK 128
 typedef struct bh_fx_params {
@@ -403,7 +405,7 @@ typedef struct bh_fx_params {
     double r_exc;                /* excision radius                                 */
     double tol;                  /* con2prim: stop when |dZ| <= tol Z (1e-12)       */
     int32_t maxiter;             /* con2prim Newton cap (30)                        */
-    int32_t limiter;             /* BH_MINMOD / BH_VANLEER / BH_MC                  */
+    int32_t limiter;             /* BH_MINMOD / BH_VANLEER / BH_MC / BH_PPM         */
     int32_t precision;           /* BH_FP64 / BH_FP64_FMA / BH_MIXED                */
     int32_t reserved;
 } bh_fx_params;
@@ -425,7 +427,7 @@ typedef struct bh_fx_grid {
     const int32_t *items_cell; int32_t nitem_cell;
     const int32_t *items_pos;  int32_t nitem_pos;
     const int32_t *items_ghost; int32_t nitem_ghost;
-    int64_t ncell;               /* entries per array (sum of (n+5)^3)               */
+    int64_t ncell;               /* entries per array (sum of (n+7)^3)               */
     double *U, *U1;
     void *W;
     double *Bf, *Bf1;
@@ -453,6 +455,9 @@ typedef struct bh_fx_grid {
                                     e < 0: the 128 positions from -(e+1) on, as in
                                     items_pos (bhgrid.blocks.flux_items builds it)  */
     int32_t nitem_flux;
+    int32_t ghost_depth;         /* ghost layers the fill covers (and items_ghost
+                                    lists): 2 (0 reads as 2), or 3, which BH_PPM
+                                    requires                                        */
 } bh_fx_grid;
 #define BH_FX_QSLOTS 6
 

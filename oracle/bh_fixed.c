@@ -195,6 +195,7 @@ static void speeds(const ksm* m, double gamma, int dd, const double* w, const dr
 }
 
 /* ------------------------------------------------------------------ PLM */
+enum { LIM_MINMOD = 0, LIM_VANLEER = 1, LIM_MC = 2, LIM_PPM = 3 };
 static double slope(double dl, double dr, int lim) {
     if (dl * dr <= 0.0) return 0.0;
     if (lim == 1) return 2.0 * dl * dr / (dl + dr);
@@ -205,6 +206,46 @@ static double slope(double dl, double dr, int lim) {
         return s * dmin(c, 2.0 * dmin(al, ar));
     }
     return s * dmin(al, ar);
+}
+
+/* PPM (Colella & Woodward 1984, J. Comput. Phys. 54, 174: eqs. 1.6-1.8 and
+ * 1.10, without contact steepening or flattening): the face between cells
+ * a[2] and a[3] of a[0..5] (cells p-3 .. p+2 for the face p-1/2).  Limited
+ * slopes of cells p-2 .. p+1, the fourth-order interface values a_{p-3/2},
+ * a_{p-1/2}, a_{p+1/2}, and the monotonised parabolas of cells p-1 (its
+ * right value is L) and p (its left value is R). */
+static double ppm_dm(double am, double a0, double ap) {
+    double dl = a0 - am, dr = ap - a0;
+    if (dl * dr <= 0.0) return 0.0;
+    double da = 0.5 * (ap - am);
+    double m = dmin(dabs(da), 2.0 * dmin(dabs(dl), dabs(dr)));
+    return da > 0.0 ? m : -m;
+}
+static void ppm_parabola(double a, double* aL, double* aR) {
+    double l = *aL, r = *aR;
+    if ((r - a) * (a - l) <= 0.0) {
+        l = a;
+        r = a;
+    } else {
+        double d = r - l, c = a - 0.5 * (l + r), d2 = d * d * (1.0 / 6.0);
+        if (d * c > d2)
+            l = 3.0 * a - 2.0 * r;
+        else if (-d2 > d * c)
+            r = 3.0 * a - 2.0 * l;
+    }
+    *aL = l;
+    *aR = r;
+}
+static void ppm_face(const double* a, double* L, double* R) {
+    double dm[4];
+    for (int q = 0; q < 4; q++) dm[q] = ppm_dm(a[q], a[q + 1], a[q + 2]);   /* cells p-2 .. p+1 */
+    double f[3];   /* a_{p-3/2}, a_{p-1/2}, a_{p+1/2} */
+    for (int q = 0; q < 3; q++) f[q] = a[q + 1] + 0.5 * (a[q + 2] - a[q + 1]) - (1.0 / 6.0) * (dm[q + 1] - dm[q]);
+    double lL = f[0], lR = f[1], rL = f[1], rR = f[2];
+    ppm_parabola(a[2], &lL, &lR);
+    ppm_parabola(a[3], &rL, &rR);
+    *L = lR;
+    *R = rL;
 }
 
 static double hll(const ksm* m, double gamma, int dd, const double* wL, const double* wR, double* F) {
@@ -468,9 +509,13 @@ typedef struct {
     int32_t* count;
 } fxo_grid;
 
+/* every block is stored as a box of GB ghost layers (and one more cell per
+ * axis above) per array: index ((i+GB) S + (j+GB)) S + (k+GB), S = n+2GB+1 */
+#define GB 3
+#define SP(n) ((n) + 2 * GB + 1)
 static int64_t bx(const fxo_block* b, int i, int j, int k) {
-    int64_t S = b->n + 5;
-    return b->off + ((int64_t)(i + 2) * S + (j + 2)) * S + (k + 2);
+    int64_t S = SP(b->n);
+    return b->off + ((int64_t)(i + GB) * S + (j + GB)) * S + (k + GB);
 }
 static void centre(const fxo_block* b, int i, int j, int k, double* x) {
     x[0] = b->x0[0] + (i + 0.5) * b->dx;
@@ -482,7 +527,7 @@ static void prims_cell(const fxo_grid* G, const fxo_block* B, int i, int j, int 
                        int with_dt) {
     const fxo_params* P = G->P;
     int64_t N = G->N, c = bx(B, i, j, k);
-    int si = (B->n + 5) * (B->n + 5), sj = B->n + 5;
+    int si = SP(B->n) * SP(B->n), sj = SP(B->n);
     double* U = stage ? G->U1 : G->U;
     const double* Bf = stage ? G->Bf1 : G->Bf;
     double x[3];
@@ -582,16 +627,16 @@ static double mm_slope(double a, double b, double c) {
  * or the mean of the two it lies between).  Pass 0: copies and
  * restrictions; pass l: prolongations into level-l blocks. */
 void fxo_ghosts(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, double* W, double* Bf,
-                double* Bf1, int stage, int maxlevel) {
+                double* Bf1, int stage, int maxlevel, int depth) {
     double* F = stage ? Bf1 : Bf;
     for (int pass = 0; pass <= maxlevel; pass++)
         for (int b = 0; b < nblock; b++) {
             int n = blk[b].n;
             if (pass > 0 && blk[b].level != pass) continue;
 #pragma omp parallel for schedule(static)
-            for (int i = -2; i < n + 2; i++)
-                for (int j = -2; j < n + 2; j++)
-                    for (int k = -2; k < n + 2; k++) {
+            for (int i = -depth; i < n + depth; i++)
+                for (int j = -depth; j < n + depth; j++)
+                    for (int k = -depth; k < n + depth; k++) {
                         if (i >= 0 && i < n && j >= 0 && j < n && k >= 0 && k < n) continue;
                         int64_t c = bx(&blk[b], i, j, k);
                         int q[3] = {i, j, k};
@@ -671,7 +716,7 @@ void fxo_ghosts(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_
 static void face(const fxo_params* P, const fxo_block* B, int64_t N, const double* W, const double* Bfs, double* F,
                  int i, int j, int k, int d) {
     int64_t c = bx(B, i, j, k);
-    int st = d == 0 ? (B->n + 5) * (B->n + 5) : (d == 1 ? B->n + 5 : 1);
+    int st = d == 0 ? SP(B->n) * SP(B->n) : (d == 1 ? SP(B->n) : 1);
     double x[3];
     centre(B, i, j, k, x);
     x[d] -= 0.5 * B->dx;
@@ -680,6 +725,12 @@ static void face(const fxo_params* P, const fxo_block* B, int64_t N, const doubl
     double wL[8], wR[8];
     for (int v = 0; v < 8; v++) {
         if (v == BB + d) continue;
+        if (P->limiter == LIM_PPM) {
+            double a6[6];
+            for (int o = 0; o < 6; o++) a6[o] = W[v * N + c + (o - 3) * st];
+            ppm_face(a6, &wL[v], &wR[v]);
+            continue;
+        }
         double a = W[v * N + c - 2 * st], b = W[v * N + c - st], cc = W[v * N + c], dd = W[v * N + c + st];
         wL[v] = b + 0.5 * slope(b - a, cc - b, P->limiter);
         wR[v] = cc - 0.5 * slope(cc - b, dd - cc, P->limiter);
@@ -725,7 +776,7 @@ void fxo_emf(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N
              int maxlevel) {
     for (int b = 0; b < nblock; b++) {
         const fxo_block* B = &blk[b];
-        int n = B->n, si = (n + 5) * (n + 5), sj = n + 5, sk = 1;
+        int n = B->n, si = SP(n) * SP(n), sj = SP(n), sk = 1;
 #pragma omp parallel for schedule(static)
         for (int i = 0; i <= n; i++)
             for (int j = 0; j <= n; j++)
@@ -797,7 +848,7 @@ void fxo_update(const fxo_params* P, int32_t nblock, const fxo_block* blk, int64
     if (stage == 0) dt[1] = dtv;
     for (int b = 0; b < nblock; b++) {
         const fxo_block* B = &blk[b];
-        int n = B->n, si = (n + 5) * (n + 5), sj = n + 5, sk = 1;
+        int n = B->n, si = SP(n) * SP(n), sj = SP(n), sk = 1;
         double idx = 1.0 / B->dx;
 #pragma omp parallel for schedule(static)
         for (int i = 0; i < n; i++)
@@ -837,7 +888,7 @@ void fxo_step(const fxo_params* P, int32_t nblock, const fxo_block* blk, const i
               int maxlevel) {
     for (int stage = 0; stage < 2; stage++) {
         fxo_prims(P, nblock, blk, nbr, N, U, U1, W, Bf, Bf1, F, dt, count, stage, stage == 0);
-        fxo_ghosts(nblock, blk, nbr, N, W, Bf, Bf1, stage, maxlevel);
+        fxo_ghosts(nblock, blk, nbr, N, W, Bf, Bf1, stage, maxlevel, P->limiter == LIM_PPM ? 3 : 2);
         fxo_fluxes(P, nblock, blk, N, W, Bf, Bf1, F, stage);
         fxo_emf(nblock, blk, nbr, N, F, E, maxlevel);
         fxo_update(P, nblock, blk, N, U, U1, W, Bf, Bf1, F, E, dt, stage);
@@ -848,7 +899,7 @@ void fxo_step(const fxo_params* P, int32_t nblock, const fxo_block* blk, const i
 void fxo_divb(int32_t nblock, const fxo_block* blk, int64_t N, const double* Bf, double* out) {
     for (int b = 0; b < nblock; b++) {
         const fxo_block* B = &blk[b];
-        int n = B->n, si = (n + 5) * (n + 5), sj = n + 5;
+        int n = B->n, si = SP(n) * SP(n), sj = SP(n);
         double mx = 0.0;
         for (int i = 0; i < n; i++)
             for (int j = 0; j < n; j++)
@@ -866,6 +917,15 @@ void fxo_divb(int32_t nblock, const fxo_block* blk, int64_t N, const double* Bf,
 }
 
 /* ---------------------------------------------- batch physics (tests) */
+/* face states of n faces from a[6][n] (cells p-3 .. p+2 of each face) */
+void fxo_ppm_batch(int64_t n, const double* a, double* L, double* R) {
+    for (int64_t t = 0; t < n; t++) {
+        double c[6];
+        for (int q = 0; q < 6; q++) c[q] = a[q * n + t];
+        ppm_face(c, &L[t], &R[t]);
+    }
+}
+
 void fxo_metric_batch(const fxo_params* P, int64_t n, const double* x, const double* y, const double* z,
                       double* out /* [n][22]: H, l[3], alpha, sqrtgam, beta[3], g[6], gi[6], r */) {
     for (int64_t q = 0; q < n; q++) {
@@ -1152,7 +1212,7 @@ void fxo_torus_init(const fxo_params* P, int32_t nblock, const fxo_block* blk, i
     }
     for (int b = 0; b < nblock; b++) {
         const fxo_block* B = &blk[b];
-        int n = B->n, si = (n + 5) * (n + 5), sj = n + 5;
+        int n = B->n, si = SP(n) * SP(n), sj = SP(n);
         for (int i = 0; i < n; i++)
             for (int j = 0; j < n; j++)
                 for (int k = 0; k < n; k++) {
@@ -1188,7 +1248,7 @@ void fxo_torus_init(const fxo_params* P, int32_t nblock, const fxo_block* blk, i
     }
     for (int b = 0; b < nblock; b++) {
         const fxo_block* B = &blk[b];
-        int n = B->n, si = (n + 5) * (n + 5), sj = n + 5;
+        int n = B->n, si = SP(n) * SP(n), sj = SP(n);
         for (int i = 0; i < n; i++)
             for (int j = 0; j < n; j++)
                 for (int k = 0; k < n; k++) {

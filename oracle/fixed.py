@@ -14,6 +14,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+GB = 3   # ghost layers of every block's box (bh_fixed.c GB)
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
 _lib = None
@@ -37,7 +38,7 @@ def lib():
         v, i32, i64, d = C.c_void_p, C.c_int32, C.c_int64, C.c_double
         L.fxo_step.argtypes = [P, i32, v, v, i64] + [v] * 9 + [C.c_int]
         L.fxo_prims.argtypes = [P, i32, v, v, i64] + [v] * 8 + [C.c_int, C.c_int]
-        L.fxo_ghosts.argtypes = [i32, v, v, i64, v, v, v, C.c_int, C.c_int]
+        L.fxo_ghosts.argtypes = [i32, v, v, i64, v, v, v, C.c_int, C.c_int, C.c_int]
         L.fxo_emf.argtypes = [i32, v, v, i64, v, v, C.c_int]
         L.fxo_fluxes.argtypes = [P, i32, v, i64, v, v, v, v, C.c_int]
         L.fxo_update.argtypes = [P, i32, v, i64, v, v, v, v, v, v, v, v, C.c_int]
@@ -46,6 +47,7 @@ def lib():
         L.fxo_deriv_batch.argtypes = [P, i64, v, v, v, v]
         L.fxo_cons_flux_batch.argtypes = [P, i64, v, v, v, C.c_int, v, v, v, v, v]
         L.fxo_hll_batch.argtypes = [P, i64, v, v, v, C.c_int, v, v, v]
+        L.fxo_ppm_batch.argtypes = [i64, v, v, v]
         L.fxo_source_batch.argtypes = [P, i64, v, v, v, v, v]
         L.fxo_c2p_batch.argtypes = [P, i64, v, v, v, v, v, v, v, v, v]
         L.fxo_fm_batch.argtypes = [d, d, d, d, d, i64, v, v, v, v]
@@ -64,8 +66,8 @@ def _p(a):
 
 def params(fx) -> FxoParams:
     """The oracle's parameter struct from a bhgpu.fixed.FxParams-like object
-    (any object with the same attributes; limiter 0/1/2 or its name)."""
-    lim = {"minmod": 0, "vanleer": 1, "mc": 2}.get(fx.limiter, fx.limiter)
+    (any object with the same attributes; limiter 0/1/2/3 or its name)."""
+    lim = {"minmod": 0, "vanleer": 1, "mc": 2, "ppm": 3}.get(fx.limiter, fx.limiter)
     r_exc = fx.r_exc
     if r_exc is None:
         r_exc = 1.2 * (fx.M + np.sqrt(fx.M * fx.M - fx.a * fx.a)) if fx.M > 0 else 0.0
@@ -80,7 +82,7 @@ class FxHost:
         self.blocks = np.ascontiguousarray(blocks)
         self.nbr = np.ascontiguousarray(nbr, np.int32)
         self.prm = prm
-        self.N = int(sum((int(n) + 5) ** 3 for n in blocks["n"]))
+        self.N = int(sum((int(n) + 2 * GB + 1) ** 3 for n in blocks["n"]))
         N = self.N
         self.U = np.zeros((8, N))
         self.U1 = np.zeros((8, N))
@@ -92,6 +94,11 @@ class FxHost:
         self.maxlevel = int(self.blocks["level"].max())
         self.dt = np.zeros(2)
         self.count = np.zeros(4, np.int32)
+
+    @property
+    def ghost_depth(self) -> int:
+        """ghost layers the fill covers: 3 for PPM's stencil, else 2"""
+        return 3 if self.prm.limiter == 3 else 2
 
     def _g(self):
         return (C.byref(self.prm), len(self.blocks), _p(self.blocks), _p(self.nbr), self.N)
@@ -106,7 +113,7 @@ class FxHost:
 
     def ghosts(self, stage=0):
         lib().fxo_ghosts(len(self.blocks), _p(self.blocks), _p(self.nbr), self.N, _p(self.W), _p(self.Bf),
-                         _p(self.Bf1), stage, self.maxlevel)
+                         _p(self.Bf1), stage, self.maxlevel, self.ghost_depth)
 
     def fluxes(self, stage=0):
         lib().fxo_fluxes(C.byref(self.prm), len(self.blocks), _p(self.blocks), self.N, _p(self.W), _p(self.Bf),
@@ -135,11 +142,11 @@ class FxHost:
 
     def interior(self, arr: np.ndarray) -> np.ndarray:
         n = int(self.blocks["n"][0])
-        S = n + 5
+        S = n + 2 * GB + 1
         out = []
         for b in self.blocks:
             box = arr[..., int(b["off"]):int(b["off"]) + S ** 3].reshape(arr.shape[:-1] + (S, S, S))
-            out.append(box[..., 2:2 + n, 2:2 + n, 2:2 + n])
+            out.append(box[..., GB:GB + n, GB:GB + n, GB:GB + n])
         return np.stack(out, axis=-4)
 
 
@@ -173,6 +180,15 @@ def hll(prm, x, y, z, dd, wL, wR):
     F = np.zeros((8, len(x)))
     lib().fxo_hll_batch(C.byref(prm), len(x), _p(x), _p(y), _p(z), dd, _p(wL), _p(wR), _p(F))
     return F
+
+
+def ppm(a):
+    """PPM face states (L, R) of the faces whose cells p-3 .. p+2 are a[6][n]"""
+    a = np.ascontiguousarray(a, np.float64)
+    n = a.shape[1]
+    L, R = np.zeros(n), np.zeros(n)
+    lib().fxo_ppm_batch(n, _p(a), _p(L), _p(R))
+    return L, R
 
 
 def source(prm, x, y, z, w):

@@ -26,7 +26,7 @@ import numpy as np
 import pytest
 
 from oracle import fixed as ofx
-from bhgrid.blocks import interior, uniform_blocks
+from bhgrid.blocks import GB, interior, uniform_blocks
 
 
 class Prm:
@@ -300,9 +300,9 @@ def _set_cells(h, fn):
     """W, U of every interior cell from fn(x, y, z) -> w[8]; face field from
     the cell values (uniform field only)"""
     for b in h.blocks:
-        n, S, off, dx = int(b["n"]), int(b["n"]) + 5, int(b["off"]), b["dx"]
-        idx = off + ((np.arange(n)[:, None, None] + 2) * S + (np.arange(n)[None, :, None] + 2)) * S + (
-            np.arange(n)[None, None, :] + 2)
+        n, S, off, dx = int(b["n"]), int(b["n"]) + 2 * GB + 1, int(b["off"]), b["dx"]
+        idx = off + ((np.arange(n)[:, None, None] + GB) * S + (np.arange(n)[None, :, None] + GB)) * S + (
+            np.arange(n)[None, None, :] + GB)
         c = (np.arange(n) + 0.5) * dx
         X = b["x0"][0] + c[:, None, None] + 0 * c[None, :, None] + 0 * c[None, None, :]
         Y = b["x0"][1] + 0 * c[:, None, None] + c[None, :, None] + 0 * c[None, None, :]
@@ -330,8 +330,8 @@ def test_uniform_state_preserved():
     assert h.divb() == 0.0
 
 
-def _sound_wave_error(N, gam=4.0 / 3.0, eps=1e-4, t_end=0.25):
-    prm = Prm(M=0.0, a=0.0, r_exc=-1.0, rho_floor=1e-12, u_floor=1e-14, cfl=0.3, limiter="mc")
+def _sound_wave_error(N, gam=4.0 / 3.0, eps=1e-4, t_end=0.25, limiter="mc"):
+    prm = Prm(M=0.0, a=0.0, r_exc=-1.0, rho_floor=1e-12, u_floor=1e-14, cfl=0.3, limiter=limiter)
     h = _flat_grid(N, 8, prm)
     rho0, p0 = 1.0, 0.6
     rhoh = rho0 + gam / (gam - 1) * p0
@@ -357,8 +357,8 @@ def _sound_wave_error(N, gam=4.0 / 3.0, eps=1e-4, t_end=0.25):
         n = int(b["n"])
         c = b["x0"][0] + (np.arange(n) + 0.5) * b["dx"]
         exact = wave(np.repeat(c, n * n), t)[1].reshape(n, n, n)
-        S = n + 5
-        box = h.W[1, int(b["off"]):int(b["off"]) + S ** 3].reshape(S, S, S)[2:2 + n, 2:2 + n, 2:2 + n]
+        S = n + 2 * GB + 1
+        box = h.W[1, int(b["off"]):int(b["off"]) + S ** 3].reshape(S, S, S)[GB:GB + n, GB:GB + n, GB:GB + n]
         err += np.abs(box - exact).sum()
     return err / N ** 3
 
@@ -379,3 +379,90 @@ def test_divergence_stays_at_roundoff_on_torus():
     assert h.divb() <= 1e-13
     assert h.count[0] == 0
     assert np.isfinite(interior(blocks, h.U)).all()
+
+
+# ---- PPM (Colella & Woodward 1984) ------------------------------------------
+def _ppm_numpy(a):
+    """CW84 eqs. 1.6-1.8 and 1.10 restated with numpy: the face between
+    cells a[2] and a[3] of a[0..5]"""
+    def dm(am, a0, ap):
+        dl, dr, da = a0 - am, ap - a0, 0.5 * (ap - am)
+        m = np.minimum(np.abs(da), 2.0 * np.minimum(np.abs(dl), np.abs(dr)))
+        return np.where(dl * dr > 0.0, np.sign(da) * m, 0.0)
+
+    d = [dm(a[q], a[q + 1], a[q + 2]) for q in range(4)]
+    f = [a[q + 1] + 0.5 * (a[q + 2] - a[q + 1]) - (d[q + 1] - d[q]) / 6.0 for q in range(3)]
+
+    def mono(c, l, r):
+        flat = (r - c) * (c - l) <= 0.0
+        dd, cc = r - l, c - 0.5 * (l + r)
+        l2 = np.where(dd * cc > dd * dd / 6.0, 3.0 * c - 2.0 * r, l)
+        r2 = np.where(-dd * dd / 6.0 > dd * cc, 3.0 * c - 2.0 * l, r)
+        return np.where(flat, c, l2), np.where(flat, c, r2)
+
+    _, L = mono(a[2], f[0], f[1])
+    R, _ = mono(a[3], f[1], f[2])
+    return L, R
+
+
+def test_ppm_faces_match_colella_woodward():
+    rng = np.random.default_rng(7)
+    n = 20000
+    a = rng.normal(size=(6, n))
+    a[:, :2000] = np.sort(a[:, :2000], axis=0)            # monotone stencils
+    a[:, 2000:3000] = np.linspace(0, 1, 6)[:, None] ** 2  # a smooth parabola
+    a[:, 3000:4000] = a[:, 3000:3001]                     # constant
+    L, R = ofx.ppm(a)
+    Ln, Rn = _ppm_numpy(a)
+    assert np.allclose(L, Ln, rtol=0, atol=1e-14) and np.allclose(R, Rn, rtol=0, atol=1e-14)
+    # face values stay between the two cells' values (positivity of rho, p)
+    lo, hi = np.minimum(a[2], a[3]), np.maximum(a[2], a[3])
+    lo1, hi1 = np.minimum(a[1], a[2]), np.maximum(a[1], a[2])
+    lo3, hi3 = np.minimum(a[3], a[4]), np.maximum(a[3], a[4])
+    assert (L >= np.minimum(lo, lo1) - 1e-15).all() and (L <= np.maximum(hi, hi1) + 1e-15).all()
+    assert (R >= np.minimum(lo, lo3) - 1e-15).all() and (R <= np.maximum(hi, hi3) + 1e-15).all()
+    # linear data: exact interface values
+    lin = np.arange(6, dtype=float)[:, None] * np.ones((1, 5))
+    L, R = ofx.ppm(lin)
+    assert np.allclose(L, 2.5) and np.allclose(R, 2.5)
+
+
+def test_ppm_sound_wave_second_order():
+    e16 = _sound_wave_error(16, limiter="ppm")
+    e32 = _sound_wave_error(32, limiter="ppm")
+    assert e32 < e16 / 3.5, (e16, e32)
+
+
+def _contact_error(N, limiter, v=0.5, t_end=0.4):
+    """L1 error of density after advecting a top-hat density jump (10:1, uniform
+    pressure and velocity) over a periodic flat box"""
+    prm = Prm(M=0.0, a=0.0, r_exc=-1.0, rho_floor=1e-12, u_floor=1e-14, cfl=0.3, limiter=limiter)
+    h = _flat_grid(N, 8, prm)
+    W = 1.0 / math.sqrt(1.0 - v * v)
+
+    def prof(X, t):
+        xs = (X - v * t) % 1.0
+        w = np.zeros((8, X.size))
+        w[0] = np.where((xs > 0.25) & (xs < 0.75), 10.0, 1.0)
+        w[1] = 1.0
+        w[2] = W * v
+        return w
+
+    _set_cells(h, lambda X, Y, Z: prof(X, 0.0))
+    t = 0.0
+    while t < t_end - 1e-12:
+        h.step()
+        t += h.dt[1]
+    rho = h.interior(h.W)[0]
+    err = 0.0
+    for q, b in enumerate(h.blocks):
+        n = int(b["n"])
+        c = b["x0"][0] + (np.arange(n) + 0.5) * b["dx"]
+        err += np.abs(rho[q] - prof(np.repeat(c, n * n), t)[0].reshape(n, n, n)).sum()
+    assert rho.min() > 0.99 and rho.max() < 10.01   # no new extrema
+    return err / N ** 3
+
+
+def test_ppm_keeps_a_contact_sharper_than_plm():
+    e = {lim: _contact_error(32, lim) for lim in ("minmod", "mc", "ppm")}
+    assert e["ppm"] < e["mc"] < e["minmod"], e

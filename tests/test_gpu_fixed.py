@@ -164,11 +164,11 @@ def test_mixed_torus_100_steps_128():
 
 
 # ---- blocks of several levels (equal cubes at 8^3, 16^3, 32^3 cells) ------
-def _leveled(precision="fp64", nb=8, r_fine=(14.0, 26.0), seed=3):
+def _leveled(precision="fp64", nb=8, r_fine=(14.0, 26.0), seed=3, **kw):
     from bhgpu.fixed import FxGrid, FxParams
     from bhgrid.blocks import torus_levels
     lv = torus_levels(nb=nb, r_fine=r_fine, seed=seed)
-    return FxGrid.leveled(-40.0, 40.0, lv, 8, FxParams(precision=precision))
+    return FxGrid.leveled(-40.0, 40.0, lv, 8, FxParams(precision=precision, **kw))
 
 
 def test_leveled_grid_has_three_levels():
@@ -331,3 +331,66 @@ def test_staged_equals_unstaged_on_blocks_of_three_sizes(precision, persistent):
         else:
             for v in range(x.shape[0]):
                 assert _rel_linf(x[v], y[v]) <= 1e-6, (name, v)
+
+
+def test_ppm_pieces_and_steps_bitwise():
+    """PPM (three ghost layers, the six-cell stencil) on 8 blocks of 16^3:
+    the ghost fill, the fluxes and two steps of the FP64 variant equal the
+    oracle bit for bit"""
+    g = _grid(32, 16, limiter="ppm")
+    assert g.ghost_depth == 3
+    g.torus_init()
+    h = _host(g)
+    _load(h, g)
+    g.prims(0, with_dt=True); h.prims(0, with_dt=True)
+    g.ghosts(0); h.ghosts(0)
+    torch.cuda.synchronize()
+    assert np.array_equal(g.W.cpu().numpy(), h.W)
+    g.fluxes(0); h.fluxes(0)
+    torch.cuda.synchronize()
+    assert np.array_equal(g.F.cpu().numpy(), h.F)
+    g.update(0); h.update(0)
+    g.prims(1); h.prims(1)
+    g.ghosts(1); h.ghosts(1)
+    g.fluxes(1); h.fluxes(1)
+    g.update(1); h.update(1)
+    for _ in range(2):
+        g.step()
+        h.step()
+    torch.cuda.synchronize()
+    for name in ("U", "Bf", "W"):
+        assert np.array_equal(g.interior(getattr(g, name)), h.interior(getattr(h, name))), name
+
+
+def test_ppm_leveled_steps_bitwise():
+    """PPM across levels: prolongation and restriction of the third ghost
+    layer, FP64 = oracle bit for bit"""
+    g = _leveled(limiter="ppm")
+    g.torus_init()
+    h = _host(g)
+    _load(h, g)
+    for _ in range(2):
+        g.step()
+        h.step()
+    torch.cuda.synchronize()
+    for name in ("U", "Bf", "W", "E"):
+        assert np.array_equal(getattr(g, name).cpu().numpy(), getattr(h, name)), name
+    assert g.divb() <= 1e-12
+
+
+def test_ppm_mixed_torus_within_1e_5_of_fp64():
+    """the mixed variant with PPM after 50 steps of the 64^3 torus: relative
+    L1 <= 1e-5 per conserved field against FP64 PPM"""
+    a = _grid(64, 64, "mixed", limiter="ppm")
+    b = _grid(64, 64, "fp64", limiter="ppm")
+    a.torus_init()
+    b.torus_init()
+    for _ in range(50):
+        a.step()
+        b.step()
+    torch.cuda.synchronize()
+    ua, ub = a.interior(a.U), b.interior(b.U)
+    assert np.isfinite(ua).all()
+    for name, vs in FIELDS.items():
+        assert _rel_l1(ua[vs], ub[vs]) <= 1e-5, name
+    assert a.counters()["c2p_failures"] == 0
