@@ -52,6 +52,9 @@ inline FxPar par_of(const bh_fx_params* p) {
     q.M = p->M; q.a = p->a; q.gamma = p->gamma;
     q.rho_fl = p->rho_floor; q.u_fl = p->u_floor; q.sigma_max = p->sigma_max; q.W_max = p->W_max;
     q.r_exc = p->r_exc; q.tol = p->tol; q.maxiter = p->maxiter; q.limiter = p->limiter;
+    q.gg = p->gamma / (p->gamma - 1.0);
+    q.gf = (p->gamma - 1.0) / p->gamma;
+    q.v2max = 1.0 - 1.0 / (p->W_max * p->W_max);
     return q;
 }
 
@@ -131,6 +134,30 @@ __global__ void k_fx_dt_init(double* dt) {
 // (U, Bf for stage 0; U1, Bf1 for stage 1); stage 0 also reduces the CFL
 // limit into dt[0]
 // ======================================================================
+// FP64 con2prim of cell c (metric m, cell field Bc) started from its previous
+// primitives; where it fails, the previous primitives with the new field
+// (counted).  Returns 1 if the conserved state must be rewritten.
+template <bool PRE32, typename WT>
+__device__ inline int c2p_cell64(const FxPar& P, const Grid& G, const KS& m, const double* U, const WT* W,
+                                 int64_t N, int64_t c, const double* Bc, double* w) {
+    C2PS cs;
+    double wo[5];
+    {
+        double u[5];
+        for (int v = 0; v < 5; v++) u[v] = U[v * N + c];
+        for (int v = 0; v < 5; v++) wo[v] = (double)W[v * N + c];
+        c2p_setup(P, m, u, Bc, wo, cs);
+    }
+    int iters = 0;
+    int st = c2p_solve<PRE32>(P, cs, iters);
+    if (st == 0) st = c2p_finish(m.gi, cs, Bc, w);
+    if (st == 0) return 0;
+    for (int v = 0; v < 5; v++) w[v] = wo[v];
+    for (int d = 0; d < 3; d++) w[P_B + d] = Bc[d];
+    atomicAdd(&G.count[0], 1);
+    return 1;
+}
+
 template <typename RT, typename WT, int MINB>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage, int with_dt, Queue Q) {
     for_items(Q, [&](int t) FX_INLINE {
@@ -147,8 +174,8 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
             const int64_t N = G.ncell;
             double x[3];
             cell_centre(B, i, j, k, x);
-            // the mixed variant beyond r ~ FX_R_FP64: geometry, floors and the
-            // floor rewrite in FP32; the Newton iterations in FP64 throughout
+            // the mixed variant beyond r ~ FX_R_FP64: geometry, con2prim,
+            // floors and the floor rewrite in FP32
             const bool g32 = fp32_geometry<RT>(x);
             // cell field: mean of the two faces (the role of f2cB, transport.cpp:60-75)
             const int si = bstride_i(B), sj = bstride_j(B);
@@ -156,48 +183,34 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
                                   0.5 * (Bf[2 * N + c] + Bf[2 * N + c + 1])};
             WT* W = (WT*)G.W;
             constexpr bool MIXED = sizeof(RT) < sizeof(double);
-            C2PS cs;
-            KS m;
-            cell_metric(P, x, g32, m);
-            {
-                const double isg = 1.0 / m.sqrtgam;
-                const double Bc[3] = {Bt[0] * isg, Bt[1] * isg, Bt[2] * isg};
-                double u[5], wo[5];
-                for (int v = 0; v < 5; v++) u[v] = U[v * N + c];
-                for (int v = 0; v < 5; v++) wo[v] = (double)W[v * N + c];
-                c2p_setup(P, m, u, Bc, wo, cs);
-            }
-            int iters = 0;
-            int st = c2p_solve<MIXED>(P, cs, iters);
-            KSb<float> mf;
-            if (MIXED) {
-                // the metric again (FP32 over most of the grid), so that it is
-                // not kept through the iterations; the opaque copy of the
-                // centre keeps the compiler from reusing the first
-                double xr[3] = {x[0], x[1], x[2]};
-                asm("" : "+d"(xr[0]), "+d"(xr[1]), "+d"(xr[2]));
-                if (g32) {
-                    ks_metric<float>(P, float(xr[0]), float(xr[1]), float(xr[2]), mf);
-                    copy_metric(mf, m);
-                } else {
-                    ks_metric(P, xr[0], xr[1], xr[2], m);
-                }
-            }
-            const double isg = 1.0 / m.sqrtgam;
-            const double Bc[3] = {Bt[0] * isg, Bt[1] * isg, Bt[2] * isg};
-            double w[8];
-            if (st == 0) st = c2p_finish(m.gi, cs, Bc, w);
+            const double dx[3] = {B.dx, B.dx, B.dx};
             int rewrite = 0;
-            if (st != 0) {
-                // keep the previous primitives with the new field
-                for (int v = 0; v < 5; v++) w[v] = (double)W[v * N + c];
-                for (int d = 0; d < 3; d++) w[P_B + d] = Bc[d];
-                atomicAdd(&G.count[0], 1);
-                rewrite = 1;
-            }
-            if (g32) {
+            if (MIXED && g32) {
+                // FP32 con2prim where its residual is well conditioned (the
+                // primitives are stored in FP32), FP64 where not
+                KSb<float> mf;
+                ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
+                const float Bcf[3] = {float(Bt[0]) * mf.alpha, float(Bt[1]) * mf.alpha, float(Bt[2]) * mf.alpha};
                 float wf[8];
-                for (int v = 0; v < 8; v++) wf[v] = float(w[v]);
+                int st;
+                {
+                    float u[5], wo[5];
+                    for (int v = 0; v < 5; v++) u[v] = float(U[v * N + c]);
+                    for (int v = 0; v < 5; v++) wo[v] = float(W[v * N + c]);
+                    C2PSb<float> cf;
+                    c2p_setup(P, mf, u, Bcf, wo, cf);
+                    int iters = 0;
+                    st = c2p_solve32(cf, iters);
+                    if (st == 0) st = c2p_finish(mf.gi, cf, Bcf, wf);
+                }
+                if (st != 0) {
+                    KS m;
+                    copy_metric(mf, m);
+                    const double Bc[3] = {Bt[0] * m.alpha, Bt[1] * m.alpha, Bt[2] * m.alpha};
+                    double w[8];
+                    rewrite = c2p_cell64<false>(P, G, m, U, W, N, c, Bc, w);
+                    for (int v = 0; v < 8; v++) wf[v] = float(w[v]);
+                }
                 if (apply_floors(P, mf, wf)) {
                     rewrite = 1;
                     atomicAdd(&G.count[1], 1);
@@ -207,12 +220,19 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
                     ks_cast(mf, mm);
                     Derived<float> d;
                     float uf[8];
-                    derive(mm, float(P.gamma), wf, d);
+                    derive(mm, float(P.gg), wf, d);
                     prim2cons(mm, float(P.gamma), wf, d, uf);
                     for (int v = 0; v < 5; v++) U[v * N + c] = (double)uf[v];
-                    for (int v = 0; v < 5; v++) w[v] = (double)wf[v];
                 }
+                for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
+                for (int v = 0; v < 8; v++) W[v * N + c] = (WT)wf[v];
+                if (with_dt) dtc = cell_dt<float>(P, mf, wf, dx);
             } else {
+                KS m;
+                ks_metric(P, x[0], x[1], x[2], m);
+                const double Bc[3] = {Bt[0] * m.alpha, Bt[1] * m.alpha, Bt[2] * m.alpha};   // B~ / sqrt(gamma)
+                double w[8];
+                rewrite = c2p_cell64<MIXED>(P, G, m, U, W, N, c, Bc, w);
                 if (apply_floors(P, m, w)) {
                     rewrite = 1;
                     atomicAdd(&G.count[1], 1);
@@ -222,16 +242,13 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
                     ks_cast(m, mm);
                     Derived<double> d;
                     double u[8];
-                    derive(mm, P.gamma, w, d);
+                    derive(mm, P.gg, w, d);
                     prim2cons(mm, P.gamma, w, d, u);
                     for (int v = 0; v < 5; v++) U[v * N + c] = u[v];
                 }
-            }
-            for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
-            for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];
-            if (with_dt) {
-                double dx[3] = {B.dx, B.dx, B.dx};
-                dtc = cell_dt<RT>(P, m, w, dx);
+                for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
+                for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];
+                if (with_dt) dtc = cell_dt<RT>(P, m, w, dx);
             }
         }
         if (with_dt) {
@@ -419,12 +436,34 @@ __device__ __forceinline__ void face_flux_at(const FxPar& P, const Grid& G, cons
                                              int d, const double* Bfs, const Sten& sten) {
     const int64_t N = G.ncell;
     const int64_t c = bidx(B, i, j, k);
-    double x[3];
-    cell_centre(B, i, j, k, x);
-    x[d] -= 0.5 * B.dx;
     KSm<RT> m;
-    face_geometry<RT>(P, x, m);
+    if (sizeof(RT) < sizeof(double)) {
+        // the face centre in FP32 (exact on these grids: binary spacings),
+        // FP64 only where the metric is evaluated in FP64
+        const float h = float(B.dx);
+        float xf[3] = {float(B.x0[0]) + (float(i) + 0.5f) * h, float(B.x0[1]) + (float(j) + 0.5f) * h,
+                       float(B.x0[2]) + (float(k) + 0.5f) * h};
+        xf[d] -= 0.5f * h;
+        if (xf[0] * xf[0] + xf[1] * xf[1] + xf[2] * xf[2] > float(FX_R_FP64 * FX_R_FP64)) {
+            KSb<float> mf;
+            ks_metric<float>(P, xf[0], xf[1], xf[2], mf);
+            ks_cast(mf, m);
+        } else {
+            double x[3];
+            cell_centre(B, i, j, k, x);
+            x[d] -= 0.5 * B.dx;
+            KS mk;
+            ks_metric(P, x[0], x[1], x[2], mk);
+            ks_cast(mk, m);
+        }
+    } else {
+        double x[3];
+        cell_centre(B, i, j, k, x);
+        x[d] -= 0.5 * B.dx;
+        face_geometry<RT>(P, x, m);
+    }
     RT wL[8], wR[8];
+#pragma unroll   // (wL, wR stay in registers only if every index is a constant)
     for (int v = 0; v < 8; v++) {
         if (v == P_B + d) continue;
         if (PPM6 && P.limiter == FX_PPM) {
@@ -436,11 +475,11 @@ __device__ __forceinline__ void face_flux_at(const FxPar& P, const Grid& G, cons
     }
     // (the limiters keep every face value between its two cells' values, so
     // face densities and pressures stay positive)
-    RT Bn = RT(Bfs[d * N + c]) / m.sqrtgam;
+    RT Bn = RT(Bfs[d * N + c]) * m.alpha;   // alpha = 1 / sqrt(gamma)
     wL[P_B + d] = Bn;
     wR[P_B + d] = Bn;
     RT F[8];
-    hll_face(m, RT(P.gamma), d, wL, wR, F);
+    hll_face(m, RT(P.gamma), RT(P.gg), d, wL, wR, F);
     FT* Fo = (FT*)G.F;
     for (int v = 0; v < 8; v++) Fo[((int64_t)d * 8 + v) * N + c] = (FT)F[v];
 }
@@ -570,24 +609,26 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux_tile(FxPar P, Grid G, 
 // Bf1 - dt curl E) / 2)
 // ======================================================================
 template <typename FT>
-__device__ inline double fget(const Grid& G, int d, int v, int64_t c) {
-    return (double)((const FT*)G.F)[((int64_t)d * 8 + v) * G.ncell + c];
+__device__ inline FT fget(const Grid& G, int d, int v, int64_t c) {
+    return ((const FT*)G.F)[((int64_t)d * 8 + v) * G.ncell + c];
 }
-// EMF components at the edges indexed like cell c
+// EMF components at the edges indexed like cell c, averaged in the flux
+// type (FP32 in the mixed variant: one conversion per edge, and every face
+// sharing the edge sees the same value, so div B stays at roundoff)
 template <typename FT>
 __device__ inline double emf_x(const Grid& G, int64_t c, int sj, int sk) {   // (i, j-1/2, k-1/2)
-    return 0.25 * (fget<FT>(G, 2, C_B + 1, c) + fget<FT>(G, 2, C_B + 1, c - sj) - fget<FT>(G, 1, C_B + 2, c) -
-                   fget<FT>(G, 1, C_B + 2, c - sk));
+    return (double)(FT(0.25) * (fget<FT>(G, 2, C_B + 1, c) + fget<FT>(G, 2, C_B + 1, c - sj) -
+                                fget<FT>(G, 1, C_B + 2, c) - fget<FT>(G, 1, C_B + 2, c - sk)));
 }
 template <typename FT>
 __device__ inline double emf_y(const Grid& G, int64_t c, int si, int sk) {   // (i-1/2, j, k-1/2)
-    return 0.25 * (fget<FT>(G, 0, C_B + 2, c) + fget<FT>(G, 0, C_B + 2, c - sk) - fget<FT>(G, 2, C_B + 0, c) -
-                   fget<FT>(G, 2, C_B + 0, c - si));
+    return (double)(FT(0.25) * (fget<FT>(G, 0, C_B + 2, c) + fget<FT>(G, 0, C_B + 2, c - sk) -
+                                fget<FT>(G, 2, C_B + 0, c) - fget<FT>(G, 2, C_B + 0, c - si)));
 }
 template <typename FT>
 __device__ inline double emf_z(const Grid& G, int64_t c, int si, int sj) {   // (i-1/2, j-1/2, k)
-    return 0.25 * (fget<FT>(G, 1, C_B + 0, c) + fget<FT>(G, 1, C_B + 0, c - si) - fget<FT>(G, 0, C_B + 1, c) -
-                   fget<FT>(G, 0, C_B + 1, c - sj));
+    return (double)(FT(0.25) * (fget<FT>(G, 1, C_B + 0, c) + fget<FT>(G, 1, C_B + 0, c - si) -
+                                fget<FT>(G, 0, C_B + 1, c) - fget<FT>(G, 0, C_B + 1, c - sj)));
 }
 template <typename FT>
 __device__ inline void face_update(const Grid& G, int d, int64_t c, int si, int sj, int sk, double idx, double dt,
@@ -709,12 +750,16 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, con
         RT w[8];
         for (int v = 0; v < 8; v++) w[v] = RT(W[v * N + c]);
         RT S[8];
-        source<RT>(mk, dk, RT(P.gamma), w, S);
+        source<RT>(mk, dk, RT(P.gg), w, S);
+        // the flux divergence in the flux type (the differences of
+        // neighbouring faces' values are exact in FP32 where they are within
+        // a factor of two of each other)
+        const FT idf = FT(idx);
         for (int v = 0; v < 5; v++) {
-            double div = (fget<FT>(G, 0, v, c + si) - fget<FT>(G, 0, v, c)) * idx +
-                         (fget<FT>(G, 1, v, c + sj) - fget<FT>(G, 1, v, c)) * idx +
-                         (fget<FT>(G, 2, v, c + sk) - fget<FT>(G, 2, v, c)) * idx;
-            double L = (double)S[v] - div;
+            FT div = (fget<FT>(G, 0, v, c + si) - fget<FT>(G, 0, v, c)) * idf +
+                     (fget<FT>(G, 1, v, c + sj) - fget<FT>(G, 1, v, c)) * idf +
+                     (fget<FT>(G, 2, v, c + sk) - fget<FT>(G, 2, v, c)) * idf;
+            double L = (double)S[v] - (double)div;
             if (stage == 0)
                 G.U1[v * N + c] = G.U[v * N + c] + dt * L;
             else
@@ -908,7 +953,7 @@ __global__ void __launch_bounds__(FX_TPB) k_fxi_pmag(FxPar P, Grid G, const int3
         KSm<double> m;
         ks_cast(mk, m);
         Derived<double> d;
-        derive(m, P.gamma, w, d);
+        derive(m, P.gg, w, d);
         pm = 0.5 * d.b2;
     }
     for (int o = 16; o > 0; o >>= 1) pm = fmax(pm, __shfl_xor_sync(0xffffffffu, pm, o));
@@ -956,7 +1001,7 @@ __global__ void __launch_bounds__(FX_TPB) k_fxi_cons(FxPar P, Grid G, const int3
     KSm<double> m;
     ks_cast(mk, m);
     Derived<double> d;
-    derive(m, P.gamma, w, d);
+    derive(m, P.gg, w, d);
     prim2cons(m, P.gamma, w, d, u);
     for (int v = 0; v < 5; v++) G.U[v * N + c] = u[v];
     for (int q = 0; q < 3; q++) G.U[(5 + q) * N + c] = Bt[q];

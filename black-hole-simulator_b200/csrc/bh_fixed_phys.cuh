@@ -46,6 +46,10 @@
 #ifndef BH_HD
 #define BH_HD __host__ __device__
 #endif
+// every function of the scheme is inlined into its kernel: an outlined call
+// would pass the small state arrays (face states, metric) through local
+// memory and lose the constant face direction
+#define BH_FI BH_HD __forceinline__
 
 namespace bhfx {
 
@@ -64,16 +68,18 @@ struct FxPar {
     double r_exc;             // cells with r < r_exc are reset to the floor state
     double tol;               // con2prim: |dZ| <= tol Z
     int maxiter, limiter;
+    // derived once per launch: Gamma/(Gamma-1), (Gamma-1)/Gamma, the v^2 of W_max
+    double gg, gf, v2max;
 };
 
 template <typename T>
-BH_HD inline T fmin_(T a, T b) { return b < a ? b : a; }
+BH_FI T fmin_(T a, T b) { return b < a ? b : a; }
 template <typename T>
-BH_HD inline T fmax_(T a, T b) { return a < b ? b : a; }
+BH_FI T fmax_(T a, T b) { return a < b ? b : a; }
 template <typename T>
-BH_HD inline T fabs_(T a) { return a < T(0) ? -a : a; }
-BH_HD inline double sqrt_(double x) { return sqrt(x); }
-BH_HD inline float sqrt_(float x) { return sqrtf(x); }
+BH_FI T fabs_(T a) { return a < T(0) ? -a : a; }
+BH_FI double sqrt_(double x) { return sqrt(x); }
+BH_FI float sqrt_(float x) { return sqrtf(x); }
 
 // ======================================================================
 // metric
@@ -81,7 +87,7 @@ BH_HD inline float sqrt_(float x) { return sqrtf(x); }
 // Kerr-Schild radius of a Cartesian point: the positive root of
 // r^4 - (R^2 - a^2) r^2 - a^2 z^2 = 0
 template <typename T>
-BH_HD inline T ks_r2(T a, T x, T y, T z) {
+BH_FI T ks_r2(T a, T x, T y, T z) {
     T a2 = a * a;
     T d = x * x + y * y + z * z - a2;
     return T(0.5) * (d + sqrt_(d * d + T(4) * a2 * z * z));
@@ -98,13 +104,13 @@ struct KSb {
     T r;
 };
 using KS = KSb<double>;
-BH_HD inline int sym(int i, int j) {   // index into the 6-entry symmetric storage
+BH_FI int sym(int i, int j) {   // index into the 6-entry symmetric storage
     int a = i < j ? i : j, b = i < j ? j : i;
     return a == 0 ? b : (a == 1 ? 2 + b : 5);
 }
 
 template <typename T>
-BH_HD inline void ks_metric(const FxPar& P, T x, T y, T z, KSb<T>& m) {
+BH_FI void ks_metric(const FxPar& P, T x, T y, T z, KSb<T>& m) {
     const T a = T(P.a), a2 = a * a;
     T r2 = ks_r2(a, x, y, z);
     T r = sqrt_(r2);
@@ -137,7 +143,7 @@ struct KSDb {
 };
 using KSD = KSDb<double>;
 template <typename T>
-BH_HD inline void ks_deriv(const FxPar& P, T x, T y, T z, const KSb<T>& m, KSDb<T>& d) {
+BH_FI void ks_deriv(const FxPar& P, T x, T y, T z, const KSb<T>& m, KSDb<T>& d) {
     const T a = T(P.a), a2 = a * a, r = m.r, r2 = r * r;
     T q = r2 * r2 + a2 * z * z;
     if (!(q > T(0)) || !(r > T(0))) {
@@ -166,13 +172,13 @@ struct KSm {
     RT alpha, sqrtgam, beta[3], g[6], gi[6];
 };
 template <typename RT, typename T>
-BH_HD inline void ks_cast(const KSb<T>& m, KSm<RT>& o) {
+BH_FI void ks_cast(const KSb<T>& m, KSm<RT>& o) {
     o.alpha = RT(m.alpha); o.sqrtgam = RT(m.sqrtgam);
     for (int i = 0; i < 3; i++) o.beta[i] = RT(m.beta[i]);
     for (int i = 0; i < 6; i++) { o.g[i] = RT(m.g[i]); o.gi[i] = RT(m.gi[i]); }
 }
 template <typename RT>
-BH_HD inline void lower(const RT* g, const RT* v, RT* o) {
+BH_FI void lower(const RT* g, const RT* v, RT* o) {
     o[0] = g[0] * v[0] + g[1] * v[1] + g[2] * v[2];
     o[1] = g[1] * v[0] + g[3] * v[1] + g[4] * v[2];
     o[2] = g[2] * v[0] + g[4] * v[1] + g[5] * v[2];
@@ -187,7 +193,8 @@ struct Derived {
     RT W, iW, rhoh, v[3], vl[3], Bl[3], B2, Bv, b2, rhohW2, ptot;
 };
 template <typename RT>
-BH_HD inline void derive(const KSm<RT>& m, RT gamma, const RT* w, Derived<RT>& d) {
+// gg = Gamma / (Gamma - 1)
+BH_FI void derive(const KSm<RT>& m, RT gg, const RT* w, Derived<RT>& d) {
     RT ut[3] = {w[P_UT], w[P_UT + 1], w[P_UT + 2]};
     RT B[3] = {w[P_B], w[P_B + 1], w[P_B + 2]};
     RT utl[3];
@@ -201,14 +208,14 @@ BH_HD inline void derive(const KSm<RT>& m, RT gamma, const RT* w, Derived<RT>& d
     d.B2 = d.Bl[0] * B[0] + d.Bl[1] * B[1] + d.Bl[2] * B[2];
     d.Bv = d.Bl[0] * d.v[0] + d.Bl[1] * d.v[1] + d.Bl[2] * d.v[2];
     d.b2 = d.B2 * iW * iW + d.Bv * d.Bv;
-    RT rhoh = w[P_RHO] + gamma / (gamma - RT(1)) * w[P_PRS];
+    RT rhoh = w[P_RHO] + gg * w[P_PRS];
     d.rhoh = rhoh;
     d.rhohW2 = rhoh * d.W * d.W;
     d.ptot = w[P_PRS] + RT(0.5) * d.b2;
 }
 // densitised conserved state of primitives w (B slots: sqrt(gamma) B)
 template <typename RT>
-BH_HD inline void prim2cons(const KSm<RT>& m, RT gamma, const RT* w, const Derived<RT>& d, RT* u) {
+BH_FI void prim2cons(const KSm<RT>& m, RT gamma, const RT* w, const Derived<RT>& d, RT* u) {
     const RT sg = m.sqrtgam;
     RT v2 = RT(1) - d.iW * d.iW;
     u[C_D] = sg * w[P_RHO] * d.W;
@@ -224,7 +231,7 @@ BH_HD inline void prim2cons(const KSm<RT>& m, RT gamma, const RT* w, const Deriv
 // sqrt(-g) = alpha sqrt(gamma))
 // ======================================================================
 template <typename RT>
-BH_HD inline void phys_flux(const KSm<RT>& m, int dd, const RT* w, const Derived<RT>& d, const RT* u, RT* F) {
+BH_FI void phys_flux(const KSm<RT>& m, int dd, const RT* w, const Derived<RT>& d, const RT* u, RT* F) {
     RT vt = m.alpha * d.v[dd] - m.beta[dd];       // coordinate transport velocity
     RT ag = m.alpha * m.sqrtgam;
     RT iW2 = d.iW * d.iW;
@@ -243,7 +250,7 @@ BH_HD inline void phys_flux(const KSm<RT>& m, int dd, const RT* w, const Derived
 
 // fast magnetosonic signal speeds lambda-, lambda+ in direction dd
 template <typename RT>
-BH_HD inline void signal_speeds(const KSm<RT>& m, RT gamma, int dd, const RT* w, const Derived<RT>& d, RT& lm,
+BH_FI void signal_speeds(const KSm<RT>& m, RT gamma, int dd, const RT* w, const Derived<RT>& d, RT& lm,
                                 RT& lp) {
     RT rhoh = d.rhoh;
     // c_s^2 + v_A^2 - c_s^2 v_A^2 with c_s^2 = Gamma p / (rho h), v_A^2 = b^2 / (rho h + b^2)
@@ -265,7 +272,7 @@ BH_HD inline void signal_speeds(const KSm<RT>& m, RT gamma, int dd, const RT* w,
 // ======================================================================
 enum { FX_MINMOD = 0, FX_VANLEER = 1, FX_MC = 2, FX_PPM = 3 };
 template <typename RT>
-BH_HD inline RT lim_slope(RT dl, RT dr, int lim) {
+BH_FI RT lim_slope(RT dl, RT dr, int lim) {
     if (dl * dr <= RT(0)) return RT(0);
     if (lim == FX_VANLEER) return RT(2) * dl * dr / (dl + dr);
     RT al = fabs_(dl), ar = fabs_(dr);
@@ -278,7 +285,7 @@ BH_HD inline RT lim_slope(RT dl, RT dr, int lim) {
 }
 // face values at i-1/2 from cells i-2, i-1 (left) and i-1, i (right)
 template <typename RT>
-BH_HD inline void plm_face(RT wmm, RT wm, RT wp, RT wpp, int lim, RT& L, RT& R) {
+BH_FI void plm_face(RT wmm, RT wm, RT wp, RT wpp, int lim, RT& L, RT& R) {
     L = wm + RT(0.5) * lim_slope(wm - wmm, wp - wm, lim);
     R = wp - RT(0.5) * lim_slope(wp - wm, wpp - wp, lim);
 }
@@ -293,7 +300,7 @@ BH_HD inline void plm_face(RT wmm, RT wm, RT wp, RT wpp, int lim, RT& L, RT& R) 
 // so face densities and pressures stay positive as with PLM.
 // ======================================================================
 template <typename RT>
-BH_HD inline RT ppm_dm(RT am, RT a0, RT ap) {
+BH_FI RT ppm_dm(RT am, RT a0, RT ap) {
     RT dl = a0 - am, dr = ap - a0;
     if (dl * dr <= RT(0)) return RT(0);
     RT da = RT(0.5) * (ap - am);
@@ -301,7 +308,7 @@ BH_HD inline RT ppm_dm(RT am, RT a0, RT ap) {
     return da > RT(0) ? m : -m;
 }
 template <typename RT>
-BH_HD inline void ppm_parabola(RT a, RT& l, RT& r) {
+BH_FI void ppm_parabola(RT a, RT& l, RT& r) {
     if ((r - a) * (a - l) <= RT(0)) {
         l = a;
         r = a;
@@ -314,7 +321,7 @@ BH_HD inline void ppm_parabola(RT a, RT& l, RT& r) {
     }
 }
 template <typename RT>
-BH_HD inline void ppm_face(const RT* a, RT& L, RT& R) {
+BH_FI void ppm_face(const RT* a, RT& L, RT& R) {
     RT dm[4];
     for (int q = 0; q < 4; q++) dm[q] = ppm_dm(a[q], a[q + 1], a[q + 2]);
     RT f[3];
@@ -333,10 +340,10 @@ BH_HD inline void ppm_face(const RT* a, RT& L, RT& R) {
 // signal speed magnitude.
 // ======================================================================
 template <typename RT>
-BH_HD inline RT hll_face(const KSm<RT>& m, RT gamma, int dd, const RT* wL, const RT* wR, RT* F) {
+BH_FI RT hll_face(const KSm<RT>& m, RT gamma, RT gg, int dd, const RT* wL, const RT* wR, RT* F) {
     Derived<RT> dL, dR;
-    derive(m, gamma, wL, dL);
-    derive(m, gamma, wR, dR);
+    derive(m, gg, wL, dL);
+    derive(m, gg, wR, dR);
     RT uL[8], uR[8], FL[8], FR[8];
     prim2cons(m, gamma, wL, dL, uL);
     prim2cons(m, gamma, wR, dR, uR);
@@ -362,11 +369,11 @@ BH_HD inline RT hll_face(const KSm<RT>& m, RT gamma, int dd, const RT* wL, const
 // geometric source of a cell (densitised: sqrt(-g) S = S here)
 // ======================================================================
 template <typename RT, typename MT>
-BH_HD inline void source(const KSb<MT>& mk, const KSDb<MT>& dk, RT gamma, const RT* w, RT* S) {
+BH_FI void source(const KSb<MT>& mk, const KSDb<MT>& dk, RT gg, const RT* w, RT* S) {
     KSm<RT> m;
     ks_cast(mk, m);
     Derived<RT> d;
-    derive(m, gamma, w, d);
+    derive(m, gg, w, d);
     const RT H = RT(mk.H);
     RT l[4] = {RT(1), RT(mk.l[0]), RT(mk.l[1]), RT(mk.l[2])};
     // four-velocity and magnetic four-vector
@@ -427,7 +434,7 @@ BH_HD inline void source(const KSb<MT>& mk, const KSDb<MT>& dk, RT gamma, const 
 // configuration asks: rho_fl r^-3/2, u_fl r^-5/2), evaluated at max(r, 1)
 // ======================================================================
 template <typename T>
-BH_HD inline void floor_state(const FxPar& P, T r, T& rho, T& p) {
+BH_FI void floor_state(const FxPar& P, T r, T& rho, T& p) {
     T re = r > T(1) ? r : T(1);
     T s = sqrt_(re);
     T ir = T(1) / (re * re * s);          // r^-5/2
@@ -457,7 +464,7 @@ struct C2Pb {
 using C2P = C2Pb<double>;
 // residual f(Z) and its derivative; v2 is clamped to v2max (clamped = 1)
 template <typename T>
-BH_HD inline void c2p_eval(const C2Pb<T>& q, T Z, T& f, T& df, T& v2, int& clamped) {
+BH_FI void c2p_eval(const C2Pb<T>& q, T Z, T& f, T& df, T& v2, int& clamped) {
     T iZ = T(1) / Z, ZB = Z + q.B2, iZB = T(1) / ZB;
     T iZB2 = iZB * iZB, iZ2 = iZ * iZ;
     v2 = q.S2 * iZB2 + q.SB2 * (q.B2 + T(2) * Z) * iZ2 * iZB2;
@@ -480,20 +487,21 @@ BH_HD inline void c2p_eval(const C2Pb<T>& q, T Z, T& f, T& df, T& v2, int& clamp
 // The solver in three parts -- setup (the metric's invariants into q),
 // solve (q and Z alone), finish (raise v with gamma^ij) -- so that a caller
 // can let the metric go while it iterates.
-struct C2PS {
-    C2P q;
-    double S[3], Bl[3], SB, Z;
+template <typename T>
+struct C2PSb {
+    C2Pb<T> q;
+    T S[3], Bl[3], SB, Z;
 };
-BH_HD inline void c2p_setup(const FxPar& P, const KS& m, const double* U, const double* B, const double* wo,
-                            C2PS& s) {
-    const double gm = P.gamma;
-    const double isg = 1.0 / m.sqrtgam;
-    C2P& q = s.q;
-    q.gf = (gm - 1.0) / gm;
+using C2PS = C2PSb<double>;
+template <typename T>
+BH_FI void c2p_setup(const FxPar& P, const KSb<T>& m, const T* U, const T* B, const T* wo, C2PSb<T>& s) {
+    const T isg = m.alpha;   // 1 / sqrt(gamma)
+    C2Pb<T>& q = s.q;
+    q.gf = T(P.gf);
     q.D = U[C_D] * isg;
-    double tau = U[C_TAU] * isg;
+    T tau = U[C_TAU] * isg;
     for (int i = 0; i < 3; i++) s.S[i] = U[C_S + i] * isg;
-    double Su[3];
+    T Su[3];
     lower(m.gi, s.S, Su);   // S^i = gamma^ij S_j
     lower(m.g, B, s.Bl);
     q.S2 = Su[0] * s.S[0] + Su[1] * s.S[1] + Su[2] * s.S[2];
@@ -502,18 +510,44 @@ BH_HD inline void c2p_setup(const FxPar& P, const KS& m, const double* U, const 
     q.SB2 = s.SB * s.SB;
     q.B4 = q.B2 * q.B2;
     q.E = tau + q.D;
-    q.v2max = 1.0 - 1.0 / (P.W_max * P.W_max);
+    q.v2max = T(P.v2max);
     // initial guess from the previous primitives
-    double uto[3] = {wo[P_UT], wo[P_UT + 1], wo[P_UT + 2]}, utl[3];
+    T uto[3] = {wo[P_UT], wo[P_UT + 1], wo[P_UT + 2]}, utl[3];
     lower(m.g, uto, utl);
-    double W2o = 1.0 + utl[0] * uto[0] + utl[1] * uto[1] + utl[2] * uto[2];
-    double Z = (wo[P_RHO] + gm / (gm - 1.0) * wo[P_PRS]) * W2o;
-    if (!(Z > 0.0) || !(Z < 1e300)) Z = q.E > q.D ? q.E : q.D;
+    T W2o = T(1) + utl[0] * uto[0] + utl[1] * uto[1] + utl[2] * uto[2];
+    T Z = (wo[P_RHO] + T(P.gg) * wo[P_PRS]) * W2o;
+    if (!(Z > T(0)) || !(Z < T(sizeof(T) < sizeof(double) ? 1e30 : 1e300))) Z = q.E > q.D ? q.E : q.D;
     s.Z = Z;
+}
+// FP32 con2prim (the mixed variant away from the hole): up to six Newton
+// iterations on the FP32 residual.  Returns 0 when they converge (|dZ| <=
+// 1e-6 Z) on a well-conditioned residual -- its rounding error, 2^-24 times
+// its largest term (E, B^2, (S.B)^2 / Z^2), moves the root by at most
+// 2^-24 * 16 Z / f'(Z), f' >= 1/2 -- else 1 (the caller solves in FP64).
+BH_FI int c2p_solve32(C2PSb<float>& s, int& iters) {
+    const C2Pb<float>& q = s.q;
+    float Z = s.Z, f, df, v2;
+    int cl = 0;
+    for (int it = 0; it < 6; it++) {
+        c2p_eval(q, Z, f, df, v2, cl);
+        if (cl || !(df >= 0.5f)) { iters = it + 1; return 1; }
+        float Zn = Z - f / df;
+        if (!(Zn > 0.0f)) { iters = it + 1; return 1; }
+        float e = fabs_(Zn - Z);
+        Z = Zn;
+        if (e <= 1e-6f * Z) {
+            iters = it + 1;
+            s.Z = Z;
+            float iz = 1.0f / Z;
+            return q.E + q.B2 + q.SB2 * iz * iz <= 16.0f * Z ? 0 : 1;
+        }
+    }
+    iters = 6;
+    return 1;
 }
 // returns 0 with s.Z the root, 1 if it was not found
 template <bool PRE32 = false>
-BH_HD inline int c2p_solve(const FxPar& P, C2PS& s, int& iters) {
+BH_FI int c2p_solve(const FxPar& P, C2PS& s, int& iters) {
     const C2P& q = s.q;
     double Z = s.Z;
     int it = 0, ok = 0, it32 = 0;
@@ -594,28 +628,29 @@ BH_HD inline int c2p_solve(const FxPar& P, C2PS& s, int& iters) {
     return ok ? 0 : 1;
 }
 // the primitives at the root; returns 0, or 2 if the state is unphysical
-BH_HD inline int c2p_finish(const double* gi, const C2PS& s, const double* B, double* w) {
-    const C2P& q = s.q;
-    const double Z = s.Z;
-    double iZ = 1.0 / Z, ZB = Z + q.B2, iZB = 1.0 / ZB;
-    double v2 = q.S2 * iZB * iZB + q.SB2 * (q.B2 + 2.0 * Z) * iZ * iZ * iZB * iZB;
+template <typename T>
+BH_FI int c2p_finish(const T* gi, const C2PSb<T>& s, const T* B, T* w) {
+    const C2Pb<T>& q = s.q;
+    const T Z = s.Z;
+    T iZ = T(1) / Z, ZB = Z + q.B2, iZB = T(1) / ZB;
+    T v2 = q.S2 * iZB * iZB + q.SB2 * (q.B2 + T(2) * Z) * iZ * iZ * iZB * iZB;
     if (!(v2 < q.v2max)) v2 = q.v2max;
-    double W2i = 1.0 - v2, Wi = sqrt(W2i);
-    double Wl = 1.0 / Wi;
-    double rho = q.D * Wi;
-    double p = q.gf * (Z * W2i - rho);
+    T W2i = T(1) - v2, Wi = sqrt_(W2i);
+    T Wl = T(1) / Wi;
+    T rho = q.D * Wi;
+    T p = q.gf * (Z * W2i - rho);
     // v_i = (S_i + (S.B / Z) B_i) / (Z + B^2), raised with gamma^ij
-    double vl[3], vu[3];
+    T vl[3], vu[3];
     for (int i = 0; i < 3; i++) vl[i] = (s.S[i] + s.SB * iZ * s.Bl[i]) * iZB;
     lower(gi, vl, vu);
     w[P_RHO] = rho;
     w[P_PRS] = p;
     for (int i = 0; i < 3; i++) { w[P_UT + i] = Wl * vu[i]; w[P_B + i] = B[i]; }
-    if (!(rho > 0.0) || !(p == p) || !(Wl == Wl)) return 2;
+    if (!(rho > T(0)) || !(p == p) || !(Wl == Wl)) return 2;
     return 0;
 }
 template <bool PRE32 = false>
-BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const double* B, const double* wo,
+BH_FI int con2prim(const FxPar& P, const KS& m, const double* U, const double* B, const double* wo,
                           double* w, int& iters) {
     C2PS s;
     c2p_setup(P, m, U, B, wo, s);
@@ -628,7 +663,7 @@ BH_HD inline int con2prim(const FxPar& P, const KS& m, const double* U, const do
 // (the caller then rewrites U = prim2cons(w))
 // ======================================================================
 template <typename T>
-BH_HD inline int apply_floors(const FxPar& P, const KSb<T>& m, T* w) {
+BH_FI int apply_floors(const FxPar& P, const KSb<T>& m, T* w) {
     T rf, pf;
     floor_state(P, m.r, rf, pf);
     int changed = 0;
@@ -666,23 +701,13 @@ BH_HD inline int apply_floors(const FxPar& P, const KSb<T>& m, T* w) {
 // CFL limit of a cell: the smallest dx_d / max|lambda_d|
 // ======================================================================
 template <typename A, typename B>
-BH_HD inline void copy_metric(const KSb<A>& m, KSb<B>& mo) {
+BH_FI void copy_metric(const KSb<A>& m, KSb<B>& mo) {
     mo.H = B(m.H); mo.alpha = B(m.alpha); mo.sqrtgam = B(m.sqrtgam); mo.r = B(m.r);
     for (int i = 0; i < 3; i++) { mo.l[i] = B(m.l[i]); mo.beta[i] = B(m.beta[i]); }
     for (int i = 0; i < 6; i++) { mo.g[i] = B(m.g[i]); mo.gi[i] = B(m.gi[i]); }
 }
-// the cell-centre metric in FP64; from the FP32 metric where g32
-BH_HD inline void cell_metric(const FxPar& P, const double* x, bool g32, KS& m) {
-    if (g32) {
-        KSb<float> mf;
-        ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
-        copy_metric(mf, m);
-    } else {
-        ks_metric(P, x[0], x[1], x[2], m);
-    }
-}
 template <typename A, typename B>
-BH_HD inline void copy_geometry(const KSb<A>& m, const KSDb<A>& d, KSb<B>& mo, KSDb<B>& dout) {
+BH_FI void copy_geometry(const KSb<A>& m, const KSDb<A>& d, KSb<B>& mo, KSDb<B>& dout) {
     mo.H = B(m.H); mo.alpha = B(m.alpha); mo.sqrtgam = B(m.sqrtgam); mo.r = B(m.r);
     for (int i = 0; i < 3; i++) { mo.l[i] = B(m.l[i]); mo.beta[i] = B(m.beta[i]); dout.dH[i] = B(d.dH[i]); }
     for (int i = 0; i < 6; i++) { mo.g[i] = B(m.g[i]); mo.gi[i] = B(m.gi[i]); }
@@ -690,14 +715,14 @@ BH_HD inline void copy_geometry(const KSb<A>& m, const KSDb<A>& d, KSb<B>& mo, K
         for (int i = 0; i < 3; i++) dout.dl[k][i] = B(d.dl[k][i]);
 }
 
-template <typename RT = double>
-BH_HD inline double cell_dt(const FxPar& P, const KS& mk, const double* w64, const double* dx) {
+template <typename RT = double, typename MT = double, typename WT = double>
+BH_FI double cell_dt(const FxPar& P, const KSb<MT>& mk, const WT* w64, const double* dx) {
     KSm<RT> m;
     ks_cast(mk, m);
     RT w[8];
     for (int v = 0; v < 8; v++) w[v] = RT(w64[v]);
     Derived<RT> d;
-    derive(m, RT(P.gamma), w, d);
+    derive(m, RT(P.gg), w, d);
     double best = 1e300;
     for (int dd = 0; dd < 3; dd++) {
         RT lm, lp;
@@ -717,13 +742,13 @@ BH_HD inline double cell_dt(const FxPar& P, const KS& mk, const double* w64, con
 // ======================================================================
 constexpr double FX_R_FP64 = 4.0;
 template <typename RT>
-BH_HD inline bool fp32_geometry(const double* x) {
+BH_FI bool fp32_geometry(const double* x) {
     if (sizeof(RT) == sizeof(double)) return false;
     return x[0] * x[0] + x[1] * x[1] + x[2] * x[2] > FX_R_FP64 * FX_R_FP64;
 }
 // spatial metric at a face centre
 template <typename RT>
-BH_HD inline void face_geometry(const FxPar& P, const double* x, KSm<RT>& m) {
+BH_FI void face_geometry(const FxPar& P, const double* x, KSm<RT>& m) {
     if (fp32_geometry<RT>(x)) {
         KSb<float> mf;
         ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
@@ -736,7 +761,7 @@ BH_HD inline void face_geometry(const FxPar& P, const double* x, KSm<RT>& m) {
 }
 // metric and derivatives at a cell centre, in RT
 template <typename RT>
-BH_HD inline void cell_geometry(const FxPar& P, const double* x, KSb<RT>& m, KSDb<RT>& d) {
+BH_FI void cell_geometry(const FxPar& P, const double* x, KSb<RT>& m, KSDb<RT>& d) {
     if (fp32_geometry<RT>(x)) {
         KSb<float> mf;
         KSDb<float> df;
@@ -759,14 +784,14 @@ BH_HD inline void cell_geometry(const FxPar& P, const double* x, KSb<RT>& m, KSD
 // ======================================================================
 // u^t u_phi of the prograde circular equatorial orbit at r (M = 1 units):
 // the torus's conserved angular momentum when its pressure peaks at r
-BH_HD inline double fm_ell(double a, double r) {
+BH_FI double fm_ell(double a, double r) {
     double sr = sqrt(r), r32 = r * sr;
     return (r * r - 2.0 * a * sr + a * a) * (r32 + a) / (r32 * (r32 - 3.0 * sr + 2.0 * a));
 }
 struct FMPoint {
     double Sig, Del, A, e2;   // Sigma, Delta, A and e^{2 nu - 2 psi} = Sigma^2 Delta / (A^2 sin^2)
 };
-BH_HD inline FMPoint fm_point(double a, double r, double s2, double c2) {
+BH_FI FMPoint fm_point(double a, double r, double s2, double c2) {
     FMPoint f;
     f.Sig = r * r + a * a * c2;
     f.Del = r * r - 2.0 * r + a * a;
@@ -776,7 +801,7 @@ BH_HD inline FMPoint fm_point(double a, double r, double s2, double c2) {
     return f;
 }
 // the FM enthalpy potential W(r, theta); ln h = W(r, theta) - W(r_in, pi/2)
-BH_HD inline double fm_potential(double a, double ell, double r, double s2, double c2) {
+BH_FI double fm_potential(double a, double ell, double r, double s2, double c2) {
     FMPoint f = fm_point(a, r, s2, c2);
     double X = sqrt(1.0 + 4.0 * ell * ell * f.e2);
     return 0.5 * log((1.0 + X) * f.A / (f.Sig * f.Del)) - 0.5 * X - 2.0 * a * r * ell / f.A;
@@ -784,7 +809,7 @@ BH_HD inline double fm_potential(double a, double ell, double r, double s2, doub
 struct FMTorus {
     double a, gamma, kappa, r_in, ell, w_in;
 };
-BH_HD inline FMTorus fm_torus(double a, double gamma, double kappa, double r_in, double r_max) {
+BH_FI FMTorus fm_torus(double a, double gamma, double kappa, double r_in, double r_max) {
     FMTorus t;
     t.a = a; t.gamma = gamma; t.kappa = kappa; t.r_in = r_in;
     t.ell = fm_ell(a, r_max);
@@ -792,7 +817,7 @@ BH_HD inline FMTorus fm_torus(double a, double gamma, double kappa, double r_in,
     return t;
 }
 // density (before normalisation) at a Cartesian KS point; 0 outside the torus
-BH_HD inline double fm_rho(const FMTorus& t, double x, double y, double z, double* lnh_out) {
+BH_FI double fm_rho(const FMTorus& t, double x, double y, double z, double* lnh_out) {
     double r = sqrt(ks_r2(t.a, x, y, z));
     if (!(r >= t.r_in)) return 0.0;
     double c = z / r, c2 = c * c, s2 = 1.0 - c2;
@@ -805,7 +830,7 @@ BH_HD inline double fm_rho(const FMTorus& t, double x, double y, double z, doubl
 }
 // four-velocity of the torus at a Cartesian KS point inside it:
 // u^t and the Cartesian u^x, u^y (u^r = u^theta = 0, u^z = 0)
-BH_HD inline void fm_velocity(const FMTorus& t, double x, double y, double z, double& ut, double& ux, double& uy) {
+BH_FI void fm_velocity(const FMTorus& t, double x, double y, double z, double& ut, double& ux, double& uy) {
     const double a = t.a;
     double r = sqrt(ks_r2(a, x, y, z));
     double c = z / r, c2 = c * c, s2 = 1.0 - c2;
@@ -821,13 +846,13 @@ BH_HD inline void fm_velocity(const FMTorus& t, double x, double y, double z, do
 // key of a cell from its global integer coordinates (x / dx - 1/2 rounded),
 // so that the seeded perturbation does not depend on how the grid is cut
 // into blocks; 21 bits per axis
-BH_HD inline uint64_t cell_key(const double* x0, double dx, int i, int j, int k) {
+BH_FI uint64_t cell_key(const double* x0, double dx, int i, int j, int k) {
     const int64_t off = 1 << 20;
     int64_t g0 = llround(x0[0] / dx) + i + off, g1 = llround(x0[1] / dx) + j + off, g2 = llround(x0[2] / dx) + k + off;
     return ((uint64_t)g0 << 42) | ((uint64_t)g1 << 21) | (uint64_t)g2;
 }
 // uniform deviate in [0, 1) from a 64-bit counter hash (SplitMix64 finaliser)
-BH_HD inline double hash_uniform(uint64_t seed, uint64_t id) {
+BH_FI double hash_uniform(uint64_t seed, uint64_t id) {
     uint64_t z = seed * 0x100000001B3ULL + id + 0x9E3779B97F4A7C15ULL;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;

@@ -735,7 +735,7 @@ static void face(const fxo_params* P, const fxo_block* B, int64_t N, const doubl
         wL[v] = b + 0.5 * slope(b - a, cc - b, P->limiter);
         wR[v] = cc - 0.5 * slope(cc - b, dd - cc, P->limiter);
     }
-    double Bn = Bfs[d * N + c] / m.sqrtgam;
+    double Bn = Bfs[d * N + c] * m.alpha; /* alpha = 1 / sqrt(gamma) */
     wL[BB + d] = Bn;
     wR[BB + d] = Bn;
     double Fo[8];
