@@ -220,7 +220,7 @@ class FxGrid:
 
     def counters(self) -> dict:
         c = self.count.cpu().numpy()
-        return {"c2p_failures": int(c[0]), "floored": int(c[1])}
+        return {"c2p_failures": int(c[0]), "floored": int(c[1]), "c2p_fp64_fallback": int(c[2])}
 
     def reset_counters(self):
         self.count.zero_()

@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
                     if (st == 0) st = c2p_finish(mf.gi, cf, Bcf, wf);
                 }
                 if (st != 0) {
+                    atomicAdd(&G.count[2], 1);
                     KS m;
                     copy_metric(mf, m);
                     const double Bc[3] = {Bt[0] * m.alpha, Bt[1] * m.alpha, Bt[2] * m.alpha};
@@ -610,7 +611,7 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux_tile(FxPar P, Grid G, 
 // ======================================================================
 template <typename FT>
 __device__ inline FT fget(const Grid& G, int d, int v, int64_t c) {
-    return ((const FT*)G.F)[((int64_t)d * 8 + v) * G.ncell + c];
+    return __ldg((const FT*)G.F + ((int64_t)d * 8 + v) * G.ncell + c);   // read-only in the update
 }
 // EMF components at the edges indexed like cell c, averaged in the flux
 // type (FP32 in the mixed variant: one conversion per edge, and every face
@@ -765,10 +766,30 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, con
             else
                 G.U[v * N + c] = 0.5 * (G.U[v * N + c] + G.U1[v * N + c] + dt * L);
         }
-        // face field: this cell's three lower faces, and the upper boundary faces
-        face_update<FT>(G, 0, c, si, sj, sk, idx, dt, stage);
-        face_update<FT>(G, 1, c, si, sj, sk, idx, dt, stage);
-        face_update<FT>(G, 2, c, si, sj, sk, idx, dt, stage);
+        // the nine distinct edge EMFs of the cell's three lower faces: ex at
+        // the edges of c, c+sj, c+sk; ey at c, c+si, c+sk; ez at c, c+si, c+sj
+        double ex[3], ey[3], ez[3];
+        if (G.E) {   // the edge EMFs of the grid (corrected at level changes)
+            const double *Ex = G.E, *Ey = G.E + N, *Ez = G.E + 2 * N;
+            ex[0] = Ex[c]; ex[1] = Ex[c + sj]; ex[2] = Ex[c + sk];
+            ey[0] = Ey[c]; ey[1] = Ey[c + si]; ey[2] = Ey[c + sk];
+            ez[0] = Ez[c]; ez[1] = Ez[c + si]; ez[2] = Ez[c + sj];
+        } else {
+            ex[0] = emf_x<FT>(G, c, sj, sk); ex[1] = emf_x<FT>(G, c + sj, sj, sk); ex[2] = emf_x<FT>(G, c + sk, sj, sk);
+            ey[0] = emf_y<FT>(G, c, si, sk); ey[1] = emf_y<FT>(G, c + si, si, sk); ey[2] = emf_y<FT>(G, c + sk, si, sk);
+            ez[0] = emf_z<FT>(G, c, si, sj); ez[1] = emf_z<FT>(G, c + si, si, sj); ez[2] = emf_z<FT>(G, c + sj, si, sj);
+        }
+        // face field: this cell's three lower faces (curl E as in face_update),
+        // and the upper boundary faces
+        const double curl[3] = {(ez[2] - ez[0]) * idx - (ey[2] - ey[0]) * idx,
+                                (ex[2] - ex[0]) * idx - (ez[1] - ez[0]) * idx,
+                                (ey[1] - ey[0]) * idx - (ex[1] - ex[0]) * idx};
+        for (int d = 0; d < 3; d++) {
+            if (stage == 0)
+                G.Bf1[d * N + c] = G.Bf[d * N + c] - dt * curl[d];
+            else
+                G.Bf[d * N + c] = 0.5 * (G.Bf[d * N + c] + G.Bf1[d * N + c] - dt * curl[d]);
+        }
         if (i == n - 1) face_update<FT>(G, 0, c + si, si, sj, sk, idx, dt, stage);
         if (j == n - 1) face_update<FT>(G, 1, c + sj, si, sj, sk, idx, dt, stage);
         if (k == n - 1) face_update<FT>(G, 2, c + sk, si, sj, sk, idx, dt, stage);

@@ -434,7 +434,9 @@ typedef struct bh_fx_grid {
     void *F;
     double *dt;                  /* device [2]: dt[0] min over cells of dx / |signal
                                     speed|, dt[1] the step's time step cfl dt[0]    */
-    int32_t *count;              /* device [4]: con2prim failures, floored cells     */
+    int32_t *count;              /* device [4]: con2prim failures, floored cells,
+                                    cells the mixed variant's FP32 con2prim handed
+                                    to FP64 (away from the hole), unused            */
     int32_t *err;                /* device error word                                */
     double *E;                   /* [3][ncell] edge EMFs, or NULL: computed on the fly
                                     (allowed only when every block has one level)  */

@@ -92,7 +92,7 @@ def test_step_pieces_bitwise():
         g.update(stage); h.update(stage)
         for name in ("U", "U1", "Bf", "Bf1"):
             assert np.array_equal(getattr(g, name).cpu().numpy(), getattr(h, name)), (stage, name)
-    assert g.counters() == {"c2p_failures": int(h.count[0]), "floored": int(h.count[1])}
+    assert g.counters() == {"c2p_failures": int(h.count[0]), "floored": int(h.count[1]), "c2p_fp64_fallback": 0}
 
 
 @pytest.mark.parametrize("steps", [1, 3])
