@@ -192,6 +192,7 @@ int fx_bad(const bh_fx_params* P, const bh_fx_grid* g) {
     if (P->limiter < BH_MINMOD || P->limiter > BH_PPM || (g->ghost_depth != 0 && g->ghost_depth != 2 && g->ghost_depth != 3) ||
         (P->limiter == BH_PPM && g->ghost_depth != 3) || (g->nitem_flux > 0 && !g->items_flux))
         return 1;
+    if (g->c2p_defer && (int64_t)g->c2p_defer_cap < (int64_t)g->nitem_cell * BH_FX_CHUNK) return 1;
     return 0;
 }
 }  // namespace
@@ -222,6 +223,14 @@ int bh_fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void
 int bh_fx_update(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* stream) {
     if (fx_bad(P, g) || stage < 0 || stage > 1) return BH_EINVAL;
     FX_DISPATCH(P, fx_update(P, g, stage, stream));
+}
+int bh_fx_emf(const bh_fx_params* P, const bh_fx_grid* g, void* stream) {
+    if (fx_bad(P, g) || !g->E) return BH_EINVAL;
+    FX_DISPATCH(P, fx_update_parts(P, g, 0, 1, stream));
+}
+int bh_fx_update_from_emf(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* stream) {
+    if (fx_bad(P, g) || !g->E || stage < 0 || stage > 1) return BH_EINVAL;
+    FX_DISPATCH(P, fx_update_parts(P, g, stage, 2, stream));
 }
 int bh_fx_tune_set(int32_t precision, int32_t kernel, int32_t ctas) {
     switch (precision) {

@@ -59,6 +59,7 @@ inline bool bh_tune_valid(int32_t kernel, int32_t ctas) {
     int fx_ghosts(const bh_fx_params*, const bh_fx_grid*, int32_t, void*);                                    \
     int fx_fluxes(const bh_fx_params*, const bh_fx_grid*, int32_t, void*);                                    \
     int fx_update(const bh_fx_params*, const bh_fx_grid*, int32_t, void*);                                    \
+    int fx_update_parts(const bh_fx_params*, const bh_fx_grid*, int32_t, int32_t, void*);                     \
     int fx_step(const bh_fx_params*, const bh_fx_grid*, void*);                                               \
     int fx_divb(const bh_fx_grid*, double*, void*);                                                           \
     int fx_torus_init(const bh_fx_params*, const bh_fx_grid*, const bh_fx_torus*, double*, double*, void*);   \

@@ -158,8 +158,98 @@ __device__ inline int c2p_cell64(const FxPar& P, const Grid& G, const KS& m, con
     return 1;
 }
 
-template <typename RT, typename WT, int MINB>
-__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage, int with_dt, Queue Q) {
+// the whole FP64 path of a cell: metric, con2prim, floors, excision, the
+// rewrite of U where the primitives changed, W and the cell field; returns
+// the cell's CFL limit (with_dt)
+template <typename RT, typename WT>
+__device__ inline double c2p_cell_fp64(const FxPar& P, const Grid& G, const bh_fx_block& B, int64_t c,
+                                       const double* x, const double* Bt, double* U, int with_dt) {
+    const int64_t N = G.ncell;
+    WT* W = (WT*)G.W;
+    KS m;
+    ks_metric(P, x[0], x[1], x[2], m);
+    const double Bc[3] = {Bt[0] * m.alpha, Bt[1] * m.alpha, Bt[2] * m.alpha};   // B~ / sqrt(gamma)
+    double w[8];
+    int rewrite = c2p_cell64<false>(P, G, m, U, W, N, c, Bc, w);
+    if (apply_floors(P, m, w)) {
+        rewrite = 1;
+        atomicAdd(&G.count[1], 1);
+    }
+    if (rewrite) {
+        KSm<double> mm;
+        ks_cast(m, mm);
+        Derived<double> d;
+        double u[8];
+        derive(mm, P.gg, w, d);
+        prim2cons(mm, P.gamma, w, d, u);
+        for (int v = 0; v < 5; v++) U[v * N + c] = u[v];
+    }
+    for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
+    for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];
+    if (!with_dt) return 1e300;
+    const double dx[3] = {B.dx, B.dx, B.dx};
+    return cell_dt<RT>(P, m, w, dx);
+}
+
+// the mixed variant's FP32 path of a cell (away from the hole): returns 0
+// and the cell's CFL limit in dtc when the FP32 con2prim succeeded (W, U
+// written), 1 when the cell needs the FP64 path (nothing written)
+__device__ inline int c2p_cell_fp32(const FxPar& P, const Grid& G, const bh_fx_block& B, int64_t c, const double* x,
+                                    const double* Bt, double* U, int with_dt, double& dtc) {
+    const int64_t N = G.ncell;
+    float* W = (float*)G.W;
+    KSb<float> mf;
+    ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
+    const float Bcf[3] = {float(Bt[0]) * mf.alpha, float(Bt[1]) * mf.alpha, float(Bt[2]) * mf.alpha};
+    float wf[8];
+    {
+        float u[5], wo[5];
+        for (int v = 0; v < 5; v++) u[v] = float(U[v * N + c]);
+        for (int v = 0; v < 5; v++) wo[v] = W[v * N + c];
+        C2PSb<float> cf;
+        c2p_setup(P, mf, u, Bcf, wo, cf);
+        int iters = 0;
+        if (c2p_solve32(cf, iters) || c2p_finish(mf.gi, cf, Bcf, wf)) return 1;
+    }
+    if (apply_floors(P, mf, wf)) {
+        atomicAdd(&G.count[1], 1);
+        KSm<float> mm;
+        ks_cast(mf, mm);
+        Derived<float> d;
+        float uf[8];
+        derive(mm, float(P.gg), wf, d);
+        prim2cons(mm, float(P.gamma), wf, d, uf);
+        for (int v = 0; v < 5; v++) U[v * N + c] = (double)uf[v];
+    }
+    for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
+    for (int v = 0; v < 8; v++) W[v * N + c] = wf[v];
+    if (with_dt) {
+        const double dx[3] = {B.dx, B.dx, B.dx};
+        dtc = cell_dt<float>(P, mf, wf, dx);
+    }
+    return 0;
+}
+
+// a cell's centre and face-averaged field (the role of f2cB, transport.cpp:60-75)
+__device__ inline void c2p_inputs(const Grid& G, const bh_fx_block& B, int i, int j, int k, int stage, double* x,
+                                  double* Bt) {
+    const int64_t N = G.ncell, c = bidx(B, i, j, k);
+    const double* Bf = stage ? G.Bf1 : G.Bf;
+    const int si = bstride_i(B), sj = bstride_j(B);
+    cell_centre(B, i, j, k, x);
+    Bt[0] = 0.5 * (Bf[c] + Bf[c + si]);
+    Bt[1] = 0.5 * (Bf[N + c] + Bf[N + c + sj]);
+    Bt[2] = 0.5 * (Bf[2 * N + c] + Bf[2 * N + c + 1]);
+}
+
+// con2prim + floors + excision on every interior cell.  The mixed variant
+// solves in FP32 beyond r ~ FX_R_FP64 where the FP32 residual is well
+// conditioned; the other cells take the FP64 path -- inline, or (DEFER)
+// appended to the list defer = [count, done, (block, cell)...] for
+// k_fx_c2p_deferred, which keeps this kernel's registers to the FP32 path's
+template <typename RT, typename WT, int MINB, bool DEFER>
+__global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage,
+                                                       int with_dt, Queue Q, int32_t* defer) {
     for_items(Q, [&](int t) FX_INLINE {
         const int32_t b = items[2 * t];
         const bh_fx_block B = G.blk[b];
@@ -170,86 +260,22 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
             const int i = e / (n * n), j = (e / n) % n, k = e % n;
             const int64_t c = bidx(B, i, j, k);
             double* U = stage ? G.U1 : G.U;
-            const double* Bf = stage ? G.Bf1 : G.Bf;
-            const int64_t N = G.ncell;
-            double x[3];
-            cell_centre(B, i, j, k, x);
-            // the mixed variant beyond r ~ FX_R_FP64: geometry, con2prim,
-            // floors and the floor rewrite in FP32
-            const bool g32 = fp32_geometry<RT>(x);
-            // cell field: mean of the two faces (the role of f2cB, transport.cpp:60-75)
-            const int si = bstride_i(B), sj = bstride_j(B);
-            const double Bt[3] = {0.5 * (Bf[c] + Bf[c + si]), 0.5 * (Bf[N + c] + Bf[N + c + sj]),
-                                  0.5 * (Bf[2 * N + c] + Bf[2 * N + c + 1])};
-            WT* W = (WT*)G.W;
+            double x[3], Bt[3];
+            c2p_inputs(G, B, i, j, k, stage, x, Bt);
             constexpr bool MIXED = sizeof(RT) < sizeof(double);
-            const double dx[3] = {B.dx, B.dx, B.dx};
-            int rewrite = 0;
-            if (MIXED && g32) {
-                // FP32 con2prim where its residual is well conditioned (the
-                // primitives are stored in FP32), FP64 where not
-                KSb<float> mf;
-                ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
-                const float Bcf[3] = {float(Bt[0]) * mf.alpha, float(Bt[1]) * mf.alpha, float(Bt[2]) * mf.alpha};
-                float wf[8];
-                int st;
-                {
-                    float u[5], wo[5];
-                    for (int v = 0; v < 5; v++) u[v] = float(U[v * N + c]);
-                    for (int v = 0; v < 5; v++) wo[v] = float(W[v * N + c]);
-                    C2PSb<float> cf;
-                    c2p_setup(P, mf, u, Bcf, wo, cf);
-                    int iters = 0;
-                    st = c2p_solve32(cf, iters);
-                    if (st == 0) st = c2p_finish(mf.gi, cf, Bcf, wf);
+            int full = 1;
+            if (MIXED && fp32_geometry<RT>(x)) {
+                full = c2p_cell_fp32(P, G, B, c, x, Bt, U, with_dt, dtc);
+                if (full) atomicAdd(&G.count[2], 1);
+            }
+            if (full) {
+                if (DEFER) {
+                    const int q = atomicAdd(&defer[0], 1);
+                    defer[2 + 2 * q] = b;
+                    defer[3 + 2 * q] = e;
+                } else {
+                    dtc = c2p_cell_fp64<RT, WT>(P, G, B, c, x, Bt, U, with_dt);
                 }
-                if (st != 0) {
-                    atomicAdd(&G.count[2], 1);
-                    KS m;
-                    copy_metric(mf, m);
-                    const double Bc[3] = {Bt[0] * m.alpha, Bt[1] * m.alpha, Bt[2] * m.alpha};
-                    double w[8];
-                    rewrite = c2p_cell64<false>(P, G, m, U, W, N, c, Bc, w);
-                    for (int v = 0; v < 8; v++) wf[v] = float(w[v]);
-                }
-                if (apply_floors(P, mf, wf)) {
-                    rewrite = 1;
-                    atomicAdd(&G.count[1], 1);
-                }
-                if (rewrite) {
-                    KSm<float> mm;
-                    ks_cast(mf, mm);
-                    Derived<float> d;
-                    float uf[8];
-                    derive(mm, float(P.gg), wf, d);
-                    prim2cons(mm, float(P.gamma), wf, d, uf);
-                    for (int v = 0; v < 5; v++) U[v * N + c] = (double)uf[v];
-                }
-                for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
-                for (int v = 0; v < 8; v++) W[v * N + c] = (WT)wf[v];
-                if (with_dt) dtc = cell_dt<float>(P, mf, wf, dx);
-            } else {
-                KS m;
-                ks_metric(P, x[0], x[1], x[2], m);
-                const double Bc[3] = {Bt[0] * m.alpha, Bt[1] * m.alpha, Bt[2] * m.alpha};   // B~ / sqrt(gamma)
-                double w[8];
-                rewrite = c2p_cell64<MIXED>(P, G, m, U, W, N, c, Bc, w);
-                if (apply_floors(P, m, w)) {
-                    rewrite = 1;
-                    atomicAdd(&G.count[1], 1);
-                }
-                if (rewrite) {
-                    KSm<double> mm;
-                    ks_cast(m, mm);
-                    Derived<double> d;
-                    double u[8];
-                    derive(mm, P.gg, w, d);
-                    prim2cons(mm, P.gamma, w, d, u);
-                    for (int v = 0; v < 5; v++) U[v * N + c] = u[v];
-                }
-                for (int d = 0; d < 3; d++) U[(5 + d) * N + c] = Bt[d];
-                for (int v = 0; v < 8; v++) W[v * N + c] = (WT)w[v];
-                if (with_dt) dtc = cell_dt<RT>(P, m, w, dx);
             }
         }
         if (with_dt) {
@@ -257,6 +283,32 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
             if ((threadIdx.x & 31) == 0 && dtc < 1e300) atomic_min_pos(G.dt, dtc);
         }
     });
+}
+
+// the FP64 path of the cells k_fx_c2p deferred; the last CTA to finish
+// clears the list for the next launch
+template <typename RT, typename WT>
+__global__ void __launch_bounds__(FX_TPB) k_fx_c2p_deferred(FxPar P, Grid G, int stage, int with_dt, int32_t* defer) {
+    const int cnt = *(volatile int32_t*)&defer[0];
+    for (int q = blockIdx.x * FX_TPB + threadIdx.x; q < cnt; q += gridDim.x * FX_TPB) {
+        const int32_t b = defer[2 + 2 * q], e = defer[3 + 2 * q];
+        const bh_fx_block B = G.blk[b];
+        const int n = B.n;
+        const int i = e / (n * n), j = (e / n) % n, k = e % n;
+        double x[3], Bt[3];
+        c2p_inputs(G, B, i, j, k, stage, x, Bt);
+        const double dtc = c2p_cell_fp64<RT, WT>(P, G, B, bidx(B, i, j, k), x, Bt, stage ? G.U1 : G.U, with_dt);
+        if (with_dt && dtc < 1e300) atomic_min_pos(G.dt, dtc);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&defer[1], 1) == (int)gridDim.x - 1) {
+            defer[0] = 0;
+            defer[1] = 0;
+            __threadfence();
+        }
+    }
 }
 
 // ======================================================================
@@ -1045,6 +1097,15 @@ inline fx::Queue fx_q(const bh_fx_grid* g, int slot, int nitem) {
     if (!g->queue) return fx::Queue{nullptr, nullptr, nitem};
     return fx::Queue{g->queue + 2 * slot, g->queue + 2 * slot + 1, nitem};
 }
+inline int fx_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+    }
+    return sms;
+}
 // CTAs of a launch: one per item, or (persistent) the resident CTAs of the
 // kernel on this device, from the occupancy calculator (cached per kernel)
 inline int fx_grid(const void* fn, int nitem, const bh_fx_grid* g) {
@@ -1061,13 +1122,7 @@ inline int fx_grid(const void* fn, int nitem, const bh_fx_grid* g) {
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, fx::FX_TPB, 0) != cudaSuccess || occ < 1) occ = 1;
             if (nkeys < 96) { keys[nkeys] = fn; vals[nkeys] = occ; nkeys++; }
         }
-        static int sms = 0;
-        if (!sms) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
-        }
-        ctas = sms * occ;
+        ctas = fx_sms() * occ;
     }
     return nitem < ctas ? nitem : ctas;
 }
@@ -1107,8 +1162,14 @@ int fx_prims(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t 
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
     if (with_dt) fx::k_fx_dt_init<<<1, 1, 0, fxs(s)>>>(g->dt);
-    if (g->nitem_cell) {
-#define L_(M) fx::k_fx_c2p<FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_c2p<FRT, FRT, M>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt, fx_q(g, QS_C2P, g->nitem_cell))
+    constexpr bool MIXED = sizeof(FRT) < sizeof(double);
+    if (g->nitem_cell && MIXED && g->c2p_defer) {
+#define L_(M) fx::k_fx_c2p<FRT, FRT, M, true><<<fx_grid((const void*)fx::k_fx_c2p<FRT, FRT, M, true>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt, fx_q(g, QS_C2P, g->nitem_cell), g->c2p_defer)
+        FX_TUNED(BH_FX_TUNE_C2P, L_)
+#undef L_
+        fx::k_fx_c2p_deferred<FRT, FRT><<<fx_sms(), fx::FX_TPB, 0, fxs(s)>>>(p, G, stage, with_dt, g->c2p_defer);
+    } else if (g->nitem_cell) {
+#define L_(M) fx::k_fx_c2p<FRT, FRT, M, false><<<fx_grid((const void*)fx::k_fx_c2p<FRT, FRT, M, false>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt, fx_q(g, QS_C2P, g->nitem_cell), nullptr)
         FX_TUNED(BH_FX_TUNE_C2P, L_)
 #undef L_
     }
@@ -1137,22 +1198,27 @@ int fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s
     }
     return fx_launched();
 }
-int fx_update(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
+// parts: 1 = the edge EMFs into E, 2 = their level-change correction and
+// the update (3 = both: the update of a stage)
+int fx_update_parts(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t parts, void* s) {
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
-    if (g->E && g->nitem_pos) {
+    if (g->E && g->nitem_pos && (parts & 1))
         fx::k_fx_emf<FRT><<<fx_grid((const void*)fx::k_fx_emf<FRT>, g->nitem_pos, g), fx::FX_TPB, 0, fxs(s)>>>(
             G, g->items_pos, fx_q(g, QS_EMF, g->nitem_pos));
-        if (g->maxlevel > 0)
-            fx::k_fx_emf_fix<<<fx_grid((const void*)fx::k_fx_emf_fix, g->nitem_pos, g), fx::FX_TPB, 0, fxs(s)>>>(
-                G, g->items_pos, fx_q(g, QS_EMF_FIX, g->nitem_pos));
-    }
+    if (!(parts & 2)) return fx_launched();
+    if (g->E && g->nitem_pos && g->maxlevel > 0)
+        fx::k_fx_emf_fix<<<fx_grid((const void*)fx::k_fx_emf_fix, g->nitem_pos, g), fx::FX_TPB, 0, fxs(s)>>>(
+            G, g->items_pos, fx_q(g, QS_EMF_FIX, g->nitem_pos));
     if (g->nitem_cell) {
 #define L_(M) fx::k_fx_update<FRT, FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_update<FRT, FRT, FRT, M>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, P->cfl, fx_q(g, QS_UPDATE, g->nitem_cell))
         FX_TUNED(BH_FX_TUNE_UPDATE, L_)
 #undef L_
     }
     return fx_launched();
+}
+int fx_update(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
+    return fx_update_parts(P, g, stage, 3, s);
 }
 int fx_step(const bh_fx_params* P, const bh_fx_grid* g, void* s) {
     for (int stage = 0; stage < 2; stage++) {

@@ -460,6 +460,11 @@ typedef struct bh_fx_grid {
     int32_t ghost_depth;         /* ghost layers the fill covers (and items_ghost
                                     lists): 2 (0 reads as 2), or 3, which BH_PPM
                                     requires                                        */
+    int32_t *c2p_defer;          /* BH_MIXED only, or NULL: device [2 + 2 cap],
+                                    zeroed once; cells whose con2prim needs FP64
+                                    are listed here by the FP32 kernel and solved by
+                                    a second one (the list clears itself)          */
+    int32_t c2p_defer_cap;       /* at least nitem_cell * BH_FX_CHUNK                */
 } bh_fx_grid;
 #define BH_FX_QSLOTS 6
 
@@ -487,6 +492,14 @@ int bh_fx_prims(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, int32
 int bh_fx_ghosts(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
 int bh_fx_fluxes(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
 int bh_fx_update(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
+/* bh_fx_update in two parts, for a grid whose blocks are shared with other
+ * processes (bhgpu.fxshard): bh_fx_emf writes the edge EMFs of the grid's own
+ * blocks (the work lists) into E; bh_fx_update_from_emf applies the
+ * level-change correction, which reads E of finer neighbours (their EMFs
+ * copied in beforehand where another process owns them), and the update.
+ * Both require E. */
+int bh_fx_emf(const bh_fx_params *P, const bh_fx_grid *g, void *stream);
+int bh_fx_update_from_emf(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
 /* max over each block's interior cells of |div B~| / max |B~| of the cell's
  * faces (a relative divergence, 0 up to roundoff under CT): out [nblock]
  * device, cleared by the call */
