@@ -58,6 +58,9 @@ _sig = {
     "bh_fx_ghosts": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
     "bh_fx_fluxes": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
     "bh_fx_update": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
+    "bh_fx_ghost_pass": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _i32, _vp],
+    "bh_fx_emf": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _vp],
+    "bh_fx_update_from_emf": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
     "bh_fx_divb": [C.POINTER(BhFxGrid), _vp, _vp],
     "bh_fx_torus_init": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), C.POINTER(BhFxTorus), _vp, _vp, _vp],
 }
@@ -112,13 +115,16 @@ class FxGrid:
     """
 
     def __init__(self, blocks: np.ndarray, nbr: np.ndarray, params: FxParams, device="cuda", emf_arrays=None,
-                 persistent=False, defer_c2p=True):
+                 persistent=False, defer_c2p=True, nactive=None, maxlevel=None):
         """emf_arrays: keep the edge EMFs in arrays (required, and the
         default, when blocks have different levels; otherwise they are
         computed on the fly by the update).  persistent: launch the step
         kernels as persistent CTAs fed by a device work queue.  defer_c2p
         (mixed variant): cells whose con2prim needs FP64 are solved by a
-        second kernel rather than inline."""
+        second kernel rather than inline.  nactive: the kernels work on
+        blocks[:nactive] only (the rest are neighbours' copies, as in a
+        sharded grid); maxlevel: the highest level of the whole domain
+        (default: of these blocks)."""
         self.params = params
         self.blocks_np = blocks
         self.nbr_np = nbr
@@ -128,9 +134,11 @@ class FxGrid:
         self.blocks = torch.from_numpy(blocks.view(np.uint8).copy()).to(dev)
         self.nbr = torch.from_numpy(nbr.copy()).to(dev)
         self.ghost_depth = ghost_depth(params.limiter)
-        self.items = {k: torch.from_numpy(work_items(blocks, k, self.ghost_depth)).to(dev)
+        self.nactive = len(blocks) if nactive is None else int(nactive)
+        act = blocks[:self.nactive]
+        self.items = {k: torch.from_numpy(work_items(act, k, self.ghost_depth)).to(dev)
                       for k in ("cell", "pos", "ghost")}
-        self.items["flux"] = torch.from_numpy(flux_items(blocks)).to(dev)
+        self.items["flux"] = torch.from_numpy(flux_items(act)).to(dev)
         wdt = torch.float32 if params.precision == "mixed" else torch.float64
         N = self.ncell
         self.U = torch.zeros((8, N), dtype=torch.float64, device=dev)
@@ -143,7 +151,7 @@ class FxGrid:
         self.count = torch.zeros(4, dtype=torch.int32, device=dev)
         self.err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.scratch = torch.zeros(4, dtype=torch.float64, device=dev)
-        self.maxlevel = int(blocks["level"].max())
+        self.maxlevel = int(blocks["level"].max()) if maxlevel is None else int(maxlevel)
         if emf_arrays is None:
             emf_arrays = self.maxlevel > 0
         self.E = torch.zeros((3, N), dtype=torch.float64, device=dev) if emf_arrays else None
@@ -169,7 +177,7 @@ class FxGrid:
 
     def _refresh(self):
         it = self.items
-        self._g = BhFxGrid(len(self.blocks_np), _ptr(self.blocks), _ptr(self.nbr),
+        self._g = BhFxGrid(self.nactive, _ptr(self.blocks), _ptr(self.nbr),
                            _ptr(it["cell"]), it["cell"].shape[0], _ptr(it["pos"]), it["pos"].shape[0],
                            _ptr(it["ghost"]), it["ghost"].shape[0], self.ncell,
                            _ptr(self.U), _ptr(self.U1), _ptr(self.W), _ptr(self.Bf), _ptr(self.Bf1), _ptr(self.F),
@@ -195,6 +203,17 @@ class FxGrid:
 
     def ghosts(self, stage=0):
         check(lib.bh_fx_ghosts(C.byref(self._p), C.byref(self._g), stage, _stream()), "bh_fx_ghosts")
+
+    def ghost_pass(self, stage, pass_):
+        check(lib.bh_fx_ghost_pass(C.byref(self._p), C.byref(self._g), stage, pass_, _stream()), "bh_fx_ghost_pass")
+
+    def emf_raw(self):
+        """the edge EMFs of the grid's own blocks into E, uncorrected"""
+        check(lib.bh_fx_emf(C.byref(self._p), C.byref(self._g), _stream()), "bh_fx_emf")
+
+    def update_from_emf(self, stage=0):
+        check(lib.bh_fx_update_from_emf(C.byref(self._p), C.byref(self._g), stage, _stream()),
+              "bh_fx_update_from_emf")
 
     def fluxes(self, stage=0):
         check(lib.bh_fx_fluxes(C.byref(self._p), C.byref(self._g), stage, _stream()), "bh_fx_fluxes")

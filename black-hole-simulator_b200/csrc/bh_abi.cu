@@ -212,6 +212,10 @@ int bh_fx_prims(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32
     if (fx_bad(P, g) || stage < 0 || stage > 1) return BH_EINVAL;
     FX_DISPATCH(P, fx_prims(P, g, stage, with_dt, stream));
 }
+int bh_fx_ghost_pass(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t pass, void* stream) {
+    if (fx_bad(P, g) || stage < 0 || stage > 1 || pass < 0 || pass > g->maxlevel) return BH_EINVAL;
+    FX_DISPATCH(P, fx_ghost_pass(P, g, stage, pass, stream));
+}
 int bh_fx_ghosts(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* stream) {
     if (fx_bad(P, g) || stage < 0 || stage > 1) return BH_EINVAL;
     FX_DISPATCH(P, fx_ghosts(P, g, stage, stream));

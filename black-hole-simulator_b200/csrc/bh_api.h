@@ -57,6 +57,7 @@ inline bool bh_tune_valid(int32_t kernel, int32_t ctas) {
     int step(const bh_params*, const bh_pool*, double, double*, const int32_t*, const int32_t*, int32_t, void*); \
     int fx_prims(const bh_fx_params*, const bh_fx_grid*, int32_t, int32_t, void*);                           \
     int fx_ghosts(const bh_fx_params*, const bh_fx_grid*, int32_t, void*);                                    \
+    int fx_ghost_pass(const bh_fx_params*, const bh_fx_grid*, int32_t, int32_t, void*);                       \
     int fx_fluxes(const bh_fx_params*, const bh_fx_grid*, int32_t, void*);                                    \
     int fx_update(const bh_fx_params*, const bh_fx_grid*, int32_t, void*);                                    \
     int fx_update_parts(const bh_fx_params*, const bh_fx_grid*, int32_t, int32_t, void*);                     \

@@ -1175,14 +1175,18 @@ int fx_prims(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t 
     }
     return fx_launched();
 }
-int fx_ghosts(const bh_fx_params*, const bh_fx_grid* g, int32_t stage, void* s) {
+int fx_ghost_pass(const bh_fx_params*, const bh_fx_grid* g, int32_t stage, int32_t pass, void* s) {
     fx::Grid G = fx::grid_of(g);
-    // pass 0: copies and restrictions; pass l: prolongations into level l
-    for (int pass = 0; pass <= g->maxlevel; pass++)
-        if (g->nitem_ghost)
-            fx::k_fx_ghost<FRT><<<fx_grid((const void*)fx::k_fx_ghost<FRT>, g->nitem_ghost, g), fx::FX_TPB, 0, fxs(s)>>>(
-                G, g->items_ghost, stage, pass, fx_q(g, QS_GHOST, g->nitem_ghost));
+    if (g->nitem_ghost)
+        fx::k_fx_ghost<FRT><<<fx_grid((const void*)fx::k_fx_ghost<FRT>, g->nitem_ghost, g), fx::FX_TPB, 0, fxs(s)>>>(
+            G, g->items_ghost, stage, pass, fx_q(g, QS_GHOST, g->nitem_ghost));
     return fx_launched();
+}
+int fx_ghosts(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
+    // pass 0: copies and restrictions; pass l: prolongations into level l
+    int rc = BH_OK;
+    for (int pass = 0; pass <= g->maxlevel && rc == BH_OK; pass++) rc = fx_ghost_pass(P, g, stage, pass, s);
+    return rc;
 }
 int fx_fluxes(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, void* s) {
     fx::FxPar p = fx::par_of(P);

@@ -490,6 +490,11 @@ int bh_fx_graph_create(const bh_fx_params *P, const bh_fx_grid *g, void *stream,
 /* the pieces of a stage (stage 0 works on U/Bf, stage 1 on U1/Bf1) */
 int bh_fx_prims(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, int32_t with_dt, void *stream);
 int bh_fx_ghosts(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
+/* one pass of bh_fx_ghosts (pass 0: copies and restrictions; pass l in
+ * 1..maxlevel: prolongations into level-l blocks), for a grid whose blocks
+ * are shared with other processes: the neighbours' boxes are exchanged
+ * between passes (bhgpu.fxshard) */
+int bh_fx_ghost_pass(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, int32_t pass, void *stream);
 int bh_fx_fluxes(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
 int bh_fx_update(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
 /* bh_fx_update in two parts, for a grid whose blocks are shared with other

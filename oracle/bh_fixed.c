@@ -626,10 +626,10 @@ static double mm_slope(double a, double b, double c) {
  * its minmod slope per direction; a face takes the coarse face it lies on
  * or the mean of the two it lies between).  Pass 0: copies and
  * restrictions; pass l: prolongations into level-l blocks. */
-void fxo_ghosts(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, double* W, double* Bf,
-                double* Bf1, int stage, int maxlevel, int depth) {
+void fxo_ghost_pass(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, double* W, double* Bf,
+                    double* Bf1, int stage, int pass, int depth) {
     double* F = stage ? Bf1 : Bf;
-    for (int pass = 0; pass <= maxlevel; pass++)
+    {
         for (int b = 0; b < nblock; b++) {
             int n = blk[b].n;
             if (pass > 0 && blk[b].level != pass) continue;
@@ -711,6 +711,12 @@ void fxo_ghosts(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_
                         }
                     }
         }
+    }
+}
+
+void fxo_ghosts(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, double* W, double* Bf,
+                double* Bf1, int stage, int maxlevel, int depth) {
+    for (int pass = 0; pass <= maxlevel; pass++) fxo_ghost_pass(nblock, blk, nbr, N, W, Bf, Bf1, stage, pass, depth);
 }
 
 static void face(const fxo_params* P, const fxo_block* B, int64_t N, const double* W, const double* Bfs, double* F,
@@ -772,8 +778,7 @@ static double ez_(const double* F, int64_t N, int64_t c, int si, int sj) {
 /* edge EMFs of every block (E_x at i in [0,n), j, k in [0,n], alike for y,
  * z) from the face fluxes; then, where a finer block touches a boundary
  * edge, the mean of its two EMFs along that edge */
-void fxo_emf(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, const double* F, double* E,
-             int maxlevel) {
+void fxo_emf_raw(int32_t nblock, const fxo_block* blk, int64_t N, const double* F, double* E) {
     for (int b = 0; b < nblock; b++) {
         const fxo_block* B = &blk[b];
         int n = B->n, si = SP(n) * SP(n), sj = SP(n), sk = 1;
@@ -787,7 +792,8 @@ void fxo_emf(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N
                     if (k < n) E[2 * N + c] = ez_(F, N, c, si, sj);
                 }
     }
-    if (maxlevel == 0) return;
+}
+void fxo_emf_fix(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, double* E) {
     for (int b = 0; b < nblock; b++) {
         const fxo_block* B = &blk[b];
         int n = B->n;
@@ -824,6 +830,12 @@ void fxo_emf(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N
                     }
                 }
     }
+}
+
+void fxo_emf(int32_t nblock, const fxo_block* blk, const int32_t* nbr, int64_t N, const double* F, double* E,
+             int maxlevel) {
+    fxo_emf_raw(nblock, blk, N, F, E);
+    if (maxlevel > 0) fxo_emf_fix(nblock, blk, nbr, N, E);
 }
 
 static void fupd(const double* E, int64_t N, double* Bf, double* Bf1, int d, int64_t c, int si, int sj, int sk,

@@ -39,6 +39,9 @@ def lib():
         L.fxo_step.argtypes = [P, i32, v, v, i64] + [v] * 9 + [C.c_int]
         L.fxo_prims.argtypes = [P, i32, v, v, i64] + [v] * 8 + [C.c_int, C.c_int]
         L.fxo_ghosts.argtypes = [i32, v, v, i64, v, v, v, C.c_int, C.c_int, C.c_int]
+        L.fxo_ghost_pass.argtypes = [i32, v, v, i64, v, v, v, C.c_int, C.c_int, C.c_int]
+        L.fxo_emf_raw.argtypes = [i32, v, i64, v, v]
+        L.fxo_emf_fix.argtypes = [i32, v, v, i64, v]
         L.fxo_emf.argtypes = [i32, v, v, i64, v, v, C.c_int]
         L.fxo_fluxes.argtypes = [P, i32, v, i64, v, v, v, v, C.c_int]
         L.fxo_update.argtypes = [P, i32, v, i64, v, v, v, v, v, v, v, v, C.c_int]
@@ -78,10 +81,13 @@ def params(fx) -> FxoParams:
 class FxHost:
     """Host copy of a block grid (the oracle's state)."""
 
-    def __init__(self, blocks: np.ndarray, nbr: np.ndarray, prm: FxoParams):
+    def __init__(self, blocks: np.ndarray, nbr: np.ndarray, prm: FxoParams, nactive=None, maxlevel=None):
+        """nactive: step blocks[:nactive] only (the rest are neighbours'
+        copies); maxlevel: of the whole domain (default: of these blocks)"""
         self.blocks = np.ascontiguousarray(blocks)
         self.nbr = np.ascontiguousarray(nbr, np.int32)
         self.prm = prm
+        self.nactive = len(self.blocks) if nactive is None else int(nactive)
         self.N = int(sum((int(n) + 2 * GB + 1) ** 3 for n in blocks["n"]))
         N = self.N
         self.U = np.zeros((8, N))
@@ -91,7 +97,7 @@ class FxHost:
         self.Bf1 = np.zeros((3, N))
         self.F = np.zeros((3, 8, N))
         self.E = np.zeros((3, N))
-        self.maxlevel = int(self.blocks["level"].max())
+        self.maxlevel = int(self.blocks["level"].max()) if maxlevel is None else int(maxlevel)
         self.dt = np.zeros(2)
         self.count = np.zeros(4, np.int32)
 
@@ -101,7 +107,7 @@ class FxHost:
         return 3 if self.prm.limiter == 3 else 2
 
     def _g(self):
-        return (C.byref(self.prm), len(self.blocks), _p(self.blocks), _p(self.nbr), self.N)
+        return (C.byref(self.prm), self.nactive, _p(self.blocks), _p(self.nbr), self.N)
 
     def step(self):
         lib().fxo_step(*self._g(), _p(self.U), _p(self.U1), _p(self.W), _p(self.Bf), _p(self.Bf1), _p(self.F),
@@ -112,26 +118,44 @@ class FxHost:
                         _p(self.dt), _p(self.count), stage, int(with_dt))
 
     def ghosts(self, stage=0):
-        lib().fxo_ghosts(len(self.blocks), _p(self.blocks), _p(self.nbr), self.N, _p(self.W), _p(self.Bf),
+        lib().fxo_ghosts(self.nactive, _p(self.blocks), _p(self.nbr), self.N, _p(self.W), _p(self.Bf),
                          _p(self.Bf1), stage, self.maxlevel, self.ghost_depth)
 
+    def ghost_pass(self, stage, pass_):
+        lib().fxo_ghost_pass(self.nactive, _p(self.blocks), _p(self.nbr), self.N, _p(self.W), _p(self.Bf),
+                             _p(self.Bf1), stage, pass_, self.ghost_depth)
+
     def fluxes(self, stage=0):
-        lib().fxo_fluxes(C.byref(self.prm), len(self.blocks), _p(self.blocks), self.N, _p(self.W), _p(self.Bf),
+        lib().fxo_fluxes(C.byref(self.prm), self.nactive, _p(self.blocks), self.N, _p(self.W), _p(self.Bf),
                          _p(self.Bf1), _p(self.F), stage)
 
     def emf(self):
-        lib().fxo_emf(len(self.blocks), _p(self.blocks), _p(self.nbr), self.N, _p(self.F), _p(self.E),
+        lib().fxo_emf(self.nactive, _p(self.blocks), _p(self.nbr), self.N, _p(self.F), _p(self.E),
                       self.maxlevel)
+
+    def emf_raw(self):
+        """the edge EMFs of the active blocks, uncorrected"""
+        lib().fxo_emf_raw(self.nactive, _p(self.blocks), self.N, _p(self.F), _p(self.E))
 
     def update(self, stage=0):
         """edge EMFs from the fluxes (corrected at level changes), then the update"""
         self.emf()
-        lib().fxo_update(C.byref(self.prm), len(self.blocks), _p(self.blocks), self.N, _p(self.U), _p(self.U1),
+        self._update(stage)
+
+    def update_from_emf(self, stage=0):
+        """the level-change correction of E (raw EMFs of every block it reads
+        already in E), then the update"""
+        if self.maxlevel > 0:
+            lib().fxo_emf_fix(self.nactive, _p(self.blocks), _p(self.nbr), self.N, _p(self.E))
+        self._update(stage)
+
+    def _update(self, stage):
+        lib().fxo_update(C.byref(self.prm), self.nactive, _p(self.blocks), self.N, _p(self.U), _p(self.U1),
                          _p(self.W), _p(self.Bf), _p(self.Bf1), _p(self.F), _p(self.E), _p(self.dt), stage)
 
     def divb(self) -> float:
         out = np.zeros(len(self.blocks))
-        lib().fxo_divb(len(self.blocks), _p(self.blocks), self.N, _p(self.Bf), _p(out))
+        lib().fxo_divb(self.nactive, _p(self.blocks), self.N, _p(self.Bf), _p(out))
         return float(out.max())
 
     def torus_init(self, r_in=6.0, r_max=12.0, kappa=1e-3, beta=100.0, noise=0.04, seed=1):

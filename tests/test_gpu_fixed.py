@@ -420,3 +420,44 @@ def test_mixed_deferred_con2prim_equals_inline():
     ca, cb = a.counters(), b.counters()
     assert ca["c2p_fp64_fallback"] == cb["c2p_fp64_fallback"] and ca["c2p_failures"] == cb["c2p_failures"] == 0
     assert a.time_step() == pytest.approx(b.time_step(), rel=1e-6)
+
+
+def test_sharded_pieces_on_one_rank_equal_the_step():
+    """bhgpu.fxshard on a one-rank group: the step as separate pieces (ghost
+    fill pass by pass, raw EMFs, correction + update; bh_fx_ghost_pass,
+    bh_fx_emf, bh_fx_update_from_emf) on the local grid built by
+    bhgrid.shard = FxGrid.step on the whole grid, bit for bit (FP64, three
+    levels)"""
+    import os
+    import socket
+    from datetime import timedelta
+    import torch.distributed as dist
+    from bhgpu.fixed import FxGrid, FxParams
+    from bhgpu.fxshard import ShardedFxGrid
+    from bhgrid.blocks import leveled_blocks, torus_levels
+    blocks, nbr = leveled_blocks(-40.0, 40.0, torus_levels(nb=8, r_fine=(14.0, 26.0), seed=3), 8)
+    prm = FxParams(precision="fp64")
+    whole = FxGrid(blocks, nbr, prm)
+    whole.torus_init()
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    dist.init_process_group("gloo", rank=0, world_size=1, timeout=timedelta(seconds=60))
+    try:
+        sh = ShardedFxGrid(blocks, nbr, lambda lb, ln, na, ml: FxGrid(lb, ln, prm, nactive=na, maxlevel=ml))
+        for name in ("U", "W", "Bf"):
+            sh.scatter(name, getattr(whole, name))
+        for _ in range(2):
+            whole.step()
+            sh.step()
+        torch.cuda.synchronize()
+        for name in ("U", "Bf"):
+            for g, box in sh.owned_boxes(name).items():
+                b = blocks[g]
+                off, n = int(b["off"]), int(b["n"])
+                ref = getattr(whole, name)[:, off:off + (n + 7) ** 3].cpu().numpy()
+                assert np.array_equal(box, ref), (name, g)
+    finally:
+        dist.destroy_process_group()
