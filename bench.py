@@ -58,7 +58,9 @@ LO, HI = -40.0, 40.0
 TORUS = dict(r_in=6.0, r_max=12.0, kappa=1e-3, beta=100.0, noise=0.04, seed=1)
 STEP_BYTES = 296          # algorithmic HBM bytes per zone-update of an RK2 step
 LAUNCHES_PER_STEP = 9     # dt init, then con2prim, ghosts, fluxes, update per stage
-DEFERRED_PER_STEP = 2     # the mixed variant's FP64 con2prim of deferred cells, per stage
+# DRAM bytes (read + write) per launch of the mixed variant's step kernels at
+# 128^3, from the ncu capture summarised in profiles/kernels_torus_128cube.md
+PROFILED_TRAFFIC = {"fluxes": 154.88e6 + 173.99e6, "update": 542.57e6 + 122.21e6, "prims": 190.09e6 + 135.60e6}
 E2E_DEPTH = 3
 
 
@@ -684,9 +686,12 @@ def run_ours(args):
                     "api": f"bhgpu.fixed.FxHostPipeline, {E2E_DEPTH} device grids, pinned host U/W/Bf in and "
                            "out every step",
                     "serial_value": world * zones / (ms_e2e_serial / 1e3), "serial_ms_per_step": ms_e2e_serial},
-            "gpu_launches": (LAUNCHES_PER_STEP + DEFERRED_PER_STEP) * args.steps,
+            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "roofline": {"bound": "hbm", "kernel": f"{kname} ({top})", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": PROFILED_TRAFFIC.get(top) if args.grid == 128 else None,
+                         "traffic_source": "ncu capture of the same kernel at 128^3 "
+                                           "(profiles/kernels_torus_128cube.md)", "peak_source": peak_kind,
                          "ms_per_launch": top_ms, "alg_bytes_per_launch": byts,
                          "launch_ms": {k: {p: round(v, 5) for p, v in d.items()} for k, d in pieces.items()},
                          "step_share": {k: round(v, 4) for k, v in share.items()},

@@ -44,8 +44,7 @@ class BhFxGrid(C.Structure):
                 ("items_pos", _vp), ("nitem_pos", _i32), ("items_ghost", _vp), ("nitem_ghost", _i32),
                 ("ncell", _i64), ("U", _vp), ("U1", _vp), ("W", _vp), ("Bf", _vp), ("Bf1", _vp), ("F", _vp),
                 ("dt", _vp), ("count", _vp), ("err", _vp), ("E", _vp), ("maxlevel", _i32), ("queue_ctas", _i32), ("queue", _vp),
-                ("items_flux", _vp), ("nitem_flux", _i32), ("ghost_depth", _i32),
-                ("c2p_defer", _vp), ("c2p_defer_cap", _i32)]
+                ("items_flux", _vp), ("nitem_flux", _i32), ("ghost_depth", _i32)]
 
 
 class BhFxTorus(C.Structure):
@@ -115,16 +114,14 @@ class FxGrid:
     """
 
     def __init__(self, blocks: np.ndarray, nbr: np.ndarray, params: FxParams, device="cuda", emf_arrays=None,
-                 persistent=False, defer_c2p=True, nactive=None, maxlevel=None):
+                 persistent=False, nactive=None, maxlevel=None):
         """emf_arrays: keep the edge EMFs in arrays (required, and the
         default, when blocks have different levels; otherwise they are
         computed on the fly by the update).  persistent: launch the step
-        kernels as persistent CTAs fed by a device work queue.  defer_c2p
-        (mixed variant): cells whose con2prim needs FP64 are solved by a
-        second kernel rather than inline.  nactive: the kernels work on
-        blocks[:nactive] only (the rest are neighbours' copies, as in a
-        sharded grid); maxlevel: the highest level of the whole domain
-        (default: of these blocks)."""
+        kernels as persistent CTAs fed by a device work queue.  nactive:
+        the kernels work on blocks[:nactive] only (the rest are neighbours'
+        copies, as in a sharded grid); maxlevel: the highest level of the
+        whole domain (default: of these blocks)."""
         self.params = params
         self.blocks_np = blocks
         self.nbr_np = nbr
@@ -156,16 +153,13 @@ class FxGrid:
             emf_arrays = self.maxlevel > 0
         self.E = torch.zeros((3, N), dtype=torch.float64, device=dev) if emf_arrays else None
         self.queue = torch.zeros(2 * QSLOTS, dtype=torch.int32, device=dev) if persistent else None
-        ncap = self.items["cell"].shape[0] * CHUNK
-        self.c2p_defer = (torch.zeros(2 + 2 * ncap, dtype=torch.int32, device=dev)
-                          if defer_c2p and params.precision == "mixed" else None)
         self._refresh()
 
     @classmethod
     def uniform(cls, lo: float, hi: float, N: int, block: int, params: FxParams, periodic=False, device="cuda",
-                emf_arrays=None, persistent=False, defer_c2p=True):
+                emf_arrays=None, persistent=False):
         blocks, nbr = uniform_blocks(lo, hi, N, block, periodic)
-        return cls(blocks, nbr, params, device, emf_arrays, persistent, defer_c2p)
+        return cls(blocks, nbr, params, device, emf_arrays, persistent)
 
     @classmethod
     def leveled(cls, lo: float, hi: float, level: np.ndarray, n0: int, params: FxParams, device="cuda",
@@ -182,8 +176,7 @@ class FxGrid:
                            _ptr(it["ghost"]), it["ghost"].shape[0], self.ncell,
                            _ptr(self.U), _ptr(self.U1), _ptr(self.W), _ptr(self.Bf), _ptr(self.Bf1), _ptr(self.F),
                            _ptr(self.dt), _ptr(self.count), _ptr(self.err), _ptr(self.E), self.maxlevel, 0, _ptr(self.queue),
-                           _ptr(it["flux"]), it["flux"].shape[0], self.ghost_depth, _ptr(self.c2p_defer),
-                           0 if self.c2p_defer is None else (self.c2p_defer.numel() - 2) // 2)
+                           _ptr(it["flux"]), it["flux"].shape[0], self.ghost_depth)
         self._p = self.params.cstruct()
 
     @property

@@ -192,7 +192,6 @@ int fx_bad(const bh_fx_params* P, const bh_fx_grid* g) {
     if (P->limiter < BH_MINMOD || P->limiter > BH_PPM || (g->ghost_depth != 0 && g->ghost_depth != 2 && g->ghost_depth != 3) ||
         (P->limiter == BH_PPM && g->ghost_depth != 3) || (g->nitem_flux > 0 && !g->items_flux))
         return 1;
-    if (g->c2p_defer && (int64_t)g->c2p_defer_cap < (int64_t)g->nitem_cell * BH_FX_CHUNK) return 1;
     return 0;
 }
 }  // namespace

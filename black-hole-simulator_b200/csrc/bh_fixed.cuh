@@ -244,12 +244,13 @@ __device__ inline void c2p_inputs(const Grid& G, const bh_fx_block& B, int i, in
 
 // con2prim + floors + excision on every interior cell.  The mixed variant
 // solves in FP32 beyond r ~ FX_R_FP64 where the FP32 residual is well
-// conditioned; the other cells take the FP64 path -- inline, or (DEFER)
-// appended to the list defer = [count, done, (block, cell)...] for
-// k_fx_c2p_deferred, which keeps this kernel's registers to the FP32 path's
-template <typename RT, typename WT, int MINB, bool DEFER>
+// conditioned; the other cells take the FP64 path.  (Handing those cells
+// to a second kernel through a list, which leaves this one the FP32 path's
+// registers, measured slower: the extra launch costs more than the
+// registers save.)
+template <typename RT, typename WT, int MINB>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const int32_t* items, int stage,
-                                                       int with_dt, Queue Q, int32_t* defer) {
+                                                       int with_dt, Queue Q) {
     for_items(Q, [&](int t) FX_INLINE {
         const int32_t b = items[2 * t];
         const bh_fx_block B = G.blk[b];
@@ -268,47 +269,13 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
                 full = c2p_cell_fp32(P, G, B, c, x, Bt, U, with_dt, dtc);
                 if (full) atomicAdd(&G.count[2], 1);
             }
-            if (full) {
-                if (DEFER) {
-                    const int q = atomicAdd(&defer[0], 1);
-                    defer[2 + 2 * q] = b;
-                    defer[3 + 2 * q] = e;
-                } else {
-                    dtc = c2p_cell_fp64<RT, WT>(P, G, B, c, x, Bt, U, with_dt);
-                }
-            }
+            if (full) dtc = c2p_cell_fp64<RT, WT>(P, G, B, c, x, Bt, U, with_dt);
         }
         if (with_dt) {
             for (int o = 16; o > 0; o >>= 1) dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
             if ((threadIdx.x & 31) == 0 && dtc < 1e300) atomic_min_pos(G.dt, dtc);
         }
     });
-}
-
-// the FP64 path of the cells k_fx_c2p deferred; the last CTA to finish
-// clears the list for the next launch
-template <typename RT, typename WT>
-__global__ void __launch_bounds__(FX_TPB) k_fx_c2p_deferred(FxPar P, Grid G, int stage, int with_dt, int32_t* defer) {
-    const int cnt = *(volatile int32_t*)&defer[0];
-    for (int q = blockIdx.x * FX_TPB + threadIdx.x; q < cnt; q += gridDim.x * FX_TPB) {
-        const int32_t b = defer[2 + 2 * q], e = defer[3 + 2 * q];
-        const bh_fx_block B = G.blk[b];
-        const int n = B.n;
-        const int i = e / (n * n), j = (e / n) % n, k = e % n;
-        double x[3], Bt[3];
-        c2p_inputs(G, B, i, j, k, stage, x, Bt);
-        const double dtc = c2p_cell_fp64<RT, WT>(P, G, B, bidx(B, i, j, k), x, Bt, stage ? G.U1 : G.U, with_dt);
-        if (with_dt && dtc < 1e300) atomic_min_pos(G.dt, dtc);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        if (atomicAdd(&defer[1], 1) == (int)gridDim.x - 1) {
-            defer[0] = 0;
-            defer[1] = 0;
-            __threadfence();
-        }
-    }
 }
 
 // ======================================================================
@@ -1162,14 +1129,8 @@ int fx_prims(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, int32_t 
     fx::FxPar p = fx::par_of(P);
     fx::Grid G = fx::grid_of(g);
     if (with_dt) fx::k_fx_dt_init<<<1, 1, 0, fxs(s)>>>(g->dt);
-    constexpr bool MIXED = sizeof(FRT) < sizeof(double);
-    if (g->nitem_cell && MIXED && g->c2p_defer) {
-#define L_(M) fx::k_fx_c2p<FRT, FRT, M, true><<<fx_grid((const void*)fx::k_fx_c2p<FRT, FRT, M, true>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt, fx_q(g, QS_C2P, g->nitem_cell), g->c2p_defer)
-        FX_TUNED(BH_FX_TUNE_C2P, L_)
-#undef L_
-        fx::k_fx_c2p_deferred<FRT, FRT><<<fx_sms(), fx::FX_TPB, 0, fxs(s)>>>(p, G, stage, with_dt, g->c2p_defer);
-    } else if (g->nitem_cell) {
-#define L_(M) fx::k_fx_c2p<FRT, FRT, M, false><<<fx_grid((const void*)fx::k_fx_c2p<FRT, FRT, M, false>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt, fx_q(g, QS_C2P, g->nitem_cell), nullptr)
+    if (g->nitem_cell) {
+#define L_(M) fx::k_fx_c2p<FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_c2p<FRT, FRT, M>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, with_dt, fx_q(g, QS_C2P, g->nitem_cell))
         FX_TUNED(BH_FX_TUNE_C2P, L_)
 #undef L_
     }

@@ -460,11 +460,6 @@ typedef struct bh_fx_grid {
     int32_t ghost_depth;         /* ghost layers the fill covers (and items_ghost
                                     lists): 2 (0 reads as 2), or 3, which BH_PPM
                                     requires                                        */
-    int32_t *c2p_defer;          /* BH_MIXED only, or NULL: device [2 + 2 cap],
-                                    zeroed once; cells whose con2prim needs FP64
-                                    are listed here by the FP32 kernel and solved by
-                                    a second one (the list clears itself)          */
-    int32_t c2p_defer_cap;       /* at least nitem_cell * BH_FX_CHUNK                */
 } bh_fx_grid;
 #define BH_FX_QSLOTS 6
 

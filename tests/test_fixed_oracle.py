@@ -466,3 +466,36 @@ def _contact_error(N, limiter, v=0.5, t_end=0.4):
 def test_ppm_keeps_a_contact_sharper_than_plm():
     e = {lim: _contact_error(32, lim) for lim in ("minmod", "mc", "ppm")}
     assert e["ppm"] < e["mc"] < e["minmod"], e
+
+
+def test_con2prim_from_the_previous_primitives_needs_about_two_evaluations():
+    """On the torus the step's con2prim starts from the previous step's
+    primitives and converges in about two residual evaluations per cell (the
+    least a Newton stop test allows is one), against over four from a cold
+    start (the floor state at rest) and twelve inside the torus: a learned
+    initial guess has at most one evaluation per cell to save here."""
+    prm = ofx.params(Prm())
+    n, G = 32, 3
+    blocks, nbr = uniform_blocks(-40.0, 40.0, n, n)
+    h = ofx.FxHost(blocks, nbr, prm)
+    h.torus_init()
+    for _ in range(3):
+        h.step()
+    w_prev = h.W.copy()
+    h.step()
+    S = n + 2 * G + 1
+
+    def inner(a):
+        return a.reshape(a.shape[0], S, S, S)[:, G:G + n, G:G + n, G:G + n].reshape(a.shape[0], -1)
+    U, W, Wo = inner(h.U), inner(h.W), inner(w_prev)
+    c = -40.0 + (np.arange(n) + 0.5) * 80.0 / n
+    X, Y, Z = (v.ravel() for v in np.meshgrid(c, c, c, indexing="ij"))
+    sel = np.sqrt(X * X + Y * Y + Z * Z) > 2.0       # outside the excised region
+    torus = W[0][sel] > 1e-3
+    _, st, it = ofx.con2prim(prm, X[sel], Y[sel], Z[sel], U[:, sel], W[5:8, sel], Wo[:, sel])
+    cold = Wo[:, sel].copy()
+    cold[0], cold[1], cold[2:5] = 1e-6, 1e-8, 0.0
+    _, st_c, it_c = ofx.con2prim(prm, X[sel], Y[sel], Z[sel], U[:, sel], W[5:8, sel], cold)
+    assert (st == 0).all() and (st_c == 0).all()
+    assert it.mean() < 2.2 and it[torus].mean() < 2.2, (it.mean(), it[torus].mean())
+    assert it_c.mean() > 4.0 and it_c[torus].mean() > 8.0, (it_c.mean(), it_c[torus].mean())

@@ -396,32 +396,6 @@ def test_ppm_mixed_torus_within_1e_5_of_fp64():
     assert a.counters()["c2p_failures"] == 0
 
 
-def test_mixed_deferred_con2prim_equals_inline():
-    """the mixed variant's FP64 con2prim cells (near the hole, and where the
-    FP32 residual is ill conditioned) solved by the second kernel from the
-    deferral list = solved inline (relative L-infinity <= 1e-6 per array
-    after five steps: the two kernels may contract differently); the list
-    clears itself"""
-    from bhgpu.fixed import FxGrid, FxParams
-    a = FxGrid.uniform(-40.0, 40.0, 64, 64, FxParams(precision="mixed"), defer_c2p=True)
-    b = FxGrid.uniform(-40.0, 40.0, 64, 64, FxParams(precision="mixed"), defer_c2p=False)
-    assert a.c2p_defer is not None and b.c2p_defer is None
-    a.torus_init()
-    b.torus_init()
-    for _ in range(5):
-        a.step()
-        b.step()
-    torch.cuda.synchronize()
-    for name in ("U", "Bf", "W"):
-        x, y = getattr(a, name).double().cpu().numpy(), getattr(b, name).double().cpu().numpy()
-        for v in range(x.shape[0]):
-            assert _rel_linf(x[v], y[v]) <= 1e-6, (name, v)
-    assert int(a.c2p_defer[:2].abs().sum().item()) == 0
-    ca, cb = a.counters(), b.counters()
-    assert ca["c2p_fp64_fallback"] == cb["c2p_fp64_fallback"] and ca["c2p_failures"] == cb["c2p_failures"] == 0
-    assert a.time_step() == pytest.approx(b.time_step(), rel=1e-6)
-
-
 def test_sharded_pieces_on_one_rank_equal_the_step():
     """bhgpu.fxshard on a one-rank group: the step as separate pieces (ghost
     fill pass by pass, raw EMFs, correction + update; bh_fx_ghost_pass,
