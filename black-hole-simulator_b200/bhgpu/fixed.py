@@ -114,14 +114,15 @@ class FxGrid:
     """
 
     def __init__(self, blocks: np.ndarray, nbr: np.ndarray, params: FxParams, device="cuda", emf_arrays=None,
-                 persistent=False, nactive=None, maxlevel=None):
+                 persistent=False, nactive=None, maxlevel=None, tile_min=TILE_MIN):
         """emf_arrays: keep the edge EMFs in arrays (required, and the
         default, when blocks have different levels; otherwise they are
         computed on the fly by the update).  persistent: launch the step
         kernels as persistent CTAs fed by a device work queue.  nactive:
         the kernels work on blocks[:nactive] only (the rest are neighbours'
         copies, as in a sharded grid); maxlevel: the highest level of the
-        whole domain (default: of these blocks)."""
+        whole domain (default: of these blocks); tile_min: the smallest
+        block the staged flux kernel tiles."""
         self.params = params
         self.blocks_np = blocks
         self.nbr_np = nbr
@@ -135,7 +136,7 @@ class FxGrid:
         act = blocks[:self.nactive]
         self.items = {k: torch.from_numpy(work_items(act, k, self.ghost_depth)).to(dev)
                       for k in ("cell", "pos", "ghost")}
-        self.items["flux"] = torch.from_numpy(flux_items(act)).to(dev)
+        self.items["flux"] = torch.from_numpy(flux_items(act, tile_min)).to(dev)
         wdt = torch.float32 if params.precision == "mixed" else torch.float64
         N = self.ncell
         self.U = torch.zeros((8, N), dtype=torch.float64, device=dev)
@@ -163,11 +164,11 @@ class FxGrid:
 
     @classmethod
     def leveled(cls, lo: float, hi: float, level: np.ndarray, n0: int, params: FxParams, device="cuda",
-                persistent=False):
+                persistent=False, tile_min=TILE_MIN):
         """Equal cubes over [lo, hi]^3 with per-cube levels (n0 2^level cells
         per axis), e.g. bhgrid.blocks.torus_levels()."""
         blocks, nbr = leveled_blocks(lo, hi, level, n0)
-        return cls(blocks, nbr, params, device, persistent=persistent)
+        return cls(blocks, nbr, params, device, persistent=persistent, tile_min=tile_min)
 
     def _refresh(self):
         it = self.items
