@@ -748,6 +748,23 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_emf_fix(Grid G, const int32_t* it
     });
 }
 
+// interior cell e of an n^3 block for the update: where n is a multiple of
+// 32, a 128-cell item is a 4 (j) x 32 (k) tile of one i-plane, so the rows
+// j-1 .. j+1 of the EMF stencil are shared within the CTA (L1) and each warp
+// still reads one row of 32 consecutive cells; else i, j, k in order
+__device__ inline void update_cell(int n, int e, int& i, int& j, int& k) {
+    if ((n & 31) == 0) {
+        const int nn = n * n, r = e % nn, t = r >> 7, l = r & 127, nt = n >> 5;
+        i = e / nn;
+        j = (t / nt) * 4 + (l >> 5);
+        k = (t % nt) * 32 + (l & 31);
+    } else {
+        i = e / (n * n);
+        j = (e / n) % n;
+        k = e % n;
+    }
+}
+
 template <typename RT, typename WT, typename FT, int MINB>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, const int32_t* items, int stage,
                                                       double cfl, Queue Q) {
@@ -757,7 +774,8 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, con
         const int n = B.n;
         const int e = items[2 * t + 1] + threadIdx.x;
         if (e >= n * n * n) return;
-        const int i = e / (n * n), j = (e / n) % n, k = e % n;
+        int i, j, k;
+        update_cell(n, e, i, j, k);
         const int64_t N = G.ncell;
         const int64_t c = bidx(B, i, j, k);
         const int si = bstride_i(B), sj = bstride_j(B), sk = 1;
