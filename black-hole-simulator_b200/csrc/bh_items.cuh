@@ -602,6 +602,25 @@ BH_HD inline void ghost_copy_item(const Pool& P, int p, int e) {
     double2 x[8];
 #pragma unroll
     for (int v = 0; v < 8; v++) x[v] = *reinterpret_cast<const double2*>(src + (size_t)v * NC + la);
+    if (dim == 2) {
+        // A k-strip pair is half of a 32-byte sector (rows of CPN = 20
+        // doubles start on sector boundaries); the other half is the row's
+        // own two interior cells next to it, which this kernel never changes.
+        // Writing them back with the pair makes every store a whole sector
+        // (no partial-sector read-modify-write below L2).
+        const int lo = side == 1 ? lg - 2 : lg + 2;   // the interior pair of the sector
+        double2 own[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) own[v] = *reinterpret_cast<const double2*>(dst + (size_t)v * NC + lo);
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+            double2 y = swap ? make_double2(x[v].y, x[v].x) : x[v];
+            double2* row = reinterpret_cast<double2*>(dst + (size_t)v * NC + (side == 1 ? lo : lg));
+            row[0] = side == 1 ? own[v] : y;
+            row[1] = side == 1 ? y : own[v];
+        }
+        return;
+    }
 #pragma unroll
     for (int v = 0; v < 8; v++) {
         double2 y = swap ? make_double2(x[v].y, x[v].x) : x[v];
