@@ -74,72 +74,42 @@ def work_items(blocks: np.ndarray, kind: str, depth: int = 2) -> np.ndarray:
     return np.concatenate(out).astype(np.int32)
 
 
-# tiles of the staged flux kernel: TILE positions (i, j, k) per tile over a
-# block's interior positions [0, n)^3 (n a multiple of 8, at least
-# TILE_MIN), plus chunks of the one-position shell around them (item
-# SHELL + first index); smaller blocks keep chunks of their whole position
-# box (item -(first index) - 1)
+# tiles of the staged flux kernel: TILE positions (i, j, k) per tile; blocks
+# below TILE_MIN cells per axis keep chunks of positions (a tile box of n + 2
+# positions per axis wastes up to (ceil((n+2)/T) T / (n+2)) of its threads)
 TILE = (4, 4, 8)
 TILE_MIN = 64
-SHELL = 1 << 30
-
-
-def _tiled(n: int, tile_min: int) -> bool:
-    return n >= tile_min and n % TILE[0] == 0 and n % TILE[1] == 0 and n % TILE[2] == 0
 
 
 def flux_items(blocks: np.ndarray, tile_min: int = TILE_MIN) -> np.ndarray:
-    """(block, e) work items of the staged flux kernel: for a block with n >=
-    tile_min, its tiles (0 <= e < SHELL: tile (ti, tj, tk) -> (ti nj + tj) nk +
-    tk over [0, n)^3, nj = n / 4, nk = n / 8) and the CHUNK-position pieces
-    of the shell [-1, n]^3 minus [0, n)^3 (e = SHELL + first index); for a
-    smaller block, the CHUNK positions of [-1, n]^3 from -(e + 1) on."""
+    """(block, e) work items of the staged flux kernel: e >= 0 is tile e of a
+    block with n >= tile_min (tile (ti, tj, tk) -> (ti nj + tj) nk + tk over
+    the position box [-1, n]^3), e < 0 the CHUNK positions from -(e + 1) on
+    of a smaller block."""
     out = []
     for b, n in enumerate(blocks["n"]):
         n = int(n)
         m = n + 2
-        if _tiled(n, tile_min):
-            nt = (n // TILE[0]) * (n // TILE[1]) * (n // TILE[2])
-            e = np.concatenate([np.arange(nt), SHELL + np.arange(0, m ** 3 - n ** 3, CHUNK)]).astype(np.int32)
+        if n >= tile_min:
+            nt = -(-m // TILE[0]) * -(-m // TILE[1]) * -(-m // TILE[2])
+            e = np.arange(nt, dtype=np.int32)
         else:
             e = -np.arange(0, m ** 3, CHUNK, dtype=np.int32) - 1
         out.append(np.stack([np.full_like(e, b), e], 1))
     return np.concatenate(out).astype(np.int32)
 
 
-def _shell_position(n: int, e: int):
-    """position of the e-th entry of the one-position shell around [0, n)^3
-    (the kernel's shell_decode with one layer), or None past its end"""
-    m, h = n + 2, 2
-    s1, s2, s3 = h * m * m, h * n * m, h * n * n
-    side = lambda q: -1 if q < 1 else n  # noqa: E731
-    if e < s1:
-        return side(e // (m * m)), (e % (m * m)) // m - 1, e % m - 1
-    e -= s1
-    if e < s2:
-        q, r = e // (n * m), e % (n * m)
-        return r // m, side(q), r % m - 1
-    e -= s2
-    if e < s3:
-        q, r = e // (n * n), e % (n * n)
-        return r // n, r % n, side(q)
-    return None
-
-
 def flux_item_positions(n: int, e: int) -> np.ndarray:
     """Positions (i, j, k) in [-1, n]^3 that item e of a block of n cells
-    covers (the kernel's decode)."""
+    covers (the kernel's decode; positions beyond n are masked)."""
     m = n + 2
     if e < 0:
         idx = np.arange(-(e + 1), min(-(e + 1) + CHUNK, m ** 3))
         return np.stack([idx // (m * m) - 1, (idx // m) % m - 1, idx % m - 1], 1)
-    if e >= SHELL:
-        pos = [_shell_position(n, e - SHELL + t) for t in range(CHUNK)]
-        return np.array([p for p in pos if p is not None], np.int64).reshape(-1, 3)
-    nj, nk = n // TILE[1], n // TILE[2]
-    o = ((e // (nj * nk)) * TILE[0], ((e // nk) % nj) * TILE[1], (e % nk) * TILE[2])
+    nj, nk = -(-m // TILE[1]), -(-m // TILE[2])
+    o = (-1 + (e // (nj * nk)) * TILE[0], -1 + ((e // nk) % nj) * TILE[1], -1 + (e % nk) * TILE[2])
     g = np.stack(np.meshgrid(*[np.arange(o[d], o[d] + TILE[d]) for d in range(3)], indexing="ij"), -1).reshape(-1, 3)
-    return g
+    return g[(g <= n).all(1)]
 
 
 def interior(blocks: np.ndarray, arr: np.ndarray) -> np.ndarray:

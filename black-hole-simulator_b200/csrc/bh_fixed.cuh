@@ -538,13 +538,10 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux(FxPar P, Grid G, const
 // into shared memory with coalesced loads along k, then computes the
 // x-, y- and z-faces of every position from there: each primitive is read
 // from L2 once per tile instead of once per face that uses it.  The work
-// items (block, e) are tiles of the block's interior positions [0, n)^3
-// (0 <= e < FX_SHELL; n a multiple of 8, so the tiles fit exactly), chunks
-// of 128 positions of the one-position shell around them (e >= FX_SHELL:
-// the transverse layer of the EMFs and the upper normal faces), or, for
-// blocks too small to tile well, chunks of 128 positions of the whole
-// position box [-1, n]^3 starting at -(e + 1), as in k_fx_flux.  The
-// arithmetic is that of k_fx_flux: the same bits.
+// items (block, e) are tiles (e >= 0, tile e of the block's position box
+// [-1, n]^3) or, for blocks too small to tile well, chunks of 128
+// positions starting at -(e + 1) as in k_fx_flux.  The arithmetic is that
+// of k_fx_flux: the same bits.
 // ----------------------------------------------------------------------
 constexpr int FX_TI = 4, FX_TJ = 4, FX_TK = 8;
 constexpr int FX_HI = FX_TI + 3, FX_HJ = FX_TJ + 3, FX_HK = FX_TK + 3;   // -2 .. T per axis
@@ -553,7 +550,6 @@ constexpr int FX_NX = FX_HI * FX_TJ * FX_TK;   // the tile and its x-halo
 constexpr int FX_NY = FX_TI * 3 * FX_TK;       // y-halo: j = -2, -1, TJ
 constexpr int FX_NZ = FX_TI * FX_TJ * 3;       // z-halo: k = -2, -1, TK
 constexpr int FX_NCROSS = FX_NX + FX_NY + FX_NZ;
-constexpr int32_t FX_SHELL = 1 << 30;
 static_assert(FX_TI * FX_TJ * FX_TK == FX_TPB, "one thread per tile position");
 
 // offsets (a, b, c) in [-2, T] of the q-th cell of the cross-shaped halo
@@ -581,22 +577,18 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux_tile(FxPar P, Grid G, 
         const int n = B.n, m = n + 2;
         const double* Bfs = stage ? G.Bf1 : G.Bf;
         const int32_t e0 = items[2 * t + 1];
-        if (e0 < 0 || e0 >= FX_SHELL) {   // a chunk of positions, as in k_fx_flux
-            int i, j, k;
-            if (e0 < 0) {
-                const int e = -(e0 + 1) + threadIdx.x;
-                if (e >= m * m * m) return;
-                i = e / (m * m) - 1; j = (e / m) % m - 1; k = e % m - 1;
-            } else if (!shell_decode(n, 1, e0 - FX_SHELL + threadIdx.x, i, j, k)) {
-                return;
-            }
+        if (e0 < 0) {   // a chunk of positions, as in k_fx_flux
+            const int e = -(e0 + 1) + threadIdx.x;
+            if (e >= m * m * m) return;
+            const int i = e / (m * m) - 1, j = (e / m) % m - 1, k = e % m - 1;
             if (i >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 0, Bfs);
             if (j >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 1, Bfs);
             if (k >= 0) face_flux<RT, WT, FT>(P, G, B, i, j, k, 2, Bfs);
             return;
         }
-        const int nj = n / FX_TJ, nk = n / FX_TK;
-        const int i0 = (e0 / (nj * nk)) * FX_TI, j0 = ((e0 / nk) % nj) * FX_TJ, k0 = (e0 % nk) * FX_TK;
+        const int nj = (m + FX_TJ - 1) / FX_TJ, nk = (m + FX_TK - 1) / FX_TK;
+        const int i0 = -1 + (e0 / (nj * nk)) * FX_TI, j0 = -1 + ((e0 / nk) % nj) * FX_TJ,
+                  k0 = -1 + (e0 % nk) * FX_TK;
         const int64_t N = G.ncell;
         const WT* W = (const WT*)G.W;
         __syncthreads();   // the previous tile's reads of sW are done
@@ -614,13 +606,17 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux_tile(FxPar P, Grid G, 
         __syncthreads();
         const int a = threadIdx.x / (FX_TJ * FX_TK), bb = (threadIdx.x / FX_TK) % FX_TJ, c = threadIdx.x % FX_TK;
         const int i = i0 + a, j = j0 + bb, k = k0 + c;
-        if (i >= n || j >= n || k >= n) return;   // (tiles fit n exactly)
+        if (i > n || j > n || k > n) return;
         const int o = box_at(a, bb, c);
         // (PLM only: the launch keeps PPM's wider stencil on k_fx_flux)
-        face_flux_at<RT, FT, false>(P, G, B, i, j, k, 0, Bfs,
-                                    [&](int v, int s) { return RT(sW[v][o + s * (FX_HJ * FX_HK)]); });
-        face_flux_at<RT, FT, false>(P, G, B, i, j, k, 1, Bfs, [&](int v, int s) { return RT(sW[v][o + s * FX_HK]); });
-        face_flux_at<RT, FT, false>(P, G, B, i, j, k, 2, Bfs, [&](int v, int s) { return RT(sW[v][o + s]); });
+        if (i >= 0)
+            face_flux_at<RT, FT, false>(P, G, B, i, j, k, 0, Bfs,
+                                        [&](int v, int s) { return RT(sW[v][o + s * (FX_HJ * FX_HK)]); });
+        if (j >= 0)
+            face_flux_at<RT, FT, false>(P, G, B, i, j, k, 1, Bfs,
+                                        [&](int v, int s) { return RT(sW[v][o + s * FX_HK]); });
+        if (k >= 0)
+            face_flux_at<RT, FT, false>(P, G, B, i, j, k, 2, Bfs, [&](int v, int s) { return RT(sW[v][o + s]); });
     });
 }
 
@@ -748,23 +744,6 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_emf_fix(Grid G, const int32_t* it
     });
 }
 
-// interior cell e of an n^3 block for the update: where n is a multiple of
-// 32, a 128-cell item is a 4 (j) x 32 (k) tile of one i-plane, so the rows
-// j-1 .. j+1 of the EMF stencil are shared within the CTA (L1) and each warp
-// still reads one row of 32 consecutive cells; else i, j, k in order
-__device__ inline void update_cell(int n, int e, int& i, int& j, int& k) {
-    if ((n & 31) == 0) {
-        const int nn = n * n, r = e % nn, t = r >> 7, l = r & 127, nt = n >> 5;
-        i = e / nn;
-        j = (t / nt) * 4 + (l >> 5);
-        k = (t % nt) * 32 + (l & 31);
-    } else {
-        i = e / (n * n);
-        j = (e / n) % n;
-        k = e % n;
-    }
-}
-
 template <typename RT, typename WT, typename FT, int MINB>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, const int32_t* items, int stage,
                                                       double cfl, Queue Q) {
@@ -774,8 +753,7 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, con
         const int n = B.n;
         const int e = items[2 * t + 1] + threadIdx.x;
         if (e >= n * n * n) return;
-        int i, j, k;
-        update_cell(n, e, i, j, k);
+        const int i = e / (n * n), j = (e / n) % n, k = e % n;
         const int64_t N = G.ncell;
         const int64_t c = bidx(B, i, j, k);
         const int si = bstride_i(B), sj = bstride_j(B), sk = 1;

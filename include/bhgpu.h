@@ -450,16 +450,12 @@ typedef struct bh_fx_grid {
                                     themselves at the end of each launch).  NULL: one
                                     CTA per work item.  Both give the same results. */
     const int32_t *items_flux;   /* device [nitem_flux][2] (block, e), or NULL/0: the work
-                                    of the staged flux kernel.  0 <= e < 2^30: tile e
-                                    of the block's interior positions [0, n)^3 (n a
-                                    multiple of 8), tiles of 4 x 4 x 8 positions (i,
-                                    j, k), index (ti * nj + tj) * nk + tk with nj =
-                                    n/4, nk = n/8; e >= 2^30: the 128 positions from
-                                    e - 2^30 on of the one-position shell [-1, n]^3
-                                    minus [0, n)^3 (the ghost shell's order with one
-                                    layer); e < 0: the 128 positions from -(e+1) on of
-                                    [-1, n]^3, as in items_pos
-                                    (bhgrid.blocks.flux_items builds it)            */
+                                    of the staged flux kernel.  e >= 0: tile e of the
+                                    block's position box [-1, n]^3, tiles of 4 x 4 x 8
+                                    positions (i, j, k), tile index (ti * nj + tj) * nk
+                                    + tk with nj = ceil((n+2)/4), nk = ceil((n+2)/8);
+                                    e < 0: the 128 positions from -(e+1) on, as in
+                                    items_pos (bhgrid.blocks.flux_items builds it)  */
     int32_t nitem_flux;
     int32_t ghost_depth;         /* ghost layers the fill covers (and items_ghost
                                     lists): 2 (0 reads as 2), or 3, which BH_PPM

@@ -24,8 +24,7 @@ def test_flux_items_cover_every_position_once(n):
     assert ((items[:, 1] >= 0) == tiled).all()
     if tiled:
         m = n + 2
-        ntile = (n // TILE[0]) * (n // TILE[1]) * (n // TILE[2])
-        assert len(items) == ntile + -(-(m ** 3 - n ** 3) // CHUNK)
+        assert len(items) == -(-m // TILE[0]) * -(-m // TILE[1]) * -(-m // TILE[2])
     else:
         assert len(items) == -(-(n + 2) ** 3 // CHUNK)
     assert (_covered(n, items) == 1).all()
