@@ -170,21 +170,19 @@ int bh_prims(const bh_params *P, const bh_pool *pool, void *stream);
 int bh_ghosts_prims(const bh_params *P, const bh_pool *pool, void *stream);
 /* No counterpart in the reference (it allocates nothing on a GPU): the
  * ghost fill and reconstruction of bh_ghosts_prims for callers that cannot
- * allocate device memory -- a host that records the time step into a CUDA
- * graph (cudaMalloc is not allowed while a stream is being captured) or
- * one whose memory arena owns every device byte and lends libraries none.
+ * allocate device memory -- e.g. one whose memory arena owns every device
+ * byte and lends libraries none.
  * The per-cell con2prim outcome that bh_ghosts_prims keeps in the caller's
  * pool->status is kept instead in a scratch array inside this library,
  * BH_STATIC_MAX_PATCHES x 8000 bytes (8 MB), which every GPU that loads
  * the library holds until the process exits; pool->status is ignored.
  * Nothing is allocated or freed; pools of more than BH_STATIC_MAX_PATCHES
  * patches are rejected with BH_ERANGE before anything is launched.
- * Every call made while its stream is not being captured looks up the
- * array's device address on the current device (cudaGetSymbolAddress), so
- * the address stays right after a device reset; a call made during a stream
- * capture reuses the address the last such call found on that device, so
- * make a first call on each device before any stream capture (BH_ECUDA
- * otherwise).  Every call uses the same array and leaves its
+ * A call whose stream is not capturing looks up the array's device address
+ * on the current device (cudaGetSymbolAddress), so the address stays right
+ * after a device reset; a call whose stream is capturing takes the address
+ * the last such lookup found on that device (BH_ECUDA if there was none).
+ * Every call uses the same array and leaves its
  * contents behind; each call writes every entry it later reads, so nothing
  * needs clearing, but calls that overlap on the GPU (concurrent streams)
  * race on the array.  Results equal bh_ghosts_prims bit for bit. */

@@ -1,7 +1,6 @@
 """bh_ghosts_prims_static: the ghost fill and reconstruction for callers
-that cannot allocate device memory (a host recording its time step into a
-CUDA graph, where cudaMalloc is not allowed during capture, or a host whose
-memory arena lends libraries no device memory).  It keeps its per-cell
+that cannot allocate device memory (a host whose memory arena lends
+libraries no device memory, for instance).  It keeps its per-cell
 scratch in an array inside the library instead of the caller's
 pool->status.
 
