@@ -60,7 +60,7 @@ STEP_BYTES = 296          # algorithmic HBM bytes per zone-update of an RK2 step
 LAUNCHES_PER_STEP = 9     # dt init, then con2prim, ghosts, fluxes, update per stage
 # DRAM bytes (read + write) per launch of the mixed variant's step kernels at
 # 128^3, from the ncu capture summarised in profiles/kernels_torus_128cube.md
-PROFILED_TRAFFIC = {"fluxes": 154.88e6 + 173.99e6, "update": 542.57e6 + 122.21e6, "prims": 190.09e6 + 135.60e6}
+PROFILED_TRAFFIC = {"fluxes": 154.77e6 + 173.75e6, "update": 542.67e6 + 123.91e6, "prims": 190.97e6 + 143.72e6}
 E2E_DEPTH = 3
 
 
