@@ -28,7 +28,7 @@ from ._lib import BH_FP64, BH_FP64_FMA, BH_MIXED, BH_MC, BH_MINMOD, BH_PPM, BH_V
 
 _vp, _d, _i32, _i64 = C.c_void_p, C.c_double, C.c_int32, C.c_int64
 GHOST = 2
-QSLOTS = 6           # BH_FX_QSLOTS
+QSLOTS = 7           # BH_FX_QSLOTS
 PRECISIONS = {"fp64": BH_FP64, "fp64-fma": BH_FP64_FMA, "mixed": BH_MIXED}
 LIMITERS = {"minmod": BH_MINMOD, "vanleer": BH_VANLEER, "mc": BH_MC, "ppm": BH_PPM}
 
@@ -347,7 +347,7 @@ class FxHostPipeline:
 # ---------------------------------------------------------------------------
 # launch-bound autotuning of the scheme's heavy kernels (bh_fx_tune_*)
 TUNE_KERNELS = ("c2p", "flux", "update")
-TUNE_KNOBS = TUNE_KERNELS + ("stage",)   # "stage": 1 = the staged flux kernel
+TUNE_KNOBS = TUNE_KERNELS + ("stage", "split")   # 1 = the staged flux kernel; the update as two kernels
 TUNE_CANDIDATES = (1, 3, 4, 5, 6, 7, 8)
 lib.bh_fx_tune_set.argtypes = [_i32, _i32, _i32]
 lib.bh_fx_tune_get.argtypes = [_i32, _i32, C.POINTER(_i32)]
@@ -356,7 +356,7 @@ lib.bh_fx_tune_get.restype = C.c_int
 
 
 def tune_set(precision: str, kernel: str, ctas: int):
-    """kernel in TUNE_KERNELS: resident CTAs per SM (1, 3..8); "stage": 0/1."""
+    """kernel in TUNE_KERNELS: resident CTAs per SM (1, 3..8); "stage", "split": 0/1."""
     check(lib.bh_fx_tune_set(PRECISIONS[precision], TUNE_KNOBS.index(kernel), ctas), "bh_fx_tune_set")
 
 
@@ -371,13 +371,15 @@ def autotune(grid: FxGrid, reps: int = 4, candidates=TUNE_CANDIDATES) -> dict:
     the flux stencil is staged in shared memory, for the grid's variant: for
     one kernel at a time (the others held), every candidate times `reps` RK2
     steps (CUDA events) from the same saved state; the fastest is kept (the
-    flux candidates are the pairs (staged, launch bound); staging is tried
-    only where the grid has blocks of TILE_MIN cells per axis or more).  The
+    flux candidates are the pairs (staged, launch bound), the update's the
+    pairs (split in two kernels, launch bound); staging is tried only where
+    the grid has blocks of TILE_MIN cells per axis or more).  The
     grid's state is restored.  In the FP64 variant every choice gives the
     same bits (no contraction); in the contracted variants ptxas may pair
     multiply-adds differently under another register budget, which moves
     results by ulps.  Returns {"choice": {knob: value}, "ms": {kernel:
-    {candidate: ms per step}}} (flux candidates keyed "s<stage>/<ctas>")."""
+    {candidate: ms per step}}} (flux and update candidates keyed
+    "s<stage or split>/<ctas>")."""
     saved = [t.clone() for t in (grid.U, grid.W, grid.Bf)]
     prec = grid.precision
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -399,15 +401,16 @@ def autotune(grid: FxGrid, reps: int = 4, candidates=TUNE_CANDIDATES) -> dict:
 
     for k in TUNE_KERNELS:
         times = {}
-        if k == "flux":
-            for st in ((0, 1) if tiled else (0,)):
+        if k in ("flux", "update"):
+            knob = "stage" if k == "flux" else "split"
+            for st in ((0, 1) if (tiled or k == "update") else (0,)):
                 for c in candidates:
-                    times[f"s{st}/{c}"] = timed(lambda: (tune_set(prec, "stage", st), tune_set(prec, k, c)))
+                    times[f"s{st}/{c}"] = timed(lambda: (tune_set(prec, knob, st), tune_set(prec, k, c)))
             best = min(times, key=times.get)
             st, c = best[1:].split("/")
-            tune_set(prec, "stage", int(st))
+            tune_set(prec, knob, int(st))
             tune_set(prec, k, int(c))
-            out["choice"]["stage"] = int(st)
+            out["choice"][knob] = int(st)
             out["choice"][k] = int(c)
         else:
             for c in candidates:

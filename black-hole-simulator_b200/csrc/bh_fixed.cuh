@@ -744,7 +744,11 @@ __global__ void __launch_bounds__(FX_TPB) k_fx_emf_fix(Grid G, const int32_t* it
     });
 }
 
-template <typename RT, typename WT, typename FT, int MINB>
+// PART 3: the whole update; 1: the conserved state (source, divergence,
+// RK); 2: the face field (EMFs, CT) -- the two halves read disjoint flux
+// components, so as two kernels (BH_FX_TUNE_SPLIT) each keeps fewer
+// registers than the whole
+template <typename RT, typename WT, typename FT, int MINB, int PART>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, const int32_t* items, int stage,
                                                       double cfl, Queue Q) {
     for_items(Q, [&](int t) FX_INLINE {
@@ -758,8 +762,9 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, con
         const int64_t c = bidx(B, i, j, k);
         const int si = bstride_i(B), sj = bstride_j(B), sk = 1;
         const double dt = cfl * G.dt[0];
-        if (stage == 0 && t == 0 && threadIdx.x == 0) G.dt[1] = dt;
+        if ((PART & 1) && stage == 0 && t == 0 && threadIdx.x == 0) G.dt[1] = dt;
         const double idx = 1.0 / B.dx;
+        if (PART & 1) {
         // source at the cell centre from the stage's primitives
         double x[3];
         cell_centre(B, i, j, k, x);
@@ -785,6 +790,8 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, con
             else
                 G.U[v * N + c] = 0.5 * (G.U[v * N + c] + G.U1[v * N + c] + dt * L);
         }
+        }
+        if (!(PART & 2)) return;
         // the nine distinct edge EMFs of the cell's three lower faces: ex at
         // the edges of c, c+sj, c+sk; ey at c, c+si, c+sk; ez at c, c+si, c+sj
         double ex[3], ey[3], ez[3];
@@ -1058,8 +1065,8 @@ using FRT = BH_REAL;
 inline cudaStream_t fxs(void* s) { return (cudaStream_t)s; }
 inline int fx_launched() { return cudaGetLastError() == cudaSuccess ? BH_OK : BH_ECUDA; }
 // work-queue slots of the step kernels
-enum { QS_C2P = 0, QS_GHOST = 1, QS_FLUX = 2, QS_EMF = 3, QS_EMF_FIX = 4, QS_UPDATE = 5 };
-static_assert(QS_UPDATE + 1 == BH_FX_QSLOTS, "queue slots");
+enum { QS_C2P = 0, QS_GHOST = 1, QS_FLUX = 2, QS_EMF = 3, QS_EMF_FIX = 4, QS_UPDATE = 5, QS_UPDATE_B = 6 };
+static_assert(QS_UPDATE_B + 1 == BH_FX_QSLOTS, "queue slots");
 inline fx::Queue fx_q(const bh_fx_grid* g, int slot, int nitem) {
     if (!g->queue) return fx::Queue{nullptr, nullptr, nitem};
     return fx::Queue{g->queue + 2 * slot, g->queue + 2 * slot + 1, nitem};
@@ -1098,7 +1105,7 @@ inline int fx_grid(const void* fn, int nitem, const bh_fx_grid* g) {
 // launch bounds of the heavy kernels: resident 128-thread CTAs per SM asked
 // of ptxas (which caps registers per thread); 1 leaves the choice to ptxas.
 // Chosen per process and variant (bh_fx_tune_set), initially 1.
-int fx_tune_tab[BH_FX_TUNE_N] = {1, 1, 1, 0};
+int fx_tune_tab[BH_FX_TUNE_N] = {1, 1, 1, 0, 0};
 #define FX_TUNED(kernel, LAUNCH)                                                  \
     switch (fx_tune_tab[kernel]) {                                                \
     case 3: LAUNCH(3); break;                                                     \
@@ -1111,7 +1118,7 @@ int fx_tune_tab[BH_FX_TUNE_N] = {1, 1, 1, 0};
     }
 
 int fx_tune_set(int32_t kernel, int32_t ctas) {
-    if (kernel == BH_FX_TUNE_STAGE) {
+    if (kernel == BH_FX_TUNE_STAGE || kernel == BH_FX_TUNE_SPLIT) {
         if (ctas != 0 && ctas != 1) return BH_EINVAL;
     } else if (kernel < 0 || kernel >= BH_FX_TUNE_N || !(ctas == 1 || (ctas >= 3 && ctas <= 8))) {
         return BH_EINVAL;
@@ -1175,8 +1182,14 @@ int fx_update_parts(const bh_fx_params* P, const bh_fx_grid* g, int32_t stage, i
     if (g->E && g->nitem_pos && g->maxlevel > 0)
         fx::k_fx_emf_fix<<<fx_grid((const void*)fx::k_fx_emf_fix, g->nitem_pos, g), fx::FX_TPB, 0, fxs(s)>>>(
             G, g->items_pos, fx_q(g, QS_EMF_FIX, g->nitem_pos));
-    if (g->nitem_cell) {
-#define L_(M) fx::k_fx_update<FRT, FRT, FRT, M><<<fx_grid((const void*)fx::k_fx_update<FRT, FRT, FRT, M>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, P->cfl, fx_q(g, QS_UPDATE, g->nitem_cell))
+    if (g->nitem_cell && fx_tune_tab[BH_FX_TUNE_SPLIT]) {
+#define L_(M) fx::k_fx_update<FRT, FRT, FRT, M, 1><<<fx_grid((const void*)fx::k_fx_update<FRT, FRT, FRT, M, 1>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, P->cfl, fx_q(g, QS_UPDATE, g->nitem_cell))
+        FX_TUNED(BH_FX_TUNE_UPDATE, L_)
+#undef L_
+        fx::k_fx_update<FRT, FRT, FRT, 8, 2><<<fx_grid((const void*)fx::k_fx_update<FRT, FRT, FRT, 8, 2>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(
+            p, G, g->items_cell, stage, P->cfl, fx_q(g, QS_UPDATE_B, g->nitem_cell));
+    } else if (g->nitem_cell) {
+#define L_(M) fx::k_fx_update<FRT, FRT, FRT, M, 3><<<fx_grid((const void*)fx::k_fx_update<FRT, FRT, FRT, M, 3>, g->nitem_cell, g), fx::FX_TPB, 0, fxs(s)>>>(p, G, g->items_cell, stage, P->cfl, fx_q(g, QS_UPDATE, g->nitem_cell))
         FX_TUNED(BH_FX_TUNE_UPDATE, L_)
 #undef L_
     }

@@ -459,7 +459,7 @@ typedef struct bh_fx_grid {
                                     lists): 2 (0 reads as 2), or 3, which BH_PPM
                                     requires                                        */
 } bh_fx_grid;
-#define BH_FX_QSLOTS 6
+#define BH_FX_QSLOTS 7
 
 /* Launch bounds of the scheme's three heavy kernels (no counterpart in the
  * reference): each is compiled for 1 (no register cap) and 3 to 8
@@ -467,9 +467,12 @@ typedef struct bh_fx_grid {
  * initially 1.  BH_FX_TUNE_STAGE (0 or 1, initially 0) selects the flux
  * kernel: 1 = the stencil staged in shared memory per tile (items_flux; grids
  * without items_flux keep the unstaged kernel), with the launch bounds of
- * BH_FX_TUNE_FLUX.  bhgpu.fixed.autotune times the candidates on a grid and
+ * BH_FX_TUNE_FLUX.  BH_FX_TUNE_SPLIT (0 or 1, initially 0): 1 = the update
+ * as two kernels, the conserved state (launch bounds of BH_FX_TUNE_UPDATE)
+ * and the face field.  bhgpu.fixed.autotune times the candidates on a grid and
  * sets the fastest.  Launches (and graphs captured) after the call use it. */
-enum { BH_FX_TUNE_C2P = 0, BH_FX_TUNE_FLUX = 1, BH_FX_TUNE_UPDATE = 2, BH_FX_TUNE_STAGE = 3, BH_FX_TUNE_N = 4 };
+enum { BH_FX_TUNE_C2P = 0, BH_FX_TUNE_FLUX = 1, BH_FX_TUNE_UPDATE = 2, BH_FX_TUNE_STAGE = 3, BH_FX_TUNE_SPLIT = 4,
+       BH_FX_TUNE_N = 5 };
 int bh_fx_tune_set(int32_t precision, int32_t kernel, int32_t ctas_per_sm);
 int bh_fx_tune_get(int32_t precision, int32_t kernel, int32_t *ctas_per_sm);
 

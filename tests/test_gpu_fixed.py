@@ -435,3 +435,26 @@ def test_sharded_pieces_on_one_rank_equal_the_step():
                 assert np.array_equal(box, ref), (name, g)
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("leveled", [False, True])
+def test_split_update_equals_the_whole_update(leveled):
+    """the update as two kernels (conserved state; face field) = the update as
+    one kernel, bit for bit in FP64, with EMFs formed inside (one level) and
+    from the EMF arrays (three levels)"""
+    from bhgpu import fixed as fxm
+    a = _leveled() if leveled else _grid(32, 16)
+    b = _leveled() if leveled else _grid(32, 16)
+    a.torus_init()
+    b.torus_init()
+    try:
+        for _ in range(3):
+            fxm.tune_set("fp64", "split", 1)
+            a.step()
+            fxm.tune_set("fp64", "split", 0)
+            b.step()
+        torch.cuda.synchronize()
+    finally:
+        fxm.tune_set("fp64", "split", 0)
+    for name in ("U", "Bf", "W"):
+        assert np.array_equal(getattr(a, name).cpu().numpy(), getattr(b, name).cpu().numpy()), name
