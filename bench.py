@@ -154,7 +154,7 @@ def arm_config(args, world):
                         "Fishbone-Moncrief r_in=6 r_max=12, Gamma=4/3, beta=100 single loop, 4% pressure noise, "
                         "excision r<1.2 r_H; corrected Valencia scheme, PLM MC + HLL + CT, RK2 CFL 0.4",
             "grid": f"{args.grid}^3", "blocks": (args.grid // args.block) ** 3,
-            "block": f"{args.block}^3 + 2 ghosts", "parallelism": f"replicas x{world}",
+            "block": f"{args.block}^3 + 3 ghost layers (2 filled for PLM)", "parallelism": f"replicas x{world}",
             "l2": "working set > L2 (the 128^3 state, primitives and fluxes exceed 126 MB)",
             "run": "free-running from the torus initial data (every step continues the last)"}
 
@@ -517,7 +517,7 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
 # device work queue), the step replayed as a CUDA graph
 AMR_CONFIGS = {
     "config3": {"n0": 8, "r_fine": (14.0, 26.0), "seed": 3, "accuracy_steps": 100,
-                "what": "3 levels: blocks of 8^3, 16^3 and 32^3 cells (+2 ghosts), seeded uneven mix "
+                "what": "3 levels: blocks of 8^3, 16^3 and 32^3 cells (+3 ghost layers), seeded uneven mix "
                         "concentrated near the hole"},
     "config5": {"n0": 4, "r_fine": (10.0, 18.0, 28.0), "seed": 5, "accuracy_steps": 200,
                 "what": "4 levels: blocks of 4^3 to 32^3 cells, effective 256^3 at the finest level"},
