@@ -26,9 +26,10 @@ value : zone-updates/s of the mixed-precision form (reconstruction, fluxes
         steps from the same initial data is reported per conserved field
         with the face field's divergence.
 e2e   : the same metric through the public API with host buffers
-        (bhgpu.fixed.FxHostPipeline): per step the state (U, W, Bf) goes up
-        from pinned host memory, is stepped, and comes back down; three
-        device grids overlap the copies of neighbouring steps.
+        (bhgpu.fixed.FxHostPipeline): per step the state a step reads (the
+        conserved fluid variables, the previous primitives and the face
+        field) goes up from pinned host memory, is stepped, and comes back
+        down; three device grids overlap the copies of neighbouring steps.
 roofline : the kernel with the largest share of the step, its algorithmic
         bytes per launch over its CUDA-event duration, against the measured
         HBM copy bandwidth (MEASURED_PEAKS.json; fallback 6650 GB/s); the
@@ -282,7 +283,9 @@ def e2e_measure(args, g0, dist):
     import torch
     from bhgpu.fixed import FxGrid, FxHostPipeline
     pin = lambda x: x.cpu().pin_memory()
-    hU, hW, hB = pin(g0.U), pin(g0.W), pin(g0.Bf)
+    # the state a step reads: U and W rows 0-4 (the cell-centred field rows
+    # are recomputed from the face field on the device) and the face field
+    hU, hW, hB = pin(g0.U[:5]), pin(g0.W[:5]), pin(g0.Bf)
     grids = [g0] + [FxGrid(g0.blocks_np, g0.nbr_np, g0.params) for _ in range(E2E_DEPTH - 1)]
     outs = [tuple(torch.empty_like(x).pin_memory() for x in (hU, hW, hB)) for _ in range(E2E_DEPTH)]
 
@@ -683,7 +686,8 @@ def run_ours(args):
                       "div_B_rel_after_timed_steps": divb_after, "counters_after_timed_steps": counters},
             "e2e": {"value": world * zones / (ms_e2e / 1e3), "unit": METRIC, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "ms_per_step": ms_e2e,
-                    "api": f"bhgpu.fixed.FxHostPipeline, {E2E_DEPTH} device grids, pinned host U/W/Bf in and "
+                    "api": f"bhgpu.fixed.FxHostPipeline, {E2E_DEPTH} device grids, pinned host state (U and W rows "
+                           "0-4, face field) in and "
                            "out every step",
                     "serial_value": world * zones / (ms_e2e_serial / 1e3), "serial_ms_per_step": ms_e2e_serial},
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,

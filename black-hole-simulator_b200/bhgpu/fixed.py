@@ -290,13 +290,19 @@ lib.bh_step_graph_destroy.restype = C.c_int
 class FxHostPipeline:
     """Host-resident torus states stepped through the GPU, copies overlapped.
 
-    Each ``submit`` uploads a state (U, W, Bf in the grid layout, pinned
-    host tensors) into one of the pipeline's device grids on a copy stream,
-    advances it ``steps`` RK2 steps on a compute stream and downloads it on
-    a second copy stream; consecutive submissions use different grids, so
-    the upload of one state, the step of the previous one and the download
-    of the one before overlap.  Each result is bit-identical to stepping the
-    state alone.  The returned event marks the end of the download.
+    A state is what a step reads: the conserved fluid variables (rows 0-4 of
+    U), the previous primitives (rows 0-4 of W: con2prim's starting point)
+    and the face field Bf, pinned host tensors in the grid layout (U and W
+    may carry all 8 rows; only rows 0-4 move).  The cell-centred field (rows
+    5-7 of U and W) is recomputed on the device from the face field by the
+    step's con2prim, so it is neither uploaded nor downloaded.  Each
+    ``submit`` uploads a state into one of the pipeline's device grids on a
+    copy stream, advances it ``steps`` RK2 steps on a compute stream and
+    downloads it on a second copy stream; consecutive submissions use
+    different grids, so the upload of one state, the step of the previous one
+    and the download of the one before overlap.  Each result is bit-identical
+    to stepping the state alone.  The returned event marks the end of the
+    download.
     """
 
     def __init__(self, grids: list[FxGrid], steps: int = 1):
@@ -317,8 +323,8 @@ class FxHostPipeline:
         with torch.cuda.stream(self.s_in):
             if self._freed[slot] is not None:
                 self.s_in.wait_event(self._freed[slot])
-            g.U.copy_(U, non_blocking=True)
-            g.W.copy_(W, non_blocking=True)
+            g.U[:5].copy_(U[:5], non_blocking=True)
+            g.W[:5].copy_(W[:5], non_blocking=True)
             g.Bf.copy_(Bf, non_blocking=True)
             loaded = torch.cuda.Event()
             loaded.record(self.s_in)
@@ -330,8 +336,8 @@ class FxHostPipeline:
             done.record(self.s_run)
         with torch.cuda.stream(self.s_out):
             self.s_out.wait_event(done)
-            out_U.copy_(g.U, non_blocking=True)
-            out_W.copy_(g.W, non_blocking=True)
+            out_U[:5].copy_(g.U[:5], non_blocking=True)
+            out_W[:5].copy_(g.W[:5], non_blocking=True)
             out_Bf.copy_(g.Bf, non_blocking=True)
             freed = torch.cuda.Event()
             freed.record(self.s_out)

@@ -458,3 +458,34 @@ def test_split_update_equals_the_whole_update(leveled):
         fxm.tune_set("fp64", "split", 0)
     for name in ("U", "Bf", "W"):
         assert np.array_equal(getattr(a, name).cpu().numpy(), getattr(b, name).cpu().numpy()), name
+
+
+def test_host_pipeline_equals_stepping_alone():
+    """three host states through a two-grid FxHostPipeline (a grid is reused
+    while other copies are in flight; only U and W rows 0-4 and the face
+    field move) = each state stepped alone on the device, bit for bit (FP64)"""
+    from bhgpu.fixed import FxHostPipeline
+    src = _grid(32, 16)
+    src.torus_init()
+    states = []
+    for _ in range(3):
+        src.step()
+        torch.cuda.synchronize()
+        states.append(tuple(x.cpu().pin_memory() for x in (src.U[:5].contiguous(), src.W[:5].contiguous(), src.Bf)))
+    ref = []
+    for U, W, B in states:
+        g = _grid(32, 16)
+        g.U[:5].copy_(U)
+        g.W[:5].copy_(W)
+        g.Bf.copy_(B)
+        g.step()
+        torch.cuda.synchronize()
+        ref.append((g.U[:5].cpu().numpy(), g.W[:5].cpu().numpy(), g.Bf.cpu().numpy()))
+    pipe = FxHostPipeline([_grid(32, 16), _grid(32, 16)])
+    outs = [tuple(torch.empty_like(x).pin_memory() for x in st) for st in states]
+    for st, out in zip(states, outs):
+        pipe.submit(*st, *out)
+    pipe.synchronize()
+    for out, r in zip(outs, ref):
+        for a, b in zip(out, r):
+            assert np.array_equal(a.numpy(), b)
