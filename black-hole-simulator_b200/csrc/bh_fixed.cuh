@@ -545,7 +545,10 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux(FxPar P, Grid G, const
 // ----------------------------------------------------------------------
 constexpr int FX_TI = 4, FX_TJ = 4, FX_TK = 8;
 constexpr int FX_HI = FX_TI + 3, FX_HJ = FX_TJ + 3, FX_HK = FX_TK + 3;   // -2 .. T per axis
-constexpr int FX_HBOX = FX_HI * FX_HJ * FX_HK;
+// row pitch of the staged box: 12 rather than FX_HK = 11 entries, so that a
+// warp's 4 rows of 8 cells fall on fewer shared banks at once
+constexpr int FX_HKP = FX_HK + 1;
+constexpr int FX_HBOX = FX_HI * FX_HJ * FX_HKP;
 constexpr int FX_NX = FX_HI * FX_TJ * FX_TK;   // the tile and its x-halo
 constexpr int FX_NY = FX_TI * 3 * FX_TK;       // y-halo: j = -2, -1, TJ
 constexpr int FX_NZ = FX_TI * FX_TJ * 3;       // z-halo: k = -2, -1, TK
@@ -565,7 +568,7 @@ __device__ inline void cross_cell(int q, int& a, int& b, int& c) {
         a = q / (FX_TJ * 3); b = (q / 3) % FX_TJ; c = h < 2 ? h - 2 : FX_TK;
     }
 }
-__device__ inline int box_at(int a, int b, int c) { return ((a + 2) * FX_HJ + (b + 2)) * FX_HK + (c + 2); }
+__device__ inline int box_at(int a, int b, int c) { return ((a + 2) * FX_HJ + (b + 2)) * FX_HKP + (c + 2); }
 
 template <typename RT, typename WT, typename FT, int MINB>
 __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux_tile(FxPar P, Grid G, const int32_t* items, int stage,
@@ -611,10 +614,10 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_flux_tile(FxPar P, Grid G, 
         // (PLM only: the launch keeps PPM's wider stencil on k_fx_flux)
         if (i >= 0)
             face_flux_at<RT, FT, false>(P, G, B, i, j, k, 0, Bfs,
-                                        [&](int v, int s) { return RT(sW[v][o + s * (FX_HJ * FX_HK)]); });
+                                        [&](int v, int s) { return RT(sW[v][o + s * (FX_HJ * FX_HKP)]); });
         if (j >= 0)
             face_flux_at<RT, FT, false>(P, G, B, i, j, k, 1, Bfs,
-                                        [&](int v, int s) { return RT(sW[v][o + s * FX_HK]); });
+                                        [&](int v, int s) { return RT(sW[v][o + s * FX_HKP]); });
         if (k >= 0)
             face_flux_at<RT, FT, false>(P, G, B, i, j, k, 2, Bfs, [&](int v, int s) { return RT(sW[v][o + s]); });
     });
