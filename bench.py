@@ -26,10 +26,12 @@ value : zone-updates/s of the mixed-precision form (reconstruction, fluxes
         steps from the same initial data is reported per conserved field
         with the face field's divergence.
 e2e   : the same metric through the public API with host buffers
-        (bhgpu.fixed.FxHostPipeline): per step the state a step reads (the
-        conserved fluid variables, the previous primitives and the face
-        field) goes up from pinned host memory, is stepped, and comes back
-        down; three device grids overlap the copies of neighbouring steps.
+        (bhgpu.fixed.FxHostPipeline.submit_packed): per step the state a
+        step reads (the interior cells' conserved fluid variables and
+        previous primitives, the blocks' own face field), packed, goes up
+        from pinned host memory, is unpacked, stepped and packed on the
+        device, and comes back down; three device grids overlap the copies of
+        neighbouring steps.
 roofline : the kernel with the largest share of the step, its algorithmic
         bytes per launch over its CUDA-event duration, against the measured
         HBM copy bandwidth (MEASURED_PEAKS.json; fallback 6650 GB/s); the
@@ -58,7 +60,7 @@ CFL = 0.4
 LO, HI = -40.0, 40.0
 TORUS = dict(r_in=6.0, r_max=12.0, kappa=1e-3, beta=100.0, noise=0.04, seed=1)
 STEP_BYTES = 296          # algorithmic HBM bytes per zone-update of an RK2 step
-LAUNCHES_PER_STEP = 9     # dt init, then con2prim, ghosts, fluxes, update per stage
+LAUNCHES_PER_STEP = 9     # dt init, then con2prim, ghosts, fluxes, update per stage (+1 per stage: split update)
 # DRAM bytes (read + write) per launch of the mixed variant's step kernels at
 # 128^3, from the ncu capture summarised in profiles/kernels_torus_128cube.md
 PROFILED_TRAFFIC = {"fluxes": 154.77e6 + 173.75e6, "update": 542.67e6 + 123.91e6, "prims": 190.97e6 + 143.72e6}
@@ -282,16 +284,21 @@ def accuracy(args, steps):
 def e2e_measure(args, g0, dist):
     import torch
     from bhgpu.fixed import FxGrid, FxHostPipeline
-    pin = lambda x: x.cpu().pin_memory()
-    # the state a step reads: U and W rows 0-4 (the cell-centred field rows
-    # are recomputed from the face field on the device) and the face field
-    hU, hW, hB = pin(g0.U[:5]), pin(g0.W[:5]), pin(g0.Bf)
+    # the state a step reads, packed: the interior cells' rows 0-4 of U and W
+    # (the cell-centred field rows are recomputed from the face field on the
+    # device) and the blocks' own faces
+    nbytes = g0.state_nbytes()
+    dbuf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    g0.pack_state(dbuf)
+    torch.cuda.synchronize()
+    hin = dbuf.cpu().pin_memory()
+    del dbuf
     grids = [g0] + [FxGrid(g0.blocks_np, g0.nbr_np, g0.params) for _ in range(E2E_DEPTH - 1)]
-    outs = [tuple(torch.empty_like(x).pin_memory() for x in (hU, hW, hB)) for _ in range(E2E_DEPTH)]
+    outs = [torch.empty_like(hin).pin_memory() for _ in range(E2E_DEPTH)]
 
     def run(pipe, nstep):
         for i in range(len(pipe.grids)):
-            pipe.submit(hU, hW, hB, *outs[i])
+            pipe.submit_packed(hin, outs[i])
         pipe.synchronize()
         if dist:
             dist.barrier()
@@ -299,7 +306,7 @@ def e2e_measure(args, g0, dist):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(pipe.s_in)
         for i in range(nstep):
-            pipe.submit(hU, hW, hB, *outs[i % len(pipe.grids)])
+            pipe.submit_packed(hin, outs[i % len(pipe.grids)])
         b.record(pipe.s_out)
         torch.cuda.synchronize()
         t = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device="cuda")
@@ -309,7 +316,6 @@ def e2e_measure(args, g0, dist):
 
     ms = run(FxHostPipeline(grids), args.e2e_steps)
     ms_serial = run(FxHostPipeline(grids[:1]), max(3, args.e2e_steps // 3))
-    nbytes = sum(x.numel() * x.element_size() for x in (hU, hW, hB))
     del grids
     return ms, ms_serial, nbytes
 
@@ -686,11 +692,11 @@ def run_ours(args):
                       "div_B_rel_after_timed_steps": divb_after, "counters_after_timed_steps": counters},
             "e2e": {"value": world * zones / (ms_e2e / 1e3), "unit": METRIC, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "ms_per_step": ms_e2e,
-                    "api": f"bhgpu.fixed.FxHostPipeline, {E2E_DEPTH} device grids, pinned host state (U and W rows "
-                           "0-4, face field) in and "
-                           "out every step",
+                    "api": f"bhgpu.fixed.FxHostPipeline.submit_packed, {E2E_DEPTH} device grids, the packed state "
+                           "(interior cells' U and W rows 0-4, the blocks' own faces) from pinned host memory in and "
+                           "out every step, unpacked and packed on the device",
                     "serial_value": world * zones / (ms_e2e_serial / 1e3), "serial_ms_per_step": ms_e2e_serial},
-            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "gpu_launches": (LAUNCHES_PER_STEP + (2 if tune_get("mixed", "split") else 0)) * args.steps,
             "roofline": {"bound": "hbm", "kernel": f"{kname} ({top})", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": PROFILED_TRAFFIC.get(top) if args.grid == 128 else None,

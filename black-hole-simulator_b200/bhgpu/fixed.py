@@ -57,6 +57,7 @@ _sig = {
     "bh_fx_ghosts": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
     "bh_fx_fluxes": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
     "bh_fx_update": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
+    "bh_fx_pack_state": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _vp, _vp, _i32, _vp],
     "bh_fx_ghost_pass": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _i32, _vp],
     "bh_fx_emf": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _vp],
     "bh_fx_update_from_emf": [C.POINTER(BhFxParams), C.POINTER(BhFxGrid), _i32, _vp],
@@ -198,6 +199,31 @@ class FxGrid:
     def ghosts(self, stage=0):
         check(lib.bh_fx_ghosts(C.byref(self._p), C.byref(self._g), stage, _stream()), "bh_fx_ghosts")
 
+    # ---- the state a step reads, packed (bh_fx_pack_state) ----
+    def state_nbytes(self) -> int:
+        """bytes of the packed state: rows 0-4 of U and W, the blocks' own
+        face field"""
+        q = self.items["cell"].shape[0] * CHUNK
+        nb = self.blocks_np["n"][:self.nactive].astype(np.int64)
+        return int(q * (5 * 8 + 5 * self.W.element_size() + 3 * 8) + 8 * 3 * int((nb * nb).sum()))
+
+    def _face_off(self):
+        if getattr(self, "_foff", None) is None:
+            nb = self.blocks_np["n"][:self.nactive].astype(np.int64)
+            off = np.concatenate([[0], np.cumsum(3 * nb * nb)[:-1]]).astype(np.int64)
+            self._foff = torch.from_numpy(off).to(self.device)
+        return self._foff
+
+    def pack_state(self, buf: torch.Tensor):
+        """the state into the device buffer buf (uint8, state_nbytes())"""
+        check(lib.bh_fx_pack_state(C.byref(self._p), C.byref(self._g), _ptr(self._face_off()), _ptr(buf), 0,
+                                   _stream()), "bh_fx_pack_state")
+
+    def unpack_state(self, buf: torch.Tensor):
+        """the grid's U, W rows 0-4 and face field from a packed state"""
+        check(lib.bh_fx_pack_state(C.byref(self._p), C.byref(self._g), _ptr(self._face_off()), _ptr(buf), 1,
+                                   _stream()), "bh_fx_pack_state")
+
     def ghost_pass(self, stage, pass_):
         check(lib.bh_fx_ghost_pass(C.byref(self._p), C.byref(self._g), stage, pass_, _stream()), "bh_fx_ghost_pass")
 
@@ -315,6 +341,40 @@ class FxHostPipeline:
         self.s_in, self.s_run, self.s_out = (torch.cuda.Stream(dev) for _ in range(3))
         self._freed: list[torch.cuda.Event | None] = [None] * len(self.grids)
         self._k = 0
+        self._bufs = None
+
+    def submit_packed(self, state_in: torch.Tensor, state_out: torch.Tensor) -> torch.cuda.Event:
+        """As submit, for a state packed by FxGrid.pack_state (pinned uint8
+        host tensors of state_nbytes()): only the interior cells' values and
+        the blocks' own faces cross the host link, unpacked and packed on the
+        device by bh_fx_pack_state."""
+        if self._bufs is None:
+            n = self.grids[0].state_nbytes()
+            self._bufs = [torch.empty(n, dtype=torch.uint8, device=g.device) for g in self.grids]
+        slot = self._k % len(self.grids)
+        self._k += 1
+        g, buf = self.grids[slot], self._bufs[slot]
+        with torch.cuda.stream(self.s_in):
+            if self._freed[slot] is not None:
+                self.s_in.wait_event(self._freed[slot])
+            buf.copy_(state_in, non_blocking=True)
+            loaded = torch.cuda.Event()
+            loaded.record(self.s_in)
+        with torch.cuda.stream(self.s_run):
+            self.s_run.wait_event(loaded)
+            g.unpack_state(buf)
+            for _ in range(self.steps):
+                g.step()
+            g.pack_state(buf)
+            done = torch.cuda.Event()
+            done.record(self.s_run)
+        with torch.cuda.stream(self.s_out):
+            self.s_out.wait_event(done)
+            state_out.copy_(buf, non_blocking=True)
+            freed = torch.cuda.Event()
+            freed.record(self.s_out)
+        self._freed[slot] = freed
+        return freed
 
     def submit(self, U, W, Bf, out_U, out_W, out_Bf) -> torch.cuda.Event:
         slot = self._k % len(self.grids)

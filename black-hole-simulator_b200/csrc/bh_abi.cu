@@ -251,6 +251,11 @@ int bh_fx_tune_get(int32_t precision, int32_t kernel, int32_t* ctas) {
     default: return BH_EINVAL;
     }
 }
+int bh_fx_pack_state(const bh_fx_params* P, const bh_fx_grid* g, const int64_t* face_off, void* packed, int32_t dir,
+                     void* stream) {
+    if (fx_bad(P, g) || !face_off || !packed || (dir != 0 && dir != 1)) return BH_EINVAL;
+    FX_DISPATCH(P, fx_pack_state(g, face_off, packed, dir, stream));
+}
 int bh_fx_divb(const bh_fx_grid* g, double* out, void* stream) {
     if (!g || g->nblock <= 0 || !g->blocks || !g->Bf || !out || (g->nitem_cell > 0 && !g->items_cell)) return BH_EINVAL;
     return vfp64::fx_divb(g, out, stream);

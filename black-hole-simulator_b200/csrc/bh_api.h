@@ -63,6 +63,7 @@ inline bool bh_tune_valid(int32_t kernel, int32_t ctas) {
     int fx_update_parts(const bh_fx_params*, const bh_fx_grid*, int32_t, int32_t, void*);                     \
     int fx_step(const bh_fx_params*, const bh_fx_grid*, void*);                                               \
     int fx_divb(const bh_fx_grid*, double*, void*);                                                           \
+    int fx_pack_state(const bh_fx_grid*, const int64_t*, void*, int32_t, void*);                              \
     int fx_torus_init(const bh_fx_params*, const bh_fx_grid*, const bh_fx_torus*, double*, double*, void*);   \
     int fx_tune_set(int32_t, int32_t);                                                                        \
     int fx_tune_get(int32_t, int32_t*);                                                                       \

@@ -826,6 +826,49 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_update(FxPar P, Grid G, con
 }
 
 // ======================================================================
+// the state a step reads, between the grid's boxes and a compact buffer
+// (dir 0: pack, 1: unpack): per interior-cell slot q = item * 128 + lane
+// (Q = nitem_cell * 128 slots) rows 0-4 of U (double [5][Q]) and of W
+// (WT [5][Q]) and the cell's three lower faces (double [3][Q]); then the
+// blocks' upper boundary faces, 3 n^2 doubles per block from face_off[b]
+// (x-faces at i = n by (j, k), y at j = n by (i, k), z at k = n by (i, j)).
+// Slots past a block's last cell are left alone.
+// ======================================================================
+template <typename WT>
+__global__ void __launch_bounds__(FX_TPB) k_fx_pack(Grid G, const int32_t* items, int nitem, const int64_t* face_off,
+                                                    char* packed, int dir) {
+    const int t = blockIdx.x;
+    const int32_t b = items[2 * t];
+    const bh_fx_block B = G.blk[b];
+    const int n = B.n;
+    const int e = items[2 * t + 1] + threadIdx.x;
+    if (e >= n * n * n) return;
+    const int i = e / (n * n), j = (e / n) % n, k = e % n;
+    const int64_t N = G.ncell, c = bidx(B, i, j, k), Q = (int64_t)nitem * FX_TPB, q = (int64_t)t * FX_TPB + threadIdx.x;
+    double* pu = (double*)packed;
+    WT* pw = (WT*)(pu + 5 * Q);
+    double* pb = (double*)(pw + 5 * Q);
+    double* pf = pb + 3 * Q + face_off[b];
+    WT* W = (WT*)G.W;
+    const int si = bstride_i(B), sj = bstride_j(B);
+    if (dir == 0) {
+        for (int v = 0; v < 5; v++) pu[v * Q + q] = G.U[v * N + c];
+        for (int v = 0; v < 5; v++) pw[v * Q + q] = W[v * N + c];
+        for (int d = 0; d < 3; d++) pb[d * Q + q] = G.Bf[d * N + c];
+        if (i == n - 1) pf[j * n + k] = G.Bf[c + si];
+        if (j == n - 1) pf[n * n + i * n + k] = G.Bf[N + c + sj];
+        if (k == n - 1) pf[2 * n * n + i * n + j] = G.Bf[2 * N + c + 1];
+    } else {
+        for (int v = 0; v < 5; v++) G.U[v * N + c] = pu[v * Q + q];
+        for (int v = 0; v < 5; v++) W[v * N + c] = pw[v * Q + q];
+        for (int d = 0; d < 3; d++) G.Bf[d * N + c] = pb[d * Q + q];
+        if (i == n - 1) G.Bf[c + si] = pf[j * n + k];
+        if (j == n - 1) G.Bf[N + c + sj] = pf[n * n + i * n + k];
+        if (k == n - 1) G.Bf[2 * N + c + 1] = pf[2 * n * n + i * n + j];
+    }
+}
+
+// ======================================================================
 // divergence of the face field: per interior cell |div B| dx / max(|B~|)
 // of its six faces; max over each block into out[b] (non-negative doubles)
 // ======================================================================
@@ -1210,6 +1253,13 @@ int fx_step(const bh_fx_params* P, const bh_fx_grid* g, void* s) {
         if (rc) return rc;
     }
     return BH_OK;
+}
+int fx_pack_state(const bh_fx_grid* g, const int64_t* face_off, void* packed, int32_t dir, void* s) {
+    fx::Grid G = fx::grid_of(g);
+    if (g->nitem_cell)
+        fx::k_fx_pack<FRT><<<g->nitem_cell, fx::FX_TPB, 0, fxs(s)>>>(G, g->items_cell, g->nitem_cell, face_off,
+                                                                     (char*)packed, dir);
+    return fx_launched();
 }
 int fx_divb(const bh_fx_grid* g, double* out, void* s) {
     fx::Grid G = fx::grid_of(g);

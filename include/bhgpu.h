@@ -501,6 +501,18 @@ int bh_fx_update(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void
  * Both require E. */
 int bh_fx_emf(const bh_fx_params *P, const bh_fx_grid *g, void *stream);
 int bh_fx_update_from_emf(const bh_fx_params *P, const bh_fx_grid *g, int32_t stage, void *stream);
+/* The state a step reads -- rows 0-4 of U (conserved fluid) and of W (the
+ * previous primitives, con2prim's start) and the blocks' own face field --
+ * between the grid's boxes and a compact device buffer (dir 0: pack, 1:
+ * unpack; the cell-centred field rows 5-7 are recomputed by the step's
+ * con2prim).  Layout, Q = nitem_cell * BH_FX_CHUNK slots, slot q = item *
+ * BH_FX_CHUNK + lane of items_cell: double U[5][Q]; W[5][Q] (float for
+ * BH_MIXED, else double); double Bf[3][Q] (each cell's three lower faces);
+ * then per block b from face_off[b] (device, doubles) its upper boundary
+ * faces, 3 n^2: x-faces at i = n in (j, k) order, y at j = n in (i, k), z at
+ * k = n in (i, j).  Slots past a block's last cell are not touched. */
+int bh_fx_pack_state(const bh_fx_params *P, const bh_fx_grid *g, const int64_t *face_off, void *packed,
+                     int32_t dir, void *stream);
 /* max over each block's interior cells of |div B~| / max |B~| of the cell's
  * faces (a relative divergence, 0 up to roundoff under CT): out [nblock]
  * device, cleared by the call */

@@ -489,3 +489,38 @@ def test_host_pipeline_equals_stepping_alone():
     for out, r in zip(outs, ref):
         for a, b in zip(out, r):
             assert np.array_equal(a.numpy(), b)
+
+
+def test_packed_state_pipeline_equals_stepping_alone():
+    """the packed state (bh_fx_pack_state: interior rows 0-4 of U and W, the
+    blocks' own faces) through a two-grid pipeline = each state stepped alone
+    and packed, byte for byte (FP64, blocks of 16^3); unpacking a packed
+    state and packing it again gives the same bytes"""
+    from bhgpu.fixed import FxHostPipeline
+    src = _grid(32, 16)
+    src.torus_init()
+    n = src.state_nbytes()
+    states, refs = [], []
+    for _ in range(3):
+        src.step()
+        buf = torch.empty(n, dtype=torch.uint8, device="cuda")
+        src.pack_state(buf)
+        torch.cuda.synchronize()
+        states.append(buf.cpu().pin_memory())
+        g = _grid(32, 16)
+        g.unpack_state(buf)
+        again = torch.empty_like(buf)
+        g.pack_state(again)
+        torch.cuda.synchronize()
+        assert torch.equal(again, buf)
+        g.step()
+        g.pack_state(again)
+        torch.cuda.synchronize()
+        refs.append(again.cpu().numpy())
+    pipe = FxHostPipeline([_grid(32, 16), _grid(32, 16)])
+    outs = [torch.empty_like(st).pin_memory() for st in states]
+    for st, out in zip(states, outs):
+        pipe.submit_packed(st, out)
+    pipe.synchronize()
+    for out, r in zip(outs, refs):
+        assert np.array_equal(out.numpy(), r)
