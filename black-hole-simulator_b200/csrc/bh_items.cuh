@@ -572,7 +572,7 @@ BH_HD inline void ghost_copy_item(const Pool& P, int p, int e) {
     // the first cell of the pair: ghost (gi, gj, gk), source (ai, aj, ak);
     // the second is k + 1 in both, except an outflow k-strip on the +k side,
     // whose layers mirror the interior (ghost 16, 17 <- 15, 14)
-    int gi, gj, gk, ai, aj, ak, src_p;
+    int gi, gj, gk, ai, aj, ak, src_p, row_end = 0;
     bool swap = false;
     if (dim == 2) {
         int t1 = rem >> 4, t2 = rem & 15;
@@ -587,6 +587,7 @@ BH_HD inline void ghost_copy_item(const Pool& P, int p, int e) {
         }
     } else {
         int gg = rem >> 7, t1 = (rem >> 3) & 15, t2 = (rem & 7) * 2;
+        row_end = t2 == 0 ? -1 : (t2 == BLK - 2 ? 1 : 0);
         strip_ijk(dim, (side == 1 ? BLK : -GH) + gg, t1, t2, gi, gj, gk);
         if (kind == BH_NB_COPY) {
             src_p = nb;
@@ -602,6 +603,23 @@ BH_HD inline void ghost_copy_item(const Pool& P, int p, int e) {
     double2 x[8];
 #pragma unroll
     for (int v = 0; v < 8; v++) x[v] = *reinterpret_cast<const double2*>(src + (size_t)v * NC + la);
+    if (row_end != 0) {
+        // The first and last pair of an x- or y-strip row share their
+        // 32-byte sector with the row's two cells beyond the strip (k = -2,
+        // -1 or 16, 17: edge cells, which no strip fills): written back with
+        // the pair, every store of the row is a whole sector.
+        const int edge = row_end < 0 ? lg - 2 : lg + 2;
+        double2 own[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) own[v] = *reinterpret_cast<const double2*>(dst + (size_t)v * NC + edge);
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+            double2* row = reinterpret_cast<double2*>(dst + (size_t)v * NC + (row_end < 0 ? edge : lg));
+            row[0] = row_end < 0 ? own[v] : x[v];
+            row[1] = row_end < 0 ? x[v] : own[v];
+        }
+        return;
+    }
     if (dim == 2) {
         // A k-strip pair is half of a 32-byte sector (rows of CPN = 20
         // doubles start on sector boundaries); the other half is the row's
