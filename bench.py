@@ -163,9 +163,9 @@ def arm_config(args, world):
 
 
 # ---------------------------------------------------------------------------
-def torus_grid(args, precision, limiter="mc"):
+def torus_grid(args, precision, limiter="mc", **kw):
     from bhgpu.fixed import FxGrid, FxParams
-    g = FxGrid.uniform(LO, HI, args.grid, args.block, FxParams(precision=precision, limiter=limiter))
+    g = FxGrid.uniform(LO, HI, args.grid, args.block, FxParams(precision=precision, limiter=limiter, **kw))
     info = g.torus_init(**TORUS)
     return g, info
 
@@ -250,13 +250,13 @@ def alg_bytes(piece, n, wb):
     raise KeyError(piece)
 
 
-def accuracy(args, steps):
+def accuracy(args, steps, **kw):
     """plain FP64 and mixed from the same initial data, `steps` steps each"""
     import numpy as np
     import torch
     from bhgpu.fixed import FxGrid, FxParams
     ref, _ = torus_grid(args, "fp64")
-    mix = FxGrid(ref.blocks_np, ref.nbr_np, FxParams(precision="mixed"))
+    mix = FxGrid(ref.blocks_np, ref.nbr_np, FxParams(precision="mixed", **kw))
     mix.copy_state_from(ref)
     ref.capture()
     mix.capture()
@@ -658,6 +658,14 @@ def run_ours(args):
         del gv
         torch.cuda.empty_cache()
     ppm["mixed_vs_plain_fp64"] = ppm["fp64"]["ms_per_step"] / ppm["mixed"]["ms_per_step"]
+    # the mixed variant with every cell's con2prim ending in FP64 Newton iterations
+    gv, _ = torus_grid(args, "mixed", c2p_fp64=True)
+    ms_v, _ = timed_steps(gv, args.steps, warm, dist)
+    del gv
+    torch.cuda.empty_cache()
+    strict = {"ms_per_step": ms_v, "zone_updates_per_s": world * args.grid ** 3 / (ms_v / 1e3),
+              "speedup_vs_plain_fp64": variants["fp64"]["ms_per_step"] / ms_v,
+              "accuracy_after_steps": accuracy(args, args.accuracy_steps, c2p_fp64=True)}
     acc = accuracy(args, args.accuracy_steps)
     if dist:
         dist.barrier()
@@ -688,6 +696,7 @@ def run_ours(args):
                                     "accuracy_after_steps": acc},
             "variants": variants,
             "ppm": ppm,
+            "mixed_c2p_fp64": strict,
             "torus": {"ell": info["ell"], "field_scale": info["field_scale"], "beta": info["beta"],
                       "div_B_rel_after_timed_steps": divb_after, "counters_after_timed_steps": counters},
             "e2e": {"value": world * zones / (ms_e2e / 1e3), "unit": METRIC, "h2d_bytes_per_step": nbytes,

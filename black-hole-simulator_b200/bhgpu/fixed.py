@@ -36,7 +36,7 @@ LIMITERS = {"minmod": BH_MINMOD, "vanleer": BH_VANLEER, "mc": BH_MC, "ppm": BH_P
 class BhFxParams(C.Structure):
     _fields_ = [("M", _d), ("a", _d), ("gamma", _d), ("cfl", _d), ("rho_floor", _d), ("u_floor", _d),
                 ("sigma_max", _d), ("W_max", _d), ("r_exc", _d), ("tol", _d), ("maxiter", _i32),
-                ("limiter", _i32), ("precision", _i32), ("reserved", _i32)]
+                ("limiter", _i32), ("precision", _i32), ("flags", _i32)]
 
 
 class BhFxGrid(C.Structure):
@@ -90,13 +90,14 @@ class FxParams:
     maxiter: int = 30
     limiter: str = "mc"           # monotonized central: no division per slope
     precision: str = "fp64"
+    c2p_fp64: bool = False        # mixed: every cell's con2prim ends with FP64 Newton iterations
 
     def cstruct(self) -> BhFxParams:
         r_exc = self.r_exc if self.r_exc is not None else (
             1.2 * horizon_radius(self.M, self.a) if self.M > 0 else 0.0)
         return BhFxParams(self.M, self.a, self.gamma, self.cfl, self.rho_floor, self.u_floor, self.sigma_max,
                           self.W_max, r_exc, self.tol, self.maxiter, LIMITERS[self.limiter],
-                          PRECISIONS[self.precision], 0)
+                          PRECISIONS[self.precision], 1 if self.c2p_fp64 else 0)
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:

@@ -55,6 +55,7 @@ inline FxPar par_of(const bh_fx_params* p) {
     q.gg = p->gamma / (p->gamma - 1.0);
     q.gf = (p->gamma - 1.0) / p->gamma;
     q.v2max = 1.0 - 1.0 / (p->W_max * p->W_max);
+    q.flags = p->flags;
     return q;
 }
 
@@ -167,10 +168,17 @@ __device__ inline double c2p_cell_fp64(const FxPar& P, const Grid& G, const bh_f
     const int64_t N = G.ncell;
     WT* W = (WT*)G.W;
     KS m;
-    ks_metric(P, x[0], x[1], x[2], m);
+    if (fp32_geometry<RT>(x)) {   // the mixed variant away from the hole: the FP32 metric
+        KSb<float> mf;
+        ks_metric<float>(P, float(x[0]), float(x[1]), float(x[2]), mf);
+        copy_metric(mf, m);
+    } else {
+        ks_metric(P, x[0], x[1], x[2], m);
+    }
     const double Bc[3] = {Bt[0] * m.alpha, Bt[1] * m.alpha, Bt[2] * m.alpha};   // B~ / sqrt(gamma)
     double w[8];
-    int rewrite = c2p_cell64<false>(P, G, m, U, W, N, c, Bc, w);
+    // (the mixed variant: up to four FP32 Newton iterations start the FP64 ones)
+    int rewrite = c2p_cell64<(sizeof(RT) < sizeof(double))>(P, G, m, U, W, N, c, Bc, w);
     if (apply_floors(P, m, w)) {
         rewrite = 1;
         atomicAdd(&G.count[1], 1);
@@ -265,7 +273,7 @@ __global__ void __launch_bounds__(FX_TPB, MINB) k_fx_c2p(FxPar P, Grid G, const 
             c2p_inputs(G, B, i, j, k, stage, x, Bt);
             constexpr bool MIXED = sizeof(RT) < sizeof(double);
             int full = 1;
-            if (MIXED && fp32_geometry<RT>(x)) {
+            if (MIXED && fp32_geometry<RT>(x) && !(P.flags & BH_FX_C2P_FP64)) {
                 full = c2p_cell_fp32(P, G, B, c, x, Bt, U, with_dt, dtc);
                 if (full) atomicAdd(&G.count[2], 1);
             }

@@ -70,6 +70,7 @@ struct FxPar {
     int maxiter, limiter;
     // derived once per launch: Gamma/(Gamma-1), (Gamma-1)/Gamma, the v^2 of W_max
     double gg, gf, v2max;
+    int flags;                // BH_FX_C2P_FP64
 };
 
 template <typename T>

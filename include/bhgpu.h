@@ -405,8 +405,13 @@ typedef struct bh_fx_params {
     int32_t maxiter;             /* con2prim Newton cap (30)                        */
     int32_t limiter;             /* BH_MINMOD / BH_VANLEER / BH_MC / BH_PPM         */
     int32_t precision;           /* BH_FP64 / BH_FP64_FMA / BH_MIXED                */
-    int32_t reserved;
+    int32_t flags;               /* BH_FX_C2P_FP64: in BH_MIXED, every cell's
+                                    con2prim ends with FP64 Newton iterations (by
+                                    default a cell whose FP32 iterations converge
+                                    on a well-conditioned residual keeps the FP32
+                                    root; the others end in FP64)                  */
 } bh_fx_params;
+#define BH_FX_C2P_FP64 1
 
 typedef struct bh_fx_block {
     int32_t n, level;

@@ -524,3 +524,23 @@ def test_packed_state_pipeline_equals_stepping_alone():
     pipe.synchronize()
     for out, r in zip(outs, refs):
         assert np.array_equal(out.numpy(), r)
+
+
+def test_mixed_with_fp64_final_con2prim_within_1e_5():
+    """the mixed variant with every cell's con2prim ending in FP64 Newton
+    iterations (BH_FX_C2P_FP64) after 20 steps of the 64^3 torus: relative L1
+    <= 1e-5 against FP64, no cell handed over from FP32, div B at roundoff"""
+    a = _grid(64, 64, "mixed", c2p_fp64=True)
+    b = _grid(64, 64, "fp64")
+    a.torus_init()
+    b.torus_init()
+    for _ in range(20):
+        a.step()
+        b.step()
+    torch.cuda.synchronize()
+    ua, ub = a.interior(a.U), b.interior(b.U)
+    for name, vs in FIELDS.items():
+        assert _rel_l1(ua[vs], ub[vs]) <= 1e-5, name
+    c = a.counters()
+    assert c["c2p_failures"] == 0 and c["c2p_fp64_fallback"] == 0
+    assert a.divb() <= 1e-12
