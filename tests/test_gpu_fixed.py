@@ -528,10 +528,10 @@ def test_packed_state_pipeline_equals_stepping_alone():
 
 def test_mixed_with_fp64_final_con2prim_within_1e_5():
     """the mixed variant with every cell's con2prim ending in FP64 Newton
-    iterations (BH_FX_C2P_FP64) after 20 steps of the 64^3 torus: relative L1
-    <= 1e-5 against FP64, no cell handed over from FP32, div B at roundoff"""
-    a = _grid(64, 64, "mixed", c2p_fp64=True)
-    b = _grid(64, 64, "fp64")
+    iterations (BH_FX_C2P_FP64) after 20 steps of the 128^3 torus: relative
+    L1 <= 1e-5 against FP64, no cell handed over from FP32, div B at roundoff"""
+    a = _grid(128, 128, "mixed", c2p_fp64=True)
+    b = _grid(128, 128, "fp64")
     a.torus_init()
     b.torus_init()
     for _ in range(20):
