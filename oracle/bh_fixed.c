@@ -196,16 +196,28 @@ static void speeds(const ksm* m, double gamma, int dd, const double* w, const dr
 
 /* ------------------------------------------------------------------ PLM */
 enum { LIM_MINMOD = 0, LIM_VANLEER = 1, LIM_MC = 2, LIM_PPM = 3 };
-static double slope(double dl, double dr, int lim) {
-    if (dl * dr <= 0.0) return 0.0;
-    if (lim == 1) return 2.0 * dl * dr / (dl + dr);
-    double al = dabs(dl), ar = dabs(dr);
-    double s = dl > 0.0 ? 1.0 : -1.0;
-    if (lim == 2) {
-        double c = 0.5 * (al + ar);
-        return s * dmin(c, 2.0 * dmin(al, ar));
+/* The face value of cell w0 toward its neighbour wn across the face, wf
+ * its other neighbour: w0 + sigma/2 with sigma the limited slope of
+ * (w0 - wf, wn - w0) (minmod, van Leer, MC; zero at an extremum).  At MC's
+ * bound sigma = 2 (wn - w0) the value is wn itself, and van Leer's with
+ * |wn - w0| < |w0 - wf| is formed from wn, so no difference of the two
+ * cells cancels against w0 (the device kernels' plm_value, same
+ * operations). */
+static double face_value(double wf, double w0, double wn, int lim) {
+    double df = w0 - wf, dn = wn - w0;
+    if (df * dn <= 0.0) return w0;
+    double af = dabs(df), an = dabs(dn);
+    if (lim == LIM_VANLEER) {
+        double q = df + dn;
+        return an < af ? wn - dn * dn / q : w0 + df * dn / q;
     }
-    return s * dmin(al, ar);
+    if (lim == LIM_MC) { /* sigma/2 = s min((af + an)/4, af, an) */
+        double t = dmin(0.25 * (af + an), af);
+        if (an < t) return wn;
+        return w0 + (dn > 0.0 ? t : -t);
+    }
+    double t = 0.5 * dmin(af, an);
+    return w0 + (dn > 0.0 ? t : -t);
 }
 
 /* PPM (Colella & Woodward 1984, J. Comput. Phys. 54, 174: eqs. 1.6-1.8 and
@@ -738,8 +750,8 @@ static void face(const fxo_params* P, const fxo_block* B, int64_t N, const doubl
             continue;
         }
         double a = W[v * N + c - 2 * st], b = W[v * N + c - st], cc = W[v * N + c], dd = W[v * N + c + st];
-        wL[v] = b + 0.5 * slope(b - a, cc - b, P->limiter);
-        wR[v] = cc - 0.5 * slope(cc - b, dd - cc, P->limiter);
+        wL[v] = face_value(a, b, cc, P->limiter);
+        wR[v] = face_value(dd, cc, b, P->limiter);
     }
     double Bn = Bfs[d * N + c] * m.alpha; /* alpha = 1 / sqrt(gamma) */
     wL[BB + d] = Bn;

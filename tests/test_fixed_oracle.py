@@ -499,3 +499,38 @@ def test_con2prim_from_the_previous_primitives_needs_about_two_evaluations():
     assert (st == 0).all() and (st_c == 0).all()
     assert it.mean() < 2.2 and it[torus].mean() < 2.2, (it.mean(), it[torus].mean())
     assert it_c.mean() > 4.0 and it_c[torus].mean() > 8.0, (it_c.mean(), it_c[torus].mean())
+
+
+def test_mc_face_value_at_a_jump_is_the_neighbours():
+    """Where MC's slope limit on the face side holds (sigma = 2 (wn - w0)),
+    the face value w0 + sigma/2 is the neighbour's value itself; the scheme
+    returns it exactly instead of forming w0 + (wn - w0), which next to a
+    floor-density cell (here 7e-8 beside 0.08) loses the small value's
+    digits.  Both face states of the face between an atmosphere cell and the
+    first dense cell are then the atmosphere cell's primitives, so the face
+    flux equals HLL of that state with itself, bit for bit."""
+    prm = Prm(M=0.0, a=0.0, r_exc=-1.0, rho_floor=1e-12, u_floor=1e-14, limiter="mc")
+    N = 16
+    h = _flat_grid(N, N, prm)
+
+    def state(X, Y, Z):
+        i = np.floor(X * N).astype(int)
+        w = np.zeros((8, X.size))
+        w[0] = np.where(i < 8, 7e-8, np.where(i == 8, 0.08, 0.37))
+        w[1] = np.where(i < 8, 4e-11, 1e-3 * w[0])
+        w[2] = 0.1
+        return w
+
+    _set_cells(h, state)
+    h.ghosts(0)
+    h.fluxes(0)
+    S = N + 2 * GB + 1
+
+    def at(i, j, k):
+        return ((i + GB) * S + (j + GB)) * S + (k + GB)
+    face, left = at(8, 5, 5), at(7, 5, 5)
+    w7 = h.W[:, left].copy()
+    w7[5] = h.Bf[0, face]       # the normal field comes from the face (alpha = 1 in flat space)
+    F = ofx.hll(h.prm, [0.5], [(5 + 0.5) / N], [(5 + 0.5) / N], 0, w7[:, None], w7[:, None])[:, 0]
+    got = h.F[0, :, face]
+    assert np.array_equal(got, F), (got, F)
