@@ -63,7 +63,9 @@ STEP_BYTES = 296          # algorithmic HBM bytes per zone-update of an RK2 step
 LAUNCHES_PER_STEP = 9     # dt init, then con2prim, ghosts, fluxes, update per stage (+1 per stage: split update)
 # DRAM bytes (read + write) per launch of the mixed variant's step kernels at
 # 128^3, from the ncu capture summarised in profiles/kernels_torus_128cube.md
-PROFILED_TRAFFIC = {"fluxes": 154.77e6 + 173.75e6, "update": 542.67e6 + 123.91e6, "prims": 190.97e6 + 143.72e6}
+# (the update as its two kernels, cells + faces: the autotuner's choice there)
+PROFILED_TRAFFIC = {"fluxes": 155.20e6 + 173.36e6, "update": (381.83e6 + 108.76e6) + (70.69e6 + 29.07e6),
+                    "prims": 190.98e6 + 145.83e6}
 E2E_DEPTH = 3
 
 
