@@ -476,11 +476,14 @@ def con2prim_batch(n_cells=1 << 24, reps=3):
         # the same with the network on the tensor cores (bh_ctop_learned)
         g.ctop_learned(U, rd, thd)
         torch.cuda.synchronize()
+        err_t = torch.zeros(1, dtype=torch.int32, device="cuda")   # checked after the loop: no sync per call
         a.record()
         for _ in range(reps):
-            Wt, Wdt, stt_, itt, pat = g.ctop_learned(U, rd, thd)
+            Wt, Wdt, stt_, itt, pat = g.ctop_learned(U, rd, thd, err=err_t)
         b.record(); torch.cuda.synchronize()
         mst = a.elapsed_time(b) / reps
+        if int(err_t.item()) != 0:
+            raise RuntimeError(f"bh_ctop_learned: device error word {int(err_t.item())} in the timed loop")
         # its second kernel alone (Newton / Brent from the same starting points)
         xi0t = g.ctop_learned(U, rd, thd, want_xi0=True)[5]
         torch.cuda.synchronize()

@@ -163,11 +163,14 @@ class C2PGuess:
                                 _stream()), "ctop with guess")
         return W, Wd, st, it, pa
 
-    def ctop_learned(self, U, r, th, want_xi0: bool = False):
+    def ctop_learned(self, U, r, th, want_xi0: bool = False, err: torch.Tensor | None = None):
         """The same as ctop() with the network on the tensor cores: one
         kernel for the metric, the preamble and the network, one for Newton
         (bh_ctop_learned).  Returns (W, Wd, status, iters, path) and, with
-        want_xi0, the starting points."""
+        want_xi0, the starting points.  err: a device int32 word of the
+        caller's that the call sets to BH_ERR_TIMEOUT if a tensor-core wait
+        ran out, left for the caller to check (the call then does not
+        synchronise); without it the call checks its own word and raises."""
         U, r, th = _dev(U, "cuda"), _dev(r, "cuda"), _dev(th, "cuda")
         n = U.shape[1]
         W = torch.empty((8, n), dtype=torch.float64, device=self.device)
@@ -176,12 +179,14 @@ class C2PGuess:
         it = torch.empty(n, dtype=torch.int32, device=self.device)
         pa = torch.empty(n, dtype=torch.int32, device=self.device)
         xi0 = torch.empty(n, dtype=torch.float64, device=self.device)
-        err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        own = err is None
+        if own:
+            err = torch.zeros(1, dtype=torch.int32, device=self.device)
         P = self._P()
         check(lib.bh_ctop_learned(C.byref(P), C.byref(self.s), _p(U), _p(r), _p(th), n,
                                   _p(xi0), _p(W), _p(Wd), _p(st), _p(it), _p(pa),
                                   _p(err), _stream()), "ctop with the tensor-core guess")
-        if int(err.item()) != 0:
+        if own and int(err.item()) != 0:
             raise RuntimeError(f"bh_ctop_learned: device error word {int(err.item())} (tensor-core wait ran out)")
         out = (W, Wd, st, it, pa)
         return out + (xi0,) if want_xi0 else out
