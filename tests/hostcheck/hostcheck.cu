@@ -8,6 +8,7 @@
 #include "bhgpu.h"
 #include "bh_items.cuh"
 #include "bh_init.cuh"
+#include "bh_fixed_phys.cuh"
 
 using namespace bh;
 
@@ -223,6 +224,15 @@ double hc_step(const bh_params* Pp, const bh_pool* pool, double cfl, const int32
     hc_rkstg(Pp, pool, dt, 1, waves, off, nwave);
     hc_floors(Pp, pool);
     return dt;
+}
+
+// the corrected scheme's PLM face value (bhfx::plm_value) of cell w0 toward
+// wn, wf its other neighbour, in double and in float (the inputs rounded)
+void hc_fx_plm(const double* wf, const double* w0, const double* wn, int lim, int64_t n, double* o64, float* o32) {
+    for (int64_t q = 0; q < n; q++) {
+        o64[q] = bhfx::plm_value<double>(wf[q], w0[q], wn[q], lim);
+        o32[q] = bhfx::plm_value<float>(float(wf[q]), float(w0[q]), float(wn[q]), lim);
+    }
 }
 
 }  // extern "C"

@@ -534,3 +534,58 @@ def test_mc_face_value_at_a_jump_is_the_neighbours():
     F = ofx.hll(h.prm, [0.5], [(5 + 0.5) / N], [(5 + 0.5) / N], 0, w7[:, None], w7[:, None])[:, 0]
     got = h.F[0, :, face]
     assert np.array_equal(got, F), (got, F)
+
+
+def _old_face_value(wf, w0, wn, lim):
+    """w0 + sigma/2 formed from the limited slope (the form before the face
+    value was taken from the neighbour at the slope limit), vectorised in
+    the arrays' own precision"""
+    t = w0.dtype.type
+    df, dn = w0 - wf, wn - w0
+    ext = df * dn <= t(0)
+    af, an = np.abs(df), np.abs(dn)
+    s = np.where(dn > t(0), t(1), t(-1)).astype(w0.dtype)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if lim == 1:
+            sig = t(2) * df * dn / (df + dn)
+        elif lim == 2:
+            sig = s * np.minimum(t(0.5) * (af + an), t(2) * np.minimum(af, an))
+        else:
+            sig = s * np.minimum(af, an)
+    return np.where(ext, w0, w0 + t(0.5) * sig)
+
+
+@pytest.mark.parametrize("lim", [0, 1, 2])
+def test_plm_face_value_rounds_as_the_slope_form(lim):
+    """The device's PLM face value (plm_value, built for the host with no
+    contraction), in double and in float, against w0 + sigma/2 from the
+    limited slope: bit for bit, except where the value reaches (MC) or
+    nears (van Leer, |dn| < |df|) the neighbour -- there it is the
+    neighbour itself (MC) or wn - dn^2/(df + dn) (van Leer)."""
+    import ctypes as C
+    from hostcheck import build, _d
+    L = C.CDLL(build())
+    rng = np.random.default_rng(11)
+    n = 400_000
+    sc = 10.0 ** rng.uniform(-8, 0, n)
+    wf, w0, wn = (rng.uniform(-1, 1, n) * sc * 10.0 ** rng.uniform(-3, 3, n) for _ in range(3))
+    o64, o32 = np.zeros(n), np.zeros(n, np.float32)
+    L.hc_fx_plm(_d(wf), _d(w0), _d(wn), C.c_int(lim), C.c_int64(n), _d(o64), _d(o32))
+    for got, (a, b, c) in ((o64, (wf, w0, wn)), (o32, tuple(v.astype(np.float32) for v in (wf, w0, wn)))):
+        t = b.dtype.type
+        old = _old_face_value(a, b, c, lim)
+        df, dn = b - a, c - b
+        af, an = np.abs(df), np.abs(dn)
+        live = df * dn > t(0)
+        if lim == 2:
+            near = live & (an < np.minimum(t(0.25) * (af + an), af))
+            assert np.array_equal(got[near], c[near])
+        elif lim == 1:
+            near = live & (an < af)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                assert np.array_equal(got[near], (c - dn * dn / (df + dn))[near])
+        else:
+            near = np.zeros(n, bool)
+        assert np.array_equal(got[~near], old[~near])
+        if lim:
+            assert near.sum() > 1000
