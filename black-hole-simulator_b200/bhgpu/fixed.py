@@ -76,7 +76,14 @@ def horizon_radius(M: float, a: float) -> float:
 
 @dataclass
 class FxParams:
-    """Physics and numerics of the corrected scheme (bh_fx_params)."""
+    """Physics and numerics of the corrected scheme (bh_fx_params).
+
+    The default floors are the Kerr torus configuration's atmosphere.  With
+    them the 128^3 torus runs cleanly for ~350 steps; after that a
+    floor-density cell above the torus reaches the W_max cap and the run
+    (FP64 as well as mixed) loses con2prim in a growing number of cells.
+    For longer runs rho_floor=1e-5, u_floor=1e-7 kept 800 steps free of
+    con2prim failures with W <= 1.5, as did W_max = 10 or 20."""
     M: float = 1.0
     a: float = 0.9375
     gamma: float = 4.0 / 3.0
