@@ -155,13 +155,22 @@ def gpu_uuid(dev):
         return None
 
 
+def l2_note(grid):
+    """the mixed step's working set against the 126 MB L2: per cell of a
+    block box U, U1 (FP64 x8), W (FP32 x8), face field and its stage copy
+    (FP64 x3 each), fluxes (FP32 x24) = 304 bytes"""
+    ws = (grid + 7) ** 3 * 304
+    rel = "exceeds" if ws > 126e6 else "fits in"
+    return f"working set {ws / 1e6:.0f} MB {rel} the 126 MB L2 (state, primitives, fluxes)"
+
+
 def arm_config(args, world):
     return {"workload": f"Kerr-Schild torus {args.grid}^3 (configuration 2): a=0.9375 over [-40,40]^3, "
                         "Fishbone-Moncrief r_in=6 r_max=12, Gamma=4/3, beta=100 single loop, 4% pressure noise, "
                         "excision r<1.2 r_H; corrected Valencia scheme, PLM MC + HLL + CT, RK2 CFL 0.4",
             "grid": f"{args.grid}^3", "blocks": (args.grid // args.block) ** 3,
             "block": f"{args.block}^3 + 3 ghost layers (2 filled for PLM)", "parallelism": f"replicas x{world}",
-            "l2": "working set > L2 (the 128^3 state, primitives and fluxes exceed 126 MB)",
+            "l2": l2_note(args.grid),
             "run": "steps 1..K from the torus initial data (re-initialised after the warm-up replays; "
                    "every step continues the last)"}
 
