@@ -5,8 +5,8 @@
 // Inference reads BF16 weights and accumulates in FP32; training keeps FP32
 // master weights, evaluates the forward pass with their BF16 roundings (the
 // weights inference will see), back-propagates in FP32 and takes Adam steps.
-// The solver's own FP64 con2prim produces the training pairs and stays the
-// judge: the guess only moves Newton's starting point.
+// The solver's own FP64 con2prim produces the training pairs and still
+// decides every cell: the guess only moves Newton's starting point.
 //
 // Parameters, FP32, one flat array (and its BF16 copy), in this order:
 //   W1 [64][6], b1 [64], W2 [64][64], b2 [64], W3 [2][64], b3 [2]
