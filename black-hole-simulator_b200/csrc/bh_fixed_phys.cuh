@@ -192,6 +192,7 @@ BH_FI void lower(const RT* g, const RT* v, RT* o) {
 template <typename RT>
 struct Derived {
     RT W, iW, rhoh, v[3], vl[3], Bl[3], B2, Bv, b2, rhohW2, ptot;
+    RT u2, ggp;   // W^2 - 1 = u_i u^i, and Gamma/(Gamma-1) p
 };
 template <typename RT>
 // gg = Gamma / (Gamma - 1)
@@ -201,6 +202,7 @@ BH_FI void derive(const KSm<RT>& m, RT gg, const RT* w, Derived<RT>& d) {
     RT utl[3];
     lower(m.g, ut, utl);
     RT u2 = utl[0] * ut[0] + utl[1] * ut[1] + utl[2] * ut[2];
+    d.u2 = u2;
     d.W = sqrt_(RT(1) + u2);
     RT iW = RT(1) / d.W;
     d.iW = iW;
@@ -209,7 +211,8 @@ BH_FI void derive(const KSm<RT>& m, RT gg, const RT* w, Derived<RT>& d) {
     d.B2 = d.Bl[0] * B[0] + d.Bl[1] * B[1] + d.Bl[2] * B[2];
     d.Bv = d.Bl[0] * d.v[0] + d.Bl[1] * d.v[1] + d.Bl[2] * d.v[2];
     d.b2 = d.B2 * iW * iW + d.Bv * d.Bv;
-    RT rhoh = w[P_RHO] + gg * w[P_PRS];
+    d.ggp = gg * w[P_PRS];
+    RT rhoh = w[P_RHO] + d.ggp;
     d.rhoh = rhoh;
     d.rhohW2 = rhoh * d.W * d.W;
     d.ptot = w[P_PRS] + RT(0.5) * d.b2;
@@ -222,8 +225,18 @@ BH_FI void prim2cons(const KSm<RT>& m, RT gamma, const RT* w, const Derived<RT>&
     u[C_D] = sg * w[P_RHO] * d.W;
     RT e = d.rhohW2 + d.B2;
     for (int i = 0; i < 3; i++) u[C_S + i] = sg * (e * d.vl[i] - d.Bv * d.Bl[i]);
-    RT E = d.rhohW2 - w[P_PRS] + RT(0.5) * d.B2 * (RT(1) + v2) - RT(0.5) * d.Bv * d.Bv;
-    u[C_TAU] = sg * E - u[C_D];
+    if (sizeof(RT) < sizeof(double)) {
+        // tau = sqrt(gamma) (E - rho W) from its non-negative parts, with
+        // W - 1 = u^2 / (1 + W): formed as sqrt(gamma) E - D it would carry
+        // an error of eps E, which for slow, cold gas (tau << E) is large
+        // relative to tau in FP32
+        RT e = w[P_RHO] * d.W * (d.u2 / (RT(1) + d.W)) + (d.ggp * d.W * d.W - w[P_PRS]) +
+               RT(0.5) * d.B2 * (RT(1) + v2) - RT(0.5) * d.Bv * d.Bv;
+        u[C_TAU] = sg * e;
+    } else {
+        RT E = d.rhohW2 - w[P_PRS] + RT(0.5) * d.B2 * (RT(1) + v2) - RT(0.5) * d.Bv * d.Bv;
+        u[C_TAU] = sg * E - u[C_D];
+    }
     for (int i = 0; i < 3; i++) u[C_B + i] = sg * w[P_B + i];
 }
 

@@ -235,4 +235,33 @@ void hc_fx_plm(const double* wf, const double* w0, const double* wn, int lim, in
     }
 }
 
+// the corrected scheme's prim2cons (derive + prim2cons) at Kerr-Schild
+// points x, y, z in double and in float (metric and primitives rounded):
+// u64[8][n], u32[8][n]
+void hc_fx_prim2cons(const bhfx::FxPar* P, const double* x, const double* y, const double* z, const double* w,
+                     int64_t n, double* u64, float* u32) {
+    for (int64_t q = 0; q < n; q++) {
+        double wd[8];
+        float wf[8];
+        for (int v = 0; v < 8; v++) { wd[v] = w[v * n + q]; wf[v] = float(wd[v]); }
+        bhfx::KS mk;
+        bhfx::ks_metric(*P, x[q], y[q], z[q], mk);
+        bhfx::KSm<double> md;
+        bhfx::ks_cast(mk, md);
+        bhfx::Derived<double> dd;
+        bhfx::derive(md, P->gg, wd, dd);
+        double ud[8];
+        bhfx::prim2cons(md, P->gamma, wd, dd, ud);
+        bhfx::KSb<float> mf;
+        bhfx::ks_metric<float>(*P, float(x[q]), float(y[q]), float(z[q]), mf);
+        bhfx::KSm<float> mm;
+        bhfx::ks_cast(mf, mm);
+        bhfx::Derived<float> df;
+        bhfx::derive(mm, float(P->gg), wf, df);
+        float uf[8];
+        bhfx::prim2cons(mm, float(P->gamma), wf, df, uf);
+        for (int v = 0; v < 8; v++) { u64[v * n + q] = ud[v]; u32[v * n + q] = uf[v]; }
+    }
+}
+
 }  // extern "C"

@@ -589,3 +589,45 @@ def test_plm_face_value_rounds_as_the_slope_form(lim):
         assert np.array_equal(got[~near], old[~near])
         if lim:
             assert near.sum() > 1000
+
+
+def test_fp32_tau_is_formed_without_cancellation():
+    """In FP32 the conserved energy tau = sqrt(gamma) (E - rho W) is formed
+    from its non-negative parts (rho W u^2/(1+W), p (Gamma W^2/(Gamma-1) - 1)
+    and the field terms), not as sqrt(gamma) E - D.  For slow, cold gas (tau
+    down to ~1e-4 of E) the FP32 tau (host build of the device code, metric
+    and primitives rounded to FP32) stays within 2e-6 of the FP64 tau
+    relative to tau itself; sqrt(gamma) E - D in FP32 would carry ~eps E/tau,
+    up to ~1e-3 here.  The FP64 form is the oracle's, bit for bit."""
+    import ctypes as C
+    from hostcheck import build, _d
+    L = C.CDLL(build())
+    rng = np.random.default_rng(5)
+    n = 20_000
+    x, y, z = sample_points(rng, n, rmin=4.5, rmax=40.0)
+    w = np.zeros((8, n))
+    w[0] = 10 ** rng.uniform(-7, 0, n)
+    w[1] = w[0] * 10 ** rng.uniform(-5, -2, n)
+    w[2:5] = rng.normal(size=(3, n)) * 10 ** rng.uniform(-3, -1, n)
+    w[5:8] = rng.normal(size=(3, n)) * np.sqrt(w[0] * 10 ** rng.uniform(-6, -3, n))
+    class FxPar(C.Structure):   # bhfx::FxPar
+        _fields_ = [(k, C.c_double) for k in ("M", "a", "gamma", "rho_fl", "u_fl", "sigma_max", "W_max", "r_exc",
+                                              "tol")] + [("maxiter", C.c_int), ("limiter", C.c_int)] + [
+            (k, C.c_double) for k in ("gg", "gf", "v2max")] + [("flags", C.c_int)]
+    g = 4.0 / 3.0
+    fxp = FxPar(M=1.0, a=0.9375, gamma=g, gg=g / (g - 1), gf=(g - 1) / g)
+    u64, u32 = np.zeros((8, n)), np.zeros((8, n), np.float32)
+    for a in (x, y, z):
+        assert a.flags["C_CONTIGUOUS"]
+    L.hc_fx_prim2cons(C.byref(fxp), _d(x), _d(y), _d(z), _d(w), C.c_int64(n), _d(u64), _d(u32))
+    tau, D = u64[4], u64[0]
+    E = tau + D
+    assert (tau / E).min() < 1e-3          # the cold, slow states the form is for
+    rel = np.abs(u32[4] - tau) / tau
+    assert rel.max() <= 2e-6, rel.max()
+    # the other conserved fields at FP32 rounding: D against itself, S
+    # against the size of its terms (E |u|)
+    assert (np.abs(u32[0] - D) / D).max() <= 2e-6
+    su = E * np.sqrt((w[2:5] ** 2).sum(0))
+    for v in (1, 2, 3):
+        assert (np.abs(u32[v] - u64[v]) / su).max() <= 2e-6, v
